@@ -1,0 +1,203 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the CPU oracles of the DIA.
+
+Two checkers, both CPU code, loaded only by tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of bench.py:
+
+* ``liboracle.so`` -- this project's plain-C restatement of INSNL1 and W3SNL1
+  (oracle/dia_body.h, following ww3-gpu kokkos/src/ww_kokkos/snl1_tables.cpp:82-329 and
+  snl1_team.hpp:351-497), in float32 (bit-exact form) and float64 (the FP64 DIA).
+* ``_ref/libref_snl1.so`` -- the reference's own C++ (snl1_tables.cpp, snl1_dia.cpp and its C
+  ABI shim snl1_shim.cpp) compiled unmodified against oracle/kokkos_compat; present when
+  oracle/Makefile's ``ref`` target ran where the reference is checked out.
+
+Arrays follow the reference's C ABI: a spectrum batch (nspec, npts) column-major is a numpy
+array of shape (npts, nspec) in C order.
+"""
+
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+REF_PATH = HERE / "_ref" / "libref_snl1.so"
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class Snl1Config(ctypes.Structure):
+    """W3GDATMD's DIA scalars in the order of ww::snl1::Config (snl1_config.hpp:54-70)."""
+
+    _fields_ = [("nk", ctypes.c_int), ("nth", ctypes.c_int)] + [
+        (n, ctypes.c_float) for n in ("xfr", "dth", "lam", "snlc1", "kdcon", "kdmn", "snls1",
+                                      "snls2", "snls3", "fachfe")]
+
+    FIELDS = ("nk", "nth", "xfr", "dth", "lam", "snlc1", "kdcon", "kdmn", "snls1", "snls2",
+              "snls3", "fachfe")
+
+    @classmethod
+    def from_mapping(cls, m):
+        return cls(*[m[k] for k in cls.FIELDS])
+
+
+def build():
+    """Compile liboracle.so (always) and the reference build (when the reference is present)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    ref = pathlib.Path(os.environ.get("WW_REFERENCE_ROOT", "/root/reference"))
+    if (ref / "kokkos/src/ww_kokkos/snl1_team.hpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        cfgp = ctypes.POINTER(Snl1Config)
+        L.oracle_insnl1_f32.argtypes = [cfgp, _f32p, _i32p, _f32p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.oracle_insnl1_f32.restype = ctypes.c_int
+        L.oracle_w3snl1_f32.argtypes = [cfgp, _f32p, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
+                                        _f32p, ctypes.c_int, ctypes.c_int]
+        L.oracle_w3snl1_f32.restype = ctypes.c_int
+        L.oracle_w3snl1_f64.argtypes = [cfgp, _f64p, ctypes.c_int, _f64p, _f64p, _f64p, _f64p,
+                                        _f64p, ctypes.c_int]
+        L.oracle_w3snl1_f64.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def insnl1(cfg, sig, o0_chain=False):
+    """INSNL1 tables: dict(scal, wts, ipim (16, nspecx), ic (16, nspec), af11), 0-based.
+
+    ``o0_chain`` multiplies AF11 = x**11 out as a -O0 gfortran build does (x^3 * x^8), the
+    build the reference's golden vector came from; the default is the -O3 power tree."""
+    L = lib()
+    c = Snl1Config.from_mapping(cfg)
+    sig = np.ascontiguousarray(sig, np.float32)
+    scal = np.zeros(5, np.int32)
+    wts = np.zeros(19, np.float32)
+    if L.oracle_insnl1_f32(ctypes.byref(c), sig, scal, wts, None, None, None, int(o0_chain)) != 0:
+        raise ValueError("INSNL1 refused the configuration")
+    nspecx, nspec = int(scal[3]), cfg["nk"] * cfg["nth"]
+    ipim = np.zeros((16, nspecx), np.int32)
+    ic = np.zeros((16, nspec), np.int32)
+    af11 = np.zeros(nspecx, np.float32)
+    L.oracle_insnl1_f32(ctypes.byref(c), sig, scal, wts, ipim.ctypes.data, ic.ctypes.data,
+                        af11.ctypes.data, int(o0_chain))
+    return {"scal": scal, "wts": wts, "ipim": ipim, "ic": ic, "af11": af11}
+
+
+def w3snl1(cfg, sig, a, cg, kdmean, nthreads=0, o0_chain=False):
+    """W3SNL1 in float32 on (npts, nspec) spectra; returns (s, d)."""
+    L = lib()
+    c = Snl1Config.from_mapping(cfg)
+    a = np.ascontiguousarray(a, np.float32)
+    cg = np.ascontiguousarray(cg, np.float32)
+    kd = np.ascontiguousarray(kdmean, np.float32)
+    s = np.empty_like(a)
+    d = np.empty_like(a)
+    if L.oracle_w3snl1_f32(ctypes.byref(c), np.ascontiguousarray(sig, np.float32), a.shape[0],
+                           a, cg, kd, s, d, nthreads, int(o0_chain)) != 0:
+        raise ValueError("W3SNL1 oracle refused the configuration")
+    return s, d
+
+
+def w3snl1_f64(cfg, sig, a, cg, kdmean, nthreads=0):
+    """The FP64 DIA: the same algorithm in double precision; returns (s, d) as float64."""
+    L = lib()
+    c = Snl1Config.from_mapping(cfg)
+    a = np.ascontiguousarray(a, np.float64)
+    s = np.empty_like(a)
+    d = np.empty_like(a)
+    if L.oracle_w3snl1_f64(ctypes.byref(c), np.ascontiguousarray(sig, np.float64), a.shape[0],
+                           a, np.ascontiguousarray(cg, np.float64),
+                           np.ascontiguousarray(kdmean, np.float64), s, d, nthreads) != 0:
+        raise ValueError("W3SNL1 oracle refused the configuration")
+    return s, d
+
+
+# ---------------------------------------------------------------- the reference's own build
+_ref = None
+
+
+def ref_available():
+    return REF_PATH.exists()
+
+
+def ref_lib():
+    """The reference's C ABI (ww_kokkos_init / ww_snl1_init / ww_snl1) plus ref_snl1_tables."""
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(str(REF_PATH), mode=ctypes.RTLD_LOCAL)
+        f = ctypes.c_float
+        L.ww_kokkos_init.argtypes = [ctypes.c_int]
+        L.ww_kokkos_init.restype = ctypes.c_int
+        L.ww_snl1_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [f] * 10 + [_f32p]
+        L.ww_snl1_init.restype = ctypes.c_int
+        L.ww_snl1.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p]
+        L.ww_snl1.restype = None
+        L.ww_snl1_last_error.restype = ctypes.c_int
+        L.ref_snl1_tables.argtypes = [ctypes.c_int, ctypes.c_int] + [f] * 10 + [
+            _f32p, _i32p, _f32p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p]
+        L.ref_snl1_tables.restype = ctypes.c_int
+        if L.ww_kokkos_init(-1) != 0:
+            raise RuntimeError("reference ww_kokkos_init failed")
+        _ref = L
+    return _ref
+
+
+def _cfg_args(cfg):
+    return [cfg[k] for k in Snl1Config.FIELDS[2:]]
+
+
+def ref_tables(cfg, sig):
+    L = ref_lib()
+    sig = np.ascontiguousarray(sig, np.float32)
+    scal = np.zeros(5, np.int32)
+    wts = np.zeros(19, np.float32)
+    halo = ctypes.c_int(0)
+    L.ref_snl1_tables(cfg["nk"], cfg["nth"], *_cfg_args(cfg), sig, scal, wts, None, None, None,
+                      ctypes.byref(halo))
+    nspecx, nspec = int(scal[3]), cfg["nk"] * cfg["nth"]
+    ipim = np.zeros((16, nspecx), np.int32)
+    ic = np.zeros((16, nspec), np.int32)
+    af11 = np.zeros(nspecx, np.float32)
+    L.ref_snl1_tables(cfg["nk"], cfg["nth"], *_cfg_args(cfg), sig, scal, wts, ipim.ctypes.data,
+                      ic.ctypes.data, af11.ctypes.data, ctypes.byref(halo))
+    return {"scal": scal, "wts": wts, "ipim": ipim, "ic": ic, "af11": af11, "halo": halo.value}
+
+
+class RefSnl1:
+    """The reference's W3SNL1 through its own C ABI (kokkos/src/fortran_iface/ww_kokkos_c.hpp)."""
+
+    def __init__(self, cfg, sig, igrid=1):
+        self.L = ref_lib()
+        self.igrid = igrid
+        self.nspec = cfg["nk"] * cfg["nth"]
+        rc = self.L.ww_snl1_init(igrid, cfg["nk"], cfg["nth"], *_cfg_args(cfg),
+                                 np.ascontiguousarray(sig, np.float32))
+        if rc != 0:
+            raise RuntimeError(f"reference ww_snl1_init returned {rc}")
+
+    def __call__(self, a, cg, kdmean, s=None, d=None):
+        a = np.ascontiguousarray(a, np.float32)
+        s = np.empty_like(a) if s is None else s
+        d = np.empty_like(a) if d is None else d
+        self.L.ww_snl1(self.igrid, a.shape[0], a, np.ascontiguousarray(cg, np.float32),
+                       np.ascontiguousarray(kdmean, np.float32), s, d)
+        rc = self.L.ww_snl1_last_error()
+        if rc != 0:
+            raise RuntimeError(f"reference ww_snl1 failed with status {rc}")
+        return s, d

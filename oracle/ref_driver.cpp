@@ -1,0 +1,51 @@
+// oracle/ref_driver.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// Flat extern "C" access to the INSNL1 tables of the reference's own C++
+// (ww::snl1::make_tables, ww3-gpu kokkos/src/ww_kokkos/snl1_tables.cpp:82-329), compiled from
+// the reference's sources by oracle/Makefile into oracle/_ref/libref_snl1.so. The reference's
+// W3SNL1 itself is reached through its own C ABI in the same library (ww_kokkos_init,
+// ww_snl1_init, ww_snl1: kokkos/src/fortran_iface/snl1_shim.cpp), so no driver is needed for
+// it. Used by the tests and by bench.py's reference arm only.
+#include <Kokkos_Core.hpp>
+
+#include "ww_kokkos/snl1_config.hpp"
+#include "ww_kokkos/snl1_tables.hpp"
+
+extern "C" int ref_snl1_tables(int nk, int nth, float xfr, float dth, float lam, float snlc1,
+                               float kdcon, float kdmn, float snls1, float snls2, float snls3,
+                               float fachfe, const float* sig, int* scal, float* wts,
+                               int* ipim, int* ic, float* af11, int* halo) {
+  const ww::snl1::Config c{nk, nth, xfr, dth, lam, snlc1, kdcon, kdmn, snls1, snls2, snls3, fachfe};
+  ww::snl1::HostRealView1D h_sig("sig", nk);
+  for (int k = 0; k < nk; ++k) h_sig(k) = sig[k];
+  const ww::snl1::Tables t = ww::snl1::make_tables(c, h_sig);
+  scal[0] = t.nfr;
+  scal[1] = t.nfrhgh;
+  scal[2] = t.nfrchg;
+  scal[3] = t.nspecx;
+  scal[4] = t.nspecy;
+  wts[0] = t.dal1;
+  wts[1] = t.dal2;
+  wts[2] = t.dal3;
+  for (int j = 0; j < 8; ++j) {
+    wts[3 + j] = t.awg[j];
+    wts[11 + j] = t.swg[j];
+  }
+  if (halo) *halo = t.halo;
+  if (ipim) {
+    for (int half = 0; half < 2; ++half)
+      for (int j = 0; j < 4; ++j)
+        for (int i = 0; i < t.nspecx; ++i) {
+          ipim[(half * 8 + j) * t.nspecx + i] = t.ip[half][j](i);
+          ipim[(half * 8 + 4 + j) * t.nspecx + i] = t.im[half][j](i);
+        }
+  }
+  if (ic) {
+    for (int j = 0; j < 8; ++j)
+      for (int col = 0; col < 2; ++col)
+        for (int i = 0; i < t.nspec; ++i) ic[(col * 8 + j) * t.nspec + i] = t.ic[j][col](i);
+  }
+  if (af11)
+    for (int i = 0; i < t.nspecx; ++i) af11[i] = t.af11(i);
+  return 0;
+}
