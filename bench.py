@@ -1,0 +1,333 @@
+"""Benchmark of the W3SNL1 (DIA) hot path on B200: sea-point·steps/s at 36x36 bins.
+
+One "step" is one W3SNL1 evaluation (the DIA nonlinear transfer S and its diagonal D) over
+every sea point of the batch. Workload: 36 x 36 spectra (frequencies geometric from 0.0373 Hz,
+ratio 1.1; 10-degree directions), seeded JONSWAP sea states in deep water (d = 4000 m) with
+Hs ~ U(0.5, 8) m, fp ~ U(0.06, 0.2) Hz, gamma ~ U(1, 5), cos^2s spreading s ~ U(2, 20), DIA
+constants lambda 0.25, C 2.78e7, KDCONV 0.75, KDMIN 0.5, CS1-3 5.5/0.833/-1.25; 262,144 sea
+points per GPU so that a pass (4.1 GB of algorithmic traffic) is 33x the L2.
+
+  value  -- device-resident: inputs in HBM, ww_snl1_device launched on torch's stream, CUDA
+            events around exactly K steps; sea-point·steps/s summed over ranks.
+  e2e    -- the public host entry ww_snl1 (ww_kokkos_c.hpp:115 semantics) on page-locked host
+            buffers: host->device copy of A/CG/KDMEAN and device->host copy of S/D inside
+            every step.
+  roofline -- the kernel's algorithmic HBM bytes (15,700 B per point: A, CG, KDMEAN in; S, D
+            out) per launch over its CUDA-event duration, against MEASURED_PEAKS.json's HBM
+            copy bandwidth.
+  cpu_baseline -- the reference's own C++ (oracle/_ref, compiled from its sources) on this
+            host's cores on a bounded sample, rank 0 only.
+
+--impl reference runs that CPU reference alone, with the same metric and config.
+Multi-GPU: the DIA is independent per sea point, so each rank runs its own points (weak
+scaling) with no collective on the data path; ranks meet only at the timing barriers.
+"""
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import __graft_entry__ as entry  # noqa: E402
+
+NPTS_PER_GPU = 262144
+NK = NTH = 36
+BYTES_PER_POINT = 4 * (NK * NTH + NK + 1 + 2 * NK * NTH)  # 15,700
+METRIC = "sea-point·steps/s at 36×36 bins: plain DIA vs gated surrogate, same Hs error"
+UNIT = "sea-point*steps/s"
+WORKLOAD = ("W3SNL1 DIA 36x36 (config 0 spectra: deep-water JONSWAP, d=4000 m), "
+            f"{NPTS_PER_GPU} sea points per GPU")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--npts", type=int, default=NPTS_PER_GPU)
+    p.add_argument("--e2e-steps", type=int, default=None)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def config(args, world):
+    return {"workload": WORKLOAD, "nk": NK, "nth": NTH, "npts_per_gpu": args.npts,
+            "global_points": args.npts * world, "depth_m": 4000.0, "seed": 2024,
+            "l2": "inputs+outputs 4.1 GB per pass > 126 MB L2 (no flush needed)",
+            "parallelism": f"points sharded over {world} GPU(s), no collective"}
+
+
+# ---------------------------------------------------------------------------- CPU reference
+def cpu_reference_rate(cfg, sig, g, seconds=10.0, max_points=4096):
+    """Points/s of the reference's C++ on the host cores (its own C ABI, OpenMP over points),
+    on a bounded sample of the workload; falls back to the oracle port when the reference
+    build is absent. Returns (rate, kind, cores, sample)."""
+    oracle = entry.load_oracle()
+    n = min(max_points, g["a"].shape[0])
+    a, cg, kd = g["a"][:n], g["cg"][:n], g["kdmean"][:n]
+    if oracle.ref_available():
+        run = oracle.RefSnl1(cfg, sig, igrid=1)
+        kind = "reference"
+        call = lambda: run(a, cg, kd)  # noqa: E731
+    else:
+        kind = "port"
+        call = lambda: oracle.w3snl1(cfg, sig, a, cg, kd)  # noqa: E731
+    call()  # warm-up
+    t0 = time.perf_counter()
+    calls = 0
+    while True:
+        call()
+        calls += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or calls >= 200:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return n * calls / el, kind, cores, f"{calls} calls x {n} points of the workload"
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    cfg, sig = synth.dia_config(NK, NTH)
+    n = 2048
+    g = synth.sea_states(n, seed=2024, depth=4000.0)
+    oracle = entry.load_oracle()
+    if oracle.ref_available():
+        run = oracle.RefSnl1(cfg, sig, igrid=1)
+        kind = "reference"
+        step = lambda: run(g["a"], g["cg"], g["kdmean"])  # noqa: E731
+    else:
+        kind = "port"
+        step = lambda: oracle.w3snl1(cfg, sig, g["a"], g["cg"], g["kdmean"])  # noqa: E731
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    rate = n * args.steps / el
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cfgd = config(args, 1)
+    cfgd["reference_sample_points_per_step"] = n
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": cfgd,
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{n} points of the workload per step, OpenMP over points"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------- B200 arm
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_point():
+    """DRAM bytes per sea point of the W3SNL1 kernel from the committed ncu capture summary
+    (profiles/snl1_rowshift_36x36.json), or None."""
+    p = ROOT / "profiles" / "snl1_rowshift_36x36.json"
+    if not p.exists():
+        return None
+    try:
+        j = json.loads(p.read_text())
+        return float(j["dram_bytes"]) / float(j["points"])
+    except Exception:
+        return None
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
+    torch.cuda.set_device(local)
+    os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    pkg = entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    cfg, sig = synth.dia_config(NK, NTH)
+    npts = args.npts
+    g = synth.sea_states_chunked(npts, seed=2024 + rank, depth=4000.0)
+    grid = pkg.Snl1Grid(cfg, sig, igrid=1)
+    dev = torch.device("cuda", local)
+    a = torch.from_numpy(g["a"]).to(dev)
+    cg = torch.from_numpy(g["cg"]).to(dev)
+    kd = torch.from_numpy(g["kdmean"]).to(dev)
+    s = torch.empty_like(a)
+    d = torch.empty_like(a)
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident value
+    for _ in range(args.warmup):
+        grid.run_device(npts, a, cg, kd, s, d, handle)
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)  # let the sampler start
+        barrier()
+        ev[0].record(stream)
+        for i in range(args.steps):
+            grid.run_device(npts, a, cg, kd, s, d, handle)
+            ev[i + 1].record(stream)
+        barrier()
+    per_launch_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    value = npts * world * args.steps / (total_ms / 1e3)
+    launch_ms = sum(per_launch_ms) / len(per_launch_ms)
+
+    # ---- end to end through the host entry, page-locked host buffers
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
+    h_a = torch.from_numpy(g["a"]).pin_memory()
+    h_cg = torch.from_numpy(g["cg"]).pin_memory()
+    h_kd = torch.from_numpy(g["kdmean"]).pin_memory()
+    h_s = torch.empty_like(h_a).pin_memory()
+    h_d = torch.empty_like(h_a).pin_memory()
+    grid.run_host(npts, h_a, h_cg, h_kd, h_s, h_d)  # warm-up (allocates the pipeline slots)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        grid.run_host(npts, h_a, h_cg, h_kd, h_s, h_d)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = npts * world * e2e_steps / e2e_s
+    same = bool(torch.equal(h_s.view(torch.int32), s.cpu().view(torch.int32)))
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = BYTES_PER_POINT * npts / (launch_ms / 1e3) / 1e9
+    tpp = ncu_traffic_per_point()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config(args, world),
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": int((h_a.numel() + h_cg.numel() + h_kd.numel()) * 4),
+                "d2h_bytes_per_step": int((h_s.numel() + h_d.numel()) * 4),
+                "steps": e2e_steps, "host_entry": "ww_snl1", "matches_device_entry": same},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": (tpp * npts if tpp else None),
+                     "kernel": "snl1_rowshift_kernel", "launch_ms": launch_ms,
+                     "algorithmic_bytes_per_point": BYTES_PER_POINT},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, sample = cpu_reference_rate(cfg, sig, g)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,115 @@
+/* include/ww_b200.h -- the C ABI of libww_b200.so.
+ *
+ * libww_b200.so is a drop-in for the C ABI that the WAVEWATCH III fork's run-time switch binds
+ * (ww3-gpu's kokkos/src/fortran_iface/ww_kokkos_c.hpp, resident_c.hpp and prop3_c.hpp): the
+ * same symbol names, argument order, Fortran column-major layouts and status codes, backed by
+ * hand-written CUDA kernels for B200 (sm_100a). Each declaration cites the reference entry it
+ * replaces. Entries marked "B200 extension" have no counterpart in the reference.
+ *
+ * Rules carried over from the reference ABI (ww_kokkos_c.hpp:6-33):
+ *  1. Arrays are Fortran-ordered (column-major), caller-owned and borrowed for the call.
+ *  2. float is WW3's default REAL; LOGICAL crosses as int 0/1.
+ *  3. Nothing throws across the boundary. Entries return or record a WwKokkosStatus, read back
+ *     with the part's *_last_error(); each failure prints one line to stderr. On a validation
+ *     failure nothing is written through output pointers. npts == 0 is a no-op.
+ *  4. Not thread-safe: one caller at a time. Contexts are kept per grid index `igrid`.
+ * The device is chosen by WW_KOKKOS_DEVICE_ID (default 0); the communicator is ignored.
+ */
+#ifndef WW_B200_H
+#define WW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: ww_kokkos_c.hpp:42-50 (same values). */
+enum WwKokkosStatus {
+  WW_KOKKOS_OK = 0,
+  WW_KOKKOS_ERR_NOT_INITIALISED = 1,
+  WW_KOKKOS_ERR_BAD_SHAPE = 2,
+  WW_KOKKOS_ERR_KERNEL = 3,
+  WW_KOKKOS_ERR_RUNTIME = 4,
+  WW_KOKKOS_ERR_UNSUPPORTED = 5,
+  WW_KOKKOS_ERR_TABLE = 6
+};
+
+/* ---------------------------------------------------------------- runtime */
+
+/* Replaces ww_kokkos_init (ww_kokkos_c.hpp:73): selects the CUDA device from
+ * WW_KOKKOS_DEVICE_ID, creates the library's streams, reads the run-time flags. Idempotent.
+ * Returns WW_KOKKOS_OK or WW_KOKKOS_ERR_RUNTIME (no usable CUDA device). */
+int ww_kokkos_init(int comm_f);
+
+/* Replaces ww_kokkos_finalize (ww_kokkos_c.hpp:79): frees every grid context and stream. Safe
+ * to call twice or before init. */
+void ww_kokkos_finalize(void);
+
+/* ---------------------------------------------------------------- W3SNL1 (the DIA) */
+
+/* Replaces ww_snl1_init (ww_kokkos_c.hpp:98-100): builds the INSNL1 tables of grid `igrid` on
+ * the host (the reference's snl1_tables.cpp:82-329 arithmetic) and uploads them. `sig` is
+ * SIG(1:nk), copied. Returns OK, NOT_INITIALISED, BAD_SHAPE or RUNTIME; on failure the grid is
+ * left unconfigured. */
+int ww_snl1_init(int igrid, int nk, int nth, float xfr, float dth, float lam, float snlc1,
+                 float kdcon, float kdmn, float snls1, float snls2, float snls3, float fachfe,
+                 const float* sig);
+
+/* B200 extension. Configures grid `igrid` from INSNL1 tables the caller already holds (WW3's
+ * own W3ADATMD arrays, so the device uses the Fortran build's exact AF11 bits), instead of
+ * rebuilding them. Same scalars as ww_snl1_init, then: scal[5] = NFR, NFRHGH, NFRCHG, NSPECX,
+ * NSPECY; wts[19] = DAL1..DAL3, AWG1..AWG8, SWG1..SWG8; ipim[16*NSPECX] = IP11..IP14,
+ * IM11..IM14, IP21..IP24, IM21..IM24; ic[16*NSPEC] = IC11, IC21 .. IC81, IC12 .. IC82;
+ * af11[NSPECX]. Index entries are 0-based (Fortran value minus one). Returns OK,
+ * NOT_INITIALISED, BAD_SHAPE (inconsistent sizes or an entry out of range) or RUNTIME. */
+int ww_snl1_init_tables(int igrid, int nk, int nth, float xfr, float dth, float lam,
+                        float snlc1, float kdcon, float kdmn, float snls1, float snls2,
+                        float snls3, float fachfe, const float* sig, const int* scal,
+                        const float* wts, const int* ipim, const int* ic, const float* af11);
+
+/* Replaces ww_snl1 (ww_kokkos_c.hpp:115-116): W3SNL1 for npts sea points from host memory.
+ * a, s, d are (nspec, npts), cg (nk, npts), kdmean (npts). s and d are overwritten. The copies
+ * in and out are pipelined with the kernel in chunks; page-locked caller memory copies fastest.
+ * Status in ww_snl1_last_error(). */
+void ww_snl1(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+             float* s, float* d);
+
+/* B200 extension. W3SNL1 on device-resident arrays (same shapes as ww_snl1), launched on the
+ * CUDA stream `stream` (a cudaStream_t; NULL is the legacy default stream) without any copy or
+ * synchronisation. Status in ww_snl1_last_error(); launch errors are reported, execution errors
+ * surface at the caller's next synchronisation. */
+void ww_snl1_device(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+                    float* s, float* d, void* stream);
+
+/* Replaces ww_snl1_enabled (ww_kokkos_c.hpp:120): 1 if WW_KOKKOS_SNL1 resolves to on (see
+ * ww_kokkos_flag) at ww_kokkos_init, else 0. */
+int ww_snl1_enabled(void);
+
+/* Replaces ww_snl1_last_error (ww_kokkos_c.hpp:133). */
+int ww_snl1_last_error(void);
+
+/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the row-shift kernel
+ * when INSNL1's tables have that form, else the gather kernel), 1 the gather kernel over the
+ * index tables, 2 the row-shift kernel. Returns the previous choice, or -1 for an unknown grid
+ * or a choice the grid's tables cannot run. */
+int ww_snl1_select_kernel(int igrid, int which);
+
+/* ---------------------------------------------------------------- run-time flags */
+
+/* Replace ww_kokkos_flag / preset_status / strict / fallback_slot / fallback_add
+ * (ww_kokkos_c.hpp:875-891, kokkos/src/fortran_iface/part_flags.cpp:67-135): a part's flag
+ * WW_KOKKOS_<PART> = "1" is on (1), any other value off; unset, WW_KOKKOS_PRESET=<name> turns on
+ * the parts of that preset (1), then WW_KOKKOS_ALL=1 turns on every part that is not opt-in (2).
+ * ww_kokkos_preset_status: 0 no preset, 1 known, -1 unknown name. ww_kokkos_strict: 1 when
+ * WW_KOKKOS_STRICT=1. The fallback slots count calls a caller left on the Fortran and print
+ * the counts once at exit. */
+int ww_kokkos_flag(const char* name);
+int ww_kokkos_preset_status(void);
+int ww_kokkos_strict(void);
+int ww_kokkos_fallback_slot(const char* part);
+void ww_kokkos_fallback_add(int slot);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WW_B200_H */

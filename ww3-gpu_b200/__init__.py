@@ -1,0 +1,208 @@
+"""ww3-gpu_b200: the W3SNL1 (DIA) hot path of WAVEWATCH III on B200 behind the reference's C ABI.
+
+The product is ``libww_b200.so`` (ww3-gpu_b200/csrc, CUDA for sm_100a), whose ``extern "C"``
+entry points are those the WW3 fork's run-time switch binds in the reference
+(ww3-gpu kokkos/src/fortran_iface/ww_kokkos_c.hpp:73-133; declared here in include/ww_b200.h).
+This module is the Python mirror of that interface: the same entry names, argument meaning and
+status codes, through ctypes, so a test reads like a call from the Fortran side.
+
+There is no CPU fallback: every compute call goes to the CUDA library, and loading fails
+loudly when the library is missing or no CUDA device is present.
+"""
+
+import ctypes
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libww_b200.so"
+CSRC = HERE / "csrc"
+
+# WwKokkosStatus (ww_kokkos_c.hpp:42-50)
+OK = 0
+ERR_NOT_INITIALISED = 1
+ERR_BAD_SHAPE = 2
+ERR_KERNEL = 3
+ERR_RUNTIME = 4
+ERR_UNSUPPORTED = 5
+ERR_TABLE = 6
+
+# ww_snl1_select_kernel choices
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT = 0, 1, 2
+
+# Every symbol include/ww_b200.h declares.
+EXPORTS = (
+    "ww_kokkos_init", "ww_kokkos_finalize", "ww_snl1_init", "ww_snl1_init_tables", "ww_snl1",
+    "ww_snl1_device", "ww_snl1_enabled", "ww_snl1_last_error", "ww_snl1_select_kernel",
+    "ww_kokkos_flag", "ww_kokkos_preset_status", "ww_kokkos_strict", "ww_kokkos_fallback_slot",
+    "ww_kokkos_fallback_add",
+)
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_F = ctypes.c_float
+_I = ctypes.c_int
+_P = ctypes.c_void_p
+
+
+def build(force=False):
+    """Compile libww_b200.so in-tree (nvcc, sm_100a)."""
+    if force or not LIB_PATH.exists():
+        subprocess.run(["make", "-s", "-C", str(CSRC)], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    """The loaded C ABI with argument types declared (loads, does not initialise CUDA)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with make -C {CSRC}")
+        L = ctypes.CDLL(str(LIB_PATH), mode=ctypes.RTLD_LOCAL)
+        L.ww_kokkos_init.argtypes = [_I]
+        L.ww_kokkos_init.restype = _I
+        L.ww_kokkos_finalize.argtypes = []
+        L.ww_kokkos_finalize.restype = None
+        L.ww_snl1_init.argtypes = [_I, _I, _I] + [_F] * 10 + [_f32p]
+        L.ww_snl1_init.restype = _I
+        L.ww_snl1_init_tables.argtypes = [_I, _I, _I] + [_F] * 10 + [_f32p, _i32p, _f32p, _i32p,
+                                                                      _i32p, _f32p]
+        L.ww_snl1_init_tables.restype = _I
+        L.ww_snl1.argtypes = [_I, _I, _P, _P, _P, _P, _P]
+        L.ww_snl1.restype = None
+        L.ww_snl1_device.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P]
+        L.ww_snl1_device.restype = None
+        L.ww_snl1_enabled.restype = _I
+        L.ww_snl1_last_error.restype = _I
+        L.ww_snl1_select_kernel.argtypes = [_I, _I]
+        L.ww_snl1_select_kernel.restype = _I
+        L.ww_kokkos_flag.argtypes = [ctypes.c_char_p]
+        L.ww_kokkos_flag.restype = _I
+        L.ww_kokkos_preset_status.restype = _I
+        L.ww_kokkos_strict.restype = _I
+        L.ww_kokkos_fallback_slot.argtypes = [ctypes.c_char_p]
+        L.ww_kokkos_fallback_slot.restype = _I
+        L.ww_kokkos_fallback_add.argtypes = [_I]
+        L.ww_kokkos_fallback_add.restype = None
+        _lib = L
+    return _lib
+
+
+class WwError(RuntimeError):
+    def __init__(self, where, code):
+        super().__init__(f"{where} failed with status {code}")
+        self.code = code
+
+
+def init(comm_f=-1):
+    """ww_kokkos_init: select the device (WW_KOKKOS_DEVICE_ID) and start the runtime."""
+    rc = lib().ww_kokkos_init(comm_f)
+    if rc != OK:
+        raise WwError("ww_kokkos_init", rc)
+
+
+def finalize():
+    lib().ww_kokkos_finalize()
+
+
+def last_error():
+    return lib().ww_snl1_last_error()
+
+
+# W3GDATMD's DIA scalars in the order of ww_snl1_init (ww_kokkos_c.hpp:98-100).
+SNL1_FIELDS = ("nk", "nth", "xfr", "dth", "lam", "snlc1", "kdcon", "kdmn", "snls1", "snls2",
+               "snls3", "fachfe")
+
+
+def _ptr(x):
+    """Data pointer of a C-contiguous numpy array or torch tensor."""
+    if isinstance(x, np.ndarray):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return x.data_ptr()
+    raise TypeError(type(x))
+
+
+class Snl1Grid:
+    """One WW3 grid's W3SNL1 context (the reference's ww_snl1_init / ww_snl1 pair).
+
+    Arrays use the C ABI layout: a (nspec, npts) Fortran array is a C-ordered (npts, nspec)
+    array here, (nk, npts) is (npts, nk)."""
+
+    def __init__(self, cfg, sig, igrid=1, tables=None):
+        self.L = lib()
+        init()
+        self.igrid = igrid
+        self.cfg = dict(cfg)
+        self.nk, self.nth = int(cfg["nk"]), int(cfg["nth"])
+        self.nspec = self.nk * self.nth
+        args = [cfg[k] for k in SNL1_FIELDS[2:]]
+        sig = np.ascontiguousarray(sig, np.float32)
+        if tables is None:
+            rc = self.L.ww_snl1_init(igrid, self.nk, self.nth, *args, sig)
+        else:
+            rc = self.L.ww_snl1_init_tables(
+                igrid, self.nk, self.nth, *args, sig,
+                np.ascontiguousarray(tables["scal"], np.int32),
+                np.ascontiguousarray(tables["wts"], np.float32),
+                np.ascontiguousarray(tables["ipim"], np.int32),
+                np.ascontiguousarray(tables["ic"], np.int32),
+                np.ascontiguousarray(tables["af11"], np.float32))
+        if rc != OK:
+            raise WwError("ww_snl1_init", rc)
+
+    def select_kernel(self, which):
+        prev = self.L.ww_snl1_select_kernel(self.igrid, which)
+        if prev < 0:
+            raise ValueError(f"kernel {which} not available for grid {self.igrid}")
+        return prev
+
+    def __call__(self, a, cg, kdmean, s=None, d=None):
+        """ww_snl1 on host arrays: copy in, kernel, copy out. Returns (s, d)."""
+        a = np.ascontiguousarray(a, np.float32)
+        cg = np.ascontiguousarray(cg, np.float32)
+        kd = np.ascontiguousarray(kdmean, np.float32)
+        npts = a.shape[0] if a.ndim == 2 else 0
+        self._check(a, cg, kd, npts)
+        s = np.empty_like(a) if s is None else s
+        d = np.empty_like(a) if d is None else d
+        self.L.ww_snl1(self.igrid, npts, _ptr(a), _ptr(cg), _ptr(kd), _ptr(s), _ptr(d))
+        rc = last_error()
+        if rc != OK:
+            raise WwError("ww_snl1", rc)
+        return s, d
+
+    def run_host(self, npts, a, cg, kdmean, s, d):
+        """ww_snl1 on caller-owned host buffers (numpy arrays or pinned torch tensors)."""
+        self.L.ww_snl1(self.igrid, npts, _ptr(a), _ptr(cg), _ptr(kdmean), _ptr(s), _ptr(d))
+        rc = last_error()
+        if rc != OK:
+            raise WwError("ww_snl1", rc)
+
+    def run_device(self, npts, a, cg, kdmean, s, d, stream=0):
+        """ww_snl1_device on device tensors, launched on CUDA stream handle ``stream``."""
+        self.L.ww_snl1_device(self.igrid, npts, _ptr(a), _ptr(cg), _ptr(kdmean), _ptr(s),
+                              _ptr(d), ctypes.c_void_p(stream))
+        rc = last_error()
+        if rc != OK:
+            raise WwError("ww_snl1_device", rc)
+
+    def _check(self, a, cg, kd, npts):
+        if a.ndim != 2 or a.shape[1] != self.nspec:
+            raise ValueError(f"a must be (npts, {self.nspec})")
+        if cg.shape != (npts, self.nk) or kd.shape != (npts,):
+            raise ValueError("cg must be (npts, nk) and kdmean (npts,)")
+
+
+def flag(name):
+    return lib().ww_kokkos_flag(name.encode())

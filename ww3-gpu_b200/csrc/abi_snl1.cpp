@@ -1,0 +1,352 @@
+// ww3-gpu_b200/csrc/abi_snl1.cpp
+// The W3SNL1 half of the C ABI: per-grid contexts (INSNL1 tables on the device), the
+// host-pointer entry ww_snl1 with its copies pipelined against the kernel, and the
+// device-resident entry ww_snl1_device.
+//
+// Reference: ww3-gpu kokkos/src/fortran_iface/snl1_shim.cpp:254-415 (validation order, status
+// codes, "nothing written on a validation failure", npts == 0 no-op, one context per igrid in a
+// never-destroyed map) and ww_kokkos_c.hpp:81-133.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "snl1_kernel.cuh"
+#include "snl1_tables.hpp"
+#include "wwb_common.hpp"
+
+namespace wwb {
+namespace {
+
+/// A device allocation owned by a context.
+template <class T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    reset();
+    if (count == 0) return;
+    WWB_CHECK(cudaMalloc(&ptr, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* host, size_t count) {
+    alloc(count);
+    if (count) WWB_CHECK(cudaMemcpy(ptr, host, count * sizeof(T), cudaMemcpyHostToDevice));
+  }
+};
+
+/// Host-pointer pipeline: kSlots chunks in flight, each on its own stream, so the H2D copy of
+/// one chunk, the kernel of the next and the D2H copy of a third overlap.
+constexpr int kSlots = 3;
+constexpr int kChunkPoints = 8192;
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  DevBuf<float> a, cg, kd, s, d;
+};
+
+struct Ctx {
+  Snl1Config cfg{};
+  Snl1Tables tab;
+  Snl1Dev dev{};
+  int kernel = kSnl1Auto;
+  DevBuf<float> sig, af11, af11_row;
+  DevBuf<int> ipim, ic, ifrow;
+  Slot slots[kSlots];
+  int slot_capacity = 0;
+  bool ready = false;
+  ~Ctx() {
+    for (auto& sl : slots)
+      if (sl.stream) cudaStreamDestroy(sl.stream);
+  }
+};
+
+std::map<int, Ctx*>& contexts() {
+  static auto* m = new std::map<int, Ctx*>();
+  return *m;
+}
+
+Status g_status;
+
+void erase(int igrid) {
+  auto& m = contexts();
+  auto it = m.find(igrid);
+  if (it != m.end()) {
+    delete it->second;
+    m.erase(it);
+  }
+}
+
+/// Uploads the tables of `c` and fills its kernel parameters.
+void publish(Ctx& c) {
+  const Snl1Tables& t = c.tab;
+  c.ipim.upload(t.ipim.data(), t.ipim.size());
+  c.ic.upload(t.ic.data(), t.ic.size());
+  c.af11.upload(t.af11.data(), t.af11.size());
+  if (t.rowshift) {
+    c.ifrow.upload(t.ifrow.data(), t.ifrow.size());
+    c.af11_row.upload(t.af11_row.data(), t.af11_row.size());
+  }
+  Snl1Dev& p = c.dev;
+  p = Snl1Dev{};
+  p.nk = c.cfg.nk;
+  p.nth = c.cfg.nth;
+  p.nfr = t.nfr;
+  p.nfrhgh = t.nfrhgh;
+  p.nfrchg = t.nfrchg;
+  p.nspec = t.nspec;
+  p.nspecx = t.nspecx;
+  p.dal1 = t.dal1;
+  p.dal2 = t.dal2;
+  p.dal3 = t.dal3;
+  for (int j = 0; j < 8; ++j) {
+    p.awg[j] = t.awg[j];
+    p.swg[j] = t.swg[j];
+    p.shift[j] = t.shift[j];
+  }
+  p.snlc1 = c.cfg.snlc1;
+  p.kdcon = c.cfg.kdcon;
+  p.kdmn = c.cfg.kdmn;
+  p.snls1 = c.cfg.snls1;
+  p.snls2 = c.cfg.snls2;
+  p.snls3 = c.cfg.snls3;
+  p.fachfe = c.cfg.fachfe;
+  p.ifrow = c.ifrow.ptr;
+  p.af11_row = c.af11_row.ptr;
+  p.ipim = c.ipim.ptr;
+  p.ic = c.ic.ptr;
+  p.af11 = c.af11.ptr;
+  c.kernel = t.rowshift ? kSnl1RowShift : kSnl1Gather;
+}
+
+int resolve_kernel(const Ctx& c) { return c.kernel; }
+
+/// Common validation of the compute entries; returns the context or nullptr (status set).
+Ctx* validate(int igrid, int npts, const void* a, const void* cg, const void* kd, const void* s,
+              const void* d, const char* who) {
+  auto it = contexts().find(igrid);
+  if (it == contexts().end() || !it->second->ready || !runtime().ready) {
+    g_status.fail(WW_KOKKOS_ERR_NOT_INITIALISED, "ww_snl1 before ww_snl1_init for this grid");
+    return nullptr;
+  }
+  if (npts < 0) {
+    g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1: npts is negative");
+    return nullptr;
+  }
+  if (npts == 0) {
+    g_status.ok();
+    return nullptr;
+  }
+  if (!a || !cg || !kd || !s || !d) {
+    g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1: null array pointer");
+    return nullptr;
+  }
+  (void)who;
+  return it->second;
+}
+
+int init_common(int igrid, const Snl1Config& cfg, const float* sig, Snl1Tables&& tab) {
+  Ctx* c = new Ctx();
+  try {
+    c->cfg = cfg;
+    c->tab = std::move(tab);
+    std::vector<float> h_sig(sig, sig + cfg.nk);
+    c->sig.upload(h_sig.data(), h_sig.size());
+    publish(*c);
+    c->dev.sig = c->sig.ptr;
+    for (auto& sl : c->slots) WWB_CHECK(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+    c->ready = true;
+  } catch (...) {
+    delete c;
+    throw;
+  }
+  contexts()[igrid] = c;
+  g_status.ok();
+  return WW_KOKKOS_OK;
+}
+
+}  // namespace
+
+void release_snl1_contexts() {
+  auto& m = contexts();
+  for (auto& kv : m) delete kv.second;
+  m.clear();
+}
+
+}  // namespace wwb
+
+using namespace wwb;
+
+extern "C" {
+
+int ww_snl1_init(int igrid, int nk, int nth, float xfr, float dth, float lam, float snlc1,
+                 float kdcon, float kdmn, float snls1, float snls2, float snls3, float fachfe,
+                 const float* sig) {
+  try {
+    erase(igrid);  // a failure below leaves the grid unconfigured, not half-configured
+    if (!runtime().ready)
+      return g_status.fail(WW_KOKKOS_ERR_NOT_INITIALISED, "ww_snl1_init before ww_kokkos_init");
+    if (nk <= 0 || nth <= 0 || sig == nullptr)
+      return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE,
+                           "ww_snl1_init: nk and nth must be > 0 and sig non-null");
+    const Snl1Config cfg{nk, nth, xfr, dth, lam, snlc1, kdcon, kdmn, snls1, snls2, snls3, fachfe};
+    Snl1Tables tab;
+    if (!build_snl1_tables(cfg, sig, tab))
+      return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1_init: no extended spectrum");
+    return init_common(igrid, cfg, sig, std::move(tab));
+  } catch (const std::bad_alloc& e) {
+    erase(igrid);
+    return g_status.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  } catch (const std::exception& e) {
+    erase(igrid);
+    return g_status.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  }
+}
+
+int ww_snl1_init_tables(int igrid, int nk, int nth, float xfr, float dth, float lam,
+                        float snlc1, float kdcon, float kdmn, float snls1, float snls2,
+                        float snls3, float fachfe, const float* sig, const int* scal,
+                        const float* wts, const int* ipim, const int* ic, const float* af11) {
+  try {
+    erase(igrid);
+    if (!runtime().ready)
+      return g_status.fail(WW_KOKKOS_ERR_NOT_INITIALISED,
+                           "ww_snl1_init_tables before ww_kokkos_init");
+    if (nk <= 0 || nth <= 0 || !sig || !scal || !wts || !ipim || !ic || !af11)
+      return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE,
+                           "ww_snl1_init_tables: bad extents or null pointer");
+    const Snl1Config cfg{nk, nth, xfr, dth, lam, snlc1, kdcon, kdmn, snls1, snls2, snls3, fachfe};
+    Snl1Tables t;
+    t.nth = nth;
+    t.nspec = nk * nth;
+    t.nfr = scal[0];
+    t.nfrhgh = scal[1];
+    t.nfrchg = scal[2];
+    t.nspecx = scal[3];
+    t.nspecy = scal[4];
+    if (t.nfr != nk || t.nfrchg < t.nfr || t.nfrhgh < t.nfrchg || t.nspecx != t.nfrchg * nth ||
+        t.nspecy != t.nfrhgh * nth)
+      return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1_init_tables: inconsistent sizes");
+    t.dal1 = wts[0];
+    t.dal2 = wts[1];
+    t.dal3 = wts[2];
+    for (int j = 0; j < 8; ++j) {
+      t.awg[j] = wts[3 + j];
+      t.swg[j] = wts[11 + j];
+    }
+    t.ipim.assign(ipim, ipim + 16 * static_cast<size_t>(t.nspecx));
+    t.ic.assign(ic, ic + 16 * static_cast<size_t>(t.nspec));
+    t.af11.assign(af11, af11 + t.nspecx);
+    // Every entry must address the scratch range the kernels hold: UE slots for the
+    // interaction tables, interaction-array slots for IC.
+    for (int v : t.ipim)
+      if (v + nth < 0 || v + nth >= t.nspecy + nth)
+        return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1_init_tables: IP/IM out of range");
+    for (int v : t.ic)
+      if (v + nth < 0 || v + nth >= t.nspecx + nth)
+        return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1_init_tables: IC out of range");
+    derive_rowshift(cfg, t);
+    return init_common(igrid, cfg, sig, std::move(t));
+  } catch (const std::bad_alloc& e) {
+    erase(igrid);
+    return g_status.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  } catch (const std::exception& e) {
+    erase(igrid);
+    return g_status.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  }
+}
+
+void ww_snl1(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+             float* s, float* d) {
+  try {
+    Ctx* c = validate(igrid, npts, a, cg, kdmean, s, d, "ww_snl1");
+    if (c == nullptr) return;
+    timers::Region t_call("snl1.call");
+    const int nspec = c->cfg.nspec(), nk = c->cfg.nk;
+    const int chunk = std::min(npts, kChunkPoints);
+    if (chunk > c->slot_capacity) {
+      for (auto& sl : c->slots) {
+        WWB_CHECK(cudaStreamSynchronize(sl.stream));
+        sl.a.alloc(static_cast<size_t>(chunk) * nspec);
+        sl.cg.alloc(static_cast<size_t>(chunk) * nk);
+        sl.kd.alloc(static_cast<size_t>(chunk));
+        sl.s.alloc(static_cast<size_t>(chunk) * nspec);
+        sl.d.alloc(static_cast<size_t>(chunk) * nspec);
+      }
+      c->slot_capacity = chunk;
+    }
+    const int kernel = resolve_kernel(*c);
+    int k = 0;
+    for (int p0 = 0; p0 < npts; p0 += chunk, ++k) {
+      Slot& sl = c->slots[k % kSlots];
+      const int n = std::min(chunk, npts - p0);
+      const size_t ns = static_cast<size_t>(n) * nspec;
+      WWB_CHECK(cudaMemcpyAsync(sl.a.ptr, a + static_cast<size_t>(p0) * nspec, ns * 4,
+                                cudaMemcpyHostToDevice, sl.stream));
+      WWB_CHECK(cudaMemcpyAsync(sl.cg.ptr, cg + static_cast<size_t>(p0) * nk,
+                                static_cast<size_t>(n) * nk * 4, cudaMemcpyHostToDevice,
+                                sl.stream));
+      WWB_CHECK(cudaMemcpyAsync(sl.kd.ptr, kdmean + p0, static_cast<size_t>(n) * 4,
+                                cudaMemcpyHostToDevice, sl.stream));
+      launch_snl1(kernel, c->dev, n, sl.a.ptr, sl.cg.ptr, sl.kd.ptr, sl.s.ptr, sl.d.ptr,
+                  sl.stream);
+      WWB_CHECK(cudaMemcpyAsync(s + static_cast<size_t>(p0) * nspec, sl.s.ptr, ns * 4,
+                                cudaMemcpyDeviceToHost, sl.stream));
+      WWB_CHECK(cudaMemcpyAsync(d + static_cast<size_t>(p0) * nspec, sl.d.ptr, ns * 4,
+                                cudaMemcpyDeviceToHost, sl.stream));
+    }
+    for (auto& sl : c->slots) WWB_CHECK(cudaStreamSynchronize(sl.stream));
+    g_status.ok();
+  } catch (const CudaError& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  } catch (const std::bad_alloc& e) {
+    g_status.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  } catch (const std::exception& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
+void ww_snl1_device(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+                    float* s, float* d, void* stream) {
+  try {
+    Ctx* c = validate(igrid, npts, a, cg, kdmean, s, d, "ww_snl1_device");
+    if (c == nullptr) return;
+    launch_snl1(resolve_kernel(*c), c->dev, npts, a, cg, kdmean, s, d,
+                static_cast<cudaStream_t>(stream));
+    g_status.ok();
+  } catch (const CudaError& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  } catch (const std::exception& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
+int ww_snl1_enabled(void) { return ww_kokkos_flag("WW_KOKKOS_SNL1") != 0 ? 1 : 0; }
+
+int ww_snl1_last_error(void) { return g_status.get(); }
+
+int ww_snl1_select_kernel(int igrid, int which) {
+  auto it = contexts().find(igrid);
+  if (it == contexts().end() || !it->second->ready) return -1;
+  Ctx& c = *it->second;
+  if (which == kSnl1RowShift && !c.tab.rowshift) return -1;
+  if (which < kSnl1Auto || which > kSnl1RowShift) return -1;
+  const int prev = c.kernel;
+  c.kernel = which == kSnl1Auto ? (c.tab.rowshift ? kSnl1RowShift : kSnl1Gather) : which;
+  return prev;
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// ww3-gpu_b200/csrc/snl1_kernel.cuh
+// W3SNL1 (the DIA) on B200: kernel parameters and launchers.
+//
+// Reference: ww3-gpu kokkos/src/ww_kokkos/snl1_team.hpp:351-497 (WW3 w3snl1md.F90 W3SNL1,
+// lines 115-473) and its batch launch snl1_dia.cpp:30-69.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace wwb {
+
+/// Everything the DIA kernels read besides the batch, passed by value as a kernel parameter.
+struct Snl1Dev {
+  int nk, nth, nfr, nfrhgh, nfrchg, nspec, nspecx;
+  float dal1, dal2, dal3;
+  float awg[8], swg[8];
+  float snlc1, kdcon, kdmn, snls1, snls2, snls3, fachfe;
+  int shift[8];             ///< row-shift form: IT_n(ITH) - ITH
+  const int* ifrow;         ///< device, 8 x NFRCHG (row-shift form)
+  const float* af11_row;    ///< device, NFRCHG (row-shift form)
+  const int* ipim;          ///< device, 16 x NSPECX (gather form)
+  const int* ic;            ///< device, 16 x NSPEC (gather form)
+  const float* af11;        ///< device, NSPECX (gather form)
+  const float* sig;         ///< device, NK
+};
+
+enum Snl1Kernel { kSnl1Auto = 0, kSnl1Gather = 1, kSnl1RowShift = 2 };
+
+/// Dynamic shared memory of each kernel, bytes.
+size_t snl1_gather_smem(const Snl1Dev& p);
+size_t snl1_rowshift_smem(const Snl1Dev& p);
+
+/// Launch W3SNL1 on npts points; a, s, d (nspec, npts) and cg (nk, npts) column-major,
+/// kdmean (npts), all device pointers. Throws CudaError on a launch failure.
+void launch_snl1(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
+                 const float* kdmean, float* s, float* d, cudaStream_t stream);
+
+}  // namespace wwb
