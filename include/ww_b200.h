@@ -93,6 +93,50 @@ int ww_snl1_last_error(void);
  * or a choice the grid's tables cannot run. */
 int ww_snl1_select_kernel(int igrid, int which);
 
+/* ---------------------------------------------------------------- the resident spectrum VA */
+/* VA(NSPEC, 0:NSEALM) of grid igrid, kept in HBM beside the Fortran array (resident_c.hpp:1-42).
+ * `va` is VA(1,0), nspec = SIZE(VA,1), nsealm = UBOUND(VA,2); the first call binds the grid to
+ * them and later calls with another address or shape are BAD_SHAPE. Return WwKokkosStatus. */
+
+/* Replaces ww_va_host_read (resident_c.hpp:46): before a host read of VA, copy d_va back when
+ * the device holds the newer bits; state BOTH. */
+int ww_va_host_read(int igrid, float* va, int nspec, int nsealm);
+
+/* Replaces ww_va_host_write (resident_c.hpp:49): ww_va_host_read, then state HOST. */
+int ww_va_host_write(int igrid, float* va, int nspec, int nsealm);
+
+/* Replaces ww_va_host_read_cols (resident_c.hpp:58): with state DEVICE, copy back only the
+ * columns cols[0..ncol) (0..nsealm, duplicates allowed), gathered on the device; state kept. */
+int ww_va_host_read_cols(int igrid, float* va, int nspec, int nsealm, int ncol, const int* cols);
+
+/* Replaces ww_va_host_wrote_cols (resident_c.hpp:69): after host statements wrote exactly the
+ * columns cols, with state DEVICE or BOTH push those columns into d_va; state kept. */
+int ww_va_host_wrote_cols(int igrid, float* va, int nspec, int nsealm, int ncol, const int* cols);
+
+/* Replaces ww_va_host_update (resident_c.hpp:75): before a host statement whose only writes of
+ * VA zero whole columns; binds or checks, no copy. */
+int ww_va_host_update(int igrid, float* va, int nspec, int nsealm);
+
+/* Replaces ww_va_device_zero_cols (resident_c.hpp:84-85): d_va(:, cols) = 0 when the device
+ * copy is newer or equal; state kept. */
+int ww_va_device_zero_cols(int igrid, float* va, int nspec, int nsealm, int ncol,
+                           const int* cols);
+
+/* Replaces ww_va_device (resident_c.hpp:89): before a launch reads d_va of a bound grid: HOST
+ * -> one H2D copy, state BOTH; write = 1 then marks DEVICE. */
+int ww_va_device(int igrid, int write);
+
+/* Replaces ww_va_report (resident_c.hpp:92): copy counters to stderr (at exit under
+ * WW_KOKKOS_VA_COUNT=1). */
+void ww_va_report(void);
+
+/* B200 extension: the device address of grid igrid's d_va (NULL before its first device
+ * sync), so a caller can run its own device code on the resident spectrum. */
+void* ww_va_device_ptr(int igrid);
+
+/* B200 extension: the state of grid igrid's VA: 0 HOST, 1 DEVICE, 2 BOTH, -1 unbound. */
+int ww_va_state(int igrid);
+
 /* ---------------------------------------------------------------- run-time flags */
 
 /* Replace ww_kokkos_flag / preset_status / strict / fallback_slot / fallback_add

@@ -440,6 +440,9 @@ struct Schedule { using type = T; };
 template <class T>
 struct IndexType { using type = T; };
 
+struct ParallelForTag {};
+struct ParallelReduceTag {};
+
 struct PerTeamValue { std::size_t value; };
 struct PerThreadValue { std::size_t value; };
 inline PerTeamValue PerTeam(std::size_t v) { return PerTeamValue{v}; }

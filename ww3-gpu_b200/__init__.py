@@ -38,7 +38,9 @@ EXPORTS = (
     "ww_kokkos_init", "ww_kokkos_finalize", "ww_snl1_init", "ww_snl1_init_tables", "ww_snl1",
     "ww_snl1_device", "ww_snl1_enabled", "ww_snl1_last_error", "ww_snl1_select_kernel",
     "ww_kokkos_flag", "ww_kokkos_preset_status", "ww_kokkos_strict", "ww_kokkos_fallback_slot",
-    "ww_kokkos_fallback_add",
+    "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
+    "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
+    "ww_va_report", "ww_va_device_ptr", "ww_va_state",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -90,6 +92,19 @@ def lib():
         L.ww_kokkos_fallback_slot.restype = _I
         L.ww_kokkos_fallback_add.argtypes = [_I]
         L.ww_kokkos_fallback_add.restype = None
+        for name in ("ww_va_host_read", "ww_va_host_write", "ww_va_host_update"):
+            getattr(L, name).argtypes = [_I, _P, _I, _I]
+            getattr(L, name).restype = _I
+        for name in ("ww_va_host_read_cols", "ww_va_host_wrote_cols", "ww_va_device_zero_cols"):
+            getattr(L, name).argtypes = [_I, _P, _I, _I, _I, _P]
+            getattr(L, name).restype = _I
+        L.ww_va_device.argtypes = [_I, _I]
+        L.ww_va_device.restype = _I
+        L.ww_va_report.restype = None
+        L.ww_va_device_ptr.argtypes = [_I]
+        L.ww_va_device_ptr.restype = _P
+        L.ww_va_state.argtypes = [_I]
+        L.ww_va_state.restype = _I
         _lib = L
     return _lib
 

@@ -26,6 +26,7 @@ Runtime& runtime() {
 }
 
 void release_snl1_contexts();  // abi_snl1.cpp
+void release_va_contexts();    // abi_va.cu
 
 namespace {
 
@@ -200,6 +201,7 @@ void ww_kokkos_finalize(void) {
   auto& rt = runtime();
   wwb::release_snl1_contexts();
   if (!rt.ready) return;
+  wwb::release_va_contexts();
   cudaDeviceSynchronize();
   if (rt.stream) cudaStreamDestroy(rt.stream);
   if (rt.copy_in) cudaStreamDestroy(rt.copy_in);
