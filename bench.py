@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--npts", type=int, default=NPTS_PER_GPU)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band"], default="auto",
+                   help="DIA kernel (ww_snl1_select_kernel); auto picks the band kernel")
     return p.parse_args()
 
 
@@ -204,8 +206,8 @@ def measured_peak_hbm():
 
 def ncu_traffic_per_point():
     """DRAM bytes per sea point of the W3SNL1 kernel from the committed ncu capture summary
-    (profiles/snl1_rowshift_36x36.json), or None."""
-    p = ROOT / "profiles" / "snl1_rowshift_36x36.json"
+    (profiles/snl1_band_36x36.json), or None."""
+    p = ROOT / "profiles" / "snl1_band_36x36.json"
     if not p.exists():
         return None
     try:
@@ -234,6 +236,12 @@ def run_b200(args):
     npts = args.npts
     g = synth.sea_states_chunked(npts, seed=2024 + rank, depth=4000.0)
     grid = pkg.Snl1Grid(cfg, sig, igrid=1)
+    kernel_ids = {"auto": pkg.KERNEL_AUTO, "gather": pkg.KERNEL_GATHER,
+                  "rowshift": pkg.KERNEL_ROWSHIFT, "band": pkg.KERNEL_BAND}
+    grid.select_kernel(kernel_ids[args.kernel])
+    kernel_name = {pkg.KERNEL_GATHER: "snl1_gather_kernel", pkg.KERNEL_ROWSHIFT:
+                   "snl1_rowshift_kernel", pkg.KERNEL_BAND: "snl1_band_kernel"}[
+                       grid.select_kernel(kernel_ids[args.kernel])]
     dev = torch.device("cuda", local)
     a = torch.from_numpy(g["a"]).to(dev)
     cg = torch.from_numpy(g["cg"]).to(dev)
@@ -305,7 +313,7 @@ def run_b200(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "traffic": (tpp * npts if tpp else None),
-                     "kernel": "snl1_rowshift_kernel", "launch_ms": launch_ms,
+                     "kernel": kernel_name, "launch_ms": launch_ms,
                      "algorithmic_bytes_per_point": BYTES_PER_POINT},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),

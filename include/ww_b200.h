@@ -87,10 +87,11 @@ int ww_snl1_enabled(void);
 /* Replaces ww_snl1_last_error (ww_kokkos_c.hpp:133). */
 int ww_snl1_last_error(void);
 
-/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the row-shift kernel
- * when INSNL1's tables have that form, else the gather kernel), 1 the gather kernel over the
- * index tables, 2 the row-shift kernel. Returns the previous choice, or -1 for an unknown grid
- * or a choice the grid's tables cannot run. */
+/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the band kernel when
+ * INSNL1's tables have the row-shift form and fit it, else the row-shift kernel, else the
+ * gather kernel), 1 the gather kernel over the index tables, 2 the row-shift kernel (one CTA
+ * per point), 3 the band kernel (register windows over frequency bands, TMA-staged input).
+ * Returns the previous choice, or -1 for an unknown grid or a choice its tables cannot run. */
 int ww_snl1_select_kernel(int igrid, int which);
 
 /* ---------------------------------------------------------------- the resident spectrum VA */
@@ -136,6 +137,37 @@ void* ww_va_device_ptr(int igrid);
 
 /* B200 extension: the state of grid igrid's VA: 0 HOST, 1 DEVICE, 2 BOTH, -1 unbound. */
 int ww_va_state(int igrid);
+
+/* ---------------------------------------------------------------- PR3/UQ propagation */
+
+/* Replaces ww_ktp3_batch (prop3_c.hpp:75-81): W3KTP3 NTIMES times on each of NPTS sea points,
+ * one intra-spectral part of W3WAVE. rpar[3] = DMIN, CTMAX, FACHFA; ipar[7] = NK, NTH, NSPEC,
+ * NK2, FLCTH, FLCK, FLCUR; sig, dsip (NK+2); ecos, esin, ec2, esc, es2, mapwn, mapwn2
+ * (NSPEC+NTH); mapth2 ((NK+2)*NTH); cg, wn (NK+2, 0:NSEA); jsea, isea (npts, 1-based);
+ * pscal (10, npts) = CTHG0S, MAX(DMIN,DW), DDDX, DDDY, CX, CY, DCXDX, DCXDY, DCYDX, DCYDY;
+ * va (NSPEC, 0:NSEALM) with ncol = NSEALM+1, updated in place; cflthmax, cflkmax (NSEALM)
+ * written at JSEA. Returns a WwKokkosStatus. */
+int ww_ktp3_batch(const float* rpar, int nrpar, const int* ipar, int nipar, const float* sig,
+                  const float* dsip, const float* ecos, const float* esin, const float* ec2,
+                  const float* esc, const float* es2, const int* mapwn, const int* mapth2,
+                  const int* mapwn2, int itstep, int ntimes, float facth, float fack, int nsea,
+                  const float* cg, const float* wn, int npts, const int* jsea, const int* isea,
+                  const float* pscal, int ncol, float* va, float* cflthmax, float* cflkmax);
+
+/* Replaces ww_ktp3_batch_va (prop3_c.hpp:86-94): ww_ktp3_batch on the resident VA of grid
+ * igrid (synced to the device first; state DEVICE afterwards); cflthmax/cflkmax stay host
+ * arrays. */
+int ww_ktp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar,
+                     const float* sig, const float* dsip, const float* ecos, const float* esin,
+                     const float* ec2, const float* esc, const float* es2, const int* mapwn,
+                     const int* mapth2, const int* mapwn2, int itstep, int ntimes, float facth,
+                     float fack, int nsea, const float* cg, const float* wn, int npts,
+                     const int* jsea, const int* isea, const float* pscal, float* va, int nspec,
+                     int nsealm, float* cflthmax, float* cflkmax);
+
+/* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* call (the reference
+ * returns it only). */
+int ww_prop3_last_error(void);
 
 /* ---------------------------------------------------------------- run-time flags */
 

@@ -6,9 +6,10 @@ Two checkers, both CPU code, loaded only by tests/, ``__graft_entry__.smoke()`` 
 * ``liboracle.so`` -- this project's plain-C restatement of INSNL1 and W3SNL1
   (oracle/dia_body.h, following ww3-gpu kokkos/src/ww_kokkos/snl1_tables.cpp:82-329 and
   snl1_team.hpp:351-497), in float32 (bit-exact form) and float64 (the FP64 DIA).
-* ``_ref/libref_snl1.so`` -- the reference's own C++ (snl1_tables.cpp, snl1_dia.cpp and its C
-  ABI shim snl1_shim.cpp) compiled unmodified against oracle/kokkos_compat; present when
-  oracle/Makefile's ``ref`` target ran where the reference is checked out.
+* ``_ref/libref_ww3.so`` -- the reference's own C++ (snl1_tables.cpp, snl1_dia.cpp, the C ABI
+  shims snl1_shim.cpp, prop3_shim.cpp and resident_shim.cpp with the headers they include)
+  compiled unmodified against oracle/kokkos_compat; present when oracle/Makefile's ``ref``
+  target ran where the reference is checked out.
 
 Arrays follow the reference's C ABI: a spectrum batch (nspec, npts) column-major is a numpy
 array of shape (npts, nspec) in C order.
@@ -22,7 +23,7 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
-REF_PATH = HERE / "_ref" / "libref_snl1.so"
+REF_PATH = HERE / "_ref" / "libref_ww3.so"
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -201,3 +202,36 @@ class RefSnl1:
         if rc != 0:
             raise RuntimeError(f"reference ww_snl1 failed with status {rc}")
         return s, d
+
+
+# ---------------------------------------------------------------- W3KTP3 through the reference
+KTP3_ARGS = ("rpar", "ipar", "sig", "dsip", "ecos", "esin", "ec2", "esc", "es2", "mapwn",
+             "mapth2", "mapwn2")
+
+
+def _ktp3_setup(L):
+    if getattr(L, "_ktp3_ready", False):
+        return
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.ww_ktp3_batch.argtypes = [P, I, P, I] + [P] * 10 + [I, I, F, F, I, P, P, I, P, P, P, I, P,
+                                                          P, P]
+    L.ww_ktp3_batch.restype = I
+    L._ktp3_ready = True
+
+
+def ktp3_call(L, case, itstep=1, ntimes=1):
+    """ww_ktp3_batch of library L (the reference build or libww_b200) on a synth.ktp3_case
+    dict; returns (status, va, cflthmax, cflkmax) as new arrays."""
+    _ktp3_setup(L)
+    va = np.array(case["va"], np.float32, copy=True)
+    cth = np.array(case["cflthmax"], np.float32, copy=True)
+    ck = np.array(case["cflkmax"], np.float32, copy=True)
+    arrs = [np.ascontiguousarray(case[k]) for k in KTP3_ARGS]
+    keep = [np.ascontiguousarray(case[k]) for k in ("cg", "wn", "jsea", "isea", "pscal")]
+    rc = L.ww_ktp3_batch(arrs[0].ctypes.data, arrs[0].size, arrs[1].ctypes.data, arrs[1].size,
+                         *[a.ctypes.data for a in arrs[2:]], itstep, ntimes, case["facth"],
+                         case["fack"], case["nsea"], keep[0].ctypes.data, keep[1].ctypes.data,
+                         case["npts"], keep[2].ctypes.data, keep[3].ctypes.data,
+                         keep[4].ctypes.data, va.shape[0], va.ctypes.data, cth.ctypes.data,
+                         ck.ctypes.data)
+    return rc, va, cth, ck

@@ -2,10 +2,11 @@
 //
 // Flat extern "C" access to the INSNL1 tables of the reference's own C++
 // (ww::snl1::make_tables, ww3-gpu kokkos/src/ww_kokkos/snl1_tables.cpp:82-329), compiled from
-// the reference's sources by oracle/Makefile into oracle/_ref/libref_snl1.so. The reference's
+// the reference's sources by oracle/Makefile into oracle/_ref/libref_ww3.so. The reference's
 // W3SNL1 itself is reached through its own C ABI in the same library (ww_kokkos_init,
 // ww_snl1_init, ww_snl1: kokkos/src/fortran_iface/snl1_shim.cpp), so no driver is needed for
-// it. Used by the tests and by bench.py's reference arm only.
+// it, nor for W3KTP3/W3XYP3 (ww_ktp3_batch, ww_xyp3_batch: prop3_shim.cpp) and the resident VA
+// (ww_va_*: resident_shim.cpp). Used by the tests and by bench.py's reference arm only.
 #include <Kokkos_Core.hpp>
 
 #include "ww_kokkos/snl1_config.hpp"
@@ -49,3 +50,7 @@ extern "C" int ref_snl1_tables(int nk, int nth, float xfr, float dth, float lam,
     for (int i = 0; i < t.nspecx; ++i) af11[i] = t.af11(i);
   return 0;
 }
+
+// prop3_shim.cpp's exit report names the unstructured-grid shim's counter, which this build
+// leaves out (that propagation scheme is not on the path); an empty report stands in for it.
+extern "C" void ww_xypug_report(void) {}

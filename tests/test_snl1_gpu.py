@@ -13,11 +13,12 @@ from conftest import assert_bitexact, cuda_available
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
 
-KERNELS = ["gather", "rowshift"]
+KERNELS = ["gather", "rowshift", "band"]
 
 
 def kernel_id(pkg, name):
-    return {"gather": pkg.KERNEL_GATHER, "rowshift": pkg.KERNEL_ROWSHIFT}[name]
+    return {"gather": pkg.KERNEL_GATHER, "rowshift": pkg.KERNEL_ROWSHIFT,
+            "band": pkg.KERNEL_BAND}[name]
 
 
 @pytest.fixture(scope="module")
@@ -95,7 +96,7 @@ def test_other_spectral_grids(pkg, oracle, nk, nth):
         try:
             grid.select_kernel(kernel_id(pkg, name))
         except ValueError:
-            assert name == "rowshift"
+            assert name in ("rowshift", "band")
             continue
         s, d = grid(a, cg, kd)
         assert_bitexact(s, s_ref, f"S {nk}x{nth} {name}")
@@ -178,7 +179,7 @@ def test_full_size_properties(pkg, oracle, synth, cfg36):
     kd = torch.from_numpy(g["kdmean"]).to(dev)
     outs = []
     stream = torch.cuda.current_stream().cuda_stream
-    for name in ("rowshift", "rowshift", "gather"):
+    for name in ("band", "band", "rowshift", "gather"):
         grid.select_kernel(kernel_id(pkg, name))
         s = torch.empty_like(a)
         d = torch.empty_like(a)

@@ -31,7 +31,7 @@ ERR_UNSUPPORTED = 5
 ERR_TABLE = 6
 
 # ww_snl1_select_kernel choices
-KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT = 0, 1, 2
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT, KERNEL_BAND = 0, 1, 2, 3
 
 # Every symbol include/ww_b200.h declares.
 EXPORTS = (
@@ -40,7 +40,8 @@ EXPORTS = (
     "ww_kokkos_flag", "ww_kokkos_preset_status", "ww_kokkos_strict", "ww_kokkos_fallback_slot",
     "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
-    "ww_va_report", "ww_va_device_ptr", "ww_va_state",
+    "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_ktp3_batch", "ww_ktp3_batch_va",
+    "ww_prop3_last_error",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -105,6 +106,13 @@ def lib():
         L.ww_va_device_ptr.restype = _P
         L.ww_va_state.argtypes = [_I]
         L.ww_va_state.restype = _I
+        L.ww_ktp3_batch.argtypes = [_P, _I, _P, _I] + [_P] * 10 + [_I, _I, _F, _F, _I, _P, _P,
+                                                                   _I, _P, _P, _P, _I, _P, _P, _P]
+        L.ww_ktp3_batch.restype = _I
+        L.ww_ktp3_batch_va.argtypes = [_I, _P, _I, _P, _I] + [_P] * 10 + [
+            _I, _I, _F, _F, _I, _P, _P, _I, _P, _P, _P, _P, _I, _I, _P, _P]
+        L.ww_ktp3_batch_va.restype = _I
+        L.ww_prop3_last_error.restype = _I
         _lib = L
     return _lib
 
@@ -221,3 +229,47 @@ class Snl1Grid:
 
 def flag(name):
     return lib().ww_kokkos_flag(name.encode())
+
+
+# ---------------------------------------------------------------- PR3/UQ
+KTP3_ARRAYS = ("sig", "dsip", "ecos", "esin", "ec2", "esc", "es2", "mapwn", "mapth2", "mapwn2")
+
+
+def ktp3_batch(case, itstep=1, ntimes=1, igrid=None, va=None):
+    """ww_ktp3_batch (or ww_ktp3_batch_va when ``igrid`` is given, on the resident VA bound to
+    the host array ``va``) with the arguments of a dict laid out as the C ABI reads them (see
+    synth.ktp3_case). Without ``igrid`` a copy of case["va"] is updated and returned.
+    Returns (status, va, cflthmax, cflkmax)."""
+    L = lib()
+    init()
+    rpar = np.ascontiguousarray(case["rpar"], np.float32)
+    ipar = np.ascontiguousarray(case["ipar"], np.int32)
+    arrs = [np.ascontiguousarray(case[k]) for k in KTP3_ARRAYS]
+    cg = np.ascontiguousarray(case["cg"], np.float32)
+    wn = np.ascontiguousarray(case["wn"], np.float32)
+    js = np.ascontiguousarray(case["jsea"], np.int32)
+    isea = np.ascontiguousarray(case["isea"], np.int32)
+    ps = np.ascontiguousarray(case["pscal"], np.float32)
+    cth = np.array(case["cflthmax"], np.float32, copy=True)
+    ck = np.array(case["cflkmax"], np.float32, copy=True)
+    head = [rpar.ctypes.data, rpar.size, ipar.ctypes.data, ipar.size] + [a.ctypes.data for a in arrs]
+    mid = [itstep, ntimes, case["facth"], case["fack"], case["nsea"], cg.ctypes.data,
+           wn.ctypes.data, case["npts"], js.ctypes.data, isea.ctypes.data, ps.ctypes.data]
+    if igrid is None:
+        v = np.array(case["va"], np.float32, copy=True)
+        rc = L.ww_ktp3_batch(*head, *mid, v.shape[0], v.ctypes.data, cth.ctypes.data,
+                             ck.ctypes.data)
+    else:
+        v = va
+        rc = L.ww_ktp3_batch_va(igrid, *head, *mid, v.ctypes.data, v.shape[1], v.shape[0] - 1,
+                                cth.ctypes.data, ck.ctypes.data)
+    return rc, v, cth, ck
+
+
+def va_host_read(igrid, va):
+    """ww_va_host_read on the (NSEALM+1, NSPEC) C-ordered host array bound to grid igrid."""
+    return lib().ww_va_host_read(igrid, va.ctypes.data, va.shape[1], va.shape[0] - 1)
+
+
+def va_host_write(igrid, va):
+    return lib().ww_va_host_write(igrid, va.ctypes.data, va.shape[1], va.shape[0] - 1)

@@ -27,6 +27,7 @@ Runtime& runtime() {
 
 void release_snl1_contexts();  // abi_snl1.cpp
 void release_va_contexts();    // abi_va.cu
+void release_prop3_staging();  // abi_prop3.cpp
 
 namespace {
 
@@ -202,6 +203,7 @@ void ww_kokkos_finalize(void) {
   wwb::release_snl1_contexts();
   if (!rt.ready) return;
   wwb::release_va_contexts();
+  wwb::release_prop3_staging();
   cudaDeviceSynchronize();
   if (rt.stream) cudaStreamDestroy(rt.stream);
   if (rt.copy_in) cudaStreamDestroy(rt.copy_in);

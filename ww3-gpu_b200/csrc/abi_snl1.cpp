@@ -117,6 +117,8 @@ void publish(Ctx& c) {
     p.swg[j] = t.swg[j];
     p.shift[j] = t.shift[j];
   }
+  p.ifrp = t.ifrp;
+  p.ifrm = t.ifrm;
   p.snlc1 = c.cfg.snlc1;
   p.kdcon = c.cfg.kdcon;
   p.kdmn = c.cfg.kdmn;
@@ -129,7 +131,23 @@ void publish(Ctx& c) {
   p.ipim = c.ipim.ptr;
   p.ic = c.ic.ptr;
   p.af11 = c.af11.ptr;
-  c.kernel = t.rowshift ? kSnl1RowShift : kSnl1Gather;
+  c.kernel = t.rowshift ? (snl1_band_ok(p) ? kSnl1Band : kSnl1RowShift) : kSnl1Gather;
+}
+
+/// The kernel `which` asks for, or -1 when these tables cannot run it.
+int pick_kernel(const Ctx& c, int which) {
+  switch (which) {
+    case kSnl1Auto:
+      return c.tab.rowshift ? (snl1_band_ok(c.dev) ? kSnl1Band : kSnl1RowShift) : kSnl1Gather;
+    case kSnl1Gather:
+      return kSnl1Gather;
+    case kSnl1RowShift:
+      return c.tab.rowshift ? kSnl1RowShift : -1;
+    case kSnl1Band:
+      return c.tab.rowshift && snl1_band_ok(c.dev) ? kSnl1Band : -1;
+    default:
+      return -1;
+  }
 }
 
 int resolve_kernel(const Ctx& c) { return c.kernel; }
@@ -309,6 +327,10 @@ void ww_snl1(int igrid, int npts, const float* a, const float* cg, const float* 
                                 cudaMemcpyDeviceToHost, sl.stream));
     }
     for (auto& sl : c->slots) WWB_CHECK(cudaStreamSynchronize(sl.stream));
+    if (snl1_take_error() != 0) {
+      g_status.fail(WW_KOKKOS_ERR_KERNEL, "ww_snl1: a bulk-copy wait of the DIA kernel gave up");
+      return;
+    }
     g_status.ok();
   } catch (const CudaError& e) {
     g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
@@ -342,10 +364,10 @@ int ww_snl1_select_kernel(int igrid, int which) {
   auto it = contexts().find(igrid);
   if (it == contexts().end() || !it->second->ready) return -1;
   Ctx& c = *it->second;
-  if (which == kSnl1RowShift && !c.tab.rowshift) return -1;
-  if (which < kSnl1Auto || which > kSnl1RowShift) return -1;
+  const int k = pick_kernel(c, which);
+  if (k < 0) return -1;
   const int prev = c.kernel;
-  c.kernel = which == kSnl1Auto ? (c.tab.rowshift ? kSnl1RowShift : kSnl1Gather) : which;
+  c.kernel = k;
   return prev;
 }
 

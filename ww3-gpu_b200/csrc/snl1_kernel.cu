@@ -307,6 +307,329 @@ __global__ void __launch_bounds__(BLOCK) snl1_gather_kernel(
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Band kernel: the B200 path.
+//
+// Persistent CTAs walk the sea points. Thread t owns direction column ITH = t % NTH and a band
+// of BR consecutive frequency rows (band t / NTH), the same band in sections 3 and 4. Along its
+// band it slides register windows over the rows the quadruplet reads: the IF1/IF2 rows (the
+// "plus" pair) and the IF3/IF4 rows (the "minus" pair) in section 3, the IF5/IF6 and IF7/IF8
+// rows in section 4, each window holding the four wrapped columns of that pair, so moving one
+// row up loads one new row of each pair. The eight wrapped columns are computed once per
+// thread. DA1C and DA2C are read back only at their own bin, so their sum is kept instead of
+// the two arrays: six interaction arrays and one sum array live in shared memory. The next point's A and CG are brought
+// into a shared staging buffer by one TMA bulk copy (cp.async.bulk, completed on an mbarrier)
+// while the current point is computed. Every floating-point operation is the reference's, in
+// its order (snl1_team.hpp:383-496).
+//
+// Row algebra (INSNL1 section 7): IF1 = f + IFRP, IF2 = IF1 + 1, IF3 = max(0, f + IFRM),
+// IF4 = max(0, f + IFRM - 1), IF5 = max(0, f - IFRP), IF6 = max(0, f - IFRP - 1),
+// IF7 = f - IFRM, IF8 = IF7 + 1, with IFRP >= 0 >= IFRM.
+//
+// Shared memory (floats): UE rows 0..NFRHGH; SA1, SA2, DA1P, DA1M, DA2P, DA2M rows 0..NFRCHG;
+// DC = DA1C + DA2C over the NSPEC bins (read back only by the thread that wrote it); CON rows
+// (2 x NK, double-buffered by point parity); AF11 rows (NFRCHG); the staging buffer
+// (NSPEC + NK, 16-byte aligned); the mbarrier.
+
+constexpr unsigned kWaitLimit = 1u << 22;  // bounded mbarrier waits (about a second)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+/// One elected thread: expect `bytes` and start the bulk copies of A and CG of point `ipt`.
+__device__ __forceinline__ void tma_fetch_point(uint64_t* bar, float* stage, const float* a,
+                                                const float* cg, int ipt, int nspec, int nk) {
+  const unsigned bytes_a = static_cast<unsigned>(nspec) * 4u;
+  const unsigned bytes_c = static_cast<unsigned>(nk) * 4u;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes_a + bytes_c)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(stage)),
+      "l"(a + static_cast<size_t>(ipt) * nspec), "r"(bytes_a), "r"(smem_u32(bar))
+      : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(stage + nspec)),
+      "l"(cg + static_cast<size_t>(ipt) * nk), "r"(bytes_c), "r"(smem_u32(bar))
+      : "memory");
+}
+
+/// Wait for phase `parity` of the mbarrier, giving up after kWaitLimit polls (then the status
+/// word records it and the kernel runs on; the host reports the failure).
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+  unsigned done = 0;
+  for (unsigned it = 0; it < kWaitLimit; ++it) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return;
+  }
+  atomicExch(err, 1);
+}
+
+template <int BLOCK, int MINB, int AS, bool TMA>
+__global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
+    const Snl1Dev p, const int npts, const float* __restrict__ a, const float* __restrict__ cg,
+    const float* __restrict__ kdmean, float* __restrict__ s, float* __restrict__ d,
+    int* __restrict__ err) {
+  extern __shared__ __align__(16) float smem[];
+  const int nth = p.nth, nfr = p.nfr, nfrhgh = p.nfrhgh, nfrchg = p.nfrchg;
+  const int nspec = p.nspec, nk = p.nk;
+  // The six interaction arrays sit AS floats apart (AS >= (NFRCHG + 1) * NTH, a compile-time
+  // stride), so one shared offset per (row, column) addresses all six with immediate offsets.
+  float* const ue = smem;
+  float* const arrs = ue + (nfrhgh + 1) * nth;
+  float* const sa1 = arrs;
+  float* const sa2 = arrs + AS;
+  float* const da1p = arrs + 2 * AS;
+  float* const da1m = arrs + 3 * AS;
+  float* const da2p = arrs + 4 * AS;
+  float* const da2m = arrs + 5 * AS;
+  float* const dcs = arrs + 6 * AS;
+  float* const conx2 = dcs + nspec;
+  float* const afr = conx2 + 2 * nk;
+  const size_t stage_off = (static_cast<size_t>(afr + nfrchg - smem) + 3) & ~static_cast<size_t>(3);
+  float* const stage = smem + stage_off;
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(stage + ((nspec + nk + 3) & ~3));
+  const int tid = threadIdx.x;
+
+  // Once per CTA: zero rows, AF11 rows, the mbarrier and the first point's bulk copy.
+  for (int i = tid; i < nth; i += BLOCK) {
+    ue[i] = 0.0f;
+    sa1[i] = sa2[i] = da1p[i] = da1m[i] = da2p[i] = da2m[i] = 0.0f;
+  }
+  for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
+  if (TMA && tid == 0) {
+    mbar_init(bar, 1);
+    if (blockIdx.x < npts) tma_fetch_point(bar, stage, a, cg, blockIdx.x, nspec, nk);
+  }
+  __syncthreads();
+
+  // This thread's column, band and wrapped columns.
+  const int G = BLOCK / nth;
+  const int ith = tid % nth, band = tid / nth;
+  const bool active = band < G;
+  const int br = (nfrchg + G - 1) / G;  // rows per band
+  const int f0 = 1 + band * br;
+  const int n3 = active ? max(0, min(br, nfrchg - f0 + 1)) : 0;
+  const int n4 = active ? max(0, min(br, nfr - f0 + 1)) : 0;
+  const int c0 = wrapc(ith + p.shift[0], nth), c1 = wrapc(ith + p.shift[1], nth);
+  const int c2 = wrapc(ith + p.shift[2], nth), c3 = wrapc(ith + p.shift[3], nth);
+  const int c4 = wrapc(ith + p.shift[4], nth), c5 = wrapc(ith + p.shift[5], nth);
+  const int c6 = wrapc(ith + p.shift[6], nth), c7 = wrapc(ith + p.shift[7], nth);
+  const int ifrp = p.ifrp, ifrm = p.ifrm;
+  const float dal1 = p.dal1, dal2 = p.dal2, dal3 = p.dal3;
+  // The UE loop of section 2 walks bins isp = tid + k * BLOCK.
+  const int dq = BLOCK / nth, dr = BLOCK % nth, q0 = tid / nth, r0 = tid % nth;
+
+  float kd_next = (blockIdx.x < npts) ? __ldg(kdmean + blockIdx.x) : 0.0f;
+  unsigned parity = 0;
+  int buf = 0;
+  for (int ipt = blockIdx.x; ipt < npts; ipt += gridDim.x, buf ^= 1) {
+    const float* const src_a = TMA ? stage : a + static_cast<size_t>(ipt) * nspec;
+    const float* const src_c = TMA ? stage + nspec : cg + static_cast<size_t>(ipt) * nk;
+    float* const conx = conx2 + buf * nk;
+    if (TMA) {
+      mbar_wait(bar, parity, err);
+      parity ^= 1u;
+    }
+    // 1. CONS; 2a. CON per frequency row.
+    const float cons = dia_cons(p, kd_next);
+    for (int k = tid; k < nk; k += BLOCK) conx[k] = kTpiInv / __ldg(p.sig + k) * src_c[k];
+    __syncthreads();
+
+    // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
+    {
+      int ifr0 = q0, col = r0;
+      for (int isp = tid; isp < nspec; isp += BLOCK) {
+        const float v = (TMA ? src_a[isp] : __ldcs(src_a + isp)) / conx[ifr0];
+        ue[isp + nth] = v;
+        if (ifr0 == nfr - 1) {
+          float t = v;
+          for (int r = nfr + 1; r <= nfrhgh; ++r) {
+            t = t * p.fachfe;
+            ue[r * nth + col] = t;
+          }
+        }
+        col += dr;
+        ifr0 += dq;
+        if (col >= nth) {
+          col -= nth;
+          ++ifr0;
+        }
+      }
+    }
+    __syncthreads();
+
+    // The next point's A and CG stream into the staging buffer while this one is computed.
+    const int inext = ipt + gridDim.x;
+    if (TMA && tid == 0 && inext < npts) tma_fetch_point(bar, stage, a, cg, inext, nspec, nk);
+    if (inext < npts) kd_next = __ldg(kdmean + inext);
+
+    // 3. Interactions over the extended spectrum, sliding up the band.
+    if (n3 > 0) {
+      float pa[4], pb[4], ma[4], mb[4];  // plus rows: c1 c2 c5 c6; minus rows: c3 c4 c7 c8
+#define WWB_LOAD_P(ROW, W)                    \
+  {                                           \
+    const int b_ = (ROW) * nth;               \
+    W[0] = ue[b_ + c0];                       \
+    W[1] = ue[b_ + c1];                       \
+    W[2] = ue[b_ + c4];                       \
+    W[3] = ue[b_ + c5];                       \
+  }
+#define WWB_LOAD_M(ROW, W)                    \
+  {                                           \
+    const int r_ = (ROW);                     \
+    const int b_ = (r_ > 0 ? r_ : 0) * nth;   \
+    W[0] = ue[b_ + c2];                       \
+    W[1] = ue[b_ + c3];                       \
+    W[2] = ue[b_ + c6];                       \
+    W[3] = ue[b_ + c7];                       \
+  }
+      WWB_LOAD_P(f0 + ifrp, pa)
+      WWB_LOAD_P(f0 + ifrp + 1, pb)
+      WWB_LOAD_M(f0 + ifrm, ma)
+      WWB_LOAD_M(f0 + ifrm - 1, mb)
+#pragma unroll 1
+      for (int k = 0; k < n3; ++k) {
+        {
+          const int f = f0 + k;
+          const int o = f * nth + ith;
+          const float e00 = ue[o];
+          const float ep1 = p.awg[0] * pb[1] + p.awg[1] * pb[0] + p.awg[2] * pa[1] + p.awg[3] * pa[0];
+          const float em1 = p.awg[4] * mb[3] + p.awg[5] * mb[2] + p.awg[6] * ma[3] + p.awg[7] * ma[2];
+          const float ep2 = p.awg[0] * pb[3] + p.awg[1] * pb[2] + p.awg[2] * pa[3] + p.awg[3] * pa[2];
+          const float em2 = p.awg[4] * mb[1] + p.awg[5] * mb[0] + p.awg[6] * ma[1] + p.awg[7] * ma[0];
+          const float ca = cons * afr[f - 1];
+          const float factor = ca * e00;
+          const float sa1a = e00 * (ep1 * dal1 + em1 * dal2);
+          const float sa1b = sa1a - ep1 * em1 * dal3;
+          const float sa2a = e00 * (ep2 * dal1 + em2 * dal2);
+          const float sa2b = sa2a - ep2 * em2 * dal3;
+          const float v1 = factor * sa1b;
+          const float v2 = factor * sa2b;
+          sa1[o] = v1;
+          sa2[o] = v2;
+          if (f <= nfr) dcs[o - nth] = ca * (sa1a + sa1b) + ca * (sa2a + sa2b);
+          da1p[o] = factor * (dal1 * e00 - dal3 * em1);
+          da1m[o] = factor * (dal2 * e00 - dal3 * ep1);
+          da2p[o] = factor * (dal1 * e00 - dal3 * em2);
+          da2m[o] = factor * (dal2 * e00 - dal3 * ep2);
+          if (k + 1 < n3) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              pa[j] = pb[j];
+              mb[j] = ma[j];
+            }
+            WWB_LOAD_P(f + 1 + ifrp + 1, pb)
+            WWB_LOAD_M(f + 1 + ifrm, ma)
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // 4. Source and diagonal terms, sliding up the band: S in one pass, D in a second, so each
+    //    pass holds one set of windows (lo rows IF5/IF6: columns c5 c6 of SA1 or DA1P and c1 c2
+    //    of SA2 or DA2P; hi rows IF7/IF8: c3 c4 of SA1 or DA1M and c7 c8 of SA2 or DA2M).
+    if (n4 > 0) {
+#define WWB_LO(A1, A2, ROW, W)                \
+  {                                           \
+    const int r_ = (ROW);                     \
+    const int b_ = (r_ > 0 ? r_ : 0) * nth;   \
+    W[0] = A1[b_ + c4];                       \
+    W[1] = A1[b_ + c5];                       \
+    W[2] = A2[b_ + c0];                       \
+    W[3] = A2[b_ + c1];                       \
+  }
+#define WWB_HI(A1, A2, ROW, W)                \
+  {                                           \
+    const int b_ = (ROW) * nth;               \
+    W[0] = A1[b_ + c2];                       \
+    W[1] = A1[b_ + c3];                       \
+    W[2] = A2[b_ + c6];                       \
+    W[3] = A2[b_ + c7];                       \
+  }
+      float l5[4], l6[4], h7[4], h8[4];
+      {
+        float* const sp = s + static_cast<size_t>(ipt) * nspec;
+        WWB_LO(sa1, sa2, f0 - ifrp, l5)
+        WWB_LO(sa1, sa2, f0 - ifrp - 1, l6)
+        WWB_HI(sa1, sa2, f0 - ifrm, h7)
+        WWB_HI(sa1, sa2, f0 - ifrm + 1, h8)
+#pragma unroll 1
+        for (int k = 0; k < n4; ++k) {
+          const int f = f0 + k;
+          const int isp = (f - 1) * nth + ith;
+          const float sv = conx[f - 1] * (-2.0f * (sa1[isp + nth] + sa2[isp + nth]) +
+                                          p.awg[0] * (l6[1] + l6[3]) + p.awg[1] * (l6[0] + l6[2]) +
+                                          p.awg[2] * (l5[1] + l5[3]) + p.awg[3] * (l5[0] + l5[2]) +
+                                          p.awg[4] * (h8[1] + h8[3]) + p.awg[5] * (h8[0] + h8[2]) +
+                                          p.awg[6] * (h7[1] + h7[3]) + p.awg[7] * (h7[0] + h7[2]));
+          __stcs(sp + isp, sv);
+          if (k + 1 < n4) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              l6[j] = l5[j];
+              h7[j] = h8[j];
+            }
+            WWB_LO(sa1, sa2, f + 1 - ifrp, l5)
+            WWB_HI(sa1, sa2, f + 1 - ifrm + 1, h8)
+          }
+        }
+      }
+      {
+        float* const dp = d + static_cast<size_t>(ipt) * nspec;
+        WWB_LO(da1p, da2p, f0 - ifrp, l5)
+        WWB_LO(da1p, da2p, f0 - ifrp - 1, l6)
+        WWB_HI(da1m, da2m, f0 - ifrm, h7)
+        WWB_HI(da1m, da2m, f0 - ifrm + 1, h8)
+#pragma unroll 1
+        for (int k = 0; k < n4; ++k) {
+          const int f = f0 + k;
+          const int isp = (f - 1) * nth + ith;
+          const float dv = -2.0f * dcs[isp] +
+                           p.swg[0] * (l6[1] + l6[3]) + p.swg[1] * (l6[0] + l6[2]) +
+                           p.swg[2] * (l5[1] + l5[3]) + p.swg[3] * (l5[0] + l5[2]) +
+                           p.swg[4] * (h8[1] + h8[3]) + p.swg[5] * (h8[0] + h8[2]) +
+                           p.swg[6] * (h7[1] + h7[3]) + p.swg[7] * (h7[0] + h7[2]);
+          __stcs(dp + isp, dv);
+          if (k + 1 < n4) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              l6[j] = l5[j];
+              h7[j] = h8[j];
+            }
+            WWB_LO(da1p, da2p, f + 1 - ifrp, l5)
+            WWB_HI(da1m, da2m, f + 1 - ifrm + 1, h8)
+          }
+        }
+      }
+#undef WWB_LO
+#undef WWB_HI
+    }
+    // The next point's barriers order its writes of UE and the arrays after this section 4.
+  }
+#undef WWB_LOAD_P
+#undef WWB_LOAD_M
+}
+
+constexpr int kBandBlock = 288;
+constexpr int kBandMinBlocks = 3;  // 3 CTAs of 288 threads per SM: at most 75 registers
+int* g_band_err = nullptr;
+
 constexpr int kRowShiftBlock = 288;
 constexpr int kGatherBlock = 256;
 
@@ -326,10 +649,80 @@ size_t snl1_rowshift_smem(const Snl1Dev& p) {
          sizeof(int) * 8 * static_cast<size_t>(p.nfrchg);
 }
 
+namespace {
+/// The interaction-array stride of the band kernel instance that fits these tables, or 0.
+int band_stride(const Snl1Dev& p) {
+  const int need = (p.nfrchg + 1) * p.nth;
+  return need <= 1536 ? 1536 : (need <= 4096 ? 4096 : 0);
+}
+}  // namespace
+
+size_t snl1_band_smem(const Snl1Dev& p) {
+  size_t floats = static_cast<size_t>(p.nfrhgh + 1) * p.nth + 6 * static_cast<size_t>(band_stride(p)) +
+                  p.nspec + 2 * p.nk + p.nfrchg;
+  floats = (floats + 3) & ~static_cast<size_t>(3);
+  floats += (static_cast<size_t>(p.nspec + p.nk) + 3) & ~static_cast<size_t>(3);
+  return floats * sizeof(float) + 16;  // + the mbarrier
+}
+
+bool snl1_band_ok(const Snl1Dev& p) {
+  if (p.ifrow == nullptr || p.af11_row == nullptr) return false;  // no row-shift form
+  if (p.nth > kBandBlock || p.ifrp < 0 || p.ifrm > 0 || band_stride(p) == 0) return false;
+  return snl1_band_smem(p) <= 227 * 1024;
+}
+
+int snl1_take_error() {
+  if (g_band_err == nullptr) return 0;
+  int v = 0;
+  WWB_CHECK(cudaMemcpy(&v, g_band_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v != 0) WWB_CHECK(cudaMemset(g_band_err, 0, sizeof(int)));
+  return v;
+}
+
+namespace {
+template <int AS, bool TMA>
+void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, const float* kd,
+                 float* s, float* d, cudaStream_t stream) {
+  static int per_sm = -1;
+  static size_t cached = 0;
+  const size_t smem = snl1_band_smem(p);
+  auto k = snl1_band_kernel<kBandBlock, kBandMinBlocks, AS, TMA>;
+  if (per_sm < 0 || cached != smem) {
+    WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    int n = 0;
+    WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kBandBlock, smem));
+    if (n < 1) throw CudaError(cudaErrorInvalidConfiguration, "snl1 band occupancy");
+    per_sm = n;
+    cached = smem;
+  }
+  if (g_band_err == nullptr) {
+    WWB_CHECK(cudaMalloc(&g_band_err, sizeof(int)));
+    WWB_CHECK(cudaMemset(g_band_err, 0, sizeof(int)));
+  }
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  const int grid = static_cast<int>(npts < resident ? npts : resident);
+  k<<<grid, kBandBlock, smem, stream>>>(p, npts, a, cg, kd, s, d, g_band_err);
+  WWB_CHECK(cudaGetLastError());
+}
+}  // namespace
+
 void launch_snl1(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                  const float* kdmean, float* s, float* d, cudaStream_t stream) {
   if (npts <= 0) return;
-  if (kernel == kSnl1RowShift) {
+  if (kernel == kSnl1Band) {
+    // The bulk copies need 16-byte aligned sources and sizes: NSPEC and NK multiples of 4.
+    const bool tma = p.nspec % 4 == 0 && p.nk % 4 == 0 &&
+                     (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
+                     (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
+    if (band_stride(p) == 1536) {
+      if (tma) launch_band<1536, true>(p, npts, a, cg, kdmean, s, d, stream);
+      else launch_band<1536, false>(p, npts, a, cg, kdmean, s, d, stream);
+    } else {
+      if (tma) launch_band<4096, true>(p, npts, a, cg, kdmean, s, d, stream);
+      else launch_band<4096, false>(p, npts, a, cg, kdmean, s, d, stream);
+    }
+  } else if (kernel == kSnl1RowShift) {
     const size_t smem = snl1_rowshift_smem(p);
     auto k = snl1_rowshift_kernel<kRowShiftBlock>;
     if (g_rowshift_ctas_per_sm < 0 || g_rowshift_smem_cached != smem) {

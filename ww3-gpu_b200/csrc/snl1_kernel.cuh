@@ -16,6 +16,7 @@ struct Snl1Dev {
   float awg[8], swg[8];
   float snlc1, kdcon, kdmn, snls1, snls2, snls3, fachfe;
   int shift[8];             ///< row-shift form: IT_n(ITH) - ITH
+  int ifrp, ifrm;           ///< row-shift form: IF1 = IFR + IFRP, IF3 = MAX(0, IFR + IFRM)
   const int* ifrow;         ///< device, 8 x NFRCHG (row-shift form)
   const float* af11_row;    ///< device, NFRCHG (row-shift form)
   const int* ipim;          ///< device, 16 x NSPECX (gather form)
@@ -24,11 +25,19 @@ struct Snl1Dev {
   const float* sig;         ///< device, NK
 };
 
-enum Snl1Kernel { kSnl1Auto = 0, kSnl1Gather = 1, kSnl1RowShift = 2 };
+enum Snl1Kernel { kSnl1Auto = 0, kSnl1Gather = 1, kSnl1RowShift = 2, kSnl1Band = 3 };
 
 /// Dynamic shared memory of each kernel, bytes.
 size_t snl1_gather_smem(const Snl1Dev& p);
 size_t snl1_rowshift_smem(const Snl1Dev& p);
+size_t snl1_band_smem(const Snl1Dev& p);
+
+/// Whether the band kernel can run these tables (row-shift form, NTH within one CTA, the
+/// rows of a band within its register windows).
+bool snl1_band_ok(const Snl1Dev& p);
+
+/// Device status word of the band kernel's bounded waits: nonzero after a wait gave up.
+int snl1_take_error();
 
 /// Launch W3SNL1 on npts points; a, s, d (nspec, npts) and cg (nk, npts) column-major,
 /// kdmean (npts), all device pointers. Throws CudaError on a launch failure.

@@ -183,6 +183,8 @@ void derive_rowshift(const Snl1Config& c, Snl1Tables& t) {
   const Geometry g = geometry(c);
   t.rowshift = false;
   shifts(g, t.shift);
+  t.ifrp = g.ifrp;
+  t.ifrm = g.ifrm;
   t.ifrow.assign(8 * static_cast<size_t>(t.nfrchg), 0);
   for (int m = 1; m <= 8; ++m)
     for (int ifr = 1; ifr <= t.nfrchg; ++ifr)

@@ -46,6 +46,7 @@ struct Snl1Tables {
   // Row-shift form, valid when rowshift is true.
   bool rowshift = false;
   int shift[8] = {};       ///< IT_n(ITH) - ITH before wrapping, n = 1..8
+  int ifrp = 0, ifrm = 0;  ///< IF1(IFR) = IFR + IFRP, IF3(IFR) = MAX(0, IFR + IFRM)
   std::vector<int> ifrow;  ///< 8 x NFRCHG: IF_m(IFR), m = 1..8, IFR = 1..NFRCHG
   std::vector<float> af11_row;  ///< NFRCHG: AF11 of each row (constant along a row)
 };

@@ -141,3 +141,99 @@ def sea_states_chunked(npts, seed=0, chunk=32768, out=None, **kw):
         for key in out:
             out[key][p0:p0 + n] = g[key]
     return out
+
+
+# ---------------------------------------------------------------------------- PR3/UQ inputs
+def spectral_arrays(nk=36, nth=36, f1=0.0373, xfr=1.1):
+    """W3GDATMD's spectral arrays for the PR3 entries, float32, built as WW3's W3GRID does:
+    SIG(0:NK+1) and DSIP(0:NK+1) from SIGMA = FR1*TPI/XFR**2 grown by XFR each bin, DSIP =
+    SIG*(XFR-1/XFR)/2; TH = (ITH-1)*DTH; ECOS, ESIN, EC2, ESC, ES2 and MAPWN over NSPEC+NTH
+    (the last NTH entries repeat the first row's trig values, MAPWN = NK+1 there)."""
+    nspec = nk * nth
+    x = np.float32(xfr)
+    sxfr = np.float32(0.5) * (x - np.float32(1.0) / x)
+    sig = np.empty(nk + 2, np.float32)
+    dsip = np.empty(nk + 2, np.float32)
+    sigma = np.float32(np.float32(f1) * TPI_F32 / (x * x))
+    for ik in range(nk + 2):
+        sigma = np.float32(sigma * x)
+        sig[ik] = sigma
+        dsip[ik] = np.float32(sigma * sxfr)
+    dth = np.float32(TPI_F32 / np.float32(nth))
+    th = (np.arange(nth, dtype=np.float32) * dth).astype(np.float32)
+    ecos = np.cos(th.astype(np.float64)).astype(np.float32)
+    esin = np.sin(th.astype(np.float64)).astype(np.float32)
+    ecos[np.abs(ecos) < 1e-5] = 0.0
+    esin[np.abs(esin) < 1e-5] = 0.0
+    ec = np.tile(ecos, nk + 1)
+    es = np.tile(esin, nk + 1)
+    mapwn = np.repeat(np.arange(1, nk + 2, dtype=np.int32), nth)
+    return {"sig": sig, "dsip": dsip, "dth": float(dth), "ecos": ec, "esin": es,
+            "ec2": (ec * ec).astype(np.float32), "esc": (ec * es).astype(np.float32),
+            "es2": (es * es).astype(np.float32), "mapwn": mapwn, "nspec": nspec}
+
+
+def prop3_spectral_maps(nk, nth):
+    """MAPTH2 ((NK+2)*NTH) and MAPWN2 (NSPEC+NTH), W3MAP3 section 5 (the reference's
+    kokkos/src/ww_kokkos/prop_map3.hpp:242-275): 1-based indices into the rotated (NK+2, NTH)
+    work spectrum; MAPWN2 lists wavenumbers 1..NK-1, then the NK row, then the zero row."""
+    nk2 = nk + 2
+    mapth2 = np.zeros(nk2 * nth, np.int32)
+    for ik in range(1, nk + 1):
+        for ith in range(1, nth + 1):
+            mapth2[(ith + (ik - 1) * nth) - 1] = (ik + 1) + (ith - 1) * nk2
+    mapwn2 = []
+    for ik in range(1, nk):
+        for ith in range(1, nth + 1):
+            mapwn2.append((ik + 1) + (ith - 1) * nk2)
+    mapwn2 += [nk + 1 + (ith - 1) * nk2 for ith in range(1, nth + 1)]
+    mapwn2 += [1 + (ith - 1) * nk2 for ith in range(1, nth + 1)]
+    return mapth2, np.array(mapwn2, np.int32)
+
+
+def ktp3_case(npts, seed=0, nk=36, nth=36, nsea=None, depth_range=(5.0, 4000.0), ntloc=2,
+              dtg=900.0, currents=True):
+    """Seeded inputs of ww_ktp3_batch for npts sea points of a grid with nsea points (points
+    listed in a shuffled order, every other column of VA left untouched). Returns a dict with
+    the C ABI's arguments by name (column-major arrays flattened as the ABI reads them)."""
+    rng = np.random.default_rng(seed)
+    nsea = nsea or npts
+    nspec, nk2 = nk * nth, nk + 2
+    sp = spectral_arrays(nk, nth)
+    mapth2, mapwn2 = prop3_spectral_maps(nk, nth)
+    dep = np.exp(rng.uniform(np.log(depth_range[0]), np.log(depth_range[1]), nsea + 1))
+    k = wavenumber(sp["sig"], dep)  # (nsea+1, nk+2), column ISEA = row here
+    kd = np.minimum(k * dep[:, None], 40.0)
+    s64 = sp["sig"].astype(np.float64)[None, :]
+    cg = 0.5 * s64 / k * (1.0 + 2.0 * kd / np.sinh(np.minimum(2.0 * kd, 80.0)))
+    g = sea_states(nsea + 1, seed=seed + 17, nk=nk, nth=nth, depth_range=depth_range)
+    nsealm = nsea
+    va = np.zeros((nsealm + 1, nspec), np.float32)
+    va[1:] = g["a"][1:]
+    isea = rng.permutation(np.arange(1, nsea + 1))[:npts].astype(np.int32)
+    jsea = isea.copy()  # one rank: JSEA = ISEA
+    lat = rng.uniform(-70.0, 70.0, npts)
+    dmin = np.float32(0.1)
+    pscal = np.zeros((npts, 10), np.float32)
+    pscal[:, 0] = -np.tan(np.deg2rad(lat)) / 6.3661975e6
+    pscal[:, 1] = np.maximum(dmin, dep[isea])
+    pscal[:, 2] = rng.normal(0.0, 2e-3, npts)
+    pscal[:, 3] = rng.normal(0.0, 2e-3, npts)
+    if currents:
+        pscal[:, 4] = rng.normal(0.0, 0.3, npts)
+        pscal[:, 5] = rng.normal(0.0, 0.3, npts)
+        pscal[:, 6:10] = rng.normal(0.0, 2e-5, (npts, 4))
+    dth = np.float32(sp["dth"])
+    return {
+        "rpar": np.array([dmin, 0.7, np.float32(1.1) ** np.float32(-7.0)], np.float32),
+        "ipar": np.array([nk, nth, nspec, nk2, 1, 1, int(currents)], np.int32),
+        "sig": sp["sig"], "dsip": sp["dsip"], "ecos": sp["ecos"], "esin": sp["esin"],
+        "ec2": sp["ec2"], "esc": sp["esc"], "es2": sp["es2"], "mapwn": sp["mapwn"],
+        "mapth2": mapth2, "mapwn2": mapwn2,
+        "facth": float(np.float32(dtg / (float(dth) * ntloc))),
+        "fack": float(np.float32(dtg / ntloc)), "nsea": nsea,
+        "cg": cg.astype(np.float32).reshape(-1), "wn": k.astype(np.float32).reshape(-1),
+        "npts": npts, "jsea": jsea, "isea": isea, "pscal": pscal.reshape(-1),
+        "va": va, "nsealm": nsealm,
+        "cflthmax": np.full(nsealm, -1.0, np.float32), "cflkmax": np.full(nsealm, -1.0, np.float32),
+    }
