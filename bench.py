@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--npts", type=int, default=NPTS_PER_GPU)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band"], default="auto",
+    p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band", "tile"], default="auto",
                    help="DIA kernel (ww_snl1_select_kernel); auto picks the band kernel")
     return p.parse_args()
 
@@ -237,10 +237,12 @@ def run_b200(args):
     g = synth.sea_states_chunked(npts, seed=2024 + rank, depth=4000.0)
     grid = pkg.Snl1Grid(cfg, sig, igrid=1)
     kernel_ids = {"auto": pkg.KERNEL_AUTO, "gather": pkg.KERNEL_GATHER,
-                  "rowshift": pkg.KERNEL_ROWSHIFT, "band": pkg.KERNEL_BAND}
+                  "rowshift": pkg.KERNEL_ROWSHIFT, "band": pkg.KERNEL_BAND,
+                  "tile": pkg.KERNEL_TILE}
     grid.select_kernel(kernel_ids[args.kernel])
     kernel_name = {pkg.KERNEL_GATHER: "snl1_gather_kernel", pkg.KERNEL_ROWSHIFT:
-                   "snl1_rowshift_kernel", pkg.KERNEL_BAND: "snl1_band_kernel"}[
+                   "snl1_rowshift_kernel", pkg.KERNEL_BAND: "snl1_band_kernel",
+                   pkg.KERNEL_TILE: "snl1_tile_kernel"}[
                        grid.select_kernel(kernel_ids[args.kernel])]
     dev = torch.device("cuda", local)
     a = torch.from_numpy(g["a"]).to(dev)

@@ -87,10 +87,12 @@ int ww_snl1_enabled(void);
 /* Replaces ww_snl1_last_error (ww_kokkos_c.hpp:133). */
 int ww_snl1_last_error(void);
 
-/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the band kernel when
- * INSNL1's tables have the row-shift form and fit it, else the row-shift kernel, else the
- * gather kernel), 1 the gather kernel over the index tables, 2 the row-shift kernel (one CTA
- * per point), 3 the band kernel (register windows over frequency bands, TMA-staged input).
+/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the tile kernel when
+ * INSNL1's tables have the row-shift form and one of its instances fits them, else the band
+ * kernel, else the row-shift kernel, else the gather kernel), 1 the gather kernel over the
+ * index tables, 2 the row-shift kernel (one CTA per point), 3 the band kernel (register
+ * windows over frequency bands, TMA-staged input), 4 the tile kernel (the band kernel compiled
+ * for 36 or 24 directions, zero-padded rows, no clamps).
  * Returns the previous choice, or -1 for an unknown grid or a choice its tables cannot run. */
 int ww_snl1_select_kernel(int igrid, int which);
 
@@ -164,6 +166,39 @@ int ww_ktp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, i
                      float fack, int nsea, const float* cg, const float* wn, int npts,
                      const int* jsea, const int* isea, const float* pscal, float* va, int nspec,
                      int nsealm, float* cflthmax, float* cflkmax);
+
+/* Replaces ww_xyp3_batch (prop3_c.hpp:25-32): W3GATH, W3XYP3, W3SCAT for every component
+ * ISPEC with on[ISPEC-1] /= 0 (W3WAVE's ISPEC loop, W3_SHRD). rpar[5] = DTCFL, DTH, XFR, WDCG,
+ * WDTH; ipar[11] = NX, NY, NSEA, NK, NTH, NSPEC, ICLOSE, FLCX, FLCY, FLAGLL, FLCUR; imaps[8] =
+ * NMX0, NMX1, NMX2, NMY0, NMY1, NMY2, NACT, NCENT; tscal[3] = DSEC21 of the day, of TBPI0 to
+ * TIME, of TBPI0 to TBPIN; mapsf (NSEA,3); clats (0:NSEA); sig (0:NK+1); ecos, esin
+ * (NSPEC+NTH); dpdx, dpdy, dqdx, dqdy, gsqrt (NY,NX); atrnx, atrny (NY*NX,-1:1); mapx2, mapy2,
+ * mapaxy, maptrn (0/1), mapsta (NY*NX); mapcxy (NSEA); cg (0:NK+1, 0:NSEA); cx, cy (0:NSEA);
+ * flbpi, nbi, isbpi (NBI), bbpi0, bbpin (NSPEC, 0:NBI); on (NSPEC); va (NSPEC, 0:NSEALM) with
+ * ncol = NSEALM+1. The averaging's order-dependent sums are reproduced bit for bit (an ordered
+ * gather per target cell). Tripole grids are UNSUPPORTED, as in the reference. */
+int ww_xyp3_batch(const float* rpar, int nrpar, const int* ipar, int nipar, const int* imaps,
+                  int nimaps, const float* tscal, int ntscal, float dtg, const int* mapsf,
+                  const float* clats, const float* sig, const float* ecos, const float* esin,
+                  const float* dpdx, const float* dpdy, const float* dqdx, const float* dqdy,
+                  const float* gsqrt, const float* atrnx, const float* atrny, const int* mapx2,
+                  const int* mapy2, const int* mapaxy, const int* mapcxy, const int* maptrn,
+                  const int* mapsta, const float* cg, const float* cx, const float* cy,
+                  int flbpi, int nbi, const int* isbpi, const float* bbpi0, const float* bbpin,
+                  const int* on, int ncol, float* va);
+
+/* Replaces ww_xyp3_batch_va (prop3_c.hpp:37-46): ww_xyp3_batch on the resident VA of grid
+ * igrid (synced to the device first, state DEVICE afterwards). */
+int ww_xyp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar,
+                     const int* imaps, int nimaps, const float* tscal, int ntscal, float dtg,
+                     const int* mapsf, const float* clats, const float* sig, const float* ecos,
+                     const float* esin, const float* dpdx, const float* dpdy, const float* dqdx,
+                     const float* dqdy, const float* gsqrt, const float* atrnx,
+                     const float* atrny, const int* mapx2, const int* mapy2, const int* mapaxy,
+                     const int* mapcxy, const int* maptrn, const int* mapsta, const float* cg,
+                     const float* cx, const float* cy, int flbpi, int nbi, const int* isbpi,
+                     const float* bbpi0, const float* bbpin, const int* on, float* va, int nspec,
+                     int nsealm);
 
 /* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* call (the reference
  * returns it only). */

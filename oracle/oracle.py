@@ -235,3 +235,45 @@ def ktp3_call(L, case, itstep=1, ntimes=1):
                          keep[4].ctypes.data, va.shape[0], va.ctypes.data, cth.ctypes.data,
                          ck.ctypes.data)
     return rc, va, cth, ck
+
+
+# ---------------------------------------------------------------- W3MAP3 and W3XYP3
+def ref_w3map3(nx, ny, nsea, nk, nth, mapsta, mapsf):
+    """The reference's W3MAP3 (prop_map3.hpp) on a grid: (mapx2, mapy2, mapaxy, mapcxy, counts)."""
+    L = ref_lib()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.ref_w3map3.argtypes = [I, I, I, I, I] + [P] * 9
+    L.ref_w3map3.restype = I
+    nxy = nx * ny
+    out = [np.zeros(nxy, np.int32) for _ in range(3)] + [np.zeros(nsea, np.int32),
+                                                         np.zeros((nk + 2) * nth, np.int32),
+                                                         np.zeros(nk * nth + nth, np.int32),
+                                                         np.zeros(8, np.int32)]
+    mapsta = np.ascontiguousarray(mapsta, np.int32)
+    mapsf = np.ascontiguousarray(mapsf, np.int32)
+    L.ref_w3map3(nx, ny, nsea, nk, nth, mapsta.ctypes.data, mapsf.ctypes.data,
+                 *[o.ctypes.data for o in out])
+    return out[0], out[1], out[2], out[3], out[6]
+
+
+XYP3_ARGS = ("mapsf", "clats", "sig", "ecos", "esin", "dpdx", "dpdy", "dqdx", "dqdy", "gsqrt",
+             "atrnx", "atrny", "mapx2", "mapy2", "mapaxy", "mapcxy", "maptrn", "mapsta", "cg",
+             "cx", "cy")
+
+
+def xyp3_call(L, case):
+    """ww_xyp3_batch of library L on a synth.xyp3_case dict; returns (status, va)."""
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.ww_xyp3_batch.argtypes = [P, I, P, I, P, I, P, I, F] + [P] * 21 + [I, I, P, P, P, P, I, P]
+    L.ww_xyp3_batch.restype = I
+    va = np.array(case["va"], np.float32, copy=True)
+    keep = {k: np.ascontiguousarray(case[k]) for k in
+            ("rpar", "ipar", "imaps", "tscal", "isbpi", "bbpi0", "bbpin", "on") + XYP3_ARGS}
+    rc = L.ww_xyp3_batch(keep["rpar"].ctypes.data, keep["rpar"].size, keep["ipar"].ctypes.data,
+                         keep["ipar"].size, keep["imaps"].ctypes.data, keep["imaps"].size,
+                         keep["tscal"].ctypes.data, keep["tscal"].size, case["dtg"],
+                         *[keep[k].ctypes.data for k in XYP3_ARGS], case["flbpi"], case["nbi"],
+                         keep["isbpi"].ctypes.data, keep["bbpi0"].ctypes.data,
+                         keep["bbpin"].ctypes.data, keep["on"].ctypes.data, va.shape[0],
+                         va.ctypes.data)
+    return rc, va

@@ -54,3 +54,30 @@ extern "C" int ref_snl1_tables(int nk, int nth, float xfr, float dth, float lam,
 // prop3_shim.cpp's exit report names the unstructured-grid shim's counter, which this build
 // leaves out (that propagation scheme is not on the path); an empty report stands in for it.
 extern "C" void ww_xypug_report(void) {}
+
+// W3MAP3 of the reference (kokkos/src/ww_kokkos/prop_map3.hpp:65-340), to build the PR3 maps of
+// synthetic grids for the tests: mapsta (NY*NX), mapsf (NSEA,3) column-major in; mapx2, mapy2,
+// mapaxy (NY*NX), mapcxy (NSEA), mapth2 ((NK+2)*NTH, zeroed), mapwn2 (NK*NTH+NTH) and
+// counts[8] = NMX0, NMX1, NMX2, NMY0, NMY1, NMY2, NACT, NCENT out.
+#include "ww_kokkos/prop_map3.hpp"
+
+extern "C" int ref_w3map3(int nx, int ny, int nsea, int nk, int nth, const int* mapsta,
+                          const int* mapsf, int* mapx2, int* mapy2, int* mapaxy, int* mapcxy,
+                          int* mapth2, int* mapwn2, int* counts) {
+  using namespace ww::prop;
+  Map3Scalars s{nx, ny, nsea, nk, nth, 1};
+  using V = Map3Views<Kokkos::HostSpace>;
+  V v;
+  v.mapsta = V::I1(mapsta, static_cast<size_t>(nx) * ny);
+  v.mapsf = V::I2(mapsf, static_cast<size_t>(nsea), 3);
+  v.mapx2 = V::W1(mapx2, static_cast<size_t>(nx) * ny);
+  v.mapy2 = V::W1(mapy2, static_cast<size_t>(nx) * ny);
+  v.mapaxy = V::W1(mapaxy, static_cast<size_t>(nx) * ny);
+  v.mapcxy = V::W1(mapcxy, static_cast<size_t>(nsea));
+  v.mapth2 = V::W1(mapth2, static_cast<size_t>(nk + 2) * nth);
+  v.mapwn2 = V::W1(mapwn2, static_cast<size_t>(nk) * nth + nth);
+  v.counts = V::W1(counts, 8);
+  Map3Counts c{};
+  w3map3(Kokkos::DefaultHostExecutionSpace(), s, v, c);
+  return 0;
+}

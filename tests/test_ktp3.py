@@ -12,7 +12,6 @@ from conftest import assert_bitexact, cuda_available
 from oracle import oracle as _oracle
 
 needs_ref = pytest.mark.skipif(not _oracle.ref_available(), reason="oracle/_ref not built")
-gpu = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
 
 
 @needs_ref
@@ -43,8 +42,8 @@ def test_reference_ktp3_still_water_no_currents_keeps_directions(oracle, synth):
 @pytest.mark.parametrize("itstep,ntimes,currents", [(1, 1, True), (2, 1, True), (2, 2, False),
                                                     (3, 3, True)])
 @needs_ref
+@pytest.mark.gpu
 def test_ktp3_gpu_bitexact(pkg, oracle, synth, itstep, ntimes, currents):
-    pytest.importorskip("torch")
     if not cuda_available():
         pytest.skip("needs a CUDA device")
     c = synth.ktp3_case(1500, seed=10 + itstep, nsea=2000, currents=currents)
@@ -55,8 +54,6 @@ def test_ktp3_gpu_bitexact(pkg, oracle, synth, itstep, ntimes, currents):
     assert_bitexact(cth, cth_r, "CFLTHMAX")
     assert_bitexact(ck, ck_r, "CFLKMAX")
 
-
-test_ktp3_gpu_bitexact = pytest.mark.gpu(test_ktp3_gpu_bitexact)
 
 
 @needs_ref

@@ -31,7 +31,7 @@ ERR_UNSUPPORTED = 5
 ERR_TABLE = 6
 
 # ww_snl1_select_kernel choices
-KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT, KERNEL_BAND = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT, KERNEL_BAND, KERNEL_TILE = 0, 1, 2, 3, 4
 
 # Every symbol include/ww_b200.h declares.
 EXPORTS = (
@@ -41,7 +41,7 @@ EXPORTS = (
     "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
     "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_ktp3_batch", "ww_ktp3_batch_va",
-    "ww_prop3_last_error",
+    "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -113,6 +113,12 @@ def lib():
             _I, _I, _F, _F, _I, _P, _P, _I, _P, _P, _P, _P, _I, _I, _P, _P]
         L.ww_ktp3_batch_va.restype = _I
         L.ww_prop3_last_error.restype = _I
+        L.ww_xyp3_batch.argtypes = [_P, _I, _P, _I, _P, _I, _P, _I, _F] + [_P] * 21 + [
+            _I, _I, _P, _P, _P, _P, _I, _P]
+        L.ww_xyp3_batch.restype = _I
+        L.ww_xyp3_batch_va.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _F] + [_P] * 21 + [
+            _I, _I, _P, _P, _P, _P, _P, _I, _I]
+        L.ww_xyp3_batch_va.restype = _I
         _lib = L
     return _lib
 
@@ -273,3 +279,31 @@ def va_host_read(igrid, va):
 
 def va_host_write(igrid, va):
     return lib().ww_va_host_write(igrid, va.ctypes.data, va.shape[1], va.shape[0] - 1)
+
+
+XYP3_ARRAYS = ("mapsf", "clats", "sig", "ecos", "esin", "dpdx", "dpdy", "dqdx", "dqdy", "gsqrt",
+               "atrnx", "atrny", "mapx2", "mapy2", "mapaxy", "mapcxy", "maptrn", "mapsta", "cg",
+               "cx", "cy")
+
+
+def xyp3_batch(case, igrid=None, va=None):
+    """ww_xyp3_batch (or ww_xyp3_batch_va on the resident VA bound to ``va`` when ``igrid`` is
+    given) with a dict of the C ABI's arguments (see synth.xyp3_case). Returns (status, va)."""
+    L = lib()
+    init()
+    keep = {k: np.ascontiguousarray(case[k]) for k in
+            ("rpar", "ipar", "imaps", "tscal", "isbpi", "bbpi0", "bbpin", "on") + XYP3_ARRAYS}
+    head = [keep["rpar"].ctypes.data, keep["rpar"].size, keep["ipar"].ctypes.data,
+            keep["ipar"].size, keep["imaps"].ctypes.data, keep["imaps"].size,
+            keep["tscal"].ctypes.data, keep["tscal"].size, case["dtg"]]
+    arrs = [keep[k].ctypes.data for k in XYP3_ARRAYS]
+    tail = [case["flbpi"], case["nbi"], keep["isbpi"].ctypes.data, keep["bbpi0"].ctypes.data,
+            keep["bbpin"].ctypes.data, keep["on"].ctypes.data]
+    if igrid is None:
+        v = np.array(case["va"], np.float32, copy=True)
+        rc = L.ww_xyp3_batch(*head, *arrs, *tail, v.shape[0], v.ctypes.data)
+    else:
+        v = va
+        rc = L.ww_xyp3_batch_va(igrid, *head, *arrs, *tail, v.ctypes.data, v.shape[1],
+                                v.shape[0] - 1)
+    return rc, v

@@ -10,12 +10,16 @@
 
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <cstdint>
 #include <new>
+#include <vector>
 
 #include "ktp3_kernel.cuh"
 #include "staging.hpp"
 #include "va.hpp"
 #include "wwb_common.hpp"
+#include "xyp3_kernel.cuh"
 
 namespace wwb {
 namespace {
@@ -116,6 +120,184 @@ int ktp3_entry(int igrid, bool resident, const float* rpar, int nrpar, const int
   return WW_KOKKOS_OK;
 }
 
+constexpr int kXyp3NRpar = 5, kXyp3NIpar = 11, kXyp3NImaps = 8, kXyp3NTscal = 3;
+constexpr int kIcloseNone = -1, kIcloseTrpl = 8;
+/// Work storage of one XYP3 chunk is capped so a call never asks for more than this.
+constexpr size_t kXyp3ChunkBytes = size_t(8) << 30;
+
+struct Xyp3Args {
+  const float *rpar, *tscal, *clats, *sig, *ecos, *esin, *dpdx, *dpdy, *dqdx, *dqdy, *gsqrt;
+  const float *atrnx, *atrny, *cg, *cx, *cy, *bbpi0, *bbpin;
+  const int *ipar, *imaps, *mapsf, *mapx2, *mapy2, *mapaxy, *mapcxy, *maptrn, *mapsta, *isbpi,
+      *on;
+  int nrpar, nipar, nimaps, ntscal, flbpi, nbi, ncol;
+  float dtg;
+  float* va;
+};
+
+int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int nsealm) {
+  if (!a.rpar || !a.ipar || !a.imaps || !a.tscal || a.nrpar != kXyp3NRpar ||
+      a.nipar != kXyp3NIpar || a.nimaps != kXyp3NImaps || a.ntscal != kXyp3NTscal)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: bad packet");
+  Xyp3Grid g{};
+  g.dtcfl = a.rpar[0];
+  g.dth = a.rpar[1];
+  g.xfr = a.rpar[2];
+  g.wdcg = a.rpar[3];
+  g.wdth = a.rpar[4];
+  g.nx = a.ipar[0];
+  g.ny = a.ipar[1];
+  g.nsea = a.ipar[2];
+  g.nk = a.ipar[3];
+  g.nth = a.ipar[4];
+  g.nspec = a.ipar[5];
+  g.iclose = a.ipar[6];
+  g.flcx = a.ipar[7];
+  g.flcy = a.ipar[8];
+  g.flagll = a.ipar[9];
+  g.flcur = a.ipar[10];
+  if (g.nx < 1 || g.ny < 1 || g.nsea < 1 || g.nk < 1 || g.nth < 1 || g.nspec != g.nk * g.nth ||
+      a.ncol < g.nsea + 1 || a.nbi < 0 || !a.mapsf || !a.clats || !a.sig || !a.ecos || !a.esin ||
+      !a.dpdx || !a.dpdy || !a.dqdx || !a.dqdy || !a.gsqrt || !a.atrnx || !a.atrny ||
+      !a.mapx2 || !a.mapy2 || !a.mapaxy || !a.mapcxy || !a.maptrn || !a.mapsta || !a.cg ||
+      !a.cx || !a.cy || !a.on || !a.va ||
+      (a.flbpi != 0 && (!a.isbpi || !a.bbpi0 || !a.bbpin)) ||
+      (resident && nspec_va != g.nspec))
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: bad sizes or null pointer");
+  if (g.iclose == kIcloseTrpl)
+    return fail(WW_KOKKOS_ERR_UNSUPPORTED, "ww_xyp3_batch: tripole grid (W3XYP3 stops there)");
+  g.global = g.iclose != kIcloseNone ? 1 : 0;
+  if (g.global && g.nx < 3)
+    return fail(WW_KOKKOS_ERR_UNSUPPORTED, "ww_xyp3_batch: a closed grid needs NX >= 3");
+  g.nmx0 = a.imaps[0];
+  g.nmx1 = a.imaps[1];
+  g.nmx2 = a.imaps[2];
+  g.nmy0 = a.imaps[3];
+  g.nmy1 = a.imaps[4];
+  g.nmy2 = a.imaps[5];
+  g.nact = a.imaps[6];
+  g.ncent = a.imaps[7];
+  const int nx = g.nx, ny = g.ny, nsea = g.nsea, nxy = nx * ny;
+  // Every map entry must address the arrays the kernels hold.
+  auto bad_counts = [&](int c0, int c1, int c2) { return c0 < 0 || c1 < c0 || c2 < c1 || c2 > nxy; };
+  if (bad_counts(g.nmx0, g.nmx1, g.nmx2) || bad_counts(g.nmy0, g.nmy1, g.nmy2) || g.nact < 0 ||
+      g.nact > nxy || g.ncent < 0 || g.ncent > nsea)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: map counts out of range");
+  for (int i = 0; i < g.nmx2; ++i)
+    if (a.mapx2[i] < 1 || a.mapx2[i] > nxy) return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: MAPX2 out of range");
+  for (int i = 0; i < g.nmy2; ++i)
+    if (a.mapy2[i] < 1 || a.mapy2[i] > nxy) return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: MAPY2 out of range");
+  for (int i = 0; i < g.nact; ++i)
+    if (a.mapaxy[i] < 1 || a.mapaxy[i] > nxy) return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: MAPAXY out of range");
+  std::vector<int> cell_sea(nxy, 0), sea_pos(nsea, 0), bnd_last(nsea, 0);
+  for (int isea = 1; isea <= nsea; ++isea) {
+    const int ix = a.mapsf[isea - 1], iy = a.mapsf[nsea + isea - 1], ixy = a.mapsf[2 * nsea + isea - 1];
+    if (ix < 1 || ix > nx || iy < 1 || iy > ny || ixy != (ix - 1) * ny + iy || cell_sea[ixy - 1] != 0)
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: MAPSF is not a map of sea cells");
+    cell_sea[ixy - 1] = isea;
+  }
+  for (int ip = 1; ip <= nsea; ++ip) {
+    const int isea = a.mapcxy[ip - 1];
+    if (isea < 1 || isea > nsea || sea_pos[isea - 1] != 0)
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: MAPCXY is not a permutation");
+    sea_pos[isea - 1] = ip;
+  }
+  const int nbi = a.flbpi != 0 ? a.nbi : 0;
+  for (int ibi = 1; ibi <= nbi; ++ibi) {
+    const int ib = a.isbpi[ibi - 1];
+    if (ib < 1 || ib > nsea) return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: ISBPI out of range");
+    bnd_last[ib - 1] = ibi;  // the last IBI naming a point wins, as the serial loop's last write
+  }
+  std::vector<int> mapstx(static_cast<size_t>(ny) * (nx + 4), 0);
+  for (int i = 1; i <= nxy; ++i) mapstx[i + 2 * ny - 1] = a.mapsta[i - 1];
+  if (g.global)
+    for (int j = 0; j < 2 * ny; ++j) {
+      mapstx[(1 - 2 * ny + j) + 2 * ny - 1] = a.mapsta[(nx - 2) * ny + j];
+      mapstx[(nxy + 1 + j) + 2 * ny - 1] = a.mapsta[j];
+    }
+  std::vector<int> list;
+  for (int isp = 1; isp <= g.nspec; ++isp)
+    if (a.on[isp - 1] != 0) list.push_back(isp);
+  if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+  timers::Region t_call("xyp3.call");
+  Staging& st = staging();
+  cudaStream_t s = runtime().stream;
+  const size_t nk2 = static_cast<size_t>(g.nk) + 2, ntab = static_cast<size_t>(g.nspec) + g.nth;
+  int slot = 0;
+  g.mapsf = st.in(slot++, a.mapsf, 3 * static_cast<size_t>(nsea), s);
+  g.clats = st.in(slot++, a.clats, static_cast<size_t>(nsea) + 1, s);
+  g.sig = st.in(slot++, a.sig, nk2, s);
+  g.ecos = st.in(slot++, a.ecos, ntab, s);
+  g.esin = st.in(slot++, a.esin, ntab, s);
+  g.dpdx = st.in(slot++, a.dpdx, static_cast<size_t>(nxy), s);
+  g.dpdy = st.in(slot++, a.dpdy, static_cast<size_t>(nxy), s);
+  g.dqdx = st.in(slot++, a.dqdx, static_cast<size_t>(nxy), s);
+  g.dqdy = st.in(slot++, a.dqdy, static_cast<size_t>(nxy), s);
+  g.gsqrt = st.in(slot++, a.gsqrt, static_cast<size_t>(nxy), s);
+  g.atrnx = st.in(slot++, a.atrnx, 3 * static_cast<size_t>(nxy), s);
+  g.atrny = st.in(slot++, a.atrny, 3 * static_cast<size_t>(nxy), s);
+  g.mapx2 = st.in(slot++, a.mapx2, static_cast<size_t>(nxy), s);
+  g.mapy2 = st.in(slot++, a.mapy2, static_cast<size_t>(nxy), s);
+  g.mapaxy = st.in(slot++, a.mapaxy, static_cast<size_t>(nxy), s);
+  g.maptrn = st.in(slot++, a.maptrn, static_cast<size_t>(nxy), s);
+  g.mapsta = st.in(slot++, a.mapsta, static_cast<size_t>(nxy), s);
+  g.mapstx = st.in(slot++, mapstx.data(), mapstx.size(), s);
+  g.cell_sea = st.in(slot++, cell_sea.data(), cell_sea.size(), s);
+  g.sea_pos = st.in(slot++, sea_pos.data(), sea_pos.size(), s);
+  g.bnd_last = st.in(slot++, bnd_last.data(), bnd_last.size(), s);
+  g.cg = st.in(slot++, a.cg, nk2 * (static_cast<size_t>(nsea) + 1), s);
+  g.cx = st.in(slot++, a.cx, static_cast<size_t>(nsea) + 1, s);
+  g.cy = st.in(slot++, a.cy, static_cast<size_t>(nsea) + 1, s);
+  const size_t nbb = nbi > 0 ? static_cast<size_t>(g.nspec) * (nbi + 1) : 1;
+  static const float kZero[1] = {0.0f};
+  g.bbpi0 = nbi > 0 ? st.in(slot++, a.bbpi0, nbb, s) : st.in(slot++, kZero, 1, s);
+  g.bbpin = nbi > 0 ? st.in(slot++, a.bbpin, nbb, s) : st.in(slot++, kZero, 1, s);
+  g.flbpi = a.flbpi != 0 ? 1 : 0;
+  g.nbi = nbi;
+  g.dsec_day = a.tscal[0];
+  g.dsec_bpi0 = a.flbpi != 0 ? a.tscal[1] : 0.0f;
+  g.dsec_bpin = a.flbpi != 0 ? a.tscal[2] : 0.0f;
+  g.dtg = a.dtg;
+  if (g.flcur != 0) xyp3_current_range(g, s);
+  float* d_va = nullptr;
+  if (resident) {
+    const int rc = va_device(igrid, a.va, nspec_va, nsealm, &d_va);
+    if (rc != WW_KOKKOS_OK) return fail(rc, "ww_xyp3_batch_va: the resident VA refused this call");
+  } else {
+    d_va = st.in(slot++, a.va, static_cast<size_t>(g.nspec) * a.ncol, s);
+  }
+  const int* d_list = st.in(slot++, list.data(), list.size(), s);
+  // Chunks of components, their work arrays carved from one staging slot.
+  const size_t per = xyp3_bytes_per_component(g);
+  const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(list.size(), kXyp3ChunkBytes / per)));
+  const size_t nq = static_cast<size_t>(ny) * (nx + 3), n1 = static_cast<size_t>(ny) * (nx + 1);
+  char* base = static_cast<char*>(st.get(slot++, per * chunk + 256));
+  for (size_t c0 = 0; c0 < list.size(); c0 += chunk) {
+    Xyp3Chunk ch{};
+    ch.ncomp = static_cast<int>(std::min<size_t>(chunk, list.size() - c0));
+    ch.isp = d_list + c0;
+    float* f = reinterpret_cast<float*>(base);
+    ch.vq = f;
+    ch.aq = ch.vq + nq * chunk;
+    ch.vlcflx = ch.aq + nq * chunk;
+    ch.vlcfly = ch.vlcflx + n1 * chunk;
+    ch.fla = ch.vlcfly + n1 * chunk;
+    ch.rdi = ch.fla + n1 * chunk;
+    ch.iixy = reinterpret_cast<int*>(ch.rdi + 4 * static_cast<size_t>(nsea) * chunk);
+    ch.comp = reinterpret_cast<Comp*>(
+        (reinterpret_cast<uintptr_t>(ch.iixy + 4 * static_cast<size_t>(nsea) * chunk) + 63) &
+        ~static_cast<uintptr_t>(63));
+    run_xyp3_chunk(g, ch, d_va, s);
+  }
+  if (resident) va_device_written(igrid);
+  else
+    WWB_CHECK(cudaMemcpyAsync(a.va, d_va, sizeof(float) * g.nspec * static_cast<size_t>(a.ncol),
+                              cudaMemcpyDeviceToHost, s));
+  WWB_CHECK(cudaStreamSynchronize(s));
+  g_prop3.ok();
+  return WW_KOKKOS_OK;
+}
+
 template <class F>
 int guarded(F&& f) {
   try {
@@ -163,6 +345,39 @@ int ww_ktp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, i
                       npts, jsea, isea, pscal, nsealm + 1, va, nspec, nsealm, cflthmax,
                       cflkmax);
   });
+}
+
+int ww_xyp3_batch(const float* rpar, int nrpar, const int* ipar, int nipar, const int* imaps,
+                  int nimaps, const float* tscal, int ntscal, float dtg, const int* mapsf,
+                  const float* clats, const float* sig, const float* ecos, const float* esin,
+                  const float* dpdx, const float* dpdy, const float* dqdx, const float* dqdy,
+                  const float* gsqrt, const float* atrnx, const float* atrny, const int* mapx2,
+                  const int* mapy2, const int* mapaxy, const int* mapcxy, const int* maptrn,
+                  const int* mapsta, const float* cg, const float* cx, const float* cy,
+                  int flbpi, int nbi, const int* isbpi, const float* bbpi0, const float* bbpin,
+                  const int* on, int ncol, float* va) {
+  const Xyp3Args a{rpar,  tscal, clats, sig,    ecos,   esin,   dpdx,   dpdy,   dqdx,   dqdy,
+                   gsqrt, atrnx, atrny, cg,     cx,     cy,     bbpi0,  bbpin,  ipar,   imaps,
+                   mapsf, mapx2, mapy2, mapaxy, mapcxy, maptrn, mapsta, isbpi,  on,     nrpar,
+                   nipar, nimaps, ntscal, flbpi, nbi, ncol, dtg, va};
+  return guarded([&] { return xyp3_entry(0, false, a, 0, 0); });
+}
+
+int ww_xyp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar,
+                     const int* imaps, int nimaps, const float* tscal, int ntscal, float dtg,
+                     const int* mapsf, const float* clats, const float* sig, const float* ecos,
+                     const float* esin, const float* dpdx, const float* dpdy, const float* dqdx,
+                     const float* dqdy, const float* gsqrt, const float* atrnx,
+                     const float* atrny, const int* mapx2, const int* mapy2, const int* mapaxy,
+                     const int* mapcxy, const int* maptrn, const int* mapsta, const float* cg,
+                     const float* cx, const float* cy, int flbpi, int nbi, const int* isbpi,
+                     const float* bbpi0, const float* bbpin, const int* on, float* va, int nspec,
+                     int nsealm) {
+  const Xyp3Args a{rpar,  tscal, clats, sig,    ecos,   esin,   dpdx,   dpdy,   dqdx,   dqdy,
+                   gsqrt, atrnx, atrny, cg,     cx,     cy,     bbpi0,  bbpin,  ipar,   imaps,
+                   mapsf, mapx2, mapy2, mapaxy, mapcxy, maptrn, mapsta, isbpi,  on,     nrpar,
+                   nipar, nimaps, ntscal, flbpi, nbi, nsealm + 1, dtg, va};
+  return guarded([&] { return xyp3_entry(igrid, true, a, nspec, nsealm); });
 }
 
 int ww_prop3_last_error(void) { return g_prop3.get(); }

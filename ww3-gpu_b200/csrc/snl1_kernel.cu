@@ -626,7 +626,239 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
 #undef WWB_LOAD_M
 }
 
+// ------------------------------------------------------------------------------------------
+// Tile kernel: the band kernel with the direction count NTH and the band height BR known at
+// compile time, for the grids that dominate (36 directions, 8 bands of 5 rows; 24 directions,
+// 12 bands of 3 rows).
+//
+// Every matrix gets PAD extra zero rows below row 0 (PAD >= MAX(IFRP, -IFRM)), so the clamped
+// rows MAX(0, IFR + IFRM) etc. of INSNL1 read zeros without a clamp: the rows a band touches are
+// then affine in its first row, each thread keeps one shared-memory pointer per (array group,
+// wrapped column) and every access in the unrolled row loops is that pointer plus a
+// compile-time offset. The arithmetic of each bin is the reference's, as in the other kernels.
+template <int NTH, int G, int BR>
+struct TileShape {
+  static constexpr int kBlock = NTH * G;
+  static constexpr int kPad = 4;                      // zero rows below row 0
+  static constexpr int kRows = G * BR;                // rows the bands cover (>= NFRCHG)
+  static constexpr int kAS = (kRows + 1 + kPad) * NTH;  // interaction-array stride
+};
+
+template <int NTH, int G, int BR, int MINB>
+__global__ void __launch_bounds__(NTH * G, MINB) snl1_tile_kernel(
+    const Snl1Dev p, const int npts, const float* __restrict__ a, const float* __restrict__ cg,
+    const float* __restrict__ kdmean, float* __restrict__ s, float* __restrict__ d,
+    int* __restrict__ err) {
+  using S = TileShape<NTH, G, BR>;
+  constexpr int BLOCK = S::kBlock, PAD = S::kPad, AS = S::kAS;
+  extern __shared__ __align__(16) float smem[];
+  const int nfr = p.nfr, nfrhgh = p.nfrhgh, nfrchg = p.nfrchg, nspec = p.nspec, nk = p.nk;
+  const int ulen = (nfrhgh + 1 + PAD) * NTH;
+  float* const ue = smem;  // row r at ue + (r + PAD) * NTH
+  float* const arrs = ue + ((ulen + 3) & ~3);
+  float* const sa1 = arrs;
+  float* const sa2 = arrs + AS;
+  float* const da1p = arrs + 2 * AS;
+  float* const da1m = arrs + 3 * AS;
+  float* const da2p = arrs + 4 * AS;
+  float* const da2m = arrs + 5 * AS;
+  float* const dcs = arrs + 6 * AS;        // rows 1..G*BR, row r at dcs + (r - 1) * NTH
+  float* const conx2 = dcs + S::kRows * NTH;
+  float* const afr = conx2 + ((2 * nk + 3) & ~3);
+  float* const stage = afr + ((nfrchg + 3) & ~3);  // 16-byte aligned: every offset above is
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(stage + ((nspec + nk + 3) & ~3));
+  const int tid = threadIdx.x;
+
+  // Once per CTA: the zero rows (PAD below row 0, and row 0) of UE and the six arrays.
+  for (int i = tid; i < (PAD + 1) * NTH; i += BLOCK) {
+    ue[i] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) arrs[j * AS + i] = 0.0f;
+  }
+  for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    if (blockIdx.x < npts) tma_fetch_point(bar, stage, a, cg, blockIdx.x, nspec, nk);
+  }
+  __syncthreads();
+
+  const int ith = tid % NTH, band = tid / NTH;
+  const int f0 = 1 + band * BR;
+  const int n3 = max(0, min(BR, nfrchg - f0 + 1));
+  const int n4 = max(0, min(BR, nfr - f0 + 1));
+  const int c0 = wrapc(ith + p.shift[0], NTH), c1 = wrapc(ith + p.shift[1], NTH);
+  const int c2 = wrapc(ith + p.shift[2], NTH), c3 = wrapc(ith + p.shift[3], NTH);
+  const int c4 = wrapc(ith + p.shift[4], NTH), c5 = wrapc(ith + p.shift[5], NTH);
+  const int c6 = wrapc(ith + p.shift[6], NTH), c7 = wrapc(ith + p.shift[7], NTH);
+  const int ifrp = p.ifrp, ifrm = p.ifrm;
+  const float dal1 = p.dal1, dal2 = p.dal2, dal3 = p.dal3;
+  // Row bases (in floats, PAD included) of this thread's band.
+  const int rP = (f0 + ifrp + PAD) * NTH;      // IF1 of the band's first row
+  const int rM = (f0 + ifrm - 1 + PAD) * NTH;  // IF4 of the band's first row
+  const int rO = (f0 + PAD) * NTH + ith;       // the band's own bins
+  const int rL = (f0 - ifrp - 1 + PAD) * NTH;  // IF6 of the band's first row
+  const int rH = (f0 - ifrm + PAD) * NTH;      // IF7 of the band's first row
+
+  float kd_next = (blockIdx.x < npts) ? __ldg(kdmean + blockIdx.x) : 0.0f;
+  unsigned parity = 0;
+  int buf = 0;
+  for (int ipt = blockIdx.x; ipt < npts; ipt += gridDim.x, buf ^= 1) {
+    float* const conx = conx2 + buf * nk;
+    mbar_wait(bar, parity, err);
+    parity ^= 1u;
+    const float cons = dia_cons(p, kd_next);
+    for (int k = tid; k < nk; k += BLOCK) conx[k] = kTpiInv / __ldg(p.sig + k) * stage[nspec + k];
+    __syncthreads();
+    // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
+    for (int isp = tid; isp < nspec; isp += BLOCK) {
+      const int ifr0 = isp / NTH, col = isp - ifr0 * NTH;
+      const float v = stage[isp] / conx[ifr0];
+      ue[(ifr0 + 1 + PAD) * NTH + col] = v;
+      if (ifr0 == nfr - 1) {
+        float t = v;
+        for (int r = nfr + 1; r <= nfrhgh; ++r) {
+          t = t * p.fachfe;
+          ue[(r + PAD) * NTH + col] = t;
+        }
+      }
+    }
+    __syncthreads();
+    const int inext = ipt + gridDim.x;
+    if (tid == 0 && inext < npts) tma_fetch_point(bar, stage, a, cg, inext, nspec, nk);
+    if (inext < npts) kd_next = __ldg(kdmean + inext);
+
+    // 3. Interactions, rows f0 .. f0+BR-1 of the band.
+    {
+      float pw[BR + 2][4];  // IF1/IF2 rows: columns c0 c1 c4 c5
+      float mw[BR + 1][4];  // IF4/IF3 rows: columns c2 c3 c6 c7
+      // Rows enter the windows one step ahead of their use, so at most three of each are live.
+#define WWB_LOAD_PW(j)                          \
+  {                                             \
+    const float* u = ue + rP + (j) * NTH;       \
+    pw[j][0] = u[c0];                           \
+    pw[j][1] = u[c1];                           \
+    pw[j][2] = u[c4];                           \
+    pw[j][3] = u[c5];                           \
+  }
+#define WWB_LOAD_MW(j)                          \
+  {                                             \
+    const float* u = ue + rM + (j) * NTH;       \
+    mw[j][0] = u[c2];                           \
+    mw[j][1] = u[c3];                           \
+    mw[j][2] = u[c6];                           \
+    mw[j][3] = u[c7];                           \
+  }
+      if (n3 > 0) {
+        WWB_LOAD_PW(0);
+        WWB_LOAD_MW(0);
+      }
+#pragma unroll
+      for (int k = 0; k < BR; ++k) {
+        if (k < n3) {
+          WWB_LOAD_PW(k + 1);
+          WWB_LOAD_MW(k + 1);
+#define pa pw[k]       // IF1 row
+#define pb pw[k + 1]   // IF2 row
+#define mb mw[k]       // IF4 row
+#define ma mw[k + 1]   // IF3 row
+          const int o = rO + k * NTH;
+          const float e00 = ue[o];
+          const float ep1 = p.awg[0] * pb[1] + p.awg[1] * pb[0] + p.awg[2] * pa[1] + p.awg[3] * pa[0];
+          const float em1 = p.awg[4] * mb[3] + p.awg[5] * mb[2] + p.awg[6] * ma[3] + p.awg[7] * ma[2];
+          const float ep2 = p.awg[0] * pb[3] + p.awg[1] * pb[2] + p.awg[2] * pa[3] + p.awg[3] * pa[2];
+          const float em2 = p.awg[4] * mb[1] + p.awg[5] * mb[0] + p.awg[6] * ma[1] + p.awg[7] * ma[0];
+          const float ca = cons * afr[f0 - 1 + k];
+          const float factor = ca * e00;
+          const float sa1a = e00 * (ep1 * dal1 + em1 * dal2);
+          const float sa1b = sa1a - ep1 * em1 * dal3;
+          const float sa2a = e00 * (ep2 * dal1 + em2 * dal2);
+          const float sa2b = sa2a - ep2 * em2 * dal3;
+          sa1[o] = factor * sa1b;
+          sa2[o] = factor * sa2b;
+          if (f0 + k <= nfr) dcs[o - (PAD + 1) * NTH] = ca * (sa1a + sa1b) + ca * (sa2a + sa2b);
+          da1p[o] = factor * (dal1 * e00 - dal3 * em1);
+          da1m[o] = factor * (dal2 * e00 - dal3 * ep1);
+          da2p[o] = factor * (dal1 * e00 - dal3 * em2);
+          da2m[o] = factor * (dal2 * e00 - dal3 * ep2);
+#undef pa
+#undef pb
+#undef mb
+#undef ma
+        }
+      }
+#undef WWB_LOAD_PW
+#undef WWB_LOAD_MW
+    }
+    __syncthreads();
+
+    // 4. Source and diagonal terms, rows f0 .. f0+BR-1 of the band (up to NFR).
+    {
+      float* const sp = s + static_cast<size_t>(ipt) * nspec + (f0 - 1) * NTH + ith;
+      float* const dp = d + static_cast<size_t>(ipt) * nspec + (f0 - 1) * NTH + ith;
+      float lw[BR + 1][4], hw[BR + 1][4];  // lo rows IF6.. (SA1 c4 c5, SA2 c0 c1); hi rows IF7..
+#define WWB_LOAD_LH(j, L1, L2, H1, H2)           \
+  {                                              \
+    const int bl = rL + (j) * NTH, bh = rH + (j) * NTH; \
+    lw[j][0] = L1[bl + c4];                      \
+    lw[j][1] = L1[bl + c5];                      \
+    lw[j][2] = L2[bl + c0];                      \
+    lw[j][3] = L2[bl + c1];                      \
+    hw[j][0] = H1[bh + c2];                      \
+    hw[j][1] = H1[bh + c3];                      \
+    hw[j][2] = H2[bh + c6];                      \
+    hw[j][3] = H2[bh + c7];                      \
+  }
+      if (n4 > 0) WWB_LOAD_LH(0, sa1, sa2, sa1, sa2);
+#pragma unroll
+      for (int k = 0; k < BR; ++k) {
+        if (k < n4) {
+          WWB_LOAD_LH(k + 1, sa1, sa2, sa1, sa2);
+#define l6 lw[k]
+#define l5 lw[k + 1]
+#define h7 hw[k]
+#define h8 hw[k + 1]
+          const int o = rO + k * NTH;
+          const float sv = conx[f0 - 1 + k] * (-2.0f * (sa1[o] + sa2[o]) +
+                                               p.awg[0] * (l6[1] + l6[3]) + p.awg[1] * (l6[0] + l6[2]) +
+                                               p.awg[2] * (l5[1] + l5[3]) + p.awg[3] * (l5[0] + l5[2]) +
+                                               p.awg[4] * (h8[1] + h8[3]) + p.awg[5] * (h8[0] + h8[2]) +
+                                               p.awg[6] * (h7[1] + h7[3]) + p.awg[7] * (h7[0] + h7[2]));
+          __stcs(sp + k * NTH, sv);
+#undef l6
+#undef l5
+#undef h7
+#undef h8
+        }
+      }
+      if (n4 > 0) WWB_LOAD_LH(0, da1p, da2p, da1m, da2m);
+#pragma unroll
+      for (int k = 0; k < BR; ++k) {
+        if (k < n4) {
+          WWB_LOAD_LH(k + 1, da1p, da2p, da1m, da2m);
+#define l6 lw[k]
+#define l5 lw[k + 1]
+#define h7 hw[k]
+#define h8 hw[k + 1]
+          const float dv = -2.0f * dcs[rO - (PAD + 1) * NTH + k * NTH] +
+                           p.swg[0] * (l6[1] + l6[3]) + p.swg[1] * (l6[0] + l6[2]) +
+                           p.swg[2] * (l5[1] + l5[3]) + p.swg[3] * (l5[0] + l5[2]) +
+                           p.swg[4] * (h8[1] + h8[3]) + p.swg[5] * (h8[0] + h8[2]) +
+                           p.swg[6] * (h7[1] + h7[3]) + p.swg[7] * (h7[0] + h7[2]);
+          __stcs(dp + k * NTH, dv);
+#undef l6
+#undef l5
+#undef h7
+#undef h8
+        }
+      }
+#undef WWB_LOAD_LH
+    }
+    // The next point's two barriers order its writes after this section 4.
+  }
+}
+
 constexpr int kBandBlock = 288;
+constexpr int kTileMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 113 registers
 constexpr int kBandMinBlocks = 3;  // 3 CTAs of 288 threads per SM: at most 75 registers
 int* g_band_err = nullptr;
 
@@ -657,6 +889,30 @@ int band_stride(const Snl1Dev& p) {
 }
 }  // namespace
 
+namespace {
+template <int NTH, int G, int BR>
+size_t tile_smem(const Snl1Dev& p) {
+  using S = TileShape<NTH, G, BR>;
+  auto r4 = [](size_t n) { return (n + 3) & ~static_cast<size_t>(3); };
+  const size_t floats = r4(static_cast<size_t>(p.nfrhgh + 1 + S::kPad) * NTH) + 6 * S::kAS +
+                        static_cast<size_t>(S::kRows) * NTH + r4(2 * p.nk) + r4(p.nfrchg) +
+                        r4(static_cast<size_t>(p.nspec + p.nk));
+  return floats * sizeof(float) + 16;
+}
+
+/// Which tile instance fits these tables: 36 (8 bands of 5 rows) or 24 (12 bands of 3), or 0.
+int tile_variant(const Snl1Dev& p) {
+  if (p.ifrow == nullptr || p.af11_row == nullptr || p.ifrp < 0 || p.ifrm > 0) return 0;
+  if (p.ifrp > 4 || -p.ifrm > 4) return 0;  // the zero rows below row 0
+  if (p.nspec % 4 != 0 || p.nk % 4 != 0) return 0;  // bulk copies of A and CG
+  if (p.nth == 36 && p.nfrchg <= 40) return 36;
+  if (p.nth == 24 && p.nfrchg <= 36) return 24;
+  return 0;
+}
+}  // namespace
+
+bool snl1_tile_ok(const Snl1Dev& p) { return tile_variant(p) != 0; }
+
 size_t snl1_band_smem(const Snl1Dev& p) {
   size_t floats = static_cast<size_t>(p.nfrhgh + 1) * p.nth + 6 * static_cast<size_t>(band_stride(p)) +
                   p.nspec + 2 * p.nk + p.nfrchg;
@@ -680,6 +936,32 @@ int snl1_take_error() {
 }
 
 namespace {
+template <int NTH, int G, int BR>
+void launch_tile(const Snl1Dev& p, int npts, const float* a, const float* cg, const float* kd,
+                 float* s, float* d, cudaStream_t stream) {
+  static int per_sm = -1;
+  static size_t cached = 0;
+  const size_t smem = tile_smem<NTH, G, BR>(p);
+  auto k = snl1_tile_kernel<NTH, G, BR, kTileMinBlocks>;
+  if (per_sm < 0 || cached != smem) {
+    WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    int n = 0;
+    WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NTH * G, smem));
+    if (n < 1) throw CudaError(cudaErrorInvalidConfiguration, "snl1 tile occupancy");
+    per_sm = n;
+    cached = smem;
+  }
+  if (g_band_err == nullptr) {
+    WWB_CHECK(cudaMalloc(&g_band_err, sizeof(int)));
+    WWB_CHECK(cudaMemset(g_band_err, 0, sizeof(int)));
+  }
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  const int grid = static_cast<int>(npts < resident ? npts : resident);
+  k<<<grid, NTH * G, smem, stream>>>(p, npts, a, cg, kd, s, d, g_band_err);
+  WWB_CHECK(cudaGetLastError());
+}
+
 template <int AS, bool TMA>
 void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, const float* kd,
                  float* s, float* d, cudaStream_t stream) {
@@ -710,11 +992,17 @@ void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, co
 void launch_snl1(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                  const float* kdmean, float* s, float* d, cudaStream_t stream) {
   if (npts <= 0) return;
+  const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
+                       (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
+  if (kernel == kSnl1Tile) {
+    const int v = tile_variant(p);
+    if (v == 36 && aligned) return launch_tile<36, 8, 5>(p, npts, a, cg, kdmean, s, d, stream);
+    if (v == 24 && aligned) return launch_tile<24, 12, 3>(p, npts, a, cg, kdmean, s, d, stream);
+    kernel = kSnl1Band;  // caller arrays not 16-byte aligned: the band kernel reads them directly
+  }
   if (kernel == kSnl1Band) {
     // The bulk copies need 16-byte aligned sources and sizes: NSPEC and NK multiples of 4.
-    const bool tma = p.nspec % 4 == 0 && p.nk % 4 == 0 &&
-                     (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
-                     (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
+    const bool tma = p.nspec % 4 == 0 && p.nk % 4 == 0 && aligned;
     if (band_stride(p) == 1536) {
       if (tma) launch_band<1536, true>(p, npts, a, cg, kdmean, s, d, stream);
       else launch_band<1536, false>(p, npts, a, cg, kdmean, s, d, stream);

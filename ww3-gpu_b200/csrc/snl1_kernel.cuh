@@ -25,7 +25,7 @@ struct Snl1Dev {
   const float* sig;         ///< device, NK
 };
 
-enum Snl1Kernel { kSnl1Auto = 0, kSnl1Gather = 1, kSnl1RowShift = 2, kSnl1Band = 3 };
+enum Snl1Kernel { kSnl1Auto = 0, kSnl1Gather = 1, kSnl1RowShift = 2, kSnl1Band = 3, kSnl1Tile = 4 };
 
 /// Dynamic shared memory of each kernel, bytes.
 size_t snl1_gather_smem(const Snl1Dev& p);
@@ -35,6 +35,10 @@ size_t snl1_band_smem(const Snl1Dev& p);
 /// Whether the band kernel can run these tables (row-shift form, NTH within one CTA, the
 /// rows of a band within its register windows).
 bool snl1_band_ok(const Snl1Dev& p);
+
+/// Whether a compile-time tile instance of the band kernel fits these tables (NTH 36 or 24,
+/// NSPEC and NK multiples of 4 for the bulk copies).
+bool snl1_tile_ok(const Snl1Dev& p);
 
 /// Device status word of the band kernel's bounded waits: nonzero after a wait gave up.
 int snl1_take_error();

@@ -1,0 +1,632 @@
+// ww3-gpu_b200/csrc/xyp3_kernel.cu
+// W3XYP3 + W3QCK3 + W3GATH/W3SCAT for sm_100a, a chunk of spectral components at a time.
+//
+// The reference runs one component per team and the averaging of section 3.a (its "scatter":
+// every sea point adds a share of its action to up to nine cells, w3pro3md.F90:1154-1276) on
+// one thread in source order, because the shares that land on one cell must be added in that
+// order to give the Fortran's bits (prop_xyp3.hpp:1154-1276 comments, and its closing note).
+// Here every phase is data-parallel over (component, element):
+//
+//  * The averaging is turned around into an ordered gather: the thread of target cell T lists
+//    the sea points that can reach it (T itself and its eight neighbours), orders them by their
+//    position in MAPCXY (the loop order: central points, then near-coast points), and replays
+//    each one's statements in source order (centre, then +1,+2,+3,+4,-1,-2,-3,-4 for a central
+//    point; centre, then +1,-1,+2,-2,+3,-3,+4,-4 with the land redirection for a near-coast
+//    one), adding only the shares that land on T, and restarting from AQ where a point under
+//    MAPTRN assigns its centre. Every addition to T therefore happens with the same operands in
+//    the same order as in the serial loop, so VQ(T) has the Fortran's bits.
+//  * The boundary restore, the global closure of the averaging and the x GSQRT that follow
+//    it are applied by the same thread to its own cell (the closure needs the ghost cell's
+//    gathered value, which the thread gathers as well).
+//  * W3QCK3's flux and propagation loops write one element per iteration; its closures copy
+//    whole rows; each is a kernel over (component, element).
+//  * The boundary update takes, for each boundary point, the value of the last IBI naming it
+//    (the serial loop's last write), found on the host once per call.
+// Arithmetic: the reference's per-element expressions and operand order (-fmad=false).
+#include "xyp3_kernel.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <vector>
+
+#include "wwb_common.hpp"
+
+namespace wwb {
+
+/// Constants of one component (W3XYP3 section 1.a, 1.c) and its buffers.
+struct Comp {
+  int isp, ik, ith, ntloc;
+  float ecosi, esini, rntloc, dtloc, dtrad, fthx, fthy, fcgx, fcgy;
+  float* q;  ///< the state (VQ)
+  float* a;  ///< the other buffer (AQ after the averaging)
+  float* vlcflx;
+  float* vlcfly;
+  float* fla;
+  float* rdi;  ///< 4 x NSEA
+  int* iixy;   ///< 4 x NSEA
+};
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr float kPi = static_cast<float>(3.141592653589793);
+constexpr float kGrav = 9.806f;
+constexpr float kTpiInv = 1.0f / (2.0f * kPi);
+constexpr float kCg0Fac = 0.575f * kGrav;       // 0.575*GRAV as REAL
+constexpr float kDera = kPi / 180.0f;           // DERA
+constexpr float kRadius = 4.E7f * kTpiInv;      // RADIUS
+constexpr float kDeraRadius = kDera * kRadius;  // DERA*RADIUS
+
+__host__ __device__ __forceinline__ float max_r(float a, float b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ float min_r(float a, float b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int fint(float x) {
+  return (x > -2147483904.0f && x < 2147483648.0f) ? static_cast<int>(x) : INT_MIN;
+}
+__host__ __device__ __forceinline__ int nint_r(float x) {
+  const float r = roundf(x);
+  return (r > -9.2233715e18f && r < 9.2233715e18f)
+             ? static_cast<int>(static_cast<long long>(r))
+             : 0;
+}
+__device__ __forceinline__ float grid2(const float* x, int ny, int iy, int ix) {
+  return x[(ix - 1) * ny + iy - 1];
+}
+
+int blocks_for(long long n) {
+  const long long b = (n + kBlock - 1) / kBlock;
+  return static_cast<int>(std::max(1LL, std::min(b, 1LL << 30)));
+}
+
+// ---- section 1.a: per-component constants ------------------------------------------------
+__global__ void comp_setup_kernel(Xyp3Grid g, int ncomp, const int* __restrict__ isps,
+                                  Comp* comps) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncomp) return;
+  Comp& k = comps[c];
+  const int isp = isps[c];
+  k.isp = isp;
+  k.ith = 1 + (isp - 1) % g.nth;
+  k.ik = 1 + (isp - 1) / g.nth;
+  const float cg0 = kCg0Fac / g.sig[1];
+  const float cga = kCg0Fac / g.sig[k.ik];
+  k.ecosi = g.ecos[k.ith - 1];
+  k.esini = g.esin[k.ith - 1];
+  const float cgx = k.ecosi * cga;
+  const float cgy = k.esini * cga;
+  float acgx, acgy, cxc, cyc;
+  if (g.flcur != 0) {
+    acgx = max_r(fabsf(cgx + g.cxmin), fabsf(cgx + g.cxmax));
+    acgy = max_r(fabsf(cgy + g.cymin), fabsf(cgy + g.cymax));
+    cxc = max_r(fabsf(g.cxmin), fabsf(g.cxmax));
+    cyc = max_r(fabsf(g.cymin), fabsf(g.cymax));
+  } else {
+    acgx = fabsf(cgx);
+    acgy = fabsf(cgy);
+    cxc = 0.0f;
+    cyc = 0.0f;
+  }
+  const float t1 = max_r(acgx, acgy);
+  const float t2 = max_r(cxc, cyc);
+  const float e = cg0 * 0.001f;
+  const float t3 = max_r(e, t2);
+  const float cgn = max_r(t1, t3);
+  k.ntloc = 1 + fint(g.dtg / ((g.dtcfl * cg0) / cgn));
+  k.rntloc = static_cast<float>(k.ntloc);
+  k.dtloc = g.dtg / k.rntloc;
+  k.dtrad = k.dtloc;
+  if (g.flagll != 0) k.dtrad = k.dtloc / kDeraRadius;
+  float fth = (g.wdth * g.dth) * k.dtloc;
+  float fcg = ((g.wdcg * 0.5f) * (g.xfr - (1.0f / g.xfr))) * k.dtloc;
+  if (g.flagll != 0) {
+    fth = (fth / kRadius) / kDera;
+    fcg = (fcg / kRadius) / kDera;
+  }
+  fcg = fcg / k.rntloc;
+  k.fthx = -(k.esini * fth);
+  k.fthy = k.ecosi * fth;
+  k.fcgx = k.ecosi * fcg;
+  k.fcgy = k.esini * fcg;
+}
+
+// ---- W3GATH, section 1.c stencil, section 2.a velocities, per (component, sea point) -----
+__device__ __forceinline__ void corner(float dxcgc, float dycgc, int ny, int& iixa, int& iixb,
+                                       float& rda, float& rdb) {
+  const int ixc = (dxcgc < 0.0f) ? -ny : ny;
+  const int iyc = (dycgc < 0.0f) ? -1 : 1;
+  iixa = ixc + iyc;
+  if (fabsf(dxcgc) > fabsf(dycgc)) {
+    iixb = ixc;
+    rda = fabsf(dycgc / dxcgc);
+    rdb = fabsf(dxcgc);
+  } else {
+    iixb = iyc;
+    rda = (fabsf(dycgc) > 1.E-5f) ? fabsf(dxcgc / dycgc) : 1.0f;
+    rdb = fabsf(dycgc);
+  }
+}
+
+__global__ void sea_setup_kernel(Xyp3Grid g, int ncomp, Comp* comps, const float* __restrict__ va) {
+  const long long n = static_cast<long long>(ncomp) * g.nsea;
+  const int qoff = g.ny - 1;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / g.nsea);
+    const int isea = 1 + static_cast<int>(t % g.nsea);
+    const Comp& k = comps[c];
+    const int ix = g.mapsf[isea - 1];
+    const int iy = g.mapsf[g.nsea + isea - 1];
+    const int ixy = g.mapsf[2 * g.nsea + isea - 1];
+    const float clat = g.clats[isea];
+    const float dpdx = grid2(g.dpdx, g.ny, iy, ix), dpdy = grid2(g.dpdy, g.ny, iy, ix);
+    const float dqdx = grid2(g.dqdx, g.ny, iy, ix), dqdy = grid2(g.dqdy, g.ny, iy, ix);
+    // Section 1.c, the averaging stencil (:983-1059).
+    float tmpx = k.fthx / clat;
+    float tmpy = k.fthy;
+    const float dxcgn = dpdx * tmpx + dpdy * tmpy;
+    const float dycgn = dqdx * tmpx + dqdy * tmpy;
+    tmpx = k.fcgx / clat;
+    tmpy = k.fcgy;
+    const float dxcgs = dpdx * tmpx + dpdy * tmpy;
+    const float dycgs = dqdx * tmpx + dqdy * tmpy;
+    int i1, i2, i3, i4;
+    float r1, r2, r3, r4;
+    corner(dxcgn + dxcgs, dycgn + dycgs, g.ny, i1, i2, r1, r2);
+    corner(dxcgn - dxcgs, dycgn - dycgs, g.ny, i3, i4, r3, r4);
+    float* rd = k.rdi + (isea - 1);
+    int* ii = k.iixy + (isea - 1);
+    rd[0] = r1;
+    rd[g.nsea] = r2;
+    rd[2 * g.nsea] = r3;
+    rd[3 * g.nsea] = r4;
+    ii[0] = i1;
+    ii[g.nsea] = i2;
+    ii[2 * g.nsea] = i3;
+    ii[3 * g.nsea] = i4;
+    // W3GATH then section 2.a (:1080-1137): this sea point's cell only.
+    const float cgi = g.cg[isea * (g.nk + 2) + k.ik];
+    const float v = va[static_cast<size_t>(isea) * g.nspec + (k.isp - 1)];
+    k.q[ixy + qoff] = (v / cgi) * clat;
+    float cxt = (k.ecosi * cgi) / clat;
+    float cyt = k.esini * cgi;
+    if (g.flcur != 0) {
+      cxt = cxt + (g.cx[isea] / g.clats[isea]);
+      cyt = cyt + g.cy[isea];
+    }
+    const float cp = cxt * dpdx + cyt * dpdy;
+    const float cq = cxt * dqdx + cyt * dqdy;
+    k.vlcflx[ixy - 1] = k.dtrad * cp;
+    k.vlcfly[ixy - 1] = k.dtrad * cq;
+  }
+}
+
+// ---- section 3.a: the averaging as an ordered gather ---------------------------------------
+/// MAPSTX(j), j in 1-2NY .. NY*(NX+2).
+__device__ __forceinline__ int stx(const Xyp3Grid& g, int j) { return g.mapstx[j + 2 * g.ny - 1]; }
+
+/// VQ(T) after the averaging loops of one component, from AQ = a (section 3.a.1, 3.a.2).
+__device__ float gather_cell(const Xyp3Grid& g, const Comp& k, const float* __restrict__ a,
+                             int T) {
+  const int ny = g.ny, nxy = g.nx * g.ny, nsea = g.nsea, qoff = ny - 1;
+  // The nine candidate sources T - d, ordered by their MAPCXY position (INT_MAX: none).
+  int pos[9], src[9];
+  const int d[9] = {0, 1, -1, ny, -ny, ny + 1, ny - 1, -ny + 1, -ny - 1};
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    const int S = T - d[j];
+    int p = INT_MAX;
+    if (S >= 1 && S <= nxy) {
+      const int isea = g.cell_sea[S - 1];
+      if (isea > 0) {
+        p = g.sea_pos[isea - 1];
+        // A near-coast point with MAPSTA <= 0 is skipped by the loop (:1191).
+        if (p > g.ncent && g.mapsta[S - 1] <= 0) p = INT_MAX;
+      }
+    }
+    pos[j] = p;
+    src[j] = S;
+  }
+  // Sorting network (9 inputs), constant indices only.
+#define WWB_CX(i, j)                                   \
+  if (pos[j] < pos[i]) {                               \
+    const int tp = pos[i];                             \
+    pos[i] = pos[j];                                   \
+    pos[j] = tp;                                       \
+    const int ts = src[i];                             \
+    src[i] = src[j];                                   \
+    src[j] = ts;                                       \
+  }
+  WWB_CX(0, 1) WWB_CX(3, 4) WWB_CX(6, 7) WWB_CX(1, 2) WWB_CX(4, 5) WWB_CX(7, 8)
+  WWB_CX(0, 1) WWB_CX(3, 4) WWB_CX(6, 7) WWB_CX(0, 3) WWB_CX(3, 6) WWB_CX(0, 3)
+  WWB_CX(1, 4) WWB_CX(4, 7) WWB_CX(1, 4) WWB_CX(2, 5) WWB_CX(5, 8) WWB_CX(2, 5)
+  WWB_CX(1, 3) WWB_CX(5, 7) WWB_CX(2, 6) WWB_CX(4, 6) WWB_CX(2, 4) WWB_CX(2, 3)
+  WWB_CX(5, 6)
+#undef WWB_CX
+  float acc = 0.0f;
+#pragma unroll 1
+  for (int j = 0; j < 9; ++j) {
+    if (pos[j] == INT_MAX) break;
+    const int S = src[j];
+    const int isea = g.cell_sea[S - 1];
+    if (g.maptrn[S - 1] != 0) {  // :1157-1158 and :1192-1193, an assignment of the centre
+      if (S == T) acc = a[S + qoff];
+      continue;
+    }
+    const float cgi = g.cg[isea * (g.nk + 2) + k.ik];
+    const float* rd = k.rdi + (isea - 1);
+    const int* ii = k.iixy + (isea - 1);
+    const float rd1 = rd[0];
+    const float rd2 = min_r(rd[nsea] * cgi, 1.0f);
+    const float rd3 = rd[2 * nsea];
+    const float rd4 = min_r(cgi * rd[3 * nsea], 1.0f);
+    const float av = a[S + qoff];
+    const int i1 = ii[0], i2 = ii[nsea], i3 = ii[2 * nsea], i4 = ii[3 * nsea];
+    if (S == T) acc = acc + (((3.0f - rd2) - rd4) * av) / 3.0f;
+    const float c1 = ((rd2 * av) * rd1) / 6.0f;
+    const float c2 = (((1.0f - rd1) * av) * rd2) / 6.0f;
+    const float c3 = ((rd4 * av) * rd3) / 6.0f;
+    const float c4 = (((1.0f - rd3) * av) * rd4) / 6.0f;
+    if (pos[j] <= g.ncent) {  // central point: +1 +2 +3 +4 -1 -2 -3 -4 (:1166-1180)
+      if (S + i1 == T) acc = acc + c1;
+      if (S + i2 == T) acc = acc + c2;
+      if (S + i3 == T) acc = acc + c3;
+      if (S + i4 == T) acc = acc + c4;
+      if (S - i1 == T) acc = acc + c1;
+      if (S - i2 == T) acc = acc + c2;
+      if (S - i3 == T) acc = acc + c3;
+      if (S - i4 == T) acc = acc + c4;
+    } else {  // near coast: +1 -1 +2 -2 +3 -3 +4 -4, land targets back to the centre
+      int ixc = (ny ^ i1) < 0 ? -ny : ny;
+      int iyc = i1 - ixc;
+      int t;
+      t = (stx(g, S + i1) >= 1 && !(stx(g, S + ixc) <= 0 && stx(g, S + iyc) <= 0)) ? S + i1 : S;
+      if (t == T) acc = acc + c1;
+      t = (stx(g, S - i1) >= 1 && !(stx(g, S - ixc) <= 0 && stx(g, S - iyc) <= 0)) ? S - i1 : S;
+      if (t == T) acc = acc + c1;
+      t = (stx(g, S + i2) >= 1) ? S + i2 : S;
+      if (t == T) acc = acc + c2;
+      t = (stx(g, S - i2) >= 1) ? S - i2 : S;
+      if (t == T) acc = acc + c2;
+      ixc = (ny ^ i3) < 0 ? -ny : ny;
+      iyc = i3 - ixc;
+      t = (stx(g, S + i3) >= 1 && !(stx(g, S + ixc) <= 0 && stx(g, S + iyc) <= 0)) ? S + i3 : S;
+      if (t == T) acc = acc + c3;
+      t = (stx(g, S - i3) >= 1 && !(stx(g, S - ixc) <= 0 && stx(g, S - iyc) <= 0)) ? S - i3 : S;
+      if (t == T) acc = acc + c3;
+      t = (stx(g, S + i4) >= 1) ? S + i4 : S;
+      if (t == T) acc = acc + c4;
+      t = (stx(g, S - i4) >= 1) ? S - i4 : S;
+      if (t == T) acc = acc + c4;
+    }
+  }
+  return acc;
+}
+
+/// Sections 3.a-3.b up to the sweeps, per (component, cell T of VQ): the averaged value, the
+/// boundary restore (:1280-1282), the global closure (:1286-1291) and x GSQRT (:1301-1306).
+/// Reads the component's state k.q as AQ and writes the new state into k.a (swapped after).
+__global__ void average_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc) {
+  const int ny = g.ny, nx = g.nx, nxy = nx * ny;
+  const int nq = ny * (nx + 3), qoff = ny - 1;
+  const long long n = static_cast<long long>(ncomp) * nq;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / nq);
+    const Comp& k = comps[c];
+    if (itloc > k.ntloc) continue;
+    const int T = static_cast<int>(t % nq) + 1 - ny;  // 1-NY .. NY*(NX+2)
+    const float* a = k.q;
+    float v = gather_cell(g, k, a, T);
+    if (T >= 1 && T <= nxy) {
+      if (g.mapsta[T - 1] == 2) v = a[T + qoff];
+      if (g.global) {
+        const int col = (T - 1) / ny + 1;
+        if (col == 1) v = v + gather_cell(g, k, a, T + nxy);
+        if (col == nx) v = v + gather_cell(g, k, a, T - nxy);
+      }
+      const int isea = g.cell_sea[T - 1];
+      if (isea > 0) {
+        const int ix = g.mapsf[isea - 1], iy = g.mapsf[g.nsea + isea - 1];
+        v = v * grid2(g.gsqrt, ny, iy, ix);
+      }
+    }
+    k.a[T + qoff] = v;
+  }
+}
+
+__global__ void swap_kernel(int ncomp, Comp* comps, int itloc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncomp || itloc > comps[c].ntloc) return;
+  float* t = comps[c].q;
+  comps[c].q = comps[c].a;
+  comps[c].a = t;
+}
+
+// ---- W3QCK3 (prop_qck3.hpp:60-224), per (component, element) ------------------------------
+struct Sweep {
+  int inc, close;
+  const int* mapbou;
+  int nb0, nb1, nb2;
+  const float* trans;
+  bool x;  ///< the x sweep (VLCFLX) or the y sweep (VLCFLY)
+};
+
+__global__ void qck3_zero_closure_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc,
+                                         Sweep w) {
+  const int ny = g.ny, nx = g.nx, my = ny;
+  const int nfla = my * (nx + 1), qoff = my - 1;
+  const long long n = static_cast<long long>(ncomp) * nfla;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / nfla);
+    const Comp& k = comps[c];
+    if (itloc > k.ntloc) continue;
+    const int i = static_cast<int>(t % nfla);
+    k.fla[i] = 0.0f;  // :1085
+    if (w.close && i < ny) {  // :1087-1112, closure part 1, a row per thread
+      const int iy = i + 1;
+      float* q = k.q;
+      float* cfll = w.x ? k.vlcflx : k.vlcfly;
+      const int iad00 = -my, iad02 = my, iadn0 = iad00 + my * nx, iadn1 = my * nx,
+                iadn2 = iad02 + my * nx;
+      q[iy + iad00 + qoff] = q[iy + iadn0 + qoff];
+      q[iy + iadn1 + qoff] = q[iy + qoff];
+      q[iy + iadn2 + qoff] = q[iy + iad02 + qoff];
+      cfll[iy + iadn1 - 1] = cfll[iy - 1];
+    }
+  }
+}
+
+__global__ void qck3_flux_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc, Sweep w) {
+  const int qoff = g.ny - 1, foff = g.ny - 1, inc = w.inc;
+  const long long n = static_cast<long long>(ncomp) * w.nb2;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / w.nb2);
+    const Comp& k = comps[c];
+    if (itloc > k.ntloc) continue;
+    const int ip = 1 + static_cast<int>(t % w.nb2);
+    const int ixy = w.mapbou[ip - 1];
+    const float* q = k.q;
+    const float* cfll = w.x ? k.vlcflx : k.vlcfly;
+    if (ip <= w.nb0) {  // :1130-1172
+      const float cfl = (cfll[ixy + inc - 1] + cfll[ixy - 1]) * 0.5f;
+      const float s = copysignf(1.1f, cfl);
+      const int ixyc = ixy - inc * fint(min_r(s, 0.0f));
+      const float c2 = cfl * cfl;
+      const float t1 = (1.0f - cfl) * q[ixy + inc + qoff];
+      const float t2 = (cfl + 1.0f) * q[ixy + qoff];
+      const float h1 = (t1 + t2) * 0.5f;
+      const float h2 = (1.0f - c2) / 6.0f;
+      const float qixyc = q[ixyc + qoff];
+      const float d2 = (q[ixyc - inc + qoff] - qixyc * 2.0f) + q[ixyc + inc + qoff];
+      const float qb = h1 - h2 * d2;
+      const int ixyu = ixyc - inc * fint(s);
+      const int ixyd = 2 * ixyc - ixyu;
+      const float qixyu = q[ixyu + qoff];
+      const float dq = q[ixyd + qoff] - qixyu;
+      const float dqnz = copysignf(max_r(fabsf(dq), 1.E-15f), dq);
+      const float qcn = min_r(max_r((qixyc - qixyu) / dqnz, -0.1f), 1.1f);
+      const float qbn0 = max_r((qb - qixyu) / dqnz, qcn);
+      const float u = min_r(qcn / max_r(fabsf(cfl), 1.E-10f), 1.0f);
+      const float qbn = min_r(qbn0, u);
+      const float qbr = qixyu + qbn * dq;
+      const float cfac = static_cast<float>(fint(fabsf(qcn - 0.5f) * 2.0f));
+      const float qb2 = qixyc * cfac + (1.0f - cfac) * qbr;
+      k.fla[ixy + foff] = cfl * qb2;
+    } else {  // :1187-1234, boundary above (CFL at IXY) or below (CFL at IXY+INC)
+      const float cfl = ip <= w.nb1 ? cfll[ixy - 1] : cfll[ixy + inc - 1];
+      const float s = copysignf(1.1f, cfl);
+      const int ixyc = ixy - inc * fint(min_r(s, 0.0f));
+      k.fla[ixy + foff] = q[ixyc + qoff] * cfl;
+    }
+  }
+}
+
+__global__ void qck3_prop_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc, Sweep w) {
+  const int ny = g.ny, nxy = g.nx * g.ny, qoff = ny - 1, foff = ny - 1, inc = w.inc;
+  const long long n = static_cast<long long>(ncomp) * g.nact;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / g.nact);
+    const Comp& k = comps[c];
+    if (itloc > k.ntloc) continue;
+    const int ip = 1 + static_cast<int>(t % g.nact);
+    const int ixy = g.mapaxy[ip - 1];
+    // :1240-1247, closure part 2 (FLA column 0 <- column NX), read where it is used.
+    int jm = ixy - inc;
+    if (w.close && jm <= 0) jm += nxy;
+    const float fm = k.fla[jm + foff];
+    const float fp = k.fla[ixy + foff];
+    const int jn = (fm > 0.0f) ? -1 : 0;
+    const int jp = (fp < 0.0f) ? 1 : 0;
+    const float tt = k.q[ixy + qoff] + fm * w.trans[static_cast<long>(jn + 1) * nxy + ixy - 1];
+    const float u = tt - fp * w.trans[static_cast<long>(jp + 1) * nxy + ixy - 1];
+    k.q[ixy + qoff] = max_r(u, 0.0f);
+  }
+}
+
+// ---- x 1/GSQRT (:1368-1373) and the boundary update (:1395-1415), per sea point -----------
+__global__ void finish_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc) {
+  const long long n = static_cast<long long>(ncomp) * g.nsea;
+  const int qoff = g.ny - 1;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / g.nsea);
+    const Comp& k = comps[c];
+    if (itloc > k.ntloc) continue;
+    const int isea = 1 + static_cast<int>(t % g.nsea);
+    const int ix = g.mapsf[isea - 1], iy = g.mapsf[g.nsea + isea - 1];
+    const int ixy = g.mapsf[2 * g.nsea + isea - 1];
+    const int ibi = g.flbpi ? g.bnd_last[isea - 1] : 0;
+    if (ibi > 0) {
+      float rd1 = g.dsec_bpi0 - ((g.dtg * static_cast<float>(k.ntloc - itloc)) / k.rntloc);
+      float rd2 = g.dsec_bpin;
+      if (rd2 > 0.001f) {
+        const float qq = rd1 / rd2;
+        rd2 = min_r(max_r(qq, 0.0f), 1.0f);
+        rd1 = 1.0f - rd2;
+      } else {
+        rd1 = 0.0f;
+        rd2 = 1.0f;
+      }
+      const float b0 = g.bbpi0[static_cast<size_t>(ibi) * g.nspec + k.isp - 1];
+      const float bn = g.bbpin[static_cast<size_t>(ibi) * g.nspec + k.isp - 1];
+      k.q[ixy + qoff] = (((b0 * rd1) + (bn * rd2)) / g.cg[isea * (g.nk + 2) + k.ik]) *
+                        g.clats[isea];
+    } else {
+      k.q[ixy + qoff] = k.q[ixy + qoff] / grid2(g.gsqrt, g.ny, iy, ix);
+    }
+  }
+}
+
+// ---- section 4 and W3SCAT, per (component, sea point) --------------------------------------
+__global__ void store_kernel(Xyp3Grid g, int ncomp, const Comp* comps, float* __restrict__ va) {
+  const long long n = static_cast<long long>(ncomp) * g.nsea;
+  const int qoff = g.ny - 1;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(t / g.nsea);
+    const Comp& k = comps[c];
+    const int isea = 1 + static_cast<int>(t % g.nsea);
+    const int ixy = g.mapsf[2 * g.nsea + isea - 1];
+    const int st = g.mapsta[ixy - 1];
+    float v = k.q[ixy + qoff];
+    if (st > 0) {
+      const float x = (g.cg[isea * (g.nk + 2) + k.ik] / g.clats[isea]) * v;
+      v = max_r(x, 0.0f);
+    }
+    if (st != 0) va[static_cast<size_t>(isea) * g.nspec + (k.isp - 1)] = v;
+  }
+}
+
+// ---- MINVAL/MAXVAL of the currents -----------------------------------------------------------
+__global__ void current_range_kernel(const float* __restrict__ cx, const float* __restrict__ cy,
+                                     int nsea, float* out) {
+  // out: cxmin, cxmax, cymin, cymax, counts of non-NaN x and y (as floats)
+  __shared__ float sh[6][kBlock];
+  float mn_x = INFINITY, mx_x = -INFINITY, mn_y = INFINITY, mx_y = -INFINITY, nx = 0, ny = 0;
+  for (int i = threadIdx.x; i < nsea; i += blockDim.x) {
+    const float a = cx[i + 1], b = cy[i + 1];
+    if (a == a) {
+      mn_x = a < mn_x ? a : mn_x;
+      mx_x = a > mx_x ? a : mx_x;
+      nx += 1.0f;
+    }
+    if (b == b) {
+      mn_y = b < mn_y ? b : mn_y;
+      mx_y = b > mx_y ? b : mx_y;
+      ny += 1.0f;
+    }
+  }
+  sh[0][threadIdx.x] = mn_x;
+  sh[1][threadIdx.x] = mx_x;
+  sh[2][threadIdx.x] = mn_y;
+  sh[3][threadIdx.x] = mx_y;
+  sh[4][threadIdx.x] = nx;
+  sh[5][threadIdx.x] = ny;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < blockDim.x; ++i) {
+      sh[0][0] = sh[0][i] < sh[0][0] ? sh[0][i] : sh[0][0];
+      sh[1][0] = sh[1][i] > sh[1][0] ? sh[1][i] : sh[1][0];
+      sh[2][0] = sh[2][i] < sh[2][0] ? sh[2][i] : sh[2][0];
+      sh[3][0] = sh[3][i] > sh[3][0] ? sh[3][i] : sh[3][0];
+      sh[4][0] += sh[4][i];
+      sh[5][0] += sh[5][i];
+    }
+    for (int j = 0; j < 6; ++j) out[j] = sh[j][0];
+  }
+}
+
+}  // namespace
+
+size_t xyp3_bytes_per_component(const Xyp3Grid& g) {
+  const size_t nq = static_cast<size_t>(g.ny) * (g.nx + 3);
+  const size_t n1 = static_cast<size_t>(g.ny) * (g.nx + 1);
+  return sizeof(float) * (2 * nq + 3 * n1 + 4 * static_cast<size_t>(g.nsea)) +
+         sizeof(int) * 4 * static_cast<size_t>(g.nsea) + sizeof(Comp);
+}
+
+void xyp3_current_range(Xyp3Grid& g, cudaStream_t s) {
+  float* d = nullptr;
+  WWB_CHECK(cudaMalloc(&d, 6 * sizeof(float)));
+  current_range_kernel<<<1, kBlock, 0, s>>>(g.cx, g.cy, g.nsea, d);
+  float h[6];
+  const cudaError_t e1 = cudaGetLastError();
+  const cudaError_t e2 = cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, s);
+  const cudaError_t e3 = cudaStreamSynchronize(s);
+  cudaFree(d);
+  WWB_CHECK(e1);
+  WWB_CHECK(e2);
+  WWB_CHECK(e3);
+  const float nan = std::nanf("");
+  const float huge = 3.40282347e38f;
+  g.cxmin = g.nsea <= 0 ? huge : (h[4] > 0 ? h[0] : nan);
+  g.cxmax = g.nsea <= 0 ? -huge : (h[4] > 0 ? h[1] : nan);
+  g.cymin = g.nsea <= 0 ? huge : (h[5] > 0 ? h[2] : nan);
+  g.cymax = g.nsea <= 0 ? -huge : (h[5] > 0 ? h[3] : nan);
+}
+
+void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s) {
+  const int nc = ch.ncomp;
+  if (nc <= 0) return;
+  const size_t nq = static_cast<size_t>(g.ny) * (g.nx + 3);
+  const size_t n1 = static_cast<size_t>(g.ny) * (g.nx + 1);
+  // Per-component buffers and constants.
+  std::vector<Comp> hc(nc);
+  for (int c = 0; c < nc; ++c) {
+    hc[c] = Comp{};
+    hc[c].q = ch.vq + c * nq;
+    hc[c].a = ch.aq + c * nq;
+    hc[c].vlcflx = ch.vlcflx + c * n1;
+    hc[c].vlcfly = ch.vlcfly + c * n1;
+    hc[c].fla = ch.fla + c * n1;
+    hc[c].rdi = ch.rdi + static_cast<size_t>(c) * 4 * g.nsea;
+    hc[c].iixy = ch.iixy + static_cast<size_t>(c) * 4 * g.nsea;
+  }
+  WWB_CHECK(cudaMemcpyAsync(ch.comp, hc.data(), sizeof(Comp) * nc, cudaMemcpyHostToDevice, s));
+  comp_setup_kernel<<<(nc + 127) / 128, 128, 0, s>>>(g, nc, ch.isp, ch.comp);
+  WWB_CHECK(cudaGetLastError());
+  std::vector<Comp> back(nc);
+  WWB_CHECK(cudaMemcpyAsync(back.data(), ch.comp, sizeof(Comp) * nc, cudaMemcpyDeviceToHost, s));
+  // FIELD = 0 (W3GATH), the four speed arrays = 0 (:944-947).
+  WWB_CHECK(cudaMemsetAsync(ch.vq, 0, sizeof(float) * nq * nc, s));
+  WWB_CHECK(cudaMemsetAsync(ch.vlcflx, 0, sizeof(float) * n1 * nc, s));
+  WWB_CHECK(cudaMemsetAsync(ch.vlcfly, 0, sizeof(float) * n1 * nc, s));
+  const long long nsea_c = static_cast<long long>(nc) * g.nsea;
+  sea_setup_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, va);
+  WWB_CHECK(cudaGetLastError());
+  WWB_CHECK(cudaStreamSynchronize(s));
+  int ntmax = 0;
+  for (const Comp& k : back) ntmax = std::max(ntmax, k.ntloc);
+  // YFIRST (:928-931): the same for every component; it alternates every sub-step.
+  const int dttst = fint(g.dsec_day);
+  bool yfirst = (nint_r(static_cast<float>(dttst) / g.dtg) % 2) == 0;
+  const Sweep sx{g.ny, g.global, g.mapx2, g.nmx0, g.nmx1, g.nmx2, g.atrnx, true};
+  const Sweep sy{1, 0, g.mapy2, g.nmy0, g.nmy1, g.nmy2, g.atrny, false};
+  const long long nfla = static_cast<long long>(nc) * n1;
+  for (int itloc = 1; itloc <= ntmax; ++itloc) {
+    average_kernel<<<blocks_for(static_cast<long long>(nc) * nq), kBlock, 0, s>>>(g, nc, ch.comp,
+                                                                                 itloc);
+    swap_kernel<<<(nc + 127) / 128, 128, 0, s>>>(nc, ch.comp, itloc);
+    const Sweep order[2] = {yfirst ? sy : sx, yfirst ? sx : sy};
+    for (const Sweep& w : order) {
+      if ((w.x && g.flcx == 0) || (!w.x && g.flcy == 0)) continue;
+      qck3_zero_closure_kernel<<<blocks_for(nfla), kBlock, 0, s>>>(g, nc, ch.comp, itloc, w);
+      if (w.nb2 > 0)
+        qck3_flux_kernel<<<blocks_for(static_cast<long long>(nc) * w.nb2), kBlock, 0, s>>>(
+            g, nc, ch.comp, itloc, w);
+      if (g.nact > 0)
+        qck3_prop_kernel<<<blocks_for(static_cast<long long>(nc) * g.nact), kBlock, 0, s>>>(
+            g, nc, ch.comp, itloc, w);
+    }
+    finish_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, itloc);
+    WWB_CHECK(cudaGetLastError());
+    yfirst = !yfirst;
+  }
+  store_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, va);
+  WWB_CHECK(cudaGetLastError());
+}
+
+}  // namespace wwb

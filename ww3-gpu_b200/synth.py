@@ -237,3 +237,108 @@ def ktp3_case(npts, seed=0, nk=36, nth=36, nsea=None, depth_range=(5.0, 4000.0),
         "va": va, "nsealm": nsealm,
         "cflthmax": np.full(nsealm, -1.0, np.float32), "cflkmax": np.full(nsealm, -1.0, np.float32),
     }
+
+
+def land_mask(nx, ny, seed=0, sea_fraction=0.7, smooth=6):
+    """Seeded smooth random land/sea mask (True = sea), periodic in longitude; the first and
+    last latitude rows are land, as W3GRID requires of a grid with PR3 propagation."""
+    rng = np.random.default_rng(seed)
+    f = rng.standard_normal((ny, nx))
+    k = np.exp(-0.5 * (np.arange(-3 * smooth, 3 * smooth + 1) / smooth) ** 2)
+    f = np.apply_along_axis(lambda r: np.convolve(np.concatenate([r[-3 * smooth:], r,
+                                                                  r[:3 * smooth]]), k, "valid"),
+                            1, f)
+    f = np.apply_along_axis(lambda c: np.convolve(c, k, "same"), 0, f)
+    sea = f > np.quantile(f, 1.0 - sea_fraction)
+    sea[0, :] = False
+    sea[-1, :] = False
+    return sea
+
+
+def xyp3_case(nx=48, ny=32, seed=0, nk=36, nth=36, iclose=2, flcur=True, flbpi=True,
+              on_fraction=1.0, dtg=900.0, ref=None):
+    """Seeded inputs of ww_xyp3_batch on an NX x NY regular lon/lat grid (0.25 degrees), the
+    W3MAP3 maps built by ``ref`` (a callable ref(nx, ny, nsea, nk, nth, mapsta, mapsf) returning
+    (mapx2, mapy2, mapaxy, mapcxy, counts), the reference's own W3MAP3 in the tests)."""
+    rng = np.random.default_rng(seed)
+    nspec = nk * nth
+    sea = land_mask(nx, ny, seed=seed)
+    mapsta2 = np.where(sea, 1, 0).astype(np.int32)  # (NY, NX)
+    # a few active boundary points and excluded sea points
+    cand = np.argwhere(sea)
+    pick = rng.permutation(len(cand))
+    for j in pick[: max(1, len(cand) // 50)]:
+        mapsta2[tuple(cand[j])] = 2
+    for j in pick[max(1, len(cand) // 50): max(2, len(cand) // 50 + len(cand) // 100)]:
+        mapsta2[tuple(cand[j])] = -1
+    # sea points row by row (IY outer), IXY = (IX-1)*NY + IY
+    ix_l, iy_l = [], []
+    for iy in range(1, ny + 1):
+        for ix in range(1, nx + 1):
+            if mapsta2[iy - 1, ix - 1] != 0:
+                ix_l.append(ix)
+                iy_l.append(iy)
+    nsea = len(ix_l)
+    ix_a = np.array(ix_l, np.int32)
+    iy_a = np.array(iy_l, np.int32)
+    mapsf = np.concatenate([ix_a, iy_a, (ix_a - 1) * ny + iy_a]).astype(np.int32)
+    mapsta = np.ascontiguousarray(mapsta2.T).reshape(-1).astype(np.int32)  # column-major (NY,NX)
+    mapx2, mapy2, mapaxy, mapcxy, counts = ref(nx, ny, nsea, nk, nth, mapsta, mapsf)
+    nxy = nx * ny
+    sp = spectral_arrays(nk, nth)
+    sx = sy = 0.25
+    lat = -80.0 + (np.arange(1, ny + 1) - 0.5) * (160.0 / ny)
+    clat_cell = np.cos(np.deg2rad(lat))
+    clats = np.ones(nsea + 1, np.float32)
+    clats[1:] = clat_cell[iy_a - 1]
+    ones = np.ones(nxy, np.float32)
+    dpdx = (ones / sx).astype(np.float32)
+    dqdy = (ones / sy).astype(np.float32)
+    dpdy = np.zeros(nxy, np.float32)
+    dqdx = np.zeros(nxy, np.float32)
+    gsqrt = np.repeat(clat_cell[None, :], nx, axis=0).reshape(-1).astype(np.float32) * sx * sy
+    atrnx = np.ones((3, nxy), np.float32)
+    atrny = np.ones((3, nxy), np.float32)
+    tr = rng.uniform(0.0, 1.0, (3, nxy)) < 0.05
+    atrnx[tr] = rng.uniform(0.2, 1.0, tr.sum())
+    atrny[tr] = rng.uniform(0.2, 1.0, tr.sum())
+    maptrn = (rng.uniform(0.0, 1.0, nxy) < 0.03).astype(np.int32)
+    dep = np.exp(rng.uniform(np.log(10.0), np.log(4000.0), nsea + 1))
+    k = wavenumber(sp["sig"], dep)
+    kd = np.minimum(k * dep[:, None], 40.0)
+    cg = 0.5 * sp["sig"].astype(np.float64)[None, :] / k * (
+        1.0 + 2.0 * kd / np.sinh(np.minimum(2.0 * kd, 80.0)))
+    cx = np.zeros(nsea + 1, np.float32)
+    cy = np.zeros(nsea + 1, np.float32)
+    if flcur:
+        cx[1:] = rng.normal(0.0, 0.4, nsea)
+        cy[1:] = rng.normal(0.0, 0.4, nsea)
+    bnd = np.nonzero(mapsta2.T.reshape(-1)[(ix_a - 1) * ny + iy_a - 1] == 2)[0] + 1  # ISEA
+    if flbpi and len(bnd) > 0:
+        isbpi = np.concatenate([bnd, bnd[:1]]).astype(np.int32)  # one point listed twice
+    else:
+        isbpi = np.zeros(1, np.int32)
+    nbi = len(isbpi) if flbpi else 0
+    g = sea_states(nsea + 1, seed=seed + 5, nk=nk, nth=nth, depth_range=(10.0, 4000.0))
+    va = np.zeros((nsea + 1, nspec), np.float32)
+    va[1:] = g["a"][1:]
+    bb0 = np.zeros((max(nbi, 0) + 1, nspec), np.float32)
+    bbn = np.zeros((max(nbi, 0) + 1, nspec), np.float32)
+    if nbi:
+        gb = sea_states(2 * nbi, seed=seed + 9, nk=nk, nth=nth)
+        bb0[1:] = gb["a"][:nbi]
+        bbn[1:] = gb["a"][nbi:]
+    on = (rng.uniform(0.0, 1.0, nspec) < on_fraction).astype(np.int32)
+    return {
+        "rpar": np.array([300.0, sp["dth"], 1.1, 1.5, 1.5], np.float32),
+        "ipar": np.array([nx, ny, nsea, nk, nth, nspec, iclose, 1, 1, 1, int(flcur)], np.int32),
+        "imaps": np.asarray(counts, np.int32),
+        "tscal": np.array([3600.0, 450.0, 900.0], np.float32), "dtg": float(np.float32(dtg)),
+        "mapsf": mapsf, "clats": clats, "sig": sp["sig"], "ecos": sp["ecos"], "esin": sp["esin"],
+        "dpdx": dpdx, "dpdy": dpdy, "dqdx": dqdx, "dqdy": dqdy, "gsqrt": gsqrt,
+        "atrnx": atrnx.reshape(-1), "atrny": atrny.reshape(-1), "mapx2": mapx2, "mapy2": mapy2,
+        "mapaxy": mapaxy, "mapcxy": mapcxy, "maptrn": maptrn, "mapsta": mapsta,
+        "cg": cg.astype(np.float32).reshape(-1), "cx": cx, "cy": cy, "flbpi": int(flbpi),
+        "nbi": nbi, "isbpi": isbpi, "bbpi0": bb0.reshape(-1), "bbpin": bbn.reshape(-1),
+        "on": on, "va": va, "nsea": nsea, "nx": nx, "ny": ny,
+    }
