@@ -204,10 +204,10 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_point():
-    """DRAM bytes per sea point of the W3SNL1 kernel from the committed ncu capture summary
-    (profiles/snl1_band_36x36.json), or None."""
-    p = ROOT / "profiles" / "snl1_band_36x36.json"
+def ncu_traffic_per_point(kernel_name):
+    """DRAM bytes per sea point of the W3SNL1 kernel `kernel_name` from the committed ncu
+    capture summary (profiles/<kernel_name>_36x36.json), or None."""
+    p = ROOT / "profiles" / f"{kernel_name}_36x36.json"
     if not p.exists():
         return None
     try:
@@ -302,7 +302,7 @@ def run_b200(args):
 
     peak, peak_kind = measured_peak_hbm()
     achieved = BYTES_PER_POINT * npts / (launch_ms / 1e3) / 1e9
-    tpp = ncu_traffic_per_point()
+    tpp = ncu_traffic_per_point(kernel_name)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -152,7 +152,7 @@ template <class DataType, class... Props>
 class View {
  public:
   static constexpr int Rank = Impl::view_rank<DataType>::value;
-  static constexpr int rank = Rank;
+  static constexpr std::integral_constant<int, Rank> rank{};  // callable, as in Kokkos 4
   using value_type = typename Impl::view_rank<DataType>::value_type;
   using non_const_value_type = std::remove_const_t<value_type>;
   using const_value_type = std::add_const_t<value_type>;
@@ -496,6 +496,12 @@ class TeamPolicy {
   TeamPolicy(int league, int, int = 1) : league_(league) {}
   TeamPolicy(const execution_space&, int league, AUTO_t, int = 1) : league_(league) {}
   TeamPolicy(const execution_space&, int league, int, int = 1) : league_(league) {}
+  /// The same league, chunk and scratch under another schedule or execution-space spelling.
+  template <class... Q>
+  TeamPolicy(const TeamPolicy<Q...>& o) : league_(o.league_size()), chunk_(o.chunk_size()) {
+    scratch_[0] = o.scratch(0);
+    scratch_[1] = o.scratch(1);
+  }
   TeamPolicy& set_scratch_size(int level, PerTeamValue t) {
     scratch_[level] = t.value;
     return *this;

@@ -859,7 +859,7 @@ __global__ void __launch_bounds__(NTH * G, MINB) snl1_tile_kernel(
 
 constexpr int kBandBlock = 288;
 constexpr int kTileMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 113 registers
-constexpr int kBandMinBlocks = 3;  // 3 CTAs of 288 threads per SM: at most 75 registers
+constexpr int kBandMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 96 registers
 int* g_band_err = nullptr;
 
 constexpr int kRowShiftBlock = 288;
