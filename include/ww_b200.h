@@ -80,6 +80,21 @@ void ww_snl1(int igrid, int npts, const float* a, const float* cg, const float* 
 void ww_snl1_device(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
                     float* s, float* d, void* stream);
 
+/* B200 extension; no counterpart in the reference. ww_snl1 (same arguments, results and status
+ * in ww_snl1_last_error) for a caller that must not allocate device memory once its set-up is
+ * over: a coupled run whose partner component has already reserved the rest of HBM through its
+ * own pool, so a late cudaMalloc would fail mid-run, or an operational forecast whose device
+ * footprint is fixed at start-up so that an out-of-memory cannot end it hours later, and where
+ * a cudaFree would stall the other components' work on the device. The copies go through one
+ * 32 MiB static device array instead of per-grid buffers: npts is limited by
+ * 3*c(npts*NSPEC) + c(npts*NK) + c(npts) <= 8388608 floats, c() rounding up to a multiple of
+ * 64 (2137 points of a 36x36 grid); a larger npts is ERR_BAD_SHAPE with nothing written. The
+ * first call on a device does the set-up (resolves the array's address); make it before any
+ * stream capture. The array is one per device for the whole process: calls that overlap in
+ * time (several host threads) race on it. No cudaMalloc, cudaFree or allocating library call. */
+void ww_snl1_noalloc(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+                     float* s, float* d);
+
 /* Replaces ww_snl1_enabled (ww_kokkos_c.hpp:120): 1 if WW_KOKKOS_SNL1 resolves to on (see
  * ww_kokkos_flag) at ww_kokkos_init, else 0. */
 int ww_snl1_enabled(void);

@@ -41,7 +41,7 @@ EXPORTS = (
     "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
     "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_ktp3_batch", "ww_ktp3_batch_va",
-    "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va",
+    "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va", "ww_snl1_noalloc",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -81,6 +81,8 @@ def lib():
         L.ww_snl1.restype = None
         L.ww_snl1_device.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P]
         L.ww_snl1_device.restype = None
+        L.ww_snl1_noalloc.argtypes = [_I, _I, _P, _P, _P, _P, _P]
+        L.ww_snl1_noalloc.restype = None
         L.ww_snl1_enabled.restype = _I
         L.ww_snl1_last_error.restype = _I
         L.ww_snl1_select_kernel.argtypes = [_I, _I]

@@ -364,6 +364,55 @@ void ww_snl1_device(int igrid, int npts, const float* a, const float* cg, const 
   }
 }
 
+void ww_snl1_noalloc(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+                     float* s, float* d) {
+  try {
+    Ctx* c = validate(igrid, npts, a, cg, kdmean, s, d, "ww_snl1_noalloc");
+    if (c == nullptr) return;
+    const size_t nspec = c->cfg.nspec(), nk = c->cfg.nk, n = static_cast<size_t>(npts);
+    auto seg = [](size_t floats) { return (floats + 63) & ~static_cast<size_t>(63); };  // 256 B
+    auto need = [&](size_t m) { return 3 * seg(m * nspec) + seg(m * nk) + seg(m); };
+    const Snl1StaticScratch sc = snl1_static_scratch();  // first call on a device: set-up
+    if (need(n) > sc.floats) {
+      size_t most = sc.floats / (3 * nspec + nk + 1);
+      while (most > 0 && need(most) > sc.floats) --most;
+      char msg[200];
+      std::snprintf(msg, sizeof msg,
+                    "ww_snl1_noalloc: %d points exceed its %zu MiB static scratch (at most %zu "
+                    "points of this grid per call)",
+                    npts, sc.floats * sizeof(float) >> 20, most);
+      g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, msg);
+      return;
+    }
+    float* const da = sc.base;
+    float* const ds = da + seg(n * nspec);
+    float* const dd = ds + seg(n * nspec);
+    float* const dcg = dd + seg(n * nspec);
+    float* const dkd = dcg + seg(n * nk);
+    cudaStream_t st = c->slots[0].stream;
+    WWB_CHECK(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
+    WWB_CHECK(cudaMemcpyAsync(da, a, n * nspec * 4, cudaMemcpyHostToDevice, st));
+    WWB_CHECK(cudaMemcpyAsync(dcg, cg, n * nk * 4, cudaMemcpyHostToDevice, st));
+    WWB_CHECK(cudaMemcpyAsync(dkd, kdmean, n * 4, cudaMemcpyHostToDevice, st));
+    launch_snl1_err(resolve_kernel(*c), c->dev, npts, da, dcg, dkd, ds, dd, sc.err, st);
+    WWB_CHECK(cudaMemcpyAsync(s, ds, n * nspec * 4, cudaMemcpyDeviceToHost, st));
+    WWB_CHECK(cudaMemcpyAsync(d, dd, n * nspec * 4, cudaMemcpyDeviceToHost, st));
+    int flag = 0;
+    WWB_CHECK(cudaMemcpyAsync(&flag, sc.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    WWB_CHECK(cudaStreamSynchronize(st));
+    if (flag != 0) {
+      g_status.fail(WW_KOKKOS_ERR_KERNEL,
+                    "ww_snl1_noalloc: a bulk-copy wait of the DIA kernel gave up");
+      return;
+    }
+    g_status.ok();
+  } catch (const CudaError& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  } catch (const std::exception& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
 int ww_snl1_enabled(void) { return ww_kokkos_flag("WW_KOKKOS_SNL1") != 0 ? 1 : 0; }
 
 int ww_snl1_last_error(void) { return g_status.get(); }

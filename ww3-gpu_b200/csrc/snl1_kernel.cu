@@ -938,7 +938,7 @@ int snl1_take_error() {
 namespace {
 template <int NTH, int G, int BR>
 void launch_tile(const Snl1Dev& p, int npts, const float* a, const float* cg, const float* kd,
-                 float* s, float* d, cudaStream_t stream) {
+                 float* s, float* d, int* err, cudaStream_t stream) {
   static int per_sm = -1;
   static size_t cached = 0;
   const size_t smem = tile_smem<NTH, G, BR>(p);
@@ -952,19 +952,15 @@ void launch_tile(const Snl1Dev& p, int npts, const float* a, const float* cg, co
     per_sm = n;
     cached = smem;
   }
-  if (g_band_err == nullptr) {
-    WWB_CHECK(cudaMalloc(&g_band_err, sizeof(int)));
-    WWB_CHECK(cudaMemset(g_band_err, 0, sizeof(int)));
-  }
   const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
   const int grid = static_cast<int>(npts < resident ? npts : resident);
-  k<<<grid, NTH * G, smem, stream>>>(p, npts, a, cg, kd, s, d, g_band_err);
+  k<<<grid, NTH * G, smem, stream>>>(p, npts, a, cg, kd, s, d, err);
   WWB_CHECK(cudaGetLastError());
 }
 
 template <int AS, bool TMA>
 void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, const float* kd,
-                 float* s, float* d, cudaStream_t stream) {
+                 float* s, float* d, int* err, cudaStream_t stream) {
   static int per_sm = -1;
   static size_t cached = 0;
   const size_t smem = snl1_band_smem(p);
@@ -978,37 +974,56 @@ void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, co
     per_sm = n;
     cached = smem;
   }
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  const int grid = static_cast<int>(npts < resident ? npts : resident);
+  k<<<grid, kBandBlock, smem, stream>>>(p, npts, a, cg, kd, s, d, err);
+  WWB_CHECK(cudaGetLastError());
+}
+
+/// The error flag of the band and tile kernels' bulk-copy waits (allocated on first use).
+int* band_err_flag() {
   if (g_band_err == nullptr) {
     WWB_CHECK(cudaMalloc(&g_band_err, sizeof(int)));
     WWB_CHECK(cudaMemset(g_band_err, 0, sizeof(int)));
   }
-  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
-  const int grid = static_cast<int>(npts < resident ? npts : resident);
-  k<<<grid, kBandBlock, smem, stream>>>(p, npts, a, cg, kd, s, d, g_band_err);
-  WWB_CHECK(cudaGetLastError());
+  return g_band_err;
 }
+
+/// Launches `kernel`; the band and tile kernels report a bulk-copy wait that gave up in `err`,
+/// or in the shared flag band_err_flag() when `err` is null.
+void launch_dispatch(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
+                     const float* kdmean, float* s, float* d, int* err, cudaStream_t stream);
 }  // namespace
 
 void launch_snl1(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                  const float* kdmean, float* s, float* d, cudaStream_t stream) {
+  launch_dispatch(kernel, p, npts, a, cg, kdmean, s, d, nullptr, stream);
+}
+
+namespace {
+void launch_dispatch(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
+                     const float* kdmean, float* s, float* d, int* err, cudaStream_t stream) {
   if (npts <= 0) return;
+  if (kernel == kSnl1Tile || kernel == kSnl1Band) {
+    if (err == nullptr) err = band_err_flag();
+  }
   const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
                        (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
   if (kernel == kSnl1Tile) {
     const int v = tile_variant(p);
-    if (v == 36 && aligned) return launch_tile<36, 8, 5>(p, npts, a, cg, kdmean, s, d, stream);
-    if (v == 24 && aligned) return launch_tile<24, 12, 3>(p, npts, a, cg, kdmean, s, d, stream);
+    if (v == 36 && aligned) return launch_tile<36, 8, 5>(p, npts, a, cg, kdmean, s, d, err, stream);
+    if (v == 24 && aligned) return launch_tile<24, 12, 3>(p, npts, a, cg, kdmean, s, d, err, stream);
     kernel = kSnl1Band;  // caller arrays not 16-byte aligned: the band kernel reads them directly
   }
   if (kernel == kSnl1Band) {
     // The bulk copies need 16-byte aligned sources and sizes: NSPEC and NK multiples of 4.
     const bool tma = p.nspec % 4 == 0 && p.nk % 4 == 0 && aligned;
     if (band_stride(p) == 1536) {
-      if (tma) launch_band<1536, true>(p, npts, a, cg, kdmean, s, d, stream);
-      else launch_band<1536, false>(p, npts, a, cg, kdmean, s, d, stream);
+      if (tma) launch_band<1536, true>(p, npts, a, cg, kdmean, s, d, err, stream);
+      else launch_band<1536, false>(p, npts, a, cg, kdmean, s, d, err, stream);
     } else {
-      if (tma) launch_band<4096, true>(p, npts, a, cg, kdmean, s, d, stream);
-      else launch_band<4096, false>(p, npts, a, cg, kdmean, s, d, stream);
+      if (tma) launch_band<4096, true>(p, npts, a, cg, kdmean, s, d, err, stream);
+      else launch_band<4096, false>(p, npts, a, cg, kdmean, s, d, err, stream);
     }
   } else if (kernel == kSnl1RowShift) {
     const size_t smem = snl1_rowshift_smem(p);
@@ -1035,6 +1050,48 @@ void launch_snl1(int kernel, const Snl1Dev& p, int npts, const float* a, const f
     k<<<npts, kGatherBlock, smem, stream>>>(p, npts, a, cg, kdmean, s, d);
     WWB_CHECK(cudaGetLastError());
   }
+}
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Storage of the entry that allocates nothing (ww_snl1_noalloc): one file-scope device array
+// for the staged A, CG, KDMEAN, S and D, and the bulk-copy error flag of its launches. Both
+// exist once per device for the whole process, so calls that overlap in time (two host
+// threads, or work still in flight on another stream) race on them.
+constexpr size_t kStaticScratchFloats = static_cast<size_t>(8) << 20;  // 32 MiB
+static __device__ __align__(256) float g_static_scratch[kStaticScratchFloats];
+static __device__ int g_static_err;
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+Snl1StaticScratch g_static_dev[kStaticMaxDevices];  // resolved addresses, per device
+}  // namespace
+
+Snl1StaticScratch snl1_static_scratch() {
+  int dev = 0;
+  WWB_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticMaxDevices)
+    throw CudaError(cudaErrorInvalidDevice, "snl1 static scratch: device ordinal out of range");
+  Snl1StaticScratch& e = g_static_dev[dev];
+  if (e.base == nullptr) {
+    // Set-up, once per device with that device current: resolve the arrays' addresses.
+    void* base = nullptr;
+    void* err = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&base, g_static_scratch);
+    if (rc != cudaSuccess) throw CudaError(rc, "snl1 static scratch: cudaGetSymbolAddress");
+    rc = cudaGetSymbolAddress(&err, g_static_err);
+    if (rc != cudaSuccess) throw CudaError(rc, "snl1 static error flag: cudaGetSymbolAddress");
+    e.floats = kStaticScratchFloats;
+    e.err = static_cast<int*>(err);
+    e.base = static_cast<float*>(base);
+  }
+  return e;
+}
+
+void launch_snl1_err(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
+                     const float* kdmean, float* s, float* d, int* err, cudaStream_t stream) {
+  if (err == nullptr) throw CudaError(cudaErrorInvalidValue, "launch_snl1_err: null error flag");
+  launch_dispatch(kernel, p, npts, a, cg, kdmean, s, d, err, stream);
 }
 
 }  // namespace wwb

@@ -48,4 +48,19 @@ int snl1_take_error();
 void launch_snl1(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                  const float* kdmean, float* s, float* d, cudaStream_t stream);
 
+/// The device array behind ww_snl1_noalloc on the current device: `floats` floats at `base`
+/// (256-byte aligned) and an int error flag. The first call on a device resolves the addresses
+/// (cudaGetSymbolAddress); later calls return them.
+struct Snl1StaticScratch {
+  float* base = nullptr;
+  size_t floats = 0;
+  int* err = nullptr;
+};
+Snl1StaticScratch snl1_static_scratch();
+
+/// launch_snl1 with the band and tile kernels' bulk-copy failures reported in `err` (non-null,
+/// zero before the launch) instead of the shared flag that snl1_take_error reads.
+void launch_snl1_err(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
+                     const float* kdmean, float* s, float* d, int* err, cudaStream_t stream);
+
 }  // namespace wwb
