@@ -131,20 +131,14 @@ void publish(Ctx& c) {
   p.ipim = c.ipim.ptr;
   p.ic = c.ic.ptr;
   p.af11 = c.af11.ptr;
-  c.kernel = !t.rowshift ? kSnl1Gather
-             : snl1_tile_ok(p) ? kSnl1Tile
-             : snl1_band_ok(p) ? kSnl1Band
-                               : kSnl1RowShift;
+  c.kernel = !t.rowshift ? kSnl1Gather : snl1_band_ok(p) ? kSnl1Band : kSnl1RowShift;
 }
 
 /// The kernel `which` asks for, or -1 when these tables cannot run it.
 int pick_kernel(const Ctx& c, int which) {
   switch (which) {
     case kSnl1Auto:
-      return !c.tab.rowshift ? kSnl1Gather
-             : snl1_tile_ok(c.dev) ? kSnl1Tile
-             : snl1_band_ok(c.dev) ? kSnl1Band
-                                   : kSnl1RowShift;
+      return !c.tab.rowshift ? kSnl1Gather : snl1_band_ok(c.dev) ? kSnl1Band : kSnl1RowShift;
     case kSnl1Gather:
       return kSnl1Gather;
     case kSnl1RowShift:
