@@ -277,3 +277,177 @@ def xyp3_call(L, case):
                          keep["bbpin"].ctypes.data, keep["on"].ctypes.data, va.shape[0],
                          va.ctypes.data)
     return rc, va
+
+
+# ------------------------------------------------------------------ ST4 and W3SRCE through the reference
+# ArrayId of the C ABI (kokkos/src/ww_kokkos/st4_arrays.hpp:41-61).
+(A_SIG, A_SIG2, A_DSIP, A_DDEN, A_DDEN2, A_ESIN, A_ECOS, A_TH, A_SATWEIGHTS, A_CUMULW, A_DCKI,
+ A_QBI, A_SATINDICES, A_IKTAB, A_TAUT, A_TAUHFT, A_TAUHFT2, A_FWTABLE) = range(18)
+NKHS, NKD, NDTAB = 2000, 1300, 2000
+
+
+def _st4_setup(L):
+    if getattr(L, "_st4_ready", False):
+        return
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.ref_st4_tables.argtypes = [P] * 16
+    L.ref_st4_tables.restype = I
+    L.ww_st4_init.argtypes = [I, P, I, P, I]
+    L.ww_st4_init.restype = I
+    L.ww_st4_set_real.argtypes = [I, I, P, I, P, P]
+    L.ww_st4_set_real.restype = I
+    L.ww_st4_set_int.argtypes = [I, I, P, I, P, P]
+    L.ww_st4_set_int.restype = I
+    L.ww_st4_commit.argtypes = [I]
+    L.ww_st4_commit.restype = I
+    L.ww_st4_last_error.restype = I
+    L.ww_sds4.argtypes = [I, I] + [P] * 8 + [I, I] + [P] * 4
+    L.ww_sds4.restype = None
+    L.ww_sin4.argtypes = [I, I] + [P] * 17
+    L.ww_sin4.restype = None
+    L.ww_spr4.argtypes = [I, I] + [P] * 20
+    L.ww_spr4.restype = None
+    L.ww_srce_init.argtypes = [I, P, I, P, I, P, P, P, P, P]
+    L.ww_srce_init.restype = I
+    L.ww_srce_batch.argtypes = [I, I, I, I, I, F, I] + [P] * 9
+    L.ww_srce_batch.restype = None
+    L.ww_srce_last_error.restype = I
+    L._st4_ready = True
+
+
+def _p(x):
+    return None if x is None else x.ctypes.data
+
+
+def st4_tables(st):
+    """The ST4 tables of the synthetic grid ``st`` (ww3_gpu_b200.synth.st4_setup) from the
+    reference's own INSIN4 and TABU_* (ref_st4_tables), and the DEL* module scalars; rpar gets
+    the DEL* written in."""
+    L = ref_lib()
+    _st4_setup(L)
+    ipar = st["ipar"]
+    nk, nth, mk, mth, mspec = (int(ipar[0]), int(ipar[1]), int(ipar[3]), int(ipar[4]),
+                               int(ipar[5]))
+    nsat = 2 * (mth // 2 - 1) + 1
+    R = st["R"]
+    tabs = float(st["rpar"][R["SINTAILPAR"]]) > 0.5
+    tabs2 = tabs and float(st["rpar"][R["TTAUWSHELTER"]]) > 0
+    t = {
+        "satweights": np.zeros(nsat * mth, np.float32),
+        "satindices": np.zeros(nsat * mth, np.int32),
+        "iktab": np.zeros(mk * NDTAB, np.int32),
+        "dcki": np.zeros(NKHS * NKD, np.float32),
+        "qbi": np.zeros(NKHS * NKD, np.float32),
+        "cumulw": np.zeros(mspec * mspec, np.float32),
+        "taut": np.zeros(201 * 201, np.float32) if tabs else None,
+        "tauhft": np.zeros(101 * 201, np.float32) if tabs else None,
+        "tauhft2": np.zeros(101 * 201 * 51, np.float32) if tabs2 else None,
+    }
+    dl = np.zeros(5, np.float32)
+    L.ref_st4_tables(_p(st["rpar"]), _p(ipar), _p(st["sig"]), _p(st["dsip"]), _p(st["th"]),
+                     _p(st["ecos"]), _p(t["satweights"]), _p(t["satindices"]), _p(t["iktab"]), _p(t["dcki"]),
+                     _p(t["qbi"]), _p(t["cumulw"]), _p(t["taut"]), _p(t["tauhft"]),
+                     _p(t["tauhft2"]), _p(dl))
+    rpar = st["rpar"].copy()
+    for j, name in enumerate(("DELUST", "DELALP", "DELTAUW", "DELU", "DELTAIL")):
+        rpar[R[name]] = dl[j]
+    t["rpar"] = rpar
+    t["nsat"] = nsat
+    return t
+
+
+def st4_registrations(st, t):
+    """(id, array, is_int, lbounds, extents) of every ST4 array, as ww_st4_set_real/int takes
+    them (st4_arrays.hpp:72-81)."""
+    ipar = st["ipar"]
+    nk, nth, nspec, mk, mth, mspec = [int(v) for v in ipar[:6]]
+    nsat = t["nsat"]
+    regs = [
+        (A_SIG, st["sig"], False, [0], [nk + 2]),
+        (A_SIG2, st["sig2"], False, [1], [nspec]),
+        (A_DSIP, st["dsip"], False, [0], [nk + 2]),
+        (A_DDEN, st["dden"], False, [1], [nk]),
+        (A_DDEN2, st["dden2"], False, [1], [nspec]),
+        (A_ESIN, st["esin"], False, [1], [nspec + nth]),
+        (A_ECOS, st["ecos"], False, [1], [nspec + nth]),
+        (A_TH, st["th"], False, [1], [nth]),
+        (A_SATWEIGHTS, t["satweights"], False, [1, 1], [nsat, mth]),
+        (A_CUMULW, t["cumulw"], False, [1, 1], [mspec, mspec]),
+        (A_DCKI, t["dcki"], False, [1, 1], [NKHS, NKD]),
+        (A_QBI, t["qbi"], False, [1, 1], [NKHS, NKD]),
+        (A_SATINDICES, t["satindices"], True, [1, 1], [nsat, mth]),
+        (A_IKTAB, t["iktab"], True, [1, 1], [mk, NDTAB]),
+        (A_FWTABLE, st["fwtable"], False, [0], [301]),
+    ]
+    if t["taut"] is not None:
+        regs.append((A_TAUT, t["taut"], False, [0, 0], [201, 201]))
+        regs.append((A_TAUHFT, t["tauhft"], False, [0, 0], [101, 201]))
+    if t["tauhft2"] is not None:
+        regs.append((A_TAUHFT2, t["tauhft2"], False, [0, 0, 0], [101, 201, 51]))
+    return regs
+
+
+def register_st4(init, set_real, set_int, commit, st, t):
+    """Configure one ST4 grid through an init/set_real/set_int/commit quadruple with the
+    reference's argument lists; returns commit's status."""
+    rc = init(_p(t["rpar"]), len(t["rpar"]), _p(st["ipar"]), len(st["ipar"]))
+    if rc != 0:
+        return rc
+    for aid, arr, is_int, lb, ext in st4_registrations(st, t):
+        lb = np.asarray(lb, np.int32)
+        ext = np.asarray(ext, np.int32)
+        f = set_int if is_int else set_real
+        rc = f(aid, _p(np.ascontiguousarray(arr)), len(ext), _p(lb), _p(ext))
+        if rc != 0:
+            return rc
+    return commit()
+
+
+class RefSt4:
+    """The reference's ST4 and W3SRCE through its own C ABI, for grid ``igrid``: ww_st4_*,
+    ww_sds4 / ww_sin4 / ww_spr4, ww_snl1_init + ww_srce_init + ww_srce_batch. ``scalar_mvec``
+    selects the build whose five libmvec loops run scalar glibc powf/expf per lane."""
+
+    def __init__(self, st, t, igrid=1, srce=None, dia=None, scalar_mvec=False):
+        path = REF_PATH.parent / ("libref_ww3_scalar.so" if scalar_mvec else "libref_ww3.so")
+        self.L = _ref_variant(path)
+        _st4_setup(self.L)
+        L, g = self.L, igrid
+        self.igrid = g
+        self.nk, self.nth = int(st["ipar"][0]), int(st["ipar"][1])
+        rc = register_st4(lambda *a: L.ww_st4_init(g, *a), lambda *a: L.ww_st4_set_real(g, *a),
+                          lambda *a: L.ww_st4_set_int(g, *a), lambda: L.ww_st4_commit(g), st, t)
+        if rc != 0:
+            raise RuntimeError(f"reference ST4 registration failed: {rc}")
+        if dia is not None:
+            cfg, sig = dia
+            if L.ww_snl1_init(g, cfg["nk"], cfg["nth"], *_cfg_args(cfg),
+                              np.ascontiguousarray(sig, np.float32)) != 0:
+                raise RuntimeError("reference ww_snl1_init failed")
+        if srce is not None:
+            rc = L.ww_srce_init(g, _p(srce["rpar"]), len(srce["rpar"]), _p(srce["ipar"]),
+                                len(srce["ipar"]), _p(srce["sig"]), _p(srce["dden"]),
+                                _p(srce["ecos"]), _p(srce["esin"]), _p(srce["mapwn"]))
+            if rc != 0:
+                raise RuntimeError(f"reference ww_srce_init returned {rc}")
+
+
+_ref_variants = {}
+
+
+def _ref_variant(path):
+    """A reference build by path (each loaded once, RTLD_LOCAL) with ww_kokkos_init done."""
+    key = str(path)
+    if key == str(REF_PATH):
+        return ref_lib()
+    if key not in _ref_variants:
+        L = ctypes.CDLL(key, mode=ctypes.RTLD_LOCAL)
+        L.ww_kokkos_init.argtypes = [ctypes.c_int]
+        L.ww_kokkos_init.restype = ctypes.c_int
+        f = ctypes.c_float
+        L.ww_snl1_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [f] * 10 + [_f32p]
+        L.ww_snl1_init.restype = ctypes.c_int
+        if L.ww_kokkos_init(-1) != 0:
+            raise RuntimeError("reference ww_kokkos_init failed")
+        _ref_variants[key] = L
+    return _ref_variants[key]

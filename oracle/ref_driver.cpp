@@ -81,3 +81,52 @@ extern "C" int ref_w3map3(int nx, int ny, int nsea, int nk, int nth, const int* 
   w3map3(Kokkos::DefaultHostExecutionSpace(), s, v, c);
   return 0;
 }
+
+// INSIN4(FLTABS=.TRUE.) of the reference (kokkos/src/ww_kokkos/st4_insin4.cpp, st4_tabu_*.cpp),
+// to build the ST4 tables of synthetic grids for the tests. rpar/ipar are the ST4 packets
+// (st4_params.hpp:79-154); sig, dsip are SIG(0:MK+1), DSIP(0:MK+1). Out, column-major with the
+// shapes of st4_arrays.hpp:93-114 (allocate_tables); th = TH(1:MTH), ecos = ECOS(1:MSPEC+MTH): satweights, satindices (2*(MTH/2-1)+1, MTH),
+// iktab (MK, NDTAB), dcki, qbi (NKHS, NKD), cumulw (MSPEC, MSPEC), taut (ITAUMAX+1, JUMAX+1),
+// tauhft (IUSTAR+1, IALPHA+1), tauhft2 (IUSTAR+1, IALPHA+1, ILEVTAIL+1) (may be null when not
+// allocated), del[5] = DELUST, DELALP, DELTAUW, DELU, DELTAIL.
+#include "ww_kokkos/st4_tables_build.hpp"
+
+extern "C" int ref_st4_tables(const float* rpar, const int* ipar, const float* sig,
+                              const float* dsip, const float* th, const float* ecos,
+                              float* satweights, int* satindices, int* iktab,
+                              float* dcki, float* qbi, float* cumulw, float* taut, float* tauhft,
+                              float* tauhft2, float* del) {
+  using namespace ww::st4;
+  Params p = unpack(rpar, ipar);
+  HostArrays a;
+  a.sig = HostArrays::V1<float>("sig", p.mk + 2);
+  a.dsip = HostArrays::V1<float>("dsip", p.mk + 2);
+  for (int i = 0; i < p.mk + 2; ++i) {
+    a.sig(i) = sig[i];
+    a.dsip(i) = dsip[i];
+  }
+  a.th = HostArrays::V1<float>("th", p.mth);
+  for (int i = 0; i < p.mth; ++i) a.th(i) = th[i];
+  a.ecos = HostArrays::V1<float>("ecos", p.mspec + p.mth);
+  for (int i = 0; i < p.mspec + p.mth; ++i) a.ecos(i) = ecos[i];
+  allocate_tables(p, a);
+  insin4(p, true, a);
+  auto out = [](const auto& v, auto* dst) {
+    if (dst && v.data()) std::memcpy(dst, v.data(), sizeof(*dst) * v.size());
+  };
+  out(a.satweights, satweights);
+  out(a.satindices, satindices);
+  out(a.iktab, iktab);
+  out(a.dcki, dcki);
+  out(a.qbi, qbi);
+  out(a.cumulw, cumulw);
+  out(a.taut, taut);
+  out(a.tauhft, tauhft);
+  out(a.tauhft2, tauhft2);
+  del[0] = p.delust;
+  del[1] = p.delalp;
+  del[2] = p.deltauw;
+  del[3] = p.delu;
+  del[4] = p.deltail;
+  return 0;
+}

@@ -44,10 +44,87 @@ def checker(tmp_path_factory):
     return exe
 
 
-def test_expf_equals_glibc(checker):
-    stride = "1" if os.environ.get("WWB_LIBM_FULL") == "1" else "61"
-    out = subprocess.run([str(checker), stride], check=True, capture_output=True, text=True).stdout
+def _mismatches(checker, fn, stride):
+    out = subprocess.run([str(checker), fn, str(stride)], check=True, capture_output=True,
+                         text=True).stdout
     default = int(re.search(r"default (\d+)", out).group(1))
     lines = [ln for ln in out.splitlines() if ln.startswith("variant")]
     per_variant = {int(ln.split()[1]): int(ln.split()[2]) for ln in lines}
+    return per_variant, default, out
+
+
+FULL = os.environ.get("WWB_LIBM_FULL") == "1"
+
+
+def test_expf_equals_glibc(checker):
+    per_variant, default, out = _mismatches(checker, "expf", 1 if FULL else 61)
     assert per_variant[default] == 0, out
+
+
+@pytest.mark.parametrize("fn", ["logf", "sincosf", "tanhf", "atanf", "log10f"])
+def test_unary_equals_glibc(checker, fn):
+    """Every 61st bit pattern (all 2^32 with WWB_LIBM_FULL=1); sincosf also against a lone
+    sinf and cosf, which the reference calls as separate functions."""
+    per_variant, _, out = _mismatches(checker, fn, 1 if FULL else 61)
+    assert per_variant[0] == 0 and per_variant[1] == 0, out
+
+
+@pytest.mark.parametrize("fn", ["powf", "atan2f"])
+def test_binary_equals_glibc(checker, fn):
+    """Seeded argument pairs: 2^32/64 of them (2^32/4 with WWB_LIBM_FULL=1)."""
+    per_variant, _, out = _mismatches(checker, fn, 4 if FULL else 64)
+    assert per_variant[0] == 0, out
+
+
+def _decimal_table(name):
+    text = HDR.read_text()
+    start = text.index(f"#define {name}")
+    body = text[start:text.index("}", start)]
+    return [float.fromhex(m) for m in re.findall(r"(-?0x[0-9a-f.]+p[+-]?\d+)", body)]
+
+
+def test_log_tables_are_generated_from_invc():
+    """ln(c) and log2(c) of the logf / powf subintervals are -ln(invc) and -log2(invc) of the
+    published 1/c values, rounded to double."""
+    getcontext().prec = 60
+    invc = _decimal_table("WWB_LOG_INVC")
+    logc = _decimal_table("WWB_LOG_LOGC")
+    log2c = _decimal_table("WWB_LOG2_LOGC")
+    assert len(invc) == len(logc) == len(log2c) == 16
+    ln2 = Decimal(2).ln()
+    for i in range(16):
+        lnc = -Decimal(invc[i]).ln()
+        assert float(lnc) == logc[i], i
+        assert float(lnc / ln2) == log2c[i], i
+
+
+def test_inv_pio4_is_two_over_pi():
+    """The sincosf reduction table is 2/pi's binary fraction in 32-bit windows 8 bits apart."""
+    getcontext().prec = 100
+    text = HDR.read_text()
+    start = text.index("#define WWB_INV_PIO4")
+    body = text[start:text.index("}", start)]
+    words = [int(m, 16) for m in re.findall(r"0x([0-9a-f]+)u", body)]
+    # pi by Machin's formula
+    def arctan_inv(n):
+        x = Decimal(1) / n
+        s, t, k = x, x, 1
+        while True:
+            t *= -x * x
+            k += 2
+            d = t / k
+            if abs(d) < Decimal(10) ** -95:
+                return s
+            s += d
+    pi = 16 * arctan_inv(5) - 4 * arctan_inv(239)
+    f, b = 2 / pi, []
+    for _ in range(30):
+        f *= 256
+        b.append(int(f))
+        f -= int(f)
+    for j, w in enumerate(words):
+        want = 0
+        for q in range(4):
+            idx = j - 3 + q
+            want = (want << 8) | (b[idx] if idx >= 0 else 0)
+        assert w == want, j

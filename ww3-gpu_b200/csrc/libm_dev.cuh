@@ -576,7 +576,7 @@ WWB_HD float atanf(float x) {
               hi3 = asfloat(0x3fc90fdau);
   const float lo0 = asfloat(0x31ac3769u), lo1 = asfloat(0x33222168u), lo2 = asfloat(0x33140fb4u),
               lo3 = asfloat(0x33a22168u);
-  const float T0 = asfloat(0x3eaaaaaau), T1 = asfloat(0xbe4ccccdu), T2 = asfloat(0x3e124925u),
+  const float T0 = asfloat(0x3eaaaaabu), T1 = asfloat(0xbe4ccccdu), T2 = asfloat(0x3e124925u),
               T3 = asfloat(0xbde38e38u), T4 = asfloat(0x3dba2e6eu), T5 = asfloat(0xbd9d8795u),
               T6 = asfloat(0x3d886b35u), T7 = asfloat(0xbd6ef16bu), T8 = asfloat(0x3d4bda59u),
               T9 = asfloat(0xbd15a221u), T10 = asfloat(0x3c8569d7u);

@@ -342,3 +342,178 @@ def xyp3_case(nx=48, ny=32, seed=0, nk=36, nth=36, iclose=2, flcur=True, flbpi=T
         "nbi": nbi, "isbpi": isbpi, "bbpi0": bb0.reshape(-1), "bbpin": bbn.reshape(-1),
         "on": on, "va": va, "nsea": nsea, "nx": nx, "ny": ny,
     }
+
+
+# ------------------------------------------------------------------------ ST4 and W3SRCE inputs
+# The ST4 / W3SRCE packets and grid arrays of a synthetic WW3 grid. WW3's namelist defaults are not
+# part of the reference (it only names them); the values below are in the ranges of WW3's ST4
+# (Ardhuin et al. 2010) configurations and exercise every branch the kernels translate: the
+# saturation-based breaking (SSDSC(1) = 1) with a directional sector (SSDSDTH < 180), the default
+# O(NK^2 NTH^2) cumulative term (SSDSC(3) < 0), swell damping through FWTABLE (SSWELLF(2) /= 0),
+# the tabulated stress and tail (SINTAILPAR(1) > 0.5, TTAUWSHELTER > 0) and the whitecap
+# outputs. Parity does not depend on the values: the oracle and the kernels get the same arrays.
+ST4_NRPAR, ST4_NIPAR = 84, 9
+SRCE_NRPAR, SRCE_NIPAR = 29, 12
+
+
+def st4_setup(nk=36, nth=36, xfr=1.1, f1=0.0373, variant="default"):
+    """ST4 rpar/ipar (float32/int32) and grid arrays (float32, at the Fortran lower bounds:
+    sig = SIG(0:NK+1), dsip = DSIP(0:NK+1), dden = DDEN(1:NK), sig2, dden2 (NSPEC),
+    esin, ecos (NSPEC+NTH), th (NTH), fwtable (0:300)). variant "analytic" uses the analytic
+    tail and Newton friction velocity (SINTAILPAR(1) < 0.5), "romero" the SSDSC(1) = 3 breaking."""
+    sig1, dth = spectral_grid(nk, nth, f1=f1, xfr=xfr)
+    x = np.float32(xfr)
+    sig = np.empty(nk + 2, np.float32)
+    sig[1:nk + 1] = sig1
+    sig[0] = np.float32(sig1[0] / x)
+    sig[nk + 1] = np.float32(sig1[-1] * x)
+    sigstep = np.float32(0.5) * (x - np.float32(1.0) / x)
+    dsip = (sig * sigstep).astype(np.float32)
+    dden = (np.float32(dth) * dsip[1:nk + 1] * sig1).astype(np.float32)
+    nspec = nk * nth
+    th = (np.arange(nth, dtype=np.float64) * float(dth)).astype(np.float32)
+    mapwn = np.repeat(np.arange(1, nk + 1), nth)
+    mapth = np.tile(np.arange(1, nth + 1), nk)
+    sig2 = sig[mapwn].astype(np.float32)
+    dden2 = dden[mapwn - 1].astype(np.float32)
+    ec = np.cos(th.astype(np.float64)).astype(np.float32)
+    es = np.sin(th.astype(np.float64)).astype(np.float32)
+    ecos = np.concatenate([ec[mapth - 1], ec]).astype(np.float32)
+    esin = np.concatenate([es[mapth - 1], es]).astype(np.float32)
+    # FWTABLE(0:300): a smooth friction-factor curve over log10(a/z0) in [-1, 8] (DELAB = 0.03).
+    delab = np.float32(9.0 / 300.0)
+    xab = -1.0 + np.arange(301) * float(delab)
+    fwtable = (0.24 * np.exp(-0.9 * np.maximum(xab, 0.0)) + 0.002).astype(np.float32)
+
+    r = np.zeros(ST4_NRPAR, np.float32)
+    R = {"DTH": 0, "XFR": 1, "FTE": 2, "FTF": 3, "AAIRCMIN": 4, "AAIRGB": 5, "IGPARS5": 6,
+         "WWNMEANPTAIL": 7, "SSTXFTFTAIL": 8, "AALPHA": 9, "BBETA": 10, "ZZ0MAX": 11,
+         "ZZ0RAT": 12, "ZZALP": 13, "SSINTHP": 14, "TTAUWSHELTER": 15, "SSWELLF": 16,
+         "SSDSC": 23, "SSDSBR": 44, "SINTAILPAR": 45, "SSDSP": 50, "WWNMEANP": 51,
+         "SSTXFTWN": 52, "SSDSBRF1": 53, "SSDSBINT": 54, "SSDSBCK": 55, "SSDSHCK": 56,
+         "SSDSABK": 57, "SSDSPBK": 58, "CAPCHNK": 59, "ZZWND": 69, "SSDSCOS": 70,
+         "SSDSDTH": 71, "SSDSBT": 72, "SSDSBM": 73, "DELUST": 78, "DELALP": 79, "DELTAUW": 80,
+         "DELU": 81, "DELTAIL": 82, "DELAB": 83}
+    assert R["DELAB"] + 1 == 84
+    sn = float(sig1[-1])
+    r[R["DTH"]] = dth
+    r[R["XFR"]] = x
+    r[R["FTE"]] = 0.25 * sn * float(dth) * sn
+    r[R["FTF"]] = 0.20 * float(dth) * sn
+    r[R["AAIRCMIN"]] = 2.0
+    r[R["AAIRGB"]] = 0.2
+    r[R["WWNMEANPTAIL"]] = -0.5
+    r[R["SSTXFTFTAIL"]] = 0.25
+    r[R["AALPHA"]] = 0.0095
+    r[R["BBETA"]] = 1.52
+    r[R["ZZ0MAX"]] = 0.0
+    r[R["ZZ0RAT"]] = 0.04
+    r[R["ZZALP"]] = 0.006
+    r[R["SSINTHP"]] = 2.0
+    r[R["TTAUWSHELTER"]] = 1.0
+    r[R["SSWELLF"]:R["SSWELLF"] + 7] = [0.66, -0.018, 0.022, 1.5e5, 1.2, 0.0, 2.3e5]
+    sdsc = np.zeros(21, np.float32)
+    sdsc[0] = 1.0          # saturation-based breaking
+    sdsc[1] = -2.2e-5      # SDSC2
+    sdsc[2] = -0.40344     # SDSCUM < 0: the default cumulative branch
+    sdsc[4] = 0.0
+    sdsc[5] = 0.3          # isotropic part
+    sdsc[6] = 0.3          # whitecap width
+    sdsc[11] = 1.0         # SIG power of the mean direction weights
+    sdsc[19] = 1.0
+    r[R["SSDSC"]:R["SSDSC"] + 21] = sdsc
+    r[R["SSDSBR"]] = 0.0009
+    r[R["SINTAILPAR"]:R["SINTAILPAR"] + 5] = [1.0, 1.0, 0.0, 1.0, 0.11]
+    r[R["SSDSP"]] = 2.0
+    r[R["WWNMEANP"]] = 0.5
+    r[R["SSTXFTWN"]] = 0.2
+    r[R["SSDSBRF1"]] = 0.5
+    r[R["ZZWND"]] = 10.0
+    r[R["SSDSCOS"]] = 2.0
+    r[R["SSDSDTH"]] = 80.0
+    r[R["SSDSBT"]] = 0.0
+    r[R["SSDSBM"]:R["SSDSBM"] + 5] = [0.0, 1.0, 0.0, 0.0, 0.0]
+    r[R["DELAB"]] = delab
+    if variant == "analytic":
+        r[R["SINTAILPAR"]:R["SINTAILPAR"] + 5] = [0.0, 1.0, 0.0, 1.0, 0.11]
+        r[R["TTAUWSHELTER"]] = 0.0
+    if variant == "romero":
+        sdsc3 = sdsc.copy()
+        sdsc3[0] = 3.0
+        sdsc3[1] = 5.0e-5
+        sdsc3[8] = 0.05
+        sdsc3[12] = 1.0
+        sdsc3[13] = 1.0
+        sdsc3[14] = 1.0
+        sdsc3[15] = 1.2
+        sdsc3[17] = 0.5
+        sdsc3[18] = 1.0
+        sdsc3[10] = 1.0
+        sdsc3[7] = 1.0
+        r[R["SSDSC"]:R["SSDSC"] + 21] = sdsc3
+        r[R["SSDSBT"]] = 0.001
+    ipar = np.array([nk, nth, nspec, nk, nth, nspec, 0, 0, 0], np.int32)
+    return {"rpar": r, "ipar": ipar, "sig": sig, "sig2": sig2, "dsip": dsip, "dden": dden,
+            "dden2": dden2, "esin": esin, "ecos": ecos, "th": th, "fwtable": fwtable,
+            "mapwn": mapwn.astype(np.int32), "R": R, "nk": nk, "nth": nth, "dth": dth}
+
+
+def srce_setup(st, ln1=0, seed=0):
+    """W3SRCE rpar/ipar and grid arrays (SIG, DDEN (NK), ECOS, ESIN (NSPEC), MAPWN (NSPEC)) for
+    the ST4 grid ``st`` of st4_setup. ``seed`` switches W3_SEED, ``ln1`` W3SLN1."""
+    nk, nth = st["nk"], st["nth"]
+    sig1 = st["sig"][1:nk + 1]
+    x = float(st["rpar"][1])
+    r = np.zeros(SRCE_NRPAR, np.float32)
+    lnx = np.log(x)
+    r[0] = 0.3                                   # DMIN
+    r[1] = 300.0                                 # DTMAX
+    r[2] = 15.0                                  # DTMIN
+    r[3] = 1.0 / lnx                             # FACTI1
+    r[4] = 1.0 - np.log(float(sig1[0])) / lnx    # FACTI2
+    r[5] = x ** -7.0                             # FACHFA = XFR**(-FACHF-2)
+    r[6] = 0.62e-3 * (2 * np.pi) ** 4 / GRAV ** 2  # FACP
+    r[7] = 0.0                                   # XFLT
+    r[8] = 0.1                                   # XREL
+    r[9] = 0.8                                   # FHMAX
+    r[10] = 2.5 * 2 * np.pi                      # FFXFM
+    r[11] = 4.0 * GRAV / 28.0                    # FFXPM
+    r[12] = 0.0                                  # FFXFA
+    r[13:17] = 0.0                               # ICESCALES
+    r[17] = 1.0e-6                               # SLNC1
+    r[18] = 1.0                                  # FSPM
+    r[19] = 1.0                                  # FSHF
+    r[20] = -0.067 / GRAV                        # SBTC1
+    r[21] = 0.25                                 # SDBC1
+    r[22] = 0.8                                  # SDBC2
+    r[23] = 0.9                                  # FACSD
+    ipar = np.array([nk, nth, nk * nth, 1, 0, 0, 0, 1, ln1, seed, 0, 0], np.int32)
+    return {"rpar": r, "ipar": ipar, "sig": sig1.copy(), "dden": st["dden"].copy(),
+            "ecos": st["ecos"][:nk * nth].copy(), "esin": st["esin"][:nk * nth].copy(),
+            "mapwn": st["mapwn"].copy()}
+
+
+def srce_points(npts, seed=0, nk=36, nth=36, depth_range=(10.0, 4000.0)):
+    """Per-point W3SRCE inputs: spec (npts, nspec) action density, wn1, cg1 (npts, nk), pin
+    (npts, 7: D_INP U10ABS U10DIR AS ICE DAIR COEF), psc (npts, 22) and whitecap (npts, 4),
+    taubbl, tauice (npts, 2). Winds U10 ~ U(3, 25) m/s from a random direction."""
+    g = sea_states(npts, seed=seed, nk=nk, nth=nth, depth_range=depth_range)
+    rng = np.random.default_rng(seed + 7)
+    sig, _ = spectral_grid(nk, nth)
+    k = wavenumber(sig, g["depth"])
+    u10 = rng.uniform(3.0, 25.0, npts)
+    udir = rng.uniform(0.0, 2 * np.pi, npts)
+    pin = np.zeros((npts, 7), np.float32)
+    pin[:, 0] = g["depth"]
+    pin[:, 1] = u10
+    pin[:, 2] = udir
+    pin[:, 5] = 1.225
+    pin[:, 6] = 1.0
+    psc = np.zeros((npts, 22), np.float32)
+    psc[:, 0] = 0.035 * u10          # USTAR
+    psc[:, 1] = udir                 # USTDIR
+    psc[:, 2] = 0.5 * (0.035 * u10) ** 2 * np.cos(udir)  # TAUWX
+    psc[:, 3] = 0.5 * (0.035 * u10) ** 2 * np.sin(udir)
+    return {"spec": g["a"], "wn1": k.astype(np.float32), "cg1": g["cg"], "pin": pin,
+            "psc": psc, "whitecap": np.zeros((npts, 4), np.float32),
+            "taubbl": np.zeros((npts, 2), np.float32), "tauice": np.zeros((npts, 2), np.float32)}
