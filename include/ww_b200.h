@@ -219,6 +219,99 @@ int ww_xyp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, i
  * returns it only). */
 int ww_prop3_last_error(void);
 
+/* ---------------------------------------------------------------- ST4 source terms (W3SRC4MD) */
+/* A grid is configured as the reference's (ww_kokkos_c.hpp:136-203): ww_st4_init with the
+ * RPAR/IPAR packets (st4_params.hpp:79-154 layout: 84 reals, 9 ints), one ww_st4_set_real/int per
+ * array (ArrayId of st4_arrays.hpp:41-61, with its rank, LBOUND and SHAPE as the Fortran has them;
+ * copied, not borrowed), then ww_st4_commit, which checks every array the configuration needs and
+ * copies them to the device. TAUT, TAUHFT, TAUHFT2, FWTABLE and the DEL* scalars are one copy per
+ * process, the last registration wins. Point entries take npts points, every per-point scalar an
+ * array of npts; OUT arguments are copied in as well as out; status in ww_st4_last_error().
+ * WW_KOKKOS_ST4_TABLES=1 is accepted and the registered tables are used. */
+
+/* Replaces ww_st4_init (ww_kokkos_c.hpp:158). OK, NOT_INITIALISED, BAD_SHAPE, UNSUPPORTED (W3_FLX5,
+ * or NTH > 128). */
+int ww_st4_init(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar);
+
+/* Replace ww_st4_set_real / ww_st4_set_int (ww_kokkos_c.hpp:163-166). OK, NOT_INITIALISED, TABLE. */
+int ww_st4_set_real(int igrid, int id, const float* data, int rank, const int* lbound,
+                    const int* extent);
+int ww_st4_set_int(int igrid, int id, const int* data, int rank, const int* lbound,
+                   const int* extent);
+
+/* Replaces ww_st4_commit (ww_kokkos_c.hpp:172). OK, NOT_INITIALISED, TABLE, RUNTIME. */
+int ww_st4_commit(int igrid);
+
+/* Replaces ww_sds4 (ww_kokkos_c.hpp:177): W3SDS4. a, srhs, ddiag, brlambda (nspec, npts);
+ * k, cg (nk, npts); whitecap (4, npts); the scalars (npts). */
+void ww_sds4(int igrid, int npts, const float* a, const float* k, const float* cg,
+             const float* ustar, const float* usdir, const float* depth, const float* dair,
+             const float* dlwmean, int flogrd57, int flogrd58, float* srhs, float* ddiag,
+             float* brlambda, float* whitecap);
+
+/* Replaces ww_sin4 (ww_kokkos_c.hpp:185): W3SIN4. a, k, s, d, llws (nspec, npts); cg (nk, npts). */
+void ww_sin4(int igrid, int npts, const float* a, const float* cg, const float* k,
+             const float* u, const float* ustar, const float* drat, const float* as,
+             const float* usdir, const float* z0, const float* cd, float* tauwx, float* tauwy,
+             float* tauwnx, float* tauwny, float* s, float* d, int* llws);
+
+/* Replaces ww_spr4 (ww_kokkos_c.hpp:193): W3SPR4 with CALC_USTAR. a, llws (nspec, npts); cg, wn
+ * (nk, npts); ustar, usdir INOUT. */
+void ww_spr4(int igrid, int npts, const float* a, const float* cg, const float* wn,
+             const float* u, const float* udir, const float* tauwx, const float* tauwy,
+             const int* llws, float* ustar, float* usdir, float* emean, float* fmean,
+             float* fmean1, float* wnmean, float* amax, float* cd, float* z0, float* charn,
+             float* fmeanws, float* dlwmean);
+
+/* Replaces ww_st4_enabled (ww_kokkos_c.hpp:198): 1 WW_KOKKOS_SDS4, 2 WW_KOKKOS_SIN4,
+ * 3 WW_KOKKOS_SPR4, 4 WW_KOKKOS_ST4_TABLES. */
+int ww_st4_enabled(int which);
+
+/* Replaces ww_st4_last_error (ww_kokkos_c.hpp:201). */
+int ww_st4_last_error(void);
+
+/* ----------------------------------------------------------- W3SRCE (source-term integration) */
+/* Replaces ww_srce_init (ww_kokkos_c.hpp:216): rpar (29), ipar (12) at srce_params.hpp:36-84's
+ * indices; sig, dden (NK), ecos, esin, mapwn (NSPEC), copied. Needs ww_snl1_init and
+ * ww_st4_commit of the grid. OK, NOT_INITIALISED, BAD_SHAPE, UNSUPPORTED (not switch_lab_shrd's
+ * source terms; W3FLD2; DIA tables not in the row-shift form). */
+int ww_srce_init(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar,
+                 const float* sig, const float* dden, const float* ecos, const float* esin,
+                 const int* mapwn);
+
+/* Replaces ww_srce (ww_kokkos_c.hpp:227): W3SRCE(srce_direct, ...) for one point, the arguments in
+ * the order of the Fortran dummy list (spec (nspec), whitecap (4), taubbl (2), tauice (2) and
+ * every pointer scalar INOUT). */
+void ww_srce(int igrid, int it, int inflags24, int flogrd57, int flogrd58, float* spec,
+             const float* wn1, const float* cg1, float d_inp, float u10abs, float u10dir,
+             float as, float ice, float dtg, float dair, float coef, float* ustar,
+             float* ustdir, float* tauwx, float* tauwy, float* dtdyn, float* fcut,
+             float* tauox, float* tauoy, float* tauwix, float* tauwiy, float* tauwnx,
+             float* tauwny, float* phiaw, float* charn, float* tws, float* phioc,
+             float* whitecap, float* phibbl, float* taubbl, float* tauice, float* phice,
+             float* tauocx, float* tauocy, float* wnmean, float* fpi, int* shave);
+
+/* Replaces ww_srce_batch (ww_kokkos_c.hpp:266): W3SRCE for npts points of a time step. spec
+ * (nspec, npts), psc (22, npts), whitecap (4, npts), taubbl, tauice (2, npts) INOUT; wn1, cg1
+ * (nk, npts), pin (7, npts) IN; shave (npts) OUT. Packet rows as WwSrceBatchIn / WwSrceBatchScal
+ * (ww_kokkos_c.hpp:231-251). One launch on a persistent grid with a work queue. */
+void ww_srce_batch(int igrid, int it, int inflags24, int flogrd57, int flogrd58, float dtg,
+                   int npts, float* spec, const float* wn1, const float* cg1, const float* pin,
+                   float* psc, float* whitecap, float* taubbl, float* tauice, int* shave);
+
+/* Replaces ww_srce_batch_va (resident_c.hpp:98): ww_srce_batch on the resident VA of the grid,
+ * point k being VA(:, jsea[k]) (1 <= jsea[k] <= nsealm); the spectra are not copied. */
+void ww_srce_batch_va(int igrid, int it, int inflags24, int flogrd57, int flogrd58, float dtg,
+                      float* va, int nspec, int nsealm, int npts, const int* jsea,
+                      const float* wn1, const float* cg1, const float* pin, float* psc,
+                      float* whitecap, float* taubbl, float* tauice, int* shave);
+
+/* Replaces ww_srce_enabled (ww_kokkos_c.hpp:272): 1 if WW_KOKKOS_SRCE resolves to on. */
+int ww_srce_enabled(void);
+
+/* Replaces ww_srce_last_error (ww_kokkos_c.hpp:275). */
+int ww_srce_last_error(void);
+
 /* ---------------------------------------------------------------- run-time flags */
 
 /* Replace ww_kokkos_flag / preset_status / strict / fallback_slot / fallback_add

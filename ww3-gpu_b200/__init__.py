@@ -42,6 +42,9 @@ EXPORTS = (
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
     "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_ktp3_batch", "ww_ktp3_batch_va",
     "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va", "ww_snl1_noalloc",
+    "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_sds4", "ww_sin4",
+    "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
+    "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -83,6 +86,33 @@ def lib():
         L.ww_snl1_device.restype = None
         L.ww_snl1_noalloc.argtypes = [_I, _I, _P, _P, _P, _P, _P]
         L.ww_snl1_noalloc.restype = None
+        L.ww_st4_init.argtypes = [_I, _P, _I, _P, _I]
+        L.ww_st4_init.restype = _I
+        L.ww_st4_set_real.argtypes = [_I, _I, _P, _I, _P, _P]
+        L.ww_st4_set_real.restype = _I
+        L.ww_st4_set_int.argtypes = [_I, _I, _P, _I, _P, _P]
+        L.ww_st4_set_int.restype = _I
+        L.ww_st4_commit.argtypes = [_I]
+        L.ww_st4_commit.restype = _I
+        L.ww_sds4.argtypes = [_I, _I] + [_P] * 8 + [_I, _I] + [_P] * 4
+        L.ww_sds4.restype = None
+        L.ww_sin4.argtypes = [_I, _I] + [_P] * 17
+        L.ww_sin4.restype = None
+        L.ww_spr4.argtypes = [_I, _I] + [_P] * 20
+        L.ww_spr4.restype = None
+        L.ww_st4_enabled.argtypes = [_I]
+        L.ww_st4_enabled.restype = _I
+        L.ww_st4_last_error.restype = _I
+        L.ww_srce_init.argtypes = [_I, _P, _I, _P, _I, _P, _P, _P, _P, _P]
+        L.ww_srce_init.restype = _I
+        L.ww_srce.argtypes = [_I, _I, _I, _I, _I, _P, _P, _P] + [_F] * 8 + [_P] * 26
+        L.ww_srce.restype = None
+        L.ww_srce_batch.argtypes = [_I, _I, _I, _I, _I, _F, _I] + [_P] * 9
+        L.ww_srce_batch.restype = None
+        L.ww_srce_batch_va.argtypes = [_I, _I, _I, _I, _I, _F, _P, _I, _I, _I] + [_P] * 9
+        L.ww_srce_batch_va.restype = None
+        L.ww_srce_enabled.restype = _I
+        L.ww_srce_last_error.restype = _I
         L.ww_snl1_enabled.restype = _I
         L.ww_snl1_last_error.restype = _I
         L.ww_snl1_select_kernel.argtypes = [_I, _I]

@@ -28,6 +28,8 @@ Runtime& runtime() {
 void release_snl1_contexts();  // abi_snl1.cpp
 void release_va_contexts();    // abi_va.cu
 void release_prop3_staging();  // abi_prop3.cpp
+void release_srce_contexts();  // abi_srce.cpp
+void release_st4_contexts();   // abi_st4.cpp
 
 namespace {
 
@@ -200,6 +202,8 @@ int ww_kokkos_init(int comm_f) {
 
 void ww_kokkos_finalize(void) {
   auto& rt = runtime();
+  wwb::release_srce_contexts();
+  wwb::release_st4_contexts();
   wwb::release_snl1_contexts();
   if (!rt.ready) return;
   wwb::release_va_contexts();

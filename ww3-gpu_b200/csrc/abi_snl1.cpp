@@ -200,6 +200,14 @@ int init_common(int igrid, const Snl1Config& cfg, const float* sig, Snl1Tables&&
 
 }  // namespace
 
+/// The DIA state of grid igrid for W3SRCE (device tables, row-shift form), or false.
+bool snl1_grid_dev(int igrid, Snl1Dev* out) {
+  auto it = contexts().find(igrid);
+  if (it == contexts().end() || !it->second->ready || !it->second->tab.rowshift) return false;
+  *out = it->second->dev;
+  return true;
+}
+
 void release_snl1_contexts() {
   auto& m = contexts();
   for (auto& kv : m) delete kv.second;

@@ -431,7 +431,7 @@ WWB_HD void sincosf_t(float y, float* sinp, float* cosp) {
     x = (FUSE & 2) ? fma_d(-(double)n, kHpi, x) : x - n * kHpi;
     const double s = (n & 3) == 0 || (n & 3) == 3 ? 1.0 : -1.0;
     sincosf_poly<FUSE>(x * s, x * x, (n & 2) != 0, n, sinp, cosp);
-  } else if (abstop12(y) < abstop12(__builtin_inff())) {
+  } else if (abstop12(y) < abstop12(asfloat(0x7f800000u))) {
     uint32_t xi = asuint(y);
     const int sign = xi >> 31;
     const unsigned base = (xi >> 26) & 15;
@@ -726,7 +726,7 @@ WWB_HD float log10f(float x) {
 /// about 1 ulp; not glibc's bits (W3SDB1 rounds the results it feeds to float).
 WWB_HD double exp_d(double x) {
   if (x != x) return x + x;
-  if (x > 709.78) return __builtin_inf();
+  if (x > 709.78) return asdouble(0x7ff0000000000000ULL);
   if (x < -745.2) return 0.0;
   const double inv = 64.0 / 0.6931471805599453;
   const double kd = x * inv;

@@ -108,7 +108,7 @@ inline SrceLayout srce_layout(const st4::Params& q, const Snl1Dev& n) {
 // ---------------------------------------------------------------------------- the DIA, one point
 /// W3SNL1 for one point in the row-shift form (the arithmetic of snl1_rowshift_kernel):
 /// a (NSPEC), cg (NK) in; s, d (NSPEC) out; scratch dia_scratch(p) floats.
-WWB_PD void dia_point(const Cta& cta, const Snl1Dev& p, const float* a, const float* cg,
+WWB_PN void dia_point(const Cta& cta, const Snl1Dev& p, const float* a, const float* cg,
                       float kdmean, float* s, float* d, float* scratch) {
   const int nth = p.nth, nfr = p.nfr, nfrhgh = p.nfrhgh, nfrchg = p.nfrchg;
   const int nspec = p.nspec, nspecx = p.nspecx, nk = p.nk;
@@ -255,11 +255,11 @@ WWB_PD void srce_sin4(const Cta& cta, const SrceCtx& x) {
 
 /// 1. Initialisation (:869-1179). spec holds the point's spectrum, wn1/cg1 its NK arrays; the
 /// shared scalars hold the INOUT packet values.
-WWB_PD void srce_init(const Cta& cta, const SrceCtx& x) {
+WWB_PN void srce_init(const Cta& cta, const SrceCtx& x) {
   const srce::Params& p = *x.p;
   const SrceLayout& L = *x.L;
   SrceSh& s = *x.sh;
-  const int nk = p.nk, nth = p.nth, nspec = p.nspec;
+  const int nk = p.nk, nspec = p.nspec;
   float* const spec = at(x, L.spec);
   PFOR(is, nspec) {
     at(x, L.vsin)[is] = at(x, L.vdin)[is] = at(x, L.vsnl)[is] = at(x, L.vdnl)[is] = 0.0f;
@@ -324,7 +324,7 @@ WWB_PD void srce_init(const Cta& cta, const SrceCtx& x) {
 }
 
 /// W3SLN1 (w3sln1md.F90:56-211) into VSLN.
-WWB_PD void srce_ln1(const Cta& cta, const SrceCtx& x) {
+WWB_PN void srce_ln1(const Cta& cta, const SrceCtx& x) {
   const srce::Params& p = *x.p;
   const SrceLayout& L = *x.L;
   SrceSh& s = *x.sh;
@@ -392,13 +392,14 @@ WWB_PD void cta_min_into(const Cta& cta, float v, float* dst, float* red) {
   cta.sync();
 #else
   (void)red;
+  (void)cta;
   *dst = mn(*dst, v);
 #endif
 }
 
 /// 2b. After the DIA (:1303-1997): W3SDS4, W3SDB1, W3SBT1, the time step, the update, the
 /// fluxes, W3SPR4, FHIGH, MLIM, SEED, the tail; then W3SIN4 (:2007) and the end test.
-WWB_PD void srce_step_c(const Cta& cta, const SrceCtx& x) {
+WWB_PN void srce_step_c(const Cta& cta, const SrceCtx& x) {
   const srce::Params& p = *x.p;
   const st4::Params& q = *x.q;
   const SrceLayout& L = *x.L;
@@ -545,7 +546,7 @@ WWB_PD void srce_step_c(const Cta& cta, const SrceCtx& x) {
   // :1484-1533, the MIN over IS.
   {
     const float afilt = s.afilt;
-    float loc = __builtin_inff();
+    float loc = dm::asfloat(0x7f800000u);
     PFOR(is, nspech) {
       const float vs = (((vsln[is] + vsin[is]) + vsnl[is]) + vsds[is]) + vsbt[is];
       const float vd = ((vdin[is] + vdnl[is]) + vdds[is]) + vdbt[is];
@@ -687,7 +688,7 @@ WWB_PD void srce_step_c(const Cta& cta, const SrceCtx& x) {
 }
 
 /// 3. After the loop (:2050-2350), FLD2 excepted (ww_srce_init refuses it).
-WWB_PD void srce_finish(const Cta& cta, const SrceCtx& x) {
+WWB_PN void srce_finish(const Cta& cta, const SrceCtx& x) {
   const srce::Params& p = *x.p;
   const SrceLayout& L = *x.L;
   SrceSh& s = *x.sh;

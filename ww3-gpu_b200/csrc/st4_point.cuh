@@ -26,8 +26,10 @@
 
 #if defined(__CUDACC__)
 #define WWB_PD __host__ __device__ __forceinline__
+#define WWB_PN __host__ __device__ __noinline__  // the large routines: called, not inlined
 #else
 #define WWB_PD inline
+#define WWB_PN inline
 #endif
 
 namespace wwb {
@@ -126,7 +128,7 @@ WWB_PD int sin4_work(const st4::Params& p) { return 3 * p.nspec; }
 /// W3SIN4 (w3src4md.F90:423-1003) for one point. a (NSPEC), cg (NK), kk(ik) = K(1+(IK-1)NTH) is
 /// kk[(ik-1)*kstride]; s, d (NSPEC) out; llws (NSPEC) out; tauwx..tauwny in/out (only thread
 /// role 0 writes them, read them after the call's final sync). eb (NK) is work.
-WWB_PD void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
+WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
                  const float* cg, const float* kk, int kstride, float u, float ustar, float drat,
                  float as, float usdir, float z0, float* tauwx, float* tauwy, float* tauwnx,
                  float* tauwny, float* s, float* d, int* llws, float* dstab, float* eb,
@@ -456,7 +458,7 @@ WWB_PD void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
 
 // ================================================================================ CALC_USTAR
 /// CALC_USTAR (w3src4md.F90:1849-2011), serial. MIN/MAX as (b < a) ? b : a (b > a) ? b : a.
-WWB_PD void calc_ustar(const st4::Params& p, const Fields& f, float windspeed, float tauw,
+WWB_PN void calc_ustar(const st4::Params& p, const Fields& f, float windspeed, float tauw,
                        float* ustar_io, float* z0, float* charn) {
   auto fmin2 = [](float a, float b) { return (b < a) ? b : a; };
   auto fmax2 = [](float a, float b) { return (b > a) ? b : a; };
@@ -540,7 +542,7 @@ struct Spr4Out {
 /// W3SPR4 (w3src4md.F90:142-384) for one point. a, llws (NSPEC); cg, wn (NK); work 4*NK floats
 /// plus 2 reals of shared scratch; o is read (ustar in) and written by role 0. The libmvec
 /// powers of :316 and :317 use scalar powf in every lane.
-WWB_PD void spr4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
+WWB_PN void spr4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
                  const float* cg, const float* wn, float u, float udir, float tauwx,
                  float tauwy, const int* llws, Spr4Out& o, float* work) {
   const int nk = p.nk, nth = p.nth;
@@ -666,7 +668,7 @@ struct Sds4Sh {
 
 /// W3SDS4 (w3src4md.F90:2043-2659) for one point. a, srhs, ddiag, brlambda (NSPEC); kk, cg (NK);
 /// whitecap (4) in/out. The libmvec loops (:2315, :2500, :2509) use scalar powf/expf per lane.
-WWB_PD void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
+WWB_PN void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
                  const float* kk, const float* cg, float ustar, float usdir, float depth,
                  float dair, float dlwmean, int flogrd57, int flogrd58, float* srhs,
                  float* ddiag, float* brlambda, float* whitecap, float* work, float* work2,
@@ -790,7 +792,7 @@ WWB_PD void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
         const int ik = ik0 + 1;
         if (ik >= ik1) {
           const int is0 = (ik - 1) * nth;
-          float lim = -__builtin_inff();
+          float lim = -dm::asfloat(0x7f800000u);
           int i = is0;
           bool found = false;
           for (; i < is0 + nth; ++i) {
@@ -801,7 +803,7 @@ WWB_PD void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
               break;
             }
           }
-          if (!found) lim = __builtin_nanf("");
+          if (!found) lim = dm::asfloat(0x7fc00000u);
           for (; i < is0 + nth; ++i)
             if (bth[i] > lim) lim = bth[i];
           bth0[ik - 1] = lim;

@@ -1,0 +1,72 @@
+// ww3-gpu_b200/csrc/st4_srce.cuh
+// Launchers of the ST4 (W3SIN4, W3SDS4, W3SPR4) and W3SRCE kernels (st4_srce_kernel.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "snl1_kernel.cuh"
+#include "srce_point.cuh"
+
+namespace wwb {
+
+/// One ST4 grid's scalars and device arrays, as the kernels read them (device-resident copy).
+struct St4Dev {
+  st4::Params p;
+  pt::Fields f;
+};
+
+/// Everything a W3SRCE launch reads besides the per-point arrays (device-resident copy).
+struct SrceDev {
+  srce::Params p;
+  pt::SrceGrid g;
+  st4::Params q;
+  pt::Fields f;
+  Snl1Dev n;
+  pt::SrceLayout L;
+};
+
+/// The flags of one W3SRCE time step.
+struct SrceStep {
+  int it, inflags24, flogrd57, flogrd58;
+  float dtg;
+};
+
+/// Threads of every ST4 / W3SRCE CTA (one CTA per point).
+constexpr int kSt4Block = 256;
+
+/// Bytes of dynamic shared memory of the W3SRCE kernel for these tables (the working set of
+/// one point); 0 when it exceeds the 227 KiB a CTA can have.
+size_t srce_smem_bytes(const pt::SrceLayout& L);
+
+/// W3SDS4 for npts points (arrays as ww_sds4 takes them, device pointers). d is the device copy.
+void launch_sds4(const St4Dev* d, const st4::Params& hp, int npts, const float* a, const float* k,
+                 const float* cg, const float* ustar, const float* usdir, const float* depth,
+                 const float* dair, const float* dlwmean, int f57, int f58, float* srhs,
+                 float* ddiag, float* brlambda, float* whitecap, cudaStream_t s);
+
+/// W3SIN4 for npts points (arrays as ww_sin4 takes them, device pointers).
+void launch_sin4(const St4Dev* d, const st4::Params& hp, int npts, const float* a,
+                 const float* cg, const float* k, const float* u, const float* ustar,
+                 const float* drat, const float* as, const float* usdir, const float* z0,
+                 float* tauwx, float* tauwy, float* tauwnx, float* tauwny, float* s, float* dd,
+                 int* llws, cudaStream_t st);
+
+/// W3SPR4 for npts points; out12 holds the 12 INOUT scalar arrays in ww_spr4's order (ustar,
+/// usdir, emean, fmean, fmean1, wnmean, amax, cd, z0, charn, fmeanws, dlwmean), each npts.
+void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* a,
+                 const float* cg, const float* wn, const float* u, const float* udir,
+                 const float* tauwx, const float* tauwy, const int* llws, float* const* out12,
+                 cudaStream_t st);
+
+/// W3SRCE for npts points on a persistent grid whose CTAs take points from a work queue
+/// (counter, zeroed here), so points with many substeps do not hold up the rest. Point n's
+/// spectrum is spec + n * nspec, or, with jsea non-null, the resident VA column
+/// spec + jsea[n] * nspec. Per-point packets as ww_srce_batch takes them (device pointers).
+void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int npts,
+                 float* spec, const int* jsea, const float* wn1, const float* cg1,
+                 const float* pin, float* psc, float* whitecap, float* taubbl, float* tauice,
+                 int* shave, int* counter, cudaStream_t st);
+
+}  // namespace wwb

@@ -1,0 +1,200 @@
+// ww3-gpu_b200/csrc/st4_srce_kernel.cu
+// The ST4 source terms and W3SRCE on sm_100a: one CTA of 256 threads per sea point, the point's
+// working set in shared memory, the phases of st4_point.cuh / srce_point.cuh.
+//
+// W3SRCE runs on a persistent grid: each CTA takes the next point from a global counter as it
+// finishes one, so the uneven number of substeps per point (the dynamic integration stops when
+// the point's DTTOT reaches DTG) balances across the SMs instead of leaving a tail of idle CTAs.
+// The scalar state of a point sits in static shared memory, its spectra and work arrays in
+// dynamic shared memory (about 100 KiB at 36x36, two CTAs per SM).
+#include "st4_srce.cuh"
+
+#include "wwb_common.hpp"
+
+namespace wwb {
+namespace {
+
+__global__ void __launch_bounds__(kSt4Block) sds4_kernel(
+    const St4Dev* __restrict__ d, int npts, const float* a, const float* k, const float* cg,
+    const float* ustar, const float* usdir, const float* depth, const float* dair,
+    const float* dlwmean, int f57, int f58, float* srhs, float* ddiag, float* brlambda,
+    float* whitecap) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ pt::Sds4Sh sh;
+  const st4::Params& p = d->p;
+  const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  float* const w = smem;
+  float* const w2 = w + ((pt::sds4_work_reals(p) + 3) & ~3);
+  int* const iw = reinterpret_cast<int*>(w2 + pt::sds4_work2_reals(p));
+  for (int n = blockIdx.x; n < npts; n += gridDim.x) {
+    const size_t os = static_cast<size_t>(n) * p.nspec, ok = static_cast<size_t>(n) * p.nk;
+    pt::sds4(cta, p, d->f, a + os, k + ok, cg + ok, ustar[n], usdir[n], depth[n], dair[n],
+             dlwmean[n], f57, f58, srhs + os, ddiag + os, brlambda + os,
+             whitecap + 4 * static_cast<size_t>(n), w, w2, iw, sh);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kSt4Block) sin4_kernel(
+    const St4Dev* __restrict__ d, int npts, const float* a, const float* cg, const float* k,
+    const float* u, const float* ustar, const float* drat, const float* as, const float* usdir,
+    const float* z0, float* tauwx, float* tauwy, float* tauwnx, float* tauwny, float* s,
+    float* dd, int* llws) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ pt::Sin4Sh sh;
+  const st4::Params& p = d->p;
+  const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  float* const dstab = smem;
+  float* const eb = dstab + 3 * p.nspec;
+  for (int n = blockIdx.x; n < npts; n += gridDim.x) {
+    const size_t os = static_cast<size_t>(n) * p.nspec, ok = static_cast<size_t>(n) * p.nk;
+    pt::sin4(cta, p, d->f, a + os, cg + ok, k + os, p.nth, u[n], ustar[n], drat[n], as[n],
+             usdir[n], z0[n], tauwx + n, tauwy + n, tauwnx + n, tauwny + n, s + os, dd + os,
+             llws + os, dstab, eb, sh);
+    __syncthreads();
+  }
+}
+
+struct Spr4Ptrs {
+  float* o[12];
+};
+
+__global__ void __launch_bounds__(kSt4Block) spr4_kernel(
+    const St4Dev* __restrict__ d, int npts, const float* a, const float* cg, const float* wn,
+    const float* u, const float* udir, const float* tauwx, const float* tauwy, const int* llws,
+    Spr4Ptrs out) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ pt::Spr4Out o;
+  const st4::Params& p = d->p;
+  const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  for (int n = blockIdx.x; n < npts; n += gridDim.x) {
+    const size_t os = static_cast<size_t>(n) * p.nspec, ok = static_cast<size_t>(n) * p.nk;
+    if (threadIdx.x == 0) {
+      float* const f = &o.ustar;
+      for (int j = 0; j < 12; ++j) f[j] = out.o[j][n];
+    }
+    __syncthreads();
+    pt::spr4(cta, p, d->f, a + os, cg + ok, wn + ok, u[n], udir[n], tauwx[n], tauwy[n],
+             llws + os, o, smem);
+    if (threadIdx.x == 0) {
+      const float* const f = &o.ustar;
+      for (int j = 0; j < 12; ++j) out.o[j][n] = f[j];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kSt4Block) srce_kernel(
+    const SrceDev* __restrict__ d, SrceStep step, int npts, float* spec, const int* jsea,
+    const float* wn1, const float* cg1, const float* pin, float* psc, float* whitecap,
+    float* taubbl, float* tauice, int* shave, int* counter) {
+  extern __shared__ __align__(16) float w[];
+  __shared__ pt::SrceSh sh;
+  __shared__ int cur;
+  const pt::SrceLayout& L = d->L;
+  const int ns = L.nspec, nk = L.nk;
+  const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  for (;;) {
+    if (threadIdx.x == 0) cur = atomicAdd(counter, 1);
+    __syncthreads();
+    const int n = cur;
+    if (n >= npts) break;
+    float* const sp =
+        spec + (jsea ? static_cast<size_t>(jsea[n]) : static_cast<size_t>(n)) * ns;
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) w[L.spec + i] = sp[i];
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+      w[L.wn1 + i] = wn1[static_cast<size_t>(n) * nk + i];
+      w[L.cg1 + i] = cg1[static_cast<size_t>(n) * nk + i];
+    }
+    if (threadIdx.x == 0)
+      pt::srce_psc_in(sh, psc + static_cast<size_t>(n) * srce::NPSC,
+                      whitecap + 4 * static_cast<size_t>(n), taubbl + 2 * static_cast<size_t>(n),
+                      tauice + 2 * static_cast<size_t>(n));
+    __syncthreads();
+    const pt::SrceCtx x{&d->p, &d->g, &d->q, &d->f, &d->n,
+                        pt::srce_in(step.it, step.inflags24, step.flogrd57, step.flogrd58,
+                                    step.dtg, pin + static_cast<size_t>(n) * srce::NPIN),
+                        w, &L, &sh};
+    pt::srce_point(cta, x);
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) sp[i] = w[L.spec + i];
+    if (threadIdx.x == 0)
+      pt::srce_psc_out(sh, psc + static_cast<size_t>(n) * srce::NPSC,
+                       whitecap + 4 * static_cast<size_t>(n), taubbl + 2 * static_cast<size_t>(n),
+                       tauice + 2 * static_cast<size_t>(n), shave + n);
+    __syncthreads();
+  }
+}
+
+/// Resident CTAs per SM of a kernel at this shared memory, at least 1.
+template <class K>
+int resident_grid(K k, size_t smem, int npts) {
+  WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+  int per_sm = 0;
+  WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kSt4Block, smem));
+  if (per_sm < 1) throw CudaError(cudaErrorInvalidConfiguration, "st4/srce occupancy");
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  return static_cast<int>(npts < resident ? npts : resident);
+}
+
+}  // namespace
+
+size_t srce_smem_bytes(const pt::SrceLayout& L) {
+  const size_t b = static_cast<size_t>(L.total) * sizeof(float) + 16;
+  return b + sizeof(pt::SrceSh) <= 227 * 1024 ? b : 0;
+}
+
+void launch_sds4(const St4Dev* d, const st4::Params& hp, int npts, const float* a, const float* k,
+                 const float* cg, const float* ustar, const float* usdir, const float* depth,
+                 const float* dair, const float* dlwmean, int f57, int f58, float* srhs,
+                 float* ddiag, float* brlambda, float* whitecap, cudaStream_t s) {
+  if (npts <= 0) return;
+  const size_t smem = sizeof(float) * (((pt::sds4_work_reals(hp) + 3) & ~3) +
+                                       pt::sds4_work2_reals(hp) + pt::sds4_work_ints(hp));
+  const int grid = resident_grid(sds4_kernel, smem, npts);
+  sds4_kernel<<<grid, kSt4Block, smem, s>>>(d, npts, a, k, cg, ustar, usdir, depth, dair, dlwmean,
+                                            f57, f58, srhs, ddiag, brlambda, whitecap);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void launch_sin4(const St4Dev* d, const st4::Params& hp, int npts, const float* a,
+                 const float* cg, const float* k, const float* u, const float* ustar,
+                 const float* drat, const float* as, const float* usdir, const float* z0,
+                 float* tauwx, float* tauwy, float* tauwnx, float* tauwny, float* s, float* dd,
+                 int* llws, cudaStream_t st) {
+  if (npts <= 0) return;
+  const size_t smem = sizeof(float) * (3 * static_cast<size_t>(hp.nspec) + hp.nk);
+  const int grid = resident_grid(sin4_kernel, smem, npts);
+  sin4_kernel<<<grid, kSt4Block, smem, st>>>(d, npts, a, cg, k, u, ustar, drat, as, usdir, z0,
+                                             tauwx, tauwy, tauwnx, tauwny, s, dd, llws);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* a,
+                 const float* cg, const float* wn, const float* u, const float* udir,
+                 const float* tauwx, const float* tauwy, const int* llws, float* const* out12,
+                 cudaStream_t st) {
+  if (npts <= 0) return;
+  Spr4Ptrs o;
+  for (int j = 0; j < 12; ++j) o.o[j] = out12[j];
+  const size_t smem = sizeof(float) * 4 * static_cast<size_t>(hp.nk);
+  const int grid = resident_grid(spr4_kernel, smem, npts);
+  spr4_kernel<<<grid, kSt4Block, smem, st>>>(d, npts, a, cg, wn, u, udir, tauwx, tauwy, llws, o);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int npts,
+                 float* spec, const int* jsea, const float* wn1, const float* cg1,
+                 const float* pin, float* psc, float* whitecap, float* taubbl, float* tauice,
+                 int* shave, int* counter, cudaStream_t st) {
+  if (npts <= 0) return;
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  const int grid = resident_grid(srce_kernel, smem, npts);
+  WWB_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), st));
+  srce_kernel<<<grid, kSt4Block, smem, st>>>(d, step, npts, spec, jsea, wn1, cg1, pin, psc,
+                                             whitecap, taubbl, tauice, shave, counter);
+  WWB_CHECK(cudaGetLastError());
+}
+
+}  // namespace wwb
