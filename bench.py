@@ -1,25 +1,30 @@
-"""Benchmark of the W3SNL1 (DIA) hot path on B200: sea-point·steps/s at 36x36 bins.
+"""Benchmark of WAVEWATCH III's per-sea-point hot path on B200: sea-point·steps/s at 36x36 bins.
 
-One "step" is one W3SNL1 evaluation (the DIA nonlinear transfer S and its diagonal D) over
-every sea point of the batch. Workload: 36 x 36 spectra (frequencies geometric from 0.0373 Hz,
-ratio 1.1; 10-degree directions), seeded JONSWAP sea states in deep water (d = 4000 m) with
-Hs ~ U(0.5, 8) m, fp ~ U(0.06, 0.2) Hz, gamma ~ U(1, 5), cos^2s spreading s ~ U(2, 20), DIA
-constants lambda 0.25, C 2.78e7, KDCONV 0.75, KDMIN 0.5, CS1-3 5.5/0.833/-1.25; 262,144 sea
-points per GPU so that a pass (4.1 GB of algorithmic traffic) is 33x the L2.
+Two workloads (--workload):
 
-  value  -- device-resident: inputs in HBM, ww_snl1_device launched on torch's stream, CUDA
-            events around exactly K steps; sea-point·steps/s summed over ranks.
-  e2e    -- the public host entry ww_snl1 (ww_kokkos_c.hpp:115 semantics) on page-locked host
-            buffers: host->device copy of A/CG/KDMEAN and device->host copy of S/D inside
-            every step.
-  roofline -- the kernel's algorithmic HBM bytes (15,700 B per point: A, CG, KDMEAN in; S, D
-            out) per launch over its CUDA-event duration, against MEASURED_PEAKS.json's HBM
-            copy bandwidth.
+* srce (default) -- the full plain source-term step W3SRCE with ST4 (W3SIN4 + W3SDS4 + W3SPR4),
+  the DIA (W3SNL1), W3SBT1 and W3SDB1 on 9520 sea points, 36 x 36 float32, DTG = 900 s with
+  dynamic substeps (uneven work per point). Spectra: seeded JONSWAP sea states (frequencies
+  geometric from 0.0373 Hz, ratio 1.1; 10-degree directions; Hs ~ U(0.5, 8) m, fp ~ U(0.06, 0.2)
+  Hz, gamma ~ U(1, 5), cos^2s spreading s ~ U(2, 20)), depths log-uniform in 10-4000 m,
+  U10 ~ U(3, 25) m/s from random directions. One step = one ww_srce_batch call over all points,
+  every step restarting from the same inputs.
+* dia -- W3SNL1 alone on 262,144 deep-water points per GPU (the DIA of the same spectra).
+
+  value  -- device-resident: inputs in HBM, the device entry (ww_srce_batch_device /
+            ww_snl1_device) launched on torch's stream, CUDA events around exactly K steps;
+            sea-point·steps/s summed over ranks.
+  e2e    -- the public host entry (ww_srce_batch / ww_snl1) on page-locked host buffers:
+            host->device copies of the step's inputs and device->host copies of its results
+            inside every step.
+  roofline -- the kernel's algorithmic HBM bytes per point (W3SRCE: 10,908 B = spectrum in and
+            out, WN1/CG1, the PIN/PSC packets, WHITECAP/TAUBBL/TAUICE, SHAVE; DIA: 15,700 B) per
+            launch over its CUDA-event duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
   cpu_baseline -- the reference's own C++ (oracle/_ref, compiled from its sources) on this
             host's cores on a bounded sample, rank 0 only.
 
 --impl reference runs that CPU reference alone, with the same metric and config.
-Multi-GPU: the DIA is independent per sea point, so each rank runs its own points (weak
+Multi-GPU: both workloads are independent per sea point, so each rank runs its own points (weak
 scaling) with no collective on the data path; ranks meet only at the timing barriers.
 """
 
@@ -44,20 +49,33 @@ METRIC = "sea-point·steps/s at 36×36 bins: plain DIA vs gated surrogate, same 
 UNIT = "sea-point*steps/s"
 WORKLOAD = ("W3SNL1 DIA 36x36 (config 0 spectra: deep-water JONSWAP, d=4000 m), "
             f"{NPTS_PER_GPU} sea points per GPU")
+SRCE_NPTS = 9520
+SRCE_BYTES_PER_POINT = 4 * (2 * NK * NTH + 2 * NK + 7 + 2 * 22 + 2 * 8 + 1)  # 10,908
+SRCE_WORKLOAD = ("W3SRCE + ST4 (W3SIN4, W3SDS4, W3SPR4) + DIA + W3SBT1 + W3SDB1, 36x36, "
+                 f"{SRCE_NPTS} sea points per GPU, DTG 900 s with dynamic substeps")
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
-    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--steps", type=int, default=None)
+    p.add_argument("--warmup", type=int, default=None)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--npts", type=int, default=NPTS_PER_GPU)
+    p.add_argument("--workload", choices=["srce", "dia"], default="srce")
+    p.add_argument("--npts", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band", "tile"], default="auto",
                    help="DIA kernel (ww_snl1_select_kernel); auto picks the band kernel")
-    return p.parse_args()
+    a = p.parse_args()
+    srce = a.workload == "srce"
+    if a.steps is None:
+        a.steps = 20 if srce else 200
+    if a.warmup is None:
+        a.warmup = 3 if srce else 5
+    if a.npts is None:
+        a.npts = SRCE_NPTS if srce else NPTS_PER_GPU
+    return a
 
 
 def dist_env():
@@ -102,7 +120,7 @@ def cpu_reference_rate(cfg, sig, g, seconds=10.0, max_points=4096):
     return n * calls / el, kind, cores, f"{calls} calls x {n} points of the workload"
 
 
-def run_reference_arm(args):
+def run_reference_dia(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
@@ -217,7 +235,7 @@ def ncu_traffic_per_point(kernel_name):
         return None
 
 
-def run_b200(args):
+def run_b200_dia(args):
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -332,11 +350,241 @@ def run_b200(args):
     return 0
 
 
+# ---------------------------------------------------------------------------- W3SRCE workload
+def srce_inputs(synth, npts, seed):
+    """The W3SRCE grid (ST4 analytic-tail configuration with this project's own ST4 tables,
+    the DIA constants of the workload) and npts seeded points."""
+    st = synth.st4_setup(NK, NTH, variant="analytic")
+    t = synth.st4_tables_own(st)
+    sr = synth.srce_setup(st)
+    cfg, sig = synth.dia_config(NK, NTH)
+    pts = synth.srce_points(npts, seed=seed, nk=NK, nth=NTH)
+    return st, t, sr, cfg, sig, pts
+
+
+def srce_config(args, world):
+    return {"workload": SRCE_WORKLOAD, "nk": NK, "nth": NTH, "npts_per_gpu": args.npts,
+            "global_points": args.npts * world, "dtg_s": 900.0,
+            "depth_m": "log-uniform 10-4000", "u10_ms": "U(3, 25)", "seed": 2026,
+            "st4": "saturation breaking with the cumulative term, analytic high-frequency tail",
+            "l2": ("every step restores its 55 MB of inputs and writes a 256 MB buffer (L2 flush) "
+                   "inside the timed region"),
+            "parallelism": f"points sharded over {world} GPU(s), no collective"}
+
+
+SRCE_ARRAYS = ("spec", "wn1", "cg1", "pin", "psc", "whitecap", "taubbl", "tauice")
+
+
+def cpu_reference_srce(st, t, sr, cfg, sig, pts, seconds=10.0, max_points=1024):
+    """Points/s of the reference's W3SRCE (its own C++ and C ABI, OpenMP over points) on this
+    host's cores, on a bounded sample of the workload."""
+    oracle = entry.load_oracle()
+    if not oracle.ref_available():
+        return None
+    n = min(max_points, pts["spec"].shape[0])
+    ref = oracle.RefSt4(st, t, igrid=7, srce=sr, dia=(cfg, sig))
+    L = ref.L
+
+    def call():
+        a = {k: pts[k][:n].copy() for k in SRCE_ARRAYS}
+        sh = __import__("numpy").zeros(n, "int32")
+        L.ww_srce_batch(7, 1, 0, 1, 1, 900.0, n, *[a[k].ctypes.data for k in ("spec", "wn1", "cg1",
+                        "pin", "psc", "whitecap", "taubbl", "tauice")], sh.ctypes.data)
+        if L.ww_srce_last_error() != 0:
+            raise RuntimeError("reference ww_srce_batch failed")
+
+    call()
+    t0 = time.perf_counter()
+    calls = 0
+    while True:
+        call()
+        calls += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or calls >= 50:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return n * calls / el, "reference", cores, f"{calls} ww_srce_batch calls x {n} points"
+
+
+def run_reference_srce(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    n = min(1024, args.npts)
+    st, t, sr, cfg, sig, pts = srce_inputs(synth, n, 2026)
+    oracle = entry.load_oracle()
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build "
+                          "(oracle/_ref) is absent"}), flush=True)
+        return 0
+    import numpy as np
+    ref = oracle.RefSt4(st, t, igrid=7, srce=sr, dia=(cfg, sig))
+    L = ref.L
+
+    def step():
+        a = {k: pts[k].copy() for k in SRCE_ARRAYS}
+        sh = np.zeros(n, np.int32)
+        L.ww_srce_batch(7, 1, 0, 1, 1, 900.0, n, *[a[k].ctypes.data for k in SRCE_ARRAYS],
+                        sh.ctypes.data)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    rate = n * args.steps / el
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cfgd = srce_config(args, 1)
+    cfgd["reference_sample_points_per_step"] = n
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": cfgd,
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{n} points of the workload per step, OpenMP over points"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200_srce(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
+    torch.cuda.set_device(local)
+    os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    pkg = entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    npts = args.npts
+    st, t, sr, cfg, sig, pts = srce_inputs(synth, npts, 2026 + rank)
+    grid = pkg.SrceGrid(1, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig, sr)
+    dev = torch.device("cuda", local)
+    d0 = {k: torch.from_numpy(pts[k]).to(dev) for k in SRCE_ARRAYS}
+    d = {k: v.clone() for k, v in d0.items()}
+    shave = torch.zeros(npts, dtype=torch.int32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    def step(ev=None):
+        for k in SRCE_ARRAYS:
+            if k not in ("wn1", "cg1", "pin"):
+                d[k].copy_(d0[k])
+        flush.zero_()
+        if ev is not None:
+            ev[0].record(stream)
+        grid.batch_device(npts, d["spec"], d["wn1"], d["cg1"], d["pin"], d["psc"],
+                          d["whitecap"], d["taubbl"], d["tauice"], shave, handle)
+        if ev is not None:
+            ev[1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    kev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        barrier()
+        t_start.record(stream)
+        for i in range(args.steps):
+            step(kev[i])
+        t_end.record(stream)
+        barrier()
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end))
+    launch_ms = sum(e[0].elapsed_time(e[1]) for e in kev) / args.steps
+    value = npts * world * args.steps / (total_ms / 1e3)
+    out_dev = {k: d[k].cpu().numpy() for k in ("spec", "psc")}
+
+    # ---- end to end through the host entry ww_srce_batch, page-locked host buffers
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
+    h = {k: torch.from_numpy(pts[k].copy()).pin_memory() for k in SRCE_ARRAYS}
+    h_shave = torch.zeros(npts, dtype=torch.int32).pin_memory()
+
+    def host_step():
+        for k in ("spec", "psc", "whitecap", "taubbl", "tauice"):
+            h[k].copy_(torch.from_numpy(pts[k]))
+        grid.batch(npts, h["spec"], h["wn1"], h["cg1"], h["pin"], h["psc"], h["whitecap"],
+                   h["taubbl"], h["tauice"], h_shave)
+
+    host_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_step()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = npts * world * e2e_steps / e2e_s
+    same = bool(np.array_equal(h["spec"].numpy().view(np.int32), out_dev["spec"].view(np.int32))
+                and np.array_equal(h["psc"].numpy().view(np.int32),
+                                   out_dev["psc"].view(np.int32)))
+    per_pt_in = NK * NTH + 2 * NK + 7 + 22 + 4 + 2 + 2 + 1
+    per_pt_out = NK * NTH + 22 + 4 + 2 + 2 + 1
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = SRCE_BYTES_PER_POINT * npts / (launch_ms / 1e3) / 1e9
+    tpp = ncu_traffic_per_point("srce_kernel")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": srce_config(args, world),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * per_pt_in * npts,
+                "d2h_bytes_per_step": 4 * per_pt_out * npts, "steps": e2e_steps,
+                "host_entry": "ww_srce_batch", "matches_device_entry": same},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": (tpp * npts if tpp else None), "kernel": "srce_kernel",
+                     "launch_ms": launch_ms,
+                     "algorithmic_bytes_per_point": SRCE_BYTES_PER_POINT,
+                     "note": ("W3SRCE is bound by FP32 issue and its serial ordered sums, not by "
+                              "HBM; the fraction shows how far from the HBM ceiling it runs")},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_srce(st, t, sr, cfg, sig, pts)
+        if r is not None:
+            rate, kind, cores, sample = r
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                    "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
-        return run_reference_arm(args)
-    return run_b200(args)
+    if args.workload == "dia":
+        return run_reference_dia(args) if args.impl == "reference" else run_b200_dia(args)
+    return run_reference_srce(args) if args.impl == "reference" else run_b200_srce(args)
 
 
 if __name__ == "__main__":

@@ -306,6 +306,15 @@ void ww_srce_batch_va(int igrid, int it, int inflags24, int flogrd57, int flogrd
                       const float* wn1, const float* cg1, const float* pin, float* psc,
                       float* whitecap, float* taubbl, float* tauice, int* shave);
 
+/* B200 extension. ww_srce_batch on device-resident arrays (same shapes), launched on the CUDA
+ * stream `stream` without copies or synchronisation; status in ww_srce_last_error(), execution
+ * errors surface at the caller's next synchronisation. Calls of one grid on different streams
+ * must not overlap (they share the grid's work-queue counter). */
+void ww_srce_batch_device(int igrid, int it, int inflags24, int flogrd57, int flogrd58,
+                          float dtg, int npts, float* spec, const float* wn1, const float* cg1,
+                          const float* pin, float* psc, float* whitecap, float* taubbl,
+                          float* tauice, int* shave, void* stream);
+
 /* Replaces ww_srce_enabled (ww_kokkos_c.hpp:272): 1 if WW_KOKKOS_SRCE resolves to on. */
 int ww_srce_enabled(void);
 

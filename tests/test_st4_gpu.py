@@ -116,9 +116,10 @@ def test_srce_batch_va_and_single_point(pkg, oracle, synth, tables):
     wc, tb, ti = pts["whitecap"][k].copy(), pts["taubbl"][k].copy(), pts["tauice"][k].copy()
     sh = np.zeros(1, np.int32)
     pin = pts["pin"][k]
+    wn1k, cg1k = pts["wn1"][k].copy(), pts["cg1"][k].copy()  # kept alive across the call
     args = [sc.p(a) for a in sc_[:16]] + [sc.p(wc), sc.p(sc_[16]), sc.p(tb), sc.p(ti)] + \
         [sc.p(a) for a in sc_[17:22]] + [sc.p(sh)]
-    L.ww_srce(ig, 1, 0, 1, 1, sc.p(spec), sc.p(pts["wn1"][k].copy()), sc.p(pts["cg1"][k].copy()),
+    L.ww_srce(ig, 1, 0, 1, 1, sc.p(spec), sc.p(wn1k), sc.p(cg1k),
               float(pin[0]), float(pin[1]), float(pin[2]), float(pin[3]), float(pin[4]), 900.0,
               float(pin[5]), float(pin[6]), *args)
     assert L.ww_srce_last_error() == 0

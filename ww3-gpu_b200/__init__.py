@@ -45,6 +45,7 @@ EXPORTS = (
     "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_sds4", "ww_sin4",
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
+    "ww_srce_batch_device",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -112,6 +113,8 @@ def lib():
         L.ww_srce_batch_va.argtypes = [_I, _I, _I, _I, _I, _F, _P, _I, _I, _I] + [_P] * 9
         L.ww_srce_batch_va.restype = None
         L.ww_srce_enabled.restype = _I
+        L.ww_srce_batch_device.argtypes = [_I, _I, _I, _I, _I, _F, _I] + [_P] * 10
+        L.ww_srce_batch_device.restype = None
         L.ww_srce_last_error.restype = _I
         L.ww_snl1_enabled.restype = _I
         L.ww_snl1_last_error.restype = _I
@@ -267,6 +270,71 @@ class Snl1Grid:
 
 def flag(name):
     return lib().ww_kokkos_flag(name.encode())
+
+
+# ---------------------------------------------------------------- ST4 and W3SRCE
+def st4_register(igrid, rpar, ipar, regs):
+    """ww_st4_init + one ww_st4_set_real/int per (id, array, is_int, lbounds, extents) +
+    ww_st4_commit for grid igrid (the sequence W3IOGR / W3KOKKOSMD performs)."""
+    L = lib()
+    init()
+    rpar = np.ascontiguousarray(rpar, np.float32)
+    ipar = np.ascontiguousarray(ipar, np.int32)
+    rc = L.ww_st4_init(igrid, rpar.ctypes.data, rpar.size, ipar.ctypes.data, ipar.size)
+    if rc != OK:
+        raise WwError("ww_st4_init", rc)
+    for aid, arr, is_int, lb, ext in regs:
+        arr = np.ascontiguousarray(arr, np.int32 if is_int else np.float32)
+        lb = np.asarray(lb, np.int32)
+        ext = np.asarray(ext, np.int32)
+        f = L.ww_st4_set_int if is_int else L.ww_st4_set_real
+        rc = f(igrid, aid, arr.ctypes.data, len(ext), lb.ctypes.data, ext.ctypes.data)
+        if rc != OK:
+            raise WwError("ww_st4_set", rc)
+    rc = L.ww_st4_commit(igrid)
+    if rc != OK:
+        raise WwError("ww_st4_commit", rc)
+
+
+class SrceGrid:
+    """One grid's W3SRCE: ST4 registered (st4_register), the DIA (Snl1Grid) and ww_srce_init.
+    ``srce`` holds rpar, ipar, sig, dden, ecos, esin, mapwn."""
+
+    def __init__(self, igrid, st4_rpar, st4_ipar, regs, dia_cfg, dia_sig, srce):
+        self.L = lib()
+        self.igrid = igrid
+        st4_register(igrid, st4_rpar, st4_ipar, regs)
+        self.dia = Snl1Grid(dia_cfg, dia_sig, igrid=igrid)
+        a = {k: np.ascontiguousarray(srce[k]) for k in ("rpar", "ipar", "sig", "dden", "ecos",
+                                                          "esin", "mapwn")}
+        rc = self.L.ww_srce_init(igrid, a["rpar"].ctypes.data, a["rpar"].size,
+                                 a["ipar"].ctypes.data, a["ipar"].size, a["sig"].ctypes.data,
+                                 a["dden"].ctypes.data, a["ecos"].ctypes.data,
+                                 a["esin"].ctypes.data, a["mapwn"].ctypes.data)
+        if rc != OK:
+            raise WwError("ww_srce_init", rc)
+
+    def _check(self, who):
+        rc = self.L.ww_srce_last_error()
+        if rc != OK:
+            raise WwError(who, rc)
+
+    def batch(self, npts, spec, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave, it=1,
+              inflags24=0, flogrd57=1, flogrd58=1, dtg=900.0):
+        """ww_srce_batch on host buffers (numpy arrays or pinned tensors), updated in place."""
+        self.L.ww_srce_batch(self.igrid, it, inflags24, flogrd57, flogrd58, dtg, npts,
+                             _ptr(spec), _ptr(wn1), _ptr(cg1), _ptr(pin), _ptr(psc),
+                             _ptr(whitecap), _ptr(taubbl), _ptr(tauice), _ptr(shave))
+        self._check("ww_srce_batch")
+
+    def batch_device(self, npts, spec, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave,
+                     stream=0, it=1, inflags24=0, flogrd57=1, flogrd58=1, dtg=900.0):
+        """ww_srce_batch_device on device tensors, launched on CUDA stream handle ``stream``."""
+        self.L.ww_srce_batch_device(self.igrid, it, inflags24, flogrd57, flogrd58, dtg, npts,
+                                    _ptr(spec), _ptr(wn1), _ptr(cg1), _ptr(pin), _ptr(psc),
+                                    _ptr(whitecap), _ptr(taubbl), _ptr(tauice), _ptr(shave),
+                                    ctypes.c_void_p(stream))
+        self._check("ww_srce_batch_device")
 
 
 # ---------------------------------------------------------------- PR3/UQ

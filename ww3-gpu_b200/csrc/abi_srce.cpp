@@ -301,6 +301,33 @@ void ww_srce(int igrid, int it, int inflags24, int flogrd57, int flogrd58, float
   }
 }
 
+void ww_srce_batch_device(int igrid, int it, int inflags24, int flogrd57, int flogrd58,
+                          float dtg, int npts, float* spec, const float* wn1, const float* cg1,
+                          const float* pin, float* psc, float* whitecap, float* taubbl,
+                          float* tauice, int* shave, void* stream) {
+  try {
+    GridCtx* g = find(igrid, "ww_srce_batch_device");
+    if (g == nullptr) return;
+    if (npts < 0 || (npts > 0 && (!spec || !wn1 || !cg1 || !pin || !psc || !whitecap ||
+                                  !taubbl || !tauice || !shave))) {
+      g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_srce_batch_device: npts < 0 or a null array");
+      return;
+    }
+    if (npts == 0) {
+      g_status.ok();
+      return;
+    }
+    SrceDev host{};
+    if (!prepare(igrid, *g, host, "ww_srce_batch_device")) return;
+    launch_srce(g->dev, host.L, SrceStep{it, inflags24, flogrd57, flogrd58, dtg}, npts, spec,
+                nullptr, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave, g->counter,
+                static_cast<cudaStream_t>(stream));
+    g_status.ok();
+  } catch (const std::exception& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
 int ww_srce_enabled(void) { return ww_kokkos_flag("WW_KOKKOS_SRCE") != 0 ? 1 : 0; }
 
 int ww_srce_last_error(void) { return g_status.get(); }

@@ -517,3 +517,76 @@ def srce_points(npts, seed=0, nk=36, nth=36, depth_range=(10.0, 4000.0)):
     return {"spec": g["a"], "wn1": k.astype(np.float32), "cg1": g["cg"], "pin": pin,
             "psc": psc, "whitecap": np.zeros((npts, 4), np.float32),
             "taubbl": np.zeros((npts, 2), np.float32), "tauice": np.zeros((npts, 2), np.float32)}
+
+
+def st4_tables_own(st):
+    """The ST4 tables of ``st`` that the analytic-tail configuration reads, built here (not by
+    the reference), for inputs of runs that have no reference at hand: SATINDICES/SATWEIGHTS
+    and CUMULW by INSIN4's formulas (w3src4md.F90:1134-1153, :1252-1282: weights
+    cos(th_i - th_j)**SSDSCOS over +-SDSNTH directions; the distance
+    sqrt(c^2 + c2^2 - 2 c c2 cos(dth)) * DSIP(ik2) / (c2 / 2) * DTH of deep-water phase speeds
+    c = g / sigma for IK2 <= IK - DIKCUMUL), DCKI/QBI/IKTAB zero (INSIN4 fills them only for
+    SSDSBCK > 0), no stress tables (SINTAILPAR(1) < 0.5). Same dict layout as the oracle's."""
+    ipar, r, R = st["ipar"], st["rpar"], st["R"]
+    nk, nth, nspec, mk, mth, mspec = [int(v) for v in ipar[:6]]
+    assert float(r[R["SINTAILPAR"]]) < 0.5, "own tables cover the analytic tail only"
+    dth = np.float32(r[R["DTH"]])
+    rade = np.float32(180.0) / np.float32(np.pi)
+    nsat = 2 * (mth // 2 - 1) + 1
+    sati = np.ones((mth, nsat), np.int32)   # (ith, row), written Fortran-ordered below
+    satw = np.zeros((mth, nsat), np.float32)
+    th = st["th"].astype(np.float64)
+    if float(r[R["SSDSDTH"]]) < 180.0:
+        sdsnth = min(int(np.floor(float(r[R["SSDSDTH"]]) / float(dth * rade) + 0.5)), nth // 2 - 1)
+        for ith in range(1, nth + 1):
+            for i_int in range(ith - sdsnth, ith + sdsnth + 1):
+                j = i_int + nth if i_int < 1 else (i_int - nth if i_int > nth else i_int)
+                row = i_int - (ith - sdsnth) + 1
+                sati[ith - 1, row - 1] = j
+                satw[ith - 1, row - 1] = np.float32(
+                    np.cos(th[ith - 1] - th[j - 1]) ** float(r[R["SSDSCOS"]]))
+    else:
+        satw[:] = 1.0
+    cumulw = np.zeros((mspec, mspec), np.float32)  # (is, is2): C order of the Fortran (is2, is)
+    if float(r[R["SSDSC"] + 2]) < 0:
+        xfr = float(r[R["XFR"]])
+        dik = int(np.floor(float(r[R["SSDSBRF1"]]) / (xfr - 1.0) + 0.5))
+        sig = st["sig"].astype(np.float64)
+        ec = st["ecos"].astype(np.float64)
+        for ik in range(1, nk + 1):
+            c = GRAV / sig[ik]
+            for ik2 in range(1, ik - dik + 1):
+                c2 = GRAV / sig[ik2]
+                d = np.abs(np.arange(nth)[:, None] - np.arange(nth)[None, :])  # |ith2 - ith|
+                v = np.sqrt(c * c + c2 * c2 - 2 * c * c2 * ec[d]) * float(st["dsip"][ik2]) / \
+                    (0.5 * c2) * float(dth)
+                cumulw[(ik - 1) * nth:ik * nth, (ik2 - 1) * nth:ik2 * nth] = v.T
+    return {"satweights": satw.reshape(-1), "satindices": sati.reshape(-1),
+            "iktab": np.zeros(mk * 2000, np.int32), "dcki": np.zeros(2000 * 1300, np.float32),
+            "qbi": np.zeros(2000 * 1300, np.float32), "cumulw": cumulw.reshape(-1),
+            "taut": None, "tauhft": None, "tauhft2": None, "rpar": r.copy(), "nsat": nsat}
+
+
+def st4_registrations(st, t):
+    """(id, array, is_int, lbounds, extents) of every ST4 array as ww_st4_set_real/int takes
+    them: ArrayId, rank and LBOUND of the reference's table (st4_arrays.hpp:41-81)."""
+    ipar = st["ipar"]
+    nk, nth, nspec, mk, mth, mspec = [int(v) for v in ipar[:6]]
+    nsat = t["nsat"]
+    regs = [
+        (0, st["sig"], False, [0], [nk + 2]), (1, st["sig2"], False, [1], [nspec]),
+        (2, st["dsip"], False, [0], [nk + 2]), (3, st["dden"], False, [1], [nk]),
+        (4, st["dden2"], False, [1], [nspec]), (5, st["esin"], False, [1], [nspec + nth]),
+        (6, st["ecos"], False, [1], [nspec + nth]), (7, st["th"], False, [1], [nth]),
+        (8, t["satweights"], False, [1, 1], [nsat, mth]),
+        (9, t["cumulw"], False, [1, 1], [mspec, mspec]),
+        (10, t["dcki"], False, [1, 1], [2000, 1300]), (11, t["qbi"], False, [1, 1], [2000, 1300]),
+        (12, t["satindices"], True, [1, 1], [nsat, mth]),
+        (13, t["iktab"], True, [1, 1], [mk, 2000]), (17, st["fwtable"], False, [0], [301]),
+    ]
+    if t.get("taut") is not None:
+        regs.append((14, t["taut"], False, [0, 0], [201, 201]))
+        regs.append((15, t["tauhft"], False, [0, 0], [101, 201]))
+    if t.get("tauhft2") is not None:
+        regs.append((16, t["tauhft2"], False, [0, 0, 0], [101, 201, 51]))
+    return regs
