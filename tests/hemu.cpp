@@ -109,7 +109,7 @@ void hemu_sin4(int npts, const float* a, const float* cg, const float* k, const 
                float* tauwny, float* s, float* d, int* llws) {
   (void)cd;
   const st4::Params& p = g_p;
-  std::vector<float> dstab(3 * p.nspec), eb(p.nk);
+  std::vector<float> dstab(3 * p.nspec), eb(pt::sin4_nk_work(p));
   static pt::Sin4Sh sh;
   const pt::Cta cta{0, 1};
   for (int n = 0; n < npts; ++n) {
@@ -126,14 +126,14 @@ void hemu_spr4(int npts, const float* a, const float* cg, const float* wn, const
                float* wnmean, float* amax, float* cd, float* z0, float* charn, float* fmeanws,
                float* dlwmean) {
   const st4::Params& p = g_p;
-  std::vector<float> w(4 * p.nk);
+  std::vector<float> w(pt::spr4_work_reals(p)), terms(pt::spr4_terms_reals(p));
   const pt::Cta cta{0, 1};
   for (int n = 0; n < npts; ++n) {
     const size_t os = static_cast<size_t>(n) * p.nspec, ok = static_cast<size_t>(n) * p.nk;
     pt::Spr4Out o{ustar[n], usdir[n], emean[n], fmean[n], fmean1[n], wnmean[n],
                   amax[n],  cd[n],    z0[n],    charn[n], fmeanws[n], dlwmean[n]};
     pt::spr4(cta, p, g_fields, a + os, cg + ok, wn + ok, u[n], udir[n], tauwx[n], tauwy[n],
-             llws + os, o, w.data());
+             llws + os, o, w.data(), terms.data());
     ustar[n] = o.ustar;
     usdir[n] = o.usdir;
     emean[n] = o.emean;

@@ -128,3 +128,15 @@ def test_inv_pio4_is_two_over_pi():
             idx = j - 3 + q
             want = (want << 8) | (b[idx] if idx >= 0 else 0)
         assert w == want, j
+
+
+def test_exp2_64_table():
+    """2^(j/64) of the double exp as double-double: hi rounded to double, lo the remainder."""
+    getcontext().prec = 60
+    vals = _decimal_table("WWB_EXP2_64_TAB")
+    assert len(vals) == 128
+    for j in range(64):
+        v = Decimal(2) ** (Decimal(j) / 64)
+        hi = float(v)
+        assert vals[2 * j] == hi, j
+        assert vals[2 * j + 1] == float(v - Decimal(hi)), j

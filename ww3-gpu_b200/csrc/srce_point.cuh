@@ -90,8 +90,8 @@ inline SrceLayout srce_layout(const st4::Params& q, const Snl1Dev& n) {
   L.cbeta = o; o += r4(nk);
   L.wnf = o; o += r4(nk);
   L.dirf = o; o += r4(nth);
-  L.sin4eb = o; o += r4(nk);
-  L.spr4w = o; o += r4(4 * nk);
+  L.sin4eb = o; o += r4(7 * nk);  // W3SIN4's NK work (sin4_nk_work)
+  L.spr4w = o; o += r4(5 * nk + 4);
   L.sds4w = o; o += r4(18 * nk);  // SDS4's NSPEC arrays live in the transient region
   L.sds4iw = o; o += r4(2 * nk);
   L.ebd = o; o += r4(2 * nk);  // NK doubles (8-byte aligned: o is a multiple of 4)
@@ -238,9 +238,10 @@ WWB_PD float* at(const SrceCtx& x, int off) { return x.w + off; }
 /// W3SPR4 with W3SRCE's arguments (:1080, :1119, :1878, :2012).
 WWB_PD void srce_spr4(const Cta& cta, const SrceCtx& x) {
   const SrceLayout& L = *x.L;
+  // The ELCS / ELSN terms go to the transient region's rows 5 and 6 (free at every call site).
   spr4(cta, *x.q, *x.f, at(x, L.spec), at(x, L.cg1), at(x, L.wn1), x.in.u10abs, x.in.u10dir,
        x.sh->tauwx, x.sh->tauwy, reinterpret_cast<const int*>(at(x, L.llws)), x.sh->r,
-       at(x, L.spr4w));
+       at(x, L.spr4w), at(x, L.trans) + 5 * ((L.nspec + 3) & ~3));
 }
 
 /// W3SIN4 with W3SRCE's arguments (:1100, :1239, :2007).

@@ -119,7 +119,11 @@ struct Sin4Sh {
   float ust, taux, tauy, cosu, sinu, ustp, usdirp;
   float ss[3][2], sn[3][2];
   float term[2][3][128];  ///< double-buffered per-direction stress terms (c, s, sign), NTH <= 128
+  float tail[6][kJtot];   ///< the analytic tail's terms that do not depend on USTR, per J
 };
+
+/// Reals of W3SIN4's NK work: EB and the six per-IK factors of the stress scan.
+WWB_PD int sin4_nk_work(const st4::Params& p) { return 7 * p.nk; }
 
 
 /// Reals of the DSTAB work W3SIN4 needs (3 x NSPEC).
@@ -134,12 +138,54 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
                  float* tauwny, float* s, float* d, int* llws, float* dstab, float* eb,
                  Sin4Sh& sh) {
   const int nk = p.nk, nth = p.nth, nspec = p.nspec;
+  // The per-IK factors of the stress scan that do not depend on the running stress (:721-738),
+  // formed in parallel: ZCN, CM, CONST2, CNST, SWELLCOEFV, SWELLCOEFT.
+  float* const zcn_k = eb + nk;
+  float* const cm_k = eb + 2 * nk;
+  float* const const2_k = eb + 3 * nk;
+  float* const cnst_k = eb + 4 * nk;
+  float* const swv_k = eb + 5 * nk;
+  float* const swt_k = eb + 6 * nk;
   // 1. Preparations (:600-675).
   PFOR(i, 3 * nspec) dstab[i] = 0.0f;
-  PFOR(ik, nk) {
-    float e = 0.0f;
-    for (int ith = 0; ith < nth; ++ith) e = e + a[ith + ik * nth];
-    eb[ik] = e;
+  {
+    const float const0 = (p.bbeta / kKappa2) * drat;
+    PFOR(ik0, nk) {
+      float e = 0.0f;
+      for (int ith = 0; ith < nth; ++ith) e = e + a[ith + ik0 * nth];
+      eb[ik0] = e;
+      const int ik = ik0 + 1;
+      const int is0 = 1 + (ik - 1) * nth;
+      const float kis = kk[(ik - 1) * kstride];
+      const float sig2is = f.sig2[is0 - 1];
+      cm_k[ik0] = kis / sig2is;
+      const2_k[ik0] = f.dden2[is0 - 1] / cg[ik - 1] * kGrav / (f.sig[ik] / kis * drat);
+      cnst_k[ik0] = sig2is * const0;
+      zcn_k[ik0] = dm::logf(kis * z0);
+      swv_k[ik0] = -(p.sswellf[4] * drat * 2.0f * kis * sqrt_f(kTwoNuAir * sig2is));
+      swt_k[ik0] = -(drat * p.sswellf[0] * 16.0f * (sig2is * sig2is) / kGrav);
+    }
+    if (p.sintailpar[0] < 0.5f) {
+      // The analytic tail's terms that depend on J only (:886-917).
+      const float signk = f.sig[nk];
+      const float zinf = dm::logf(signk * signk / kGrav);
+      const float dely = (kLogTpiOver005 - zinf) / static_cast<float>(kJtot);
+      PFOR(j0, kJtot) {
+        const float y = dm::expf(zinf + static_cast<float>(j0) * dely);
+        const float ykm = (y / kKm);
+        const float ykm2 = ykm * ykm;
+        const float tensk = 1.0f + ykm2;
+        sh.tail[0][j0] = y;
+        sh.tail[1][j0] = ykm;
+        sh.tail[2][j0] = sqrt_f(kGrav * tensk / y);
+        sh.tail[3][j0] = 0.5f * (3.0f * ykm2 + 1.0f) * sqrt_f(kGrav / (y * tensk));
+        if (p.sintailpar[2] > 0.0f) {
+          const float ykm1 = (ykm - 1.0f);
+          sh.tail[4][j0] = dm::expf(-0.25f * (ykm1 * ykm1));
+          sh.tail[5][j0] = dm::tanhf((y - 20.0f) / 5.0f);
+        }
+      }
+    }
   }
   cta.sync();
   if (cta.role(0)) {
@@ -242,15 +288,14 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
         usdirp = dm::atan2f(taupy, taupx);
         dm::sincosf(usdirp, &sinu, &cosu);
         const int is0 = 1 + (ik - 1) * nth;
-        const float kis = kk[(ik - 1) * kstride];
         const float sig2is = f.sig2[is0 - 1];
-        const float cm = kis / sig2is;
+        const float cm = cm_k[ik - 1];
         const float ucn = ustp * cm + p.zzalp;
-        const float const2 = f.dden2[is0 - 1] / cg[ik - 1] * kGrav / (f.sig[ik] / kis * drat);
-        const float cnst = sig2is * const0;
-        const float zcn = dm::logf(kis * z0);
-        const float swellcoefv = -(p.sswellf[4] * drat * 2.0f * kis * sqrt_f(kTwoNuAir * sig2is));
-        const float swellcoeft = -(drat * p.sswellf[0] * 16.0f * (sig2is * sig2is) / kGrav);
+        const float const2 = const2_k[ik - 1];
+        const float cnst = cnst_k[ik - 1];
+        const float zcn = zcn_k[ik - 1];
+        const float swellcoefv = swv_k[ik - 1];
+        const float swellcoeft = swt_k[ik - 1];
         for (int ith = cta.tid; ith < nth; ith += nscan) {
           const int is = ith + 1 + (ik - 1) * nth;
           const float ecos = f.ecos[is - 1], esin = f.esin[is - 1];
@@ -374,12 +419,8 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
       float tau1 = 0.0f;
       for (int j = 1; j <= kJtot; ++j) {
         const float w = (j == 1 || j == kJtot) ? 0.5f : 1.0f;
-        const float y = dm::expf(zinf + static_cast<float>(j - 1) * dely);
-        const float ykm = (y / kKm);
-        const float ykm2 = ykm * ykm;
-        const float tensk = 1.0f + ykm2;
-        const float cm = sqrt_f(kGrav * tensk / y);
-        const float cgtail = 0.5f * (3.0f * ykm2 + 1.0f) * sqrt_f(kGrav / (y * tensk));
+        const float cm = sh.tail[2][j - 1];
+        const float cgtail = sh.tail[3][j - 1];
         const float zx = ustr / cm + p.zzalp;
         const float zarg = min_r(kKappa / zx, 20.0f);
         const float zmu = min_r(kGrav * zz0 / (cm * cm) * dm::expf(zarg), 1.0f);
@@ -394,10 +435,9 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
           } else {
             alpham = 0.01f * (1.0f + 3.0f * dm::logf(ustr / cm));
           }
-          const float ykm1 = (ykm - 1.0f);
-          const float fm = dm::expf(-0.25f * (ykm1 * ykm1));
+          const float fm = sh.tail[4][j - 1];
           const float alphat = alpham * (kCmm / cm) * fm;
-          const float th = dm::tanhf((y - 20.0f) / 5.0f);
+          const float th = sh.tail[5][j - 1];
           levtail = levtail0 * 0.5f * (1.0f - th) + p.sintailpar[2] * 0.5f * (1.0f + th) * alphat;
         } else {
           levtail = levtail0;
@@ -539,18 +579,28 @@ struct Spr4Out {
   float ustar, usdir, emean, fmean, fmean1, wnmean, amax, cd, z0, charn, fmeanws, dlwmean;
 };
 
-/// W3SPR4 (w3src4md.F90:142-384) for one point. a, llws (NSPEC); cg, wn (NK); work 4*NK floats
-/// plus 2 reals of shared scratch; o is read (ustar in) and written by role 0. The libmvec
-/// powers of :316 and :317 use scalar powf in every lane.
+/// Reals of W3SPR4 work: EB, EB2, the two powers and SIGFAC (NK each) and three chain results;
+/// terms holds 2 x NSPEC more (the ELCS / ELSN terms).
+WWB_PD int spr4_work_reals(const st4::Params& p) { return 5 * p.nk + 4; }
+WWB_PD int spr4_terms_reals(const st4::Params& p) { return 2 * p.nspec; }
+
+/// W3SPR4 (w3src4md.F90:142-384) for one point. a, llws (NSPEC); cg, wn (NK); o is read (ustar
+/// in) and written by role 0. The libmvec powers of :316 and :317 use scalar powf in every lane.
+/// ELCS and ELSN are one running sum each over IK then ITH, AMAX one running MAX: their terms
+/// are formed in parallel, then each chain runs on its own thread in the reference's order.
 WWB_PN void spr4(const Cta& cta, const st4::Params& p, const Fields& f, const float* a,
                  const float* cg, const float* wn, float u, float udir, float tauwx,
-                 float tauwy, const int* llws, Spr4Out& o, float* work) {
-  const int nk = p.nk, nth = p.nth;
+                 float tauwy, const int* llws, Spr4Out& o, float* work, float* terms) {
+  const int nk = p.nk, nth = p.nth, nspec = p.nspec;
   float* const eb = work;
   float* const eb2 = work + nk;
   float* const pwsig = work + 2 * nk;
   float* const pwwn = work + 3 * nk;
-  // Per-IK direction sums (independent over IK) and the two powers.
+  float* const sigfac = work + 4 * nk;
+  float* const chains = work + 5 * nk;  // ELCS, ELSN, AMAX
+  float* const tc = terms;
+  float* const ts = terms + nspec;
+  // Per-IK direction sums (independent over IK), the two powers and SIGFAC.
   PFOR(ik0, nk) {
     const int ik = ik0 + 1;
     float ebk = 0.0f, eb2k = 0.0f;
@@ -564,24 +614,37 @@ WWB_PN void spr4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
     eb2[ik0] = eb2k;
     pwsig[ik0] = dm::powf(f.sig[ik], 2.0f * p.wwnmeanptail);
     pwwn[ik0] = dm::powf(wn[ik0], p.wwnmeanp);
+    sigfac[ik0] = dm::powf(f.sig[ik], p.ssdsc[11]) * f.dden[ik - 1] / cg[ik - 1];
+  }
+  cta.sync();
+  PFOR(is0, nspec) {
+    const float aa = a[is0];
+    const float sf = sigfac[is0 / nth];
+    tc[is0] = aa * f.ecos[is0] * sf;
+    ts[is0] = aa * f.esin[is0] * sf;
+  }
+  cta.sync();
+  if (cta.role(0)) {
+    float v = 0.0f;
+    for (int i = 0; i < nspec; ++i) v = v + tc[i];
+    chains[0] = v;
+  }
+  if (cta.role(1)) {
+    float v = 0.0f;
+    for (int i = 0; i < nspec; ++i) v = v + ts[i];
+    chains[1] = v;
+  }
+  if (cta.role(2)) {
+    float v = 0.0f;
+    for (int i = 0; i < nspec; ++i) v = max_r(v, a[i]);
+    chains[2] = v;
   }
   cta.sync();
   if (cta.role(0)) {
     const float eps = 1.E-7f;
     float ustar = max_r(0.0001f, o.ustar);
-    // ELCS, ELSN: one running sum each over IK then ITH; AMAX over all bins.
-    float elcs = 0.0f, elsn = 0.0f, amax = 0.0f;
-    for (int ik = 1; ik <= nk; ++ik) {
-      const float sigfac = dm::powf(f.sig[ik], p.ssdsc[11]) * f.dden[ik - 1] / cg[ik - 1];
-      for (int ith = 1; ith <= nth; ++ith) {
-        const int is = ith + (ik - 1) * nth;
-        const float aa = a[(ik - 1) * nth + ith - 1];
-        elcs = elcs + aa * f.ecos[is - 1] * sigfac;
-        elsn = elsn + aa * f.esin[is - 1] * sigfac;
-        amax = max_r(amax, aa);
-      }
-    }
-    const float dlwmean = dm::atan2f(elsn, elcs);
+    const float dlwmean = dm::atan2f(chains[1], chains[0]);
+    const float amax = chains[2];
     float emean = 0.0f, fmean = 0.0f, fmean1 = 0.0f, wnmean = 0.0f, emeanws = 0.0f,
           fmeanws = 0.0f;
     for (int ik = 1; ik <= nk; ++ik) {
@@ -1048,13 +1111,16 @@ WWB_PN void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
     cta.sync();
   }
 
-  // Whitecap parameters (:2581-2650); an early return leaves WHITECAP as it came.
+  // Whitecap parameters (:2581-2650); an early return leaves WHITECAP as it came. COEF4, COEF5
+  // and the mean foam thickness of each IK are independent over IK (parallel); the sums over IK
+  // (the coverage recurrence, the air entrainment and the foam sum) stay serial in IK order.
   if (flogrd57 || flogrd58) {
-    if (cta.role(0)) {
-      float wc0 = zero, wc1 = zero, wc3 = zero;
-      const int fl = ffloor(p.aaircmin);
-      const int ikc = fl < nk ? fl : nk;
-      for (int ik = 1; ik <= ikc; ++ik) {
+    const int fl = ffloor(p.aaircmin);
+    const int ikc = fl < nk ? fl : nk;
+    float* const mftk = s1;  // S1 is free after the breaking cases: MFT of each IK
+    PFOR(ik0, nk) {
+      const int ik = ik0 + 1;
+      if (ik <= ikc) {
         const float c = f.sig[ik] / kk[ik - 1];
         const int is0 = (ik - 1) * nth;
         float v = zero;
@@ -1066,8 +1132,29 @@ WWB_PN void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
         for (int i = is0; i < is0 + nth; ++i) w = w + (brlambda[i] * (-ssdsc[1])) * pw;
         coef5[ik - 1] = ((((c * c) * c) * w) * p.aairgb / kGrav) * f.dden[ik - 1] /
                         (f.sig[ik] * cg[ik - 1]);
+      } else {
+        coef4[ik - 1] = zero;
+        coef5[ik - 1] = zero;
       }
-      for (int ik = ikc + 1; ik <= nk; ++ik) coef4[ik - 1] = coef5[ik - 1] = zero;
+      if (flogrd58 && ik >= ik1) {
+        const float tstr = kTstrFac / f.sig[ik];
+        const float tmax = kTmaxFac / f.sig[ik];
+        const float dt = tmax / 50.0f;
+        float mft = zero;
+        for (int it = 1; it <= 50; ++it) {
+          const float t = static_cast<float>(it) * dt;
+          if (t < tstr) {
+            mft = mft + ((0.4f / (kk[ik - 1] * tstr)) * t) * dt;
+          } else {
+            mft = mft + ((0.4f / kk[ik - 1]) * dm::expf(-((t - tstr) / 3.8f))) * dt;
+          }
+        }
+        mftk[ik - 1] = mft / tmax;
+      }
+    }
+    cta.sync();
+    if (cta.role(0)) {
+      float wc0 = zero, wc1 = zero, wc3 = zero;
       if (flogrd57) {
         for (int ik = ik1; ik <= ikc; ++ik) {
           wc0 = wc0 + coef4[ik - 1] * (one - wc0);
@@ -1075,22 +1162,7 @@ WWB_PN void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
         }
       }
       if (flogrd58) {
-        for (int ik = ik1; ik <= nk; ++ik) {
-          const float tstr = kTstrFac / f.sig[ik];
-          const float tmax = kTmaxFac / f.sig[ik];
-          const float dt = tmax / 50.0f;
-          float mft = zero;
-          for (int it = 1; it <= 50; ++it) {
-            const float t = static_cast<float>(it) * dt;
-            if (t < tstr) {
-              mft = mft + ((0.4f / (kk[ik - 1] * tstr)) * t) * dt;
-            } else {
-              mft = mft + ((0.4f / kk[ik - 1]) * dm::expf(-((t - tstr) / 3.8f))) * dt;
-            }
-          }
-          mft = mft / tmax;
-          wc1 = wc1 + coef4[ik - 1] * mft;
-        }
+        for (int ik = ik1; ik <= nk; ++ik) wc1 = wc1 + coef4[ik - 1] * mftk[ik - 1];
       }
       whitecap[0] = wc0;
       whitecap[1] = wc1;

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kSt4Block) spr4_kernel(
     }
     __syncthreads();
     pt::spr4(cta, p, d->f, a + os, cg + ok, wn + ok, u[n], udir[n], tauwx[n], tauwy[n],
-             llws + os, o, smem);
+             llws + os, o, smem, smem + ((pt::spr4_work_reals(p) + 3) & ~3));
     if (threadIdx.x == 0) {
       const float* const f = &o.ustar;
       for (int j = 0; j < 12; ++j) out.o[j][n] = f[j];
@@ -163,7 +163,7 @@ void launch_sin4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
                  float* tauwx, float* tauwy, float* tauwnx, float* tauwny, float* s, float* dd,
                  int* llws, cudaStream_t st) {
   if (npts <= 0) return;
-  const size_t smem = sizeof(float) * (3 * static_cast<size_t>(hp.nspec) + hp.nk);
+  const size_t smem = sizeof(float) * (3 * static_cast<size_t>(hp.nspec) + pt::sin4_nk_work(hp));
   const int grid = resident_grid(sin4_kernel, smem, npts);
   sin4_kernel<<<grid, kSt4Block, smem, st>>>(d, npts, a, cg, k, u, ustar, drat, as, usdir, z0,
                                              tauwx, tauwy, tauwnx, tauwny, s, dd, llws);
@@ -177,7 +177,8 @@ void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
   if (npts <= 0) return;
   Spr4Ptrs o;
   for (int j = 0; j < 12; ++j) o.o[j] = out12[j];
-  const size_t smem = sizeof(float) * 4 * static_cast<size_t>(hp.nk);
+  const size_t smem = sizeof(float) * (((pt::spr4_work_reals(hp) + 3) & ~3) +
+                                       static_cast<size_t>(pt::spr4_terms_reals(hp)));
   const int grid = resident_grid(spr4_kernel, smem, npts);
   spr4_kernel<<<grid, kSt4Block, smem, st>>>(d, npts, a, cg, wn, u, udir, tauwx, tauwy, llws, o);
   WWB_CHECK(cudaGetLastError());
