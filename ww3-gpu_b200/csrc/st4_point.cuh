@@ -263,7 +263,7 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
   //    the terms of its directions, and then adds all directions' terms in ITH order.
   const int nscan = nth < cta.nthr ? nth : cta.nthr;
   const bool scan = cta.tid < nscan;
-  const float const0 = sh.const0, uorb = sh.uorb, pturb = sh.pturb, pvisc = sh.pvisc,
+  const float uorb = sh.uorb, pturb = sh.pturb, pvisc = sh.pvisc,
               fw = sh.fw, fu = sh.fu, fud = sh.fud, ustarsigma = sh.ustarsigma;
   float ust = ustar, taux = 0.0f, tauy = 0.0f, cosu = 0.0f, sinu = 0.0f, ustp = 0.0f,
         usdirp = 0.0f;
