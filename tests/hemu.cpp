@@ -20,6 +20,7 @@ st4::GridReg g_grid;
 st4::ModuleReg g_mod;
 std::vector<float> g_satw_t;
 std::vector<int> g_sati_t;
+std::vector<float> g_cumulw_t;
 pt::Fields g_fields{};
 st4::Params g_p{};
 bool g_ready = false;
@@ -72,12 +73,13 @@ int hemu_st4_commit(void) {
     return 6;
   }
   st4::transpose_sat(g_grid, g_satw_t, g_sati_t);
+  st4::transpose_cumulw(g_grid, g_cumulw_t);
   const auto& a = g_grid.a;
   const auto& m = g_mod.a;
   st4::FieldPtrs q{fp(a[st4::A_SIG]), fp(a[st4::A_SIG2]), fp(a[st4::A_DSIP]),
                    fp(a[st4::A_DDEN]), fp(a[st4::A_DDEN2]), fp(a[st4::A_ESIN]),
                    fp(a[st4::A_ECOS]), fp(a[st4::A_TH]), g_satw_t.data(),
-                   fp(a[st4::A_CUMULW]), fp(a[st4::A_DCKI]), fp(a[st4::A_QBI]),
+                   g_cumulw_t.data(), fp(a[st4::A_DCKI]), fp(a[st4::A_QBI]),
                    fp(m[st4::A_TAUT]), fp(m[st4::A_TAUHFT]), fp(m[st4::A_TAUHFT2]),
                    fp(m[st4::A_FWTABLE]), g_sati_t.data(), ip(a[st4::A_IKTAB])};
   g_fields = st4::make_fields(g_grid, q);

@@ -57,6 +57,7 @@ struct GridCtx {
   DevVec<int> i[st4::NARRAYS];
   DevVec<float> satw_t;
   DevVec<int> sati_t;
+  DevVec<float> cumulw_t;
   St4Dev host{};                    ///< the kernel parameters (module state of the commit)
   St4Dev* dev = nullptr;            ///< their device copy
   ~GridCtx() {
@@ -86,7 +87,7 @@ void refresh(GridCtx& g) {
   st4::FieldPtrs q{g.f[st4::A_SIG].ptr,   g.f[st4::A_SIG2].ptr,  g.f[st4::A_DSIP].ptr,
                    g.f[st4::A_DDEN].ptr,  g.f[st4::A_DDEN2].ptr, g.f[st4::A_ESIN].ptr,
                    g.f[st4::A_ECOS].ptr,  g.f[st4::A_TH].ptr,    g.satw_t.ptr,
-                   g.f[st4::A_CUMULW].ptr, g.f[st4::A_DCKI].ptr, g.f[st4::A_QBI].ptr,
+                   g.cumulw_t.ptr, g.f[st4::A_DCKI].ptr, g.f[st4::A_QBI].ptr,
                    m.f[st4::A_TAUT].ptr,  m.f[st4::A_TAUHFT].ptr, m.f[st4::A_TAUHFT2].ptr,
                    m.f[st4::A_FWTABLE].ptr, g.sati_t.ptr,         g.i[st4::A_IKTAB].ptr};
   (void)a;
@@ -260,6 +261,10 @@ int ww_st4_commit(int igrid) {
     st4::transpose_sat(g.reg, wt, itt);
     g.satw_t.upload(wt);
     g.sati_t.upload(itt);
+    std::vector<float> ct;
+    st4::transpose_cumulw(g.reg, ct);
+    g.cumulw_t.upload(ct);
+    g.f[st4::A_CUMULW].upload({});  // only the transposed copy is read
     refresh(g);
     g.ready = true;
     g_status.ok();

@@ -88,7 +88,7 @@ struct Fields {
   const float* satw_t;  ///< SATWEIGHTS transposed: (ith-1) + (j-1)*sat_ld
   const int* sati_t;
   int nsat, sat_ld;
-  const float* cumulw;  ///< CUMULW(i,j) = cumulw[(i-1) + (j-1)*cumulw_ld]
+  const float* cumulw;  ///< CUMULW transposed: CUMULW(i,j) = cumulw[(j-1) + (i-1)*cumulw_ld]
   int cumulw_ld;
   const float *dcki, *qbi;  ///< (NKHS, NKD)
   const int* iktab;         ///< IKTAB(ik,id) = iktab[(ik-1) + (id-1)*iktab_ld]
@@ -1095,8 +1095,11 @@ WWB_PN void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
             if (bth0[ik2 - 1] > p.ssdsbr) {
               const int is2 = (ik2 - 1) * nth;
               float v = zero;
-              const float* const col = f.cumulw + static_cast<size_t>(is - 1) * f.cumulw_ld;
-              for (int j = 1; j <= nth; ++j) v = v + col[is2 + j - 1] * brlambda[is2 + j - 1];
+              // CUMULW(IS2+J, IS) for the threads' consecutive IS are consecutive in the
+              // transposed copy: one coalesced row per J.
+              const float* const row = f.cumulw + static_cast<size_t>(is2) * f.cumulw_ld + (is - 1);
+              for (int j = 1; j <= nth; ++j)
+                v = v + row[static_cast<size_t>(j - 1) * f.cumulw_ld] * brlambda[is2 + j - 1];
               renewalfreq = renewalfreq + v;
             }
           }

@@ -140,10 +140,20 @@ inline void transpose_sat(const GridReg& g, std::vector<float>& w_t, std::vector
     }
 }
 
+/// CUMULW transposed (MSPEC x MSPEC, square): W3SDS4's cumulative term walks rows IS2 for
+/// consecutive IS, which the transpose makes contiguous.
+inline void transpose_cumulw(const GridReg& g, std::vector<float>& t) {
+  const Reg& c = g.a[A_CUMULW];
+  const size_t n = c.ext[0];
+  t.assign(n * n, 0.0f);
+  for (size_t j = 0; j < n; ++j)
+    for (size_t i = 0; i < n; ++i) t[j + i * n] = c.f[i + j * n];
+}
+
 /// Fields over host-resident copies (the CPU build of the kernels) or over device copies whose
 /// pointers the caller fills in the same order (abi_st4.cpp).
 struct FieldPtrs {
-  const float *sig, *sig2, *dsip, *dden, *dden2, *esin, *ecos, *th, *satw_t, *cumulw, *dcki,
+  const float *sig, *sig2, *dsip, *dden, *dden2, *esin, *ecos, *th, *satw_t, *cumulw_t, *dcki,
       *qbi, *taut, *tauhft, *tauhft2, *fwtable;
   const int *sati_t, *iktab;
 };
@@ -162,7 +172,7 @@ inline pt::Fields make_fields(const GridReg& g, const FieldPtrs& q) {
   f.sati_t = q.sati_t;
   f.nsat = g.a[A_SATWEIGHTS].ext[0];
   f.sat_ld = g.a[A_SATWEIGHTS].ext[1];
-  f.cumulw = q.cumulw;
+  f.cumulw = q.cumulw_t;
   f.cumulw_ld = g.a[A_CUMULW].ext[0];
   f.dcki = q.dcki;
   f.qbi = q.qbi;
