@@ -31,6 +31,8 @@
 // The reference (ww3-gpu kokkos/src/ww_kokkos/libm_device.hpp:33-52) calls expf in W3SNL1's
 // CONS (snl1_team.hpp:386-390), the ST4 source terms and W3SRCE call the rest
 // (st4_sin4.hpp, st4_sds4.hpp, st4_spr4.hpp, srce_kernel.hpp, srce_db1.hpp).
+// The device copies of the tables are global-memory arrays read through the read-only cache:
+// lanes of a warp index them with different values, which constant memory would serialize.
 #pragma once
 
 #include <stdint.h>
@@ -57,13 +59,13 @@ namespace dm {
    0x3fef5818dcfba487ULL, 0x3fef7c97337b9b5fULL, 0x3fefa4afa2a490daULL, 0x3fefd0765b6e4540ULL}
 
 #if defined(__CUDACC__)
-__device__ __constant__ static const uint64_t kExp2fTabDev[32] = WWB_EXP2F_TAB;
+__device__ static const uint64_t kExp2fTabDev[32] = WWB_EXP2F_TAB;
 #endif
 static const uint64_t kExp2fTabHost[32] = WWB_EXP2F_TAB;
 
 WWB_HD uint64_t exp2f_tab(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return kExp2fTabDev[i];
+  return __ldg(reinterpret_cast<const unsigned long long*>(&kExp2fTabDev[i]));
 #else
   return kExp2fTabHost[i];
 #endif
@@ -177,9 +179,9 @@ WWB_HD float fma_f(float a, float b, float c) {
    0x1.e840b4ac4e4d2p-3, 0x1.40645f0c6651cp-2, 0x1.88e9c2c1b9ff8p-2, 0x1.ce0a44eb17bccp-2}
 
 #if defined(__CUDACC__)
-__device__ __constant__ static const double kLogInvcDev[16] = WWB_LOG_INVC;
-__device__ __constant__ static const double kLogLogcDev[16] = WWB_LOG_LOGC;
-__device__ __constant__ static const double kLog2LogcDev[16] = WWB_LOG2_LOGC;
+__device__ static const double kLogInvcDev[16] = WWB_LOG_INVC;
+__device__ static const double kLogLogcDev[16] = WWB_LOG_LOGC;
+__device__ static const double kLog2LogcDev[16] = WWB_LOG2_LOGC;
 #endif
 static const double kLogInvcHost[16] = WWB_LOG_INVC;
 static const double kLogLogcHost[16] = WWB_LOG_LOGC;
@@ -187,21 +189,21 @@ static const double kLog2LogcHost[16] = WWB_LOG2_LOGC;
 
 WWB_HD double log_invc(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return kLogInvcDev[i];
+  return __ldg(&kLogInvcDev[i]);
 #else
   return kLogInvcHost[i];
 #endif
 }
 WWB_HD double log_logc(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return kLogLogcDev[i];
+  return __ldg(&kLogLogcDev[i]);
 #else
   return kLogLogcHost[i];
 #endif
 }
 WWB_HD double log2_logc(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return kLog2LogcDev[i];
+  return __ldg(&kLog2LogcDev[i]);
 #else
   return kLog2LogcHost[i];
 #endif
@@ -378,12 +380,12 @@ constexpr double kPi63 = 0x1.921fb54442d18p-62;       // pi * 2^-63
    0x57d1f534u, 0xd1f534ddu, 0xf534ddc0u, 0x34ddc0dbu, 0xddc0db62u, 0xc0db6295u,         \
    0xdb629599u, 0x6295993cu, 0x95993c43u, 0x993c4390u, 0x3c439041u}
 #if defined(__CUDACC__)
-__device__ __constant__ static const uint32_t kInvPio4Dev[24] = WWB_INV_PIO4;
+__device__ static const uint32_t kInvPio4Dev[24] = WWB_INV_PIO4;
 #endif
 static const uint32_t kInvPio4Host[24] = WWB_INV_PIO4;
 WWB_HD uint32_t inv_pio4(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return kInvPio4Dev[i];
+  return __ldg(reinterpret_cast<const unsigned int*>(&kInvPio4Dev[i]));
 #else
   return kInvPio4Host[i];
 #endif
@@ -757,12 +759,12 @@ WWB_HD float log10f(float x) {
    0x1.ea4afa2a490dap+0, -0x1.e9c23179c2893p-54, 0x1.efa1bee615a27p+0, 0x1.dc7f486a4b6b0p-54, \
    0x1.f50765b6e4540p+0, 0x1.9d3e12dd8a18bp-54, 0x1.fa7c1819e90d8p+0, 0x1.74853f3a5931ep-55}
 #if defined(__CUDACC__)
-__device__ __constant__ static const double kExp2_64Dev[128] = WWB_EXP2_64_TAB;
+__device__ static const double kExp2_64Dev[128] = WWB_EXP2_64_TAB;
 #endif
 static const double kExp2_64Host[128] = WWB_EXP2_64_TAB;
 WWB_HD double exp2_64(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return kExp2_64Dev[i];
+  return __ldg(&kExp2_64Dev[i]);
 #else
   return kExp2_64Host[i];
 #endif

@@ -267,7 +267,6 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
               fw = sh.fw, fu = sh.fu, fud = sh.fud, ustarsigma = sh.ustarsigma;
   float ust = ustar, taux = 0.0f, tauy = 0.0f, cosu = 0.0f, sinu = 0.0f, ustp = 0.0f,
         usdirp = 0.0f;
-  float ss[3][2] = {{0, 0}, {0, 0}, {0, 0}}, sn[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   const int istab_first = p.stab3 ? 1 : 3, istab_last = p.stab3 ? 2 : 3;
   int parity = 0;
   for (int istab = istab_first; istab <= istab_last; ++istab) {
@@ -277,13 +276,12 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
     dm::sincosf(usdir, &su, &cu);
     taux = (ust * ust) * cu;
     tauy = (ust * ust) * su;
-    float* const ssi = ss[istab - 1];
-    float* const sni = sn[istab - 1];
-    ssi[0] = ssi[1] = sni[0] = sni[1] = 0.0f;
+    // The running sums of this pass (STRESSSTAB, STRESSSTABN of ISTAB), in registers.
+    float ssi0 = 0.0f, ssi1 = 0.0f, sni0 = 0.0f, sni1 = 0.0f;
     for (int ik = 1; ik <= nk; ++ik, parity ^= 1) {
       if (scan) {
-        const float taupx = taux - fabs_f(p.ttauwshelter) * ssi[0];
-        const float taupy = tauy - fabs_f(p.ttauwshelter) * ssi[1];
+        const float taupx = taux - fabs_f(p.ttauwshelter) * ssi0;
+        const float taupy = tauy - fabs_f(p.ttauwshelter) * ssi1;
         ustp = min_r(dm::powf((taupx * taupx + taupy * taupy), 0.25f), max_r(ust, 0.3f));
         usdirp = dm::atan2f(taupy, taupx);
         dm::sincosf(usdirp, &sinu, &cosu);
@@ -336,15 +334,22 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
       cta.sync();
       if (scan) {
         for (int ith = 0; ith < nth; ++ith) {
+          const float t0 = sh.term[parity][0][ith], t1 = sh.term[parity][1][ith];
           if (sh.term[parity][2][ith] != 0.0f) {
-            sni[0] = sni[0] + sh.term[parity][0][ith];
-            sni[1] = sni[1] + sh.term[parity][1][ith];
+            sni0 = sni0 + t0;
+            sni1 = sni1 + t1;
           } else {
-            ssi[0] = ssi[0] + sh.term[parity][0][ith];
-            ssi[1] = ssi[1] + sh.term[parity][1][ith];
+            ssi0 = ssi0 + t0;
+            ssi1 = ssi1 + t1;
           }
         }
       }
+    }
+    if (cta.role(0)) {
+      sh.ss[istab - 1][0] = ssi0;
+      sh.ss[istab - 1][1] = ssi1;
+      sh.sn[istab - 1][0] = sni0;
+      sh.sn[istab - 1][1] = sni1;
     }
   }
   if (cta.role(0)) {
@@ -355,11 +360,6 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
     sh.sinu = sinu;
     sh.ustp = ustp;
     sh.usdirp = usdirp;
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 2; ++j) {
-        sh.ss[i][j] = ss[i][j];
-        sh.sn[i][j] = sn[i][j];
-      }
   }
   cta.sync();
 
