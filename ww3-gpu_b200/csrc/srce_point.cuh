@@ -49,6 +49,7 @@ struct SrceSh {
   float depth, drat, icescaleln, icescalein, icescalenl, icescaleds;
   float fage, fhigh, dttot, dt, tauwax, tauway, hstot, vddb, afilt, dtred;
   int nsteps, nkh, nkh1, nspech, done, nscut;
+  int sin4_valid;  ///< the last W3SIN4's outputs hold for the next step's first call
   float red[32];
   Sin4Sh sin4;
   Sds4Sh sds4;
@@ -320,6 +321,7 @@ WWB_PN void srce_init(const Cta& cta, const SrceCtx& x) {
     s.fage = 0.0f;
     s.fhigh = mx((p.ffxfm + 0.0f) * mx(s.r.fmeanws, s.r.fmean1), p.ffxpm / s.r.ustar);
     s.done = 0;
+    s.sin4_valid = 0;
   }
   cta.sync();
 }
@@ -362,11 +364,15 @@ WWB_PN void srce_ln1(const Cta& cta, const SrceCtx& x) {
   cta.sync();
 }
 
-/// 2. The start of a step (:1210-1239): the step count, W3SLN1, W3SIN4.
+/// 2. The start of a step (:1210-1239): the step count, W3SLN1, W3SIN4. W3SIN4 here reads
+/// exactly what the previous step's closing W3SIN4 (:2007) read when no W3SPR4 ran after it
+/// (:2012 runs only for SINTAILPAR(4) < 0.5): the spectrum, USTAR, Z0 and the wind are then
+/// unchanged and its outputs (VSIN, VDIN, LLWS, TAUWX/Y, TAUWAX/Y) are still in place, so the
+/// call is not repeated. The bits are the same either way.
 WWB_PD void srce_step_a(const Cta& cta, const SrceCtx& x) {
   if (cta.role(0)) x.sh->nsteps = x.sh->nsteps + 1;
   if (x.p->ln1) srce_ln1(cta, x);
-  srce_sin4(cta, x);
+  if (!x.sh->sin4_valid) srce_sin4(cta, x);
 }
 
 /// The step's DIA (:1259-1263) with KDMEAN = WNMEAN * DEPTH.
@@ -604,21 +610,25 @@ WWB_PN void srce_step_c(const Cta& cta, const SrceCtx& x) {
     cta.sync();
     if (cta.role(0)) {
       float v = s.phiaw;
+#pragma unroll 8
       for (int is = 0; is < nspec; ++is) v = t_phiaw[is] + v;
       s.phiaw = v;
     }
     if (cta.role(1)) {
       float v = s.phibbl;
+#pragma unroll 8
       for (int is = 0; is < nspec; ++is) v = v - t_phibbl[is];
       s.phibbl = v;
     }
     if (cta.role(2)) {
       float v = 0.0f;
+#pragma unroll 8
       for (int is = 0; is < nspec; ++is) v = v + t_wc[is];
       s.whitecap[2] = sqrt_f(v) * 4.0f;
     }
     if (cta.role(3)) {
       float v = 0.0f;
+#pragma unroll 8
       for (int is = 0; is < nspec; ++is) v = v + t_hs[is];
       s.hstot = sqrt_f(v) * 4.0f;
     }
@@ -684,7 +694,10 @@ WWB_PN void srce_step_c(const Cta& cta, const SrceCtx& x) {
   }
   srce_sin4(cta, x);  // :2007
   if (q.sintailpar[3] < 0.5f) srce_spr4(cta, x);  // :2012
-  if (cta.role(0)) s.done = s.dttot >= 0.9999f * x.in.dtg ? 1 : 0;
+  if (cta.role(0)) {
+    s.done = s.dttot >= 0.9999f * x.in.dtg ? 1 : 0;
+    s.sin4_valid = q.sintailpar[3] < 0.5f ? 0 : 1;
+  }
   cta.sync();
 }
 

@@ -43,9 +43,10 @@ struct Cta {
     __syncthreads();
 #endif
   }
-  /// Whether this thread runs serial role r (roles spread over the threads, all on thread 0 of a
-  /// one-thread CTA).
-  WWB_PD bool role(int r) const { return tid == r % nthr; }
+  /// Whether this thread runs serial role r: role r is the first thread of warp r (so roles of
+  /// one phase run side by side, not serialized within a warp); all on thread 0 of a one-thread
+  /// CTA.
+  WWB_PD bool role(int r) const { return tid == (32 * r) % nthr; }
 };
 
 #define PFOR(i, n) for (int i = cta.tid; i < (n); i += cta.nthr)
@@ -119,7 +120,7 @@ struct Sin4Sh {
   float ust, taux, tauy, cosu, sinu, ustp, usdirp;
   float ss[3][2], sn[3][2];
   float term[2][3][128];  ///< double-buffered per-direction stress terms (c, s, sign), NTH <= 128
-  float tail[6][kJtot];   ///< the analytic tail's terms that do not depend on USTR, per J
+  float tail[7][kJtot];   ///< the analytic tail's terms that do not depend on USTR, per J
 };
 
 /// Reals of W3SIN4's NK work: EB and the six per-IK factors of the stress scan.
@@ -179,6 +180,7 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
         sh.tail[1][j0] = ykm;
         sh.tail[2][j0] = sqrt_f(kGrav * tensk / y);
         sh.tail[3][j0] = 0.5f * (3.0f * ykm2 + 1.0f) * sqrt_f(kGrav / (y * tensk));
+        sh.tail[6][j0] = kGrav * z0 / (sh.tail[2][j0] * sh.tail[2][j0]);
         if (p.sintailpar[2] > 0.0f) {
           const float ykm1 = (ykm - 1.0f);
           sh.tail[4][j0] = dm::expf(-0.25f * (ykm1 * ykm1));
@@ -333,6 +335,7 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
       }
       cta.sync();
       if (scan) {
+#pragma unroll 4
         for (int ith = 0; ith < nth; ++ith) {
           const float t0 = sh.term[parity][0][ith], t1 = sh.term[parity][1][ith];
           if (sh.term[parity][2][ith] != 0.0f) {
@@ -411,7 +414,6 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
     float tauhf;
     if (p.sintailpar[0] < 0.5f) {
       float ustr = ust3;
-      const float zz0 = z0;
       const float signk = f.sig[nk];
       const float zinf = dm::logf(signk * signk / kGrav);
       const float dely = (kLogTpiOver005 - zinf) / static_cast<float>(kJtot);
@@ -423,7 +425,7 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
         const float cgtail = sh.tail[3][j - 1];
         const float zx = ustr / cm + p.zzalp;
         const float zarg = min_r(kKappa / zx, 20.0f);
-        const float zmu = min_r(kGrav * zz0 / (cm * cm) * dm::expf(zarg), 1.0f);
+        const float zmu = min_r(sh.tail[6][j - 1] * dm::expf(zarg), 1.0f);
         const float zlog = min_r(dm::logf(zmu), 0.0f);
         const float zlog2 = zlog * zlog;
         const float zbeta = sh.const1 * zmu * (zlog2 * zlog2);
@@ -626,16 +628,19 @@ WWB_PN void spr4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
   cta.sync();
   if (cta.role(0)) {
     float v = 0.0f;
+#pragma unroll 8
     for (int i = 0; i < nspec; ++i) v = v + tc[i];
     chains[0] = v;
   }
   if (cta.role(1)) {
     float v = 0.0f;
+#pragma unroll 8
     for (int i = 0; i < nspec; ++i) v = v + ts[i];
     chains[1] = v;
   }
   if (cta.role(2)) {
     float v = 0.0f;
+#pragma unroll 8
     for (int i = 0; i < nspec; ++i) v = max_r(v, a[i]);
     chains[2] = v;
   }
