@@ -215,6 +215,33 @@ int ww_xyp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, i
                      const float* bbpi0, const float* bbpin, const int* on, float* va, int nspec,
                      int nsealm);
 
+/* Replaces ww_xyp3_batch_mpi (prop3_c.hpp:48-63, prop3_shim.cpp:1068-1099): ww_xyp3_batch_va
+ * under W3_MPI. Sea point ISEA is column K = (ISEA-1)/naproc + 1 of rank IP =
+ * MOD(ISEA-1,naproc) + 1. This rank's (iaproc's) points are its VA columns; rank IP's value of
+ * the L-th component with on /= 0 (ascending) is rbuf[poff[IP-1] + L*nsealm + K-1] (W3GATH's
+ * GSTORE), and W3SCAT writes the same place of sbuf (SSTORE, 0 past NSEA). poff holds the
+ * blocks in rank order, NSPLOC*nsealm each (iaproc's entry not read); nbuf =
+ * (naproc-1)*NSPLOC*nsealm. Other shapes: BAD_SHAPE, nothing written. */
+int ww_xyp3_batch_mpi(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar,
+                      const int* imaps, int nimaps, const float* tscal, int ntscal, float dtg,
+                      const int* mapsf, const float* clats, const float* sig, const float* ecos,
+                      const float* esin, const float* dpdx, const float* dpdy, const float* dqdx,
+                      const float* dqdy, const float* gsqrt, const float* atrnx,
+                      const float* atrny, const int* mapx2, const int* mapy2, const int* mapaxy,
+                      const int* mapcxy, const int* maptrn, const int* mapsta, const float* cg,
+                      const float* cx, const float* cy, int flbpi, int nbi, const int* isbpi,
+                      const float* bbpi0, const float* bbpin, const int* on, float* va,
+                      int nspec, int nsealm, int naproc, int iaproc, const int* poff,
+                      const float* rbuf, float* sbuf, int nbuf);
+
+/* Replace ww_xyp3_mpi_pack / ww_xyp3_mpi_unpack (prop3_c.hpp:65-70, prop3_shim.cpp:1101-1123):
+ * buf[J*nsealm + K-1] = VA(isps[J], K), K = 1 .. nsealm, from the resident VA of grid igrid
+ * (pack: state unchanged), or back into it (unpack: state DEVICE afterwards). */
+int ww_xyp3_mpi_pack(int igrid, float* va, int nspec, int nsealm, const int* isps, int nisp,
+                     float* buf);
+int ww_xyp3_mpi_unpack(int igrid, float* va, int nspec, int nsealm, const int* isps, int nisp,
+                       const float* buf);
+
 /* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* call (the reference
  * returns it only). */
 int ww_prop3_last_error(void);

@@ -133,6 +133,12 @@ struct Xyp3Args {
   int nrpar, nipar, nimaps, ntscal, flbpi, nbi, ncol;
   float dtg;
   float* va;
+  // ww_xyp3_batch_mpi only (naproc > 0): the ranks, the offsets of the other ranks' blocks, the
+  // received values (GSTORE) and the values to send back (SSTORE), nbuf floats each.
+  int naproc = 0, iaproc = 0, nbuf = 0;
+  const int* poff = nullptr;
+  const float* rbuf = nullptr;
+  float* sbuf = nullptr;
 };
 
 int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int nsealm) {
@@ -157,7 +163,7 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
   g.flagll = a.ipar[9];
   g.flcur = a.ipar[10];
   if (g.nx < 1 || g.ny < 1 || g.nsea < 1 || g.nk < 1 || g.nth < 1 || g.nspec != g.nk * g.nth ||
-      a.ncol < g.nsea + 1 || a.nbi < 0 || !a.mapsf || !a.clats || !a.sig || !a.ecos || !a.esin ||
+      (a.naproc == 0 && a.ncol < g.nsea + 1) || a.nbi < 0 || !a.mapsf || !a.clats || !a.sig || !a.ecos || !a.esin ||
       !a.dpdx || !a.dpdy || !a.dqdx || !a.dqdy || !a.gsqrt || !a.atrnx || !a.atrny ||
       !a.mapx2 || !a.mapy2 || !a.mapaxy || !a.mapcxy || !a.maptrn || !a.mapsta || !a.cg ||
       !a.cx || !a.cy || !a.on || !a.va ||
@@ -166,6 +172,24 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
     return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch: bad sizes or null pointer");
   if (g.iclose == kIcloseTrpl)
     return fail(WW_KOKKOS_ERR_UNSUPPORTED, "ww_xyp3_batch: tripole grid (W3XYP3 stops there)");
+  int nsploc = 0;
+  for (int isp = 0; isp < g.nspec; ++isp) nsploc += a.on[isp] != 0 ? 1 : 0;
+  if (a.naproc != 0) {
+    // Every sea point is some rank's column K <= NSEALM, and every other rank's block holds this
+    // rank's NSPLOC components of NSEALM values each, in rank order (prop3_shim.cpp:793-811).
+    const long long nsealm_ll = a.ncol - 1;
+    if (!resident || a.naproc < 1 || a.iaproc < 1 || a.iaproc > a.naproc || nsealm_ll < 1 ||
+        nsealm_ll * a.naproc < g.nsea || !a.poff ||
+        a.nbuf != static_cast<long long>(a.naproc - 1) * nsploc * nsealm_ll ||
+        (a.nbuf > 0 && (!a.rbuf || !a.sbuf)))
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch_mpi: bad ranks, offsets or buffers");
+    for (int ip = 1, off = 0; ip <= a.naproc; ++ip) {
+      if (ip == a.iaproc) continue;
+      if (a.poff[ip - 1] != off)
+        return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_batch_mpi: offsets not in rank order");
+      off += nsploc * static_cast<int>(nsealm_ll);
+    }
+  }
   g.global = g.iclose != kIcloseNone ? 1 : 0;
   if (g.global && g.nx < 3)
     return fail(WW_KOKKOS_ERR_UNSUPPORTED, "ww_xyp3_batch: a closed grid needs NX >= 3");
@@ -267,6 +291,17 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
     d_va = st.in(slot++, a.va, static_cast<size_t>(g.nspec) * a.ncol, s);
   }
   const int* d_list = st.in(slot++, list.data(), list.size(), s);
+  const size_t nbuf = static_cast<size_t>(a.nbuf);
+  if (a.naproc > 0) {
+    g.naproc = a.naproc;
+    g.iaproc = a.iaproc;
+    g.nsealm = a.ncol - 1;
+    g.poff = st.in(slot++, a.poff, static_cast<size_t>(a.naproc), s);
+    g.rbuf = st.in(slot++, a.rbuf, nbuf, s);
+    // SSTORE starts at 0 and W3SCAT writes sea points only: entries past NSEA stay 0.
+    g.sbuf = static_cast<float*>(st.get(slot++, nbuf * sizeof(float)));
+    if (nbuf > 0) WWB_CHECK(cudaMemsetAsync(g.sbuf, 0, nbuf * sizeof(float), s));
+  }
   // Chunks of components, their work arrays carved from one staging slot.
   const size_t per = xyp3_bytes_per_component(g);
   const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(list.size(), kXyp3ChunkBytes / per)));
@@ -275,6 +310,7 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
   for (size_t c0 = 0; c0 < list.size(); c0 += chunk) {
     Xyp3Chunk ch{};
     ch.ncomp = static_cast<int>(std::min<size_t>(chunk, list.size() - c0));
+    ch.l0 = static_cast<int>(c0);
     ch.isp = d_list + c0;
     float* f = reinterpret_cast<float*>(base);
     ch.vq = f;
@@ -293,7 +329,45 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
   else
     WWB_CHECK(cudaMemcpyAsync(a.va, d_va, sizeof(float) * g.nspec * static_cast<size_t>(a.ncol),
                               cudaMemcpyDeviceToHost, s));
+  if (a.naproc > 0 && nbuf > 0)
+    WWB_CHECK(cudaMemcpyAsync(a.sbuf, g.sbuf, nbuf * sizeof(float), cudaMemcpyDeviceToHost, s));
   WWB_CHECK(cudaStreamSynchronize(s));
+  g_prop3.ok();
+  return WW_KOKKOS_OK;
+}
+
+/// ww_xyp3_mpi_pack (unpack false) and ww_xyp3_mpi_unpack (unpack true) on the resident VA of
+/// grid igrid (prop3_shim.cpp:887-925): buf[J*NSEALM + K-1] and VA(ISPS(J+1), K).
+int xyp3_mpi_move(bool unpack, int igrid, float* va, int nspec, int nsealm, const int* isps,
+                  int nisp, float* buf) {
+  if (!va || nspec < 1 || nsealm < 1 || nisp < 0 || nisp > nspec ||
+      (nisp > 0 && (!isps || !buf)))
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_mpi_pack/unpack: bad sizes or null pointer");
+  for (int j = 0; j < nisp; ++j)
+    if (isps[j] < 1 || isps[j] > nspec)
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_xyp3_mpi_pack/unpack: a component outside VA");
+  if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+  timers::Region t_call(unpack ? "xyp3.unpack" : "xyp3.pack");
+  float* d_va = nullptr;
+  const int rc = va_device(igrid, va, nspec, nsealm, &d_va);
+  if (rc != WW_KOKKOS_OK)
+    return fail(rc, "ww_xyp3_mpi_pack/unpack: the resident VA refused this call");
+  const size_t n = static_cast<size_t>(nisp) * nsealm;
+  if (n > 0) {
+    Staging& st = staging();
+    cudaStream_t s = runtime().stream;
+    // Slots past the XYP3 call's, so a pack between two steps reuses its own buffers.
+    constexpr int kSlot = 64;
+    const int* d_isps = st.in(kSlot, isps, static_cast<size_t>(nisp), s);
+    float* d_buf = unpack ? st.in(kSlot + 1, static_cast<const float*>(buf), n, s)
+                          : static_cast<float*>(st.get(kSlot + 1, n * sizeof(float)));
+    launch_va_components(unpack, d_va, nspec, nsealm, d_isps, nisp, d_buf, s);
+    if (!unpack)
+      WWB_CHECK(cudaMemcpyAsync(buf, d_buf, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    WWB_CHECK(cudaStreamSynchronize(s));
+  }
+  // A pack only read the device copy; an unpack wrote it.
+  if (unpack) va_device_written(igrid);
   g_prop3.ok();
   return WW_KOKKOS_OK;
 }
@@ -378,6 +452,43 @@ int ww_xyp3_batch_va(int igrid, const float* rpar, int nrpar, const int* ipar, i
                    mapsf, mapx2, mapy2, mapaxy, mapcxy, maptrn, mapsta, isbpi,  on,     nrpar,
                    nipar, nimaps, ntscal, flbpi, nbi, nsealm + 1, dtg, va};
   return guarded([&] { return xyp3_entry(igrid, true, a, nspec, nsealm); });
+}
+
+int ww_xyp3_batch_mpi(int igrid, const float* rpar, int nrpar, const int* ipar, int nipar,
+                      const int* imaps, int nimaps, const float* tscal, int ntscal, float dtg,
+                      const int* mapsf, const float* clats, const float* sig, const float* ecos,
+                      const float* esin, const float* dpdx, const float* dpdy, const float* dqdx,
+                      const float* dqdy, const float* gsqrt, const float* atrnx,
+                      const float* atrny, const int* mapx2, const int* mapy2, const int* mapaxy,
+                      const int* mapcxy, const int* maptrn, const int* mapsta, const float* cg,
+                      const float* cx, const float* cy, int flbpi, int nbi, const int* isbpi,
+                      const float* bbpi0, const float* bbpin, const int* on, float* va,
+                      int nspec, int nsealm, int naproc, int iaproc, const int* poff,
+                      const float* rbuf, float* sbuf, int nbuf) {
+  Xyp3Args a{rpar,  tscal, clats, sig,    ecos,   esin,   dpdx,   dpdy,   dqdx,   dqdy,
+             gsqrt, atrnx, atrny, cg,     cx,     cy,     bbpi0,  bbpin,  ipar,   imaps,
+             mapsf, mapx2, mapy2, mapaxy, mapcxy, maptrn, mapsta, isbpi,  on,     nrpar,
+             nipar, nimaps, ntscal, flbpi, nbi, nsealm + 1, dtg, va};
+  // naproc < 1 is refused as a bad rank count, not taken for W3_SHRD.
+  a.naproc = naproc < 1 ? -1 : naproc;
+  a.iaproc = iaproc;
+  a.poff = poff;
+  a.rbuf = rbuf;
+  a.sbuf = sbuf;
+  a.nbuf = nbuf;
+  return guarded([&] { return xyp3_entry(igrid, true, a, nspec, nsealm); });
+}
+
+int ww_xyp3_mpi_pack(int igrid, float* va, int nspec, int nsealm, const int* isps, int nisp,
+                     float* buf) {
+  return guarded([&] { return xyp3_mpi_move(false, igrid, va, nspec, nsealm, isps, nisp, buf); });
+}
+
+int ww_xyp3_mpi_unpack(int igrid, float* va, int nspec, int nsealm, const int* isps, int nisp,
+                       const float* buf) {
+  return guarded([&] {
+    return xyp3_mpi_move(true, igrid, va, nspec, nsealm, isps, nisp, const_cast<float*>(buf));
+  });
 }
 
 int ww_prop3_last_error(void) { return g_prop3.get(); }

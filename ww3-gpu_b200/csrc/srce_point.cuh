@@ -610,25 +610,25 @@ WWB_PN void srce_step_c(const Cta& cta, const SrceCtx& x) {
     cta.sync();
     if (cta.role(0)) {
       float v = s.phiaw;
-#pragma unroll 8
+WWB_UNROLL(8)
       for (int is = 0; is < nspec; ++is) v = t_phiaw[is] + v;
       s.phiaw = v;
     }
     if (cta.role(1)) {
       float v = s.phibbl;
-#pragma unroll 8
+WWB_UNROLL(8)
       for (int is = 0; is < nspec; ++is) v = v - t_phibbl[is];
       s.phibbl = v;
     }
     if (cta.role(2)) {
       float v = 0.0f;
-#pragma unroll 8
+WWB_UNROLL(8)
       for (int is = 0; is < nspec; ++is) v = v + t_wc[is];
       s.whitecap[2] = sqrt_f(v) * 4.0f;
     }
     if (cta.role(3)) {
       float v = 0.0f;
-#pragma unroll 8
+WWB_UNROLL(8)
       for (int is = 0; is < nspec; ++is) v = v + t_hs[is];
       s.hstot = sqrt_f(v) * 4.0f;
     }

@@ -27,9 +27,12 @@
 #if defined(__CUDACC__)
 #define WWB_PD __host__ __device__ __forceinline__
 #define WWB_PN __host__ __device__ __noinline__  // the large routines: called, not inlined
+#define WWB_PRAGMA(x) _Pragma(#x)
+#define WWB_UNROLL(n) WWB_PRAGMA(unroll n)
 #else
 #define WWB_PD inline
 #define WWB_PN inline
+#define WWB_UNROLL(n)
 #endif
 
 namespace wwb {
@@ -335,7 +338,7 @@ WWB_PN void sin4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
       }
       cta.sync();
       if (scan) {
-#pragma unroll 4
+WWB_UNROLL(4)
         for (int ith = 0; ith < nth; ++ith) {
           const float t0 = sh.term[parity][0][ith], t1 = sh.term[parity][1][ith];
           if (sh.term[parity][2][ith] != 0.0f) {
@@ -628,19 +631,19 @@ WWB_PN void spr4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
   cta.sync();
   if (cta.role(0)) {
     float v = 0.0f;
-#pragma unroll 8
+WWB_UNROLL(8)
     for (int i = 0; i < nspec; ++i) v = v + tc[i];
     chains[0] = v;
   }
   if (cta.role(1)) {
     float v = 0.0f;
-#pragma unroll 8
+WWB_UNROLL(8)
     for (int i = 0; i < nspec; ++i) v = v + ts[i];
     chains[1] = v;
   }
   if (cta.role(2)) {
     float v = 0.0f;
-#pragma unroll 8
+WWB_UNROLL(8)
     for (int i = 0; i < nspec; ++i) v = max_r(v, a[i]);
     chains[2] = v;
   }

@@ -146,7 +146,32 @@ __device__ __forceinline__ void corner(float dxcgc, float dycgc, int ny, int& ii
   }
 }
 
-__global__ void sea_setup_kernel(Xyp3Grid g, int ncomp, Comp* comps, const float* __restrict__ va) {
+/// W3GATH's value of component isp (the l-th listed) at sea point isea: VA under W3_SHRD, this
+/// rank's VA column or the received block of its owner under W3_MPI (prop3_shim.cpp:111-141).
+__device__ __forceinline__ float va_get(const Xyp3Grid& g, const float* __restrict__ va, int isea,
+                                        int l, int isp) {
+  if (g.naproc == 0) return va[static_cast<size_t>(isea) * g.nspec + (isp - 1)];
+  const int ip = (isea - 1) % g.naproc + 1, k = (isea - 1) / g.naproc + 1;
+  if (ip == g.iaproc) return va[static_cast<size_t>(k) * g.nspec + (isp - 1)];
+  return g.rbuf[static_cast<size_t>(g.poff[ip - 1]) + static_cast<size_t>(l) * g.nsealm + (k - 1)];
+}
+
+/// W3SCAT's store of v, the counterpart of va_get.
+__device__ __forceinline__ void va_put(const Xyp3Grid& g, float* __restrict__ va, int isea, int l,
+                                       int isp, float v) {
+  if (g.naproc == 0) {
+    va[static_cast<size_t>(isea) * g.nspec + (isp - 1)] = v;
+    return;
+  }
+  const int ip = (isea - 1) % g.naproc + 1, k = (isea - 1) / g.naproc + 1;
+  if (ip == g.iaproc)
+    va[static_cast<size_t>(k) * g.nspec + (isp - 1)] = v;
+  else
+    g.sbuf[static_cast<size_t>(g.poff[ip - 1]) + static_cast<size_t>(l) * g.nsealm + (k - 1)] = v;
+}
+
+__global__ void sea_setup_kernel(Xyp3Grid g, int ncomp, int l0, Comp* comps,
+                                 const float* __restrict__ va) {
   const long long n = static_cast<long long>(ncomp) * g.nsea;
   const int qoff = g.ny - 1;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
@@ -185,7 +210,7 @@ __global__ void sea_setup_kernel(Xyp3Grid g, int ncomp, Comp* comps, const float
     ii[3 * g.nsea] = i4;
     // W3GATH then section 2.a (:1080-1137): this sea point's cell only.
     const float cgi = g.cg[isea * (g.nk + 2) + k.ik];
-    const float v = va[static_cast<size_t>(isea) * g.nspec + (k.isp - 1)];
+    const float v = va_get(g, va, isea, l0 + c, k.isp);
     k.q[ixy + qoff] = (v / cgi) * clat;
     float cxt = (k.ecosi * cgi) / clat;
     float cyt = k.esini * cgi;
@@ -481,7 +506,8 @@ __global__ void finish_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itlo
 }
 
 // ---- section 4 and W3SCAT, per (component, sea point) --------------------------------------
-__global__ void store_kernel(Xyp3Grid g, int ncomp, const Comp* comps, float* __restrict__ va) {
+__global__ void store_kernel(Xyp3Grid g, int ncomp, int l0, const Comp* comps,
+                             float* __restrict__ va) {
   const long long n = static_cast<long long>(ncomp) * g.nsea;
   const int qoff = g.ny - 1;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
@@ -496,7 +522,7 @@ __global__ void store_kernel(Xyp3Grid g, int ncomp, const Comp* comps, float* __
       const float x = (g.cg[isea * (g.nk + 2) + k.ik] / g.clats[isea]) * v;
       v = max_r(x, 0.0f);
     }
-    if (st != 0) va[static_cast<size_t>(isea) * g.nspec + (k.isp - 1)] = v;
+    if (st != 0) va_put(g, va, isea, l0 + c, k.isp, v);
   }
 }
 
@@ -568,6 +594,32 @@ void xyp3_current_range(Xyp3Grid& g, cudaStream_t s) {
   g.cymax = g.nsea <= 0 ? -huge : (h[5] > 0 ? h[3] : nan);
 }
 
+// ---- the components other ranks own, between the resident VA and a message buffer ----------
+__global__ void va_components_kernel(bool unpack, float* __restrict__ va, int nspec, int nsealm,
+                                     const int* __restrict__ isps, int nisp,
+                                     float* __restrict__ buf) {
+  const long long n = static_cast<long long>(nisp) * nsealm;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(t / nsealm);
+    const int k = 1 + static_cast<int>(t % nsealm);
+    float* v = va + static_cast<size_t>(k) * nspec + (isps[j] - 1);
+    if (unpack)
+      *v = buf[t];
+    else
+      buf[t] = *v;
+  }
+}
+
+void launch_va_components(bool unpack, float* va, int nspec, int nsealm, const int* isps,
+                          int nisp, float* buf, cudaStream_t s) {
+  const long long n = static_cast<long long>(nisp) * nsealm;
+  if (n <= 0) return;
+  va_components_kernel<<<blocks_for(n), kBlock, 0, s>>>(unpack, va, nspec, nsealm, isps, nisp,
+                                                        buf);
+  WWB_CHECK(cudaGetLastError());
+}
+
 void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s) {
   const int nc = ch.ncomp;
   if (nc <= 0) return;
@@ -595,7 +647,7 @@ void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s)
   WWB_CHECK(cudaMemsetAsync(ch.vlcflx, 0, sizeof(float) * n1 * nc, s));
   WWB_CHECK(cudaMemsetAsync(ch.vlcfly, 0, sizeof(float) * n1 * nc, s));
   const long long nsea_c = static_cast<long long>(nc) * g.nsea;
-  sea_setup_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, va);
+  sea_setup_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.l0, ch.comp, va);
   WWB_CHECK(cudaGetLastError());
   WWB_CHECK(cudaStreamSynchronize(s));
   int ntmax = 0;
@@ -625,7 +677,7 @@ void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s)
     WWB_CHECK(cudaGetLastError());
     yfirst = !yfirst;
   }
-  store_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, va);
+  store_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.l0, ch.comp, va);
   WWB_CHECK(cudaGetLastError());
 }
 

@@ -42,11 +42,20 @@ struct Xyp3Grid {
   int flbpi, nbi;
   float dsec_day, dsec_bpi0, dsec_bpin, dtg;
   float cxmin, cxmax, cymin, cymax;  ///< MINVAL/MAXVAL of CX, CY over the sea (FLCUR)
+  // W3_MPI (naproc > 0): sea point ISEA is column K = (ISEA-1)/NAPROC + 1 of rank
+  // IP = MOD(ISEA-1,NAPROC) + 1. This rank's points are VA columns; another rank's value of the
+  // L-th listed component is rbuf[poff[IP-1] + L*NSEALM + K-1] (W3GATH's GSTORE) and W3SCAT's
+  // SSTORE goes to the same place of sbuf. naproc == 0: W3_SHRD, column ISEA of VA.
+  int naproc, iaproc, nsealm;
+  const int* poff;
+  const float* rbuf;
+  float* sbuf;
 };
 
 /// One chunk of components: their indices and the device work arrays (component-major).
 struct Xyp3Chunk {
   int ncomp;
+  int l0;             ///< place of the chunk's first component in the list of all components
   const int* isp;     ///< 1-based ISP of each component
   float* vq;          ///< ncomp x NQ, NQ = NY*(NX+3): FIELD(1-NY : NY*(NX+2))
   float* aq;          ///< ncomp x NQ
@@ -64,6 +73,11 @@ size_t xyp3_bytes_per_component(const Xyp3Grid& g);
 /// W3GATH, W3XYP3 and W3SCAT for every component of the chunk, on the resident VA
 /// (NSPEC, 0:NSEALM) va. The chunk's arrays must be allocated (xyp3_bytes_per_component).
 void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& c, float* va, cudaStream_t s);
+
+/// ww_xyp3_mpi_pack (unpack false): buf[J*NSEALM + K-1] = VA(ISPS(J+1), K), K = 1 .. NSEALM;
+/// ww_xyp3_mpi_unpack (unpack true) the other way. d_isps holds nisp 1-based components.
+void launch_va_components(bool unpack, float* va, int nspec, int nsealm, const int* isps,
+                          int nisp, float* buf, cudaStream_t s);
 
 /// MINVAL/MAXVAL of CX(1:NSEA), CY(1:NSEA) as gfortran evaluates them (NaN entries skipped,
 /// NaN when all are NaN, +-HUGE when empty), into g.cxmin .. g.cymax.

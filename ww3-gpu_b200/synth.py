@@ -248,7 +248,9 @@ def land_mask(nx, ny, seed=0, sea_fraction=0.7, smooth=6):
     f = np.apply_along_axis(lambda r: np.convolve(np.concatenate([r[-3 * smooth:], r,
                                                                   r[:3 * smooth]]), k, "valid"),
                             1, f)
-    f = np.apply_along_axis(lambda c: np.convolve(c, k, "same"), 0, f)
+    # latitude: edge-padded, so the mask keeps NY rows whatever NY is against the kernel
+    f = np.apply_along_axis(lambda c: np.convolve(np.pad(c, 3 * smooth, mode="edge"), k, "valid"),
+                            0, f)
     sea = f > np.quantile(f, 1.0 - sea_fraction)
     sea[0, :] = False
     sea[-1, :] = False
