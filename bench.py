@@ -223,9 +223,11 @@ def measured_peak_hbm():
 
 
 def ncu_traffic_per_point(kernel_name):
-    """DRAM bytes per sea point of the W3SNL1 kernel `kernel_name` from the committed ncu
-    capture summary (profiles/<kernel_name>_36x36.json), or None."""
+    """DRAM bytes per sea point of kernel `kernel_name` from the committed ncu capture summary
+    (profiles/<kernel_name>_36x36.json, or without the _kernel suffix), or None."""
     p = ROOT / "profiles" / f"{kernel_name}_36x36.json"
+    if not p.exists():
+        p = ROOT / "profiles" / f"{kernel_name.removesuffix('_kernel')}_36x36.json"
     if not p.exists():
         return None
     try:
