@@ -210,7 +210,7 @@ void hemu_srce_batch(int it, int inflags24, int flogrd57, int flogrd58, float dt
                      float* spec, const float* wn1, const float* cg1, const float* pin,
                      float* psc, float* whitecap, float* taubbl, float* tauice, int* shave) {
   const pt::SrceLayout L = pt::srce_layout(g_p, g_ndev);
-  std::vector<float> w(L.total + 4);
+  std::vector<float> w(L.total_s + 4), gw(L.total_g + 4);
   static pt::SrceSh sh;
   const pt::Cta cta{0, 1};
   const int ns = g_sp.nspec, nk = g_sp.nk;
@@ -224,7 +224,8 @@ void hemu_srce_batch(int it, int inflags24, int flogrd57, int flogrd58, float dt
     pt::srce_psc_in(sh, ps, whitecap + 4 * static_cast<size_t>(n),
                     taubbl + 2 * static_cast<size_t>(n), tauice + 2 * static_cast<size_t>(n));
     pt::SrceCtx x{&g_sp, &g_sgrid, &g_p, &g_fields, &g_ndev,
-                  pt::srce_in(it, inflags24, flogrd57, flogrd58, dtg, pi), w.data(), &L, &sh};
+                  pt::srce_in(it, inflags24, flogrd57, flogrd58, dtg, pi), w.data(), gw.data(),
+                  &L, &sh};
     pt::srce_point(cta, x);
     std::memcpy(sp, w.data() + L.spec, sizeof(float) * ns);
     pt::srce_psc_out(sh, ps, whitecap + 4 * static_cast<size_t>(n),

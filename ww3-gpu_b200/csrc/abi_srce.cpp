@@ -53,10 +53,10 @@ struct GridCtx {
   DevVec<float> sig, dden, ecos, esin;
   DevVec<int> mapwn;
   SrceDev* dev = nullptr;   ///< device copy of the launch parameters, rebuilt at every call
-  int* counter = nullptr;   ///< the work queue's counter
+  SrceWork work;            ///< the work queue's counter, the working sets' global part
   ~GridCtx() {
     if (dev) cudaFree(dev);
-    if (counter) cudaFree(counter);
+    work.release();
   }
 };
 
@@ -100,7 +100,6 @@ bool prepare(int igrid, GridCtx& g, SrceDev& host, const char* who) {
   host.n = n;
   host.L = pt::srce_layout(q.p, n);
   if (g.dev == nullptr) WWB_CHECK(cudaMalloc(&g.dev, sizeof(SrceDev)));
-  if (g.counter == nullptr) WWB_CHECK(cudaMalloc(&g.counter, sizeof(int)));
   WWB_CHECK(cudaMemcpy(g.dev, &host, sizeof(SrceDev), cudaMemcpyHostToDevice));
   return true;
 }
@@ -124,7 +123,7 @@ void run_batch(int igrid, GridCtx& g, const SrceStep& step, int npts, float* spe
         *dti = c.in(tauice, 2 * n, s);
   int* dsh = c.in(shave, n, s);
   launch_srce(g.dev, host.L, step, npts, dspec, djsea, dwn, dcg, dpin, dpsc, dwc, dtb, dti, dsh,
-              g.counter, s);
+              g.work, s);
   if (!va_dev) out(spec, dspec, ns, s);
   out(psc, dpsc, n * srce::NPSC, s);
   out(whitecap, dwc, 4 * n, s);
@@ -320,7 +319,7 @@ void ww_srce_batch_device(int igrid, int it, int inflags24, int flogrd57, int fl
     SrceDev host{};
     if (!prepare(igrid, *g, host, "ww_srce_batch_device")) return;
     launch_srce(g->dev, host.L, SrceStep{it, inflags24, flogrd57, flogrd58, dtg}, npts, spec,
-                nullptr, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave, g->counter,
+                nullptr, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave, g->work,
                 static_cast<cudaStream_t>(stream));
     g_status.ok();
   } catch (const std::exception& e) {

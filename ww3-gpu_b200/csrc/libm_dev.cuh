@@ -40,9 +40,13 @@
 
 #if defined(__CUDACC__)
 #define WWB_HD __host__ __device__ __forceinline__
+// The public functions are called, not inlined: a kernel that calls them from dozens of sites
+// stays small enough for the instruction cache when several CTAs run different phases.
+#define WWB_HC static __host__ __device__ __noinline__
 #else
 #include <math.h>
 #define WWB_HD inline
+#define WWB_HC inline
 #endif
 
 namespace wwb {
@@ -63,9 +67,24 @@ __device__ static const uint64_t kExp2fTabDev[32] = WWB_EXP2F_TAB;
 #endif
 static const uint64_t kExp2fTabHost[32] = WWB_EXP2F_TAB;
 
+#if defined(__CUDA_ARCH__)
+/// Table loads through the read-only path, kept in L1 ahead of streamed data (evict_last): the
+/// tables are a few KB, and a serial chain pays an L2 round trip for every miss.
+__device__ __forceinline__ uint64_t tab_ld64(const void* p) {
+  uint64_t v;
+  asm("ld.global.nc.L1::evict_last.b64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint32_t tab_ld32(const void* p) {
+  uint32_t v;
+  asm("ld.global.nc.L1::evict_last.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+#endif
+
 WWB_HD uint64_t exp2f_tab(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return __ldg(reinterpret_cast<const unsigned long long*>(&kExp2fTabDev[i]));
+  return tab_ld64(&kExp2fTabDev[i]);
 #else
   return kExp2fTabHost[i];
 #endif
@@ -148,7 +167,7 @@ WWB_HD float expf_t(float x) {
 #ifndef WWB_EXPF_FUSE
 #define WWB_EXPF_FUSE 7
 #endif
-WWB_HD float expf(float x) { return expf_t<WWB_EXPF_FUSE>(x); }
+WWB_HC float expf(float x) { return expf_t<WWB_EXPF_FUSE>(x); }
 
 WWB_HD float fma_f(float a, float b, float c) {
 #if defined(__CUDA_ARCH__)
@@ -189,21 +208,21 @@ static const double kLog2LogcHost[16] = WWB_LOG2_LOGC;
 
 WWB_HD double log_invc(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return __ldg(&kLogInvcDev[i]);
+  return asdouble(tab_ld64(&kLogInvcDev[i]));
 #else
   return kLogInvcHost[i];
 #endif
 }
 WWB_HD double log_logc(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return __ldg(&kLogLogcDev[i]);
+  return asdouble(tab_ld64(&kLogLogcDev[i]));
 #else
   return kLogLogcHost[i];
 #endif
 }
 WWB_HD double log2_logc(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return __ldg(&kLog2LogcDev[i]);
+  return asdouble(tab_ld64(&kLog2LogcDev[i]));
 #else
   return kLog2LogcHost[i];
 #endif
@@ -251,7 +270,7 @@ WWB_HD float logf_t(float x) {
 #ifndef WWB_LOGF_FUSE
 #define WWB_LOGF_FUSE 7
 #endif
-WWB_HD float logf(float x) { return logf_t<WWB_LOGF_FUSE>(x); }
+WWB_HC float logf(float x) { return logf_t<WWB_LOGF_FUSE>(x); }
 
 // ------------------------------------------------------------------------------------ powf
 // log1p(r)/ln2 ~ A0 r^5 + A1 r^4 + A2 r^3 + A3 r^2 + A4 r (published coefficients).
@@ -359,7 +378,7 @@ WWB_HD float powf_t(float x, float y) {
 #ifndef WWB_POWF_FUSE
 #define WWB_POWF_FUSE 7
 #endif
-WWB_HD float powf(float x, float y) { return powf_t<WWB_POWF_FUSE>(x, y); }
+WWB_HC float powf(float x, float y) { return powf_t<WWB_POWF_FUSE>(x, y); }
 
 // --------------------------------------------------------------------------------- sincosf
 // Cosine 1 + c1 x^2 + ... (c0 = 1) and sine x + s1 x^3 + s2 x^5 + s3 x^7 coefficients of the
@@ -385,7 +404,7 @@ __device__ static const uint32_t kInvPio4Dev[24] = WWB_INV_PIO4;
 static const uint32_t kInvPio4Host[24] = WWB_INV_PIO4;
 WWB_HD uint32_t inv_pio4(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return __ldg(reinterpret_cast<const unsigned int*>(&kInvPio4Dev[i]));
+  return tab_ld32(&kInvPio4Dev[i]);
 #else
   return kInvPio4Host[i];
 #endif
@@ -459,7 +478,7 @@ WWB_HD void sincosf_t(float y, float* sinp, float* cosp) {
 #ifndef WWB_SINCOSF_FUSE
 #define WWB_SINCOSF_FUSE 3
 #endif
-WWB_HD void sincosf(float x, float* s, float* c) { sincosf_t<WWB_SINCOSF_FUSE>(x, s, c); }
+WWB_HC void sincosf(float x, float* s, float* c) { sincosf_t<WWB_SINCOSF_FUSE>(x, s, c); }
 
 // ------------------------------------------------------------------------------ expm1f, tanhf
 /// fdlibm expm1f (float, no fused operations).
@@ -545,7 +564,7 @@ WWB_HD float expm1f(float x) {
 }
 
 /// fdlibm tanhf.
-WWB_HD float tanhf(float x) {
+WWB_HC float tanhf(float x) {
   const float one = 1.0f, two = 2.0f, tiny = 1.0e-30f;
   const uint32_t jx = asuint(x);
   const uint32_t ix = jx & 0x7fffffffu;
@@ -572,7 +591,7 @@ WWB_HD float tanhf(float x) {
 
 // ----------------------------------------------------------------------------- atanf, atan2f
 /// fdlibm atanf.
-WWB_HD float atanf(float x) {
+WWB_HC float atanf(float x) {
   const float one = 1.0f, huge = 1.0e30f;
   const float hi0 = asfloat(0x3eed6338u), hi1 = asfloat(0x3f490fdau), hi2 = asfloat(0x3f7b985eu),
               hi3 = asfloat(0x3fc90fdau);
@@ -696,11 +715,11 @@ WWB_HD float atan2f_t(float y, float x) {
 #ifndef WWB_ATAN2F_KLIM
 #define WWB_ATAN2F_KLIM 60
 #endif
-WWB_HD float atan2f(float y, float x) { return atan2f_t<WWB_ATAN2F_KLIM>(y, x); }
+WWB_HC float atan2f(float y, float x) { return atan2f_t<WWB_ATAN2F_KLIM>(y, x); }
 
 // ----------------------------------------------------------------------------------- log10f
 /// fdlibm log10f over logf.
-WWB_HD float log10f(float x) {
+WWB_HC float log10f(float x) {
   const float two25 = asfloat(0x4c000000u), ivln10 = asfloat(0x3ede5bd9u),
               log10_2hi = asfloat(0x3e9a2080u), log10_2lo = asfloat(0x355427dbu);
   int32_t hx = (int32_t)asuint(x);
@@ -764,7 +783,7 @@ __device__ static const double kExp2_64Dev[128] = WWB_EXP2_64_TAB;
 static const double kExp2_64Host[128] = WWB_EXP2_64_TAB;
 WWB_HD double exp2_64(unsigned i) {
 #if defined(__CUDA_ARCH__)
-  return __ldg(&kExp2_64Dev[i]);
+  return asdouble(tab_ld64(&kExp2_64Dev[i]));
 #else
   return kExp2_64Host[i];
 #endif
@@ -773,7 +792,7 @@ WWB_HD double exp2_64(unsigned i) {
 /// exp(x) in double: x = k ln2/64 + r, 2^(k/64) = 2^e 2^(j/64) from the double-double table,
 /// e^r by a degree-11 Taylor sum (|r| <= ln2/128). Accurate to about 1 ulp; not glibc's bits
 /// (W3SDB1 rounds the results it feeds to float).
-WWB_HD double exp_d(double x) {
+WWB_HC double exp_d(double x) {
   if (x != x) return x + x;
   if (x > 709.78) return asdouble(0x7ff0000000000000ULL);
   if (x < -745.2) return 0.0;
@@ -821,7 +840,7 @@ WWB_HD double expm1_small_d(double x) {
 }
 
 /// tanh(x) in double: expm1(2x) / (expm1(2x) + 2) for |x| < 0.5, 1 - 2 / (exp(2|x|) + 1) above.
-WWB_HD double tanh_d(double x) {
+WWB_HC double tanh_d(double x) {
   if (x != x) return x + x;
   const double ax = x < 0 ? -x : x;
   if (ax > 22.0) return x < 0 ? -1.0 : 1.0;

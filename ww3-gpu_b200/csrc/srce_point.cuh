@@ -9,12 +9,17 @@
 // row-shift form as in snl1_kernel.cu). Each statement keeps the reference's operand order;
 // MAX/MIN sites keep its operand order (mx(a,b) = a > b ? a : b, mn(a,b) = a < b ? a : b).
 //
-// Layout of one point's working set (floats, shared memory on the device):
-//   persistent  SPEC SPECINIT VSIN VDIN VSNL VDNL VSDB VSLN (NSPEC each), LLWS (NSPEC ints),
-//               WN1 CG1 DAM CBETA WNF (NK), DIRF (NTH), ST4 work (NK arrays), EB (NK doubles)
-//   transient   one region reused in turn by W3SIN4 (DSTAB), the DIA (UE and the eight
-//               interaction arrays), W3SDS4 (VSDS VDDS BRLAMBDA BTH PB PB2) and the update
-//               (VSBT VDBT and the four ordered-sum term arrays).
+// Layout of one point's working set (floats). What a serial chain reads, or what is read
+// everywhere, sits in the CTA's shared memory; arrays that only parallel loops touch sit in the
+// point's slice of a global scratch buffer, which stays in L2. That keeps the shared part near
+// 37 KB at 36x36, so four CTAs share an SM.
+//   shared      SPEC, LLWS (NSPEC ints), WN1 CG1 DAM CBETA WNF (NK), DIRF (NTH), the ST4 NK
+//               work arrays, EB (NK doubles), and one region reused in turn by the four
+//               ordered-sum term arrays, W3SPR4's chain terms, the DIA's UE, SA1 and SA2, and
+//               the closing band sums
+//   global      SPECINIT VSIN VDIN VSNL VDNL VSDB VSLN (NSPEC each), and one region reused in
+//               turn by W3SIN4 (DSTAB), the DIA (DA1P DA1M DA2P DA2M, DA1C + DA2C, CON),
+//               W3SDS4 (VSDS VDDS BRLAMBDA BTH PB PB2) and VSBT VDBT.
 #pragma once
 
 #include "snl1_kernel.cuh"
@@ -55,36 +60,47 @@ struct SrceSh {
   Sds4Sh sds4;
 };
 
+/// An offset with this bit is into the point's global scratch, otherwise into its shared part.
+constexpr int kInGlobal = 1 << 30;
+
+/// Whether W3SRCE's working set is split between shared memory and global scratch (four CTAs
+/// of 128 threads per SM) or held in shared memory whole (two CTAs of 256).
+#ifndef WWB_SRCE_SPLIT
+#define WWB_SRCE_SPLIT 1
+#endif
+constexpr bool kSrceSplit = WWB_SRCE_SPLIT != 0;
+
 /// Offsets (in floats) of the working set; see the file header.
 struct SrceLayout {
   int nspec, nk, nth;
   int spec, specinit, vsin, vdin, vsnl, vdnl, vsdb, vsln, llws;
   int wn1, cg1, dam, cbeta, wnf, dirf, sin4eb, spr4w, sds4w, sds4iw, ebd;
-  int trans, trans_len, total;
+  int ser, ser_len;      ///< shared region of the serial chains' operands
+  int trans, trans_len;  ///< global region of the parallel phases' arrays
+  int total_s, total_g;  ///< floats of shared memory and of global scratch per point
 };
 
-/// Floats of the DIA's per-point scratch (row-shift form).
-WWB_PD int dia_scratch(const Snl1Dev& p) {
-  return (p.nfrhgh + 1) * p.nth + 8 * (p.nfrchg + 1) * p.nth + p.nk;
+/// Floats of the DIA's per-point scratch (row-shift form) in shared memory (UE, SA1, SA2: the
+/// arrays its gathers read most) and in global memory (DA1P, DA1M, DA2P, DA2M, DA1C + DA2C,
+/// CON).
+WWB_PD int dia_shared(const Snl1Dev& p) {
+  return (p.nfrhgh + 1) * p.nth + 2 * (p.nfrchg + 1) * p.nth;
+}
+WWB_PD int dia_global(const Snl1Dev& p) {
+  return 4 * (p.nfrchg + 1) * p.nth + p.nspec + p.nk;
 }
 
-inline SrceLayout srce_layout(const st4::Params& q, const Snl1Dev& n) {
+inline SrceLayout srce_layout(const st4::Params& q, const Snl1Dev& n, bool split = kSrceSplit) {
   SrceLayout L{};
   const int ns = q.nspec, nk = q.nk, nth = q.nth;
   auto r4 = [](int x) { return (x + 3) & ~3; };
+  const int R = r4(ns);
   L.nspec = ns;
   L.nk = nk;
   L.nth = nth;
-  int o = 0;
-  L.spec = o; o += r4(ns);
-  L.specinit = o; o += r4(ns);
-  L.vsin = o; o += r4(ns);
-  L.vdin = o; o += r4(ns);
-  L.vsnl = o; o += r4(ns);
-  L.vdnl = o; o += r4(ns);
-  L.vsdb = o; o += r4(ns);
-  L.vsln = o; o += r4(ns);
-  L.llws = o; o += r4(ns);
+  int o = 0;  // shared
+  L.spec = o; o += R;
+  L.llws = o; o += R;
   L.wn1 = o; o += r4(nk);
   L.cg1 = o; o += r4(nk);
   L.dam = o; o += r4(nk);
@@ -93,33 +109,57 @@ inline SrceLayout srce_layout(const st4::Params& q, const Snl1Dev& n) {
   L.dirf = o; o += r4(nth);
   L.sin4eb = o; o += r4(7 * nk);  // W3SIN4's NK work (sin4_nk_work)
   L.spr4w = o; o += r4(5 * nk + 4);
-  L.sds4w = o; o += r4(18 * nk);  // SDS4's NSPEC arrays live in the transient region
+  L.sds4w = o; o += r4(18 * nk);
   L.sds4iw = o; o += r4(2 * nk);
   L.ebd = o; o += r4(2 * nk);  // NK doubles (8-byte aligned: o is a multiple of 4)
-  L.trans = o;
-  int t = 9 * r4(ns);
-  const int d = r4(dia_scratch(n));
-  if (d > t) t = d;
-  if (3 * r4(ns) > t) t = 3 * r4(ns);
+  L.ser = o;
+  int sl = 4 * R;  // the ordered-sum terms; W3SPR4's two chain arrays; the band sums (3 NK)
+  if (r4(dia_shared(n)) > sl) sl = r4(dia_shared(n));
+  if (r4(3 * nk) > sl) sl = r4(3 * nk);
+  L.ser_len = sl;
+  o += sl;
+  // The rest in global scratch, or (split false) after the shared part.
+  const int flag = split ? kInGlobal : 0;
+  int g = split ? 0 : o;
+  L.specinit = flag | g; g += R;
+  L.vsin = flag | g; g += R;
+  L.vdin = flag | g; g += R;
+  L.vsnl = flag | g; g += R;
+  L.vdnl = flag | g; g += R;
+  L.vsdb = flag | g; g += R;
+  L.vsln = flag | g; g += R;
+  L.trans = flag | g;
+  int t = 6 * R;  // W3SDS4's outputs and NSPEC work; W3SIN4's DSTAB is 3 NSPEC
+  if (r4(dia_global(n)) > t) t = r4(dia_global(n));
   L.trans_len = t;
-  L.total = o + t;
+  g += t;
+  L.total_s = split ? o : g;
+  L.total_g = split ? g : 0;
   return L;
 }
 
 // ---------------------------------------------------------------------------- the DIA, one point
 /// W3SNL1 for one point in the row-shift form (the arithmetic of snl1_rowshift_kernel):
-/// a (NSPEC), cg (NK) in; s, d (NSPEC) out; scratch dia_scratch(p) floats.
+/// a (NSPEC), cg (NK) in; s, d (NSPEC) out; scratch dia_shared(p) floats in ss (UE, SA1, SA2)
+/// and dia_global(p) floats in gs (DA1P, DA1M, DA2P, DA2M, DC = DA1C + DA2C, CON). DA1C and
+/// DA2C are read back only at their own bin, so their sum is kept (the same two roundings).
 WWB_PN void dia_point(const Cta& cta, const Snl1Dev& p, const float* a, const float* cg,
-                      float kdmean, float* s, float* d, float* scratch) {
+                      float kdmean, float* s, float* d, float* ss, float* gs) {
   const int nth = p.nth, nfr = p.nfr, nfrhgh = p.nfrhgh, nfrchg = p.nfrchg;
   const int nspec = p.nspec, nspecx = p.nspecx, nk = p.nk;
   const int alen = (nfrchg + 1) * nth;
-  float* const ue = scratch;
-  float* const arr = ue + (nfrhgh + 1) * nth;
-  float* const conx = arr + 8 * alen;
+  float* const ue = ss;
+  float* const sa1 = ue + (nfrhgh + 1) * nth;
+  float* const sa2 = sa1 + alen;
+  float* const da1p = gs;
+  float* const da1m = da1p + alen;
+  float* const da2p = da1m + alen;
+  float* const da2m = da2p + alen;
+  float* const dc = da2m + alen;
+  float* const conx = dc + nspec;
   PFOR(i, nth) {
     ue[i] = 0.0f;
-    for (int k = 0; k < 8; ++k) arr[k * alen + i] = 0.0f;
+    sa1[i] = sa2[i] = da1p[i] = da1m[i] = da2p[i] = da2m[i] = 0.0f;
   }
   PFOR(k, nk) conx[k] = kTpiInv / p.sig[k] * cg[k];
   // Section 1: CONS (snl1_team.hpp:383-390).
@@ -167,25 +207,16 @@ WWB_PN void dia_point(const Cta& cta, const Snl1Dev& p, const float* a, const fl
     const float sa2a = e00 * (ep2 * dal1 + em2 * dal2);
     const float sa2b = sa2a - ep2 * em2 * dal3;
     const int o = isp + nth;
-    arr[0 * alen + o] = factor * sa1b;
-    arr[1 * alen + o] = factor * sa2b;
-    arr[2 * alen + o] = ca * (sa1a + sa1b);
-    arr[3 * alen + o] = factor * (dal1 * e00 - dal3 * em1);
-    arr[4 * alen + o] = factor * (dal2 * e00 - dal3 * ep1);
-    arr[5 * alen + o] = ca * (sa2a + sa2b);
-    arr[6 * alen + o] = factor * (dal1 * e00 - dal3 * em2);
-    arr[7 * alen + o] = factor * (dal2 * e00 - dal3 * ep2);
+    sa1[o] = factor * sa1b;
+    sa2[o] = factor * sa2b;
+    if (isp < nspec) dc[isp] = ca * (sa1a + sa1b) + ca * (sa2a + sa2b);
+    da1p[o] = factor * (dal1 * e00 - dal3 * em1);
+    da1m[o] = factor * (dal2 * e00 - dal3 * ep1);
+    da2p[o] = factor * (dal1 * e00 - dal3 * em2);
+    da2m[o] = factor * (dal2 * e00 - dal3 * ep2);
   }
   cta.sync();
   {
-    const float* const sa1 = arr;
-    const float* const sa2 = arr + alen;
-    const float* const da1c = arr + 2 * alen;
-    const float* const da1p = arr + 3 * alen;
-    const float* const da1m = arr + 4 * alen;
-    const float* const da2c = arr + 5 * alen;
-    const float* const da2p = arr + 6 * alen;
-    const float* const da2m = arr + 7 * alen;
     PFOR(isp, nspec) {
       const int ifr0 = isp / nth, ith = isp - ifr0 * nth;
       int c[8];
@@ -207,7 +238,7 @@ WWB_PN void dia_point(const Cta& cta, const Snl1Dev& p, const float* a, const fl
                              p.awg[5] * (sa1[r8 + c[2]] + sa2[r8 + c[6]]) +
                              p.awg[6] * (sa1[r7 + c[3]] + sa2[r7 + c[7]]) +
                              p.awg[7] * (sa1[r7 + c[2]] + sa2[r7 + c[6]]));
-      d[isp] = -2.0f * (da1c[o] + da2c[o]) + p.swg[0] * (da1p[r6 + c[5]] + da2p[r6 + c[1]]) +
+      d[isp] = -2.0f * dc[isp] + p.swg[0] * (da1p[r6 + c[5]] + da2p[r6 + c[1]]) +
                p.swg[1] * (da1p[r6 + c[4]] + da2p[r6 + c[0]]) +
                p.swg[2] * (da1p[r5 + c[5]] + da2p[r5 + c[1]]) +
                p.swg[3] * (da1p[r5 + c[4]] + da2p[r5 + c[0]]) +
@@ -229,20 +260,23 @@ struct SrceCtx {
   const Fields* f;
   const Snl1Dev* n;
   SrceIn in;
-  float* w;  ///< the working set (SrceLayout)
+  float* w;   ///< the shared part of the working set (SrceLayout)
+  float* gw;  ///< the global part
   const SrceLayout* L;
   SrceSh* sh;
 };
 
-WWB_PD float* at(const SrceCtx& x, int off) { return x.w + off; }
+WWB_PD float* at(const SrceCtx& x, int off) {
+  return (off & kInGlobal) ? x.gw + (off & ~kInGlobal) : x.w + off;
+}
 
 /// W3SPR4 with W3SRCE's arguments (:1080, :1119, :1878, :2012).
 WWB_PD void srce_spr4(const Cta& cta, const SrceCtx& x) {
   const SrceLayout& L = *x.L;
-  // The ELCS / ELSN terms go to the transient region's rows 5 and 6 (free at every call site).
+  // The ELCS / ELSN terms go to the shared serial region (free at every call site).
   spr4(cta, *x.q, *x.f, at(x, L.spec), at(x, L.cg1), at(x, L.wn1), x.in.u10abs, x.in.u10dir,
        x.sh->tauwx, x.sh->tauwy, reinterpret_cast<const int*>(at(x, L.llws)), x.sh->r,
-       at(x, L.spr4w), at(x, L.trans) + 5 * ((L.nspec + 3) & ~3));
+       at(x, L.spr4w), at(x, L.ser));
 }
 
 /// W3SIN4 with W3SRCE's arguments (:1100, :1239, :2007).
@@ -379,7 +413,7 @@ WWB_PD void srce_step_a(const Cta& cta, const SrceCtx& x) {
 WWB_PD void srce_dia(const Cta& cta, const SrceCtx& x) {
   const SrceLayout& L = *x.L;
   dia_point(cta, *x.n, at(x, L.spec), at(x, L.cg1), x.sh->r.wnmean * x.sh->depth,
-            at(x, L.vsnl), at(x, L.vdnl), at(x, L.trans));
+            at(x, L.vsnl), at(x, L.vdnl), at(x, L.ser), at(x, L.trans));
 }
 
 /// The CTA-wide MIN of v over the threads' values with mn(), combined into *dst = mn(*dst, .).
@@ -420,10 +454,11 @@ WWB_PN void srce_step_c(const Cta& cta, const SrceCtx& x) {
   float* const brlambda = T + 2 * R;
   float* const vsbt = T + 3 * R;  // after W3SDS4 (its BTH, PB, PB2 live at 3R..5R)
   float* const vdbt = T + 4 * R;
-  float* const t_phiaw = T + 5 * R;
-  float* const t_phibbl = T + 6 * R;
-  float* const t_wc = T + 7 * R;
-  float* const t_hs = T + 8 * R;
+  float* const S = at(x, L.ser);  // the ordered sums' terms, read by one thread each
+  float* const t_phiaw = S;
+  float* const t_phibbl = S + R;
+  float* const t_wc = S + 2 * R;
+  float* const t_hs = S + 3 * R;
   const float* const vsin = at(x, L.vsin);
   const float* const vdin = at(x, L.vdin);
   float* const vsnl = at(x, L.vsnl);
@@ -709,7 +744,7 @@ WWB_PN void srce_finish(const Cta& cta, const SrceCtx& x) {
   const int nk = p.nk, nth = p.nth, nspec = p.nspec;
   float* const spec = at(x, L.spec);
   const float* const specinit = at(x, L.specinit);
-  float* const T = at(x, L.trans);  // per-IK band sums: eband, a1band, b1band
+  float* const T = at(x, L.ser);  // per-IK band sums: eband, a1band, b1band
   PFOR(ik, nk) {
     float eband = 0.0f, a1band = 0.0f, b1band = 0.0f;
     for (int ith = 0; ith < nth; ++ith) {

@@ -33,8 +33,29 @@ struct SrceStep {
   float dtg;
 };
 
-/// Threads of every ST4 / W3SRCE CTA (one CTA per point).
+/// Threads of every ST4 CTA (one CTA per point).
 constexpr int kSt4Block = 256;
+
+/// Threads of a W3SRCE CTA, and the CTAs per SM it is built for: one point's serial chains
+/// leave most of its warps waiting at barriers, so more points per SM (their shared part fits
+/// four times, their registers four times 128 threads) beat more threads per point.
+constexpr int kSrceBlock = pt::kSrceSplit ? 128 : 256;
+constexpr int kSrceMinBlocks = pt::kSrceSplit ? 4 : 2;
+
+/// One grid's W3SRCE work buffers: the work queue's counter and the global part of the resident
+/// CTAs' working sets (grow-only; it stays in L2 at these sizes). Owned by the grid's context.
+struct SrceWork {
+  int* counter = nullptr;
+  float* scratch = nullptr;
+  size_t scratch_n = 0;
+  void release() {
+    if (counter) cudaFree(counter);
+    if (scratch) cudaFree(scratch);
+    counter = nullptr;
+    scratch = nullptr;
+    scratch_n = 0;
+  }
+};
 
 /// Bytes of dynamic shared memory of the W3SRCE kernel for these tables (the working set of
 /// one point); 0 when it exceeds the 227 KiB a CTA can have.
@@ -61,12 +82,12 @@ void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
                  cudaStream_t st);
 
 /// W3SRCE for npts points on a persistent grid whose CTAs take points from a work queue
-/// (counter, zeroed here), so points with many substeps do not hold up the rest. Point n's
+/// (work.counter, zeroed here), so points with many substeps do not hold up the rest. Point n's
 /// spectrum is spec + n * nspec, or, with jsea non-null, the resident VA column
 /// spec + jsea[n] * nspec. Per-point packets as ww_srce_batch takes them (device pointers).
 void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int npts,
                  float* spec, const int* jsea, const float* wn1, const float* cg1,
                  const float* pin, float* psc, float* whitecap, float* taubbl, float* tauice,
-                 int* shave, int* counter, cudaStream_t st);
+                 int* shave, SrceWork& work, cudaStream_t st);
 
 }  // namespace wwb

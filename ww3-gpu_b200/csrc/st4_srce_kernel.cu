@@ -84,15 +84,16 @@ __global__ void __launch_bounds__(kSt4Block) spr4_kernel(
   }
 }
 
-__global__ void __launch_bounds__(kSt4Block) srce_kernel(
+__global__ void __launch_bounds__(kSrceBlock, kSrceMinBlocks) srce_kernel(
     const SrceDev* __restrict__ d, SrceStep step, int npts, float* spec, const int* jsea,
     const float* wn1, const float* cg1, const float* pin, float* psc, float* whitecap,
-    float* taubbl, float* tauice, int* shave, int* counter) {
+    float* taubbl, float* tauice, int* shave, int* counter, float* scratch) {
   extern __shared__ __align__(16) float w[];
   __shared__ pt::SrceSh sh;
   __shared__ int cur;
   const pt::SrceLayout& L = d->L;
   const int ns = L.nspec, nk = L.nk;
+  float* const gw = scratch + static_cast<size_t>(blockIdx.x) * static_cast<size_t>(L.total_g);
   const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
   for (;;) {
     if (threadIdx.x == 0) cur = atomicAdd(counter, 1);
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(kSt4Block) srce_kernel(
     const pt::SrceCtx x{&d->p, &d->g, &d->q, &d->f, &d->n,
                         pt::srce_in(step.it, step.inflags24, step.flogrd57, step.flogrd58,
                                     step.dtg, pin + static_cast<size_t>(n) * srce::NPIN),
-                        w, &L, &sh};
+                        w, gw, &L, &sh};
     pt::srce_point(cta, x);
     for (int i = threadIdx.x; i < ns; i += blockDim.x) sp[i] = w[L.spec + i];
     if (threadIdx.x == 0)
@@ -127,11 +128,11 @@ __global__ void __launch_bounds__(kSt4Block) srce_kernel(
 
 /// Resident CTAs per SM of a kernel at this shared memory, at least 1.
 template <class K>
-int resident_grid(K k, size_t smem, int npts) {
+int resident_grid(K k, size_t smem, int npts, int block = kSt4Block) {
   WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
   int per_sm = 0;
-  WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kSt4Block, smem));
+  WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem));
   if (per_sm < 1) throw CudaError(cudaErrorInvalidConfiguration, "st4/srce occupancy");
   const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
   return static_cast<int>(npts < resident ? npts : resident);
@@ -140,7 +141,7 @@ int resident_grid(K k, size_t smem, int npts) {
 }  // namespace
 
 size_t srce_smem_bytes(const pt::SrceLayout& L) {
-  const size_t b = static_cast<size_t>(L.total) * sizeof(float) + 16;
+  const size_t b = static_cast<size_t>(L.total_s) * sizeof(float) + 16;
   return b + sizeof(pt::SrceSh) <= 227 * 1024 ? b : 0;
 }
 
@@ -187,14 +188,26 @@ void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
 void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int npts,
                  float* spec, const int* jsea, const float* wn1, const float* cg1,
                  const float* pin, float* psc, float* whitecap, float* taubbl, float* tauice,
-                 int* shave, int* counter, cudaStream_t st) {
+                 int* shave, SrceWork& work, cudaStream_t st) {
   if (npts <= 0) return;
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
-  const int grid = resident_grid(srce_kernel, smem, npts);
-  WWB_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), st));
-  srce_kernel<<<grid, kSt4Block, smem, st>>>(d, step, npts, spec, jsea, wn1, cg1, pin, psc,
-                                             whitecap, taubbl, tauice, shave, counter);
+  const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock);
+  const size_t need = static_cast<size_t>(grid) * static_cast<size_t>(L.total_g);
+  if (work.counter == nullptr) WWB_CHECK(cudaMalloc(&work.counter, sizeof(int)));
+  if (need > work.scratch_n) {  // (nothing when the working set is all shared)
+    // The previous launches on this grid's stream may still read the old buffer.
+    WWB_CHECK(cudaStreamSynchronize(st));
+    if (work.scratch) WWB_CHECK(cudaFree(work.scratch));
+    work.scratch = nullptr;
+    work.scratch_n = 0;
+    WWB_CHECK(cudaMalloc(&work.scratch, need * sizeof(float)));
+    work.scratch_n = need;
+  }
+  WWB_CHECK(cudaMemsetAsync(work.counter, 0, sizeof(int), st));
+  srce_kernel<<<grid, kSrceBlock, smem, st>>>(d, step, npts, spec, jsea, wn1, cg1, pin, psc,
+                                              whitecap, taubbl, tauice, shave, work.counter,
+                                              work.scratch);
   WWB_CHECK(cudaGetLastError());
 }
 
