@@ -242,8 +242,30 @@ int ww_xyp3_mpi_pack(int igrid, float* va, int nspec, int nsealm, const int* isp
 int ww_xyp3_mpi_unpack(int igrid, float* va, int nspec, int nsealm, const int* isps, int nisp,
                        const float* buf);
 
-/* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* call (the reference
- * returns it only). */
+/* B200 extension; the reference has no C entry for it (its W3MAP3 runs inside the W3WAVE port
+ * as one serial thread, prop_map3.hpp:100-340). W3MAP3 on the device, as ordered stream
+ * compactions with the reference's results: mapsta (NY*NX) and mapsf (NSEA,3) in; mapx2,
+ * mapy2, mapaxy (NY*NX), mapcxy (NSEA) and counts[8] = NMX0, NMX1, NMX2, NMY0, NMY1, NMY2,
+ * NACT, NCENT out when gtype < 3 (GTYPE >= 3 leaves them); mapth2 ((NK+2)*NTH) and mapwn2
+ * (NSPEC+NTH) written only when mapth2[0] is 0. List entries past the counters keep their
+ * values. MAPSF must address cells of the grid (else BAD_SHAPE). */
+int ww_map3(int nx, int ny, int nsea, int nk, int nth, int gtype, const int* mapsta,
+            const int* mapsf, int* mapx2, int* mapy2, int* mapaxy, int* mapcxy, int* mapth2,
+            int* mapwn2, int* counts);
+
+/* ww_map3 on device arrays, on the caller's CUDA stream; counts (host, 8 ints) after a sync.
+ * MAPSF is not checked (it is device memory). */
+int ww_map3_device(int nx, int ny, int nsea, int nk, int nth, int gtype, const int* mapsta,
+                   const int* mapsf, int* mapx2, int* mapy2, int* mapaxy, int* mapcxy,
+                   int* mapth2, int* mapwn2, int* counts, void* stream);
+
+/* B200 extension (prop_mapt.hpp:55-79): W3MAPT, MAPTRN (NY*NX, 0/1) of the NSEA sea cells from
+ * ATRNX/ATRNY (NY*NX, -1:1); other cells keep their values. */
+int ww_mapt(int nx, int ny, int nsea, const int* mapsf, const float* atrnx, const float* atrny,
+            int* maptrn);
+
+/* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* / ww_map3* / ww_mapt
+ * call (the reference returns it only). */
 int ww_prop3_last_error(void);
 
 /* ---------------------------------------------------------------- ST4 source terms (W3SRC4MD) */

@@ -256,6 +256,41 @@ def ref_w3map3(nx, ny, nsea, nk, nth, mapsta, mapsf):
     return out[0], out[1], out[2], out[3], out[6]
 
 
+def ref_w3map3_all(nx, ny, nsea, nk, nth, mapsta, mapsf, mapth2=None):
+    """The reference's W3MAP3 with every output: dict of mapx2, mapy2, mapaxy, mapcxy, mapth2,
+    mapwn2, counts (the maps zero-initialised, mapth2 as given or zero)."""
+    L = ref_lib()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.ref_w3map3.argtypes = [I, I, I, I, I] + [P] * 9
+    L.ref_w3map3.restype = I
+    nxy = nx * ny
+    out = {"mapx2": np.zeros(nxy, np.int32), "mapy2": np.zeros(nxy, np.int32),
+           "mapaxy": np.zeros(nxy, np.int32), "mapcxy": np.zeros(max(nsea, 1), np.int32),
+           "mapth2": (np.zeros((nk + 2) * nth, np.int32) if mapth2 is None
+                      else np.array(mapth2, np.int32, copy=True)),
+           "mapwn2": np.zeros(nk * nth + nth, np.int32), "counts": np.zeros(8, np.int32)}
+    sta = np.ascontiguousarray(mapsta, np.int32)
+    sf = np.ascontiguousarray(mapsf, np.int32)
+    L.ref_w3map3(nx, ny, nsea, nk, nth, sta.ctypes.data, sf.ctypes.data,
+                 *[out[k].ctypes.data for k in ("mapx2", "mapy2", "mapaxy", "mapcxy", "mapth2",
+                                                "mapwn2", "counts")])
+    return out
+
+
+def ref_w3mapt(nx, ny, nsea, mapsf, atrnx, atrny, maptrn):
+    """The reference's W3MAPT; returns MAPTRN."""
+    L = ref_lib()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.ref_w3mapt.argtypes = [I, I, I, P, P, P, P]
+    L.ref_w3mapt.restype = I
+    t = np.array(maptrn, np.int32, copy=True)
+    sf = np.ascontiguousarray(mapsf, np.int32)
+    ax = np.ascontiguousarray(atrnx, np.float32)
+    ay = np.ascontiguousarray(atrny, np.float32)
+    L.ref_w3mapt(nx, ny, nsea, sf.ctypes.data, ax.ctypes.data, ay.ctypes.data, t.ctypes.data)
+    return t
+
+
 XYP3_ARGS = ("mapsf", "clats", "sig", "ecos", "esin", "dpdx", "dpdy", "dqdx", "dqdy", "gsqrt",
              "atrnx", "atrny", "mapx2", "mapy2", "mapaxy", "mapcxy", "maptrn", "mapsta", "cg",
              "cx", "cy")

@@ -82,6 +82,22 @@ extern "C" int ref_w3map3(int nx, int ny, int nsea, int nk, int nth, const int* 
   return 0;
 }
 
+// W3MAPT of the reference (kokkos/src/ww_kokkos/prop_mapt.hpp:55-79): MAPTRN of the NSEA sea
+// cells from ATRNX/ATRNY (NY*NX, -1:1), column-major.
+#include "ww_kokkos/prop_mapt.hpp"
+
+extern "C" int ref_w3mapt(int nx, int ny, int nsea, const int* mapsf, const float* atrnx,
+                          const float* atrny, int* maptrn) {
+  using namespace ww::prop;
+  using H = Kokkos::HostSpace;
+  const size_t nxy = static_cast<size_t>(nx) * ny;
+  Kokkos::View<const int**, Kokkos::LayoutLeft, H> sf(mapsf, static_cast<size_t>(nsea), 3);
+  Kokkos::View<const float**, Kokkos::LayoutLeft, H> ax(atrnx, nxy, 3), ay(atrny, nxy, 3);
+  Kokkos::View<int*, Kokkos::LayoutLeft, H> t(maptrn, nxy);
+  w3mapt(Kokkos::DefaultHostExecutionSpace(), nsea, sf, ax, ay, t);
+  return 0;
+}
+
 // INSIN4(FLTABS=.TRUE.) of the reference (kokkos/src/ww_kokkos/st4_insin4.cpp, st4_tabu_*.cpp),
 // to build the ST4 tables of synthetic grids for the tests. rpar/ipar are the ST4 packets
 // (st4_params.hpp:79-154); sig, dsip are SIG(0:MK+1), DSIP(0:MK+1). Out, column-major with the

@@ -46,6 +46,7 @@ EXPORTS = (
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
+    "ww_map3", "ww_map3_device", "ww_mapt",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -384,6 +385,41 @@ def va_host_write(igrid, va):
 XYP3_ARRAYS = ("mapsf", "clats", "sig", "ecos", "esin", "dpdx", "dpdy", "dqdx", "dqdy", "gsqrt",
                "atrnx", "atrny", "mapx2", "mapy2", "mapaxy", "mapcxy", "maptrn", "mapsta", "cg",
                "cx", "cy")
+
+
+def map3(nx, ny, nsea, nk, nth, mapsta, mapsf, gtype=1, mapth2=None):
+    """W3MAP3 through ww_map3: returns (status, dict of mapx2, mapy2, mapaxy, mapcxy, mapth2,
+    mapwn2, counts). mapsta is MAPSTA(NY,NX) flattened column-major, mapsf MAPSF(NSEA,3)."""
+    L = lib()
+    init()
+    nxy = nx * ny
+    out = {"mapx2": np.zeros(nxy, np.int32), "mapy2": np.zeros(nxy, np.int32),
+           "mapaxy": np.zeros(nxy, np.int32), "mapcxy": np.zeros(max(nsea, 1), np.int32),
+           "mapth2": (np.zeros((nk + 2) * nth, np.int32) if mapth2 is None
+                      else np.array(mapth2, np.int32, copy=True)),
+           "mapwn2": np.zeros(nk * nth + nth, np.int32), "counts": np.zeros(8, np.int32)}
+    sta = np.ascontiguousarray(mapsta, np.int32)
+    sf = np.ascontiguousarray(mapsf, np.int32)
+    L.ww_map3.argtypes = [_I] * 6 + [_P] * 9
+    L.ww_map3.restype = _I
+    rc = L.ww_map3(nx, ny, nsea, nk, nth, gtype, sta.ctypes.data, sf.ctypes.data,
+                   *[out[k].ctypes.data for k in ("mapx2", "mapy2", "mapaxy", "mapcxy", "mapth2",
+                                                  "mapwn2", "counts")])
+    return rc, out
+
+
+def mapt(nx, ny, nsea, mapsf, atrnx, atrny, maptrn):
+    """W3MAPT through ww_mapt; returns (status, maptrn)."""
+    L = lib()
+    init()
+    t = np.array(maptrn, np.int32, copy=True)
+    sf = np.ascontiguousarray(mapsf, np.int32)
+    ax = np.ascontiguousarray(atrnx, np.float32)
+    ay = np.ascontiguousarray(atrny, np.float32)
+    L.ww_mapt.argtypes = [_I, _I, _I, _P, _P, _P, _P]
+    L.ww_mapt.restype = _I
+    rc = L.ww_mapt(nx, ny, nsea, sf.ctypes.data, ax.ctypes.data, ay.ctypes.data, t.ctypes.data)
+    return rc, t
 
 
 def xyp3_batch(case, igrid=None, va=None):

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ktp3_kernel.cuh"
+#include "map3_kernel.cuh"
 #include "staging.hpp"
 #include "va.hpp"
 #include "wwb_common.hpp"
@@ -372,6 +373,28 @@ int xyp3_mpi_move(bool unpack, int igrid, float* va, int nspec, int nsealm, cons
   return WW_KOKKOS_OK;
 }
 
+Map3Work& map3_work() {
+  static auto* w = new Map3Work();
+  return *w;
+}
+
+/// W3MAP3's inputs must address the grid: MAPSF's IX, IY in range and IXY = IY + (IX-1)*NY.
+int map3_check(int nx, int ny, int nsea, int nk, int nth, const int* mapsta, const int* mapsf,
+               const void* mapx2, const void* mapy2, const void* mapaxy, const void* mapcxy,
+               const void* mapth2, const void* mapwn2, const void* counts, bool host_mapsf) {
+  if (nx < 1 || ny < 1 || nsea < 0 || nk < 1 || nth < 1 ||
+      static_cast<long long>(nx) * ny > (1ll << 31) - 1 || !mapsta || (nsea > 0 && !mapsf) ||
+      !mapx2 || !mapy2 || !mapaxy || (nsea > 0 && !mapcxy) || !mapth2 || !mapwn2 || !counts)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_map3: bad sizes or null pointer");
+  if (host_mapsf)
+    for (int i = 0; i < nsea; ++i) {
+      const int ix = mapsf[i], iy = mapsf[nsea + i], ixy = mapsf[2 * nsea + i];
+      if (ix < 1 || ix > nx || iy < 1 || iy > ny || ixy != (ix - 1) * ny + iy)
+        return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_map3: MAPSF is not a map of cells of the grid");
+    }
+  return WW_KOKKOS_OK;
+}
+
 template <class F>
 int guarded(F&& f) {
   try {
@@ -385,7 +408,10 @@ int guarded(F&& f) {
 
 }  // namespace
 
-void release_prop3_staging() { staging().release(); }
+void release_prop3_staging() {
+  staging().release();
+  map3_work().release();
+}
 
 }  // namespace wwb
 
@@ -488,6 +514,103 @@ int ww_xyp3_mpi_unpack(int igrid, float* va, int nspec, int nsealm, const int* i
                        const float* buf) {
   return guarded([&] {
     return xyp3_mpi_move(true, igrid, va, nspec, nsealm, isps, nisp, const_cast<float*>(buf));
+  });
+}
+
+int ww_map3(int nx, int ny, int nsea, int nk, int nth, int gtype, const int* mapsta,
+            const int* mapsf, int* mapx2, int* mapy2, int* mapaxy, int* mapcxy, int* mapth2,
+            int* mapwn2, int* counts) {
+  return guarded([&] {
+    if (const int rc = map3_check(nx, ny, nsea, nk, nth, mapsta, mapsf, mapx2, mapy2, mapaxy,
+                                  mapcxy, mapth2, mapwn2, counts, true);
+        rc != WW_KOKKOS_OK)
+      return rc;
+    if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+    timers::Region t_call("map3.call");
+    Staging& st = staging();
+    cudaStream_t s = runtime().stream;
+    const size_t nxy = static_cast<size_t>(nx) * ny, nth2 = static_cast<size_t>(nk + 2) * nth,
+                 nwn2 = static_cast<size_t>(nk) * nth + nth;
+    // Slots past the PR3 calls' own. The maps come in as well as out: entries past the
+    // counters keep the caller's values.
+    constexpr int k0 = 80;
+    const int* d_sta = st.in(k0, mapsta, nxy, s);
+    const int* d_sf = st.in(k0 + 1, mapsf, 3 * static_cast<size_t>(nsea), s);
+    int* d_x2 = st.in(k0 + 2, mapx2, nxy, s);
+    int* d_y2 = st.in(k0 + 3, mapy2, nxy, s);
+    int* d_axy = st.in(k0 + 4, mapaxy, nxy, s);
+    int* d_cxy = st.in(k0 + 5, mapcxy, static_cast<size_t>(nsea), s);
+    int* d_th2 = st.in(k0 + 6, mapth2, nth2, s);
+    int* d_wn2 = st.in(k0 + 7, mapwn2, nwn2, s);
+    Map3Work& w = map3_work();
+    launch_map3(Map3Grid{nx, ny, nsea, nk, nth, gtype}, d_sta, d_sf, d_x2, d_y2, d_axy, d_cxy,
+                d_th2, d_wn2, w, s);
+    auto out = [&](int* h, const int* d, size_t n) {
+      if (n) WWB_CHECK(cudaMemcpyAsync(h, d, n * sizeof(int), cudaMemcpyDeviceToHost, s));
+    };
+    if (gtype < 3) {
+      out(mapx2, d_x2, nxy);
+      out(mapy2, d_y2, nxy);
+      out(mapaxy, d_axy, nxy);
+      out(mapcxy, d_cxy, static_cast<size_t>(nsea));
+      out(counts, w.counts, 8);
+    }
+    out(mapth2, d_th2, nth2);
+    out(mapwn2, d_wn2, nwn2);
+    WWB_CHECK(cudaStreamSynchronize(s));
+    g_prop3.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_map3_device(int nx, int ny, int nsea, int nk, int nth, int gtype, const int* mapsta,
+                   const int* mapsf, int* mapx2, int* mapy2, int* mapaxy, int* mapcxy,
+                   int* mapth2, int* mapwn2, int* counts, void* stream) {
+  return guarded([&] {
+    if (const int rc = map3_check(nx, ny, nsea, nk, nth, mapsta, mapsf, mapx2, mapy2, mapaxy,
+                                  mapcxy, mapth2, mapwn2, counts, false);
+        rc != WW_KOKKOS_OK)
+      return rc;
+    if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Map3Work& w = map3_work();
+    launch_map3(Map3Grid{nx, ny, nsea, nk, nth, gtype}, mapsta, mapsf, mapx2, mapy2, mapaxy,
+                mapcxy, mapth2, mapwn2, w, s);
+    if (gtype < 3) {
+      WWB_CHECK(cudaMemcpyAsync(counts, w.counts, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      WWB_CHECK(cudaStreamSynchronize(s));
+    }
+    g_prop3.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_mapt(int nx, int ny, int nsea, const int* mapsf, const float* atrnx, const float* atrny,
+            int* maptrn) {
+  return guarded([&] {
+    if (nx < 1 || ny < 1 || nsea < 0 || (nsea > 0 && (!mapsf || !atrnx || !atrny || !maptrn)))
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_mapt: bad sizes or null pointer");
+    const long long nxy = static_cast<long long>(nx) * ny;
+    for (int i = 0; i < nsea; ++i)
+      if (mapsf[2 * nsea + i] < 1 || mapsf[2 * nsea + i] > nxy)
+        return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_mapt: MAPSF(:,3) outside the grid");
+    if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+    if (nsea == 0) {
+      g_prop3.ok();
+      return static_cast<int>(WW_KOKKOS_OK);
+    }
+    Staging& st = staging();
+    cudaStream_t s = runtime().stream;
+    constexpr int k0 = 90;
+    const int* d_sf = st.in(k0, mapsf, 3 * static_cast<size_t>(nsea), s);
+    const float* d_x = st.in(k0 + 1, atrnx, 3 * static_cast<size_t>(nxy), s);
+    const float* d_y = st.in(k0 + 2, atrny, 3 * static_cast<size_t>(nxy), s);
+    int* d_t = st.in(k0 + 3, maptrn, static_cast<size_t>(nxy), s);
+    launch_mapt(nsea, static_cast<int>(nxy), d_sf, d_x, d_y, d_t, s);
+    WWB_CHECK(cudaMemcpyAsync(maptrn, d_t, sizeof(int) * nxy, cudaMemcpyDeviceToHost, s));
+    WWB_CHECK(cudaStreamSynchronize(s));
+    g_prop3.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
   });
 }
 

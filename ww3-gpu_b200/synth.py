@@ -245,8 +245,8 @@ def land_mask(nx, ny, seed=0, sea_fraction=0.7, smooth=6):
     rng = np.random.default_rng(seed)
     f = rng.standard_normal((ny, nx))
     k = np.exp(-0.5 * (np.arange(-3 * smooth, 3 * smooth + 1) / smooth) ** 2)
-    f = np.apply_along_axis(lambda r: np.convolve(np.concatenate([r[-3 * smooth:], r,
-                                                                  r[:3 * smooth]]), k, "valid"),
+    # longitude: periodic padding (wraps as often as needed when NX is below the kernel)
+    f = np.apply_along_axis(lambda r: np.convolve(np.pad(r, 3 * smooth, mode="wrap"), k, "valid"),
                             1, f)
     # latitude: edge-padded, so the mask keeps NY rows whatever NY is against the kernel
     f = np.apply_along_axis(lambda c: np.convolve(np.pad(c, 3 * smooth, mode="edge"), k, "valid"),
@@ -255,6 +255,24 @@ def land_mask(nx, ny, seed=0, sea_fraction=0.7, smooth=6):
     sea[0, :] = False
     sea[-1, :] = False
     return sea
+
+
+def sea_grid(nx, ny, seed=0, sea_fraction=0.7, boundary=0.02, excluded=0.01):
+    """A seeded NX x NY lon/lat grid's MAPSTA (1 active sea, 2 boundary input, -1 excluded sea,
+    0 land; rows 1 and NY land) flattened column-major as MAPSTA(NY,NX), and MAPSF(NSEA,3) of
+    its sea points numbered row by row (IY outer), as W3GRID numbers them."""
+    rng = np.random.default_rng(seed + 101)
+    sea = land_mask(nx, ny, seed=seed, sea_fraction=sea_fraction)
+    sta = np.where(sea, 1, 0).astype(np.int32)  # (NY, NX)
+    u = rng.uniform(0.0, 1.0, sta.shape)
+    sta[sea & (u < boundary)] = 2
+    sta[sea & (u >= boundary) & (u < boundary + excluded)] = -1
+    iy, ix = np.nonzero(sta != 0)  # row-major over (IY, IX): IY outer, IX inner
+    ix = (ix + 1).astype(np.int32)
+    iy = (iy + 1).astype(np.int32)
+    mapsf = np.concatenate([ix, iy, (ix - 1) * ny + iy]).astype(np.int32)
+    mapsta = np.ascontiguousarray(sta.T).reshape(-1).astype(np.int32)
+    return mapsta, mapsf, int(ix.size)
 
 
 def xyp3_case(nx=48, ny=32, seed=0, nk=36, nth=36, iclose=2, flcur=True, flbpi=True,
