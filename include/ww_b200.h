@@ -264,8 +264,19 @@ int ww_map3_device(int nx, int ny, int nsea, int nk, int nth, int gtype, const i
 int ww_mapt(int nx, int ny, int nsea, const int* mapsf, const float* atrnx, const float* atrny,
             int* maptrn);
 
-/* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* / ww_map3* / ww_mapt
- * call (the reference returns it only). */
+/* B200 extension (updt_utrn.hpp:93-362, W3UTRN of w3updtmd.F90:2809-3194): the transparencies
+ * ATRNX/ATRNY (NY*NX, -1:1) from TRNX/TRNY (NY*NX), the ice concentration ICE (0:NSEA) and the
+ * icebergs BERG (NSEA) of grid (NX, NY) with NSEA sea points (MAPSF (NSEA,3), MAPSTA (NY,NX),
+ * HPFAC/HQFAC (NY,NX)). trny_before is the REAL just before TRNY(1) in the caller's memory
+ * (read as TRNY(0) for a sea point in cell 1 under TRFLAG 1, 3, 5). The ice arrays may be null
+ * when TRFLAG < 3. */
+int ww_utrn(int nx, int ny, int nsea, int trflag, float fice0, float ficen, float ficel,
+            float ffacberg, int flagll, float trny_before, const float* trnx, const float* trny,
+            const int* mapsf, const int* mapsta, const float* hpfac, const float* hqfac,
+            const float* ice, const float* berg, float* atrnx, float* atrny);
+
+/* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* / ww_map3* / ww_mapt /
+ * ww_utrn call (the reference returns it only). */
 int ww_prop3_last_error(void);
 
 /* ---------------------------------------------------------------- ST4 source terms (W3SRC4MD) */

@@ -291,6 +291,25 @@ def ref_w3mapt(nx, ny, nsea, mapsf, atrnx, atrny, maptrn):
     return t
 
 
+def ref_w3utrn(nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, flagll, trny_before,
+               trnx, trny, mapsf, mapsta, hpfac, hqfac, ice, berg):
+    """The reference's W3UTRN; returns (atrnx, atrny), each 3*NX*NY column-major."""
+    L = ref_lib()
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.ref_w3utrn.argtypes = [I] * 4 + [F] * 4 + [I, F] + [P] * 10
+    L.ref_w3utrn.restype = I
+    nxy = nx * ny
+    ax = np.zeros(3 * nxy, np.float32)
+    ay = np.zeros(3 * nxy, np.float32)
+    keep = [np.ascontiguousarray(a, t) for a, t in ((trnx, np.float32), (trny, np.float32),
+                                                     (mapsf, np.int32), (mapsta, np.int32),
+                                                     (hpfac, np.float32), (hqfac, np.float32),
+                                                     (ice, np.float32), (berg, np.float32))]
+    L.ref_w3utrn(nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, int(flagll), trny_before,
+                 *[k.ctypes.data for k in keep], ax.ctypes.data, ay.ctypes.data)
+    return ax, ay
+
+
 XYP3_ARGS = ("mapsf", "clats", "sig", "ecos", "esin", "dpdx", "dpdy", "dqdx", "dqdy", "gsqrt",
              "atrnx", "atrny", "mapx2", "mapy2", "mapaxy", "mapcxy", "maptrn", "mapsta", "cg",
              "cx", "cy")

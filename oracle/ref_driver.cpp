@@ -8,6 +8,7 @@
 // it, nor for W3KTP3/W3XYP3 (ww_ktp3_batch, ww_xyp3_batch: prop3_shim.cpp) and the resident VA
 // (ww_va_*: resident_shim.cpp). Used by the tests and by bench.py's reference arm only.
 #include <Kokkos_Core.hpp>
+#include <vector>
 
 #include "ww_kokkos/snl1_config.hpp"
 #include "ww_kokkos/snl1_tables.hpp"
@@ -95,6 +96,47 @@ extern "C" int ref_w3mapt(int nx, int ny, int nsea, const int* mapsf, const floa
   Kokkos::View<const float**, Kokkos::LayoutLeft, H> ax(atrnx, nxy, 3), ay(atrny, nxy, 3);
   Kokkos::View<int*, Kokkos::LayoutLeft, H> t(maptrn, nxy);
   w3mapt(Kokkos::DefaultHostExecutionSpace(), nsea, sf, ax, ay, t);
+  return 0;
+}
+
+// W3UTRN of the reference (kokkos/src/ww_kokkos/updt_utrn.hpp:302-362): ATRNX/ATRNY
+// (NY*NX, 3) from TRNX/TRNY, ICE (0:NSEA), BERG (NSEA), MAPSF (NSEA,3), MAPSTA/HPFAC/HQFAC (NY,NX).
+#include "ww_kokkos/updt_utrn.hpp"
+
+extern "C" int ref_w3utrn(int nx, int ny, int nsea, int trflag, float fice0, float ficen,
+                          float ficel, float ffacberg, int flagll, float trny_before,
+                          const float* trnx, const float* trny, const int* mapsf,
+                          const int* mapsta, const float* hpfac, const float* hqfac,
+                          const float* ice, const float* berg, float* atrnx, float* atrny) {
+  using namespace ww::updt;
+  using V = UtrnViews<Kokkos::HostSpace>;
+  const size_t nxy = static_cast<size_t>(nx) * ny;
+  UtrnScalars s{};
+  s.nx = nx;
+  s.ny = ny;
+  s.nsea = nsea;
+  s.trflag = trflag;
+  s.fice0 = fice0;
+  s.ficen = ficen;
+  s.ficel = ficel;
+  s.ffacberg = ffacberg;
+  s.flagll = flagll != 0;
+  s.trny_before = trny_before;
+  std::vector<float> tri(2 * nxy, 0.0f);
+  V v;
+  v.trnx = V::R1(trnx, nxy);
+  v.trny = V::R1(trny, nxy);
+  v.ice = V::R1(ice, static_cast<size_t>(nsea) + 1);
+  v.berg = V::R1(berg, static_cast<size_t>(nsea > 0 ? nsea : 1));
+  v.mapsf = V::I2(mapsf, static_cast<size_t>(nsea), 3);
+  v.mapsta = V::I2(mapsta, static_cast<size_t>(ny), static_cast<size_t>(nx));
+  v.hpfac = V::R2(hpfac, static_cast<size_t>(ny), static_cast<size_t>(nx));
+  v.hqfac = V::R2(hqfac, static_cast<size_t>(ny), static_cast<size_t>(nx));
+  v.atrnx = V::W2(atrnx, nxy, 3);
+  v.atrny = V::W2(atrny, nxy, 3);
+  v.trix = V::W1(tri.data(), nxy);
+  v.triy = V::W1(tri.data() + nxy, nxy);
+  w3utrn(Kokkos::DefaultHostExecutionSpace(), s, v);
   return 0;
 }
 

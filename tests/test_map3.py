@@ -95,3 +95,40 @@ def test_map3_validation(pkg, synth):
     bad[0] = 21  # IX > NX
     rc, _ = pkg.map3(20, 12, nsea, 6, 8, sta, bad)
     assert rc == 2
+
+
+def _utrn_inputs(synth, nx, ny, seed):
+    sta, sf, nsea = synth.sea_grid(nx, ny, seed=seed)
+    rng = np.random.default_rng(seed + 50)
+    nxy = nx * ny
+    trnx = np.where(rng.uniform(0, 1, nxy) < 0.8, 1.0, rng.uniform(0.0, 1.0, nxy)).astype(np.float32)
+    trny = np.where(rng.uniform(0, 1, nxy) < 0.8, 1.0, rng.uniform(0.0, 1.0, nxy)).astype(np.float32)
+    hpfac = rng.uniform(0.05, 0.5, nxy).astype(np.float32)
+    hqfac = rng.uniform(0.05, 0.5, nxy).astype(np.float32)
+    ice = np.where(rng.uniform(0, 1, nsea + 1) < 0.6, 0.0, rng.uniform(0.0, 1.0, nsea + 1))
+    ice = ice.astype(np.float32)
+    berg = np.where(rng.uniform(0, 1, nsea) < 0.9, 0.0, rng.uniform(0.0, 3.0, nsea))
+    return sta, sf, nsea, trnx, trny, hpfac, hqfac, ice, berg.astype(np.float32)
+
+
+# (trflag, fice0, ficen, ficel, ffacberg, flagll): every branch of W3UTRN
+UTRN = [(0, 0.0, 0.0, 0.0, 0.0, 1), (1, 0.0, 0.0, 0.0, 0.0, 1), (2, 0.0, 0.0, 0.0, 0.0, 0),
+        (3, 0.5, 0.75, 0.0, 10.0, 1), (4, 0.5, 0.75, 0.0, 10.0, 0), (5, 0.5, 0.75, 2.0e4, 5.0, 1),
+        (3, 0.5, 0.5, 0.0, 10.0, 1)]
+
+
+@needs_ref
+@pytest.mark.gpu
+@pytest.mark.parametrize("params", UTRN)
+@pytest.mark.parametrize("nx,ny,seed", [(48, 32, 2), (1440, 720, 6)])
+def test_utrn_equals_reference(pkg, synth, params, nx, ny, seed):
+    _gpu()
+    sta, sf, nsea, trnx, trny, hpfac, hqfac, ice, berg = _utrn_inputs(synth, nx, ny, seed)
+    trflag, fice0, ficen, ficel, ffacberg, flagll = params
+    args = (nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, flagll, np.float32(0.625),
+            trnx, trny, sf, sta, hpfac, hqfac, ice, berg)
+    rx, ry = _oracle.ref_w3utrn(*args)
+    rc, gx, gy = pkg.utrn(*args)
+    assert rc == 0
+    assert np.array_equal(gx.view(np.uint32), rx.view(np.uint32)), "ATRNX"
+    assert np.array_equal(gy.view(np.uint32), ry.view(np.uint32)), "ATRNY"

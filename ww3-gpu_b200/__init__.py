@@ -46,7 +46,7 @@ EXPORTS = (
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
-    "ww_map3", "ww_map3_device", "ww_mapt",
+    "ww_map3", "ww_map3_device", "ww_mapt", "ww_utrn",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -420,6 +420,25 @@ def mapt(nx, ny, nsea, mapsf, atrnx, atrny, maptrn):
     L.ww_mapt.restype = _I
     rc = L.ww_mapt(nx, ny, nsea, sf.ctypes.data, ax.ctypes.data, ay.ctypes.data, t.ctypes.data)
     return rc, t
+
+
+def utrn(nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, flagll, trny_before, trnx, trny,
+         mapsf, mapsta, hpfac, hqfac, ice, berg):
+    """W3UTRN through ww_utrn; returns (status, atrnx, atrny), each (3*NX*NY) column-major."""
+    L = lib()
+    init()
+    nxy = nx * ny
+    ax = np.zeros(3 * nxy, np.float32)
+    ay = np.zeros(3 * nxy, np.float32)
+    keep = [np.ascontiguousarray(a, t) for a, t in ((trnx, np.float32), (trny, np.float32),
+                                                     (mapsf, np.int32), (mapsta, np.int32),
+                                                     (hpfac, np.float32), (hqfac, np.float32),
+                                                     (ice, np.float32), (berg, np.float32))]
+    L.ww_utrn.argtypes = [_I] * 4 + [_F] * 4 + [_I, _F] + [_P] * 10
+    L.ww_utrn.restype = _I
+    rc = L.ww_utrn(nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, int(flagll),
+                   trny_before, *[k.ctypes.data for k in keep], ax.ctypes.data, ay.ctypes.data)
+    return rc, ax, ay
 
 
 def xyp3_batch(case, igrid=None, va=None):

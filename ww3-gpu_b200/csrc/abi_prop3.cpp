@@ -18,6 +18,7 @@
 #include "ktp3_kernel.cuh"
 #include "map3_kernel.cuh"
 #include "staging.hpp"
+#include "utrn_kernel.cuh"
 #include "va.hpp"
 #include "wwb_common.hpp"
 #include "xyp3_kernel.cuh"
@@ -608,6 +609,52 @@ int ww_mapt(int nx, int ny, int nsea, const int* mapsf, const float* atrnx, cons
     int* d_t = st.in(k0 + 3, maptrn, static_cast<size_t>(nxy), s);
     launch_mapt(nsea, static_cast<int>(nxy), d_sf, d_x, d_y, d_t, s);
     WWB_CHECK(cudaMemcpyAsync(maptrn, d_t, sizeof(int) * nxy, cudaMemcpyDeviceToHost, s));
+    WWB_CHECK(cudaStreamSynchronize(s));
+    g_prop3.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_utrn(int nx, int ny, int nsea, int trflag, float fice0, float ficen, float ficel,
+            float ffacberg, int flagll, float trny_before, const float* trnx, const float* trny,
+            const int* mapsf, const int* mapsta, const float* hpfac, const float* hqfac,
+            const float* ice, const float* berg, float* atrnx, float* atrny) {
+  return guarded([&] {
+    if (nx < 1 || ny < 1 || nsea < 0 || static_cast<long long>(nx) * ny > (1ll << 31) - 1 ||
+        !atrnx || !atrny || (nsea > 0 && (!mapsf || !mapsta || !trnx || !trny)))
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_utrn: bad sizes or null pointer");
+    const UtrnGrid g{nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, flagll ? 1 : 0,
+                     trny_before};
+    const bool ice_on = trflag != 0 && utrn_needs_ice(g);
+    if (ice_on && nsea > 0 && (!hpfac || !hqfac || !ice || !berg))
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_utrn: ice arrays missing");
+    for (int i = 0; i < nsea; ++i) {
+      const int ix = mapsf[i], iy = mapsf[nsea + i], ixy = mapsf[2 * nsea + i];
+      if (ix < 1 || ix > nx || iy < 1 || iy > ny || ixy != (ix - 1) * ny + iy)
+        return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_utrn: MAPSF is not a map of cells of the grid");
+    }
+    if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+    timers::Region t_call("utrn.call");
+    Staging& st = staging();
+    cudaStream_t s = runtime().stream;
+    const size_t nxy = static_cast<size_t>(nx) * ny, ns = static_cast<size_t>(nsea);
+    constexpr int k0 = 100;
+    const int* d_sf = nsea ? st.in(k0, mapsf, 3 * ns, s) : nullptr;
+    const int* d_sta = nsea ? st.in(k0 + 1, mapsta, nxy, s) : nullptr;
+    const float* d_tx = nsea ? st.in(k0 + 2, trnx, nxy, s) : nullptr;
+    const float* d_ty = nsea ? st.in(k0 + 3, trny, nxy, s) : nullptr;
+    const bool ice_arrays = ice_on && nsea > 0;
+    const float* d_hp = ice_arrays ? st.in(k0 + 4, hpfac, nxy, s) : nullptr;
+    const float* d_hq = ice_arrays ? st.in(k0 + 5, hqfac, nxy, s) : nullptr;
+    const float* d_ice = ice_arrays ? st.in(k0 + 6, ice, ns + 1, s) : nullptr;
+    const float* d_berg = ice_arrays ? st.in(k0 + 7, berg, ns, s) : nullptr;
+    float* d_ax = static_cast<float*>(st.get(k0 + 8, 3 * nxy * sizeof(float)));
+    float* d_ay = static_cast<float*>(st.get(k0 + 9, 3 * nxy * sizeof(float)));
+    float* d_tri = ice_on ? static_cast<float*>(st.get(k0 + 10, 2 * nxy * sizeof(float))) : nullptr;
+    launch_utrn(g, d_sf, d_sta, d_tx, d_ty, d_hp, d_hq, d_ice, d_berg, d_ax, d_ay, d_tri,
+                d_tri ? d_tri + nxy : nullptr, s);
+    WWB_CHECK(cudaMemcpyAsync(atrnx, d_ax, 3 * nxy * sizeof(float), cudaMemcpyDeviceToHost, s));
+    WWB_CHECK(cudaMemcpyAsync(atrny, d_ay, 3 * nxy * sizeof(float), cudaMemcpyDeviceToHost, s));
     WWB_CHECK(cudaStreamSynchronize(s));
     g_prop3.ok();
     return static_cast<int>(WW_KOKKOS_OK);
