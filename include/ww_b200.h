@@ -275,6 +275,25 @@ int ww_utrn(int nx, int ny, int nsea, int trflag, float fice0, float ficen, floa
             const int* mapsf, const int* mapsta, const float* hpfac, const float* hqfac,
             const float* ice, const float* berg, float* atrnx, float* atrny);
 
+/* ---------------------------------------------------------------- a whole step as one graph */
+/* B200 extension; the reference has no counterpart (its W3WAVE port calls the entries one by
+ * one, wave_w3wave.hpp:577-800). Between ww_step_begin(igrid) and ww_step_end(igrid), the calls
+ * ww_ktp3_batch_va, ww_xyp3_batch_va and ww_srce_batch_va of grid igrid are validated and their
+ * inputs copied to device buffers the step owns, but their kernels do not run: they are
+ * recorded, in call order. ww_step_end captures them into one CUDA graph; ww_step_run replays
+ * it nrep times on the resident VA (state DEVICE afterwards) on `stream` (NULL: the library's
+ * stream, synchronised before returning), with no host work and no copies. Each replay repeats
+ * the recorded calls with their recorded scalars (the time of day, the boundary times, DTG);
+ * W3SRCE's per-point packets (PSC, WHITECAP, TAUBBL, TAUICE, SHAVE) and W3KTP3's CFL maxima stay
+ * on the device, the packets carrying over from one replay to the next. ww_xyp3_batch_mpi is not
+ * recorded (UNSUPPORTED). Return WwKokkosStatus. */
+int ww_step_begin(int igrid);
+int ww_step_end(int igrid);
+int ww_step_run(int igrid, int nrep, void* stream);
+int ww_step_free(int igrid);
+/* The number of calls the grid's step holds, or -1 for a grid without one. */
+int ww_step_ops(int igrid);
+
 /* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* / ww_map3* / ww_mapt /
  * ww_utrn call (the reference returns it only). */
 int ww_prop3_last_error(void);

@@ -46,7 +46,8 @@ EXPORTS = (
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
-    "ww_map3", "ww_map3_device", "ww_mapt", "ww_utrn",
+    "ww_map3", "ww_map3_device", "ww_mapt", "ww_utrn", "ww_step_begin", "ww_step_end",
+    "ww_step_run", "ww_step_free", "ww_step_ops",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -328,6 +329,16 @@ class SrceGrid:
                              _ptr(whitecap), _ptr(taubbl), _ptr(tauice), _ptr(shave))
         self._check("ww_srce_batch")
 
+    def batch_va(self, npts, va, jsea, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave,
+                 it=1, inflags24=0, flogrd57=1, flogrd58=1, dtg=900.0):
+        """ww_srce_batch_va on the resident VA bound to the host array ``va`` (NSEALM+1 rows of
+        NSPEC); jsea (npts, 1-based columns) and the packets are host arrays, updated in place."""
+        self.L.ww_srce_batch_va(self.igrid, it, inflags24, flogrd57, flogrd58, dtg, _ptr(va),
+                                va.shape[1], va.shape[0] - 1, npts, _ptr(jsea), _ptr(wn1),
+                                _ptr(cg1), _ptr(pin), _ptr(psc), _ptr(whitecap), _ptr(taubbl),
+                                _ptr(tauice), _ptr(shave))
+        self._check("ww_srce_batch_va")
+
     def batch_device(self, npts, spec, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave,
                      stream=0, it=1, inflags24=0, flogrd57=1, flogrd58=1, dtg=900.0):
         """ww_srce_batch_device on device tensors, launched on CUDA stream handle ``stream``."""
@@ -439,6 +450,45 @@ def utrn(nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, flagll, trny_befor
     rc = L.ww_utrn(nx, ny, nsea, trflag, fice0, ficen, ficel, ffacberg, int(flagll),
                    trny_before, *[k.ctypes.data for k in keep], ax.ctypes.data, ay.ctypes.data)
     return rc, ax, ay
+
+
+class Step:
+    """A whole time step of grid ``igrid`` recorded once (ww_step_begin .. ww_step_end) and
+    replayed as one CUDA graph (ww_step_run). Use as ``with Step(igrid) as st: <_va calls>``,
+    then ``st.run(n)``."""
+
+    def __init__(self, igrid):
+        self.L = lib()
+        init()
+        self.igrid = igrid
+        for name in ("ww_step_begin", "ww_step_end", "ww_step_free", "ww_step_ops"):
+            getattr(self.L, name).argtypes = [_I]
+            getattr(self.L, name).restype = _I
+        self.L.ww_step_run.argtypes = [_I, _I, _P]
+        self.L.ww_step_run.restype = _I
+
+    def __enter__(self):
+        rc = self.L.ww_step_begin(self.igrid)
+        if rc != OK:
+            raise WwError("ww_step_begin", rc)
+        return self
+
+    def __exit__(self, et, ev, tb):
+        rc = self.L.ww_step_end(self.igrid)
+        if rc != OK and et is None:
+            raise WwError("ww_step_end", rc)
+        return False
+
+    def ops(self):
+        return self.L.ww_step_ops(self.igrid)
+
+    def run(self, nrep=1, stream=None):
+        rc = self.L.ww_step_run(self.igrid, nrep, stream)
+        if rc != OK:
+            raise WwError("ww_step_run", rc)
+
+    def free(self):
+        self.L.ww_step_free(self.igrid)
 
 
 def xyp3_batch(case, igrid=None, va=None):

@@ -30,6 +30,7 @@ void release_va_contexts();    // abi_va.cu
 void release_prop3_staging();  // abi_prop3.cpp
 void release_srce_contexts();  // abi_srce.cpp
 void release_st4_contexts();   // abi_st4.cpp
+void release_steps();          // abi_step.cpp
 
 namespace {
 
@@ -202,6 +203,7 @@ int ww_kokkos_init(int comm_f) {
 
 void ww_kokkos_finalize(void) {
   auto& rt = runtime();
+  wwb::release_steps();
   wwb::release_srce_contexts();
   wwb::release_st4_contexts();
   wwb::release_snl1_contexts();

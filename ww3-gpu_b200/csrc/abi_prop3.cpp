@@ -18,6 +18,7 @@
 #include "ktp3_kernel.cuh"
 #include "map3_kernel.cuh"
 #include "staging.hpp"
+#include "step.hpp"
 #include "utrn_kernel.cuh"
 #include "va.hpp"
 #include "wwb_common.hpp"
@@ -78,8 +79,11 @@ int ktp3_entry(int igrid, bool resident, const float* rpar, int nrpar, const int
     return WW_KOKKOS_OK;
   }
   timers::Region t_call("ktp3.call");
-  Staging& st = staging();
-  cudaStream_t s = runtime().stream;
+  // While the grid records a step, the inputs go to buffers the step owns (see step.hpp).
+  StepRecorder* const rec = resident ? step_recorder(igrid) : nullptr;
+  std::shared_ptr<Staging> own = rec ? std::make_shared<Staging>() : nullptr;
+  Staging& st = rec ? *own : staging();
+  cudaStream_t s = rec ? step_stream(rec) : runtime().stream;
   const size_t ntab = static_cast<size_t>(nspec) + nth;
   const size_t ncell = static_cast<size_t>(nk2) * (static_cast<size_t>(nsea) + 1);
   const size_t ncfl = static_cast<size_t>(ncol) - 1;
@@ -109,6 +113,17 @@ int ktp3_entry(int igrid, bool resident, const float* rpar, int nrpar, const int
   // CFLTHMAX/CFLKMAX come in as well as out: entries of points not listed keep their values.
   float* d_cth = st.in(slot++, cflthmax, ncfl, s);
   float* d_ck = st.in(slot++, cflkmax, ncfl, s);
+  if (rec) {
+    // CFLTHMAX/CFLKMAX of the replays stay on the device.
+    WWB_CHECK(cudaStreamSynchronize(s));
+    step_keep(rec, own);
+    step_add(rec, [=](cudaStream_t ss) {
+      launch_ktp3(p, itstep, ntimes, facth, fack, npts, d_js, d_is, d_ps, d_cg, d_wn, d_va,
+                  d_cth, d_ck, ss);
+    });
+    g_prop3.ok();
+    return WW_KOKKOS_OK;
+  }
   launch_ktp3(p, itstep, ntimes, facth, fack, npts, d_js, d_is, d_ps, d_cg, d_wn, d_va, d_cth,
               d_ck, s);
   if (resident) va_device_written(igrid);
@@ -246,8 +261,12 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
     if (a.on[isp - 1] != 0) list.push_back(isp);
   if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
   timers::Region t_call("xyp3.call");
-  Staging& st = staging();
-  cudaStream_t s = runtime().stream;
+  StepRecorder* const rec = resident ? step_recorder(igrid) : nullptr;
+  if (rec && a.naproc != 0)
+    return fail(WW_KOKKOS_ERR_UNSUPPORTED, "ww_xyp3_batch_mpi: not recorded into a step");
+  std::shared_ptr<Staging> own = rec ? std::make_shared<Staging>() : nullptr;
+  Staging& st = rec ? *own : staging();
+  cudaStream_t s = rec ? step_stream(rec) : runtime().stream;
   const size_t nk2 = static_cast<size_t>(g.nk) + 2, ntab = static_cast<size_t>(g.nspec) + g.nth;
   int slot = 0;
   g.mapsf = st.in(slot++, a.mapsf, 3 * static_cast<size_t>(nsea), s);
@@ -309,6 +328,7 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
   const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(list.size(), kXyp3ChunkBytes / per)));
   const size_t nq = static_cast<size_t>(ny) * (nx + 3), n1 = static_cast<size_t>(ny) * (nx + 1);
   char* base = static_cast<char*>(st.get(slot++, per * chunk + 256));
+  std::vector<std::pair<Xyp3Chunk, int>> recorded;  // chunks and sub-step counts of a step
   for (size_t c0 = 0; c0 < list.size(); c0 += chunk) {
     Xyp3Chunk ch{};
     ch.ncomp = static_cast<int>(std::min<size_t>(chunk, list.size() - c0));
@@ -325,7 +345,24 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
     ch.comp = reinterpret_cast<Comp*>(
         (reinterpret_cast<uintptr_t>(ch.iixy + 4 * static_cast<size_t>(nsea) * chunk) + 63) &
         ~static_cast<uintptr_t>(63));
-    run_xyp3_chunk(g, ch, d_va, s);
+    if (rec) {
+      // The chunks share the work arrays (they run one after another); each keeps its own
+      // per-component constants.
+      ch.comp = static_cast<Comp*>(st.get(slot++, xyp3_comp_bytes() * ch.ncomp));
+      const int ntmax = setup_xyp3_chunk(g, ch, s);
+      recorded.emplace_back(ch, ntmax);
+    } else {
+      run_xyp3_chunk(g, ch, d_va, s);
+    }
+  }
+  if (rec) {
+    WWB_CHECK(cudaStreamSynchronize(s));
+    step_keep(rec, own);
+    step_add(rec, [g, recorded, d_va](cudaStream_t ss) {
+      for (const auto& cn : recorded) launch_xyp3_chunk(g, cn.first, d_va, cn.second, ss);
+    });
+    g_prop3.ok();
+    return WW_KOKKOS_OK;
   }
   if (resident) va_device_written(igrid);
   else

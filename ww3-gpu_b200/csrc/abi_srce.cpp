@@ -19,6 +19,7 @@
 
 #include "st4_srce.cuh"
 #include "staging.hpp"
+#include "step.hpp"
 #include "va.hpp"
 #include "wwb_common.hpp"
 
@@ -111,6 +112,41 @@ void run_batch(int igrid, GridCtx& g, const SrceStep& step, int npts, float* spe
   SrceDev host{};
   if (!prepare(igrid, g, host, who)) return;
   const size_t n = npts, ns = n * g.p.nspec, nk = n * g.p.nk;
+  if (StepRecorder* rec = va_dev ? step_recorder(igrid) : nullptr) {
+    // A recorded step: the launch parameters, the inputs and the work buffers are the step's
+    // own; the per-point packets (PSC, WHITECAP, TAUBBL, TAUICE, SHAVE) stay on the device and
+    // carry over from one replay to the next.
+    cudaStream_t s = step_stream(rec);
+    auto cur = std::make_shared<Cursor>();
+    auto work = std::shared_ptr<SrceWork>(new SrceWork(), [](SrceWork* w) {
+      w->release();
+      delete w;
+    });
+    SrceDev* d = nullptr;
+    WWB_CHECK(cudaMalloc(&d, sizeof(SrceDev)));
+    auto dk = std::shared_ptr<SrceDev>(d, [](SrceDev* p) { cudaFree(p); });
+    WWB_CHECK(cudaMemcpy(d, &host, sizeof(SrceDev), cudaMemcpyHostToDevice));
+    const int* djsea = cur->in(jsea, n, s);
+    const float *dwn = cur->in(wn1, nk, s), *dcg = cur->in(cg1, nk, s),
+                *dpin = cur->in(pin, n * srce::NPIN, s);
+    float* dpsc = cur->in(psc, n * srce::NPSC, s);
+    float *dwc = cur->in(whitecap, 4 * n, s), *dtb = cur->in(taubbl, 2 * n, s),
+          *dti = cur->in(tauice, 2 * n, s);
+    int* dsh = cur->in(shave, n, s);
+    srce_reserve(host.L, npts, *work, s);
+    WWB_CHECK(cudaStreamSynchronize(s));
+    step_keep(rec, cur);
+    step_keep(rec, work);
+    step_keep(rec, dk);
+    const pt::SrceLayout L = host.L;
+    SrceWork* const w = work.get();
+    step_add(rec, [=](cudaStream_t ss) {
+      launch_srce(d, L, step, npts, va_dev, djsea, dwn, dcg, dpin, dpsc, dwc, dtb, dti, dsh, *w,
+                  ss);
+    });
+    g_status.ok();
+    return;
+  }
   cudaStream_t s = runtime().stream;
   Cursor& c = staging();
   c.next = 0;

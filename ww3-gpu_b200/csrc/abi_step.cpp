@@ -1,0 +1,173 @@
+// ww3-gpu_b200/csrc/abi_step.cpp
+// ww_step_begin / ww_step_end / ww_step_run / ww_step_free: a whole time step on a grid's
+// resident VA recorded once and replayed as one CUDA graph (see step.hpp).
+//
+// What W3WAVE does between two output times on a PR3 grid is, per time step, W3KTP3 on every
+// sea point, W3XYP3 on every spectral component, W3KTP3 again and W3SRCE on every sea point
+// (ww3-gpu kokkos/src/ww_kokkos/wave_w3wave.hpp:577-800 orders them; the fork calls the C
+// entries ww_ktp3_batch_va, ww_xyp3_batch_va and ww_srce_batch_va one after another). Their
+// host work (validation, derived maps, copies of the grid's arrays) depends only on the grid
+// and the recorded arguments, so it is done once while recording; the replay is launches only.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "step.hpp"
+#include "va.hpp"
+#include "wwb_common.hpp"
+
+namespace wwb {
+
+struct StepRecorder {
+  bool recording = false;
+  std::vector<std::function<void(cudaStream_t)>> ops;
+  std::vector<std::shared_ptr<void>> keep;
+  cudaStream_t stage = nullptr;  ///< staging stream of the recorded calls
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int nops = 0;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  void clear() {
+    drop_graph();
+    ops.clear();
+    keep.clear();
+    recording = false;
+    nops = 0;
+  }
+  ~StepRecorder() {
+    clear();
+    if (stage) cudaStreamDestroy(stage);
+  }
+};
+
+namespace {
+
+Status g_step;
+
+std::map<int, std::unique_ptr<StepRecorder>>& recs() {
+  static auto* m = new std::map<int, std::unique_ptr<StepRecorder>>();
+  return *m;
+}
+
+StepRecorder* find(int igrid) {
+  auto it = recs().find(igrid);
+  return it == recs().end() ? nullptr : it->second.get();
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc& e) {
+    return g_step.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  } catch (const std::exception& e) {
+    return g_step.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
+}  // namespace
+
+StepRecorder* step_recorder(int igrid) {
+  StepRecorder* r = find(igrid);
+  return (r && r->recording) ? r : nullptr;
+}
+
+void step_keep(StepRecorder* r, std::shared_ptr<void> obj) { r->keep.push_back(std::move(obj)); }
+
+void step_add(StepRecorder* r, std::function<void(cudaStream_t)> op) {
+  r->ops.push_back(std::move(op));
+}
+
+cudaStream_t step_stream(StepRecorder* r) { return r->stage; }
+
+void release_steps() { recs().clear(); }
+
+}  // namespace wwb
+
+using namespace wwb;
+
+extern "C" {
+
+int ww_step_begin(int igrid) {
+  return guarded([&] {
+    if (!runtime().ready) return g_step.fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+    auto& r = recs()[igrid];
+    if (!r) r = std::make_unique<StepRecorder>();
+    if (r->recording) return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_begin: already recording");
+    // Recording again replaces the grid's step.
+    r->clear();
+    if (!r->stage) WWB_CHECK(cudaStreamCreateWithFlags(&r->stage, cudaStreamNonBlocking));
+    r->recording = true;
+    g_step.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_step_end(int igrid) {
+  return guarded([&] {
+    StepRecorder* r = find(igrid);
+    if (!r || !r->recording) return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_end: not recording");
+    r->recording = false;
+    cudaStream_t cap = nullptr;
+    WWB_CHECK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    // Relaxed: the launchers look up occupancies and set function attributes, which are not
+    // stream work; they allocate nothing here (the recorded calls reserved their buffers).
+    WWB_CHECK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
+    bool failed = false;
+    try {
+      for (auto& op : r->ops) op(cap);
+    } catch (...) {
+      failed = true;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (failed || e != cudaSuccess || g == nullptr) {
+      if (g) cudaGraphDestroy(g);
+      r->clear();
+      return g_step.fail(WW_KOKKOS_ERR_KERNEL, "ww_step_end: the step's launches could not be captured");
+    }
+    r->graph = g;
+    WWB_CHECK(cudaGraphInstantiate(&r->exec, r->graph, 0));
+    r->nops = static_cast<int>(r->ops.size());
+    g_step.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_step_run(int igrid, int nrep, void* stream) {
+  return guarded([&] {
+    StepRecorder* r = find(igrid);
+    if (!r || r->recording || !r->exec)
+      return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_run: no recorded step for this grid");
+    if (nrep < 0) return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_run: nrep < 0");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : runtime().stream;
+    for (int i = 0; i < nrep; ++i) WWB_CHECK(cudaGraphLaunch(r->exec, s));
+    if (nrep > 0) va_device_written(igrid);
+    if (!stream) WWB_CHECK(cudaStreamSynchronize(s));
+    g_step.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_step_free(int igrid) {
+  StepRecorder* r = find(igrid);
+  if (r) r->clear();
+  g_step.ok();
+  return WW_KOKKOS_OK;
+}
+
+int ww_step_ops(int igrid) {
+  StepRecorder* r = find(igrid);
+  return r ? static_cast<int>(r->ops.size()) : -1;
+}
+
+}  // extern "C"

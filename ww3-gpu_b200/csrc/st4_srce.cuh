@@ -81,6 +81,10 @@ void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
                  const float* tauwx, const float* tauwy, const int* llws, float* const* out12,
                  cudaStream_t st);
 
+/// Allocates the work buffers launch_srce needs for npts points of these tables (none when they
+/// fit), so that a later launch allocates nothing.
+void srce_reserve(const pt::SrceLayout& L, int npts, SrceWork& work, cudaStream_t st);
+
 /// W3SRCE for npts points on a persistent grid whose CTAs take points from a work queue
 /// (work.counter, zeroed here), so points with many substeps do not hold up the rest. Point n's
 /// spectrum is spec + n * nspec, or, with jsea non-null, the resident VA column

@@ -185,6 +185,23 @@ void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
   WWB_CHECK(cudaGetLastError());
 }
 
+void srce_reserve(const pt::SrceLayout& L, int npts, SrceWork& work, cudaStream_t st) {
+  if (npts <= 0) return;
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock);
+  const size_t need = static_cast<size_t>(grid) * static_cast<size_t>(L.total_g);
+  if (work.counter == nullptr) WWB_CHECK(cudaMalloc(&work.counter, sizeof(int)));
+  if (need > work.scratch_n) {
+    WWB_CHECK(cudaStreamSynchronize(st));
+    if (work.scratch) WWB_CHECK(cudaFree(work.scratch));
+    work.scratch = nullptr;
+    work.scratch_n = 0;
+    WWB_CHECK(cudaMalloc(&work.scratch, need * sizeof(float)));
+    work.scratch_n = need;
+  }
+}
+
 void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int npts,
                  float* spec, const int* jsea, const float* wn1, const float* cg1,
                  const float* pin, float* psc, float* whitecap, float* taubbl, float* tauice,
@@ -193,17 +210,9 @@ void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int n
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
   const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock);
-  const size_t need = static_cast<size_t>(grid) * static_cast<size_t>(L.total_g);
-  if (work.counter == nullptr) WWB_CHECK(cudaMalloc(&work.counter, sizeof(int)));
-  if (need > work.scratch_n) {  // (nothing when the working set is all shared)
-    // The previous launches on this grid's stream may still read the old buffer.
-    WWB_CHECK(cudaStreamSynchronize(st));
-    if (work.scratch) WWB_CHECK(cudaFree(work.scratch));
-    work.scratch = nullptr;
-    work.scratch_n = 0;
-    WWB_CHECK(cudaMalloc(&work.scratch, need * sizeof(float)));
-    work.scratch_n = need;
-  }
+  // The work buffers fit after srce_reserve; otherwise (re)allocate them first, after the
+  // previous launches on this stream that may still read the old ones.
+  srce_reserve(L, npts, work, st);
   WWB_CHECK(cudaMemsetAsync(work.counter, 0, sizeof(int), st));
   srce_kernel<<<grid, kSrceBlock, smem, st>>>(d, step, npts, spec, jsea, wn1, cg1, pin, psc,
                                               whitecap, taubbl, tauice, shave, work.counter,

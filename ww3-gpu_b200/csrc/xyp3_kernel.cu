@@ -359,6 +359,13 @@ __global__ void average_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itl
   }
 }
 
+__global__ void comp_reset_kernel(int ncomp, Comp* comps, float* vq, float* aq, size_t nq) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncomp) return;
+  comps[c].q = vq + c * nq;
+  comps[c].a = aq + c * nq;
+}
+
 __global__ void swap_kernel(int ncomp, Comp* comps, int itloc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncomp || itloc > comps[c].ntloc) return;
@@ -620,9 +627,9 @@ void launch_va_components(bool unpack, float* va, int nspec, int nsealm, const i
   WWB_CHECK(cudaGetLastError());
 }
 
-void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s) {
+int setup_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, cudaStream_t s) {
   const int nc = ch.ncomp;
-  if (nc <= 0) return;
+  if (nc <= 0) return 0;
   const size_t nq = static_cast<size_t>(g.ny) * (g.nx + 3);
   const size_t n1 = static_cast<size_t>(g.ny) * (g.nx + 1);
   // Per-component buffers and constants.
@@ -642,6 +649,20 @@ void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s)
   WWB_CHECK(cudaGetLastError());
   std::vector<Comp> back(nc);
   WWB_CHECK(cudaMemcpyAsync(back.data(), ch.comp, sizeof(Comp) * nc, cudaMemcpyDeviceToHost, s));
+  WWB_CHECK(cudaStreamSynchronize(s));
+  int ntmax = 0;
+  for (const Comp& k : back) ntmax = std::max(ntmax, k.ntloc);
+  return ntmax;
+}
+
+void launch_xyp3_chunk(const Xyp3Grid& g, const Xyp3Chunk& ch, float* va, int ntmax,
+                       cudaStream_t s) {
+  const int nc = ch.ncomp;
+  if (nc <= 0) return;
+  const size_t nq = static_cast<size_t>(g.ny) * (g.nx + 3);
+  const size_t n1 = static_cast<size_t>(g.ny) * (g.nx + 1);
+  // The sub-steps swap each component's two buffers: start from the set-up assignment.
+  comp_reset_kernel<<<(nc + 127) / 128, 128, 0, s>>>(nc, ch.comp, ch.vq, ch.aq, nq);
   // FIELD = 0 (W3GATH), the four speed arrays = 0 (:944-947).
   WWB_CHECK(cudaMemsetAsync(ch.vq, 0, sizeof(float) * nq * nc, s));
   WWB_CHECK(cudaMemsetAsync(ch.vlcflx, 0, sizeof(float) * n1 * nc, s));
@@ -649,9 +670,6 @@ void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s)
   const long long nsea_c = static_cast<long long>(nc) * g.nsea;
   sea_setup_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.l0, ch.comp, va);
   WWB_CHECK(cudaGetLastError());
-  WWB_CHECK(cudaStreamSynchronize(s));
-  int ntmax = 0;
-  for (const Comp& k : back) ntmax = std::max(ntmax, k.ntloc);
   // YFIRST (:928-931): the same for every component; it alternates every sub-step.
   const int dttst = fint(g.dsec_day);
   bool yfirst = (nint_r(static_cast<float>(dttst) / g.dtg) % 2) == 0;
@@ -679,6 +697,13 @@ void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s)
   }
   store_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.l0, ch.comp, va);
   WWB_CHECK(cudaGetLastError());
+}
+
+size_t xyp3_comp_bytes() { return sizeof(Comp); }
+
+void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, float* va, cudaStream_t s) {
+  const int ntmax = setup_xyp3_chunk(g, ch, s);
+  launch_xyp3_chunk(g, ch, va, ntmax, s);
 }
 
 }  // namespace wwb

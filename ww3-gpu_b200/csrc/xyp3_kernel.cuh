@@ -70,9 +70,21 @@ struct Xyp3Chunk {
 /// Bytes of work storage per component.
 size_t xyp3_bytes_per_component(const Xyp3Grid& g);
 
+/// Bytes of one component's constants (the chunk's comp array holds one per component).
+size_t xyp3_comp_bytes();
+
 /// W3GATH, W3XYP3 and W3SCAT for every component of the chunk, on the resident VA
 /// (NSPEC, 0:NSEALM) va. The chunk's arrays must be allocated (xyp3_bytes_per_component).
 void run_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& c, float* va, cudaStream_t s);
+
+/// The first half of run_xyp3_chunk: the components' constants (sub-step counts, rotated
+/// speeds) into the chunk's device array; returns the largest sub-step count (synchronises).
+int setup_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& c, cudaStream_t s);
+
+/// The second half: one propagation of the chunk's components on va with ntmax sub-steps,
+/// launches only (no host synchronisation, no host memory), so a stream capture can record it.
+void launch_xyp3_chunk(const Xyp3Grid& g, const Xyp3Chunk& c, float* va, int ntmax,
+                       cudaStream_t s);
 
 /// ww_xyp3_mpi_pack (unpack false): buf[J*NSEALM + K-1] = VA(ISPS(J+1), K), K = 1 .. NSEALM;
 /// ww_xyp3_mpi_unpack (unpack true) the other way. d_isps holds nisp 1-based components.
