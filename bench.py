@@ -23,7 +23,14 @@ Two workloads (--workload):
   cpu_baseline -- the reference's own C++ (oracle/_ref, compiled from its sources) on this
             host's cores on a bounded sample, rank 0 only.
 
---impl reference runs that CPU reference alone, with the same metric and config.
+* step -- the resident whole step (config 2's shape at --nx x --ny, default 360 x 180, about
+  45,000 sea points; 1440 x 720 is the survey's size): W3KTP3, W3XYP3, W3KTP3 and W3SRCE on the
+  resident VA, recorded once and replayed as one CUDA graph per step (ww_step_run); the grid's
+  maps from this project's device W3MAP3. e2e uploads the host VA, runs the step and reads the VA
+  back, every step.
+
+--impl reference runs that CPU reference alone, with the same metric and config (for step, on a
+grid a quarter of the size in each direction).
 Multi-GPU: both workloads are independent per sea point, so each rank runs its own points (weak
 scaling) with no collective on the data path; ranks meet only at the timing barriers.
 """
@@ -61,7 +68,9 @@ def parse():
     p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=None)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--workload", choices=["srce", "dia"], default="srce")
+    p.add_argument("--workload", choices=["srce", "dia", "step"], default="srce")
+    p.add_argument("--nx", type=int, default=360, help="step workload: grid longitudes")
+    p.add_argument("--ny", type=int, default=180, help="step workload: grid latitudes")
     p.add_argument("--npts", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -70,9 +79,9 @@ def parse():
     a = p.parse_args()
     srce = a.workload == "srce"
     if a.steps is None:
-        a.steps = 20 if srce else 200
+        a.steps = {"srce": 20, "dia": 200, "step": 10}[a.workload]
     if a.warmup is None:
-        a.warmup = 3 if srce else 5
+        a.warmup = 5 if a.workload == "dia" else 3
     if a.npts is None:
         a.npts = SRCE_NPTS if srce else NPTS_PER_GPU
     return a
@@ -582,10 +591,299 @@ def run_b200_srce(args):
     return 0
 
 
+# ---------------------------------------------------------------- the resident whole step
+STEP_WORKLOAD = ("resident whole step on a {nx}x{ny} lon/lat grid ({nsea} sea points, seeded "
+                 "smooth land mask, ~70% sea, boundary and excluded points): W3KTP3, W3XYP3 "
+                 "(PR3/UQ), W3KTP3, W3SRCE + ST4 + DIA, 36x36, one CUDA graph per step")
+# VA read and written by each of the four parts: the minimum HBM traffic of an unfused step.
+STEP_BYTES_PER_POINT = 4 * 2 * 4 * NK * NTH  # 41,472
+
+
+def step_inputs(synth, map3, nx, ny, seed):
+    """A grid's whole-step inputs: the W3SRCE/ST4/DIA configuration of the srce workload, the
+    PR3 grid (maps from ``map3``, a W3MAP3), the W3KTP3 arguments and the points' packets."""
+    st = synth.st4_setup(NK, NTH, variant="analytic")
+    t = synth.st4_tables_own(st)
+    sr = synth.srce_setup(st)
+    cfg, sig = synth.dia_config(NK, NTH)
+    xc = synth.xyp3_case(nx, ny, seed=seed, nk=NK, nth=NTH, ref=map3)
+    nsea = xc["nsea"]
+    kc = synth.ktp3_case(nsea, seed=seed + 1, nk=NK, nth=NTH, nsea=nsea)
+    pts = synth.srce_points(nsea, seed=seed + 2, nk=NK, nth=NTH)
+    return st, t, sr, cfg, sig, xc, kc, pts
+
+
+STEP_PACKETS = ("wn1", "cg1", "pin", "psc", "whitecap", "taubbl", "tauice")
+
+
+def step_calls(lib_calls, va, kc, xc, pts, nsea):
+    """The four calls of one step through ``lib_calls`` (ktp3, xyp3, srce callables)."""
+    import numpy as np
+    ktp3, xyp3, srce = lib_calls
+    jsea = np.arange(1, nsea + 1, dtype=np.int32)
+    packets = {k: np.array(pts[k], copy=True) for k in STEP_PACKETS}
+    shave = np.zeros(nsea, np.int32)
+
+    def one():
+        ktp3(kc, 1, va)
+        xyp3(xc, va)
+        ktp3(kc, 2, va)
+        srce(va, jsea, packets, shave)
+    return one
+
+
+def step_config(args, world, nsea):
+    return {"workload": STEP_WORKLOAD.format(nx=args.nx, ny=args.ny, nsea=nsea), "nk": NK,
+            "nth": NTH, "nx": args.nx, "ny": args.ny, "nsea_per_gpu": nsea,
+            "global_points": nsea * world, "dtg_s": 900.0, "seed": 2026,
+            "st4": "saturation breaking with the cumulative term, analytic high-frequency tail",
+            "l2": "the resident VA (NSPEC x NSEA floats) is larger than L2",
+            "parallelism": f"one grid per GPU ({world}), no collective"}
+
+
+def run_b200_step(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
+    torch.cuda.set_device(local)
+    os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    pkg = entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    pkg.init()
+
+    def map3(nx, ny, nsea, nk, nth, mapsta, mapsf):  # this project's device W3MAP3
+        rc, m = pkg.map3(nx, ny, nsea, nk, nth, mapsta, mapsf)
+        if rc != 0:
+            raise SystemExit(f"ww_map3 failed ({rc})")
+        return m["mapx2"], m["mapy2"], m["mapaxy"], m["mapcxy"][:nsea], m["counts"]
+
+    st, t, sr, cfg, sig, xc, kc, pts = step_inputs(synth, map3, args.nx, args.ny, 2026 + rank)
+    nsea = xc["nsea"]
+    ig = 1
+    grid = pkg.SrceGrid(ig, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig, sr)
+    va = np.array(xc["va"], np.float32, copy=True)
+
+    def srce(v, jsea, pk, shave):
+        grid.batch_va(nsea, v, jsea, pk["wn1"], pk["cg1"], pk["pin"], pk["psc"], pk["whitecap"],
+                      pk["taubbl"], pk["tauice"], shave)
+
+    one = step_calls((lambda c, it, v: pkg.ktp3_batch(c, it, 1, ig, v),
+                      lambda c, v: pkg.xyp3_batch(c, ig, v), srce), va, kc, xc, pts, nsea)
+    step = pkg.Step(ig)
+    with step:
+        one()
+    nodes = step.nodes()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    for _ in range(args.warmup):
+        step.run(1, handle)
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        barrier()
+        ev[0].record(stream)
+        for i in range(args.steps):
+            step.run(1, handle)
+            ev[i + 1].record(stream)
+        barrier()
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    value = nsea * world * args.steps / (total_ms / 1e3)
+
+    # ---- end to end: the host VA uploaded, the step, the VA read back, every step
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
+    L = pkg.lib()
+    hva = va  # the Fortran array the resident VA mirrors
+
+    def host_step():
+        assert L.ww_va_host_write(ig, hva.ctypes.data, hva.shape[1], hva.shape[0] - 1) == 0
+        step.run(1, None)
+        assert L.ww_va_host_read(ig, hva.ctypes.data, hva.shape[1], hva.shape[0] - 1) == 0
+
+    host_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_step()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = nsea * world * e2e_steps / e2e_s
+    va_bytes = int(va.nbytes)
+    peak, peak_kind = measured_peak_hbm()
+    step_ms = statistics.median(per)
+    achieved = STEP_BYTES_PER_POINT * nsea / (step_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": step_config(args, world, nsea),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": va_bytes,
+                "d2h_bytes_per_step": va_bytes, "steps": e2e_steps,
+                "host_entry": "ww_va_host_write + ww_step_run + ww_va_host_read"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": None, "kernel": "the step graph (srce_kernel dominant)",
+                     "launch_ms": step_ms, "algorithmic_bytes_per_point": STEP_BYTES_PER_POINT,
+                     "note": ("the VA read and written by each of the four parts; W3SRCE, about "
+                              "95% of the step, is bound by its serial chains, not by HBM")},
+        "gpu_launches": nodes * args.steps,
+        "graph_nodes": nodes,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_step(synth, max(args.nx // 4, 8), max(args.ny // 4, 8))
+        if r is not None:
+            rate, kind, cores, sample = r
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                    "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    step.free()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def reference_step_calls(oracle, synth, nx, ny, igrid):
+    """The reference's four calls of a whole step (its C ABI, resident VA in host memory) on an
+    nx x ny grid of the workload; returns (callable one step, nsea)."""
+    import numpy as np
+    st, t, sr, cfg, sig, xc, kc, pts = step_inputs(synth, oracle.ref_w3map3, nx, ny, 2026)
+    nsea = xc["nsea"]
+    ref = oracle.RefSt4(st, t, igrid=igrid, srce=sr, dia=(cfg, sig))
+    L = ref.L
+    va = np.array(xc["va"], np.float32, copy=True)
+    K = ("sig", "dsip", "ecos", "esin", "ec2", "esc", "es2", "mapwn", "mapth2", "mapwn2")
+    X = ("mapsf", "clats", "sig", "ecos", "esin", "dpdx", "dpdy", "dqdx", "dqdy", "gsqrt",
+         "atrnx", "atrny", "mapx2", "mapy2", "mapaxy", "mapcxy", "maptrn", "mapsta", "cg", "cx",
+         "cy")
+    kk = {k: np.ascontiguousarray(v) for k, v in kc.items() if isinstance(v, np.ndarray)}
+    xk = {k: np.ascontiguousarray(v) for k, v in xc.items() if isinstance(v, np.ndarray)}
+    cth = np.array(kc["cflthmax"], np.float32, copy=True)
+    ck = np.array(kc["cflkmax"], np.float32, copy=True)
+
+    def ktp3(c, it, v):
+        L.ww_ktp3_batch_va(igrid, kk["rpar"].ctypes.data, kk["rpar"].size, kk["ipar"].ctypes.data,
+                           kk["ipar"].size, *[kk[a].ctypes.data for a in K], it, 1, c["facth"],
+                           c["fack"], c["nsea"], kk["cg"].ctypes.data, kk["wn"].ctypes.data,
+                           c["npts"], kk["jsea"].ctypes.data, kk["isea"].ctypes.data,
+                           kk["pscal"].ctypes.data, v.ctypes.data, v.shape[1], v.shape[0] - 1,
+                           cth.ctypes.data, ck.ctypes.data)
+
+    def xyp3(c, v):
+        L.ww_xyp3_batch_va(igrid, xk["rpar"].ctypes.data, xk["rpar"].size, xk["ipar"].ctypes.data,
+                           xk["ipar"].size, xk["imaps"].ctypes.data, xk["imaps"].size,
+                           xk["tscal"].ctypes.data, xk["tscal"].size, c["dtg"],
+                           *[xk[a].ctypes.data for a in X], c["flbpi"], c["nbi"],
+                           xk["isbpi"].ctypes.data, xk["bbpi0"].ctypes.data,
+                           xk["bbpin"].ctypes.data, xk["on"].ctypes.data, v.ctypes.data,
+                           v.shape[1], v.shape[0] - 1)
+
+    def srce(v, jsea, pk, shave):
+        L.ww_srce_batch_va(igrid, 1, 0, 1, 1, 900.0, v.ctypes.data, v.shape[1], v.shape[0] - 1,
+                           nsea, jsea.ctypes.data, *[pk[k].ctypes.data for k in STEP_PACKETS],
+                           shave.ctypes.data)
+
+    c_int, c_float, c_void = (__import__("ctypes").c_int, __import__("ctypes").c_float,
+                              __import__("ctypes").c_void_p)
+    L.ww_ktp3_batch_va.argtypes = [c_int, c_void, c_int, c_void, c_int] + [c_void] * 10 + [
+        c_int, c_int, c_float, c_float, c_int, c_void, c_void, c_int, c_void, c_void, c_void,
+        c_void, c_int, c_int, c_void, c_void]
+    L.ww_xyp3_batch_va.argtypes = [c_int, c_void, c_int, c_void, c_int, c_void, c_int, c_void,
+                                   c_int, c_float] + [c_void] * 21 + [
+        c_int, c_int, c_void, c_void, c_void, c_void, c_void, c_int, c_int]
+    L.ww_srce_batch_va.argtypes = [c_int, c_int, c_int, c_int, c_int, c_float, c_void, c_int,
+                                   c_int, c_int] + [c_void] * 9
+    return step_calls((ktp3, xyp3, srce), va, kc, xc, pts, nsea), nsea
+
+
+def cpu_reference_step(synth, nx, ny, seconds=10.0):
+    """Sea-point·steps/s of the reference's whole step on this host's cores, on a smaller grid
+    of the workload (its own C++, the resident VA in host memory)."""
+    oracle = entry.load_oracle()
+    if not oracle.ref_available():
+        return None
+    one, nsea = reference_step_calls(oracle, synth, nx, ny, 8)
+    one()
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        one()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 20:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return (nsea * n / el, "reference", cores,
+            f"{n} whole steps of a {nx}x{ny} grid of the workload ({nsea} sea points)")
+
+
+def run_reference_step(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    oracle = entry.load_oracle()
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build "
+                          "(oracle/_ref) is absent"}), flush=True)
+        return 0
+    nx, ny = max(args.nx // 4, 8), max(args.ny // 4, 8)
+    one, nsea = reference_step_calls(oracle, synth, nx, ny, 9)
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    el = time.perf_counter() - t0
+    rate = nsea * args.steps / el
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cfgd = step_config(args, 1, nsea)
+    cfgd["reference_sample_grid"] = f"{nx}x{ny}"
+    sample = f"whole steps of a {nx}x{ny} grid of the workload ({nsea} sea points)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": cfgd,
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.workload == "dia":
         return run_reference_dia(args) if args.impl == "reference" else run_b200_dia(args)
+    if args.workload == "step":
+        return run_reference_step(args) if args.impl == "reference" else run_b200_step(args)
     return run_reference_srce(args) if args.impl == "reference" else run_b200_srce(args)
 
 

@@ -293,6 +293,8 @@ int ww_step_run(int igrid, int nrep, void* stream);
 int ww_step_free(int igrid);
 /* The number of calls the grid's step holds, or -1 for a grid without one. */
 int ww_step_ops(int igrid);
+/* The number of nodes (kernels, memsets) of the grid's captured step graph, or -1. */
+int ww_step_nodes(int igrid);
 
 /* B200 extension: the status of the most recent ww_ktp3_* / ww_xyp3_* / ww_map3* / ww_mapt /
  * ww_utrn call (the reference returns it only). */

@@ -47,7 +47,7 @@ EXPORTS = (
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
     "ww_map3", "ww_map3_device", "ww_mapt", "ww_utrn", "ww_step_begin", "ww_step_end",
-    "ww_step_run", "ww_step_free", "ww_step_ops",
+    "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -461,7 +461,8 @@ class Step:
         self.L = lib()
         init()
         self.igrid = igrid
-        for name in ("ww_step_begin", "ww_step_end", "ww_step_free", "ww_step_ops"):
+        for name in ("ww_step_begin", "ww_step_end", "ww_step_free", "ww_step_ops",
+                     "ww_step_nodes"):
             getattr(self.L, name).argtypes = [_I]
             getattr(self.L, name).restype = _I
         self.L.ww_step_run.argtypes = [_I, _I, _P]
@@ -481,6 +482,9 @@ class Step:
 
     def ops(self):
         return self.L.ww_step_ops(self.igrid)
+
+    def nodes(self):
+        return self.L.ww_step_nodes(self.igrid)
 
     def run(self, nrep=1, stream=None):
         rc = self.L.ww_step_run(self.igrid, nrep, stream)

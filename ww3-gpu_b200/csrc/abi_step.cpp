@@ -165,6 +165,14 @@ int ww_step_free(int igrid) {
   return WW_KOKKOS_OK;
 }
 
+int ww_step_nodes(int igrid) {
+  StepRecorder* r = find(igrid);
+  if (!r || !r->graph) return -1;
+  size_t n = 0;
+  if (cudaGraphGetNodes(r->graph, nullptr, &n) != cudaSuccess) return -1;
+  return static_cast<int>(n);
+}
+
 int ww_step_ops(int igrid) {
   StepRecorder* r = find(igrid);
   return r ? static_cast<int>(r->ops.size()) : -1;
