@@ -49,6 +49,10 @@ int main(int argc, char** argv) {
         if (!same(s, ::sinf(x)) || !same(c, ::cosf(x))) ++bad[1];
       } else if (!std::strcmp(fn, "tanhf")) {
         if (!same(wwb::dm::tanhf(x), ::tanhf(x))) ++bad[0];
+      } else if (!std::strcmp(fn, "sinhf")) {
+        if (!same(wwb::dm::sinhf(x), ::sinhf(x))) ++bad[0];
+      } else if (!std::strcmp(fn, "coshf")) {
+        if (!same(wwb::dm::coshf(x), ::coshf(x))) ++bad[0];
       } else if (!std::strcmp(fn, "atanf")) {
         if (!same(wwb::dm::atanf(x), ::atanf(x))) ++bad[0];
       } else if (!std::strcmp(fn, "log10f")) {

@@ -61,7 +61,7 @@ def test_expf_equals_glibc(checker):
     assert per_variant[default] == 0, out
 
 
-@pytest.mark.parametrize("fn", ["logf", "sincosf", "tanhf", "atanf", "log10f"])
+@pytest.mark.parametrize("fn", ["logf", "sincosf", "tanhf", "atanf", "log10f", "sinhf", "coshf"])
 def test_unary_equals_glibc(checker, fn):
     """Every 61st bit pattern (all 2^32 with WWB_LIBM_FULL=1); sincosf also against a lone
     sinf and cosf, which the reference calls as separate functions."""

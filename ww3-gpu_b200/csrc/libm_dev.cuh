@@ -589,6 +589,58 @@ WWB_HC float tanhf(float x) {
   return (jx & 0x80000000u) ? -z : z;
 }
 
+// ------------------------------------------------------------------------------ sinhf, coshf
+/// sinhf as glibc's e_sinhf.c computes it (fdlibm's method): expm1f below 22, expf up to the
+/// overflow threshold.
+WWB_HC float sinhf(float x) {
+  const float one = 1.0f, shuge = 1.0e37f;
+  const uint32_t jx = asuint(x);
+  const uint32_t ix = jx & 0x7fffffffu;
+  if (ix >= 0x7f800000u) return x + x;
+  const float h = (jx & 0x80000000u) ? -0.5f : 0.5f;
+  const float ax = fabsf(x);
+  if (ix < 0x41b00000u) {  // |x| < 22 (glibc's bound of the expm1f branch)
+    if (ix < 0x31800000u) {  // |x| < 2**-28 (glibc's threshold)
+      if (shuge + x > one) return x;
+    }
+    const float t = expm1f(ax);
+    if (ix < 0x3f800000u) return h * (2.0f * t - t * t / (t + one));
+    return h * (t + t / (t + one));
+  }
+  if (ix < 0x42b17180u) return h * expf(ax);  // |x| in [22, log(maxfloat)]
+  if (ix <= 0x42b2d4fcu) {                   // |x| up to the overflow threshold
+    const float w = expf(0.5f * ax);
+    const float t = h * w;
+    return t * w;
+  }
+  return x * shuge;
+}
+
+/// coshf as glibc's e_coshf.c computes it (fdlibm's method).
+WWB_HC float coshf(float x) {
+  const float one = 1.0f, half = 0.5f, huge = 1.0e30f;
+  const uint32_t ix = asuint(x) & 0x7fffffffu;
+  if (ix >= 0x7f800000u) return x * x;
+  const float ax = fabsf(x);
+  if (ix < 0x3eb17218u) {  // |x| < 0.5*ln2
+    const float t = expm1f(ax);
+    const float w = one + t;
+    if (ix < 0x24000000u) return w;  // cosh(tiny) = 1
+    return one + (t * t) / (w + w);
+  }
+  if (ix < 0x41100000u) {  // |x| < 9
+    const float t = expf(ax);
+    return half * t + half / t;
+  }
+  if (ix < 0x42b17180u) return half * expf(ax);
+  if (ix <= 0x42b2d4fcu) {
+    const float w = expf(half * ax);
+    const float t = half * w;
+    return t * w;
+  }
+  return huge * huge;
+}
+
 // ----------------------------------------------------------------------------- atanf, atan2f
 /// fdlibm atanf.
 WWB_HC float atanf(float x) {
