@@ -300,6 +300,43 @@ int ww_step_nodes(int igrid);
  * ww_utrn call (the reference returns it only). */
 int ww_prop3_last_error(void);
 
+/* ---------------------------------------------------------------- gridded output (W3OUTG) */
+/* Replaces ww_outg_va (outg_c.hpp:97-120): W3OUTG (VA, .FALSE., FLOUTG, FLOUTG2) of
+ * w3iogomd.F90:1201-2380, sections 1-4 and the space-time extremes, on the resident VA of grid
+ * igrid (read on the device; VA crosses only when the host holds the newer bits). ipar is the
+ * WwOutgIpar packet (25 ints: NK, NTH, NSEAL, NSEA, NX, NY, NFLD, NOGRP, NGRPP, FLOUTG, FLOUTG2,
+ * OARST, OMPG, P2MSF(2:3), E3DF(2,1:5), E3DF(3,1:5)), rpar the WwOutgRpar packet (10 reals: DTH,
+ * XFR, FTE, FTWL, FTTR, UNDEF, STEXU, STEYU, STEDU, WSCUT). flogrd, flogr2, flogrr are LOGICAL(4)
+ * (NOGRP,NGRPP); va is VA(1,0), nspec = SIZE(VA,1), nsealm = UBOUND(VA,2); cg, wn (0:NK+1,0:NSEA),
+ * dw (0:NSEA), sig (0:NK+1), dden, dsii (NK), ecos .. esc (NTH), mapsf (NSEA,3), mapsta (NY,NX).
+ * fields: the 46 arrays of WwOutgField (40 of NFLD; EF .. STH2M (NFLD, E3DF(2,k):E3DF(3,k)),
+ * P2SMS (NFLD, P2MSF(2):P2MSF(3)); a 2-D field the grid does not allocate is NULL). The fields
+ * are computed into device buffers kept between calls; those W3IOGO writes (FLOGRD under FLOUTG,
+ * FLOGR2 under FLOUTG2) and, when OARST, those W3IORS writes (FLOGRR) come back, the others keep
+ * their host bits. OK, NOT_INITIALISED, BAD_SHAPE, UNSUPPORTED (CALC_U3STOKES, SKEWNESS or
+ * CALC_WBT requested: FLOLOC(6,8), (6,12), (8,7..9), (2,17); or the grid is recording a step),
+ * a resident-VA status, RUNTIME, KERNEL. */
+int ww_outg_va(int igrid, const int* ipar, int nipar, const float* rpar, int nrpar,
+               const int* flogrd, const int* flogr2, const int* flogrr, float* va, int nspec,
+               int nsealm, const float* cg, const float* wn, const float* dw, const float* sig,
+               const float* dden, const float* dsii, const float* ecos, const float* esin,
+               const float* ec2, const float* es2, const float* esc, const int* mapsf,
+               const int* mapsta, float* const* fields, int nfields);
+
+/* Replaces ww_outg_part (outg_c.hpp:122-125): section 6 of W3OUTG (w3iogomd.F90:2242-2340), the
+ * partition fields from W3CPRT's table. ipar is the WwOutgPartIpar packet (13 ints: NSEAL, NSEA,
+ * NX, NY, NROW, NOSWLL, NICP, NDTP, DIMP = 15, NOGRP, NGRPP, FLOUTG, FLOUTG2), rpar (UNDEF,
+ * WSCUT); icprt (NICP,2), dtprt (DIMP,NDTP); fields the 17 arrays of WwOutgPartField (15 of
+ * (NROW, 0:NOSWLL), PWST and PNR (NROW)). Field k comes back when FLOGRD(4,k) (FLOUTG) or
+ * FLOGR2(4,k) (FLOUTG2) is set. OK, NOT_INITIALISED, BAD_SHAPE (also when a sea point's ICPRT
+ * names columns outside DTPRT), RUNTIME, KERNEL. */
+int ww_outg_part(const int* ipar, int nipar, const float* rpar, int nrpar, const int* flogrd,
+                 const int* flogr2, const int* mapsf, const int* mapsta, const int* icprt,
+                 const float* dtprt, float* const* fields, int nfields);
+
+/* B200 extension: the status of the most recent ww_outg_va / ww_outg_part call. */
+int ww_outg_last_error(void);
+
 /* ---------------------------------------------------------------- ST4 source terms (W3SRC4MD) */
 /* A grid is configured as the reference's (ww_kokkos_c.hpp:136-203): ww_st4_init with the
  * RPAR/IPAR packets (st4_params.hpp:79-154 layout: 84 reals, 9 ints), one ww_st4_set_real/int per

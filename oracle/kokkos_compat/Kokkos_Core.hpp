@@ -27,6 +27,8 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <functional>
 #include <limits>
 #include <memory>
@@ -412,6 +414,12 @@ inline void initialize(const InitializationSettings& = {}) {
 }
 inline void initialize(int&, char**) { initialize(); }
 inline bool is_initialized() { return Impl::initialized_flag(); }
+
+/// Kokkos::abort: print the message and stop, as Kokkos does on the host.
+[[noreturn]] inline void abort(const char* msg) {
+  std::fprintf(stderr, "Kokkos::abort: %s\n", msg);
+  std::abort();
+}
 inline bool is_finalized() { return Impl::finalized_flag(); }
 inline void push_finalize_hook(std::function<void()> f) {
   Impl::finalize_hooks().push_back(std::move(f));

@@ -24,3 +24,19 @@ __attribute__((visibility("hidden"))) __m128 _ZGVbN4v_expf(__m128 x) {
   for (int l = 0; l < 4; ++l) r[l] = expf(a[l]);
   return _mm_loadu_ps(r);
 }
+
+/* The two libmvec entry points of the reference's W3OUTG (iogo_w3outg.hpp:37-40: the THMP
+ * sine and cosine of the space-time extremes), likewise scalar per lane. */
+__attribute__((visibility("hidden"))) __m128 _ZGVbN4v_sinf(__m128 x) {
+  float a[4], r[4];
+  _mm_storeu_ps(a, x);
+  for (int l = 0; l < 4; ++l) r[l] = sinf(a[l]);
+  return _mm_loadu_ps(r);
+}
+
+__attribute__((visibility("hidden"))) __m128 _ZGVbN4v_cosf(__m128 x) {
+  float a[4], r[4];
+  _mm_storeu_ps(a, x);
+  for (int l = 0; l < 4; ++l) r[l] = cosf(a[l]);
+  return _mm_loadu_ps(r);
+}

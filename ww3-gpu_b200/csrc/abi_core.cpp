@@ -31,6 +31,7 @@ void release_prop3_staging();  // abi_prop3.cpp
 void release_srce_contexts();  // abi_srce.cpp
 void release_st4_contexts();   // abi_st4.cpp
 void release_steps();          // abi_step.cpp
+void release_outg_staging();   // abi_outg.cpp
 
 namespace {
 
@@ -210,6 +211,7 @@ void ww_kokkos_finalize(void) {
   if (!rt.ready) return;
   wwb::release_va_contexts();
   wwb::release_prop3_staging();
+  wwb::release_outg_staging();
   cudaDeviceSynchronize();
   if (rt.stream) cudaStreamDestroy(rt.stream);
   if (rt.copy_in) cudaStreamDestroy(rt.copy_in);

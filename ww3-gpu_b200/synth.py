@@ -610,3 +610,117 @@ def st4_registrations(st, t):
     if t.get("tauhft2") is not None:
         regs.append((16, t["tauhft2"], False, [0, 0, 0], [101, 201, 51]))
     return regs
+
+
+# W3OUTG packets (outg_c.hpp:12-47, :74-104): FLOGRD(NOGRP, NGRPP) with WW3's NOGRP = 10 and
+# NGRPP = 18, and the (group, index) entries the device W3OUTG leaves to the Fortran.
+OUTG_NOGRP, OUTG_NGRPP = 10, 18
+OUTG_UNSUPPORTED = ((6, 8), (6, 12), (8, 7), (8, 8), (8, 9), (2, 17))
+
+
+def outg_flags(select="all", seed=0):
+    """FLOGRD as int32 (NOGRP*NGRPP, column-major): every output the device W3OUTG computes
+    ("all"), none ("none"), or a seeded half of them ("some")."""
+    f = np.zeros(OUTG_NOGRP * OUTG_NGRPP, np.int32)
+    if select == "none":
+        return f
+    rng = np.random.default_rng(seed + 17)
+    for j in range(1, OUTG_NGRPP + 1):
+        for i in range(1, OUTG_NOGRP + 1):
+            if (i, j) in OUTG_UNSUPPORTED:
+                continue
+            f[(i - 1) + (j - 1) * OUTG_NOGRP] = 1 if select == "all" else int(rng.uniform() < 0.5)
+    return f
+
+
+def outg_case(nx=40, ny=30, seed=0, nk=30, nth=24, xfr=1.1, ompg=0, ste=(1000.0, 1000.0, 3600.0),
+              select="all", floutg2=0, oarst=0, nsealm_extra=2, e3df=None, p2=(3, 12)):
+    """Seeded inputs of ww_outg_va on an NX x NY grid (sea_grid: active, boundary and excluded
+    points), JONSWAP spectra of random depth (some points calm: a zero spectrum), the W3GDATMD
+    arrays at their Fortran bounds, FLOGRD/FLOGR2/FLOGRR, and 46 prefilled field arrays (EF ..
+    STH2M over E3DF(2,k):E3DF(3,k), P2SMS over P2MSF(2):P2MSF(3)). ``ste`` = (STEXU, STEYU, STEDU);
+    ``e3df`` = (E3DF(2,1:5), E3DF(3,1:5)) and ``p2`` = P2MSF(2:3) may reach outside 1..NK."""
+    rng = np.random.default_rng(seed)
+    mapsta, mapsf, nsea = sea_grid(nx, ny, seed=seed)
+    nsealm = nsea + nsealm_extra
+    sp = spectral_arrays(nk, nth, xfr=xfr)
+    sig = sp["sig"]
+    dth = np.float32(sp["dth"])
+    x = np.float32(xfr)
+    dsii = np.empty(nk, np.float32)
+    dsii[:] = np.float32(0.5) * sig[1:nk + 1] * (x - np.float32(1.0) / x)
+    dsii[0] = np.float32(0.5) * sig[1] * (x - np.float32(1.0))
+    dsii[nk - 1] = np.float32(0.5) * sig[nk] * (x - np.float32(1.0)) / x
+    dden = (dth * dsii * sig[1:nk + 1]).astype(np.float32)
+    th = np.arange(nth, dtype=np.float64) * float(dth)
+    ecos = np.cos(th).astype(np.float32)
+    esin = np.sin(th).astype(np.float32)
+    ecos[np.abs(ecos) < 1e-5] = 0.0
+    esin[np.abs(esin) < 1e-5] = 0.0
+    st = sea_states(nsea, seed=seed + 5, nk=nk, nth=nth, depth_range=(1.0, 3000.0), bimodal=0.3)
+    va = np.zeros((nsealm + 1, nk * nth), np.float32)
+    va[1:nsea + 1] = st["a"]
+    calm = rng.uniform(0, 1, nsea) < 0.05
+    va[1:nsea + 1][calm] = 0.0
+    va[nsea + 1:] = rng.uniform(0, 1e-3, (nsealm - nsea, nk * nth)).astype(np.float32)
+    dep = np.concatenate([[1.0], st["depth"].astype(np.float64)])
+    s64 = sig.astype(np.float64)
+    k = wavenumber(s64, dep)
+    kd = k * dep[:, None]
+    cg = 0.5 * s64[None, :] / k * (1.0 + 2.0 * kd / np.sinh(np.minimum(2.0 * kd, 80.0)))
+    signk = sig[nk]
+    fte = np.float32(0.25) * signk * dth * signk
+    ftwl = np.float32(GRAV / 6.0) / (signk * signk) * dth * signk
+    fttr = np.float32(0.20) * dth * signk
+    rpar = np.array([dth, x, fte, ftwl, fttr, -999.9, ste[0], ste[1], ste[2], 0.8], np.float32)
+    e3df2, e3df3 = e3df if e3df is not None else ([1, 3, 1, 2, 5], [nk, 10, nk, 20, nk - 1])
+    ipar = np.array([nk, nth, nsea, nsea, nx, ny, nsealm, OUTG_NOGRP, OUTG_NGRPP, 1, floutg2,
+                     oarst, ompg, p2[0], p2[1], *e3df2, *e3df3], np.int32)
+    fields = [rng.standard_normal(nsealm).astype(np.float32) for _ in range(40)]
+    for k3 in range(5):
+        fields.append(rng.standard_normal((e3df3[k3] - e3df2[k3] + 1, nsealm)).astype(np.float32))
+    fields.append(rng.standard_normal((p2[1] - p2[0] + 1, nsealm)).astype(np.float32))
+    return {
+        "ipar": ipar, "rpar": rpar, "flogrd": outg_flags(select, seed),
+        "flogr2": outg_flags("some", seed + 1), "flogrr": outg_flags("some", seed + 2),
+        "va": va, "nsealm": nsealm, "nsea": nsea,
+        "cg": np.ascontiguousarray(cg, np.float32), "wn": np.ascontiguousarray(k, np.float32),
+        "dw": dep.astype(np.float32), "sig": sig, "dden": dden, "dsii": dsii,
+        "ecos": ecos, "esin": esin, "ec2": (ecos * ecos).astype(np.float32),
+        "es2": (esin * esin).astype(np.float32), "esc": (ecos * esin).astype(np.float32),
+        "mapsf": mapsf, "mapsta": mapsta, "fields": fields,
+    }
+
+
+def outg_part_case(nx=40, ny=30, seed=0, noswll=3, select="all", floutg2=0):
+    """Seeded inputs of ww_outg_part: W3CPRT's ICPRT (NSEALM+1, 2) and DTPRT (15, NDTP) for the
+    sea points of sea_grid (0 to 7 partitions a point, the first the whole spectrum; UNDEF in
+    some directions; wind-sea fractions on both sides of WSCUT = 0.8), and 17 prefilled fields."""
+    rng = np.random.default_rng(seed)
+    mapsta, mapsf, nsea = sea_grid(nx, ny, seed=seed)
+    nsealm = nsea + 1
+    nicp = nsealm + 1
+    n1 = rng.integers(0, 8, nicp).astype(np.int32)
+    n2 = np.ones(nicp, np.int32)
+    pos = 1
+    for j in range(nicp):
+        n2[j] = pos
+        pos += max(int(n1[j]), 1)
+    ndtp = pos - 1
+    dtprt = rng.uniform(0.0, 20.0, (ndtp, 15)).astype(np.float32)
+    dtprt[:, 5] = rng.uniform(0.0, 1.0, ndtp).astype(np.float32)
+    undef = np.float32(-999.9)
+    dtprt[rng.uniform(0, 1, ndtp) < 0.1, 3] = undef
+    dtprt[rng.uniform(0, 1, ndtp) < 0.1, 6] = undef
+    icprt = np.concatenate([n1, n2]).astype(np.int32)
+    flog = np.zeros(OUTG_NOGRP * OUTG_NGRPP, np.int32)
+    for j in range(1, 18):
+        if select == "all" or rng.uniform() < 0.5:
+            flog[3 + (j - 1) * OUTG_NOGRP] = 1
+    ipar = np.array([nsea, nsea, nx, ny, nsealm, noswll, nicp, ndtp, 15, OUTG_NOGRP, OUTG_NGRPP,
+                     1, floutg2], np.int32)
+    fields = [rng.standard_normal((noswll + 1, nsealm)).astype(np.float32) for _ in range(15)]
+    fields += [rng.standard_normal(nsealm).astype(np.float32) for _ in range(2)]
+    return {"ipar": ipar, "rpar": np.array([undef, 0.8], np.float32), "flogrd": flog,
+            "flogr2": outg_flags("none"), "mapsf": mapsf, "mapsta": mapsta, "icprt": icprt,
+            "dtprt": np.ascontiguousarray(dtprt), "fields": fields, "nsea": nsea}
