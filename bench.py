@@ -1,6 +1,6 @@
 """Benchmark of WAVEWATCH III's per-sea-point hot path on B200: sea-point·steps/s at 36x36 bins.
 
-Two workloads (--workload):
+Four workloads (--workload):
 
 * srce (default) -- the full plain source-term step W3SRCE with ST4 (W3SIN4 + W3SDS4 + W3SPR4),
   the DIA (W3SNL1), W3SBT1 and W3SDB1 on 9520 sea points, 36 x 36 float32, DTG = 900 s with
@@ -28,6 +28,10 @@ Two workloads (--workload):
   resident VA, recorded once and replayed as one CUDA graph per step (ww_step_run); the grid's
   maps from this project's device W3MAP3. e2e uploads the host VA, runs the step and reads the VA
   back, every step.
+
+* outg -- W3OUTG (ww_outg_device on device arrays; e2e: ww_outg_va with the VA newer on the
+  host, the grid arrays copied in and the requested fields copied back) on the resident VA of the
+  same --nx x --ny grid, every field the device computes requested, space-time extremes on.
 
 --impl reference runs that CPU reference alone, with the same metric and config (for step, on a
 grid a quarter of the size in each direction).
@@ -68,9 +72,9 @@ def parse():
     p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=None)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--workload", choices=["srce", "dia", "step"], default="srce")
-    p.add_argument("--nx", type=int, default=360, help="step workload: grid longitudes")
-    p.add_argument("--ny", type=int, default=180, help="step workload: grid latitudes")
+    p.add_argument("--workload", choices=["srce", "dia", "step", "outg"], default="srce")
+    p.add_argument("--nx", type=int, default=360, help="step/outg workloads: grid longitudes")
+    p.add_argument("--ny", type=int, default=180, help="step/outg workloads: grid latitudes")
     p.add_argument("--npts", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -79,7 +83,7 @@ def parse():
     a = p.parse_args()
     srce = a.workload == "srce"
     if a.steps is None:
-        a.steps = {"srce": 20, "dia": 200, "step": 10}[a.workload]
+        a.steps = {"srce": 20, "dia": 200, "step": 10, "outg": 20}[a.workload]
     if a.warmup is None:
         a.warmup = 5 if a.workload == "dia" else 3
     if a.npts is None:
@@ -878,12 +882,253 @@ def run_reference_step(args):
     return 0
 
 
+# ---------------------------------------------------------------------------- W3OUTG workload
+OUTG_WORKLOAD = ("W3OUTG (ww_outg_va: sections 1-4 and the space-time extremes, every field "
+                 "the device computes requested) on the resident VA of a {nx}x{ny} grid "
+                 "({nsea} sea points), 36x36")
+OUTG_STE = (1000.0, 1000.0, 3600.0)
+
+
+def outg_bytes_per_point(c):
+    """The algorithmic HBM bytes of one sea point of W3OUTG: its VA column, CG and WN (NK+2
+    each), DW, MAPSF, MAPSTA, and every field it writes (40 + the 2-D fields' columns)."""
+    nk, nth = int(c["ipar"][0]), int(c["ipar"][1])
+    ncol = sum(f.shape[0] for f in c["fields"][40:])
+    return 4 * (nk * nth + 2 * (nk + 2) + 1 + 3 + 1 + 40 + ncol)
+
+
+def outg_config(args, world, c):
+    return {"workload": OUTG_WORKLOAD.format(nx=args.nx, ny=args.ny, nsea=c["nsea"]),
+            "nk": NK, "nth": NTH, "nx": args.nx, "ny": args.ny, "nsea_per_gpu": c["nsea"],
+            "global_points": c["nsea"] * world, "seed": 2026,
+            "space_time_extremes": {"stexu": OUTG_STE[0], "steyu": OUTG_STE[1],
+                                    "stedu": OUTG_STE[2]},
+            "l2": "the resident VA (NSPEC x NSEA floats) is larger than L2",
+            "parallelism": f"one grid per GPU ({world}), no collective"}
+
+
+def outg_ref_lib():
+    import ctypes
+    oracle = entry.load_oracle()
+    if not oracle.ref_available():
+        return None
+    L = oracle._ref_variant(oracle.REF_PATH)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.ww_outg_va.argtypes = [I, P, I, P, I, P, P, P, P, I, I] + [P] * 13 + [P, I]
+    L.ww_outg_va.restype = I
+    return L
+
+
+def outg_call(L, igrid, c, fields, va):
+    """ww_outg_va of library L on case c (synth.outg_case) into ``fields``."""
+    import ctypes
+    ptrs = (ctypes.c_void_p * 46)(*[f.ctypes.data for f in fields])
+    a = [c[k].ctypes.data for k in ("cg", "wn", "dw", "sig", "dden", "dsii", "ecos", "esin",
+                                    "ec2", "es2", "esc", "mapsf", "mapsta")]
+    return L.ww_outg_va(igrid, c["ipar"].ctypes.data, 25, c["rpar"].ctypes.data, 10,
+                        c["flogrd"].ctypes.data, c["flogr2"].ctypes.data, c["flogrr"].ctypes.data,
+                        va.ctypes.data, va.shape[1], va.shape[0] - 1, *a, ptrs, 46)
+
+
+def cpu_reference_outg(c, seconds=10.0, max_calls=20):
+    L = outg_ref_lib()
+    if L is None:
+        return None
+    import numpy as np
+    va = np.array(c["va"], copy=True)
+    f = [np.array(x, copy=True) for x in c["fields"]]
+    if outg_call(L, 21, c, f, va) != 0:
+        return None
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        outg_call(L, 21, c, f, va)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= max_calls:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return (c["nsea"] * n / el, "reference", cores,
+            f"{n} W3OUTG calls on the workload's grid ({c['nsea']} sea points), OpenMP over points")
+
+
+def run_b200_outg(args):
+    import ctypes
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
+    torch.cuda.set_device(local)
+    os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    pkg = entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    pkg.init()
+    c = synth.outg_case(args.nx, args.ny, seed=2026 + rank, nk=NK, nth=NTH, ste=OUTG_STE)
+    nsea, nseal = c["nsea"], int(c["ipar"][2])
+    L = pkg.lib()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.ww_outg_device.argtypes = [P, I, P, I, P, P, P, I, I] + [P] * 14 + [P, I, P]
+    L.ww_outg_device.restype = I
+    L.ww_outg_va.argtypes = [I, P, I, P, I, P, P, P, P, I, I] + [P] * 13 + [P, I]
+    L.ww_outg_va.restype = I
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def d(x):
+        return torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+
+    names = ("cg", "wn", "dw", "sig", "dden", "dsii", "ecos", "esin", "ec2", "es2", "esc",
+             "mapsf", "mapsta")
+    arrs = [d(c[k]) for k in names]
+    d_va = d(c["va"])
+    d_f = [d(f) for f in c["fields"]]
+    ebd = torch.empty(NK * nseal, dtype=torch.float32, device=dev)
+    ptrs = (ctypes.c_void_p * 46)(*[t.data_ptr() for t in d_f])
+
+    def call():
+        rc = L.ww_outg_device(c["ipar"].ctypes.data, 25, c["rpar"].ctypes.data, 10,
+                              c["flogrd"].ctypes.data, c["flogr2"].ctypes.data, d_va.data_ptr(),
+                              c["va"].shape[1], c["va"].shape[0] - 1,
+                              *[t.data_ptr() for t in arrs], ebd.data_ptr(), ptrs, 46, handle)
+        if rc != 0:
+            raise SystemExit(f"ww_outg_device failed ({rc})")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    for _ in range(args.warmup):
+        call()
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        barrier()
+        ev[0].record(stream)
+        for i in range(args.steps):
+            call()
+            ev[i + 1].record(stream)
+        barrier()
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    value = nsea * world * args.steps / (total_ms / 1e3)
+
+    # ---- end to end: ww_outg_va with the VA newer on the host (it crosses every call), the
+    # grid arrays copied in and the requested fields copied back
+    hva = np.array(c["va"], copy=True)
+    hf = [np.array(x, copy=True) for x in c["fields"]]
+    ig = 1
+
+    def host_call():
+        assert L.ww_va_host_write(ig, hva.ctypes.data, hva.shape[1], hva.shape[0] - 1) == 0
+        rc = outg_call(L, ig, c, hf, hva)
+        if rc != 0:
+            raise SystemExit(f"ww_outg_va failed ({rc})")
+
+    host_call()
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_call()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = nsea * world * e2e_steps / e2e_s
+    in_bytes = int(hva.nbytes) + sum(int(c[k].nbytes) for k in names) + int(c["fields"][39].nbytes)
+    out_bytes = 4 * (40 * int(c["ipar"][6]) + nseal * sum(f.shape[0] for f in c["fields"][40:]))
+    peak, peak_kind = measured_peak_hbm()
+    bpp = outg_bytes_per_point(c)
+    call_ms = statistics.median(per)
+    achieved = bpp * nsea / (call_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": outg_config(args, world, c),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": out_bytes, "steps": e2e_steps,
+                "host_entry": "ww_va_host_write + ww_outg_va"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": None, "kernel": "outg_init_kernel + outg_point_kernel",
+                     "launch_ms": call_ms, "algorithmic_bytes_per_point": bpp},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_outg(c)
+        if r is not None:
+            rate, kind, cores, sample = r
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                    "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_reference_outg(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    L = outg_ref_lib()
+    if L is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build "
+                          "(oracle/_ref) is absent"}), flush=True)
+        return 0
+    import numpy as np
+    c = synth.outg_case(args.nx, args.ny, seed=2026, nk=NK, nth=NTH, ste=OUTG_STE)
+    va = np.array(c["va"], copy=True)
+    f = [np.array(x, copy=True) for x in c["fields"]]
+    for _ in range(args.warmup):
+        outg_call(L, 22, c, f, va)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        outg_call(L, 22, c, f, va)
+    el = time.perf_counter() - t0
+    rate = c["nsea"] * args.steps / el
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = f"W3OUTG calls on the workload's grid ({c['nsea']} sea points), OpenMP over points"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": outg_config(args, 1, c),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.workload == "dia":
         return run_reference_dia(args) if args.impl == "reference" else run_b200_dia(args)
     if args.workload == "step":
         return run_reference_step(args) if args.impl == "reference" else run_b200_step(args)
+    if args.workload == "outg":
+        return run_reference_outg(args) if args.impl == "reference" else run_b200_outg(args)
     return run_reference_srce(args) if args.impl == "reference" else run_b200_srce(args)
 
 

@@ -323,6 +323,20 @@ int ww_outg_va(int igrid, const int* ipar, int nipar, const float* rpar, int nrp
                const float* ec2, const float* es2, const float* esc, const int* mapsf,
                const int* mapsta, float* const* fields, int nfields);
 
+/* B200 extension: ww_outg_va on device arrays, launched on `stream` (a cudaStream_t; NULL the
+ * legacy default stream) with no copy and no synchronisation. The packets and flogrd/flogr2 are
+ * host memory and are checked as ww_outg_va checks them; d_va is VA(1,0) on the device; cg ..
+ * mapsta as ww_outg_va, in device memory (a MAPSF cell outside the grid reads as land); ebd is
+ * NK*NSEAL floats of device work; fields the 46 device arrays (every 1-D one; a 2-D one only
+ * when requested). CGE keeps its values at points that are not sea. Status also in
+ * ww_outg_last_error(). */
+int ww_outg_device(const int* ipar, int nipar, const float* rpar, int nrpar, const int* flogrd,
+                   const int* flogr2, const float* d_va, int nspec, int nsealm, const float* cg,
+                   const float* wn, const float* dw, const float* sig, const float* dden,
+                   const float* dsii, const float* ecos, const float* esin, const float* ec2,
+                   const float* es2, const float* esc, const int* mapsf, const int* mapsta,
+                   float* ebd, float* const* fields, int nfields, void* stream);
+
 /* Replaces ww_outg_part (outg_c.hpp:122-125): section 6 of W3OUTG (w3iogomd.F90:2242-2340), the
  * partition fields from W3CPRT's table. ipar is the WwOutgPartIpar packet (13 ints: NSEAL, NSEA,
  * NX, NY, NROW, NOSWLL, NICP, NDTP, DIMP = 15, NOGRP, NGRPP, FLOUTG, FLOUTG2), rpar (UNDEF,

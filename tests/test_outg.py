@@ -225,3 +225,44 @@ def test_outg_case_shapes(synth):
     nicp = int(p["ipar"][6])
     n1, n2 = p["icprt"][:nicp], p["icprt"][nicp:]
     assert np.all(n2 >= 1) and np.all(n2 + np.maximum(n1, 1) - 1 <= p["ipar"][7])
+
+
+@needs_ref
+@pytest.mark.gpu
+def test_outg_device_equals_host_entry(pkg, synth):
+    """ww_outg_device on device arrays (torch's stream) gives the fields ww_outg_va gives."""
+    import torch
+
+    L = _gpu_lib(pkg)
+    L.ww_outg_device.argtypes = [P, I, P, I, P, P, P, I, I] + [P] * 14 + [P, I, P]
+    L.ww_outg_device.restype = I
+    c = synth.outg_case(seed=11, ste=(1000.0, 1000.0, 3600.0))
+    want = _wanted(c)
+    f_host = _copy_fields(c["fields"])
+    va = np.array(c["va"], copy=True)
+    assert call_outg(L, 830, c, f_host, va) == OK
+    dev = torch.device("cuda", 0)
+
+    def d(x):
+        return torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+
+    arrs = {k: d(c[k]) for k in ("cg", "wn", "dw", "sig", "dden", "dsii", "ecos", "esin", "ec2",
+                                 "es2", "esc", "mapsf", "mapsta")}
+    d_va = d(c["va"])
+    d_f = [d(f) for f in c["fields"]]
+    nk, nseal = int(c["ipar"][0]), int(c["ipar"][2])
+    ebd = torch.empty(nk * nseal, dtype=torch.float32, device=dev)
+    ptrs = (ctypes.c_void_p * 46)(*[t.data_ptr() for t in d_f])
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    rc = L.ww_outg_device(c["ipar"].ctypes.data, 25, c["rpar"].ctypes.data, 10,
+                          c["flogrd"].ctypes.data, c["flogr2"].ctypes.data, d_va.data_ptr(),
+                          c["va"].shape[1], c["va"].shape[0] - 1,
+                          *[arrs[k].data_ptr() for k in ("cg", "wn", "dw", "sig", "dden", "dsii",
+                                                          "ecos", "esin", "ec2", "es2", "esc",
+                                                          "mapsf", "mapsta")],
+                          ebd.data_ptr(), ptrs, 46, stream)
+    assert rc == OK
+    torch.cuda.synchronize()
+    for k in range(46):
+        if want[k]:
+            assert_bitexact(d_f[k].cpu().numpy(), f_host[k], f"device entry: {NAMES[k]}")

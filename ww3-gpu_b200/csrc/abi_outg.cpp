@@ -152,21 +152,40 @@ bool mapsf_ok(const int* mapsf, int nsea, int nseal, int nx, int ny) {
   return true;
 }
 
-int run_outg(int igrid, const int* ipar, const float* rpar, const int* flogrd, const int* flogr2,
-             const int* flogrr, float* va, int nspec, int nsealm, const float* cg,
-             const float* wn, const float* dw, const float* sig, const float* dden,
-             const float* dsii, const float* ecos, const float* esin, const float* ec2,
-             const float* es2, const float* esc, const int* mapsf, const int* mapsta,
-             float* const* fields) {
-  const int nk = ipar[kNk], nth = ipar[kNth], nseal = ipar[kNseal], nsea = ipar[kNsea];
-  const int nx = ipar[kNx], ny = ipar[kNy], nfld = ipar[kNfld], nogrp = ipar[kNogrp];
-  const int ngrpp = ipar[kNgrpp];
-  if (nk < 1 || nth < 1 || nspec != nk * nth || nseal < 0 || nseal > nsealm || nsea < nseal ||
-      nx < 1 || ny < 1 || nfld < nseal || nogrp < 10 || ngrpp < 1)
-    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_va: bad sizes");
-  for (int k = 0; k < kOutgN1d; ++k)
-    if (fields[k] == nullptr) return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_va: a null 1-D field");
+/// The packets of one W3OUTG call, checked: the kernel's scalars and flags, the extents of the
+/// 2-D fields, and FLOLOC. Returns OK or the status (message prefixed by `who`).
+struct OutgCall {
   OutgArgs a{};
+  size_t n2[kOutgNField - kOutgN1d] = {};
+  bool floutg = false, floutg2 = false, oarst = false;
+  int nogrp = 0, ngrpp = 0;
+  const int *flogrd = nullptr, *flogr2 = nullptr;
+  /// FLOGRD(NOGRP,NGRPP), LOGICAL(4); an index past NGRPP is never set.
+  bool lgrd(const int* f, int i, int j) const {
+    return j <= ngrpp && f[(i - 1) + (j - 1) * nogrp] != 0;
+  }
+  bool floloc(int i, int j) const {
+    return (floutg && lgrd(flogrd, i, j)) || (floutg2 && lgrd(flogr2, i, j));
+  }
+};
+
+int outg_packets(const int* ipar, const float* rpar, const int* flogrd, const int* flogr2,
+                 int nspec, int nsealm, float* const* fields, const char* who, OutgCall& c) {
+  char msg[128];
+  const auto bad = [&](int code, const char* what) {
+    std::snprintf(msg, sizeof msg, "%s: %s", who, what);
+    return fail(code, msg);
+  };
+  const int nk = ipar[kNk], nth = ipar[kNth], nseal = ipar[kNseal], nsea = ipar[kNsea];
+  const int nx = ipar[kNx], ny = ipar[kNy], nfld = ipar[kNfld];
+  c.nogrp = ipar[kNogrp];
+  c.ngrpp = ipar[kNgrpp];
+  if (nk < 1 || nth < 1 || nspec != nk * nth || nseal < 0 || nseal > nsealm || nsea < nseal ||
+      nx < 1 || ny < 1 || nfld < nseal || c.nogrp < 10 || c.ngrpp < 1)
+    return bad(WW_KOKKOS_ERR_BAD_SHAPE, "bad sizes");
+  for (int k = 0; k < kOutgN1d; ++k)
+    if (fields[k] == nullptr) return bad(WW_KOKKOS_ERR_BAD_SHAPE, "a null 1-D field");
+  OutgArgs& a = c.a;
   a.nk = nk;
   a.nth = nth;
   a.nseal = nseal;
@@ -191,32 +210,45 @@ int run_outg(int igrid, const int* ipar, const float* rpar, const int* flogrd, c
     a.e3df3[k] = ipar[kE3df3 + k];
   }
   a.ompg = ipar[kOmpg] != 0;
-  const bool floutg = ipar[kFloutg] != 0, floutg2 = ipar[kFloutg2] != 0;
-  const bool oarst = ipar[kOarst] != 0;
-  // FLOGRD(NOGRP,NGRPP), LOGICAL(4); an index past NGRPP is never set.
-  const auto lgrd = [&](const int* f, int i, int j) {
-    return j <= ngrpp && f[(i - 1) + (j - 1) * nogrp] != 0;
-  };
-  const auto floloc = [&](int i, int j) {
-    return (floutg && lgrd(flogrd, i, j)) || (floutg2 && lgrd(flogr2, i, j));
-  };
+  c.floutg = ipar[kFloutg] != 0;
+  c.floutg2 = ipar[kFloutg2] != 0;
+  c.oarst = ipar[kOarst] != 0;
+  c.flogrd = flogrd;
+  c.flogr2 = flogr2;
   // The fields the caller leaves to the Fortran W3OUTG: CALC_U3STOKES, SKEWNESS, CALC_WBT.
-  if (floloc(6, 8) || floloc(6, 12) || floloc(8, 7) || floloc(8, 8) || floloc(8, 9) ||
-      floloc(2, 17))
-    return fail(WW_KOKKOS_ERR_UNSUPPORTED,
-                "ww_outg_va: a field left to the Fortran W3OUTG is requested");
-  size_t n2[kOutgNField - kOutgN1d];
+  if (c.floloc(6, 8) || c.floloc(6, 12) || c.floloc(8, 7) || c.floloc(8, 8) ||
+      c.floloc(8, 9) || c.floloc(2, 17))
+    return bad(WW_KOKKOS_ERR_UNSUPPORTED, "a field left to the Fortran W3OUTG is requested");
   for (int k = 0; k < 5; ++k) {
-    a.f3[k] = floloc(3, k + 1);
-    n2[k] = a.e3df3[k] >= a.e3df2[k] ? static_cast<size_t>(a.e3df3[k] - a.e3df2[k] + 1) : 0;
-    if (a.f3[k] && (fields[OG_EF + k] == nullptr || n2[k] == 0))
-      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_va: a requested 3-D field is not allocated");
+    a.f3[k] = c.floloc(3, k + 1);
+    c.n2[k] = a.e3df3[k] >= a.e3df2[k] ? static_cast<size_t>(a.e3df3[k] - a.e3df2[k] + 1) : 0;
+    if (a.f3[k] && (fields[OG_EF + k] == nullptr || c.n2[k] == 0))
+      return bad(WW_KOKKOS_ERR_BAD_SHAPE, "a requested 3-D field is not allocated");
   }
-  a.f69 = floloc(6, 9);
-  n2[5] = a.p2msf3 >= a.p2msf2 ? static_cast<size_t>(a.p2msf3 - a.p2msf2 + 1) : 0;
-  if (a.f69 && (fields[OG_P2SMS] == nullptr || n2[5] == 0))
-    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_va: P2SMS is requested and not allocated");
+  a.f69 = c.floloc(6, 9);
+  c.n2[5] = a.p2msf3 >= a.p2msf2 ? static_cast<size_t>(a.p2msf3 - a.p2msf2 + 1) : 0;
+  if (a.f69 && (fields[OG_P2SMS] == nullptr || c.n2[5] == 0))
+    return bad(WW_KOKKOS_ERR_BAD_SHAPE, "P2SMS is requested and not allocated");
   a.ste = (a.stexu > 0.0f && a.steyu > 0.0f) || a.stedu > 0.0f;
+  return WW_KOKKOS_OK;
+}
+
+int run_outg(int igrid, const int* ipar, const float* rpar, const int* flogrd, const int* flogr2,
+             const int* flogrr, float* va, int nspec, int nsealm, const float* cg,
+             const float* wn, const float* dw, const float* sig, const float* dden,
+             const float* dsii, const float* ecos, const float* esin, const float* ec2,
+             const float* es2, const float* esc, const int* mapsf, const int* mapsta,
+             float* const* fields) {
+  OutgCall c;
+  const int prc = outg_packets(ipar, rpar, flogrd, flogr2, nspec, nsealm, fields, "ww_outg_va", c);
+  if (prc != WW_KOKKOS_OK) return prc;
+  OutgArgs& a = c.a;
+  const int nk = a.nk, nth = a.nth, nseal = a.nseal, nsea = a.nsea, nx = a.nx, ny = a.ny;
+  const int nfld = a.nfld;
+  const size_t* n2 = c.n2;
+  const bool oarst = c.oarst;
+  const auto floloc = [&](int i, int j) { return c.floloc(i, j); };
+  const auto lgrd = [&](const int* f, int i, int j) { return c.lgrd(f, i, j); };
   if (!mapsf_ok(mapsf, nsea, nseal, nx, ny))
     return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_va: MAPSF names a cell outside the grid");
   if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
@@ -302,6 +334,46 @@ int run_outg(int igrid, const int* ipar, const float* rpar, const int* flogrd, c
   }
   g_calls.fetch_add(1, std::memory_order_relaxed);
   g_points.fetch_add(nseal, std::memory_order_relaxed);
+  g_outg.ok();
+  return WW_KOKKOS_OK;
+}
+
+int run_outg_device(const int* ipar, const float* rpar, const int* flogrd, const int* flogr2,
+                    const float* d_va, int nspec, int nsealm, const float* cg, const float* wn,
+                    const float* dw, const float* sig, const float* dden, const float* dsii,
+                    const float* ecos, const float* esin, const float* ec2, const float* es2,
+                    const float* esc, const int* mapsf, const int* mapsta, float* ebd,
+                    float* const* fields, void* stream) {
+  OutgCall c;
+  const int prc =
+      outg_packets(ipar, rpar, flogrd, flogr2, nspec, nsealm, fields, "ww_outg_device", c);
+  if (prc != WW_KOKKOS_OK) return prc;
+  if (c.a.nseal > 0 && ebd == nullptr)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_device: a null EBD work array");
+  if (!runtime().ready) return fail(WW_KOKKOS_ERR_NOT_INITIALISED, "before ww_kokkos_init");
+  OutgArgs& a = c.a;
+  a.va = d_va;
+  a.cg = cg;
+  a.wn = wn;
+  a.dw = dw;
+  a.sig = sig;
+  a.dden = dden;
+  a.dsii = dsii;
+  a.ecos = ecos;
+  a.esin = esin;
+  a.ec2 = ec2;
+  a.es2 = es2;
+  a.esc = esc;
+  a.mapsf = mapsf;
+  a.mapsta = mapsta;
+  a.ebd = ebd;
+  for (int k = 0; k < kOutgNField; ++k) {
+    const bool on = k < kOutgN1d || (k < OG_P2SMS ? a.f3[k - kOutgN1d] != 0 : a.f69 != 0);
+    a.f[k] = on ? fields[k] : nullptr;
+  }
+  launch_outg(a, static_cast<cudaStream_t>(stream));
+  g_calls.fetch_add(1, std::memory_order_relaxed);
+  g_points.fetch_add(a.nseal, std::memory_order_relaxed);
   g_outg.ok();
   return WW_KOKKOS_OK;
 }
@@ -400,6 +472,26 @@ int ww_outg_va(int igrid, const int* ipar, int nipar, const float* rpar, int nrp
   return guarded([&] {
     return run_outg(igrid, ipar, rpar, flogrd, flogr2, flogrr, va, nspec, nsealm, cg, wn, dw, sig,
                     dden, dsii, ecos, esin, ec2, es2, esc, mapsf, mapsta, fields);
+  });
+}
+
+int ww_outg_device(const int* ipar, int nipar, const float* rpar, int nrpar, const int* flogrd,
+                   const int* flogr2, const float* d_va, int nspec, int nsealm, const float* cg,
+                   const float* wn, const float* dw, const float* sig, const float* dden,
+                   const float* dsii, const float* ecos, const float* esin, const float* ec2,
+                   const float* es2, const float* esc, const int* mapsf, const int* mapsta,
+                   float* ebd, float* const* fields, int nfields, void* stream) {
+  if (ipar == nullptr || rpar == nullptr || nipar != kNIpar || nrpar != kNRpar ||
+      nfields != kOutgNField || fields == nullptr || flogrd == nullptr || flogr2 == nullptr)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_device: bad packet");
+  if (d_va == nullptr || cg == nullptr || wn == nullptr || dw == nullptr || sig == nullptr ||
+      dden == nullptr || dsii == nullptr || ecos == nullptr || esin == nullptr || ec2 == nullptr ||
+      es2 == nullptr || esc == nullptr || mapsf == nullptr || mapsta == nullptr)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_outg_device: a null pointer");
+  return guarded([&] {
+    return run_outg_device(ipar, rpar, flogrd, flogr2, d_va, nspec, nsealm, cg, wn, dw, sig,
+                           dden, dsii, ecos, esin, ec2, es2, esc, mapsf, mapsta, ebd, fields,
+                           stream);
   });
 }
 

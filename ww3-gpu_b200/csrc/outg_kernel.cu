@@ -83,7 +83,9 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
   const int j0 = jsea - 1;
   const int isea = jsea;  // W3_SHRD: ISEA = JSEA
   const int ix = a.mapsf[isea - 1], iy = a.mapsf[a.nsea + isea - 1];
-  const bool sea = a.mapsta[(ix - 1) * a.ny + (iy - 1)] > 0;
+  // A MAPSF cell outside the grid (only a device caller can pass one unchecked) reads as land.
+  const bool in_grid = ix >= 1 && ix <= a.nx && iy >= 1 && iy <= a.ny;
+  const bool sea = in_grid && a.mapsta[(ix - 1) * a.ny + (iy - 1)] > 0;
   const float* __restrict__ A = a.va + static_cast<size_t>(jsea) * a.nspec;  // A(ITH,IK)
   auto AA = [&](int ith, int ik) { return A[(ith - 1) + (ik - 1) * nth]; };
   auto cg = [&](int ik) { return a.cg[static_cast<size_t>(isea) * nk2 + ik]; };
