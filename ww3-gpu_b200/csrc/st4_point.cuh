@@ -81,6 +81,17 @@ WWB_PD int nint(float x) {
                                                    : 0;
 }
 WWB_PD float fabs_f(float x) { return fabsf(x); }
+/// A load of a large read-only table that is streamed once per use (CUMULW): it is not kept in
+/// L1, so the small tables and the stack that the serial chains read stay there.
+WWB_PD float ld_stream(const float* p) {
+#if defined(__CUDA_ARCH__)
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+#else
+  return *p;
+#endif
+}
 WWB_PD float sqrt_f(float x) { return sqrtf(x); }
 WWB_PD bool isnan_f(float x) { return x != x; }
 
@@ -1104,10 +1115,12 @@ WWB_PN void sds4(const Cta& cta, const st4::Params& p, const Fields& f, const fl
               const int is2 = (ik2 - 1) * nth;
               float v = zero;
               // CUMULW(IS2+J, IS) for the threads' consecutive IS are consecutive in the
-              // transposed copy: one coalesced row per J.
-              const float* const row = f.cumulw + static_cast<size_t>(is2) * f.cumulw_ld + (is - 1);
+              // transposed copy: one coalesced row per J, streamed past L1.
+              const float* const row =
+                  f.cumulw + static_cast<size_t>(is2) * f.cumulw_ld + (is - 1);
               for (int j = 1; j <= nth; ++j)
-                v = v + row[static_cast<size_t>(j - 1) * f.cumulw_ld] * brlambda[is2 + j - 1];
+                v = v + ld_stream(row + static_cast<size_t>(j - 1) * f.cumulw_ld) *
+                            brlambda[is2 + j - 1];
               renewalfreq = renewalfreq + v;
             }
           }
