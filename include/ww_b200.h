@@ -300,6 +300,44 @@ int ww_step_nodes(int igrid);
  * ww_utrn call (the reference returns it only). */
 int ww_prop3_last_error(void);
 
+/* ---------------------------------------------------------------- W3WAVE's support routines */
+/* Replace the entries of ww_kokkos_c.hpp:893-921 (argument tables in the reference's
+ * wave_support_shim.cpp): W3GATH, W3SCAT (W3_SHRD), W3UWND (WNT1, RWND), W3UTRN (IC0), W3DZXY,
+ * W3MAP3, W3MAPT (PR3) and DISTAB. No per-grid state: every call passes its sizes, copies its
+ * arrays in and its results out. Each returns OK, NOT_INITIALISED, BAD_SHAPE, KERNEL or RUNTIME
+ * (BAD_SHAPE also for a MAPSF or MAPFS entry outside the grid, which the kernels would index).
+ * MAPSF is MAPSF(MSEA,3); VA is VA(NSPEC, 0:NSEALM) with ncol = NSEALM+1 columns; FIELD is
+ * FIELD(1-NY:NY*(NX+2)). WW_KOKKOS_WAVE_COUNT=1 prints "ww_kokkos: W3<R> calls: N" at exit. */
+int ww_wave_gath(int ispec, int nspec, int nsea, int ncol, int msea, int nx, int ny,
+                 const float* va, const int* mapsf, float* field);
+int ww_wave_scat(int ispec, int nspec, int nsea, int ncol, int msea, int nx, int ny,
+                 const int* mapsta, const float* field, const int* mapsf, float* va);
+/* dt0n = DSEC21(TW0,TWN), dt0t = DSEC21(TW0,TIME) as stored REALs; wx0..dtn (NX,NY); cx, cy and
+ * ua0..u10d (NSEA); UA0..ASI are written when flfrst, read otherwise. */
+int ww_wave_uwnd(int flfrst, float dt0n, float dt0t, int flcur, float rwindc, int nsea, int msea,
+                 int nx, int ny, const int* mapsf, const float* wx0, const float* wy0,
+                 const float* dt0, const float* wxn, const float* wyn, const float* dtn,
+                 const float* cx, const float* cy, float* ua0, float* uai, float* ud0,
+                 float* udi, float* as0, float* asi, float* ua, float* ud, float* as,
+                 float* u10, float* u10d);
+/* trny[-1] is read as the Fortran's TRNY(0) under TRFLAG 1, 3, 5 when cell 1 is a sea point. */
+int ww_wave_utrn(int nx, int ny, int nsea, int msea, int trflag, float fice0, float ficen,
+                 float ficel, float ffacberg, int flagll, const float* trnx, const float* trny,
+                 const int* mapsf, const int* mapsta, const float* hpfac, const float* hqfac,
+                 const float* ice, const float* berg, float* atrnx, float* atrny);
+int ww_wave_dzxy(int nsea, int nx, int ny, const float* zz, const int* mapsta, const int* mapfs,
+                 const float* dpdx, const float* dpdy, const float* dqdx, const float* dqdy,
+                 int flagll, int iclose, float* dzzdx, float* dzzdy);
+/* GTYPE < 3 only (BAD_SHAPE otherwise); counts = NMX0..NMX2, NMY0..NMY2, NACT, NCENT. */
+int ww_wave_map3(int nx, int ny, int nsea, int msea, int nk, int nth, int gtype, const int* mapsta,
+                 const int* mapsf, int* mapx2, int* mapy2, int* mapaxy, int* mapcxy, int* mapth2,
+                 int* mapwn2, int* counts);
+int ww_wave_mapt(int nsea, int msea, int ncell, const int* mapsf, const float* atrnx,
+                 const float* atrny, int* maptrn);
+/* NAR1D must be 121; ewn1, ecg1 (0:NAR1D) in: the Fortran's tables (the differing values are
+ * counted on stderr), out: the device's; n1max, dsie likewise. */
+int ww_wave_distab(int nar1d, float* ewn1, float* ecg1, int* n1max, float* dsie);
+
 /* ---------------------------------------------------------------- gridded output (W3OUTG) */
 /* Replaces ww_outg_va (outg_c.hpp:97-120): W3OUTG (VA, .FALSE., FLOUTG, FLOUTG2) of
  * w3iogomd.F90:1201-2380, sections 1-4 and the space-time extremes, on the resident VA of grid

@@ -22,6 +22,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -162,6 +163,7 @@ class View {
   using reference_type = value_type&;
   using array_layout = typename Impl::view_props<Props...>::layout;
   using memory_space = HostSpace;
+  using device_type = HostSpace;
   using execution_space = void;
   using HostMirror = View;
   using host_mirror_type = View;
@@ -199,7 +201,8 @@ class View {
   template <class D2, class... P2,
             class = std::enable_if_t<
                 View<D2, P2...>::Rank == Rank &&
-                std::is_same_v<typename View<D2, P2...>::array_layout, array_layout> &&
+                (Rank <= 1 ||
+                 std::is_same_v<typename View<D2, P2...>::array_layout, array_layout>) &&
                 std::is_convertible_v<typename View<D2, P2...>::value_type*, value_type*>>>
   View(const View<D2, P2...>& o) {
     ptr_ = o.data();
@@ -555,6 +558,24 @@ class RangePolicy {
   std::int64_t b_, e_;
 };
 
+template <unsigned N>
+struct Rank {};
+
+/// A 2-D iteration space [b0, e0) x [b1, e1); the policy's Rank<2> is the only one used.
+template <class... P>
+class MDRangePolicy {
+ public:
+  using execution_space = typename Impl::policy_exec<P...>::type;
+  using point = std::array<std::int64_t, 2>;
+  MDRangePolicy(const point& b, const point& e) : b_(b), e_(e) {}
+  MDRangePolicy(const execution_space&, const point& b, const point& e) : b_(b), e_(e) {}
+  const point& lower() const { return b_; }
+  const point& upper() const { return e_; }
+
+ private:
+  point b_, e_;
+};
+
 template <class Member>
 struct TeamThreadRangeBoundaries {
   int start;
@@ -628,6 +649,20 @@ void parallel_for(const std::string&, const RangePolicy<P...>& pol, const F& f) 
 }
 template <class... P, class F>
 void parallel_for(const RangePolicy<P...>& pol, const F& f) { parallel_for(std::string(), pol, f); }
+template <class... P, class F>
+void parallel_for(const std::string&, const MDRangePolicy<P...>& pol, const F& f) {
+  using Exec = typename MDRangePolicy<P...>::execution_space;
+  const bool par = Exec::kParallel && !Impl::nested();
+  const std::int64_t b0 = pol.lower()[0], e0 = pol.upper()[0];
+  const std::int64_t b1 = pol.lower()[1], e1 = pol.upper()[1];
+#pragma omp parallel for if (par) schedule(static)
+  for (std::int64_t i = b0; i < e0; ++i)
+    for (std::int64_t j = b1; j < e1; ++j) f(static_cast<int>(i), static_cast<int>(j));
+}
+template <class... P, class F>
+void parallel_for(const MDRangePolicy<P...>& pol, const F& f) {
+  parallel_for(std::string(), pol, f);
+}
 template <class F>
 void parallel_for(const std::string& label, std::size_t n, const F& f) {
   parallel_for(label, RangePolicy<>(0, static_cast<std::int64_t>(n)), f);

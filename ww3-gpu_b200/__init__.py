@@ -48,7 +48,8 @@ EXPORTS = (
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
     "ww_map3", "ww_map3_device", "ww_mapt", "ww_utrn", "ww_step_begin", "ww_step_end",
     "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes", "ww_outg_va", "ww_outg_part",
-    "ww_outg_last_error", "ww_outg_device",
+    "ww_outg_last_error", "ww_outg_device", "ww_wave_gath", "ww_wave_scat", "ww_wave_uwnd",
+    "ww_wave_utrn", "ww_wave_dzxy", "ww_wave_map3", "ww_wave_mapt", "ww_wave_distab",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")

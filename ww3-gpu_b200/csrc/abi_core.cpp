@@ -32,6 +32,7 @@ void release_srce_contexts();  // abi_srce.cpp
 void release_st4_contexts();   // abi_st4.cpp
 void release_steps();          // abi_step.cpp
 void release_outg_staging();   // abi_outg.cpp
+void release_wave_staging();   // abi_wave.cpp
 
 namespace {
 
@@ -212,6 +213,7 @@ void ww_kokkos_finalize(void) {
   wwb::release_va_contexts();
   wwb::release_prop3_staging();
   wwb::release_outg_staging();
+  wwb::release_wave_staging();
   cudaDeviceSynchronize();
   if (rt.stream) cudaStreamDestroy(rt.stream);
   if (rt.copy_in) cudaStreamDestroy(rt.copy_in);
