@@ -1,6 +1,6 @@
 """Benchmark of WAVEWATCH III's per-sea-point hot path on B200: sea-point·steps/s at 36x36 bins.
 
-Four workloads (--workload):
+Five workloads (--workload):
 
 * srce (default) -- the full plain source-term step W3SRCE with ST4 (W3SIN4 + W3SDS4 + W3SPR4),
   the DIA (W3SNL1), W3SBT1 and W3SDB1 on 9520 sea points, 36 x 36 float32, DTG = 900 s with
@@ -29,6 +29,10 @@ Four workloads (--workload):
   maps from this project's device W3MAP3. e2e uploads the host VA, runs the step and reads the VA
   back, every step.
 
+* multigrid -- config 4's plain form: 16 regional grids of uneven size (sea points log-uniform
+  in 5k-400k times --scale, default 1/16), each with its own winds and depths, every grid's
+  whole step recorded once and all grids replayed as one CUDA graph per step (ww_steps_run),
+  the grids' branches side by side; the line also gives the grid-after-grid replay.
 * outg -- W3OUTG (ww_outg_device on device arrays; e2e: ww_outg_va with the VA newer on the
   host, the grid arrays copied in and the requested fields copied back) on the resident VA of the
   same --nx x --ny grid, every field the device computes requested, space-time extremes on.
@@ -72,7 +76,10 @@ def parse():
     p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=None)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--workload", choices=["srce", "dia", "step", "outg"], default="srce")
+    p.add_argument("--workload", choices=["srce", "dia", "step", "outg", "multigrid"],
+                   default="srce")
+    p.add_argument("--scale", type=float, default=1.0 / 16.0,
+                   help="multigrid workload: factor on the 5k-400k sea points of each grid")
     p.add_argument("--nx", type=int, default=360, help="step/outg workloads: grid longitudes")
     p.add_argument("--ny", type=int, default=180, help="step/outg workloads: grid latitudes")
     p.add_argument("--npts", type=int, default=None)
@@ -83,7 +90,7 @@ def parse():
     a = p.parse_args()
     srce = a.workload == "srce"
     if a.steps is None:
-        a.steps = {"srce": 20, "dia": 200, "step": 10, "outg": 20}[a.workload]
+        a.steps = {"srce": 20, "dia": 200, "step": 10, "outg": 20, "multigrid": 5}[a.workload]
     if a.warmup is None:
         a.warmup = 5 if a.workload == "dia" else 3
     if a.npts is None:
@@ -882,6 +889,195 @@ def run_reference_step(args):
     return 0
 
 
+# ------------------------------------------------------------------------ multi-grid workload
+MULTI_NGRIDS = 16
+MULTI_WORKLOAD = ("{ngrids} regional grids of uneven size (sea points log-uniform in {lo}-{hi}, "
+                  "seeded; {total} in all), each with its own wind field and depth, 36x36: every "
+                  "grid's resident whole step (W3KTP3, W3XYP3, W3KTP3, W3SRCE + ST4 + DIA) "
+                  "recorded once, all grids replayed as one CUDA graph per step (ww_steps_run), "
+                  "the grids' branches side by side")
+
+
+def multi_shapes(scale, seed=2026):
+    """(nx, ny) of each grid: sea points log-uniform in [5000, 400000] * scale, on a 2:1 lon/lat
+    grid whose smooth land mask leaves about 70 % sea."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    target = np.exp(rng.uniform(np.log(5000.0), np.log(400000.0), MULTI_NGRIDS)) * scale
+    shapes = []
+    for n in target:
+        ny = max(8, int(round((n / 0.7 / 2.0) ** 0.5)))
+        shapes.append((2 * ny, ny))
+    return shapes
+
+
+def run_b200_multigrid(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
+    torch.cuda.set_device(local)
+    os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    pkg = entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    pkg.init()
+
+    def map3(nx, ny, nsea, nk, nth, mapsta, mapsf):  # this project's device W3MAP3
+        rc, m = pkg.map3(nx, ny, nsea, nk, nth, mapsta, mapsf)
+        if rc != 0:
+            raise SystemExit(f"ww_map3 failed ({rc})")
+        return m["mapx2"], m["mapy2"], m["mapaxy"], m["mapcxy"][:nsea], m["counts"]
+
+    shapes = multi_shapes(args.scale, 2026 + rank)
+    grids = []
+    for k, (nx, ny) in enumerate(shapes):
+        ig = 100 + k
+        st, t, sr, cfg, sig, xc, kc, pts = step_inputs(synth, map3, nx, ny, 3000 + 17 * k + rank)
+        nsea = xc["nsea"]
+        grid = pkg.SrceGrid(ig, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig,
+                            sr)
+        va = np.array(xc["va"], np.float32, copy=True)
+
+        def srce(v, jsea, pk, shave, grid=grid, nsea=nsea):
+            grid.batch_va(nsea, v, jsea, pk["wn1"], pk["cg1"], pk["pin"], pk["psc"],
+                          pk["whitecap"], pk["taubbl"], pk["tauice"], shave)
+
+        one = step_calls((lambda c, it, v, ig=ig: pkg.ktp3_batch(c, it, 1, ig, v),
+                          lambda c, v, ig=ig: pkg.xyp3_batch(c, ig, v), srce), va, kc, xc, pts,
+                         nsea)
+        step = pkg.Step(ig)
+        with step:
+            one()
+        grids.append({"ig": ig, "nsea": nsea, "va": va, "step": step, "grid": grid,
+                      "nx": nx, "ny": ny})
+    igs = [g["ig"] for g in grids]
+    total = sum(g["nsea"] for g in grids)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    def timed(fn, steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        barrier()
+        ev[0].record(stream)
+        for i in range(steps):
+            fn()
+            ev[i + 1].record(stream)
+        barrier()
+        return max_over_ranks(ev[0].elapsed_time(ev[-1])), [
+            ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+
+    together = lambda: pkg.steps_run(igs, 1, handle)  # noqa: E731
+
+    def one_by_one():
+        for g in grids:
+            g["step"].run(1, handle)
+
+    for _ in range(args.warmup):
+        together()
+    barrier()
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        total_ms, per = timed(together, args.steps)
+    seq_ms, _ = timed(one_by_one, max(1, min(args.steps, 3)))
+    seq_steps = max(1, min(args.steps, 3))
+    value = total * world * args.steps / (total_ms / 1e3)
+    seq_value = total * world * seq_steps / (seq_ms / 1e3)
+
+    # ---- end to end: every grid's host VA uploaded, the combined step, every VA read back
+    L = pkg.lib()
+    e2e_steps = args.e2e_steps or max(2, min(args.steps, 3))
+
+    def host_step():
+        for g in grids:
+            v = g["va"]
+            assert L.ww_va_host_write(g["ig"], v.ctypes.data, v.shape[1], v.shape[0] - 1) == 0
+        pkg.steps_run(igs, 1, None)
+        for g in grids:
+            v = g["va"]
+            assert L.ww_va_host_read(g["ig"], v.ctypes.data, v.shape[1], v.shape[0] - 1) == 0
+
+    host_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_step()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    va_bytes = int(sum(g["va"].nbytes for g in grids))
+    peak, peak_kind = measured_peak_hbm()
+    step_ms = statistics.median(per)
+    achieved = STEP_BYTES_PER_POINT * total / (step_ms / 1e3) / 1e9
+    lo, hi = int(5000 * args.scale), int(400000 * args.scale)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": MULTI_WORKLOAD.format(ngrids=len(grids), lo=lo, hi=hi,
+                                                     total=total),
+                   "nk": NK, "nth": NTH, "ngrids": len(grids), "scale": args.scale,
+                   "grids": [[g["nx"], g["ny"], g["nsea"]] for g in grids],
+                   "sea_points_per_gpu": total, "dtg_s": 900.0,
+                   "source_terms": "plain DIA (the learned surrogate is not built)",
+                   "l2": "the grids' resident VAs together are larger than L2",
+                   "parallelism": f"all grids on each GPU ({world}), no collective"},
+        "sequential": {"value": seq_value, "unit": UNIT, "steps": seq_steps,
+                       "ms_per_step": seq_ms / seq_steps,
+                       "note": "the same recorded steps replayed grid after grid (ww_step_run)"},
+        "e2e": {"value": total * world * e2e_steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": va_bytes, "d2h_bytes_per_step": va_bytes,
+                "steps": e2e_steps,
+                "host_entry": "ww_va_host_write + ww_steps_run + ww_va_host_read"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": None, "kernel": "the combined step graph (srce_kernel dominant)",
+                     "launch_ms": step_ms, "algorithmic_bytes_per_point": STEP_BYTES_PER_POINT},
+        "gpu_launches": sum(g["step"].nodes() for g in grids) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_step(synth, 90, 45)
+        if r is not None:
+            rate, kind, cores, sample = r
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                    "sample": sample + " (per-point cost does not depend on the "
+                                    "grid split)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for g in grids:
+        g["step"].free()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_reference_multigrid(args):
+    """The reference's own four calls per step on a 90 x 45 grid of the workload: its per-point
+    cost does not depend on how the points are split into grids."""
+    a = argparse.Namespace(**vars(args))
+    a.nx, a.ny = 360, 180
+    return run_reference_step(a)
+
+
 # ---------------------------------------------------------------------------- W3OUTG workload
 OUTG_WORKLOAD = ("W3OUTG (ww_outg_va: sections 1-4 and the space-time extremes, every field "
                  "the device computes requested) on the resident VA of a {nx}x{ny} grid "
@@ -1129,6 +1325,9 @@ def main():
         return run_reference_step(args) if args.impl == "reference" else run_b200_step(args)
     if args.workload == "outg":
         return run_reference_outg(args) if args.impl == "reference" else run_b200_outg(args)
+    if args.workload == "multigrid":
+        return (run_reference_multigrid(args) if args.impl == "reference"
+                else run_b200_multigrid(args))
     return run_reference_srce(args) if args.impl == "reference" else run_b200_srce(args)
 
 

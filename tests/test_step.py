@@ -168,3 +168,46 @@ def test_step_protocol(pkg):
     assert step.ops() == 0
     step.run(3)  # an empty step replays nothing
     step.free()
+
+
+def test_steps_run_grids_side_by_side(pkg, oracle, synth):
+    """Three grids of different sizes, each with its own recorded step: ww_steps_run replays
+    them as one graph (the grids' branches side by side) and gives every grid the VA that its
+    own ww_step_run gives."""
+    st = synth.st4_setup(variant="default")
+    t = oracle.st4_tables(st)
+    sr = synth.srce_setup(st)
+    cases = []
+    for nx, ny, seed in [(24, 18, 51), (40, 22, 52), (16, 12, 53)]:
+        xc = synth.xyp3_case(nx, ny, seed=seed, ref=oracle.ref_w3map3)
+        nsea = xc["nsea"]
+        cases.append((xc, synth.ktp3_case(nsea, seed=seed + 1, nsea=nsea),
+                      synth.srce_points(nsea, seed=seed + 2)))
+
+    def record(base):
+        calls, steps = [], []
+        for k, (xc, kc, pts) in enumerate(cases):
+            ig = base + k
+            L = _gpu_grid(pkg, oracle, synth, st, t, sr, ig)
+            c = Calls(L, ig, np.array(xc["va"], np.float32, copy=True), kc, xc, pts)
+            step = pkg.Step(ig)
+            with step:
+                c.step()
+            calls.append(c)
+            steps.append(step)
+        return calls, steps
+
+    sep_calls, sep_steps = record(720)
+    for s in sep_steps:
+        s.run(2)
+    va_sep = [np.array(c.read(), copy=True) for c in sep_calls]
+    com_calls, com_steps = record(730)
+    pkg.steps_run([730, 731, 732], 2)
+    va_com = [np.array(c.read(), copy=True) for c in com_calls]
+    for k in range(3):
+        assert_bitexact(va_com[k], va_sep[k], f"grid {k}: ww_steps_run vs ww_step_run")
+        assert not np.array_equal(va_com[k], cases[k][0]["va"])
+    with pytest.raises(pkg.WwError):
+        pkg.steps_run([730, 730], 1)  # a grid listed twice
+    for s in sep_steps + com_steps:
+        s.free()

@@ -47,7 +47,7 @@ EXPORTS = (
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
     "ww_map3", "ww_map3_device", "ww_mapt", "ww_utrn", "ww_step_begin", "ww_step_end",
-    "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes", "ww_outg_va", "ww_outg_part",
+    "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes", "ww_steps_run", "ww_outg_va", "ww_outg_part",
     "ww_outg_last_error", "ww_outg_device", "ww_wave_gath", "ww_wave_scat", "ww_wave_uwnd",
     "ww_wave_utrn", "ww_wave_dzxy", "ww_wave_map3", "ww_wave_mapt", "ww_wave_distab",
 )
@@ -495,6 +495,18 @@ class Step:
 
     def free(self):
         self.L.ww_step_free(self.igrid)
+
+
+def steps_run(igrids, nrep=1, stream=None):
+    """ww_steps_run: the recorded steps of several grids replayed as one CUDA graph, the grids
+    side by side."""
+    L = lib()
+    L.ww_steps_run.argtypes = [_P, _I, _I, _P]
+    L.ww_steps_run.restype = _I
+    ids = np.ascontiguousarray(igrids, np.int32)
+    rc = L.ww_steps_run(ids.ctypes.data, ids.size, nrep, stream)
+    if rc != OK:
+        raise WwError("ww_steps_run", rc)
 
 
 def xyp3_batch(case, igrid=None, va=None):

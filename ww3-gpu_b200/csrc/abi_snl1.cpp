@@ -17,6 +17,7 @@
 
 #include "snl1_kernel.cuh"
 #include "snl1_tables.hpp"
+#include "step.hpp"
 #include "wwb_common.hpp"
 
 namespace wwb {
@@ -32,7 +33,7 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { reset(); }
   void reset() {
-    if (ptr) cudaFree(ptr);
+    free_table(ptr);
     ptr = nullptr;
     n = 0;
   }

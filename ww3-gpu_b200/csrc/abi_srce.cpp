@@ -38,11 +38,9 @@ struct DevVec {
   DevVec() = default;
   DevVec(const DevVec&) = delete;
   DevVec& operator=(const DevVec&) = delete;
-  ~DevVec() {
-    if (ptr) cudaFree(ptr);
-  }
+  ~DevVec() { free_table(ptr); }
   void upload(const T* h, size_t n) {
-    if (ptr) cudaFree(ptr);
+    free_table(ptr);
     ptr = nullptr;
     WWB_CHECK(cudaMalloc(&ptr, (n ? n : 1) * sizeof(T)));
     if (n) WWB_CHECK(cudaMemcpy(ptr, h, n * sizeof(T), cudaMemcpyHostToDevice));

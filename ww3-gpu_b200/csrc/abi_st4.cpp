@@ -21,6 +21,7 @@
 #include "st4_registry.hpp"
 #include "st4_srce.cuh"
 #include "staging.hpp"
+#include "step.hpp"
 #include "wwb_common.hpp"
 
 namespace wwb {
@@ -36,11 +37,9 @@ struct DevVec {
   DevVec() = default;
   DevVec(const DevVec&) = delete;
   DevVec& operator=(const DevVec&) = delete;
-  ~DevVec() {
-    if (ptr) cudaFree(ptr);
-  }
+  ~DevVec() { free_table(ptr); }
   void upload(const std::vector<T>& h) {
-    if (ptr) cudaFree(ptr);
+    free_table(ptr);
     ptr = nullptr;
     n = h.size();
     if (n == 0) return;

@@ -30,4 +30,9 @@ cudaStream_t step_stream(StepRecorder* r);
 /// Frees every recorded step (ww_kokkos_finalize).
 void release_steps();
 
+/// Frees a device table of a grid's configuration (DIA, ST4, W3SRCE arrays) that a new
+/// registration replaces: at once when no recorded step exists, else when the last recorded step
+/// is freed, since a recorded step keeps the table addresses it was recorded with.
+void free_table(void* p);
+
 }  // namespace wwb
