@@ -31,8 +31,9 @@ Five workloads (--workload):
 
 * multigrid -- config 4's plain form: 16 regional grids of uneven size (sea points log-uniform
   in 5k-400k times --scale, default 1/16), each with its own winds and depths, every grid's
-  whole step recorded once and all grids replayed as one CUDA graph per step (ww_steps_run),
-  the grids' branches side by side; the line also gives the grid-after-grid replay.
+  whole step recorded once and all grids' graphs replayed one after another per step
+  (ww_steps_run); the line also gives the replay by one ww_step_run call per grid
+  ("sequential").
 * outg -- W3OUTG (ww_outg_device on device arrays; e2e: ww_outg_va with the VA newer on the
   host, the grid arrays copied in and the requested fields copied back) on the resident VA of the
   same --nx x --ny grid, every field the device computes requested, space-time extremes on.
@@ -894,8 +895,8 @@ MULTI_NGRIDS = 16
 MULTI_WORKLOAD = ("{ngrids} regional grids of uneven size (sea points log-uniform in {lo}-{hi}, "
                   "seeded; {total} in all), each with its own wind field and depth, 36x36: every "
                   "grid's resident whole step (W3KTP3, W3XYP3, W3KTP3, W3SRCE + ST4 + DIA) "
-                  "recorded once, all grids replayed as one CUDA graph per step (ww_steps_run), "
-                  "the grids' branches side by side")
+                  "recorded once as a CUDA graph, all grids' graphs replayed one after another "
+                  "per step (ww_steps_run)")
 
 
 def multi_shapes(scale, seed=2026):

@@ -291,10 +291,10 @@ int ww_step_begin(int igrid);
 int ww_step_end(int igrid);
 int ww_step_run(int igrid, int nrep, void* stream);
 int ww_step_free(int igrid);
-/* B200 extension: the recorded steps of ngrids distinct grids replayed nrep times as one CUDA
- * graph, each grid's step a branch with no edge to the others, so the grids' kernels run side by
- * side (several regional grids of uneven size on one GPU). The combined graph is built on the
- * first call for this list and kept while none of the grids re-records. Return WwKokkosStatus. */
+/* B200 extension: the recorded steps of ngrids distinct grids replayed nrep times, the grids one
+ * after another in list order on `stream` (NULL: the library's stream, synchronised before
+ * returning): several regional grids of uneven size on one GPU in one call, with no host work
+ * besides the graph launches. Return WwKokkosStatus. */
 int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream);
 /* The number of calls the grid's step holds, or -1 for a grid without one. */
 int ww_step_ops(int igrid);

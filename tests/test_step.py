@@ -172,7 +172,7 @@ def test_step_protocol(pkg):
 
 def test_steps_run_grids_side_by_side(pkg, oracle, synth):
     """Three grids of different sizes, each with its own recorded step: ww_steps_run replays
-    them as one graph (the grids' branches side by side) and gives every grid the VA that its
+    them in one call and gives every grid the VA that its
     own ww_step_run gives."""
     st = synth.st4_setup(variant="default")
     t = oracle.st4_tables(st)

@@ -498,8 +498,7 @@ class Step:
 
 
 def steps_run(igrids, nrep=1, stream=None):
-    """ww_steps_run: the recorded steps of several grids replayed as one CUDA graph, the grids
-    side by side."""
+    """ww_steps_run: the recorded steps of several grids replayed one grid after another."""
     L = lib()
     L.ww_steps_run.argtypes = [_P, _I, _I, _P]
     L.ww_steps_run.restype = _I

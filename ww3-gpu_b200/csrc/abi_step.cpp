@@ -52,24 +52,6 @@ namespace {
 
 Status g_step;
 
-/// The steps of several grids as one graph: each grid's recorded step a child graph (a copy),
-/// with no edge between grids, so the replay runs the grids' kernels side by side.
-struct MultiStep {
-  std::vector<int> igrids;
-  std::vector<cudaGraph_t> members;  ///< the grids' recorded graphs when this was built
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  ~MultiStep() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-  }
-};
-
-std::vector<std::unique_ptr<MultiStep>>& multis() {
-  static auto* v = new std::vector<std::unique_ptr<MultiStep>>();
-  return *v;
-}
-
 /// Tables replaced while a recorded step may still read them.
 std::vector<void*>& retired() {
   static auto* v = new std::vector<void*>();
@@ -134,7 +116,6 @@ void free_table(void* p) {
 }
 
 void release_steps() {
-  multis().clear();
   recs().clear();
   flush_retired();
 }
@@ -211,47 +192,24 @@ int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream) {
   return guarded([&] {
     if (igrids == nullptr || ngrids < 1 || nrep < 0)
       return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_run: bad grid list or nrep");
-    std::vector<int> ids(igrids, igrids + ngrids);
-    std::vector<cudaGraph_t> members;
+    std::vector<StepRecorder*> rs;
     for (int k = 0; k < ngrids; ++k) {
       for (int j = 0; j < k; ++j)
-        if (ids[j] == ids[k])
+        if (igrids[j] == igrids[k])
           return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_run: a grid is listed twice");
-      StepRecorder* r = find(ids[k]);
-      if (!r || r->recording || !r->graph)
+      StepRecorder* r = find(igrids[k]);
+      if (!r || r->recording || !r->exec)
         return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_run: a grid has no recorded step");
-      members.push_back(r->graph);
+      rs.push_back(r);
     }
-    MultiStep* m = nullptr;
-    for (auto& c : multis())
-      if (c->igrids == ids && c->members == members) m = c.get();
-    if (m == nullptr) {
-      auto fresh = std::make_unique<MultiStep>();
-      fresh->igrids = ids;
-      fresh->members = members;
-      WWB_CHECK(cudaGraphCreate(&fresh->graph, 0));
-      for (cudaGraph_t g : members) {
-        cudaGraphNode_t node;
-        WWB_CHECK(cudaGraphAddChildGraphNode(&node, fresh->graph, nullptr, 0, g));
-      }
-      WWB_CHECK(cudaGraphInstantiate(&fresh->exec, fresh->graph, 0));
-      // A grid's step re-recorded makes the old combination stale: keep only current ones.
-      auto& v = multis();
-      for (auto it = v.begin(); it != v.end();) {
-        bool stale = false;
-        for (size_t k = 0; k < (*it)->igrids.size(); ++k) {
-          StepRecorder* r = find((*it)->igrids[k]);
-          if (!r || r->graph != (*it)->members[k]) stale = true;
-        }
-        it = stale ? v.erase(it) : it + 1;
-      }
-      v.push_back(std::move(fresh));
-      m = v.back().get();
-    }
+    // The grids' graphs one after another on one stream: a graph of all the grids' steps, as
+    // branches side by side or chained, measured slower (the grids' persistent W3SRCE launches
+    // compete for the same SMs when side by side).
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : runtime().stream;
-    for (int i = 0; i < nrep; ++i) WWB_CHECK(cudaGraphLaunch(m->exec, s));
+    for (int i = 0; i < nrep; ++i)
+      for (StepRecorder* r : rs) WWB_CHECK(cudaGraphLaunch(r->exec, s));
     if (nrep > 0)
-      for (int id : ids) va_device_written(id);
+      for (int k = 0; k < ngrids; ++k) va_device_written(igrids[k]);
     if (!stream) WWB_CHECK(cudaStreamSynchronize(s));
     g_step.ok();
     return static_cast<int>(WW_KOKKOS_OK);
@@ -261,10 +219,7 @@ int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream) {
 int ww_step_free(int igrid) {
   StepRecorder* r = find(igrid);
   if (r) r->clear();
-  if (!any_step()) {
-    multis().clear();
-    flush_retired();
-  }
+  if (!any_step()) flush_retired();
   g_step.ok();
   return WW_KOKKOS_OK;
 }
