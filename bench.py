@@ -762,6 +762,7 @@ def run_b200_step(args):
                               "95% of the step, is bound by its serial chains, not by HBM")},
         "gpu_launches": nodes * args.steps,
         "graph_nodes": nodes,
+        "per_step_ms": [round(x, 3) for x in per],
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
