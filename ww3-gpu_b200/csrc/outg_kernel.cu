@@ -1,11 +1,11 @@
 // ww3-gpu_b200/csrc/outg_kernel.cu
-// W3OUTG on sm_100a (see outg_kernel.cuh): one thread per sea point reads its column of the
-// resident VA and forms every integral in the reference's statement order.
+// W3OUTG on sm_100a (see outg_kernel.cuh): a CTA takes eight sea points; their per-IK work runs
+// one thread per (point, IK) and one thread per point adds it up in the reference's order.
 //
 // Reference: ww3-gpu kokkos/src/ww_kokkos/iogo_w3outg.hpp:198-598 (w3outg_point: sections 2-4 and
 // the space-time extremes of w3iogomd.F90:1201-2380), :603-690 (w3outg_part_point, section 6),
-// :693-713 (the whole-array assignments of section 1). The sums over ITH and IK of a point are
-// sequential in the reference, so a point is one thread: no reduction is reordered. MAX/MIN keep
+// :693-713 (the whole-array assignments of section 1). The sums over ITH (per IK) and over IK
+// (per point) are sequential in the reference and stay so: no reduction is reordered. MAX/MIN keep
 // the object's operand order per site (gt_sel / lt_sel), the folded PARAMETERs their float bits,
 // and the libm calls are the glibc-equal device functions; the THMP sine and cosine, which the
 // reference's host object takes from libmvec's 4-lane entries for most points, are the scalar
@@ -75,40 +75,47 @@ __global__ void outg_init_kernel(OutgArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
-  const int jsea = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (jsea > a.nseal) return;
+// ---------------------------------------------------------------------------------------------
+// W3OUTG with the point's independent work spread over the CTA: P points per CTA; the per-IK
+// work of section 2 (the band sums over ITH and every per-IK term) and of the space-time
+// extremes (the rotated band sums, the 21 PHI sums) runs one thread per (point, IK) or (point,
+// ITL); one thread per point then adds the terms over IK in the reference's order. Every sum keeps
+// its order and every term its association, so the bits are those of the one-thread form.
+constexpr int kOutgThreads = 128;
+constexpr int kRec = 32;  // floats of one (point, IK) record
+
+// Record slots (section 2's per-IK terms; the raw band sums of IK = NK for 3.b and MSC).
+enum : int {
+  R_EBD = 0, R_ETF, R_EWN, R_ETR, R_ET1, R_EET1, R_ET02, R_ETX, R_ETY, R_TUSX, R_TUSY, R_ETXX,
+  R_QK2, R_ETYY, R_ETXY, R_PRMS, R_F2, R_TPMS, R_ABR, R_ABA, R_ABD, R_UBR, R_UBA, R_UBD, R_USSX,
+  R_USSY, R_BHD, R_SXX, R_SYY, R_SXY, R_KD6, R_AB
+};
+static_assert(R_AB < kRec, "record layout");
+
+__global__ void __launch_bounds__(kOutgThreads) outg_cta_kernel(OutgArgs a, int P) {
+  extern __shared__ float sm[];
   const float zero = 0.0f, half = 0.5f, one = 1.0f, two = 2.0f, k1em7 = 1.E-7f;
-  const int nk = a.nk, nth = a.nth, nk2 = nk + 2;
-  const int j0 = jsea - 1;
-  const int isea = jsea;  // W3_SHRD: ISEA = JSEA
-  const int ix = a.mapsf[isea - 1], iy = a.mapsf[a.nsea + isea - 1];
-  // A MAPSF cell outside the grid (only a device caller can pass one unchecked) reads as land.
-  const bool in_grid = ix >= 1 && ix <= a.nx && iy >= 1 && iy <= a.ny;
-  const bool sea = in_grid && a.mapsta[(ix - 1) * a.ny + (iy - 1)] > 0;
-  const float* __restrict__ A = a.va + static_cast<size_t>(jsea) * a.nspec;  // A(ITH,IK)
-  auto AA = [&](int ith, int ik) { return A[(ith - 1) + (ik - 1) * nth]; };
-  auto cg = [&](int ik) { return a.cg[static_cast<size_t>(isea) * nk2 + ik]; };
-  auto wn = [&](int ik) { return a.wn[static_cast<size_t>(isea) * nk2 + ik]; };
-  float* const EBD = a.ebd + static_cast<size_t>(j0) * nk;
+  const int nk = a.nk, nth = a.nth, nk2 = nk + 2, tid = threadIdx.x;
+  const int first = blockIdx.x * P;  // the CTA's first point, 0-based
+  const int np = min(P, a.nseal - first);
+  float* const rec = sm;                                   // [P][nk][kRec]
+  float* const rot = rec + static_cast<size_t>(P) * nk * kRec;  // cth, sth, t02p, phi[21]
+  auto R = [&](int p, int ik) { return rec + (static_cast<size_t>(p) * nk + (ik - 1)) * kRec; };
+  // Per point: cth, sth, t02p, the raw band sums of IK = NK (6), PHI(21).
+  auto RT = [&](int p) { return rot + static_cast<size_t>(p) * 32; };
 
-  // 1. This point's share of the accumulators.
-  float et = zero, et02 = zero, ewn = zero, etr = zero, et1 = zero, eet1 = zero;
-  float etx = zero, ety = zero, etxx = zero, etyy = zero, etxy = zero;
-  float abr = zero, aba = zero, abd = zero, ubr = zero, uba = zero, ubd = zero;
-  float sxx = zero, syy = zero, sxy = zero, ussx = zero, ussy = zero, tusx = zero, tusy = zero;
-  float mscx = zero, mscy = zero, mscd = zero, prms = zero, tpms = zero, ettpmm = zero;
-  float etf = zero, qk2 = zero, bhd = zero;
-  float ab = zero, abx = zero, aby = zero, abx2 = zero, aby2 = zero, ab2x = zero, ab2y = zero;
-  float abxx = zero, abyy = zero, abxy = zero, abyx = zero, abst = zero, qk1 = zero;
-
-  // 2. The band sums per IK and their integrals.
-  for (int ik = 1; ik <= nk; ++ik) {
-    ab = zero; abx = zero; aby = zero; abx2 = zero; aby2 = zero; ab2x = zero; ab2y = zero;
-    abxx = zero; abyy = zero; abxy = zero; abyx = zero; abst = zero; qk1 = zero;
-    const float cgk = cg(ik), wnk = wn(ik), sigk = a.sig[ik];
+  // Phase A: one thread per (point, IK).
+  for (int pair = tid; pair < np * nk; pair += blockDim.x) {
+    const int p = pair / nk, ik = pair - p * nk + 1;
+    const int j0 = first + p, isea = j0 + 1;
+    const float* __restrict__ A = a.va + static_cast<size_t>(isea) * a.nspec + (ik - 1) * nth;
+    const float cgk = a.cg[static_cast<size_t>(isea) * nk2 + ik];
+    const float wnk = a.wn[static_cast<size_t>(isea) * nk2 + ik];
+    const float sigk = a.sig[ik];
+    float ab = zero, abx = zero, aby = zero, abx2 = zero, aby2 = zero, ab2x = zero, ab2y = zero;
+    float abxx = zero, abyy = zero, abxy = zero, abyx = zero, abst = zero, qk1 = zero;
     for (int ith = 1; ith <= nth; ++ith) {
-      const float aj = AA(ith, ik);
+      const float aj = A[ith - 1];
       const float ec = a.ecos[ith - 1], es = a.esin[ith - 1], c2 = a.ec2[ith - 1],
                   s2 = a.es2[ith - 1], sc = a.esc[ith - 1];
       ab = ab + aj;
@@ -120,7 +127,7 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
       ab2y = ab2y + aj * (two * sc);
       abyx = abyx + aj * sc;
       if (ith <= nth / 2) {
-        const float ah = AA(ith + nth / 2, ik);
+        const float ah = A[ith + nth / 2 - 1];
         abst = abst + aj * ah;
         const float q = aj + ah;
         qk1 = qk1 + q * q;
@@ -130,78 +137,63 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
       abyy = abyy + ((one + s2) * factor - half) * aj;
       abxy = abxy + sc * factor * aj;
     }
+    float* const r = R(p, ik);
     const float dsik = a.dsii[ik - 1];
     const float factor = a.dden[ik - 1] / cgk;
     float ebd = ab * factor;
-    et = et + ebd;
-    etf = etf + ebd * cgk;
-    ewn = ewn + ebd / wnk;
-    etr = etr + ebd / sigk;
-    et1 = et1 + ebd * sigk;
-    eet1 = eet1 + ebd * ebd * sigk / dsik;
-    et02 = et02 + ebd * (sigk * sigk);
-    etx = etx + abx * factor;
-    ety = ety + aby * factor;
-    tusx = tusx + abx * factor * kGrav * wnk / sigk;
-    tusy = tusy + aby * factor * kGrav * wnk / sigk;
+    r[R_EBD] = ebd;
+    r[R_ETF] = ebd * cgk;
+    r[R_EWN] = ebd / wnk;
+    r[R_ETR] = ebd / sigk;
+    r[R_ET1] = ebd * sigk;
+    r[R_EET1] = ebd * ebd * sigk / dsik;
+    r[R_ET02] = ebd * (sigk * sigk);
+    r[R_ETX] = abx * factor;
+    r[R_ETY] = aby * factor;
+    r[R_TUSX] = abx * factor * kGrav * wnk / sigk;
+    r[R_TUSY] = aby * factor * kGrav * wnk / sigk;
     const float wn2 = wnk * wnk;
-    etxx = etxx + abx2 * factor * wn2;
-    qk2 = qk2 + qk1 * factor * sigk / wnk;
-    etyy = etyy + aby2 * factor * wn2;
-    etxy = etxy + abyx * factor * wn2;
-
+    r[R_ETXX] = abx2 * factor * wn2;
+    r[R_QK2] = qk1 * factor * sigk / wnk;
+    r[R_ETYY] = aby2 * factor * wn2;
+    r[R_ETXY] = abyx * factor * wn2;
     const float jac = kTpi * sigk / cgk;
     const float factor2 = two * a.dth / kTpi2 * sigk * (jac * jac) * abst;
-    prms = prms + factor2 * two * dsik;
+    r[R_PRMS] = factor2 * two * dsik;
+    r[R_F2] = factor2;
+    r[R_TPMS] = kTpi / sigk;
     if (a.f69 && ik >= a.p2msf2 && ik <= a.p2msf3)
       put(a.f[OG_P2SMS], j0 + static_cast<size_t>(ik - a.p2msf2) * a.nfld, factor2 * two * kTpi);
-    if (factor2 > ettpmm) {
-      ettpmm = factor2;
-      tpms = kTpi / sigk;
-    }
-    if (ik == nk) {
-      const float s2 = sigk * sigk;
-      const float s5 = s2 * sigk * s2;
-      const float fac5 = s5 / kGrav2 / dsik;
-      const float ma = abx2 * factor * fac5;
-      const float mc = aby2 * factor * fac5;
-      const float mb = abyx * factor * fac5;
-      mscd = half * dm::atan2f(two * mb, ma - mc);
-      float cs, sn;
-      dm::sincosf(mscd, &sn, &cs);
-      mscx = ma * (cs * cs) + two * mb * sn * cs + ma * (sn * sn);
-      mscy = mc * (cs * cs) - two * mb * sn * cs + ma * (sn * sn);
-    }
-
     const float kd = gt_sel(wnk * a.dw[isea], 0.001f);
     float ussco;
+    r[R_KD6] = kd < 6.0f ? one : zero;
     if (kd < 6.0f) {
       const float sh = dm::sinhf(kd);
       const float fkd = factor / (sh * sh);
-      abr = abr + ab * fkd;
-      aba = aba + abx * fkd;
-      abd = abd + aby * fkd;
+      r[R_ABR] = ab * fkd;
+      r[R_ABA] = abx * fkd;
+      r[R_ABD] = aby * fkd;
       const float sg2 = sigk * sigk;
-      ubr = ubr + ab * sg2 * fkd;
-      uba = uba + abx * sg2 * fkd;
-      ubd = ubd + aby * sg2 * fkd;
+      r[R_UBR] = ab * sg2 * fkd;
+      r[R_UBA] = abx * sg2 * fkd;
+      r[R_UBD] = aby * sg2 * fkd;
       ussco = fkd * sigk * wnk * dm::coshf(two * kd);
-      bhd = bhd + kGrav * wnk * ebd / dm::sinhf(two * kd);
+      r[R_BHD] = kGrav * wnk * ebd / dm::sinhf(two * kd);
     } else {
       ussco = factor * sigk * two * wnk;
     }
     abxx = gt_sel(abxx, zero) * factor;
     abyy = gt_sel(zero, abyy) * factor;
     abxy = abxy * factor;
-    sxx = sxx + abxx;
-    syy = syy + abyy;
-    sxy = sxy + abxy;
+    r[R_SXX] = abxx;
+    r[R_SYY] = abyy;
+    r[R_SXY] = abxy;
     ebd = ebd / dsik;
-    EBD[ik - 1] = ebd;
+    a.ebd[static_cast<size_t>(j0) * nk + (ik - 1)] = ebd;
     if (a.f3[0] && ik >= a.e3df2[0] && ik <= a.e3df3[0])
       put(a.f[OG_EF], j0 + static_cast<size_t>(ik - a.e3df2[0]) * a.nfld, ebd * kTpi);
-    ussx = ussx + abx * ussco;
-    ussy = ussy + aby * ussco;
+    r[R_USSX] = abx * ussco;
+    r[R_USSY] = aby * ussco;
     if (a.f3[1] && ik >= a.e3df2[1] && ik <= a.e3df3[1])
       put(a.f[OG_TH1M], j0 + static_cast<size_t>(ik - a.e3df2[1]) * a.nfld,
           fmodf(630.0f - kRade * dm::atan2f(aby, abx), 360.0f));
@@ -218,21 +210,106 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
     if (a.f3[4] && ik >= a.e3df2[4] && ik <= a.e3df3[4])
       put(a.f[OG_STH2M], j0 + static_cast<size_t>(ik - a.e3df2[4]) * a.nfld,
           sqrtf(fabsf(half * (one - m2))) * kRade);
+    if (ik == nk) {  // the raw band sums of IK = NK (3.b's tail and MSC)
+      float* const t = RT(p);
+      t[3] = ab;
+      t[4] = abx;
+      t[5] = aby;
+      t[6] = abx2;
+      t[7] = aby2;
+      t[8] = abyx;
+    }
   }
+  __syncthreads();
 
-  // Space-time extremes, on ET, ET02, ET1, ETX, ETY before the tail of 3.b.
-  if (a.ste) {
-    const float undef = a.undef;
-    float thmp = undef;
-    if (sea && fabsf(etx) + fabsf(ety) > k1em7) thmp = dm::atan2f(ety, etx);
-    float sth, cth;
-    dm::sincosf(thmp, &sth, &cth);
-
-    float mssxm = zero, mssym = zero, mssxtm = zero, mssytm = zero, mssxym = zero;
+  // Phase B: one thread per point adds the terms over IK in order.
+  const bool mine = tid < np;
+  const int p = tid, j0 = first + tid, isea = j0 + 1;
+  float et = zero, et02 = zero, ewn = zero, etr = zero, et1 = zero, eet1 = zero;
+  float etx = zero, ety = zero, etxx = zero, etyy = zero, etxy = zero;
+  float abr = zero, aba = zero, abd = zero, ubr = zero, uba = zero, ubd = zero;
+  float sxx = zero, syy = zero, sxy = zero, ussx = zero, ussy = zero, tusx = zero, tusy = zero;
+  float mscx = zero, mscy = zero, mscd = zero, prms = zero, tpms = zero, ettpmm = zero;
+  float etf = zero, qk2 = zero, bhd = zero;
+  bool sea = false;
+  if (mine) {
+    const int ix = a.mapsf[isea - 1], iy = a.mapsf[a.nsea + isea - 1];
+    const bool in_grid = ix >= 1 && ix <= a.nx && iy >= 1 && iy <= a.ny;
+    sea = in_grid && a.mapsta[(ix - 1) * a.ny + (iy - 1)] > 0;
     for (int ik = 1; ik <= nk; ++ik) {
+      const float* const r = R(p, ik);
+      et = et + r[R_EBD];
+      etf = etf + r[R_ETF];
+      ewn = ewn + r[R_EWN];
+      etr = etr + r[R_ETR];
+      et1 = et1 + r[R_ET1];
+      eet1 = eet1 + r[R_EET1];
+      et02 = et02 + r[R_ET02];
+      etx = etx + r[R_ETX];
+      ety = ety + r[R_ETY];
+      tusx = tusx + r[R_TUSX];
+      tusy = tusy + r[R_TUSY];
+      etxx = etxx + r[R_ETXX];
+      qk2 = qk2 + r[R_QK2];
+      etyy = etyy + r[R_ETYY];
+      etxy = etxy + r[R_ETXY];
+      prms = prms + r[R_PRMS];
+      if (r[R_F2] > ettpmm) {
+        ettpmm = r[R_F2];
+        tpms = r[R_TPMS];
+      }
+      if (r[R_KD6] != zero) {
+        abr = abr + r[R_ABR];
+        aba = aba + r[R_ABA];
+        abd = abd + r[R_ABD];
+        ubr = ubr + r[R_UBR];
+        uba = uba + r[R_UBA];
+        ubd = ubd + r[R_UBD];
+        bhd = bhd + r[R_BHD];
+      }
+      sxx = sxx + r[R_SXX];
+      syy = syy + r[R_SYY];
+      sxy = sxy + r[R_SXY];
+      ussx = ussx + r[R_USSX];
+      ussy = ussy + r[R_USSY];
+    }
+    {  // MSC from the band sums of IK = NK
+      const float* const t = RT(p);
+      const float sigk = a.sig[nk], dsik = a.dsii[nk - 1];
+      const float factor = a.dden[nk - 1] / a.cg[static_cast<size_t>(isea) * nk2 + nk];
+      const float s2 = sigk * sigk;
+      const float s5 = s2 * sigk * s2;
+      const float fac5 = s5 / kGrav2 / dsik;
+      const float ma = t[6] * factor * fac5;
+      const float mc = t[7] * factor * fac5;
+      const float mb = t[8] * factor * fac5;
+      mscd = half * dm::atan2f(two * mb, ma - mc);
+      float cs, sn;
+      dm::sincosf(mscd, &sn, &cs);
+      mscx = ma * (cs * cs) + two * mb * sn * cs + ma * (sn * sn);
+      mscy = mc * (cs * cs) - two * mb * sn * cs + ma * (sn * sn);
+    }
+    if (a.ste) {
+      float thmp = a.undef;
+      if (sea && fabsf(etx) + fabsf(ety) > k1em7) thmp = dm::atan2f(ety, etx);
+      float sth, cth;
+      dm::sincosf(thmp, &sth, &cth);
+      RT(p)[0] = cth;
+      RT(p)[1] = sth;
+    }
+  }
+  __syncthreads();
+
+  // Phase C: the rotated band sums, one thread per (point, IK), into the records.
+  if (a.ste) {
+    for (int pair = tid; pair < np * nk; pair += blockDim.x) {
+      const int q = pair / nk, ik = pair - q * nk + 1;
+      const int jq = first + q, iq = jq + 1;
+      const float* __restrict__ A = a.va + static_cast<size_t>(iq) * a.nspec + (ik - 1) * nth;
+      const float cth = RT(q)[0], sth = RT(q)[1];
       float abx2m = zero, aby2m = zero, abxm = zero, abym = zero, abxym = zero;
       for (int ith = 1; ith <= nth; ++ith) {
-        const float aj = AA(ith, ik);
+        const float aj = A[ith - 1];
         const float ec = a.ecos[ith - 1], es = a.esin[ith - 1];
         const float u = ec * cth + es * sth;
         const float v = es * cth - ec * sth;
@@ -242,33 +319,48 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
         abym = abym + aj * v;
         abxym = abxym + aj * u * v;
       }
-      const float wnk = wn(ik);
-      const float factor = a.dden[ik - 1] / cg(ik);
+      const float wnk = a.wn[static_cast<size_t>(iq) * nk2 + ik];
+      const float factor = a.dden[ik - 1] / a.cg[static_cast<size_t>(iq) * nk2 + ik];
       const float wn2 = wnk * wnk;
-      mssxm = mssxm + abx2m * factor * wn2;
-      mssym = mssym + aby2m * factor * wn2;
-      mssxtm = mssxtm + abxm * factor * wnk * a.sig[ik];
-      mssytm = mssytm + abym * factor * wnk * a.sig[ik];
-      mssxym = mssxym + abxym * factor * wn2;
+      float* const r = R(q, ik);
+      r[0] = abx2m * factor * wn2;
+      r[1] = aby2m * factor * wn2;
+      r[2] = abxm * factor * wnk * a.sig[ik];
+      r[3] = abym * factor * wnk * a.sig[ik];
+      r[4] = abxym * factor * wn2;
     }
+  }
+  __syncthreads();
 
+  // Phase D: the space-time extremes' scalars of each point.
+  float sqet = zero, mode = zero, den = zero;
+  if (a.ste && mine) {
+    const float undef = a.undef;
+    float mssxm = zero, mssym = zero, mssxtm = zero, mssytm = zero, mssxym = zero;
+    for (int ik = 1; ik <= nk; ++ik) {
+      const float* const r = R(p, ik);
+      mssxm = mssxm + r[0];
+      mssym = mssym + r[1];
+      mssxtm = mssxtm + r[2];
+      mssytm = mssytm + r[3];
+      mssxym = mssxym + r[4];
+    }
     float t02p = undef, wl02x = undef, wl02y = undef, alpxt = undef, alpyt = undef,
           alpxy = undef;
-    float nv = undef, ns = undef, nb = undef, mu = undef, ni = undef, mode = undef;
+    float nv = undef, ns = undef, nb = undef, mu = undef, ni = undef;
+    mode = undef;
     if (et02 > k1em7) t02p = kTpi * sqrtf(et / et02);
     if (mssxm > k1em7) wl02x = kTpi * sqrtf(et / mssxm);
     if (mssym > k1em7) wl02y = kTpi * sqrtf(et / mssym);
     if (mssxm > k1em7 && et02 > k1em7) alpxt = mssxtm / sqrtf(mssxm * et02);
     if (mssym > k1em7 && et02 > k1em7) alpyt = mssytm / sqrtf(mssym * et02);
     if (mssxm > k1em7 && mssym > k1em7) alpxy = mssxym / sqrtf(mssxm * mssym);
-
     float stex = zero, stey = zero;
     if (a.stexu > zero && a.steyu > zero) {
       stex = a.stexu;
       stey = a.steyu;
     }
     const float sted = gt_sel(a.stedu, zero);
-
     if (wl02x > k1em7 && wl02y > k1em7 && t02p > k1em7) {
       const float ax2 = alpxt * alpxt, ay2 = alpyt * alpyt, axy2 = alpxy * alpxy;
       nv = kTpi * (stex * stey * sted) / (wl02x * wl02y * t02p) *
@@ -280,7 +372,6 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
     }
     if (et1 > k1em7) ni = sqrtf(et * et02 / (et1 * et1) - one);
     if (et > k1em7) mu = et1 * et1 / kGrav * dm::powf(et, -1.5f) * (one - ni + ni * ni);
-
     if (stex == zero && stey == zero) {
       mode = sqrtf(two * dm::logf(nb));
     } else if (sted == zero) {
@@ -290,51 +381,59 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
       const float t = two * dm::logf(nv);
       mode = sqrtf(t + two * dm::logf(t + two * dm::logf(t)));
     }
-
-    const float sqet = sqrtf(et);
+    sqet = sqrtf(et);
     const float mode2 = mode * mode;
-    const float den = mode - (two * nv * mode + ns) / (nv * mode2 + ns * mode + nb);
+    den = mode - (two * nv * mode + ns) / (nv * mode2 + ns * mode + nb);
     const float mum = one + mu * mode;
     put(a.f[OG_STMAXE], j0, sqet * (mode + half * mu * mode2 + 0.5772f * mum / den));
     put(a.f[OG_STMAXD], j0, sqet * (kPi * mum / kSqrt6 / den));
+    RT(p)[2] = t02p;
+  }
+  __syncthreads();
 
-    float phist = zero;
-    if (t02p > k1em7) {
-      float phi[21];
-#pragma unroll
-      for (int itl = 0; itl < 21; ++itl) phi[itl] = zero;
+  // Phase E: PHI(ITL), one thread per (point, ITL); TLPHI is stepped as the reference steps it.
+  if (a.ste) {
+    for (int pair = tid; pair < np * 21; pair += blockDim.x) {
+      const int q = pair / 21, itl = pair - q * 21;
+      const float t02p = RT(q)[2];
+      if (!(t02p > k1em7)) continue;
+      const float* const ebd = a.ebd + static_cast<size_t>(first + q) * nk;
       float tlphi = 0.3f * t02p;
+      for (int k = 0; k < itl; ++k) tlphi = tlphi + t02p / 20.0f;
       const float xfr = a.xfr, x2 = xfr * xfr, x3 = xfr * x2;
-#pragma unroll
-      for (int itl = 0; itl < 21; ++itl) {
-        for (int ik = 1; ik <= nk - 3; ik += 4) {
-          const float sigk = a.sig[ik];
-          phi[itl] = phi[itl] + (x3 * EBD[ik + 2] * cosf_(x3 * sigk * tlphi) +
-                                 x2 * EBD[ik + 1] * cosf_(x2 * sigk * tlphi) +
-                                 xfr * EBD[ik] * cosf_(xfr * sigk * tlphi) +
-                                 EBD[ik - 1] * cosf_(sigk * tlphi)) *
-                                    a.dsii[ik - 1];
-        }
-        tlphi = tlphi + t02p / 20.0f;
+      float ph = zero;
+      for (int ik = 1; ik <= nk - 3; ik += 4) {
+        const float sigk = a.sig[ik];
+        ph = ph + (x3 * ebd[ik + 2] * cosf_(x3 * sigk * tlphi) +
+                   x2 * ebd[ik + 1] * cosf_(x2 * sigk * tlphi) +
+                   xfr * ebd[ik] * cosf_(xfr * sigk * tlphi) + ebd[ik - 1] * cosf_(sigk * tlphi)) *
+                      a.dsii[ik - 1];
       }
-#pragma unroll
-      for (int itl = 0; itl < 21; ++itl) phi[itl] = phi[itl] / et;
-      // MINVAL: from the first element that is not a NaN, then a < min ? a : min; 21 NaNs
-      // give NaN.
+      RT(q)[9 + itl] = ph;
+    }
+  }
+  __syncthreads();
+  if (!mine) return;
+
+  // Phase F: the rest of the point (one thread each).
+  if (a.ste) {
+    float phist = zero;
+    const float t02p = RT(p)[2];
+    if (t02p > k1em7) {
+      // MINVAL: from the first element that is not a NaN, then a < min ? a : min.
       float mn = __int_as_float(0x7fc00000);
       bool found = false;
-#pragma unroll
       for (int m = 0; m < 21; ++m) {
+        const float ph = RT(p)[9 + m] / et;
         if (found) {
-          mn = lt_sel(phi[m], mn);
-        } else if (phi[m] == phi[m]) {
-          mn = phi[m];
+          mn = lt_sel(ph, mn);
+        } else if (ph == ph) {
+          mn = ph;
           found = true;
         }
       }
       phist = fabsf(mn);
     }
-
     const float stmaxel = sqet * (mode + 0.5772f / den);
     const float stmaxdl = sqet * (kPiSqrt6 / den);
     put(a.f[OG_HCMAXE], j0, stmaxel * (one + phist));
@@ -343,6 +442,13 @@ __global__ void __launch_bounds__(128) outg_point_kernel(OutgArgs a) {
     put(a.f[OG_HMAXE], j0, stmaxel * sq2);
     put(a.f[OG_HMAXD], j0, stmaxdl * sq2);
   }
+  // The band sums of IK = NK that 3.b's tail reads.
+  const float ab = RT(p)[3], abx = RT(p)[4], aby = RT(p)[5];
+  const float abxx = R(p, nk)[R_SXX], abyy = R(p, nk)[R_SYY], abxy = R(p, nk)[R_SXY];
+  const float* __restrict__ A = a.va + static_cast<size_t>(isea) * a.nspec;
+  auto AA = [&](int ith, int ik) { return A[(ith - 1) + (ik - 1) * nth]; };
+  auto cg = [&](int ik) { return a.cg[static_cast<size_t>(isea) * nk2 + ik]; };
+  const float* const EBD = a.ebd + static_cast<size_t>(j0) * nk;
 
   // 3.a
   {
@@ -533,7 +639,14 @@ void launch_outg(const OutgArgs& a, cudaStream_t s) {
   if (a.nfld > 0) outg_init_kernel<<<blocks_for(a.nfld, 256), 256, 0, s>>>(a);
   WWB_CHECK(cudaGetLastError());
   if (a.nseal <= 0) return;
-  outg_point_kernel<<<(a.nseal + 127) / 128, 128, 0, s>>>(a);
+  // Eight points per CTA: their (point, IK) records take about 37 KB at 36 frequencies, so
+  // five CTAs share an SM.
+  constexpr int kPoints = 8;
+  const size_t smem = sizeof(float) * kPoints * (static_cast<size_t>(a.nk) * kRec + 32);
+  if (smem > 48 * 1024)
+    WWB_CHECK(cudaFuncSetAttribute(outg_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+  outg_cta_kernel<<<(a.nseal + kPoints - 1) / kPoints, kOutgThreads, smem, s>>>(a, kPoints);
   WWB_CHECK(cudaGetLastError());
 }
 
