@@ -511,6 +511,98 @@ int ww_kokkos_strict(void);
 int ww_kokkos_fallback_slot(const char* part);
 void ww_kokkos_fallback_add(int slot);
 
+/* ---------------------------------------------------------------- learned DIA surrogate */
+/* B200 extensions with no counterpart in the reference (ww3-gpu has no learned component). The
+ * surrogate stands in for W3SNL1 (snl1_team.hpp:351-497) behind a per-point gate; rejected
+ * points are computed by the plain, bit-exact DIA kernel. Device pointers throughout, except
+ * where an argument says host. Status codes as above, read with ww_mlp_last_error /
+ * ww_sur_last_error. */
+
+/* A plain MLP din -> dh -> dh -> dh -> dout with GELU (tanh form) between layers, BF16 weights
+ * and activations, FP32 accumulation on the tensor cores (tcgen05) and FP32 master weights,
+ * trained with AdamW. Widths are multiples of 64; the loss is the mean squared error over the
+ * first nvalid output columns; cap is the largest training batch (a multiple of 128). */
+int ww_mlp_create(int din, int dh, int dout, int nvalid, int cap, unsigned long long seed,
+                  int* handle);
+int ww_mlp_destroy(int handle);
+/* Parameters as host floats, layer by layer: W (n x k, row-major) then b (n). */
+long long ww_mlp_param_count(int handle);
+int ww_mlp_set_params(int handle, const float* host);
+int ww_mlp_get_params(int handle, float* host);
+/* The gradient of the last ww_mlp_train_step with apply == 0, same layout. */
+int ww_mlp_get_grads(int handle, float* host);
+/* One step on `rows` rows (a multiple of 128): x bf16 (rows x din), t fp32 (rows x ldt).
+ * Forward, loss, backward; with apply != 0 also an AdamW update (lr, decoupled decay wd).
+ * loss3 (host, may be null) receives the step's loss. */
+int ww_mlp_train_step(int handle, int rows, const void* x, const float* t, int ldt, float lr,
+                      float wd, int apply, float* loss3);
+/* Inference: out fp32 (rows x dout) from x bf16 (rows x din). */
+int ww_mlp_forward(int handle, int rows, const void* x, float* out);
+/* The library's tensor-core GEMM on its own: C = A . B^T with A bf16 (M x K, row stride lda),
+ * B bf16 (N x K, row stride ldb), tile width bn (64, 128, 192, 256; N a multiple), K a multiple
+ * of 64, and epilogue `mode`: 1 z = C + bias -> aux = z, out = gelu(z), out_t = out^T; 2 out =
+ * gelu(C + bias); 3 out_f32 = C + bias; 4 out = C * gelu'(aux), out_t = out^T; 5 out_f32 += C
+ * with the reduction split in `splits` parts. Synchronous on `stream`. */
+int ww_mlp_gemm(int mode, int M, int N, int K, int bn, int splits, const void* a, int lda,
+                const void* b, int ldb, const float* bias, void* out, void* out_t, void* aux,
+                float* out_f32, int ldo, int ldt, void* stream);
+int ww_mlp_last_error(void);
+
+/* The surrogate of DIA grid igrid (ww_snl1_init first): an MLP with NSPEC + 2 inputs (the
+ * log-normalised spectrum, rotated to its dominant direction, and two depth features), three
+ * hidden layers of `nhidden`, NSPEC outputs (the normalised S_nl) and one error head. */
+int ww_sur_init(int igrid, int nhidden, unsigned long long seed);
+/* npts synthetic sea states (JONSWAP wind sea, cos^2s spreading, a swell system on a fraction
+ * `bimodal` of points, depth log-uniform in [dmin, dmax]) as A (nspec x npts), CG (nk x npts),
+ * KDMEAN (npts), seeded per point index p0 + i. */
+int ww_sur_synth(int igrid, int npts, unsigned long long seed, float bimodal, float dmin,
+                 float dmax, long long p0, float* a, float* cg, float* kdmean, void* stream);
+/* Builds the training set on the device: npts synthetic sea states labelled by the plain DIA
+ * kernel and normalised; the last `holdout` are never drawn by training. */
+int ww_sur_dataset(int igrid, long long npts, long long holdout, unsigned long long seed,
+                   float bimodal, float dmin, float dmax);
+/* Weights of the loss terms besides the MSE: mu for the squared Hs-tendency error relative to
+ * the gross tendency, lambda for the error head. */
+int ww_sur_loss_weights(int igrid, float mu, float lambda);
+/* `steps` AdamW steps on random batches of `batch` rows (warm-up, cosine decay lr -> lr_end);
+ * losses (host, 3 x steps, may be null) receives each step's loss terms. */
+int ww_sur_train(int igrid, int steps, int batch, float lr, float lr_end, float wd,
+                 unsigned long long seed, float* losses);
+/* Loss terms (host loss3) of the current network on dataset rows [p0, p0 + npts). */
+int ww_sur_eval(int igrid, long long p0, int npts, float* loss3);
+/* Gate thresholds: energy residual bound and predicted log-error bound. */
+int ww_sur_gate(int igrid, float energy, float log_err);
+/* Sets the gate from npts fresh synthetic points judged by the FP64 DIA: points whose energy
+ * residual is within `energy` are accepted in order of predicted error while the mean Hs-
+ * tendency error over all npts (a rejected point counting zero) stays within target_err.
+ * out (host, 4): log-error threshold, accepted fraction, mean error with the gate, without. */
+int ww_sur_calibrate(int igrid, int npts, unsigned long long seed, float bimodal, float dmin,
+                     float dmax, float energy, float target_err, float* out);
+/* The gated W3SNL1: arguments as ww_snl1_device (ww_kokkos_c.hpp:102-118 for their meaning),
+ * plus accepted (npts ints, may be null): 1 where the surrogate's S was kept (D is then 0: the
+ * surrogate does not model the diagonal term), 0 where the plain DIA computed S and D.
+ * Asynchronous on `stream`. */
+void ww_snl1_gated(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+                   float* s, float* d, int* accepted, void* stream);
+/* The network alone: out fp32 (rows x the padded output width, NSPEC + 1 rounded up to 64)
+ * from normalised inputs x bf16 (rows x the padded input width, NSPEC + 2 rounded up to 64):
+ * the four tensor-core GEMMs of one inference, asynchronous on `stream`. */
+int ww_sur_forward(int igrid, int rows, const void* x, float* out, void* stream);
+/* Points the last ww_snl1_gated sent to the plain DIA (synchronises `stream`), or -1. */
+int ww_sur_fallback_count(int igrid, void* stream);
+/* The FP64 DIA on npts points and the error of s_cand (may be null) against it: stats (npts x
+ * 10 doubles, device) per point: Hs, Hs tendency of the FP64 S and of the candidate, gross Hs
+ * tendency, band tendency error and magnitude, squared S error and FP64 S norm, mean-frequency
+ * tendency of the FP64 S and of the candidate. s64, d64 (npts x nspec doubles) may be null. */
+int ww_sur_judge(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
+                 const float* s_cand, double* stats, double* s64, double* d64, void* stream);
+/* Trained state as host floats: the MLP's parameters (ww_mlp_set_params layout) then the NK
+ * target scales. */
+long long ww_sur_param_count(int igrid);
+int ww_sur_get_params(int igrid, float* host);
+int ww_sur_set_params(int igrid, const float* host);
+int ww_sur_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,12 @@ EXPORTS = (
     "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes", "ww_steps_run", "ww_outg_va", "ww_outg_part",
     "ww_outg_last_error", "ww_outg_device", "ww_wave_gath", "ww_wave_scat", "ww_wave_uwnd",
     "ww_wave_utrn", "ww_wave_dzxy", "ww_wave_map3", "ww_wave_mapt", "ww_wave_distab",
+    "ww_mlp_create", "ww_mlp_destroy", "ww_mlp_param_count", "ww_mlp_set_params",
+    "ww_mlp_get_params", "ww_mlp_get_grads", "ww_mlp_train_step", "ww_mlp_forward",
+    "ww_mlp_gemm", "ww_mlp_last_error", "ww_sur_init", "ww_sur_synth", "ww_sur_dataset",
+    "ww_sur_loss_weights", "ww_sur_train", "ww_sur_eval", "ww_sur_gate", "ww_sur_calibrate",
+    "ww_snl1_gated", "ww_sur_forward", "ww_sur_fallback_count", "ww_sur_judge", "ww_sur_param_count",
+    "ww_sur_get_params", "ww_sur_set_params", "ww_sur_last_error",
 )
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -158,6 +164,41 @@ def lib():
         L.ww_xyp3_batch_va.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _F] + [_P] * 21 + [
             _I, _I, _P, _P, _P, _P, _P, _I, _I]
         L.ww_xyp3_batch_va.restype = _I
+        _LL, _U64 = ctypes.c_longlong, ctypes.c_ulonglong
+        L.ww_mlp_create.argtypes = [_I, _I, _I, _I, _I, _U64, ctypes.POINTER(_I)]
+        L.ww_mlp_destroy.argtypes = [_I]
+        L.ww_mlp_param_count.argtypes = [_I]
+        L.ww_mlp_param_count.restype = _LL
+        for name in ("ww_mlp_set_params", "ww_mlp_get_params", "ww_mlp_get_grads"):
+            getattr(L, name).argtypes = [_I, _P]
+        L.ww_mlp_train_step.argtypes = [_I, _I, _P, _P, _I, _F, _F, _I, _P]
+        L.ww_mlp_forward.argtypes = [_I, _I, _P, _P]
+        L.ww_mlp_gemm.argtypes = [_I, _I, _I, _I, _I, _I, _P, _I, _P, _I] + [_P] * 5 + [_I, _I, _P]
+        L.ww_sur_init.argtypes = [_I, _I, _U64]
+        L.ww_sur_synth.argtypes = [_I, _I, _U64, _F, _F, _F, _LL, _P, _P, _P, _P]
+        L.ww_sur_dataset.argtypes = [_I, _LL, _LL, _U64, _F, _F, _F]
+        L.ww_sur_loss_weights.argtypes = [_I, _F, _F]
+        L.ww_sur_train.argtypes = [_I, _I, _I, _F, _F, _F, _U64, _P]
+        L.ww_sur_eval.argtypes = [_I, _LL, _I, _P]
+        L.ww_sur_gate.argtypes = [_I, _F, _F]
+        L.ww_sur_calibrate.argtypes = [_I, _I, _U64, _F, _F, _F, _F, _F, _P]
+        L.ww_snl1_gated.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _P]
+        L.ww_snl1_gated.restype = None
+        L.ww_sur_fallback_count.argtypes = [_I, _P]
+        L.ww_sur_forward.argtypes = [_I, _I, _P, _P, _P]
+        L.ww_sur_judge.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.ww_sur_param_count.argtypes = [_I]
+        L.ww_sur_param_count.restype = _LL
+        L.ww_sur_get_params.argtypes = [_I, _P]
+        L.ww_sur_set_params.argtypes = [_I, _P]
+        for name in ("ww_mlp_create", "ww_mlp_destroy", "ww_mlp_set_params", "ww_mlp_get_params",
+                     "ww_mlp_get_grads", "ww_mlp_train_step", "ww_mlp_forward", "ww_mlp_gemm",
+                     "ww_mlp_last_error", "ww_sur_init", "ww_sur_synth", "ww_sur_dataset",
+                     "ww_sur_loss_weights", "ww_sur_train", "ww_sur_eval", "ww_sur_gate",
+                     "ww_sur_calibrate", "ww_sur_fallback_count", "ww_sur_judge",
+                     "ww_sur_forward",
+                     "ww_sur_get_params", "ww_sur_set_params", "ww_sur_last_error"):
+            getattr(L, name).restype = _I
         _lib = L
     return _lib
 

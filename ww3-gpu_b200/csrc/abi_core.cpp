@@ -33,6 +33,7 @@ void release_st4_contexts();   // abi_st4.cpp
 void release_steps();          // abi_step.cpp
 void release_outg_staging();   // abi_outg.cpp
 void release_wave_staging();   // abi_wave.cpp
+void release_sur_contexts();   // abi_sur.cpp
 
 namespace {
 
@@ -206,6 +207,7 @@ int ww_kokkos_init(int comm_f) {
 void ww_kokkos_finalize(void) {
   auto& rt = runtime();
   wwb::release_steps();
+  wwb::release_sur_contexts();
   wwb::release_srce_contexts();
   wwb::release_st4_contexts();
   wwb::release_snl1_contexts();

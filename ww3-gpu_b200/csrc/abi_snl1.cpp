@@ -61,6 +61,7 @@ struct Slot {
 
 struct Ctx {
   Snl1Config cfg{};
+  std::vector<float> sig_host;
   Snl1Tables tab;
   Snl1Dev dev{};
   int kernel = kSnl1Auto;
@@ -186,6 +187,7 @@ int init_common(int igrid, const Snl1Config& cfg, const float* sig, Snl1Tables&&
     c->tab = std::move(tab);
     std::vector<float> h_sig(sig, sig + cfg.nk);
     c->sig.upload(h_sig.data(), h_sig.size());
+    c->sig_host = h_sig;
     publish(*c);
     c->dev.sig = c->sig.ptr;
     for (auto& sl : c->slots) WWB_CHECK(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
@@ -206,6 +208,15 @@ bool snl1_grid_dev(int igrid, Snl1Dev* out) {
   auto it = contexts().find(igrid);
   if (it == contexts().end() || !it->second->ready || !it->second->tab.rowshift) return false;
   *out = it->second->dev;
+  return true;
+}
+
+/// The configuration and SIG(1:NK) of grid igrid, or false.
+bool snl1_grid_config(int igrid, Snl1Config* cfg, std::vector<float>* sig) {
+  auto it = contexts().find(igrid);
+  if (it == contexts().end() || !it->second->ready) return false;
+  *cfg = it->second->cfg;
+  *sig = it->second->sig_host;
   return true;
 }
 

@@ -1,0 +1,749 @@
+// ww3-gpu_b200/csrc/mlp_ops.cu
+// Element-wise kernels of the learned DIA surrogate (declared and explained in mlp_ops.cuh).
+// None of this is bit-exact work: it is the approximate path, measured against the FP64 DIA at
+// the end of this file, so fused multiply-adds and CUDA's own math functions are used freely.
+#include <cuda_bf16.h>
+
+#include <cmath>
+
+#include "mlp_ops.cuh"
+#include "wwb_common.hpp"
+
+namespace wwb {
+namespace mlp {
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+constexpr double kGrav = 9.806;  // the reference's GRAV (kokkos/src/ww_kokkos/st4_params.hpp:28)
+constexpr float kTpiInvF = static_cast<float>(1.0 / (2.0 * 3.141592653589793));
+constexpr float kInputFloor = 1e-6f;  // U + floor before the log
+constexpr float kInputScale = 1.0f / 7.0f;
+constexpr int kThreads = 256;
+
+/// splitmix64's output function (S. Vigna, public domain): a counter-based generator, so every
+/// point's draws depend only on (seed, point index, draw number).
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double uniform(uint64_t seed, uint64_t i, uint32_t j) {
+  const uint64_t h = mix64(mix64(seed) ^ (i * 0x100000001B3ull + j * 0x9E3779B97F4A7C15ull));
+  return static_cast<double>(h >> 11) * 0x1.0p-53;
+}
+
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  T t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : T(0);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) red[0] = t;
+  }
+  __syncthreads();
+  t = red[0];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float block_max(float v, float* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) t = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, o));
+    if (threadIdx.x == 0) red[0] = t;
+  }
+  __syncthreads();
+  const float t = red[0];
+  __syncthreads();
+  return t;
+}
+
+/// CONS of W3SNL1 section 1 (snl1_team.hpp:386-390) in float with CUDA's expf.
+__device__ __forceinline__ float cons_of(const SurGrid& g, float kd) {
+  const float x0 = g.kdcon * kd;
+  const float x = x0 < g.kdmn ? g.kdmn : x0;
+  const float y = g.snls3 * x;
+  const float x2 = -1.e15f < y ? y : -1.e15f;
+  return g.snlc1 * (1.0f + g.snls1 / x * (1.0f - g.snls2 * x) * expf(x2));
+}
+
+// ------------------------------------------------------------------------------ synthetic data
+
+__device__ double jonswap(double f, double fp, double gam) {
+  const double sg = f <= fp ? 0.07 : 0.09;
+  const double r = exp(-(f - fp) * (f - fp) / (2.0 * sg * sg * fp * fp));
+  const double q = fp / f;
+  return pow(f, -5.0) * exp(-1.25 * q * q * q * q) * pow(gam, r);
+}
+
+__global__ void synth_kernel(SurGrid g, SynthDraw dr, long long p0, int npts, float* a,
+                             float* cg, float* kdm) {
+  const int ip = blockIdx.x;
+  if (ip >= npts) return;
+  __shared__ double ef1[64], ef2[64], cgk[64], kdk[64], dir1[64], dir2[64];
+  __shared__ double tot[6];
+  const int nk = g.nk, nth = g.nth, tid = threadIdx.x;
+  const uint64_t gi = static_cast<uint64_t>(p0 + ip);
+  const double hs = 0.5 + 7.5 * uniform(dr.seed, gi, 0);
+  const double fp = 0.06 + 0.14 * uniform(dr.seed, gi, 1);
+  const double gam = 1.0 + 4.0 * uniform(dr.seed, gi, 2);
+  const double spr = 2.0 + 18.0 * uniform(dr.seed, gi, 3);
+  const double thm = 2.0 * kPi * uniform(dr.seed, gi, 4);
+  double dep = dr.dmin;
+  if (dr.dmax > dr.dmin)
+    dep = exp(log(dr.dmin) + (log(dr.dmax) - log(dr.dmin)) * uniform(dr.seed, gi, 5));
+  const bool swell = uniform(dr.seed, gi, 6) < dr.bimodal;
+  const double hs2 = 0.5 + 2.5 * uniform(dr.seed, gi, 7);
+  const double fp2 = 0.05 + 0.04 * uniform(dr.seed, gi, 8);
+  const double thm2 = 2.0 * kPi * uniform(dr.seed, gi, 9);
+  for (int k = tid; k < nk; k += blockDim.x) {
+    const double s = g.sig[k], f = s / (2.0 * kPi);
+    ef1[k] = jonswap(f, fp, gam) / (2.0 * kPi);
+    ef2[k] = swell ? jonswap(f, fp2, 3.3) / (2.0 * kPi) : 0.0;
+    // k from s^2 = g k tanh(k d) by Newton from the deep-water value.
+    double wk = s * s / kGrav;
+    for (int it = 0; it < 30; ++it) {
+      const double kd = fmin(wk * dep, 40.0);
+      const double t = tanh(kd);
+      const double f0 = kGrav * wk * t - s * s;
+      const double f1 = kGrav * t + kGrav * wk * dep * (1.0 - t * t);
+      wk -= f0 / f1;
+    }
+    const double kd = wk * dep;
+    cgk[k] = 0.5 * s / wk * (1.0 + 2.0 * kd / sinh(fmin(2.0 * kd, 80.0)));
+    kdk[k] = kd;
+  }
+  for (int t = tid; t < nth; t += blockDim.x) {
+    const double th = t * static_cast<double>(g.dth);
+    const double c1 = cos(0.5 * (th - thm)), c2 = cos(0.5 * (th - thm2));
+    dir1[t] = pow(c1 * c1, spr);
+    dir2[t] = pow(c2 * c2, 20.0);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const double xfr = g.xfr, dth = g.dth;
+    double d1 = 0, d2 = 0, m1 = 0, m2 = 0;
+    for (int t = 0; t < nth; ++t) {
+      d1 += dir1[t];
+      d2 += dir2[t];
+    }
+    for (int k = 0; k < nk; ++k) {
+      const double dsii = 0.5 * static_cast<double>(g.sig[k]) * (xfr - 1.0 / xfr);
+      m1 += ef1[k] * dsii;
+      m2 += ef2[k] * dsii;
+    }
+    const double c1 = m1 > 0 ? (hs / 4.0) * (hs / 4.0) / m1 / (d1 * dth) : 0.0;
+    const double c2 = (swell && m2 > 0) ? (hs2 / 4.0) * (hs2 / 4.0) / m2 / (d2 * dth) : 0.0;
+    double esum = 0, ekd = 0;
+    for (int k = 0; k < nk; ++k) {
+      const double e = ef1[k] * c1 * d1 + ef2[k] * c2 * d2;
+      esum += e;
+      ekd += e * kdk[k];
+    }
+    tot[0] = c1;
+    tot[1] = c2;
+    tot[2] = esum > 0 ? ekd / esum : 0.0;
+  }
+  __syncthreads();
+  const double c1 = tot[0], c2 = tot[1];
+  const size_t nspec = static_cast<size_t>(nk) * nth;
+  for (int i = tid; i < nk * nth; i += blockDim.x) {
+    const int k = i / nth, t = i % nth;
+    const double e = ef1[k] * dir1[t] * c1 + ef2[k] * dir2[t] * c2;
+    a[ip * nspec + i] = static_cast<float>(e * cgk[k] / static_cast<double>(g.sig[k]));
+  }
+  for (int k = tid; k < nk; k += blockDim.x) cg[static_cast<size_t>(ip) * nk + k] = static_cast<float>(cgk[k]);
+  if (tid == 0) kdm[ip] = static_cast<float>(tot[2]);
+}
+
+// ------------------------------------------------------------------------- input normalisation
+
+__global__ void prep_kernel(SurGrid g, int npts, const float* __restrict__ a,
+                            const float* __restrict__ cg, const float* __restrict__ kdm,
+                            __nv_bfloat16* __restrict__ x, int ldx, float* __restrict__ scale,
+                            int* __restrict__ shift) {
+  extern __shared__ float sm[];
+  const int ip = blockIdx.x, tid = threadIdx.x;
+  const int nk = g.nk, nth = g.nth, nspec = g.nspec;
+  float* const ue = sm;                 // nspec
+  float* const conx = ue + nspec;       // nk
+  float* const dsum = conx + nk;        // nth
+  float* const red = dsum + nth;        // 32
+  __shared__ int s_shift;
+  const float* ap = a + static_cast<size_t>(ip) * nspec;
+  for (int k = tid; k < nk; k += blockDim.x)
+    conx[k] = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
+  __syncthreads();
+  float mx = 0.0f;
+  for (int i = tid; i < nspec; i += blockDim.x) {
+    const float v = __ldg(ap + i) / conx[i / nth];
+    ue[i] = v;
+    mx = fmaxf(mx, v);
+  }
+  const float umax = block_max(mx, red);
+  for (int t = tid; t < nth; t += blockDim.x) {
+    float s = 0.0f;
+    for (int k = 0; k < nk; ++k) s += ue[k * nth + t];
+    dsum[t] = s;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int best = 0;
+    for (int t = 1; t < nth; ++t)
+      if (dsum[t] > dsum[best]) best = t;
+    s_shift = best;
+    const float kd = __ldg(kdm + ip);
+    const float c = cons_of(g, kd);
+    scale[ip] = c * umax * umax * umax;
+    shift[ip] = best;
+    // Depth features: ln kdmean and the relative depth factor of CONS.
+    __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
+    if (g.din > nspec) xr[nspec] = __float2bfloat16_rn(logf(fmaxf(kd, 1e-2f)) * 0.2f);
+    if (g.din > nspec + 1) xr[nspec + 1] = __float2bfloat16_rn(c / g.snlc1 - 1.0f);
+  }
+  __syncthreads();
+  const int sh = s_shift;
+  const float inv = umax > 0.0f ? 1.0f / umax : 0.0f;
+  __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
+  for (int i = tid; i < nspec; i += blockDim.x) {
+    const int k = i / nth, j = i % nth;
+    int jj = j + sh;
+    if (jj >= nth) jj -= nth;
+    const float u = ue[k * nth + jj] * inv;
+    xr[i] = __float2bfloat16_rn(logf(u + kInputFloor) * kInputScale + 1.0f);
+  }
+  for (int i = nspec + 2 + tid; i < g.din; i += blockDim.x) xr[i] = __float2bfloat16_rn(0.0f);
+}
+
+// ------------------------------------------------------------------------------ target side
+
+__global__ void rowscale_kernel(SurGrid g, int npts, const float* __restrict__ s,
+                                const float* __restrict__ cg, const float* __restrict__ scale,
+                                const int* __restrict__ shift, double* acc,
+                                unsigned long long* cnt) {
+  __shared__ double rs[64];
+  const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth;
+  const float sc = scale[ip];
+  (void)shift;
+  if (!(sc > 0.0f)) return;
+  for (int k = tid; k < nk; k += blockDim.x) rs[k] = 0.0;
+  __syncthreads();
+  const float* sp = s + static_cast<size_t>(ip) * g.nspec;
+  for (int i = tid; i < g.nspec; i += blockDim.x) {
+    const int k = i / nth;
+    const float conx = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
+    const double v = static_cast<double>(sp[i]) / (static_cast<double>(sc) * conx);
+    atomicAdd(&rs[k], v * v);
+  }
+  __syncthreads();
+  for (int k = tid; k < nk; k += blockDim.x) atomicAdd(acc + k, rs[k]);
+  if (tid == 0) atomicAdd(cnt, 1ull);
+}
+
+__global__ void targets_kernel(SurGrid g, int npts, const float* __restrict__ s,
+                               const float* __restrict__ cg, const float* __restrict__ scale,
+                               const int* __restrict__ shift, float* __restrict__ t, int ldt) {
+  const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth;
+  const float sc = scale[ip];
+  const int sh = shift[ip];
+  const float* sp = s + static_cast<size_t>(ip) * g.nspec;
+  float* tp = t + static_cast<size_t>(ip) * ldt;
+  for (int i = tid; i < g.nspec; i += blockDim.x) {
+    const int k = i / nth, j = i % nth;
+    int jj = j + sh;
+    if (jj >= nth) jj -= nth;
+    const float conx = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
+    const float den = sc * conx * __ldg(g.rowscale + k);
+    tp[i] = den > 0.0f ? sp[k * nth + jj] / den : 0.0f;
+  }
+}
+
+// ------------------------------------------------------------------------ inference output side
+
+__global__ void post_kernel(SurGrid g, GateParams gate, int npts, const float* __restrict__ out,
+                            int ldo, const float* __restrict__ cg, const float* __restrict__ scale,
+                            const int* __restrict__ shift, float* __restrict__ s,
+                            float* __restrict__ d, int* __restrict__ accepted,
+                            int* __restrict__ rej_list, int* __restrict__ nrej,
+                            int* __restrict__ nrej_total) {
+  __shared__ float red[32];
+  __shared__ float conx[64];
+  const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth, nspec = g.nspec;
+  const float* op = out + static_cast<size_t>(ip) * ldo;
+  for (int k = tid; k < nk; k += blockDim.x)
+    conx[k] = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
+  float r = 0.0f, gs = 0.0f;
+  for (int i = tid; i < nspec; i += blockDim.x) {
+    const float w = __ldg(g.omega + i / nth), v = op[i];
+    r += w * v;
+    gs += w * fabsf(v);
+  }
+  r = block_sum(r, red);
+  gs = block_sum(gs, red);
+  const float head = g.dout > nspec ? op[nspec] : -INFINITY;
+  const bool ok = isfinite(r) && isfinite(gs) && fabsf(r) <= gate.energy * gs &&
+                  head <= gate.log_err;
+  if (tid == 0) {
+    if (accepted) accepted[ip] = ok ? 1 : 0;
+    if (!ok) {
+      rej_list[atomicAdd(nrej, 1)] = ip;
+      if (nrej_total) atomicAdd(nrej_total, 1);
+    }
+  }
+  if (!ok) return;  // the plain DIA writes this point's S and D
+  const float sc = scale[ip];
+  const int sh = shift[ip];
+  float* sp = s + static_cast<size_t>(ip) * nspec;
+  float* dp = d + static_cast<size_t>(ip) * nspec;
+  for (int i = tid; i < nspec; i += blockDim.x) {
+    const int k = i / nth, j = i % nth;
+    int jj = j + sh;
+    if (jj >= nth) jj -= nth;
+    sp[k * nth + jj] = op[i] * __ldg(g.rowscale + k) * sc * conx[k];
+    dp[i] = 0.0f;
+  }
+}
+
+// ------------------------------------------------------------------------------ training side
+
+__global__ void loss_kernel(SurGrid g, LossWeights lw, int m, int nvalid,
+                            const float* __restrict__ out, int ldo, const float* __restrict__ t,
+                            int ldt, __nv_bfloat16* __restrict__ grad, int ldg,
+                            float* __restrict__ loss) {
+  __shared__ float red[32];
+  const int ip = blockIdx.x, tid = threadIdx.x;
+  const float* op = out + static_cast<size_t>(ip) * ldo;
+  const float* tp = t + static_cast<size_t>(ip) * ldt;
+  const bool energy = lw.mu > 0.0f && g.omega != nullptr;
+  float r = 0.0f, gs = 0.0f, se = 0.0f;
+  for (int i = tid; i < nvalid; i += blockDim.x) {
+    const float dv = op[i] - tp[i];
+    se += dv * dv;
+    if (energy) {
+      const float w = __ldg(g.omega + i / g.nth);
+      r += w * dv;
+      gs += w * fabsf(tp[i]);
+    }
+  }
+  se = block_sum(se, red);
+  if (energy) {
+    r = block_sum(r, red);
+    gs = block_sum(gs, red);
+  }
+  const bool have_e = energy && gs > 1e-30f;
+  const float rel = have_e ? r / gs : 0.0f;
+  const float inv_m = 1.0f / static_cast<float>(m);
+  const float c_mse = 2.0f * inv_m / static_cast<float>(nvalid);
+  const float c_e = have_e ? lw.mu * 2.0f * rel / gs * inv_m : 0.0f;
+  const bool head = lw.head && g.dout > nvalid;
+  const float target_h = logf(fabsf(rel) + 1e-4f);
+  __nv_bfloat16* gp = grad + static_cast<size_t>(ip) * ldg;
+  const int width = g.dout;
+  for (int i = tid; i < width; i += blockDim.x) {
+    float v = 0.0f;
+    if (i < nvalid) {
+      v = c_mse * (op[i] - tp[i]);
+      if (have_e) v += c_e * __ldg(g.omega + i / g.nth);
+    } else if (head && i == nvalid) {
+      v = lw.lambda * 2.0f * (op[i] - target_h) * inv_m;
+    }
+    gp[i] = __float2bfloat16_rn(v);
+  }
+  if (tid == 0) {
+    atomicAdd(loss + 0, se * inv_m / static_cast<float>(nvalid));
+    if (have_e) atomicAdd(loss + 1, lw.mu * rel * rel * inv_m);
+    if (head) {
+      const float h = op[nvalid] - target_h;
+      atomicAdd(loss + 2, lw.lambda * h * h * inv_m);
+    }
+  }
+}
+
+__global__ void gather_kernel(int m, long long n, uint64_t seed, long long offset,
+                              const __nv_bfloat16* __restrict__ xs, int ldx,
+                              const float* __restrict__ ts, int ldt, __nv_bfloat16* __restrict__ xb,
+                              float* __restrict__ tb) {
+  const int r = blockIdx.x;
+  if (r >= m) return;
+  long long src = offset + r;
+  if (seed != 0) src = static_cast<long long>(mix64(mix64(seed) ^ static_cast<uint64_t>(r)) % static_cast<uint64_t>(n));
+  const uint4* xsrc = reinterpret_cast<const uint4*>(xs + src * ldx);
+  uint4* xdst = reinterpret_cast<uint4*>(xb + static_cast<size_t>(r) * ldx);
+  for (int i = threadIdx.x; i < ldx / 8; i += blockDim.x) xdst[i] = __ldg(xsrc + i);
+  const float4* tsrc = reinterpret_cast<const float4*>(ts + src * ldt);
+  float4* tdst = reinterpret_cast<float4*>(tb + static_cast<size_t>(r) * ldt);
+  for (int i = threadIdx.x; i < ldt / 4; i += blockDim.x) tdst[i] = __ldg(tsrc + i);
+}
+
+__global__ void transpose_kernel(const __nv_bfloat16* __restrict__ src, int rows, int cols,
+                                 int lds, __nv_bfloat16* __restrict__ dst, int ldd) {
+  __shared__ __nv_bfloat16 tile[32][34];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int rr = threadIdx.y; rr < 32; rr += 8) {
+    const int r = r0 + rr, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[rr][threadIdx.x] = src[static_cast<size_t>(r) * lds + c];
+  }
+  __syncthreads();
+  for (int cc = threadIdx.y; cc < 32; cc += 8) {
+    const int c = c0 + cc, r = r0 + threadIdx.x;
+    if (c < cols && r < rows) dst[static_cast<size_t>(c) * ldd + r] = tile[threadIdx.x][cc];
+  }
+}
+
+__global__ void colsum_kernel(const __nv_bfloat16* __restrict__ gt, int n, int m, int ldt,
+                              float* __restrict__ db) {
+  const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const __nv_bfloat16* p = gt + static_cast<size_t>(row) * ldt;
+  float acc = 0.0f;
+  for (int i = lane * 8; i < m; i += 256) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p + i);
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[q]));
+      acc += f.x + f.y;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) db[row] = acc;
+}
+
+__global__ void adamw_kernel(Adam h, int n, int k, float* __restrict__ w, float* __restrict__ m,
+                             float* __restrict__ v, float* __restrict__ g,
+                             __nv_bfloat16* __restrict__ wb, __nv_bfloat16* __restrict__ wt,
+                             int update) {
+  __shared__ __nv_bfloat16 tile[32][34];
+  const int c = blockIdx.x * 32 + threadIdx.x;
+  for (int rr = threadIdx.y; rr < 32; rr += 8) {
+    const int r = blockIdx.y * 32 + rr;
+    if (r < n && c < k) {
+      const size_t i = static_cast<size_t>(r) * k + c;
+      float wi = w[i];
+      if (update) {
+        const float gi = g[i];
+        const float mi = h.beta1 * m[i] + (1.0f - h.beta1) * gi;
+        const float vi = h.beta2 * v[i] + (1.0f - h.beta2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        g[i] = 0.0f;
+        wi = wi - h.lr * ((mi / h.c1) / (sqrtf(vi / h.c2) + h.eps) + h.wd * wi);
+        w[i] = wi;
+      }
+      const __nv_bfloat16 b = __float2bfloat16_rn(wi);
+      wb[i] = b;
+      tile[rr][threadIdx.x] = b;
+    }
+  }
+  __syncthreads();
+  for (int cc = threadIdx.y; cc < 32; cc += 8) {
+    const int col = blockIdx.x * 32 + cc, r = blockIdx.y * 32 + threadIdx.x;
+    if (col < k && r < n) wt[static_cast<size_t>(col) * n + r] = tile[threadIdx.x][cc];
+  }
+}
+
+__global__ void adamw_vec_kernel(Adam h, int n, float* w, float* m, float* v, const float* g) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = h.beta1 * m[i] + (1.0f - h.beta1) * gi;
+  const float vi = h.beta2 * v[i] + (1.0f - h.beta2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  w[i] = w[i] - h.lr * ((mi / h.c1) / (sqrtf(vi / h.c2) + h.eps) + h.wd * w[i]);
+}
+
+__global__ void init_kernel(uint64_t seed, int n, int k, int nvalid, float gain, float* w) {
+  const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<size_t>(n) * k) return;
+  const int r = static_cast<int>(i / k);
+  const float a = gain * sqrtf(3.0f / static_cast<float>(k));
+  w[i] = r < nvalid ? static_cast<float>((2.0 * uniform(seed, i, 77) - 1.0) * a) : 0.0f;
+}
+
+// ------------------------------------------------------------------------------- the FP64 DIA
+
+__global__ void dia_f64_kernel(DiaF64 t, int npts, const float* __restrict__ a,
+                               const float* __restrict__ cg, const float* __restrict__ kdm,
+                               const float* __restrict__ sc, double* __restrict__ stats,
+                               double* __restrict__ s64, double* __restrict__ d64) {
+  extern __shared__ double dsm[];
+  __shared__ double red[32];
+  const int ip = blockIdx.x, tid = threadIdx.x, nb = blockDim.x;
+  const int nth = t.nth, nfr = t.nfr, nspec = t.nspec, nspecx = t.nspecx, nk = t.nk;
+  const int nspecy = t.nfrhgh * nth;
+  double* const ue = dsm;
+  double* arr[8];
+  for (int j = 0; j < 8; ++j) arr[j] = ue + (nspecy + nth) + static_cast<size_t>(j) * (nspecx + nth);
+  double* const sa1 = arr[0];
+  double* const sa2 = arr[1];
+  double* const da1c = arr[2];
+  double* const da1p = arr[3];
+  double* const da1m = arr[4];
+  double* const da2c = arr[5];
+  double* const da2p = arr[6];
+  double* const da2m = arr[7];
+  double* const conx = arr[7] + (nspecx + nth);  // nk
+  double* const rowr = conx + nk;                // nk: band tendency of the FP64 S
+  double* const rowc = rowr + nk;                // nk: band tendency of the candidate
+  const double tpiinv = 1.0 / (2.0 * kPi);
+
+  // 1. CONS (snl1_team.hpp:383-390), MAX(a, b) as (a < b) ? b : a.
+  const double kd = kdm[ip];
+  const double x0 = t.kdcon * kd;
+  const double x = x0 < t.kdmn ? t.kdmn : x0;
+  const double y0 = t.snls3 * x;
+  const double x2 = -1.e15 < y0 ? y0 : -1.e15;
+  const double cons = t.snlc1 * (1.0 + t.snls1 / x * (1.0 - t.snls2 * x) * exp(x2));
+
+  // 2. UE = A / CONX, the zero bins and the parametric tail (:392-426).
+  const float* ap = a + static_cast<size_t>(ip) * nspec;
+  for (int k = tid; k < nk; k += nb) {
+    conx[k] = tpiinv / t.sig[k] * static_cast<double>(cg[static_cast<size_t>(ip) * nk + k]);
+    rowr[k] = 0.0;
+    rowc[k] = 0.0;
+  }
+  for (int i = tid; i < nth; i += nb) {
+    ue[i] = 0.0;
+    for (int j = 0; j < 8; ++j) arr[j][i] = 0.0;
+  }
+  __syncthreads();
+  for (int i = tid; i < nspec; i += nb) ue[i + nth] = static_cast<double>(ap[i]) / conx[i / nth];
+  __syncthreads();
+  for (int ifr = nfr; ifr < t.nfrhgh; ++ifr) {
+    for (int i = tid; i < nth; i += nb) ue[ifr * nth + i + nth] = ue[ifr * nth + i] * t.fachfe;
+    __syncthreads();
+  }
+
+  // 3. Interactions over the extended spectrum (:433-473), through the index tables.
+  for (int isp = tid; isp < nspecx; isp += nb) {
+    auto U = [&](int j) { return ue[t.ipim[static_cast<size_t>(j) * nspecx + isp] + nth]; };
+    const double e00 = ue[isp + nth];
+    const double ep1 = t.awg[0] * U(0) + t.awg[1] * U(1) + t.awg[2] * U(2) + t.awg[3] * U(3);
+    const double em1 = t.awg[4] * U(4) + t.awg[5] * U(5) + t.awg[6] * U(6) + t.awg[7] * U(7);
+    const double ep2 = t.awg[0] * U(8) + t.awg[1] * U(9) + t.awg[2] * U(10) + t.awg[3] * U(11);
+    const double em2 = t.awg[4] * U(12) + t.awg[5] * U(13) + t.awg[6] * U(14) + t.awg[7] * U(15);
+    const double af = t.af11[isp / nth];
+    const double factor = cons * af * e00;
+    const double sa1a = e00 * (ep1 * t.dal1 + em1 * t.dal2);
+    const double sa1b = sa1a - ep1 * em1 * t.dal3;
+    const double sa2a = e00 * (ep2 * t.dal1 + em2 * t.dal2);
+    const double sa2b = sa2a - ep2 * em2 * t.dal3;
+    sa1[isp + nth] = factor * sa1b;
+    sa2[isp + nth] = factor * sa2b;
+    da1c[isp + nth] = cons * af * (sa1a + sa1b);
+    da1p[isp + nth] = factor * (t.dal1 * e00 - t.dal3 * em1);
+    da1m[isp + nth] = factor * (t.dal2 * e00 - t.dal3 * ep1);
+    da2c[isp + nth] = cons * af * (sa2a + sa2b);
+    da2p[isp + nth] = factor * (t.dal1 * e00 - t.dal3 * em2);
+    da2m[isp + nth] = factor * (t.dal2 * e00 - t.dal3 * ep2);
+  }
+  __syncthreads();
+
+  // 4. S and D (:475-496), and the candidate's error terms bin by bin.
+  const double xfr = t.xfr;
+  double m0 = 0, m1 = 0, ts = 0, tc = 0, tg = 0, ss = 0, sc1 = 0, e2 = 0, r2 = 0;
+  for (int isp = tid; isp < nspec; isp += nb) {
+    auto C1 = [&](int j) { return t.ic[static_cast<size_t>(j) * nspec + isp] + nth; };
+    auto C2 = [&](int j) { return t.ic[static_cast<size_t>(8 + j) * nspec + isp] + nth; };
+    const int k = isp / nth;
+    double acc = -2.0 * (sa1[isp + nth] + sa2[isp + nth]);
+    double dac = -2.0 * (da1c[isp + nth] + da2c[isp + nth]);
+    for (int j = 0; j < 8; ++j) {
+      acc += t.awg[j] * (sa1[C1(j)] + sa2[C2(j)]);
+      dac += t.swg[j] * (j < 4 ? (da1p[C1(j)] + da2p[C2(j)]) : (da1m[C1(j)] + da2m[C2(j)]));
+    }
+    const double sv = conx[k] * acc;
+    if (s64) s64[static_cast<size_t>(ip) * nspec + isp] = sv;
+    if (d64) d64[static_cast<size_t>(ip) * nspec + isp] = dac;
+    const double sig = t.sig[k];
+    const double dden = t.dth * (0.5 * sig * (xfr - 1.0 / xfr)) * sig;
+    const double w = dden / static_cast<double>(cg[static_cast<size_t>(ip) * nk + k]);
+    const double av = ap[isp];
+    const double cv = sc ? static_cast<double>(sc[static_cast<size_t>(ip) * nspec + isp]) : 0.0;
+    m0 += w * av;
+    m1 += w * sig * av;
+    ts += w * sv;
+    tc += w * cv;
+    tg += w * fabs(sv);
+    ss += w * sig * sv;
+    sc1 += w * sig * cv;
+    e2 += (cv - sv) * (cv - sv);
+    r2 += sv * sv;
+    atomicAdd(rowr + k, w * sv);
+    atomicAdd(rowc + k, w * cv);
+  }
+  m0 = block_sum(m0, red);
+  m1 = block_sum(m1, red);
+  ts = block_sum(ts, red);
+  tc = block_sum(tc, red);
+  tg = block_sum(tg, red);
+  ss = block_sum(ss, red);
+  sc1 = block_sum(sc1, red);
+  e2 = block_sum(e2, red);
+  r2 = block_sum(r2, red);
+  if (tid == 0) {
+    double bn = 0, bd = 0;
+    for (int k = 0; k < nk; ++k) {
+      bn += fabs(rowc[k] - rowr[k]);
+      bd += fabs(rowr[k]);
+    }
+    const double hs = 4.0 * sqrt(m0 > 0 ? m0 : 0.0);
+    const double f = hs > 0 ? 8.0 / hs : 0.0;
+    double* o = stats + static_cast<size_t>(ip) * 10;
+    o[0] = hs;
+    o[1] = f * ts;
+    o[2] = f * tc;
+    o[3] = f * tg;
+    o[4] = f * bn;
+    o[5] = f * bd;
+    o[6] = e2;
+    o[7] = r2;
+    o[8] = m0 > 0 ? (ss * m0 - m1 * ts) / (m0 * m0) : 0.0;
+    o[9] = m0 > 0 ? (sc1 * m0 - m1 * tc) / (m0 * m0) : 0.0;
+  }
+}
+
+inline dim3 grid1(long long n) { return dim3(static_cast<unsigned>(n)); }
+
+}  // namespace
+
+void synth(const SurGrid& g, const SynthDraw& d, long long p0, int npts, float* a, float* cg,
+           float* kdmean, cudaStream_t st) {
+  if (npts <= 0) return;
+  if (g.nk > 64 || g.nth > 64) throw CudaError(cudaErrorInvalidValue, "synth: NK or NTH above 64");
+  synth_kernel<<<grid1(npts), 64, 0, st>>>(g, d, p0, npts, a, cg, kdmean);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void prep(const SurGrid& g, int npts, const float* a, const float* cg, const float* kdmean,
+          __nv_bfloat16* x, int ldx, float* scale, int* shift, cudaStream_t st) {
+  if (npts <= 0) return;
+  const size_t smem = (static_cast<size_t>(g.nspec) + g.nk + g.nth + 32) * sizeof(float);
+  prep_kernel<<<grid1(npts), kThreads, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, scale, shift);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
+                  const int* shift, double* acc, unsigned long long* cnt, cudaStream_t st) {
+  if (npts <= 0) return;
+  if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "rowscale: NK above 64");
+  rowscale_kernel<<<grid1(npts), kThreads, 0, st>>>(g, npts, s, cg, scale, shift, acc, cnt);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void targets(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
+             const int* shift, float* t, int ldt, cudaStream_t st) {
+  if (npts <= 0) return;
+  targets_kernel<<<grid1(npts), kThreads, 0, st>>>(g, npts, s, cg, scale, shift, t, ldt);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, int ldo,
+          const float* cg, const float* scale, const int* shift, float* s, float* d,
+          int* accepted, int* rej_list, int* nrej, int* nrej_total, cudaStream_t st) {
+  if (npts <= 0) return;
+  if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "post: NK above 64");
+  post_kernel<<<grid1(npts), kThreads, 0, st>>>(g, gate, npts, out, ldo, cg, scale, shift, s, d,
+                                                 accepted, rej_list, nrej, nrej_total);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void loss_grad(const SurGrid& g, const LossWeights& w, int m, int nvalid, const float* out,
+               int ldo, const float* t, int ldt, __nv_bfloat16* grad, int ldg, float* loss,
+               cudaStream_t st) {
+  if (m <= 0) return;
+  loss_kernel<<<grid1(m), kThreads, 0, st>>>(g, w, m, nvalid, out, ldo, t, ldt, grad, ldg, loss);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void gather_batch(int m, long long n, uint64_t seed, long long offset, const __nv_bfloat16* xs,
+                  int ldx, const float* ts, int ldt, __nv_bfloat16* xb, float* tb,
+                  cudaStream_t st) {
+  if (m <= 0) return;
+  if (ldx % 8 || ldt % 4) throw CudaError(cudaErrorInvalidValue, "gather: unaligned rows");
+  gather_kernel<<<grid1(m), 128, 0, st>>>(m, n, seed, offset, xs, ldx, ts, ldt, xb, tb);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void transpose(const __nv_bfloat16* src, int rows, int cols, int lds, __nv_bfloat16* dst, int ldd,
+               cudaStream_t st) {
+  if (rows <= 0 || cols <= 0) return;
+  const dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+  transpose_kernel<<<grid, block, 0, st>>>(src, rows, cols, lds, dst, ldd);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void colsum(const __nv_bfloat16* gt, int n, int m, int ldt, float* db, cudaStream_t st) {
+  if (n <= 0) return;
+  if (m % 8 || ldt % 8) throw CudaError(cudaErrorInvalidValue, "colsum: rows not multiples of 8");
+  colsum_kernel<<<(n + 7) / 8, 256, 0, st>>>(gt, n, m, ldt, db);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void adamw(const Adam& h, int n, int k, float* w, float* m, float* v, float* g,
+           __nv_bfloat16* wb, __nv_bfloat16* wt, cudaStream_t st) {
+  const dim3 grid((k + 31) / 32, (n + 31) / 32), block(32, 8);
+  adamw_kernel<<<grid, block, 0, st>>>(h, n, k, w, m, v, g, wb, wt, 1);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void adamw_vec(const Adam& h, int n, float* w, float* m, float* v, const float* g,
+               cudaStream_t st) {
+  adamw_vec_kernel<<<(n + 255) / 256, 256, 0, st>>>(h, n, w, m, v, g);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void to_bf16(const float* w, int n, int k, __nv_bfloat16* wb, __nv_bfloat16* wt, cudaStream_t st) {
+  const dim3 grid((k + 31) / 32, (n + 31) / 32), block(32, 8);
+  Adam h{};
+  adamw_kernel<<<grid, block, 0, st>>>(h, n, k, const_cast<float*>(w), nullptr, nullptr, nullptr,
+                                       wb, wt, 0);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void init_weights(uint64_t seed, int n, int k, int nrows_valid, float gain, float* w,
+                  __nv_bfloat16* wb, __nv_bfloat16* wt, cudaStream_t st) {
+  const size_t total = static_cast<size_t>(n) * k;
+  init_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(seed, n, k, nrows_valid,
+                                                                          gain, w);
+  WWB_CHECK(cudaGetLastError());
+  to_bf16(w, n, k, wb, wt, st);
+}
+
+size_t dia_f64_smem(const DiaF64& t) {
+  const size_t nspecy = static_cast<size_t>(t.nfrhgh) * t.nth;
+  return (nspecy + t.nth + 8 * static_cast<size_t>(t.nspecx + t.nth) + 3 * t.nk) * sizeof(double);
+}
+
+void dia_f64_judge(const DiaF64& t, int npts, const float* a, const float* cg,
+                   const float* kdmean, const float* s_cand, double* stats, double* s64,
+                   double* d64, cudaStream_t st) {
+  if (npts <= 0) return;
+  const size_t smem = dia_f64_smem(t);
+  if (smem > 227 * 1024) throw CudaError(cudaErrorInvalidValue, "FP64 DIA: tables too large");
+  static size_t set = 0;
+  if (smem > set) {
+    WWB_CHECK(cudaFuncSetAttribute(dia_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    set = smem;
+  }
+  dia_f64_kernel<<<grid1(npts), kThreads, smem, st>>>(t, npts, a, cg, kdmean, s_cand, stats, s64,
+                                                       d64);
+  WWB_CHECK(cudaGetLastError());
+}
+
+}  // namespace mlp
+}  // namespace wwb

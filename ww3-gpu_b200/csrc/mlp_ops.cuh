@@ -1,0 +1,139 @@
+// ww3-gpu_b200/csrc/mlp_ops.cuh
+// The surrogate's element-wise device work around the tensor-core GEMM: synthetic sea states,
+// the spectrum normalisation (input side) and its inverse (output side, with the gate), the
+// training loss and output gradient, bias gradients, transposes, AdamW, and the FP64 DIA that
+// every surrogate result is measured against.
+//
+// Normalisation. W3SNL1 (kokkos/src/ww_kokkos/snl1_team.hpp:383-496) computes, per point,
+//   S(k, th) = CONS(kdmean) * CONX(k) * G(UE)(k, th),  UE = A / CONX,  CONX = CG / (2 pi sigma),
+// with G a cubic form of UE (sections 3-4). So with umax = max UE and U = UE / umax,
+//   S = CONS * umax^3 * CONX(k) * G(U),
+// and the network only has to learn G on spectra of unit peak: depth enters through CONX and
+// CONS, amplitude through umax^3, both applied exactly outside the network. Directions are
+// rotated so the spectrum's dominant direction comes first (the DIA commutes with a cyclic shift
+// of directions, its index tables being circulant in direction), and the rotation is undone on
+// the output. Network input: ln(U + 1e-6) / 7 + 1 per bin, then ln(kdmean) / 5 and
+// CONS / SNLC1 - 1; target: G(U)(k, th) / rowscale(k), rowscale the per-frequency RMS of G over
+// the first chunk of the training set.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace wwb {
+namespace mlp {
+
+/// Per-grid constants of the surrogate's pre- and post-processing.
+struct SurGrid {
+  int nk, nth, nspec;
+  int din, dout;          ///< padded network widths (multiples of 64)
+  const float* sig;       ///< device, NK
+  const float* rowscale;  ///< device, NK (target scale per frequency row)
+  const float* omega;     ///< device, NK: rowscale * DDEN / (2 pi sigma), the Hs-tendency weight
+                          ///< of a normalised output bin
+  float snlc1, kdcon, kdmn, snls1, snls2, snls3;
+  float dth, xfr;
+};
+
+/// Sea-state draw of the synthetic training and test sets (JONSWAP wind sea with cos^2s
+/// spreading, optionally a swell system), seeded per point.
+struct SynthDraw {
+  uint64_t seed;
+  double bimodal;    ///< fraction of points with an added swell system
+  double dmin, dmax; ///< depth drawn log-uniformly in [dmin, dmax] (dmin == dmax: fixed)
+};
+
+/// Gate thresholds: a point keeps the surrogate's S when the energy residual of its output
+/// |sum w S| / sum w |S| is at most `energy` and the network's own predicted error (the
+/// log of its Hs-tendency error, output column NSPEC) is at most `log_err`.
+struct GateParams {
+  float energy;
+  float log_err;
+};
+
+void synth(const SurGrid& g, const SynthDraw& d, long long p0, int npts, float* a, float* cg,
+           float* kdmean, cudaStream_t st);
+
+/// Network input rows x (npts x ldx bf16) plus per-point scale and direction shift.
+void prep(const SurGrid& g, int npts, const float* a, const float* cg, const float* kdmean,
+          __nv_bfloat16* x, int ldx, float* scale, int* shift, cudaStream_t st);
+
+/// Accumulate sum over points and directions of (S / (scale CONX))^2 per row into acc (double,
+/// NK, zeroed by the caller), and count the points with a nonzero scale into cnt.
+void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
+                  const int* shift, double* acc, unsigned long long* cnt, cudaStream_t st);
+
+/// Normalised targets t (npts x ldt fp32) from the DIA's S.
+void targets(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
+             const int* shift, float* t, int ldt, cudaStream_t st);
+
+/// Output side of inference: S (de-normalised, rotated back) and D = 0 for accepted points, the
+/// compacted list of rejected points (count at *nrej, zeroed by the caller; also added to
+/// *nrej_total when given), per-point flag.
+void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, int ldo,
+          const float* cg, const float* scale, const int* shift, float* s, float* d,
+          int* accepted, int* rej_list, int* nrej, int* nrej_total, cudaStream_t st);
+
+/// Training loss and the output gradient. out (m x ldo fp32), t (m x ldt): grad (m x dout bf16)
+/// = dL/dout; loss (3 floats: MSE, energy-budget, error-head terms) accumulated.
+struct LossWeights {
+  float mu;      ///< weight of the squared relative Hs-tendency error
+  float lambda;  ///< weight of the error head
+  int head;      ///< 1: column NSPEC is trained as the error head
+};
+void loss_grad(const SurGrid& g, const LossWeights& w, int m, int nvalid, const float* out,
+               int ldo, const float* t, int ldt, __nv_bfloat16* grad, int ldg, float* loss,
+               cudaStream_t st);
+
+/// Batch rows r < m of the training set: x rows idx(r) and t rows idx(r), idx(r) a seeded draw
+/// in [0, n) (or r + offset when seed == 0).
+void gather_batch(int m, long long n, uint64_t seed, long long offset, const __nv_bfloat16* xs,
+                  int ldx, const float* ts, int ldt, __nv_bfloat16* xb, float* tb,
+                  cudaStream_t st);
+
+/// dst (cols x rows) = src (rows x cols)^T, bf16; ld's in elements.
+void transpose(const __nv_bfloat16* src, int rows, int cols, int lds, __nv_bfloat16* dst, int ldd,
+               cudaStream_t st);
+
+/// db[n] = sum over m of gt[n][m] (gt is the transposed gradient, n rows of m).
+void colsum(const __nv_bfloat16* gt, int n, int m, int ldt, float* db, cudaStream_t st);
+
+/// AdamW on one weight matrix (n x k) and its bias: fp32 master w, moments m, v, gradient g
+/// (zeroed after use), the bf16 copy wb (n x k) and its transpose wt (k x n).
+struct Adam {
+  float lr, beta1, beta2, eps, wd;
+  float c1, c2;  ///< bias corrections 1 - beta^t
+};
+void adamw(const Adam& h, int n, int k, float* w, float* m, float* v, float* g,
+           __nv_bfloat16* wb, __nv_bfloat16* wt, cudaStream_t st);
+void adamw_vec(const Adam& h, int n, float* w, float* m, float* v, const float* g,
+               cudaStream_t st);
+
+/// Weights U(-a, a), a = gain * sqrt(3 / fan_in), rows >= nrows_valid zero; fp32 and bf16 copies.
+void init_weights(uint64_t seed, int n, int k, int nrows_valid, float gain, float* w,
+                  __nv_bfloat16* wb, __nv_bfloat16* wt, cudaStream_t st);
+void to_bf16(const float* w, int n, int k, __nv_bfloat16* wb, __nv_bfloat16* wt, cudaStream_t st);
+
+/// The FP64 DIA (the same four sections as W3SNL1 in double precision, tables in double) and
+/// the error of a candidate S against it, per point, as 10 doubles:
+///   0 Hs, 1 Hs tendency of the FP64 S, 2 Hs tendency of the candidate, 3 gross Hs tendency
+///   (sum of |S| terms), 4 sum |band tendency error|, 5 sum |band tendency|, 6 sum (S - S64)^2,
+///   7 sum S64^2, 8 mean-frequency tendency of the FP64 S, 9 of the candidate.
+struct DiaF64 {
+  int nk, nth, nfr, nfrhgh, nfrchg, nspec, nspecx;
+  double dal1, dal2, dal3, awg[8], swg[8];
+  double snlc1, kdcon, kdmn, snls1, snls2, snls3, fachfe, dth, xfr;
+  const int* ipim;       ///< device, 16 x NSPECX
+  const int* ic;         ///< device, 16 x NSPEC
+  const double* af11;    ///< device, NFRCHG (per row)
+  const double* sig;     ///< device, NK
+};
+size_t dia_f64_smem(const DiaF64& t);
+void dia_f64_judge(const DiaF64& t, int npts, const float* a, const float* cg,
+                   const float* kdmean, const float* s_cand, double* stats, double* s64,
+                   double* d64, cudaStream_t st);
+
+}  // namespace mlp
+}  // namespace wwb

@@ -379,12 +379,17 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* e
   atomicExch(err, 1);
 }
 
-template <int BLOCK, int MINB, int AS, bool TMA>
+// LIST: the batch is the points pidx[0 .. min(npts, *pcount)) of the arrays (the gated
+// surrogate's fallback list, whose length is known only on the device); otherwise points
+// 0 .. npts. Either way each point's arithmetic is the same.
+template <int BLOCK, int MINB, int AS, bool TMA, bool LIST = false>
 __global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
-    const Snl1Dev p, const int npts, const float* __restrict__ a, const float* __restrict__ cg,
+    const Snl1Dev p, int npts, const float* __restrict__ a, const float* __restrict__ cg,
     const float* __restrict__ kdmean, float* __restrict__ s, float* __restrict__ d,
-    int* __restrict__ err) {
+    int* __restrict__ err, const int* __restrict__ pidx, const int* __restrict__ pcount) {
   extern __shared__ __align__(16) float smem[];
+  if (LIST) npts = min(npts, __ldg(pcount));
+  auto pt = [&](int i) { return LIST ? __ldg(pidx + i) : i; };
   const int nth = p.nth, nfr = p.nfr, nfrhgh = p.nfrhgh, nfrchg = p.nfrchg;
   const int nspec = p.nspec, nk = p.nk;
   // The six interaction arrays sit AS floats apart (AS >= (NFRCHG + 1) * NTH, a compile-time
@@ -413,7 +418,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
   for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
   if (TMA && tid == 0) {
     mbar_init(bar, 1);
-    if (blockIdx.x < npts) tma_fetch_point(bar, stage, a, cg, blockIdx.x, nspec, nk);
+    if (blockIdx.x < npts) tma_fetch_point(bar, stage, a, cg, pt(blockIdx.x), nspec, nk);
   }
   __syncthreads();
 
@@ -434,10 +439,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
   // The UE loop of section 2 walks bins isp = tid + k * BLOCK.
   const int dq = BLOCK / nth, dr = BLOCK % nth, q0 = tid / nth, r0 = tid % nth;
 
-  float kd_next = (blockIdx.x < npts) ? __ldg(kdmean + blockIdx.x) : 0.0f;
+  float kd_next = (blockIdx.x < npts) ? __ldg(kdmean + pt(blockIdx.x)) : 0.0f;
   unsigned parity = 0;
   int buf = 0;
-  for (int ipt = blockIdx.x; ipt < npts; ipt += gridDim.x, buf ^= 1) {
+  for (int ipt0 = blockIdx.x; ipt0 < npts; ipt0 += gridDim.x, buf ^= 1) {
+    const int ipt = pt(ipt0);
     const float* const src_a = TMA ? stage : a + static_cast<size_t>(ipt) * nspec;
     const float* const src_c = TMA ? stage + nspec : cg + static_cast<size_t>(ipt) * nk;
     float* const conx = conx2 + buf * nk;
@@ -474,9 +480,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
     __syncthreads();
 
     // The next point's A and CG stream into the staging buffer while this one is computed.
-    const int inext = ipt + gridDim.x;
-    if (TMA && tid == 0 && inext < npts) tma_fetch_point(bar, stage, a, cg, inext, nspec, nk);
-    if (inext < npts) kd_next = __ldg(kdmean + inext);
+    const int inext = ipt0 + gridDim.x;
+    if (TMA && tid == 0 && inext < npts) tma_fetch_point(bar, stage, a, cg, pt(inext), nspec, nk);
+    if (inext < npts) kd_next = __ldg(kdmean + pt(inext));
 
     // 3. Interactions over the extended spectrum, sliding up the band.
     if (n3 > 0) {
@@ -976,7 +982,7 @@ void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, co
   }
   const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
   const int grid = static_cast<int>(npts < resident ? npts : resident);
-  k<<<grid, kBandBlock, smem, stream>>>(p, npts, a, cg, kd, s, d, err);
+  k<<<grid, kBandBlock, smem, stream>>>(p, npts, a, cg, kd, s, d, err, nullptr, nullptr);
   WWB_CHECK(cudaGetLastError());
 }
 
@@ -1092,6 +1098,50 @@ void launch_snl1_err(int kernel, const Snl1Dev& p, int npts, const float* a, con
                      const float* kdmean, float* s, float* d, int* err, cudaStream_t stream) {
   if (err == nullptr) throw CudaError(cudaErrorInvalidValue, "launch_snl1_err: null error flag");
   launch_dispatch(kernel, p, npts, a, cg, kdmean, s, d, err, stream);
+}
+
+namespace {
+template <int AS, bool TMA>
+void launch_band_list(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
+                      const float* a, const float* cg, const float* kd, float* s, float* d,
+                      int* err, cudaStream_t stream) {
+  static int per_sm = -1;
+  static size_t cached = 0;
+  const size_t smem = snl1_band_smem(p);
+  auto k = snl1_band_kernel<kBandBlock, kBandMinBlocks, AS, TMA, true>;
+  if (per_sm < 0 || cached != smem) {
+    WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    int n = 0;
+    WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kBandBlock, smem));
+    if (n < 1) throw CudaError(cudaErrorInvalidConfiguration, "snl1 band occupancy");
+    per_sm = n;
+    cached = smem;
+  }
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  const int grid = static_cast<int>(capacity < resident ? capacity : resident);
+  k<<<grid, kBandBlock, smem, stream>>>(p, capacity, a, cg, kd, s, d, err, pidx, pcount);
+  WWB_CHECK(cudaGetLastError());
+}
+}  // namespace
+
+bool launch_snl1_list(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
+                      const float* a, const float* cg, const float* kdmean, float* s, float* d,
+                      int* err, cudaStream_t stream) {
+  if (capacity <= 0) return true;
+  if (!snl1_band_ok(p)) return false;
+  if (err == nullptr) err = band_err_flag();
+  const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
+                       (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
+  const bool tma = p.nspec % 4 == 0 && p.nk % 4 == 0 && aligned;
+  if (band_stride(p) == 1536) {
+    if (tma) launch_band_list<1536, true>(p, capacity, pidx, pcount, a, cg, kdmean, s, d, err, stream);
+    else launch_band_list<1536, false>(p, capacity, pidx, pcount, a, cg, kdmean, s, d, err, stream);
+  } else {
+    if (tma) launch_band_list<4096, true>(p, capacity, pidx, pcount, a, cg, kdmean, s, d, err, stream);
+    else launch_band_list<4096, false>(p, capacity, pidx, pcount, a, cg, kdmean, s, d, err, stream);
+  }
+  return true;
 }
 
 }  // namespace wwb

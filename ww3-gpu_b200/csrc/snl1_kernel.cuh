@@ -63,4 +63,11 @@ Snl1StaticScratch snl1_static_scratch();
 void launch_snl1_err(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                      const float* kdmean, float* s, float* d, int* err, cudaStream_t stream);
 
+/// The band kernel on the points pidx[0 .. min(capacity, *pcount)) of the arrays (pidx and
+/// pcount device pointers; the count may be written by an earlier kernel on `stream`). Returns
+/// false, launching nothing, when the band kernel cannot run these tables.
+bool launch_snl1_list(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
+                      const float* a, const float* cg, const float* kdmean, float* s, float* d,
+                      int* err, cudaStream_t stream);
+
 }  // namespace wwb

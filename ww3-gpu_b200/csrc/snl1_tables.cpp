@@ -178,6 +178,66 @@ bool build_snl1_tables(const Snl1Config& c, const float* sig, Snl1Tables& t) {
   return true;
 }
 
+bool build_snl1_weights_f64(const Snl1Config& c, const float* sig, const Snl1Tables& t,
+                            Snl1WeightsF64& w) {
+  const double one = 1.0, lam = c.lam, dth = c.dth, xfr = c.xfr;
+  auto powi_d = [](double x, int n) {
+    unsigned m = n < 0 ? static_cast<unsigned>(-n) : static_cast<unsigned>(n);
+    double y = (m & 1u) ? x : 1.0;
+    while ((m >>= 1u) != 0u) {
+      x = x * x;
+      if (m & 1u) y = y * x;
+    }
+    return n < 0 ? 1.0 / y : y;
+  };
+  auto pow11_d = [](double x) {
+    const double x2 = x * x, x3 = x2 * x, x5 = x2 * x3, x6 = x3 * x3;
+    return x5 * x6;
+  };
+  const double lamm2_b = one - lam, lamp2_b = one + lam;
+  const double lamm2 = lamm2_b * lamm2_b, lamp2 = lamp2_b * lamp2_b;
+  const double delth3 = std::acos((lamm2 * lamm2 + 4.0 - lamp2 * lamp2) / (4.0 * lamm2));
+  const double delth4 = std::asin(-std::sin(delth3) * lamm2 / lamp2);
+  const double p2 = lamp2_b * lamp2_b, m2 = lamm2_b * lamm2_b;
+  w.dal1 = one / (p2 * p2);
+  w.dal2 = one / (m2 * m2);
+  w.dal3 = 2.0 * w.dal1 * w.dal2;
+  const double cthp = std::fabs(delth4 / dth);
+  const int ithp = static_cast<int>(cthp);
+  const double wthp = cthp - ithp, wthp1 = one - wthp;
+  const double cthm = std::fabs(delth3 / dth);
+  const int ithm = static_cast<int>(cthm);
+  const double wthm = cthm - ithm, wthm1 = one - wthm;
+  const double xfrln = std::log(xfr);
+  const int ifrp = static_cast<int>(std::log(one + lam) / xfrln), ifrp1 = ifrp + 1;
+  const double wfrp = (one + lam - powi_d(xfr, ifrp)) / (powi_d(xfr, ifrp1) - powi_d(xfr, ifrp));
+  const double wfrp1 = one - wfrp;
+  const int ifrm = static_cast<int>(std::log(one - lam) / xfrln), ifrm1 = ifrm - 1;
+  const double wfrm = (powi_d(xfr, ifrm) - (one - lam)) / (powi_d(xfr, ifrm) - powi_d(xfr, ifrm1));
+  const double wfrm1 = one - wfrm;
+  const Geometry gf = geometry(c);
+  if (ithp != gf.ithp || ithm != gf.ithm || ifrp != gf.ifrp || ifrm != gf.ifrm) return false;
+  w.awg[0] = wthp * wfrp;
+  w.awg[1] = wthp1 * wfrp;
+  w.awg[2] = wthp * wfrp1;
+  w.awg[3] = wthp1 * wfrp1;
+  w.awg[4] = wthm * wfrm;
+  w.awg[5] = wthm1 * wfrm;
+  w.awg[6] = wthm * wfrm1;
+  w.awg[7] = wthm1 * wfrm1;
+  for (int j = 0; j < 8; ++j) w.swg[j] = w.awg[j] * w.awg[j];
+  const double tpiinv = 1.0 / (2.0 * 3.141592653589793);
+  w.af11_row.assign(static_cast<size_t>(t.nfrchg), 0.0);
+  for (int ifr = 0; ifr < t.nfr && ifr < t.nfrchg; ++ifr)
+    w.af11_row[ifr] = pow11_d(static_cast<double>(sig[ifr]) * tpiinv);
+  double fr = static_cast<double>(sig[t.nfr - 1]) * tpiinv;
+  for (int ifr = t.nfr; ifr < t.nfrchg; ++ifr) {
+    fr = fr * xfr;
+    w.af11_row[ifr] = pow11_d(fr);
+  }
+  return true;
+}
+
 void derive_rowshift(const Snl1Config& c, Snl1Tables& t) {
   const int nth = c.nth;
   const Geometry g = geometry(c);

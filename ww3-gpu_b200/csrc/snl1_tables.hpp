@@ -60,4 +60,15 @@ bool build_snl1_tables(const Snl1Config& c, const float* sig, Snl1Tables& t);
 /// entry of `t` (which may come from the caller). Also checks AF11 is constant along rows.
 void derive_rowshift(const Snl1Config& c, Snl1Tables& t);
 
+/// INSNL1's weights in double precision for the FP64 DIA: the same steps as the float tables
+/// with every real in double (the FP64 restatement of W3SNL1 that surrogate errors are measured
+/// against). af11 has one value per row (NFRCHG). Returns false when the double geometry's
+/// integer offsets differ from the float tables' (the index tables would then differ too).
+struct Snl1WeightsF64 {
+  double dal1 = 0, dal2 = 0, dal3 = 0, awg[8] = {}, swg[8] = {};
+  std::vector<double> af11_row;
+};
+bool build_snl1_weights_f64(const Snl1Config& c, const float* sig, const Snl1Tables& t,
+                            Snl1WeightsF64& w);
+
 }  // namespace wwb
