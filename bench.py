@@ -77,8 +77,8 @@ def parse():
     p.add_argument("--steps", type=int, default=None)
     p.add_argument("--warmup", type=int, default=None)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--workload", choices=["srce", "dia", "step", "outg", "multigrid"],
-                   default="srce")
+    p.add_argument("--workload", choices=["surrogate", "srce", "dia", "step", "outg",
+                                          "multigrid"], default="surrogate")
     p.add_argument("--scale", type=float, default=1.0 / 16.0,
                    help="multigrid workload: factor on the 5k-400k sea points of each grid")
     p.add_argument("--nx", type=int, default=360, help="step/outg workloads: grid longitudes")
@@ -86,14 +86,28 @@ def parse():
     p.add_argument("--npts", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--train-steps", type=int, default=6000,
+                   help="surrogate workload: AdamW steps of batch 8192 before the timing")
+    p.add_argument("--sur-lr", type=float, default=1e-3)
+    p.add_argument("--sur-mu", type=float, default=1.0,
+                   help="surrogate loss weight of the squared Hs-tendency error")
+    p.add_argument("--sur-lambda", type=float, default=0.05,
+                   help="surrogate loss weight of the error head")
+    p.add_argument("--sur-energy", type=float, default=0.05,
+                   help="gate: largest energy residual of an accepted point")
+    p.add_argument("--sur-target", type=float, default=0.02,
+                   help="gate calibration: mean Hs-tendency error budget")
+    p.add_argument("--no-srce-line", action="store_true",
+                   help="surrogate workload: leave out the W3SRCE line it carries")
     p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band", "tile"], default="auto",
                    help="DIA kernel (ww_snl1_select_kernel); auto picks the band kernel")
     a = p.parse_args()
     srce = a.workload == "srce"
     if a.steps is None:
-        a.steps = {"srce": 20, "dia": 200, "step": 10, "outg": 20, "multigrid": 5}[a.workload]
+        a.steps = {"surrogate": 50, "srce": 20, "dia": 200, "step": 10, "outg": 20,
+                   "multigrid": 5}[a.workload]
     if a.warmup is None:
-        a.warmup = 5 if a.workload == "dia" else 3
+        a.warmup = 5 if a.workload in ("dia", "surrogate") else 3
     if a.npts is None:
         a.npts = SRCE_NPTS if srce else NPTS_PER_GPU
     return a
@@ -475,7 +489,9 @@ def run_reference_srce(args):
     return 0
 
 
-def run_b200_srce(args):
+def run_b200_srce(args, quiet=False, npts=None, steps=None, warmup=None, igrid=1):
+    """The W3SRCE line; with quiet=True (called from another workload, one GPU) it is returned
+    instead of printed, for npts points over steps timed steps on grid igrid."""
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -485,13 +501,15 @@ def run_b200_srce(args):
         raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
     torch.cuda.set_device(local)
     os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
-    if world > 1:
+    if world > 1 and not quiet:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     pkg = entry.load_package()
     synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
-    npts = args.npts
+    npts = npts or args.npts
+    steps = steps or steps
+    warmup = warmup or warmup
     st, t, sr, cfg, sig, pts = srce_inputs(synth, npts, 2026 + rank)
-    grid = pkg.SrceGrid(1, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig, sr)
+    grid = pkg.SrceGrid(igrid, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig, sr)
     dev = torch.device("cuda", local)
     d0 = {k: torch.from_numpy(pts[k]).to(dev) for k in SRCE_ARRAYS}
     d = {k: v.clone() for k, v in d0.items()}
@@ -524,26 +542,26 @@ def run_b200_srce(args):
         if ev is not None:
             ev[1].record(stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     barrier()
-    kev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    kev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         time.sleep(0.3)
         barrier()
         t_start.record(stream)
-        for i in range(args.steps):
+        for i in range(steps):
             step(kev[i])
         t_end.record(stream)
         barrier()
     total_ms = max_over_ranks(t_start.elapsed_time(t_end))
-    launch_ms = sum(e[0].elapsed_time(e[1]) for e in kev) / args.steps
-    value = npts * world * args.steps / (total_ms / 1e3)
+    launch_ms = sum(e[0].elapsed_time(e[1]) for e in kev) / steps
+    value = npts * world * steps / (total_ms / 1e3)
     out_dev = {k: d[k].cpu().numpy() for k in ("spec", "psc")}
 
     # ---- end to end through the host entry ww_srce_batch, page-locked host buffers
-    e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
+    e2e_steps = args.e2e_steps or max(3, min(steps, 5))
     h = {k: torch.from_numpy(pts[k].copy()).pin_memory() for k in SRCE_ARRAYS}
     h_shave = torch.zeros(npts, dtype=torch.int32).pin_memory()
 
@@ -571,8 +589,8 @@ def run_b200_srce(args):
     achieved = SRCE_BYTES_PER_POINT * npts / (launch_ms / 1e3) / 1e9
     tpp = ncu_traffic_per_point("srce_kernel")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": srce_config(args, world),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * per_pt_in * npts,
@@ -586,15 +604,17 @@ def run_b200_srce(args):
                      "algorithmic_bytes_per_point": SRCE_BYTES_PER_POINT,
                      "note": ("W3SRCE is bound by FP32 issue and its serial ordered sums, not by "
                               "HBM; the fraction shows how far from the HBM ceiling it runs")},
-        "gpu_launches": args.steps,
+        "gpu_launches": steps,
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not quiet:
         r = cpu_reference_srce(st, t, sr, cfg, sig, pts)
         if r is not None:
             rate, kind, cores, sample = r
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                                     "sample": sample}
+    if quiet:
+        return line
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -1334,8 +1354,261 @@ def run_reference_outg(args):
     return 0
 
 
+# ---------------------------------------------------------------- the gated DIA surrogate
+SUR_WORKLOAD = ("W3SNL1 36x36 on 262,144 sea points per GPU of the learned-surrogate workload's "
+                "spectra (JONSWAP wind seas, 20% with a swell system, depth log-uniform 5-4000 m): "
+                "the gated surrogate (BF16 MLP 1296->1024->1024->1024->1296 on tcgen05, per-point "
+                "gate, rejected points on the plain DIA) against the plain DIA")
+SUR_FLOP_PER_POINT = 2 * (1296 * 1024 + 2 * 1024 * 1024 + 1024 * 1296)  # 9.50e6, the model's
+SUR_TRAIN_POINTS = 2_000_000
+SUR_HOLDOUT = 65_536
+SUR_BATCH = 8192
+SUR_INFER_ROWS = 65_536
+
+
+def measured_peak_bf16():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+        except Exception:
+            pass
+    return 1590.0, "fallback"
+
+
+def sur_config(args, world, train):
+    return {"workload": SUR_WORKLOAD, "nk": NK, "nth": NTH, "npts_per_gpu": args.npts,
+            "global_points": args.npts * world, "seed": 2024,
+            "training": train,
+            "hs_error": ("per point |dHs/dt(S) - dHs/dt(S64)| / (8/Hs sum |S64| DDEN/CG), "
+                         "Hs = 4 sqrt(sum A DDEN/CG) as in the reference's W3SRCE "
+                         "(srce_kernel.hpp:415-430); S64 = this library's FP64 DIA on the device; "
+                         "a rejected point counts its plain-DIA error"),
+            "l2": "inputs 1.4 GB and outputs 2.7 GB per pass > 126 MB L2 (no flush needed)",
+            "parallelism": f"points sharded over {world} GPU(s), no collective; each GPU trains "
+                           "its own copy of the surrogate"}
+
+
+def run_reference_surrogate(args):
+    """The reference has no learned part: its arm is its plain DIA (its own C++ on the host
+    cores) on the same spectra, the method the gated surrogate stands in for."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    cfg, sig = synth.dia_config(NK, NTH)
+    n = 2048
+    g = synth.sea_states(n, seed=2024, depth_range=(5.0, 4000.0), bimodal=0.2)
+    oracle = entry.load_oracle()
+    if oracle.ref_available():
+        run = oracle.RefSnl1(cfg, sig, igrid=1)
+        kind = "reference"
+        step = lambda: run(g["a"], g["cg"], g["kdmean"])  # noqa: E731
+    else:
+        kind = "port"
+        step = lambda: oracle.w3snl1(cfg, sig, g["a"], g["cg"], g["kdmean"])  # noqa: E731
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    rate = n * args.steps / el
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cfgd = sur_config(args, 1, "none: the reference has no learned part; this is its plain DIA")
+    cfgd["reference_sample_points_per_step"] = n
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": cfgd,
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{n} points of the workload's spectra per step, OpenMP over "
+                                   "points (the plain DIA: the reference has no surrogate)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200_surrogate(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device; the B200 arm has no CPU fallback")
+    torch.cuda.set_device(local)
+    os.environ.setdefault("WW_KOKKOS_DEVICE_ID", str(local))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    pkg = entry.load_package()
+    synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
+    sur = __import__("ww3_gpu_b200.surrogate", fromlist=["surrogate"])
+    cfg, sig = synth.dia_config(NK, NTH)
+    grid = pkg.Snl1Grid(cfg, sig, igrid=1)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    handle = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- set-up (untimed): training data from the plain DIA kernel, training, gate calibration
+    t_setup = time.perf_counter()
+    model = sur.Surrogate(1, nhidden=1024, seed=2024 + rank)
+    model.dataset(SUR_TRAIN_POINTS, SUR_HOLDOUT, seed=2024 + rank, bimodal=0.2, dmin=5.0,
+                  dmax=4000.0)
+    model.loss_weights(args.sur_mu, args.sur_lambda)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter()
+    losses = model.train(args.train_steps, batch=SUR_BATCH, lr=args.sur_lr, lr_end=args.sur_lr * 0.01,
+                         seed=7 + rank)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t_train
+    holdout = model.eval(SUR_TRAIN_POINTS - SUR_HOLDOUT, SUR_HOLDOUT)
+    cal = model.calibrate(65536, seed=90_001 + rank, bimodal=0.2, dmin=5.0, dmax=4000.0,
+                          energy=args.sur_energy, target=args.sur_target)
+    setup_s = time.perf_counter() - t_setup
+
+    npts = args.npts
+    a = torch.empty(npts, NK * NTH, device=dev)
+    cg = torch.empty(npts, NK, device=dev)
+    kd = torch.empty(npts, device=dev)
+    model.synth(npts, a, cg, kd, seed=31_337 + rank, bimodal=0.2, dmin=5.0, dmax=4000.0)
+    s = torch.empty_like(a)
+    d = torch.empty_like(a)
+    s_plain = torch.empty_like(a)
+    d_plain = torch.empty_like(a)
+    barrier()
+
+    def timed(fn, steps, warmup, ev_per_step=False):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    # ---- the plain DIA (the method without the learned part), same points, same clock
+    plain_ms = timed(lambda: grid.run_device(npts, a, cg, kd, s_plain, d_plain, handle),
+                     args.steps, args.warmup) / args.steps
+    # ---- the gated surrogate: value
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        total_ms = timed(lambda: model.gated(npts, a, cg, kd, s, d, None, handle), args.steps,
+                         args.warmup)
+    gated_ms = total_ms / args.steps
+    value = npts * world * args.steps / (total_ms / 1e3)
+    fallback = model.fallback_count(handle)
+
+    # ---- every result's error against the FP64 DIA (this library's, on the device)
+    stats = torch.empty(npts, 10, dtype=torch.float64, device=dev)
+    model.judge(npts, a, cg, kd, s, stats, stream=handle)
+    err_gated = sur.error_summary(stats.cpu().numpy())
+    model.judge(npts, a, cg, kd, s_plain, stats, stream=handle)
+    err_plain = sur.error_summary(stats.cpu().numpy())
+
+    # ---- the network alone (the four tcgen05 GEMMs), for the roofline
+    rows = SUR_INFER_ROWS
+    x = torch.randn(rows, 1344, device=dev).to(torch.bfloat16)
+    out = torch.empty(rows, 1344, device=dev)
+    fwd_ms = timed(lambda: model.forward(rows, x, out, handle), 20, 3) / 20
+    achieved = SUR_FLOP_PER_POINT * rows / (fwd_ms / 1e3) / 1e12
+    peak, peak_kind = measured_peak_bf16()
+
+    # ---- end to end: page-locked host inputs in, S and D out, every step
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
+    h_a, h_cg, h_kd = a.cpu().pin_memory(), cg.cpu().pin_memory(), kd.cpu().pin_memory()
+    h_s = torch.empty_like(h_a).pin_memory()
+    h_d = torch.empty_like(h_a).pin_memory()
+    da, dcg, dkd = torch.empty_like(a), torch.empty_like(cg), torch.empty_like(kd)
+    ds, dd = torch.empty_like(a), torch.empty_like(a)
+
+    def e2e_step():
+        da.copy_(h_a, non_blocking=True)
+        dcg.copy_(h_cg, non_blocking=True)
+        dkd.copy_(h_kd, non_blocking=True)
+        model.gated(npts, da, dcg, dkd, ds, dd, None, handle)
+        h_s.copy_(ds, non_blocking=True)
+        h_d.copy_(dd, non_blocking=True)
+
+    e2e_ms = timed(e2e_step, e2e_steps, 1)
+    e2e_value = npts * world * e2e_steps / (e2e_ms / 1e3)
+    same = bool(torch.equal(h_s.view(torch.int32), s.cpu().view(torch.int32)))
+
+    chunks = (npts + SUR_INFER_ROWS - 1) // SUR_INFER_ROWS
+    train = {"points": SUR_TRAIN_POINTS, "holdout": SUR_HOLDOUT, "steps": args.train_steps,
+             "batch": SUR_BATCH, "lr": args.sur_lr, "mu": args.sur_mu, "lambda": args.sur_lambda,
+             "train_s": train_s, "ms_per_step": 1e3 * train_s / max(1, args.train_steps),
+             "setup_s": setup_s, "loss_first": [float(v) for v in losses[:50].mean(axis=0)],
+             "loss_last": [float(v) for v in losses[-200:].mean(axis=0)],
+             "holdout_loss": [float(v) for v in holdout], "gate": cal,
+             "train_tflops": (3 * SUR_FLOP_PER_POINT * SUR_BATCH * args.train_steps
+                              / max(train_s, 1e-9) / 1e12)}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": gated_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network / f32 fallback",
+        "data": "synthetic", "config": sur_config(args, world, train),
+        "plain_dia": {"value": npts * world / (plain_ms / 1e3), "unit": UNIT,
+                      "ms_per_step": plain_ms, "kernel": "snl1_band_kernel",
+                      "error_vs_fp64": err_plain},
+        "speedup_vs_plain": plain_ms / gated_ms,
+        "accepted_fraction": 1.0 - fallback / npts,
+        "error_vs_fp64": err_gated,
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": int((h_a.numel() + h_cg.numel() + h_kd.numel()) * 4),
+                "d2h_bytes_per_step": int((h_s.numel() + h_d.numel()) * 4),
+                "steps": e2e_steps, "entry": "ww_snl1_gated on copies of page-locked host buffers",
+                "matches_device_entry": same},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops, burst)",
+                     "traffic": None, "kernel": "gemm_kernel (tcgen05, 4 launches per forward)",
+                     "forward_ms_65536_rows": fwd_ms,
+                     "algorithmic_flop_per_point": SUR_FLOP_PER_POINT},
+        "gpu_launches": args.steps * chunks * 7,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        g = {"a": a[:4096].cpu().numpy(), "cg": cg[:4096].cpu().numpy(),
+             "kdmean": kd[:4096].cpu().numpy()}
+        rate, kind, cores, sample = cpu_reference_rate(cfg, sig, g)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": sample + " (the plain DIA: the reference has no "
+                                                   "surrogate)"}
+    if rank == 0 and world == 1 and not args.no_srce_line:
+        line["w3srce_config1"] = run_b200_srce(args, quiet=True, npts=SRCE_NPTS, steps=10, igrid=2,
+                                               warmup=3)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "surrogate":
+        return (run_reference_surrogate(args) if args.impl == "reference"
+                else run_b200_surrogate(args))
     if args.workload == "dia":
         return run_reference_dia(args) if args.impl == "reference" else run_b200_dia(args)
     if args.workload == "step":

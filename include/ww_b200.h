@@ -90,8 +90,10 @@ void ww_snl1_device(int igrid, int npts, const float* a, const float* cg, const 
  * 3*c(npts*NSPEC) + c(npts*NK) + c(npts) <= 8388608 floats, c() rounding up to a multiple of
  * 64 (2137 points of a 36x36 grid); a larger npts is ERR_BAD_SHAPE with nothing written. The
  * first call on a device does the set-up (resolves the array's address); make it before any
- * stream capture. The array is one per device for the whole process: calls that overlap in
- * time (several host threads) race on it. No cudaMalloc, cudaFree or allocating library call. */
+ * stream capture. The device current at the call must be the one of the grid's ww_snl1_init
+ * (else ERR_BAD_SHAPE, nothing written). The array is one per device for the whole process:
+ * calls that overlap in time (several host threads) race on it. No cudaMalloc, cudaFree or
+ * allocating library call. */
 void ww_snl1_noalloc(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
                      float* s, float* d);
 

@@ -85,6 +85,42 @@ def test_srce_batch_bitexact(pkg, oracle, synth, tables, variant, ln1, seed, it,
     assert np.array_equal(g["shave"], r["shave"])
 
 
+def test_srce_bench_workload_bitexact(pkg, oracle, synth):
+    """Exactly the inputs bench.py's W3SRCE line times: the analytic-tail ST4 configuration with
+    this project's own ST4 tables (synth.st4_tables_own, registered on both sides), the default
+    W3SRCE packets, 9520 points of seed 2026. The reference's C++ (scalar-libmvec build) and the
+    GPU agree bit for bit through the host entry ww_srce_batch and the device entry
+    ww_srce_batch_device the bench calls."""
+    import torch
+
+    st = synth.st4_setup(variant="analytic")
+    t = synth.st4_tables_own(st)
+    sr = synth.srce_setup(st)
+    ig = 240
+    ref = oracle.RefSt4(st, t, igrid=ig, srce=sr, dia=synth.dia_config(), scalar_mvec=True)
+    L, be = gpu_setup(pkg, oracle, synth, st, t, ig, srce=sr)
+    pts = synth.srce_points(9520, seed=2026)
+    r = sc.ref_backend(ref.L, ig).srce_batch(pts, it=1)
+    assert ref.L.ww_srce_last_error() == 0
+    g = be.srce_batch(pts, it=1)
+    assert L.ww_srce_last_error() == 0
+    for k in ("spec", "psc", "whitecap", "taubbl", "tauice"):
+        assert_bitexact(g[k], r[k], f"bench workload, host entry, {k}")
+    assert np.array_equal(g["shave"], r["shave"])
+    dv = {k: torch.from_numpy(np.ascontiguousarray(pts[k])).cuda()
+          for k in ("spec", "wn1", "cg1", "pin", "psc", "whitecap", "taubbl", "tauice")}
+    shave = torch.zeros(9520, dtype=torch.int32, device="cuda")
+    L.ww_srce_batch_device(ig, 1, 0, 1, 1, 900.0, 9520,
+                           *[dv[k].data_ptr() for k in ("spec", "wn1", "cg1", "pin", "psc",
+                                                        "whitecap", "taubbl", "tauice")],
+                           shave.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert L.ww_srce_last_error() == 0
+    for k in ("spec", "psc", "whitecap", "taubbl", "tauice"):
+        assert_bitexact(dv[k].cpu().numpy(), r[k], f"bench workload, device entry, {k}")
+    assert np.array_equal(shave.cpu().numpy(), r["shave"])
+
+
 def test_srce_batch_va_and_single_point(pkg, oracle, synth, tables):
     """The resident-VA batch writes the same spectra into the VA columns JSEA names, and the
     one-point entry ww_srce gives the batch's result for that point."""

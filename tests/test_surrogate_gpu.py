@@ -248,12 +248,12 @@ def test_training_gains_over_the_untrained_network(model, sur):
     after = _errors(model, sur, 4096, seed=41)
     cal1 = model.calibrate(8192, seed=42, target=0.02)
     print(f"held-out MSE {before_loss[0]:.4g} -> {after_loss[0]:.4g}; "
-          f"Hs-tendency error {before['hs_tendency_err_mean']:.4g} -> "
-          f"{after['hs_tendency_err_mean']:.4g}; S rel L2 {before['s_rel_l2']:.4g} -> "
+          f"band Hs-tendency error {before['hs_band_err_mean']:.4g} -> "
+          f"{after['hs_band_err_mean']:.4g}; S rel L2 {before['s_rel_l2']:.4g} -> "
           f"{after['s_rel_l2']:.4g}; gate keeps {cal0['accepted']:.3f} -> {cal1['accepted']:.3f}")
     assert np.isfinite(losses).all()
     assert after_loss[0] < 0.2 * before_loss[0]
     assert after["s_rel_l2"] < 0.5 * before["s_rel_l2"]
-    assert after["hs_tendency_err_mean"] < 0.5 * before["hs_tendency_err_mean"]
+    assert after["hs_band_err_mean"] < 0.5 * before["hs_band_err_mean"]
     assert cal1["accepted"] > cal0["accepted"]
     assert cal1["mean_err_gated"] <= 0.02 + 1e-6

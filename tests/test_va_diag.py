@@ -31,7 +31,7 @@ rc, out, _, _ = pkg.ktp3_batch(case)            # the same call on the host-poin
 assert rc == 0
 rc, _, _, _ = pkg.ktp3_batch(case, igrid=5, va=va)   # resident: the device copy is now newer
 print("rc1", rc)
-print("poisoned", int(np.all(va.view(np.uint32) == 0x7FC0BAD0)))
+print("poisoned", int(np.all(va.view(np.uint32) == 0x7FC0FA11)))
 pkg.va_host_read(5, va)
 print("restored", int(np.array_equal(va.view(np.uint32), out.view(np.uint32))))
 va[1, 0] += 1.0                                  # a host change that no ww_va_host_write declares
@@ -67,4 +67,4 @@ def test_check_catches_an_undeclared_host_write():
 def test_count_report():
     vals, err = run_child("WW_KOKKOS_VA_COUNT")
     assert vals["rc1"] == "0" and vals["rc2"] == "0", (vals, err)
-    assert "VA host-to-device copies" in err and "VA device-to-host copies" in err, err
+    assert "[va] traffic:" in err and "whole uploads" in err and "whole downloads" in err, err

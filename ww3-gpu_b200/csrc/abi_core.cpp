@@ -4,7 +4,7 @@
 //
 // Reference behaviour kept: ww_kokkos_init picks the device from WW_KOKKOS_DEVICE_ID and
 // ignores the communicator (ww3-gpu kokkos/src/fortran_iface/ww_kokkos_c.hpp:52-73,
-// snl1_shim.cpp:128-144, 196-237); the flag rules are those of part_flags.cpp:1-135; the
+// snl1_shim.cpp:128-144, 196-237); the flag rules are those of part_flags.cpp (its behaviour, not its code); the
 // timer totals print at exit in the format of timers.cpp:37-43.
 #include <cuda_runtime.h>
 
@@ -13,8 +13,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "wwb_common.hpp"
 
@@ -52,56 +55,62 @@ int device_id_from_env() {
   return static_cast<int>(id);
 }
 
-// ---- run-time flags -------------------------------------------------------------------
-struct Preset {
-  const char* name;
-  const char* parts;
-};
-// The reference's one preset (kokkos/src/fortran_iface/presets.txt).
-constexpr Preset kPresets[] = {{"resident", "SRCE,XYP3,KTP3,OUTG,IOPE,UPDV,CPRT"}};
-constexpr Preset kUnknown{"", ""};
-// Parts that WW_KOKKOS_ALL does not turn on (part_flags.cpp:60-64).
-constexpr const char* kOptInOnly[] = {"WW_KOKKOS_XYP1", "WW_KOKKOS_KTP1", "WW_KOKKOS_XYP2",
-                                      "WW_KOKKOS_KTP2", "WW_KOKKOS_XYPUG", "WW_KOKKOS_XYP3",
-                                      "WW_KOKKOS_KTP3", "WW_KOKKOS_OUTG", "WW_KOKKOS_IOPE",
-                                      "WW_KOKKOS_UPDV", "WW_KOKKOS_CPRT",
-                                      "WW_KOKKOS_ST4_TABLES"};
+// ---- run-time switches ---------------------------------------------------------------------
+// The environment the WW3 fork's switch reads, resolved once per process: WW_KOKKOS_PRESET
+// (a named set of parts, the reference's presets.txt), WW_KOKKOS_ALL and WW_KOKKOS_STRICT.
+// A part's own variable WW_KOKKOS_<PART> is read at each ww_kokkos_flag call and wins over both.
+bool is_one(const char* v) { return v != nullptr && v[0] == '1' && v[1] == '\0'; }
 
-const Preset* preset() {
-  static const Preset* const p = []() -> const Preset* {
-    const char* v = std::getenv("WW_KOKKOS_PRESET");
-    if (v == nullptr || *v == '\0') return nullptr;
-    for (const Preset& q : kPresets)
-      if (std::strcmp(v, q.name) == 0) return &q;
-    return &kUnknown;
-  }();
-  return p;
-}
+struct Switches {
+  int preset = 0;                      // ww_kokkos_preset_status: 0 none, 1 known, -1 unknown
+  std::set<std::string> preset_parts;  // parts the preset turns on, without the prefix
+  bool all = false;
+  bool strict = false;
 
-bool in_list(const char* part, const char* list) {
-  const size_t n = std::strlen(part);
-  const char* s = list;
-  while (*s != '\0') {
-    const char* e = std::strchr(s, ',');
-    const size_t m = e ? static_cast<size_t>(e - s) : std::strlen(s);
-    if (m == n && std::strncmp(s, part, n) == 0) return true;
-    if (e == nullptr) break;
-    s = e + 1;
+  static const Switches& get() {
+    static const Switches s = [] {
+      // The presets of the reference (kokkos/src/fortran_iface/presets.txt), by name.
+      static const std::map<std::string, std::set<std::string>> known = {
+          {"resident", {"SRCE", "XYP3", "KTP3", "OUTG", "IOPE", "UPDV", "CPRT"}}};
+      Switches x;
+      const char* name = std::getenv("WW_KOKKOS_PRESET");
+      if (name != nullptr && name[0] != '\0') {
+        const auto it = known.find(name);
+        x.preset = it == known.end() ? -1 : 1;
+        if (it != known.end()) x.preset_parts = it->second;
+      }
+      x.all = is_one(std::getenv("WW_KOKKOS_ALL"));
+      x.strict = is_one(std::getenv("WW_KOKKOS_STRICT"));
+      return x;
+    }();
+    return s;
   }
-  return false;
+};
+
+/// Parts that only their own variable or a preset turns on: WW_KOKKOS_ALL leaves them off (the
+/// reference's opt-in parts, kokkos/src/fortran_iface/part_flags.cpp:83-87).
+bool opt_in_only(const std::string& part) {
+  static const std::set<std::string> parts = {"XYP1", "KTP1", "XYP2", "KTP2", "XYPUG", "XYP3",
+                                              "KTP3", "OUTG", "IOPE", "UPDV", "CPRT",
+                                              "ST4_TABLES"};
+  return parts.count(part) != 0;
 }
 
-constexpr int kMaxSlots = 64;
-char g_slot_name[kMaxSlots][25] = {};
-long long g_slot_count[kMaxSlots] = {};
-int g_nslots = 0;
-
-void print_fallbacks() {
-  std::fprintf(stderr, "ww_b200: calls left on the Fortran (WW_KOKKOS_STRICT=1 stops instead):");
-  for (int i = 0; i < g_nslots; ++i)
-    std::fprintf(stderr, " %s=%lld", g_slot_name[i], g_slot_count[i]);
-  std::fprintf(stderr, "\n");
-}
+/// Counters of calls a caller left on the Fortran, one per part, printed once at exit.
+struct FallbackTally {
+  static constexpr size_t kParts = 64;    // at most this many parts
+  static constexpr size_t kNameMax = 24;  // characters of a part name
+  std::vector<std::pair<std::string, long long>> parts;
+  static FallbackTally& get() {
+    static auto* t = new FallbackTally();
+    return *t;
+  }
+  static void print() {
+    std::string line = "ww_b200: Fortran fallbacks by part (WW_KOKKOS_STRICT=1 stops instead):";
+    for (const auto& [name, n] : get().parts) line += " " + name + "=" + std::to_string(n);
+    std::fprintf(stderr, "%s\n", line.c_str());
+  }
+};
 
 // ---- timers -----------------------------------------------------------------------------
 struct Total {
@@ -226,43 +235,36 @@ void ww_kokkos_finalize(void) {
 
 int ww_kokkos_flag(const char* name) {
   if (name == nullptr) return 0;
-  if (const char* v = std::getenv(name)) return std::strcmp(v, "1") == 0 ? 1 : 0;
-  constexpr const char kPrefix[] = "WW_KOKKOS_";
-  const wwb::Preset* p = wwb::preset();
-  if (p != nullptr && std::strncmp(name, kPrefix, sizeof kPrefix - 1) == 0 &&
-      wwb::in_list(name + sizeof kPrefix - 1, p->parts))
-    return 1;
-  for (const char* q : wwb::kOptInOnly)
-    if (std::strcmp(name, q) == 0) return 0;
-  const char* all = std::getenv("WW_KOKKOS_ALL");
-  return (all != nullptr && std::strcmp(all, "1") == 0) ? 2 : 0;
+  if (const char* own = std::getenv(name)) return wwb::is_one(own) ? 1 : 0;
+  const wwb::Switches& sw = wwb::Switches::get();
+  const std::string full(name), prefix("WW_KOKKOS_");
+  if (full.compare(0, prefix.size(), prefix) == 0) {
+    const std::string part = full.substr(prefix.size());
+    if (sw.preset_parts.count(part) != 0) return 1;
+    if (wwb::opt_in_only(part)) return 0;
+  }
+  return sw.all ? 2 : 0;
 }
 
-int ww_kokkos_preset_status(void) {
-  const wwb::Preset* p = wwb::preset();
-  return p == nullptr ? 0 : (p == &wwb::kUnknown ? -1 : 1);
-}
+int ww_kokkos_preset_status(void) { return wwb::Switches::get().preset; }
 
-int ww_kokkos_strict(void) {
-  static const int strict = [] {
-    const char* v = std::getenv("WW_KOKKOS_STRICT");
-    return (v != nullptr && std::strcmp(v, "1") == 0) ? 1 : 0;
-  }();
-  return strict;
-}
+int ww_kokkos_strict(void) { return wwb::Switches::get().strict ? 1 : 0; }
 
 int ww_kokkos_fallback_slot(const char* part) {
-  if (part == nullptr || std::strlen(part) >= sizeof wwb::g_slot_name[0]) return -1;
-  for (int i = 0; i < wwb::g_nslots; ++i)
-    if (std::strcmp(wwb::g_slot_name[i], part) == 0) return i;
-  if (wwb::g_nslots == wwb::kMaxSlots) return -1;
-  if (wwb::g_nslots == 0) std::atexit(wwb::print_fallbacks);
-  std::strcpy(wwb::g_slot_name[wwb::g_nslots], part);
-  return wwb::g_nslots++;
+  using wwb::FallbackTally;
+  if (part == nullptr || std::strlen(part) > FallbackTally::kNameMax) return -1;
+  auto& parts = FallbackTally::get().parts;
+  for (size_t i = 0; i < parts.size(); ++i)
+    if (parts[i].first == part) return static_cast<int>(i);
+  if (parts.size() == FallbackTally::kParts) return -1;
+  if (parts.empty()) std::atexit(FallbackTally::print);
+  parts.emplace_back(part, 0);
+  return static_cast<int>(parts.size() - 1);
 }
 
 void ww_kokkos_fallback_add(int slot) {
-  if (slot >= 0 && slot < wwb::g_nslots) ++wwb::g_slot_count[slot];
+  auto& parts = wwb::FallbackTally::get().parts;
+  if (slot >= 0 && static_cast<size_t>(slot) < parts.size()) ++parts[slot].second;
 }
 
 }  // extern "C"

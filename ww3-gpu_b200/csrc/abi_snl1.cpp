@@ -61,6 +61,7 @@ struct Slot {
 
 struct Ctx {
   Snl1Config cfg{};
+  int device = -1;  ///< the device current at ww_snl1_init: the tables live there
   std::vector<float> sig_host;
   Snl1Tables tab;
   Snl1Dev dev{};
@@ -188,6 +189,7 @@ int init_common(int igrid, const Snl1Config& cfg, const float* sig, Snl1Tables&&
     std::vector<float> h_sig(sig, sig + cfg.nk);
     c->sig.upload(h_sig.data(), h_sig.size());
     c->sig_host = h_sig;
+    WWB_CHECK(cudaGetDevice(&c->device));
     publish(*c);
     c->dev.sig = c->sig.ptr;
     for (auto& sl : c->slots) WWB_CHECK(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
@@ -386,6 +388,15 @@ void ww_snl1_noalloc(int igrid, int npts, const float* a, const float* cg, const
     const size_t nspec = c->cfg.nspec(), nk = c->cfg.nk, n = static_cast<size_t>(npts);
     auto seg = [](size_t floats) { return (floats + 63) & ~static_cast<size_t>(63); };  // 256 B
     auto need = [&](size_t m) { return 3 * seg(m * nspec) + seg(m * nk) + seg(m); };
+    // The static array is per device and picked by the current device; the grid's tables and
+    // stream belong to the device of its ww_snl1_init, so the two must be the same.
+    int current = -1;
+    WWB_CHECK(cudaGetDevice(&current));
+    if (current != c->device) {
+      g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE,
+                    "ww_snl1_noalloc: the current device is not the one this grid was set up on");
+      return;
+    }
     const Snl1StaticScratch sc = snl1_static_scratch();  // first call on a device: set-up
     if (need(n) > sc.floats) {
       size_t most = sc.floats / (3 * nspec + nk + 1);

@@ -215,7 +215,8 @@ void mlp_forward_infer(Mlp& m, int rows, cudaStream_t st, const bf16* x = nullpt
 /// forward with the training epilogues, loss and output gradient, backward, then AdamW when
 /// `apply`. `sg` carries the surrogate's loss terms (null: plain MSE).
 void mlp_train_step(Mlp& m, int rows, const float* t, int ldt, const SurGrid* sg,
-                    const LossWeights& lw, const Adam* adam, float* loss, cudaStream_t st) {
+                    const float* ps, const LossWeights& lw, const Adam* adam, float* loss,
+                    cudaStream_t st) {
   if (rows % 128 != 0 || rows > m.cap)
     throw CudaError(cudaErrorInvalidValue, "training batch must be a multiple of 128 within capacity");
   const int cap = m.cap;
@@ -248,8 +249,8 @@ void mlp_train_step(Mlp& m, int rows, const float* t, int ldt, const SurGrid* sg
   SurGrid plain{};
   plain.dout = m.dout;
   plain.nth = 1;
-  loss_grad(sg ? *sg : plain, lw, rows, m.nvalid, m.out.p, m.dout, t, ldt, m.g4.p, m.dout, loss,
-            st);
+  loss_grad(sg ? *sg : plain, lw, rows, m.nvalid, m.out.p, m.dout, t, ldt, sg ? ps : nullptr,
+            m.g4.p, m.dout, loss, st);
   transpose(m.g4.p, rows, m.dout, m.dout, m.g4t.p, cap, st);
   // Backward: layer l's input gradient G (rows x n_l) and its transpose GT (n_l x rows).
   const bf16* G = m.g4.p;
@@ -352,13 +353,13 @@ struct Sur {
   std::vector<float> sig;
   Mlp net;
   SurGrid g{};
-  DBuf<float> rowscale, omega;
-  // dataset: normalised inputs and targets
+  DBuf<float> rowscale;
+  // dataset: normalised inputs, targets and per-point scales (2 NK floats each)
   long long n_data = 0, n_train = 0;
   DBuf<bf16> xs;
-  DBuf<float> ts;
+  DBuf<float> ts, pss, tb_ps;
   // inference scratch (per chunk)
-  DBuf<float> scale;
+  DBuf<float> ps, gv;
   DBuf<int> shift, rej, nrej, nrej_total;
   GateParams gate{0.05f, 1e30f};
   LossWeights lw{0.0f, 0.0f, 1};
@@ -384,8 +385,9 @@ Sur* find_sur(int igrid) {
 
 void sur_scratch(Sur& s, int rows) {
   mlp_infer_alloc(s.net, rows);
-  if (s.scale.n < static_cast<size_t>(rows)) {
-    s.scale.alloc(rows);
+  if (s.shift.n < static_cast<size_t>(rows)) {
+    s.ps.alloc(static_cast<size_t>(rows) * 2 * s.g.nk);
+    s.gv.alloc(static_cast<size_t>(rows) * 2);
     s.shift.alloc(rows);
     s.rej.alloc(rows);
   }
@@ -408,11 +410,11 @@ void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* k
     const float* cp = cg + static_cast<size_t>(p0) * nk;
     float* sp = so + static_cast<size_t>(p0) * nspec;
     float* dp = dd + static_cast<size_t>(p0) * nspec;
-    prep(s.g, n, ap, cp, kd + p0, s.net.ix0.p, s.net.din, s.scale.p, s.shift.p, st);
+    prep(s.g, n, ap, cp, kd + p0, s.net.ix0.p, s.net.din, s.ps.p, s.shift.p, st);
     mlp_forward_infer(s.net, n, st);
     WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
-    post(s.g, gate, n, s.net.iout.p, s.net.dout, cp, s.scale.p, s.shift.p, sp, dp,
-         accepted ? accepted + p0 : nullptr, s.rej.p, s.nrej.p, s.nrej_total.p, st);
+    post(s.g, gate, n, s.net.iout.p, s.net.dout, s.ps.p, s.shift.p, sp, dp,
+         accepted ? accepted + p0 : nullptr, nullptr, s.rej.p, s.nrej.p, s.nrej_total.p, st);
     if (fallback &&
         !launch_snl1_list(s.dia, n, s.rej.p, s.nrej.p, ap, cp, kd + p0, sp, dp, nullptr, st))
       throw CudaError(cudaErrorInvalidValue, "gated DIA: the band kernel cannot run this grid");
@@ -460,18 +462,9 @@ void build_f64(Sur& s) {
   s.f64_ok = dia_f64_smem(f) <= 227 * 1024;
 }
 
-/// rowscale (and the Hs-tendency weights omega) from host values.
+/// The per-row target scales from host values.
 void set_rowscale(Sur& s, const std::vector<float>& rs) {
-  const int nk = s.cfg.nk;
-  std::vector<float> om(nk);
-  const double xfr = s.cfg.xfr, dth = s.cfg.dth;
-  for (int k = 0; k < nk; ++k) {
-    const double sig = s.sig[k];
-    const double dden = dth * 0.5 * sig * (xfr - 1.0 / xfr) * sig;
-    om[k] = static_cast<float>(rs[k] * dden / (2.0 * 3.141592653589793 * sig));
-  }
-  WWB_CHECK(cudaMemcpy(s.rowscale.p, rs.data(), nk * 4, cudaMemcpyHostToDevice));
-  WWB_CHECK(cudaMemcpy(s.omega.p, om.data(), nk * 4, cudaMemcpyHostToDevice));
+  WWB_CHECK(cudaMemcpy(s.rowscale.p, rs.data(), rs.size() * 4, cudaMemcpyHostToDevice));
 }
 
 int sur_fail(int code, const char* what) { return g_sur_status.fail(code, what); }
@@ -564,8 +557,8 @@ int ww_mlp_train_step(int handle, int rows, const void* x, const float* t, int l
     for (Layer& L : m.L) L.g.zero(m.st);
     Adam h{};
     if (apply) h = adam_at(++m.step, lr, wd);
-    mlp_train_step(m, rows, t, ldt, nullptr, LossWeights{0.0f, 0.0f, 0}, apply ? &h : nullptr,
-                   m.loss.p, m.st);
+    mlp_train_step(m, rows, t, ldt, nullptr, nullptr, LossWeights{0.0f, 0.0f, 0},
+                   apply ? &h : nullptr, m.loss.p, m.st);
     if (loss3) WWB_CHECK(cudaMemcpyAsync(loss3, m.loss.p, 12, cudaMemcpyDeviceToHost, m.st));
     if (take_err(m)) return g_mlp_status.fail(WW_KOKKOS_ERR_KERNEL, "ww_mlp_train_step: a GEMM wait gave up");
     g_mlp_status.ok();
@@ -669,7 +662,6 @@ int ww_sur_init(int igrid, int nhidden, unsigned long long seed) {
     const int dout = (nspec + 1 + 63) / 64 * 64;  // + the error head
     mlp_alloc(s->net, din, nhidden, dout, nspec, 8192, seed);
     s->rowscale.alloc(nk);
-    s->omega.alloc(nk);
     set_rowscale(*s, std::vector<float>(nk, 1.0f));
     SurGrid& g = s->g;
     g.nk = nk;
@@ -679,7 +671,6 @@ int ww_sur_init(int igrid, int nhidden, unsigned long long seed) {
     g.dout = dout;
     g.sig = s->dia.sig;
     g.rowscale = s->rowscale.p;
-    g.omega = s->omega.p;
     g.snlc1 = s->cfg.snlc1;
     g.kdcon = s->cfg.kdcon;
     g.kdmn = s->cfg.kdmn;
@@ -723,24 +714,25 @@ int ww_sur_dataset(int igrid, long long npts, long long holdout, unsigned long l
     const int nspec = s->g.nspec, nk = s->g.nk, din = s->net.din;
     cudaStream_t st = s->net.st;
     constexpr int kChunk = 65536;
-    DBuf<float> a, cg, kd, so, dd, sc;
+    DBuf<float> a, cg, kd, so, dd;
     DBuf<int> sh;
     a.alloc(static_cast<size_t>(kChunk) * nspec);
     cg.alloc(static_cast<size_t>(kChunk) * nk);
     kd.alloc(kChunk);
     so.alloc(static_cast<size_t>(kChunk) * nspec);
     dd.alloc(static_cast<size_t>(kChunk) * nspec);
-    sc.alloc(kChunk);
     sh.alloc(kChunk);
     s->xs.alloc(static_cast<size_t>(npts) * din);
     s->ts.alloc(static_cast<size_t>(npts) * nspec);
+    s->pss.alloc(static_cast<size_t>(npts) * 2 * nk);
     const SynthDraw draw{seed, bimodal, dmin, dmax};
     for (long long p0 = 0; p0 < npts; p0 += kChunk) {
       const int n = static_cast<int>(std::min<long long>(kChunk, npts - p0));
       synth(s->g, draw, p0, n, a.p, cg.p, kd.p, st);
       launch_snl1(snl1_band_ok(s->dia) ? kSnl1Band : kSnl1Gather, s->dia, n, a.p, cg.p, kd.p,
                   so.p, dd.p, st);
-      prep(s->g, n, a.p, cg.p, kd.p, s->xs.p + static_cast<size_t>(p0) * din, din, sc.p, sh.p, st);
+      float* const psc = s->pss.p + static_cast<size_t>(p0) * 2 * nk;
+      prep(s->g, n, a.p, cg.p, kd.p, s->xs.p + static_cast<size_t>(p0) * din, din, psc, sh.p, st);
       if (p0 == 0) {  // the target scale per frequency row, from the first chunk
         DBuf<double> acc;
         DBuf<unsigned long long> cnt;
@@ -748,7 +740,7 @@ int ww_sur_dataset(int igrid, long long npts, long long holdout, unsigned long l
         cnt.alloc(1);
         acc.zero(st);
         cnt.zero(st);
-        rowscale_acc(s->g, n, so.p, cg.p, sc.p, sh.p, acc.p, cnt.p, st);
+        rowscale_acc(s->g, n, so.p, psc, acc.p, cnt.p, st);
         std::vector<double> h(nk);
         unsigned long long c = 0;
         WWB_CHECK(cudaMemcpyAsync(h.data(), acc.p, nk * 8, cudaMemcpyDeviceToHost, st));
@@ -765,7 +757,7 @@ int ww_sur_dataset(int igrid, long long npts, long long holdout, unsigned long l
           if (!(rs[k] > 1e-6 * mx)) rs[k] = static_cast<float>(mx > 0 ? 1e-6 * mx : 1.0);
         set_rowscale(*s, rs);
       }
-      targets(s->g, n, so.p, cg.p, sc.p, sh.p, s->ts.p + static_cast<size_t>(p0) * nspec, nspec, st);
+      targets(s->g, n, so.p, psc, sh.p, s->ts.p + static_cast<size_t>(p0) * nspec, nspec, st);
     }
     WWB_CHECK(cudaStreamSynchronize(st));
     if (snl1_take_error() != 0) return sur_fail(WW_KOKKOS_ERR_KERNEL, "ww_sur_dataset: a DIA wait gave up");
@@ -801,6 +793,7 @@ int ww_sur_train(int igrid, int steps, int batch, float lr, float lr_end, float 
     cudaStream_t st = m.st;
     if (!s->ts.p) return sur_fail(WW_KOKKOS_ERR_NOT_INITIALISED, "ww_sur_train: no dataset");
     m.tb.alloc(static_cast<size_t>(m.cap) * s->g.nspec);
+    s->tb_ps.alloc(static_cast<size_t>(m.cap) * 2 * s->g.nk);
     DBuf<float> hist;
     hist.alloc(static_cast<size_t>(std::max(steps, 1)) * 3);
     hist.zero(st);
@@ -814,10 +807,10 @@ int ww_sur_train(int igrid, int steps, int batch, float lr, float lr_end, float 
         rate = lr_end + 0.5 * (lr - lr_end) * (1.0 + std::cos(3.141592653589793 * f));
       }
       const uint64_t draw = (seed ^ 0x5DEECE66Dull) * 6364136223846793005ull + static_cast<uint64_t>(i) + 1;
-      gather_batch(batch, s->n_train, draw | 1ull, 0, s->xs.p, m.din, s->ts.p, s->g.nspec, m.x0.p,
-                   m.tb.p, st);
+      gather_batch(batch, s->n_train, draw | 1ull, 0, s->xs.p, m.din, s->ts.p, s->g.nspec,
+                   s->pss.p, 2 * s->g.nk, m.x0.p, m.tb.p, s->tb_ps.p, st);
       const Adam h = adam_at(++m.step, static_cast<float>(rate), wd);
-      mlp_train_step(m, batch, m.tb.p, s->g.nspec, &s->g, s->lw, &h,
+      mlp_train_step(m, batch, m.tb.p, s->g.nspec, &s->g, s->tb_ps.p, s->lw, &h,
                      hist.p + static_cast<size_t>(i) * 3, st);
     }
     if (losses && steps > 0)
@@ -853,8 +846,8 @@ int ww_sur_eval(int igrid, long long p0, int npts, float* loss3) {
       gs.alloc(static_cast<size_t>(n) * m.dout);
       LossWeights lw = s->lw;
       loss_grad(s->g, lw, n, s->g.nspec, m.iout.p, m.dout,
-                s->ts.p + static_cast<size_t>(p0 + q) * s->g.nspec, s->g.nspec, gs.p, m.dout,
-                acc.p, st);
+                s->ts.p + static_cast<size_t>(p0 + q) * s->g.nspec, s->g.nspec,
+                s->pss.p + static_cast<size_t>(p0 + q) * 2 * s->g.nk, gs.p, m.dout, acc.p, st);
       float h[3];
       WWB_CHECK(cudaMemcpyAsync(h, acc.p, 12, cudaMemcpyDeviceToHost, st));
       WWB_CHECK(cudaStreamSynchronize(st));
@@ -990,42 +983,36 @@ int ww_sur_calibrate(int igrid, int npts, unsigned long long seed, float bimodal
       const int n = std::min(kInferRows, npts - p0);
       sur_scratch(*s, n);
       prep(s->g, n, a.p + static_cast<size_t>(p0) * nspec, cg.p + static_cast<size_t>(p0) * nk,
-           kd.p + p0, s->net.ix0.p, s->net.din, s->scale.p, s->shift.p, st);
+           kd.p + p0, s->net.ix0.p, s->net.din, s->ps.p, s->shift.p, st);
       mlp_forward_infer(s->net, n, st);
       WWB_CHECK(cudaMemsetAsync(s->nrej.p, 0, sizeof(int), st));
-      post(s->g, open, n, s->net.iout.p, s->net.dout, cg.p + static_cast<size_t>(p0) * nk,
-           s->scale.p, s->shift.p, so.p + static_cast<size_t>(p0) * nspec,
-           dd.p + static_cast<size_t>(p0) * nspec, nullptr, s->rej.p, s->nrej.p, nullptr, st);
+      post(s->g, open, n, s->net.iout.p, s->net.dout, s->ps.p, s->shift.p,
+           so.p + static_cast<size_t>(p0) * nspec, dd.p + static_cast<size_t>(p0) * nspec,
+           nullptr, s->gv.p, s->rej.p, s->nrej.p, nullptr, st);
       // The gate's two inputs per point: the head (column NSPEC) and the energy residual.
-      std::vector<float> rows(static_cast<size_t>(n) * s->net.dout);
-      WWB_CHECK(cudaMemcpyAsync(rows.data(), s->net.iout.p, rows.size() * 4, cudaMemcpyDeviceToHost, st));
-      std::vector<float> om(nk);
-      WWB_CHECK(cudaMemcpyAsync(om.data(), s->omega.p, nk * 4, cudaMemcpyDeviceToHost, st));
+      std::vector<float> gv(static_cast<size_t>(n) * 2);
+      WWB_CHECK(cudaMemcpyAsync(gv.data(), s->gv.p, gv.size() * 4, cudaMemcpyDeviceToHost, st));
       WWB_CHECK(cudaStreamSynchronize(st));
       for (int i = 0; i < n; ++i) {
-        const float* r = rows.data() + static_cast<size_t>(i) * s->net.dout;
-        double num = 0, den = 0;
-        for (int j = 0; j < nspec; ++j) {
-          num += om[j / s->g.nth] * r[j];
-          den += om[j / s->g.nth] * std::fabs(r[j]);
-        }
-        head[p0 + i] = r[nspec];
-        res[p0 + i] = den > 0 ? static_cast<float>(std::fabs(num) / den) : 1e30f;
+        head[p0 + i] = gv[2 * i];
+        res[p0 + i] = gv[2 * i + 1];
       }
     }
     dia_f64_judge(s->f64, npts, a.p, cg.p, kd.p, so.p, stats.p, nullptr, nullptr, st);
     WWB_CHECK(cudaMemcpyAsync(st_h.data(), stats.p, st_h.size() * 8, cudaMemcpyDeviceToHost, st));
     WWB_CHECK(cudaStreamSynchronize(st));
     // Points the energy test passes, in order of predicted error; accept the longest prefix
-    // whose summed Hs-tendency error stays within target_err per point of the whole set (a
-    // rejected point is computed by the plain DIA, whose error is counted as zero).
+    // whose summed band Hs-tendency error stays within target_err per point of the whole set
+    // (a rejected point is computed by the plain DIA, whose error is counted as zero).
     std::vector<int> order;
     for (int i = 0; i < npts; ++i)
       if (res[i] <= energy) order.push_back(i);
     std::sort(order.begin(), order.end(), [&](int x, int y) { return head[x] < head[y]; });
+    // The error of a point: the band-resolved Hs-tendency error, sum over frequency bands of
+    // |band tendency - FP64 band tendency| over sum of |FP64 band tendency|.
     auto err_of = [&](int i) {
       const double* o = st_h.data() + static_cast<size_t>(i) * 10;
-      return o[3] > 0 ? std::fabs(o[2] - o[1]) / o[3] : 0.0;
+      return o[5] > 0 ? o[4] / o[5] : 0.0;
     };
     double sum = 0;
     int take = 0;

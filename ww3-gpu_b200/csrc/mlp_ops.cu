@@ -170,9 +170,25 @@ __global__ void synth_kernel(SurGrid g, SynthDraw dr, long long p0, int npts, fl
 
 // ------------------------------------------------------------------------- input normalisation
 
+/// The original direction of canonical column j: the spectrum is rotated by `sh` and, when
+/// bit 16 of the packed shift is set, reflected (j -> -j), so column 0 is its dominant
+/// direction and columns 1..NTH/2-1 its heavier side. The DIA commutes with both (its index
+/// tables are circulant in direction and symmetric under reflection).
+__device__ __forceinline__ int orig_col(int packed, int j, int nth) {
+  const int sh = packed & 0xFFFF;
+  int c = (packed >> 16) ? sh - j : sh + j;
+  c %= nth;
+  return c < 0 ? c + nth : c;
+}
+
+/// ln of the quadrature weight DDEN(k) = DTH * DSII(k) * SIG(k), DSII = SIG (XFR - 1/XFR) / 2.
+__device__ __forceinline__ float ln_dden(const SurGrid& g, float sig) {
+  return logf(g.dth * 0.5f * sig * (g.xfr - 1.0f / g.xfr) * sig);
+}
+
 __global__ void prep_kernel(SurGrid g, int npts, const float* __restrict__ a,
                             const float* __restrict__ cg, const float* __restrict__ kdm,
-                            __nv_bfloat16* __restrict__ x, int ldx, float* __restrict__ scale,
+                            __nv_bfloat16* __restrict__ x, int ldx, float* __restrict__ ps,
                             int* __restrict__ shift) {
   extern __shared__ float sm[];
   const int ip = blockIdx.x, tid = threadIdx.x;
@@ -180,9 +196,13 @@ __global__ void prep_kernel(SurGrid g, int npts, const float* __restrict__ a,
   float* const ue = sm;                 // nspec
   float* const conx = ue + nspec;       // nk
   float* const dsum = conx + nk;        // nth
-  float* const red = dsum + nth;        // 32
+  float* const rmax = dsum + nth;       // nk: largest UE of each row
+  float* const lw = rmax + nk;          // nk: ln of each row's Hs-tendency weight
+  float* const red = lw + nk;           // 32
   __shared__ int s_shift;
+  __shared__ float s_cons;
   const float* ap = a + static_cast<size_t>(ip) * nspec;
+  float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
   for (int k = tid; k < nk; k += blockDim.x)
     conx[k] = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
   __syncthreads();
@@ -198,30 +218,61 @@ __global__ void prep_kernel(SurGrid g, int npts, const float* __restrict__ a,
     for (int k = 0; k < nk; ++k) s += ue[k * nth + t];
     dsum[t] = s;
   }
+  for (int k = tid; k < nk; k += blockDim.x) {
+    float m = 0.0f;
+    for (int t = 0; t < nth; ++t) m = fmaxf(m, ue[k * nth + t]);
+    rmax[k] = m;
+  }
+  if (tid == 0) s_cons = cons_of(g, __ldg(kdm + ip));
+  __syncthreads();
+  // Per row: the largest cubic term ln(AF11 u^3) of the row (u its largest UE) ...
+  for (int k = tid; k < nk; k += blockDim.x)
+    lw[k] = 3.0f * logf(fmaxf(rmax[k], fmaxf(umax * 1e-12f, 1e-30f))) +
+            11.0f * logf(__ldg(g.sig + k) * kTpiInvF);
+  __syncthreads();
+  // ... and lambda(k) = ln CONS + ln CONX(k) + the largest such term within kReach rows of k
+  // (the rows whose quadruplets reach row k), so S(k, .) e^-lambda is of order one; then the
+  // row's weight in the Hs tendency.
+  constexpr int kReach = 5;
+  for (int k = tid; k < nk; k += blockDim.x) {
+    float l = -INFINITY;
+    for (int q = max(0, k - kReach); q <= min(nk - 1, k + kReach); ++q) l = fmaxf(l, lw[q]);
+    pp[k] = umax > 0.0f ? logf(s_cons) + logf(conx[k]) + l : -1e30f;
+  }
+  __syncthreads();
+  for (int k = tid; k < nk; k += blockDim.x)
+    lw[k] = pp[k] + ln_dden(g, __ldg(g.sig + k)) - logf(__ldg(cg + static_cast<size_t>(ip) * nk + k));
   __syncthreads();
   if (tid == 0) {
     int best = 0;
     for (int t = 1; t < nth; ++t)
       if (dsum[t] > dsum[best]) best = t;
-    s_shift = best;
-    const float kd = __ldg(kdm + ip);
-    const float c = cons_of(g, kd);
-    scale[ip] = c * umax * umax * umax;
-    shift[ip] = best;
+    float up = 0.0f, lo = 0.0f;
+    for (int j = 1; j < (nth + 1) / 2; ++j) {
+      up += dsum[(best + j) % nth];
+      lo += dsum[(best + nth - j) % nth];
+    }
+    const int packed = best | (lo > up ? 1 << 16 : 0);
+    s_shift = packed;
+    shift[ip] = packed;
+    float lmax = -INFINITY;
+    for (int k = 0; k < nk; ++k) lmax = fmaxf(lmax, lw[k]);
+    red[0] = lmax;
     // Depth features: ln kdmean and the relative depth factor of CONS.
+    const float kd = __ldg(kdm + ip);
     __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
     if (g.din > nspec) xr[nspec] = __float2bfloat16_rn(logf(fmaxf(kd, 1e-2f)) * 0.2f);
-    if (g.din > nspec + 1) xr[nspec + 1] = __float2bfloat16_rn(c / g.snlc1 - 1.0f);
+    if (g.din > nspec + 1) xr[nspec + 1] = __float2bfloat16_rn(s_cons / g.snlc1 - 1.0f);
   }
   __syncthreads();
+  for (int k = tid; k < nk; k += blockDim.x)
+    pp[nk + k] = umax > 0.0f ? expf(lw[k] - red[0]) : 0.0f;
   const int sh = s_shift;
   const float inv = umax > 0.0f ? 1.0f / umax : 0.0f;
   __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
   for (int i = tid; i < nspec; i += blockDim.x) {
     const int k = i / nth, j = i % nth;
-    int jj = j + sh;
-    if (jj >= nth) jj -= nth;
-    const float u = ue[k * nth + jj] * inv;
+    const float u = ue[k * nth + orig_col(sh, j, nth)] * inv;
     xr[i] = __float2bfloat16_rn(logf(u + kInputFloor) * kInputScale + 1.0f);
   }
   for (int i = nspec + 2 + tid; i < g.din; i += blockDim.x) xr[i] = __float2bfloat16_rn(0.0f);
@@ -230,21 +281,18 @@ __global__ void prep_kernel(SurGrid g, int npts, const float* __restrict__ a,
 // ------------------------------------------------------------------------------ target side
 
 __global__ void rowscale_kernel(SurGrid g, int npts, const float* __restrict__ s,
-                                const float* __restrict__ cg, const float* __restrict__ scale,
-                                const int* __restrict__ shift, double* acc,
+                                const float* __restrict__ ps, double* acc,
                                 unsigned long long* cnt) {
   __shared__ double rs[64];
   const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth;
-  const float sc = scale[ip];
-  (void)shift;
-  if (!(sc > 0.0f)) return;
+  const float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
+  if (!(pp[0] > -1e29f)) return;  // an empty spectrum
   for (int k = tid; k < nk; k += blockDim.x) rs[k] = 0.0;
   __syncthreads();
   const float* sp = s + static_cast<size_t>(ip) * g.nspec;
   for (int i = tid; i < g.nspec; i += blockDim.x) {
     const int k = i / nth;
-    const float conx = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
-    const double v = static_cast<double>(sp[i]) / (static_cast<double>(sc) * conx);
+    const double v = static_cast<double>(sp[i]) * exp(-static_cast<double>(pp[k]));
     atomicAdd(&rs[k], v * v);
   }
   __syncthreads();
@@ -253,65 +301,70 @@ __global__ void rowscale_kernel(SurGrid g, int npts, const float* __restrict__ s
 }
 
 __global__ void targets_kernel(SurGrid g, int npts, const float* __restrict__ s,
-                               const float* __restrict__ cg, const float* __restrict__ scale,
-                               const int* __restrict__ shift, float* __restrict__ t, int ldt) {
+                               const float* __restrict__ ps, const int* __restrict__ shift,
+                               float* __restrict__ t, int ldt) {
   const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth;
-  const float sc = scale[ip];
+  const float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
   const int sh = shift[ip];
   const float* sp = s + static_cast<size_t>(ip) * g.nspec;
   float* tp = t + static_cast<size_t>(ip) * ldt;
   for (int i = tid; i < g.nspec; i += blockDim.x) {
     const int k = i / nth, j = i % nth;
-    int jj = j + sh;
-    if (jj >= nth) jj -= nth;
-    const float conx = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
-    const float den = sc * conx * __ldg(g.rowscale + k);
-    tp[i] = den > 0.0f ? sp[k * nth + jj] / den : 0.0f;
+    const double den = exp(static_cast<double>(pp[k])) * __ldg(g.rowscale + k);
+    tp[i] = den > 0.0 ? static_cast<float>(static_cast<double>(sp[k * nth + orig_col(sh, j, nth)]) / den)
+                      : 0.0f;
   }
 }
 
 // ------------------------------------------------------------------------ inference output side
 
 __global__ void post_kernel(SurGrid g, GateParams gate, int npts, const float* __restrict__ out,
-                            int ldo, const float* __restrict__ cg, const float* __restrict__ scale,
-                            const int* __restrict__ shift, float* __restrict__ s,
-                            float* __restrict__ d, int* __restrict__ accepted,
+                            int ldo, const float* __restrict__ ps, const int* __restrict__ shift,
+                            float* __restrict__ s, float* __restrict__ d,
+                            int* __restrict__ accepted, float* __restrict__ gv,
                             int* __restrict__ rej_list, int* __restrict__ nrej,
                             int* __restrict__ nrej_total) {
   __shared__ float red[32];
-  __shared__ float conx[64];
+  __shared__ float scl[64], wgt[64];
   const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth, nspec = g.nspec;
   const float* op = out + static_cast<size_t>(ip) * ldo;
-  for (int k = tid; k < nk; k += blockDim.x)
-    conx[k] = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
+  const float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
+  for (int k = tid; k < nk; k += blockDim.x) {
+    const float rsk = __ldg(g.rowscale + k);
+    scl[k] = rsk * expf(pp[k]);
+    wgt[k] = rsk * pp[nk + k];
+  }
+  __syncthreads();
   float r = 0.0f, gs = 0.0f;
   for (int i = tid; i < nspec; i += blockDim.x) {
-    const float w = __ldg(g.omega + i / nth), v = op[i];
+    const float w = wgt[i / nth], v = op[i];
     r += w * v;
     gs += w * fabsf(v);
   }
   r = block_sum(r, red);
   gs = block_sum(gs, red);
   const float head = g.dout > nspec ? op[nspec] : -INFINITY;
-  const bool ok = isfinite(r) && isfinite(gs) && fabsf(r) <= gate.energy * gs &&
+  const float resid = gs > 0.0f ? fabsf(r) / gs : 0.0f;
+  const bool ok = isfinite(r) && isfinite(gs) && isfinite(head) && resid <= gate.energy &&
                   head <= gate.log_err;
   if (tid == 0) {
     if (accepted) accepted[ip] = ok ? 1 : 0;
+    if (gv) {
+      gv[2 * ip] = head;
+      gv[2 * ip + 1] = resid;
+    }
     if (!ok) {
       rej_list[atomicAdd(nrej, 1)] = ip;
       if (nrej_total) atomicAdd(nrej_total, 1);
     }
   }
   if (!ok) return;  // the plain DIA writes this point's S and D
-  const float sc = scale[ip];
   const int sh = shift[ip];
   float* sp = s + static_cast<size_t>(ip) * nspec;
   float* dp = d + static_cast<size_t>(ip) * nspec;
   for (int i = tid; i < nspec; i += blockDim.x) {
     const int k = i / nth, j = i % nth;
-    int jj = j + sh;
-    if (jj >= nth) jj -= nth;
-    sp[k * nth + jj] = op[i] * __ldg(g.rowscale + k) * sc * conx[k];
+    sp[k * nth + orig_col(sh, j, nth)] = op[i] * scl[k];
     dp[i] = 0.0f;
   }
 }
@@ -320,42 +373,63 @@ __global__ void post_kernel(SurGrid g, GateParams gate, int npts, const float* _
 
 __global__ void loss_kernel(SurGrid g, LossWeights lw, int m, int nvalid,
                             const float* __restrict__ out, int ldo, const float* __restrict__ t,
-                            int ldt, __nv_bfloat16* __restrict__ grad, int ldg,
-                            float* __restrict__ loss) {
+                            int ldt, const float* __restrict__ ps, __nv_bfloat16* __restrict__ grad,
+                            int ldg, float* __restrict__ loss) {
   __shared__ float red[32];
-  const int ip = blockIdx.x, tid = threadIdx.x;
+  __shared__ float wgt[64], dband[64], tband[64];
+  const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk;
   const float* op = out + static_cast<size_t>(ip) * ldo;
   const float* tp = t + static_cast<size_t>(ip) * ldt;
-  const bool energy = lw.mu > 0.0f && g.omega != nullptr;
-  float r = 0.0f, gs = 0.0f, se = 0.0f;
+  // The band terms need rows of NTH bins: the surrogate's targets (nvalid == NSPEC).
+  const bool energy = ps != nullptr && nvalid == g.nspec && nk <= 64;
+  if (energy) {
+    const float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
+    for (int k = tid; k < nk; k += blockDim.x) {
+      wgt[k] = __ldg(g.rowscale + k) * pp[nk + k];
+      dband[k] = 0.0f;
+      tband[k] = 0.0f;
+    }
+    __syncthreads();
+  }
+  float se = 0.0f;
   for (int i = tid; i < nvalid; i += blockDim.x) {
     const float dv = op[i] - tp[i];
     se += dv * dv;
     if (energy) {
-      const float w = __ldg(g.omega + i / g.nth);
-      r += w * dv;
-      gs += w * fabsf(tp[i]);
+      const int k = i / g.nth;
+      atomicAdd(&dband[k], wgt[k] * dv);
+      atomicAdd(&tband[k], wgt[k] * tp[i]);
     }
   }
   se = block_sum(se, red);
+  // Per frequency band k: the error of the band's Hs (energy) tendency d(k) and the tendency
+  // t(k); the band error is sum |d| / sum |t|, the loss term sum d^2 / (sum |t|)^2.
+  float den = 0.0f, num = 0.0f, sq = 0.0f;
   if (energy) {
-    r = block_sum(r, red);
-    gs = block_sum(gs, red);
+    __syncthreads();
+    for (int k = 0; k < nk; ++k) {
+      den += fabsf(tband[k]);
+      num += fabsf(dband[k]);
+      sq += dband[k] * dband[k];
+    }
   }
-  const bool have_e = energy && gs > 1e-30f;
-  const float rel = have_e ? r / gs : 0.0f;
+  const bool have_e = energy && den > 1e-30f;
+  const float band_err = have_e ? num / den : 0.0f;
   const float inv_m = 1.0f / static_cast<float>(m);
   const float c_mse = 2.0f * inv_m / static_cast<float>(nvalid);
-  const float c_e = have_e ? lw.mu * 2.0f * rel / gs * inv_m : 0.0f;
+  const float c_e = have_e ? lw.mu * 2.0f / (den * den) * inv_m : 0.0f;
   const bool head = lw.head && g.dout > nvalid;
-  const float target_h = logf(fabsf(rel) + 1e-4f);
+  const float target_h = logf(band_err + 1e-3f);
   __nv_bfloat16* gp = grad + static_cast<size_t>(ip) * ldg;
   const int width = g.dout;
   for (int i = tid; i < width; i += blockDim.x) {
     float v = 0.0f;
     if (i < nvalid) {
       v = c_mse * (op[i] - tp[i]);
-      if (have_e) v += c_e * __ldg(g.omega + i / g.nth);
+      if (have_e) {
+        const int k = i / g.nth;
+        v += c_e * dband[k] * wgt[k];
+      }
     } else if (head && i == nvalid) {
       v = lw.lambda * 2.0f * (op[i] - target_h) * inv_m;
     }
@@ -363,7 +437,7 @@ __global__ void loss_kernel(SurGrid g, LossWeights lw, int m, int nvalid,
   }
   if (tid == 0) {
     atomicAdd(loss + 0, se * inv_m / static_cast<float>(nvalid));
-    if (have_e) atomicAdd(loss + 1, lw.mu * rel * rel * inv_m);
+    if (have_e) atomicAdd(loss + 1, lw.mu * sq / (den * den) * inv_m);
     if (head) {
       const float h = op[nvalid] - target_h;
       atomicAdd(loss + 2, lw.lambda * h * h * inv_m);
@@ -373,8 +447,9 @@ __global__ void loss_kernel(SurGrid g, LossWeights lw, int m, int nvalid,
 
 __global__ void gather_kernel(int m, long long n, uint64_t seed, long long offset,
                               const __nv_bfloat16* __restrict__ xs, int ldx,
-                              const float* __restrict__ ts, int ldt, __nv_bfloat16* __restrict__ xb,
-                              float* __restrict__ tb) {
+                              const float* __restrict__ ts, int ldt, const float* __restrict__ pss,
+                              int ldp, __nv_bfloat16* __restrict__ xb, float* __restrict__ tb,
+                              float* __restrict__ psb) {
   const int r = blockIdx.x;
   if (r >= m) return;
   long long src = offset + r;
@@ -385,6 +460,7 @@ __global__ void gather_kernel(int m, long long n, uint64_t seed, long long offse
   const float4* tsrc = reinterpret_cast<const float4*>(ts + src * ldt);
   float4* tdst = reinterpret_cast<float4*>(tb + static_cast<size_t>(r) * ldt);
   for (int i = threadIdx.x; i < ldt / 4; i += blockDim.x) tdst[i] = __ldg(tsrc + i);
+  for (int i = threadIdx.x; i < ldp; i += blockDim.x) psb[static_cast<size_t>(r) * ldp + i] = pss[src * ldp + i];
 }
 
 __global__ void transpose_kernel(const __nv_bfloat16* __restrict__ src, int rows, int cols,
@@ -629,52 +705,56 @@ void synth(const SurGrid& g, const SynthDraw& d, long long p0, int npts, float* 
 }
 
 void prep(const SurGrid& g, int npts, const float* a, const float* cg, const float* kdmean,
-          __nv_bfloat16* x, int ldx, float* scale, int* shift, cudaStream_t st) {
+          __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st) {
   if (npts <= 0) return;
-  const size_t smem = (static_cast<size_t>(g.nspec) + g.nk + g.nth + 32) * sizeof(float);
-  prep_kernel<<<grid1(npts), kThreads, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, scale, shift);
+  if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "prep: NK above 64");
+  const size_t smem = (static_cast<size_t>(g.nspec) + 3 * g.nk + g.nth + 32) * sizeof(float);
+  prep_kernel<<<grid1(npts), kThreads, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, ps, shift);
   WWB_CHECK(cudaGetLastError());
 }
 
-void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
-                  const int* shift, double* acc, unsigned long long* cnt, cudaStream_t st) {
+void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* ps, double* acc,
+                  unsigned long long* cnt, cudaStream_t st) {
   if (npts <= 0) return;
   if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "rowscale: NK above 64");
-  rowscale_kernel<<<grid1(npts), kThreads, 0, st>>>(g, npts, s, cg, scale, shift, acc, cnt);
+  rowscale_kernel<<<grid1(npts), kThreads, 0, st>>>(g, npts, s, ps, acc, cnt);
   WWB_CHECK(cudaGetLastError());
 }
 
-void targets(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
-             const int* shift, float* t, int ldt, cudaStream_t st) {
+void targets(const SurGrid& g, int npts, const float* s, const float* ps, const int* shift,
+             float* t, int ldt, cudaStream_t st) {
   if (npts <= 0) return;
-  targets_kernel<<<grid1(npts), kThreads, 0, st>>>(g, npts, s, cg, scale, shift, t, ldt);
+  targets_kernel<<<grid1(npts), kThreads, 0, st>>>(g, npts, s, ps, shift, t, ldt);
   WWB_CHECK(cudaGetLastError());
 }
 
 void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, int ldo,
-          const float* cg, const float* scale, const int* shift, float* s, float* d,
-          int* accepted, int* rej_list, int* nrej, int* nrej_total, cudaStream_t st) {
+          const float* ps, const int* shift, float* s, float* d, int* accepted, float* gv,
+          int* rej_list, int* nrej, int* nrej_total, cudaStream_t st) {
   if (npts <= 0) return;
   if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "post: NK above 64");
-  post_kernel<<<grid1(npts), kThreads, 0, st>>>(g, gate, npts, out, ldo, cg, scale, shift, s, d,
-                                                 accepted, rej_list, nrej, nrej_total);
+  post_kernel<<<grid1(npts), kThreads, 0, st>>>(g, gate, npts, out, ldo, ps, shift, s, d,
+                                                 accepted, gv, rej_list, nrej, nrej_total);
   WWB_CHECK(cudaGetLastError());
 }
 
 void loss_grad(const SurGrid& g, const LossWeights& w, int m, int nvalid, const float* out,
-               int ldo, const float* t, int ldt, __nv_bfloat16* grad, int ldg, float* loss,
-               cudaStream_t st) {
+               int ldo, const float* t, int ldt, const float* ps, __nv_bfloat16* grad, int ldg,
+               float* loss, cudaStream_t st) {
   if (m <= 0) return;
-  loss_kernel<<<grid1(m), kThreads, 0, st>>>(g, w, m, nvalid, out, ldo, t, ldt, grad, ldg, loss);
+  if (ps != nullptr && g.nk > 64) throw CudaError(cudaErrorInvalidValue, "loss: NK above 64");
+  loss_kernel<<<grid1(m), kThreads, 0, st>>>(g, w, m, nvalid, out, ldo, t, ldt, ps, grad, ldg,
+                                             loss);
   WWB_CHECK(cudaGetLastError());
 }
 
 void gather_batch(int m, long long n, uint64_t seed, long long offset, const __nv_bfloat16* xs,
-                  int ldx, const float* ts, int ldt, __nv_bfloat16* xb, float* tb,
-                  cudaStream_t st) {
+                  int ldx, const float* ts, int ldt, const float* pss, int ldp,
+                  __nv_bfloat16* xb, float* tb, float* psb, cudaStream_t st) {
   if (m <= 0) return;
   if (ldx % 8 || ldt % 4) throw CudaError(cudaErrorInvalidValue, "gather: unaligned rows");
-  gather_kernel<<<grid1(m), 128, 0, st>>>(m, n, seed, offset, xs, ldx, ts, ldt, xb, tb);
+  gather_kernel<<<grid1(m), 128, 0, st>>>(m, n, seed, offset, xs, ldx, ts, ldt, pss, ldp, xb, tb,
+                                          psb);
   WWB_CHECK(cudaGetLastError());
 }
 

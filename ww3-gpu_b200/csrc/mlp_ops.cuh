@@ -6,15 +6,20 @@
 //
 // Normalisation. W3SNL1 (kokkos/src/ww_kokkos/snl1_team.hpp:383-496) computes, per point,
 //   S(k, th) = CONS(kdmean) * CONX(k) * G(UE)(k, th),  UE = A / CONX,  CONX = CG / (2 pi sigma),
-// with G a cubic form of UE (sections 3-4). So with umax = max UE and U = UE / umax,
-//   S = CONS * umax^3 * CONX(k) * G(U),
-// and the network only has to learn G on spectra of unit peak: depth enters through CONX and
-// CONS, amplitude through umax^3, both applied exactly outside the network. Directions are
-// rotated so the spectrum's dominant direction comes first (the DIA commutes with a cyclic shift
-// of directions, its index tables being circulant in direction), and the rotation is undone on
-// the output. Network input: ln(U + 1e-6) / 7 + 1 per bin, then ln(kdmean) / 5 and
-// CONS / SNLC1 - 1; target: G(U)(k, th) / rowscale(k), rowscale the per-frequency RMS of G over
-// the first chunk of the training set.
+// with G a cubic form of UE whose terms at row k carry AF11 = f^11 of rows near k (sections
+// 3-4). So S(k, .) scales, point by point and row by row, as
+//   e^lambda(k) = CONS * CONX(k) * AF11(k) * u(k)^3,  u(k) = the largest UE within 3 rows of k,
+// and T = S / (e^lambda(k) rowscale(k)) is of order one in every row of every spectrum (rowscale
+// the per-row RMS of S e^-lambda over the first chunk of the training set). The network maps
+// the spectrum's shape to T; depth (CONX, CONS), amplitude and the steep frequency dependence
+// are applied exactly outside it. Directions are rotated so the spectrum's dominant direction
+// comes first (the DIA commutes with a cyclic shift of directions, its index tables being
+// circulant in direction), and the rotation is undone on the output. Network input:
+// ln(UE / max UE + 1e-6) / 7 + 1 per bin, then ln(kdmean) / 5 and CONS / SNLC1 - 1.
+//
+// Per point the normalisation keeps 2 NK floats ("ps"): lambda(k), then the weight of row k in
+// the Hs tendency, e^lambda(k) DDEN(k) / CG(k) divided by its largest value (DDEN = DTH DSII SIG,
+// DSII = SIG (XFR - 1/XFR) / 2).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -30,9 +35,7 @@ struct SurGrid {
   int nk, nth, nspec;
   int din, dout;          ///< padded network widths (multiples of 64)
   const float* sig;       ///< device, NK
-  const float* rowscale;  ///< device, NK (target scale per frequency row)
-  const float* omega;     ///< device, NK: rowscale * DDEN / (2 pi sigma), the Hs-tendency weight
-                          ///< of a normalised output bin
+  const float* rowscale;  ///< device, NK: RMS of the scaled targets per frequency row
   float snlc1, kdcon, kdmn, snls1, snls2, snls3;
   float dth, xfr;
 };
@@ -46,8 +49,9 @@ struct SynthDraw {
 };
 
 /// Gate thresholds: a point keeps the surrogate's S when the energy residual of its output
-/// |sum w S| / sum w |S| is at most `energy` and the network's own predicted error (the
-/// log of its Hs-tendency error, output column NSPEC) is at most `log_err`.
+/// |sum w S| / sum w |S| (w = DDEN / CG, the Hs-tendency weight) is at most `energy` and the
+/// network's own predicted error (the log of its Hs-tendency error, output column NSPEC) is at
+/// most `log_err`.
 struct GateParams {
   float energy;
   float log_err;
@@ -56,25 +60,27 @@ struct GateParams {
 void synth(const SurGrid& g, const SynthDraw& d, long long p0, int npts, float* a, float* cg,
            float* kdmean, cudaStream_t st);
 
-/// Network input rows x (npts x ldx bf16) plus per-point scale and direction shift.
+/// Network input rows x (npts x ldx bf16), the per-point scales ps (npts x 2 NK) and the
+/// direction shift.
 void prep(const SurGrid& g, int npts, const float* a, const float* cg, const float* kdmean,
-          __nv_bfloat16* x, int ldx, float* scale, int* shift, cudaStream_t st);
+          __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st);
 
-/// Accumulate sum over points and directions of (S / (scale CONX))^2 per row into acc (double,
-/// NK, zeroed by the caller), and count the points with a nonzero scale into cnt.
-void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
-                  const int* shift, double* acc, unsigned long long* cnt, cudaStream_t st);
+/// Accumulate sum over points and directions of (S e^-lambda)^2 per row into acc (double, NK,
+/// zeroed by the caller), and count the points with a nonempty spectrum into cnt.
+void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* ps, double* acc,
+                  unsigned long long* cnt, cudaStream_t st);
 
 /// Normalised targets t (npts x ldt fp32) from the DIA's S.
-void targets(const SurGrid& g, int npts, const float* s, const float* cg, const float* scale,
-             const int* shift, float* t, int ldt, cudaStream_t st);
+void targets(const SurGrid& g, int npts, const float* s, const float* ps, const int* shift,
+             float* t, int ldt, cudaStream_t st);
 
 /// Output side of inference: S (de-normalised, rotated back) and D = 0 for accepted points, the
 /// compacted list of rejected points (count at *nrej, zeroed by the caller; also added to
-/// *nrej_total when given), per-point flag.
+/// *nrej_total when given), per-point flag, and (gv, may be null) each point's head output and
+/// energy residual.
 void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, int ldo,
-          const float* cg, const float* scale, const int* shift, float* s, float* d,
-          int* accepted, int* rej_list, int* nrej, int* nrej_total, cudaStream_t st);
+          const float* ps, const int* shift, float* s, float* d, int* accepted, float* gv,
+          int* rej_list, int* nrej, int* nrej_total, cudaStream_t st);
 
 /// Training loss and the output gradient. out (m x ldo fp32), t (m x ldt): grad (m x dout bf16)
 /// = dL/dout; loss (3 floats: MSE, energy-budget, error-head terms) accumulated.
@@ -83,15 +89,16 @@ struct LossWeights {
   float lambda;  ///< weight of the error head
   int head;      ///< 1: column NSPEC is trained as the error head
 };
+/// ps (m x 2 NK, may be null: no energy term) gives each row's Hs-tendency weights.
 void loss_grad(const SurGrid& g, const LossWeights& w, int m, int nvalid, const float* out,
-               int ldo, const float* t, int ldt, __nv_bfloat16* grad, int ldg, float* loss,
-               cudaStream_t st);
+               int ldo, const float* t, int ldt, const float* ps, __nv_bfloat16* grad, int ldg,
+               float* loss, cudaStream_t st);
 
-/// Batch rows r < m of the training set: x rows idx(r) and t rows idx(r), idx(r) a seeded draw
-/// in [0, n) (or r + offset when seed == 0).
+/// Batch rows r < m of the training set: x, t and ps rows idx(r), idx(r) a seeded draw in
+/// [0, n) (or r + offset when seed == 0).
 void gather_batch(int m, long long n, uint64_t seed, long long offset, const __nv_bfloat16* xs,
-                  int ldx, const float* ts, int ldt, __nv_bfloat16* xb, float* tb,
-                  cudaStream_t st);
+                  int ldx, const float* ts, int ldt, const float* pss, int ldp,
+                  __nv_bfloat16* xb, float* tb, float* psb, cudaStream_t st);
 
 /// dst (cols x rows) = src (rows x cols)^T, bf16; ld's in elements.
 void transpose(const __nv_bfloat16* src, int rows, int cols, int lds, __nv_bfloat16* dst, int ldd,

@@ -363,9 +363,10 @@ __device__ __forceinline__ void tma_fetch_point(uint64_t* bar, float* stage, con
       : "memory");
 }
 
-/// Wait for phase `parity` of the mbarrier, giving up after kWaitLimit polls (then the status
-/// word records it and the kernel runs on; the host reports the failure).
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+/// Wait for phase `parity` of the mbarrier, giving up after kWaitLimit polls: then the status
+/// word records it (the host reports the failure) and false is returned, and the caller's CTA
+/// stops at its next barrier (see the point loops) without starting another bulk copy.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
   unsigned done = 0;
   for (unsigned it = 0; it < kWaitLimit; ++it) {
     asm volatile(
@@ -374,9 +375,10 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* e
         : "=r"(done)
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
-    if (done) return;
+    if (done) return true;
   }
   atomicExch(err, 1);
+  return false;
 }
 
 // LIST: the batch is the points pidx[0 .. min(npts, *pcount)) of the arrays (the gated
@@ -447,14 +449,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_band_kernel(
     const float* const src_a = TMA ? stage : a + static_cast<size_t>(ipt) * nspec;
     const float* const src_c = TMA ? stage + nspec : cg + static_cast<size_t>(ipt) * nk;
     float* const conx = conx2 + buf * nk;
+    bool lost = false;
     if (TMA) {
-      mbar_wait(bar, parity, err);
+      lost = !mbar_wait(bar, parity, err);
       parity ^= 1u;
     }
     // 1. CONS; 2a. CON per frequency row.
     const float cons = dia_cons(p, kd_next);
     for (int k = tid; k < nk; k += BLOCK) conx[k] = kTpiInv / __ldg(p.sig + k) * src_c[k];
-    __syncthreads();
+    // A bulk copy whose wait gave up ends this CTA's work here, all its threads together, so no
+    // later copy is started on a barrier whose phase did not complete.
+    if (__syncthreads_or(lost)) break;
 
     // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
     {
@@ -710,11 +715,11 @@ __global__ void __launch_bounds__(NTH * G, MINB) snl1_tile_kernel(
   int buf = 0;
   for (int ipt = blockIdx.x; ipt < npts; ipt += gridDim.x, buf ^= 1) {
     float* const conx = conx2 + buf * nk;
-    mbar_wait(bar, parity, err);
+    const bool lost = !mbar_wait(bar, parity, err);
     parity ^= 1u;
     const float cons = dia_cons(p, kd_next);
     for (int k = tid; k < nk; k += BLOCK) conx[k] = kTpiInv / __ldg(p.sig + k) * stage[nspec + k];
-    __syncthreads();
+    if (__syncthreads_or(lost)) break;  // as in the band kernel: stop together, fetch no more
     // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
     for (int isp = tid; isp < nspec; isp += BLOCK) {
       const int ifr0 = isp / NTH, col = isp - ifr0 * NTH;

@@ -207,10 +207,19 @@ class Surrogate:
 
 
 def error_summary(stats):
-    """Aggregate ww_sur_judge statistics (npts x 10, numpy float64) into the reported errors:
-    the mean Hs-tendency error relative to the gross tendency (the gate's budget), the mean
-    relative error of the band-wise energy tendency, the relative L2 error of S, and the median
-    relative error of the net Hs tendency and of the mean-frequency tendency."""
+    """Aggregate ww_sur_judge statistics (npts x 10, numpy float64) into the reported errors of a
+    candidate S against the FP64 DIA, per point then averaged:
+
+    - hs_band_err: the band-resolved Hs-tendency error, sum over frequency bands k of
+      |tau_k(S) - tau_k(S64)| over sum of |tau_k(S64)|, tau_k = 8/Hs sum_th S DDEN/CG the band's
+      share of dHs/dt (Hs = 4 sqrt(sum A DDEN/CG), the reference's W3SRCE definition). The
+      gate's error budget. A zero S scores 1.
+    - hs_tendency_err: |dHs/dt(S) - dHs/dt(S64)| over the gross tendency 8/Hs sum |S64| DDEN/CG.
+      The DIA nearly conserves energy (its net tendency is a few 1e-3 of the gross), so this is
+      small even for a poor S; reported, not used to judge.
+    - net_hs_tendency_relerr_median: the same difference over |dHs/dt(S64)| itself (median).
+    - tm_tendency_relerr_median: relative error of the mean-frequency tendency (median).
+    - s_rel_l2: relative L2 error of S over all points and bins."""
     st = np.asarray(stats, np.float64)
     gross = np.where(st[:, J_TAU_GROSS] > 0, st[:, J_TAU_GROSS], np.inf)
     e_hs = np.abs(st[:, J_TAU_CAND] - st[:, J_TAU_REF]) / gross
@@ -218,7 +227,9 @@ def error_summary(stats):
     s_l2 = np.sqrt(st[:, J_S_ERR2].sum() / max(st[:, J_S_REF2].sum(), 1e-300))
     net = np.abs(st[:, J_TAU_CAND] - st[:, J_TAU_REF]) / np.maximum(np.abs(st[:, J_TAU_REF]), 1e-300)
     fm = np.abs(st[:, J_FM_CAND] - st[:, J_FM_REF]) / np.maximum(np.abs(st[:, J_FM_REF]), 1e-300)
-    return {"hs_tendency_err_mean": float(e_hs.mean()), "hs_tendency_err_max": float(e_hs.max()),
-            "band_tendency_err_mean": float(band.mean()), "s_rel_l2": float(s_l2),
+    return {"hs_band_err_mean": float(band.mean()), "hs_band_err_p90": float(np.quantile(band, 0.9)),
+            "hs_band_err_max": float(band.max()),
+            "hs_tendency_err_mean": float(e_hs.mean()), "hs_tendency_err_max": float(e_hs.max()),
+            "s_rel_l2": float(s_l2),
             "net_hs_tendency_relerr_median": float(np.median(net)),
             "tm_tendency_relerr_median": float(np.median(fm))}

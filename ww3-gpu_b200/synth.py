@@ -192,10 +192,12 @@ def prop3_spectral_maps(nk, nth):
 
 
 def ktp3_case(npts, seed=0, nk=36, nth=36, nsea=None, depth_range=(5.0, 4000.0), ntloc=2,
-              dtg=900.0, currents=True):
+              dtg=900.0, currents=True, spectra="jonswap"):
     """Seeded inputs of ww_ktp3_batch for npts sea points of a grid with nsea points (points
     listed in a shuffled order, every other column of VA left untouched). Returns a dict with
-    the C ABI's arguments by name (column-major arrays flattened as the ABI reads them)."""
+    the C ABI's arguments by name (column-major arrays flattened as the ABI reads them).
+    spectra="uniform" fills VA with U(0, 1) values instead of sea states (grids of 10^5-10^6
+    points, where only the index arithmetic at size is under test)."""
     rng = np.random.default_rng(seed)
     nsea = nsea or npts
     nspec, nk2 = nk * nth, nk + 2
@@ -206,10 +208,8 @@ def ktp3_case(npts, seed=0, nk=36, nth=36, nsea=None, depth_range=(5.0, 4000.0),
     kd = np.minimum(k * dep[:, None], 40.0)
     s64 = sp["sig"].astype(np.float64)[None, :]
     cg = 0.5 * s64 / k * (1.0 + 2.0 * kd / np.sinh(np.minimum(2.0 * kd, 80.0)))
-    g = sea_states(nsea + 1, seed=seed + 17, nk=nk, nth=nth, depth_range=depth_range)
     nsealm = nsea
-    va = np.zeros((nsealm + 1, nspec), np.float32)
-    va[1:] = g["a"][1:]
+    va = _spectra(spectra, nsea, seed + 17, nk, nth, depth_range)
     isea = rng.permutation(np.arange(1, nsea + 1))[:npts].astype(np.int32)
     jsea = isea.copy()  # one rank: JSEA = ISEA
     lat = rng.uniform(-70.0, 70.0, npts)
@@ -237,6 +237,17 @@ def ktp3_case(npts, seed=0, nk=36, nth=36, nsea=None, depth_range=(5.0, 4000.0),
         "va": va, "nsealm": nsealm,
         "cflthmax": np.full(nsealm, -1.0, np.float32), "cflkmax": np.full(nsealm, -1.0, np.float32),
     }
+
+
+def _spectra(kind, nsea, seed, nk, nth, depth_range):
+    """VA(NSPEC, 0:NSEA) as a C-ordered (nsea + 1, nspec) array, column 0 zero: seeded sea
+    states, or U(0, 1) values for kind "uniform"."""
+    va = np.zeros((nsea + 1, nk * nth), np.float32)
+    if kind == "uniform":
+        va[1:] = np.random.default_rng(seed).random((nsea, nk * nth), dtype=np.float32)
+    else:
+        va[1:] = sea_states(nsea + 1, seed=seed, nk=nk, nth=nth, depth_range=depth_range)["a"][1:]
+    return va
 
 
 def land_mask(nx, ny, seed=0, sea_fraction=0.7, smooth=6):
@@ -276,10 +287,12 @@ def sea_grid(nx, ny, seed=0, sea_fraction=0.7, boundary=0.02, excluded=0.01):
 
 
 def xyp3_case(nx=48, ny=32, seed=0, nk=36, nth=36, iclose=2, flcur=True, flbpi=True,
-              on_fraction=1.0, dtg=900.0, ref=None):
+              on_fraction=1.0, dtg=900.0, ref=None, spectra="jonswap", on_components=None):
     """Seeded inputs of ww_xyp3_batch on an NX x NY regular lon/lat grid (0.25 degrees), the
     W3MAP3 maps built by ``ref`` (a callable ref(nx, ny, nsea, nk, nth, mapsta, mapsf) returning
-    (mapx2, mapy2, mapaxy, mapcxy, counts), the reference's own W3MAP3 in the tests)."""
+    (mapx2, mapy2, mapaxy, mapcxy, counts), the reference's own W3MAP3 in the tests).
+    spectra="uniform" fills VA with U(0, 1) values (see ktp3_case); on_components=n switches on
+    n spectral components spread evenly over NSPEC instead of a random on_fraction."""
     rng = np.random.default_rng(seed)
     nspec = nk * nth
     sea = land_mask(nx, ny, seed=seed)
@@ -339,9 +352,7 @@ def xyp3_case(nx=48, ny=32, seed=0, nk=36, nth=36, iclose=2, flcur=True, flbpi=T
     else:
         isbpi = np.zeros(1, np.int32)
     nbi = len(isbpi) if flbpi else 0
-    g = sea_states(nsea + 1, seed=seed + 5, nk=nk, nth=nth, depth_range=(10.0, 4000.0))
-    va = np.zeros((nsea + 1, nspec), np.float32)
-    va[1:] = g["a"][1:]
+    va = _spectra(spectra, nsea, seed + 5, nk, nth, (10.0, 4000.0))
     bb0 = np.zeros((max(nbi, 0) + 1, nspec), np.float32)
     bbn = np.zeros((max(nbi, 0) + 1, nspec), np.float32)
     if nbi:
@@ -349,6 +360,9 @@ def xyp3_case(nx=48, ny=32, seed=0, nk=36, nth=36, iclose=2, flcur=True, flbpi=T
         bb0[1:] = gb["a"][:nbi]
         bbn[1:] = gb["a"][nbi:]
     on = (rng.uniform(0.0, 1.0, nspec) < on_fraction).astype(np.int32)
+    if on_components is not None:
+        on = np.zeros(nspec, np.int32)
+        on[np.linspace(0, nspec - 1, on_components).round().astype(int)] = 1
     return {
         "rpar": np.array([300.0, sp["dth"], 1.1, 1.5, 1.5], np.float32),
         "ipar": np.array([nx, ny, nsea, nk, nth, nspec, iclose, 1, 1, 1, int(flcur)], np.int32),
