@@ -86,7 +86,7 @@ def parse():
     p.add_argument("--npts", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--train-steps", type=int, default=6000,
+    p.add_argument("--train-steps", type=int, default=20000,
                    help="surrogate workload: AdamW steps of batch 8192 before the timing")
     p.add_argument("--sur-lr", type=float, default=1e-3)
     p.add_argument("--sur-mu", type=float, default=1.0,
@@ -1380,10 +1380,13 @@ def sur_config(args, world, train):
     return {"workload": SUR_WORKLOAD, "nk": NK, "nth": NTH, "npts_per_gpu": args.npts,
             "global_points": args.npts * world, "seed": 2024,
             "training": train,
-            "hs_error": ("per point |dHs/dt(S) - dHs/dt(S64)| / (8/Hs sum |S64| DDEN/CG), "
-                         "Hs = 4 sqrt(sum A DDEN/CG) as in the reference's W3SRCE "
-                         "(srce_kernel.hpp:415-430); S64 = this library's FP64 DIA on the device; "
-                         "a rejected point counts its plain-DIA error"),
+            "hs_error": ("band-resolved Hs-tendency error per point: sum over frequency bands k "
+                         "of |tau_k(S) - tau_k(S64)| / sum_k |tau_k(S64)|, tau_k = 8/Hs sum_theta "
+                         "S DDEN/CG (the band's share of dHs/dt; Hs = 4 sqrt(sum A DDEN/CG) as in "
+                         "the reference's W3SRCE, srce_kernel.hpp:415-430); S64 = this library's "
+                         "FP64 DIA on the device; a rejected point counts its plain-DIA error; "
+                         "the gate is calibrated so the mean over points is at most the budget"),
+            "hs_error_budget": None,
             "l2": "inputs 1.4 GB and outputs 2.7 GB per pass > 126 MB L2 (no flush needed)",
             "parallelism": f"points sharded over {world} GPU(s), no collective; each GPU trains "
                            "its own copy of the surrogate"}
@@ -1537,19 +1540,18 @@ def run_b200_surrogate(args):
     h_a, h_cg, h_kd = a.cpu().pin_memory(), cg.cpu().pin_memory(), kd.cpu().pin_memory()
     h_s = torch.empty_like(h_a).pin_memory()
     h_d = torch.empty_like(h_a).pin_memory()
-    da, dcg, dkd = torch.empty_like(a), torch.empty_like(cg), torch.empty_like(kd)
-    ds, dd = torch.empty_like(a), torch.empty_like(a)
 
     def e2e_step():
-        da.copy_(h_a, non_blocking=True)
-        dcg.copy_(h_cg, non_blocking=True)
-        dkd.copy_(h_kd, non_blocking=True)
-        model.gated(npts, da, dcg, dkd, ds, dd, None, handle)
-        h_s.copy_(ds, non_blocking=True)
-        h_d.copy_(dd, non_blocking=True)
+        model.gated_host(npts, h_a, h_cg, h_kd, h_s, h_d)
 
-    e2e_ms = timed(e2e_step, e2e_steps, 1)
-    e2e_value = npts * world * e2e_steps / (e2e_ms / 1e3)
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = npts * world * e2e_steps / e2e_s
     same = bool(torch.equal(h_s.view(torch.int32), s.cpu().view(torch.int32)))
 
     chunks = (npts + SUR_INFER_ROWS - 1) // SUR_INFER_ROWS
@@ -1561,11 +1563,13 @@ def run_b200_surrogate(args):
              "holdout_loss": [float(v) for v in holdout], "gate": cal,
              "train_tflops": (3 * SUR_FLOP_PER_POINT * SUR_BATCH * args.train_steps
                               / max(train_s, 1e-9) / 1e12)}
+    cfgd = sur_config(args, world, train)
+    cfgd["hs_error_budget"] = args.sur_target
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": gated_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network / f32 fallback",
-        "data": "synthetic", "config": sur_config(args, world, train),
+        "data": "synthetic", "config": cfgd,
         "plain_dia": {"value": npts * world / (plain_ms / 1e3), "unit": UNIT,
                       "ms_per_step": plain_ms, "kernel": "snl1_band_kernel",
                       "error_vs_fp64": err_plain},
@@ -1575,7 +1579,8 @@ def run_b200_surrogate(args):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": int((h_a.numel() + h_cg.numel() + h_kd.numel()) * 4),
                 "d2h_bytes_per_step": int((h_s.numel() + h_d.numel()) * 4),
-                "steps": e2e_steps, "entry": "ww_snl1_gated on copies of page-locked host buffers",
+                "steps": e2e_steps, "host_entry": "ww_snl1_gated_host (page-locked host buffers; copies "
+                                                  "pipelined with the compute in 65,536-point chunks)",
                 "matches_device_entry": same},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,

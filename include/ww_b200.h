@@ -586,6 +586,12 @@ int ww_sur_calibrate(int igrid, int npts, unsigned long long seed, float bimodal
  * Asynchronous on `stream`. */
 void ww_snl1_gated(int igrid, int npts, const float* a, const float* cg, const float* kdmean,
                    float* s, float* d, int* accepted, void* stream);
+/* The gated W3SNL1 on host arrays, as ww_snl1 (ww_kokkos_c.hpp:115-116) takes them: the
+ * copies in and out are pipelined with the compute in chunks of 65,536 points on three slots
+ * (page-locked caller memory copies fastest); D is 0 where the surrogate was kept. Synchronous.
+ * Status in ww_sur_last_error(). */
+void ww_snl1_gated_host(int igrid, int npts, const float* a, const float* cg,
+                        const float* kdmean, float* s, float* d);
 /* The network alone: out fp32 (rows x the padded output width, NSPEC + 1 rounded up to 64)
  * from normalised inputs x bf16 (rows x the padded input width, NSPEC + 2 rounded up to 64):
  * the four tensor-core GEMMs of one inference, asynchronous on `stream`. */

@@ -257,3 +257,24 @@ def test_training_gains_over_the_untrained_network(model, sur):
     assert after["hs_band_err_mean"] < 0.5 * before["hs_band_err_mean"]
     assert cal1["accepted"] > cal0["accepted"]
     assert cal1["mean_err_gated"] <= 0.02 + 1e-6
+
+
+def test_gated_host_entry_equals_device_entry(model, dia):
+    """ww_snl1_gated_host (host arrays, copies pipelined over three chunk slots) gives the
+    device entry's bits, on a batch of three chunks with a partial gate."""
+    import torch
+
+    n = 150_000
+    a, cg, kd = _inputs(model, n, seed=34)
+    model.gate(0.05, 1e30)
+    s = torch.zeros(n, 1296, device="cuda")
+    d = torch.zeros_like(s)
+    model.gated(n, a, cg, kd, s, d)
+    nrej = model.fallback_count()
+    h = [t.cpu().pin_memory() for t in (a, cg, kd)]
+    hs = torch.full((n, 1296), float("nan")).pin_memory()
+    hd = torch.full((n, 1296), float("nan")).pin_memory()
+    model.gated_host(n, *h, hs, hd)
+    assert model.fallback_count() == nrej
+    assert_bitexact(hs.numpy(), s.cpu().numpy(), "host entry S")
+    assert_bitexact(hd.numpy(), d.cpu().numpy(), "host entry D")

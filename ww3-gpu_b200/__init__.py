@@ -54,7 +54,7 @@ EXPORTS = (
     "ww_mlp_get_params", "ww_mlp_get_grads", "ww_mlp_train_step", "ww_mlp_forward",
     "ww_mlp_gemm", "ww_mlp_last_error", "ww_sur_init", "ww_sur_synth", "ww_sur_dataset",
     "ww_sur_loss_weights", "ww_sur_train", "ww_sur_eval", "ww_sur_gate", "ww_sur_calibrate",
-    "ww_snl1_gated", "ww_sur_forward", "ww_sur_fallback_count", "ww_sur_judge", "ww_sur_param_count",
+    "ww_snl1_gated", "ww_snl1_gated_host", "ww_sur_forward", "ww_sur_fallback_count", "ww_sur_judge", "ww_sur_param_count",
     "ww_sur_get_params", "ww_sur_set_params", "ww_sur_last_error",
 )
 
@@ -184,6 +184,8 @@ def lib():
         L.ww_sur_calibrate.argtypes = [_I, _I, _U64, _F, _F, _F, _F, _F, _P]
         L.ww_snl1_gated.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _P]
         L.ww_snl1_gated.restype = None
+        L.ww_snl1_gated_host.argtypes = [_I, _I, _P, _P, _P, _P, _P]
+        L.ww_snl1_gated_host.restype = None
         L.ww_sur_fallback_count.argtypes = [_I, _P]
         L.ww_sur_forward.argtypes = [_I, _I, _P, _P, _P]
         L.ww_sur_judge.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]

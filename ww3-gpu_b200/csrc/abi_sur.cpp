@@ -367,6 +367,23 @@ struct Sur {
   DiaF64 f64{};
   bool f64_ok = false;
   DBuf<double> af11d, sigd;
+  // host-pointer entry: three chunk slots, copies in and out overlapping the compute
+  struct Pipe {
+    static constexpr int kSlots = 3;
+    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    cudaEvent_t copied[kSlots] = {}, computed[kSlots] = {}, drained[kSlots] = {};
+    DBuf<float> a[kSlots], cg[kSlots], kd[kSlots], s[kSlots], d[kSlots];
+    bool ready = false;
+    ~Pipe() {
+      for (int k = 0; k < kSlots; ++k) {
+        if (copied[k]) cudaEventDestroy(copied[k]);
+        if (computed[k]) cudaEventDestroy(computed[k]);
+        if (drained[k]) cudaEventDestroy(drained[k]);
+      }
+      for (cudaStream_t x : {in, comp, out})
+        if (x) cudaStreamDestroy(x);
+    }
+  } pipe;
 };
 
 std::map<int, std::unique_ptr<Sur>>& surs() {
@@ -400,10 +417,11 @@ void sur_scratch(Sur& s, int rows) {
 /// The surrogate's S for npts points (device arrays) into s/d, gated, with the plain DIA on the
 /// rejected points; accepted (optional) gets 1/0 per point.
 void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* kd, float* so,
-               float* dd, int* accepted, const GateParams& gate, cudaStream_t st, bool fallback) {
+               float* dd, int* accepted, const GateParams& gate, cudaStream_t st, bool fallback,
+               bool reset_count = true) {
   const int nspec = s.g.nspec, nk = s.g.nk;
   sur_scratch(s, std::min(npts, kInferRows));
-  WWB_CHECK(cudaMemsetAsync(s.nrej_total.p, 0, sizeof(int), st));
+  if (reset_count) WWB_CHECK(cudaMemsetAsync(s.nrej_total.p, 0, sizeof(int), st));
   for (int p0 = 0; p0 < npts; p0 += kInferRows) {
     const int n = std::min(kInferRows, npts - p0);
     const float* ap = a + static_cast<size_t>(p0) * nspec;
@@ -892,6 +910,79 @@ void ww_snl1_gated(int igrid, int npts, const float* a, const float* cg, const f
     }
     sur_apply(*sp, npts, a, cg, kdmean, s, d, accepted, sp->gate, static_cast<cudaStream_t>(stream),
               true);
+    g_sur_status.ok();
+  } catch (const std::exception& e) {
+    sur_fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
+void ww_snl1_gated_host(int igrid, int npts, const float* a, const float* cg,
+                        const float* kdmean, float* s, float* d) {
+  try {
+    Sur* sp = find_sur(igrid);
+    if (!sp) return;
+    if (npts < 0) {
+      sur_fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1_gated_host: npts is negative");
+      return;
+    }
+    if (npts == 0) {
+      g_sur_status.ok();
+      return;
+    }
+    if (!a || !cg || !kdmean || !s || !d) {
+      sur_fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_snl1_gated_host: null array pointer");
+      return;
+    }
+    Sur& S = *sp;
+    auto& P = S.pipe;
+    const size_t nspec = S.g.nspec, nk = S.g.nk;
+    if (!P.ready) {
+      WWB_CHECK(cudaStreamCreateWithFlags(&P.in, cudaStreamNonBlocking));
+      WWB_CHECK(cudaStreamCreateWithFlags(&P.comp, cudaStreamNonBlocking));
+      WWB_CHECK(cudaStreamCreateWithFlags(&P.out, cudaStreamNonBlocking));
+      for (int k = 0; k < Sur::Pipe::kSlots; ++k) {
+        WWB_CHECK(cudaEventCreateWithFlags(&P.copied[k], cudaEventDisableTiming));
+        WWB_CHECK(cudaEventCreateWithFlags(&P.computed[k], cudaEventDisableTiming));
+        WWB_CHECK(cudaEventCreateWithFlags(&P.drained[k], cudaEventDisableTiming));
+        P.a[k].alloc(kInferRows * nspec);
+        P.cg[k].alloc(kInferRows * nk);
+        P.kd[k].alloc(kInferRows);
+        P.s[k].alloc(kInferRows * nspec);
+        P.d[k].alloc(kInferRows * nspec);
+      }
+      P.ready = true;
+    }
+    timers::Region t_call("snl1.gated.call");
+    // Chunk c: copy in on `in`, compute on `comp`, copy out on `out`, slot c % 3; a slot is
+    // refilled only after its previous chunk's results left (the event of its copy out).
+    int c = 0;
+    for (int p0 = 0; p0 < npts; p0 += kInferRows, ++c) {
+      const int k = c % Sur::Pipe::kSlots;
+      const size_t n = static_cast<size_t>(std::min(kInferRows, npts - p0));
+      WWB_CHECK(cudaStreamWaitEvent(P.in, P.drained[k], 0));
+      WWB_CHECK(cudaMemcpyAsync(P.a[k].p, a + p0 * nspec, n * nspec * 4, cudaMemcpyHostToDevice, P.in));
+      WWB_CHECK(cudaMemcpyAsync(P.cg[k].p, cg + p0 * nk, n * nk * 4, cudaMemcpyHostToDevice, P.in));
+      WWB_CHECK(cudaMemcpyAsync(P.kd[k].p, kdmean + p0, n * 4, cudaMemcpyHostToDevice, P.in));
+      WWB_CHECK(cudaEventRecord(P.copied[k], P.in));
+      WWB_CHECK(cudaStreamWaitEvent(P.comp, P.copied[k], 0));
+      sur_apply(S, static_cast<int>(n), P.a[k].p, P.cg[k].p, P.kd[k].p, P.s[k].p, P.d[k].p,
+                nullptr, S.gate, P.comp, true, c == 0);
+      WWB_CHECK(cudaEventRecord(P.computed[k], P.comp));
+      WWB_CHECK(cudaStreamWaitEvent(P.out, P.computed[k], 0));
+      WWB_CHECK(cudaMemcpyAsync(s + p0 * nspec, P.s[k].p, n * nspec * 4, cudaMemcpyDeviceToHost, P.out));
+      WWB_CHECK(cudaMemcpyAsync(d + p0 * nspec, P.d[k].p, n * nspec * 4, cudaMemcpyDeviceToHost, P.out));
+      WWB_CHECK(cudaEventRecord(P.drained[k], P.out));
+    }
+    WWB_CHECK(cudaStreamSynchronize(P.out));
+    WWB_CHECK(cudaStreamSynchronize(P.comp));
+    if (take_err(S.net)) {
+      sur_fail(WW_KOKKOS_ERR_KERNEL, "ww_snl1_gated_host: a GEMM wait gave up");
+      return;
+    }
+    if (snl1_take_error() != 0) {
+      sur_fail(WW_KOKKOS_ERR_KERNEL, "ww_snl1_gated_host: a DIA wait gave up");
+      return;
+    }
     g_sur_status.ok();
   } catch (const std::exception& e) {
     sur_fail(WW_KOKKOS_ERR_KERNEL, e.what());

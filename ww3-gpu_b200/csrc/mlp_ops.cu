@@ -53,23 +53,6 @@ __device__ __forceinline__ T block_sum(T v, T* red) {
   return t;
 }
 
-__device__ __forceinline__ float block_max(float v, float* red) {
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    float t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
-    for (int o = 16; o > 0; o >>= 1) t = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, o));
-    if (threadIdx.x == 0) red[0] = t;
-  }
-  __syncthreads();
-  const float t = red[0];
-  __syncthreads();
-  return t;
-}
-
 /// CONS of W3SNL1 section 1 (snl1_team.hpp:386-390) in float with CUDA's expf.
 __device__ __forceinline__ float cons_of(const SurGrid& g, float kd) {
   const float x0 = g.kdcon * kd;
@@ -186,96 +169,168 @@ __device__ __forceinline__ float ln_dden(const SurGrid& g, float sig) {
   return logf(g.dth * 0.5f * sig * (g.xfr - 1.0f / g.xfr) * sig);
 }
 
-__global__ void prep_kernel(SurGrid g, int npts, const float* __restrict__ a,
-                            const float* __restrict__ cg, const float* __restrict__ kdm,
-                            __nv_bfloat16* __restrict__ x, int ldx, float* __restrict__ ps,
-                            int* __restrict__ shift) {
+__device__ __forceinline__ float warp_sum(float v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+constexpr int kPointsPerCta = 8;  // one warp per sea point in the pre- and post-processing
+
+/// Floats of shared memory per warp of prep_kernel.
+__host__ __device__ inline int prep_floats(int nspec, int nk, int nth) {
+  return nspec + 4 * nk + nth;
+}
+
+__global__ void __launch_bounds__(32 * kPointsPerCta)
+    prep_kernel(SurGrid g, int npts, const float* __restrict__ a, const float* __restrict__ cg,
+                const float* __restrict__ kdm, __nv_bfloat16* __restrict__ x, int ldx,
+                float* __restrict__ ps, int* __restrict__ shift) {
   extern __shared__ float sm[];
-  const int ip = blockIdx.x, tid = threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ip = blockIdx.x * kPointsPerCta + warp;
+  if (ip >= npts) return;  // warp-uniform: the rest of the kernel is per warp
   const int nk = g.nk, nth = g.nth, nspec = g.nspec;
-  float* const ue = sm;                 // nspec
-  float* const conx = ue + nspec;       // nk
-  float* const dsum = conx + nk;        // nth
-  float* const rmax = dsum + nth;       // nk: largest UE of each row
-  float* const lw = rmax + nk;          // nk: ln of each row's Hs-tendency weight
-  float* const red = lw + nk;           // 32
-  __shared__ int s_shift;
-  __shared__ float s_cons;
+  float* const ue = sm + static_cast<size_t>(warp) * prep_floats(nspec, nk, nth);
+  float* const rcon = ue + nspec;  // nk: 1 / CONX
+  float* const dsum = rcon + nk;   // nth: the spectrum summed over frequency per direction
+  float* const rmax = dsum + nth;  // nk: largest UE of each row
+  float* const lw = rmax + nk;     // nk: scratch per row
+  float* const lam = lw + nk;      // nk
   const float* ap = a + static_cast<size_t>(ip) * nspec;
+  const float* cgp = cg + static_cast<size_t>(ip) * nk;
   float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
-  for (int k = tid; k < nk; k += blockDim.x)
-    conx[k] = kTpiInvF / __ldg(g.sig + k) * __ldg(cg + static_cast<size_t>(ip) * nk + k);
-  __syncthreads();
+  for (int k = lane; k < nk; k += 32) rcon[k] = __ldg(g.sig + k) / (kTpiInvF * __ldg(cgp + k));
+  __syncwarp();
+  // UE = A / CONX, four bins per load (NTH a multiple of 4: the four share a row).
   float mx = 0.0f;
-  for (int i = tid; i < nspec; i += blockDim.x) {
-    const float v = __ldg(ap + i) / conx[i / nth];
-    ue[i] = v;
-    mx = fmaxf(mx, v);
+  if ((nth & 3) == 0 && (reinterpret_cast<uintptr_t>(ap) & 15) == 0) {
+    const float4* a4 = reinterpret_cast<const float4*>(ap);
+    float4* u4 = reinterpret_cast<float4*>(ue);
+    const int q4 = nth >> 2;
+    for (int q = lane; q < nspec / 4; q += 32) {
+      float4 v = __ldg(a4 + q);
+      const float r = rcon[q / q4];
+      v.x *= r;
+      v.y *= r;
+      v.z *= r;
+      v.w *= r;
+      u4[q] = v;
+      mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    }
+  } else {
+    for (int i = lane; i < nspec; i += 32) {
+      const float v = __ldg(ap + i) * rcon[i / nth];
+      ue[i] = v;
+      mx = fmaxf(mx, v);
+    }
   }
-  const float umax = block_max(mx, red);
-  for (int t = tid; t < nth; t += blockDim.x) {
+  const float umax = warp_max(mx);
+  __syncwarp();
+  for (int t = lane; t < nth; t += 32) {
     float s = 0.0f;
     for (int k = 0; k < nk; ++k) s += ue[k * nth + t];
     dsum[t] = s;
   }
-  for (int k = tid; k < nk; k += blockDim.x) {
+  const float floor = fmaxf(umax * 1e-12f, 1e-30f);
+  for (int k = lane; k < nk; k += 32) {
     float m = 0.0f;
-    for (int t = 0; t < nth; ++t) m = fmaxf(m, ue[k * nth + t]);
+    const float* row = ue + k * nth;
+    for (int t = 0; t < nth; ++t) m = fmaxf(m, row[t]);
     rmax[k] = m;
+    // the row's largest cubic term, ln(AF11 u^3)
+    lw[k] = 3.0f * __logf(fmaxf(m, floor)) + 11.0f * __logf(__ldg(g.sig + k) * kTpiInvF);
   }
-  if (tid == 0) s_cons = cons_of(g, __ldg(kdm + ip));
-  __syncthreads();
-  // Per row: the largest cubic term ln(AF11 u^3) of the row (u its largest UE) ...
-  for (int k = tid; k < nk; k += blockDim.x)
-    lw[k] = 3.0f * logf(fmaxf(rmax[k], fmaxf(umax * 1e-12f, 1e-30f))) +
-            11.0f * logf(__ldg(g.sig + k) * kTpiInvF);
-  __syncthreads();
-  // ... and lambda(k) = ln CONS + ln CONX(k) + the largest such term within kReach rows of k
-  // (the rows whose quadruplets reach row k), so S(k, .) e^-lambda is of order one; then the
-  // row's weight in the Hs tendency.
+  __syncwarp();
+  // Dominant direction (lowest index on ties), then which side of it is heavier.
+  float bv = -1.0f;
+  int bi = 0;
+  for (int t = lane; t < nth; t += 32)
+    if (dsum[t] > bv) {
+      bv = dsum[t];
+      bi = t;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  float up = 0.0f, lo = 0.0f;
+  for (int j = 1 + lane; j < (nth + 1) / 2; j += 32) {
+    int cu = bi + j, cl = bi - j;
+    if (cu >= nth) cu -= nth;
+    if (cl < 0) cl += nth;
+    up += dsum[cu];
+    lo += dsum[cl];
+  }
+  up = warp_sum(up);
+  lo = warp_sum(lo);
+  const int packed = bi | (lo > up ? 1 << 16 : 0);
+  const float kd = __ldg(kdm + ip);
+  const float cons = cons_of(g, kd);
+  const float lcons = __logf(cons);
+  // lambda(k) = ln CONS + ln CONX(k) + the largest cubic term within kReach rows of k (the rows
+  // whose quadruplets reach row k): S(k, .) e^-lambda is of order one.
   constexpr int kReach = 5;
-  for (int k = tid; k < nk; k += blockDim.x) {
+  for (int k = lane; k < nk; k += 32) {
     float l = -INFINITY;
     for (int q = max(0, k - kReach); q <= min(nk - 1, k + kReach); ++q) l = fmaxf(l, lw[q]);
-    pp[k] = umax > 0.0f ? logf(s_cons) + logf(conx[k]) + l : -1e30f;
+    lam[k] = umax > 0.0f ? lcons - __logf(rcon[k]) + l : -1e30f;
   }
-  __syncthreads();
-  for (int k = tid; k < nk; k += blockDim.x)
-    lw[k] = pp[k] + ln_dden(g, __ldg(g.sig + k)) - logf(__ldg(cg + static_cast<size_t>(ip) * nk + k));
-  __syncthreads();
-  if (tid == 0) {
-    int best = 0;
-    for (int t = 1; t < nth; ++t)
-      if (dsum[t] > dsum[best]) best = t;
-    float up = 0.0f, lo = 0.0f;
-    for (int j = 1; j < (nth + 1) / 2; ++j) {
-      up += dsum[(best + j) % nth];
-      lo += dsum[(best + nth - j) % nth];
-    }
-    const int packed = best | (lo > up ? 1 << 16 : 0);
-    s_shift = packed;
-    shift[ip] = packed;
-    float lmax = -INFINITY;
-    for (int k = 0; k < nk; ++k) lmax = fmaxf(lmax, lw[k]);
-    red[0] = lmax;
-    // Depth features: ln kdmean and the relative depth factor of CONS.
-    const float kd = __ldg(kdm + ip);
-    __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
-    if (g.din > nspec) xr[nspec] = __float2bfloat16_rn(logf(fmaxf(kd, 1e-2f)) * 0.2f);
-    if (g.din > nspec + 1) xr[nspec + 1] = __float2bfloat16_rn(s_cons / g.snlc1 - 1.0f);
+  __syncwarp();
+  // The row's weight in the Hs tendency, e^lambda DDEN / CG, scaled by its largest value.
+  float wmax = -INFINITY;
+  for (int k = lane; k < nk; k += 32) {
+    lw[k] = lam[k] + ln_dden(g, __ldg(g.sig + k)) - __logf(__ldg(cgp + k));
+    wmax = fmaxf(wmax, lw[k]);
   }
-  __syncthreads();
-  for (int k = tid; k < nk; k += blockDim.x)
-    pp[nk + k] = umax > 0.0f ? expf(lw[k] - red[0]) : 0.0f;
-  const int sh = s_shift;
+  wmax = warp_max(wmax);
+  for (int k = lane; k < nk; k += 32) {
+    pp[k] = lam[k];
+    pp[nk + k] = umax > 0.0f ? __expf(lw[k] - wmax) : 0.0f;
+  }
+  if (lane == 0) shift[ip] = packed;
+  // The network input, row by row, two canonical columns per lane.
   const float inv = umax > 0.0f ? 1.0f / umax : 0.0f;
   __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
-  for (int i = tid; i < nspec; i += blockDim.x) {
-    const int k = i / nth, j = i % nth;
-    const float u = ue[k * nth + orig_col(sh, j, nth)] * inv;
-    xr[i] = __float2bfloat16_rn(logf(u + kInputFloor) * kInputScale + 1.0f);
+  const int sh = packed & 0xFFFF;
+  const bool flip = (packed >> 16) != 0;
+  auto col = [&](int j) {
+    int c = flip ? sh - j : sh + j;
+    if (c >= nth) c -= nth;
+    if (c < 0) c += nth;
+    return c;
+  };
+  if ((nth & 1) == 0) {
+    const int half = nth >> 1;
+    for (int k = 0; k < nk; ++k) {
+      const float* row = ue + k * nth;
+      for (int l = lane; l < half; l += 32) {
+        const float u0 = row[col(2 * l)] * inv, u1 = row[col(2 * l + 1)] * inv;
+        const float x0 = __logf(u0 + kInputFloor) * kInputScale + 1.0f;
+        const float x1 = __logf(u1 + kInputFloor) * kInputScale + 1.0f;
+        *reinterpret_cast<__nv_bfloat162*>(xr + k * nth + 2 * l) = __floats2bfloat162_rn(x0, x1);
+      }
+    }
+  } else {
+    for (int k = 0; k < nk; ++k)
+      for (int j = lane; j < nth; j += 32)
+        xr[k * nth + j] =
+            __float2bfloat16_rn(__logf(ue[k * nth + col(j)] * inv + kInputFloor) * kInputScale + 1.0f);
   }
-  for (int i = nspec + 2 + tid; i < g.din; i += blockDim.x) xr[i] = __float2bfloat16_rn(0.0f);
+  // Depth features: ln kdmean and the relative depth factor of CONS; zero padding.
+  for (int i = nspec + lane; i < g.din; i += 32) {
+    float v = 0.0f;
+    if (i == nspec) v = __logf(fmaxf(kd, 1e-2f)) * 0.2f;
+    if (i == nspec + 1) v = cons / g.snlc1 - 1.0f;
+    xr[i] = __float2bfloat16_rn(v);
+  }
 }
 
 // ------------------------------------------------------------------------------ target side
@@ -318,36 +373,40 @@ __global__ void targets_kernel(SurGrid g, int npts, const float* __restrict__ s,
 
 // ------------------------------------------------------------------------ inference output side
 
-__global__ void post_kernel(SurGrid g, GateParams gate, int npts, const float* __restrict__ out,
-                            int ldo, const float* __restrict__ ps, const int* __restrict__ shift,
-                            float* __restrict__ s, float* __restrict__ d,
-                            int* __restrict__ accepted, float* __restrict__ gv,
-                            int* __restrict__ rej_list, int* __restrict__ nrej,
-                            int* __restrict__ nrej_total) {
-  __shared__ float red[32];
-  __shared__ float scl[64], wgt[64];
-  const int ip = blockIdx.x, tid = threadIdx.x, nk = g.nk, nth = g.nth, nspec = g.nspec;
+__global__ void __launch_bounds__(32 * kPointsPerCta)
+    post_kernel(SurGrid g, GateParams gate, int npts, const float* __restrict__ out, int ldo,
+                const float* __restrict__ ps, const int* __restrict__ shift,
+                float* __restrict__ s, float* __restrict__ d, int* __restrict__ accepted,
+                float* __restrict__ gv, int* __restrict__ rej_list, int* __restrict__ nrej,
+                int* __restrict__ nrej_total) {
+  __shared__ float rows[kPointsPerCta][2][64];  // per warp: scale and Hs-tendency weight per row
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ip = blockIdx.x * kPointsPerCta + warp;
+  if (ip >= npts) return;  // warp-uniform
+  const int nk = g.nk, nth = g.nth, nspec = g.nspec;
   const float* op = out + static_cast<size_t>(ip) * ldo;
   const float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
-  for (int k = tid; k < nk; k += blockDim.x) {
+  float* const scl = rows[warp][0];
+  float* const wgt = rows[warp][1];
+  for (int k = lane; k < nk; k += 32) {
     const float rsk = __ldg(g.rowscale + k);
     scl[k] = rsk * expf(pp[k]);
     wgt[k] = rsk * pp[nk + k];
   }
-  __syncthreads();
+  __syncwarp();
   float r = 0.0f, gs = 0.0f;
-  for (int i = tid; i < nspec; i += blockDim.x) {
+  for (int i = lane; i < nspec; i += 32) {
     const float w = wgt[i / nth], v = op[i];
     r += w * v;
     gs += w * fabsf(v);
   }
-  r = block_sum(r, red);
-  gs = block_sum(gs, red);
+  r = warp_sum(r);
+  gs = warp_sum(gs);
   const float head = g.dout > nspec ? op[nspec] : -INFINITY;
   const float resid = gs > 0.0f ? fabsf(r) / gs : 0.0f;
   const bool ok = isfinite(r) && isfinite(gs) && isfinite(head) && resid <= gate.energy &&
                   head <= gate.log_err;
-  if (tid == 0) {
+  if (lane == 0) {
     if (accepted) accepted[ip] = ok ? 1 : 0;
     if (gv) {
       gv[2 * ip] = head;
@@ -362,10 +421,15 @@ __global__ void post_kernel(SurGrid g, GateParams gate, int npts, const float* _
   const int sh = shift[ip];
   float* sp = s + static_cast<size_t>(ip) * nspec;
   float* dp = d + static_cast<size_t>(ip) * nspec;
-  for (int i = tid; i < nspec; i += blockDim.x) {
-    const int k = i / nth, j = i % nth;
+  for (int i = lane; i < nspec; i += 32) {
+    const int k = i / nth, j = i - k * nth;
     sp[k * nth + orig_col(sh, j, nth)] = op[i] * scl[k];
-    dp[i] = 0.0f;
+  }
+  if ((nspec & 3) == 0 && (reinterpret_cast<uintptr_t>(dp) & 15) == 0) {
+    float4* d4 = reinterpret_cast<float4*>(dp);
+    for (int q = lane; q < nspec / 4; q += 32) d4[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  } else {
+    for (int i = lane; i < nspec; i += 32) dp[i] = 0.0f;
   }
 }
 
@@ -708,8 +772,17 @@ void prep(const SurGrid& g, int npts, const float* a, const float* cg, const flo
           __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st) {
   if (npts <= 0) return;
   if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "prep: NK above 64");
-  const size_t smem = (static_cast<size_t>(g.nspec) + 3 * g.nk + g.nth + 32) * sizeof(float);
-  prep_kernel<<<grid1(npts), kThreads, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, ps, shift);
+  const size_t smem =
+      static_cast<size_t>(kPointsPerCta) * prep_floats(g.nspec, g.nk, g.nth) * sizeof(float);
+  static size_t set = 48 * 1024;
+  if (smem > set) {
+    WWB_CHECK(cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    set = smem;
+  }
+  const unsigned blocks = static_cast<unsigned>((npts + kPointsPerCta - 1) / kPointsPerCta);
+  prep_kernel<<<blocks, 32 * kPointsPerCta, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, ps,
+                                                         shift);
   WWB_CHECK(cudaGetLastError());
 }
 
@@ -733,8 +806,9 @@ void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, 
           int* rej_list, int* nrej, int* nrej_total, cudaStream_t st) {
   if (npts <= 0) return;
   if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "post: NK above 64");
-  post_kernel<<<grid1(npts), kThreads, 0, st>>>(g, gate, npts, out, ldo, ps, shift, s, d,
-                                                 accepted, gv, rej_list, nrej, nrej_total);
+  const unsigned blocks = static_cast<unsigned>((npts + kPointsPerCta - 1) / kPointsPerCta);
+  post_kernel<<<blocks, 32 * kPointsPerCta, 0, st>>>(g, gate, npts, out, ldo, ps, shift, s, d,
+                                                      accepted, gv, rej_list, nrej, nrej_total);
   WWB_CHECK(cudaGetLastError());
 }
 

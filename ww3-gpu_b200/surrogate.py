@@ -180,6 +180,11 @@ class Surrogate:
                              _p(accepted), _stream(stream))
         self._ok(self.L.ww_sur_last_error(), "ww_snl1_gated")
 
+    def gated_host(self, npts, a, cg, kdmean, s, d):
+        """ww_snl1_gated_host on host arrays (numpy or page-locked torch tensors)."""
+        self.L.ww_snl1_gated_host(self.igrid, npts, _p(a), _p(cg), _p(kdmean), _p(s), _p(d))
+        self._ok(self.L.ww_sur_last_error(), "ww_snl1_gated_host")
+
     def forward(self, rows, x, out, stream=None):
         """The network alone on normalised inputs (the four GEMMs of one inference)."""
         self._ok(self.L.ww_sur_forward(self.igrid, rows, _p(x), _p(out), _stream(stream)),
