@@ -359,7 +359,7 @@ struct Sur {
   DBuf<bf16> xs;
   DBuf<float> ts, pss, tb_ps;
   // inference scratch (per chunk)
-  DBuf<float> ps, gv;
+  DBuf<float> ps, gv, gsum, head;
   DBuf<int> shift, rej, nrej, nrej_total;
   GateParams gate{0.05f, 1e30f};
   LossWeights lw{0.0f, 0.0f, 1};
@@ -405,6 +405,8 @@ void sur_scratch(Sur& s, int rows) {
   if (s.shift.n < static_cast<size_t>(rows)) {
     s.ps.alloc(static_cast<size_t>(rows) * 2 * s.g.nk);
     s.gv.alloc(static_cast<size_t>(rows) * 2);
+    s.gsum.alloc(static_cast<size_t>(rows) * 2);
+    s.head.alloc(rows);
     s.shift.alloc(rows);
     s.rej.alloc(rows);
   }
@@ -412,6 +414,42 @@ void sur_scratch(Sur& s, int rows) {
     s.nrej.alloc(1);
     s.nrej_total.alloc(1);
   }
+}
+
+/// One chunk (n <= kInferRows points) through the network with the fused output epilogue:
+/// S and D of every point, then the gate (rejected points listed in s.rej, counted in s.nrej).
+void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* kd, float* so,
+                   float* dd, int* accepted, float* gv, const GateParams& gate, int* total,
+                   cudaStream_t st) {
+  Mlp& m = s.net;
+  prep(s.g, n, a, cg, kd, m.ix0.p, m.din, s.ps.p, s.shift.p, st);
+  const bf16* in = m.ix0.p;
+  int kin = m.din;
+  for (int l = 0; l < 3; ++l) {
+    GemmArgs g = args(n, m.dh, kin, m);
+    g.bias = m.L[l].b.p;
+    g.out = m.ih[l & 1].p;
+    g.ldo = m.dh;
+    run_gemm(kEpiGeluInfer, g, make_operand(in, n, kin, kin, kBM),
+             make_operand(m.L[l].wb.p, m.dh, kin, kin, g.bn), st);
+    in = m.ih[l & 1].p;
+    kin = m.dh;
+  }
+  WWB_CHECK(cudaMemsetAsync(s.gsum.p, 0, static_cast<size_t>(n) * 2 * sizeof(float), st));
+  // D = 0 for every point (the surrogate does not model the diagonal term); the plain DIA
+  // overwrites the rejected points' D afterwards.
+  WWB_CHECK(cudaMemsetAsync(dd, 0, static_cast<size_t>(n) * s.g.nspec * sizeof(float), st));
+  GemmArgs g = args(n, m.dout, m.dh, m);
+  g.bias = m.L[3].b.p;
+  g.ldo = m.dout;
+  g.sur = SurOut{s.ps.p, s.shift.p, s.rowscale.p, so, dd, s.head.p, s.gsum.p, s.g.nspec,
+                 s.g.nth, s.g.nk};
+  const char* why = nullptr;
+  if (!sur_out_ok(g, &why)) throw CudaError(cudaErrorInvalidValue, why);
+  run_gemm(kEpiSurOut, g, make_operand(in, n, m.dh, m.dh, kBM),
+           make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, g.bn), st);
+  WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
+  gate_points(gate, n, s.gsum.p, s.head.p, accepted, gv, s.rej.p, s.nrej.p, total, st);
 }
 
 /// The surrogate's S for npts points (device arrays) into s/d, gated, with the plain DIA on the
@@ -428,11 +466,8 @@ void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* k
     const float* cp = cg + static_cast<size_t>(p0) * nk;
     float* sp = so + static_cast<size_t>(p0) * nspec;
     float* dp = dd + static_cast<size_t>(p0) * nspec;
-    prep(s.g, n, ap, cp, kd + p0, s.net.ix0.p, s.net.din, s.ps.p, s.shift.p, st);
-    mlp_forward_infer(s.net, n, st);
-    WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
-    post(s.g, gate, n, s.net.iout.p, s.net.dout, s.ps.p, s.shift.p, sp, dp,
-         accepted ? accepted + p0 : nullptr, nullptr, s.rej.p, s.nrej.p, s.nrej_total.p, st);
+    sur_chunk_out(s, n, ap, cp, kd + p0, sp, dp, accepted ? accepted + p0 : nullptr, nullptr,
+                  gate, s.nrej_total.p, st);
     if (fallback &&
         !launch_snl1_list(s.dia, n, s.rej.p, s.nrej.p, ap, cp, kd + p0, sp, dp, nullptr, st))
       throw CudaError(cudaErrorInvalidValue, "gated DIA: the band kernel cannot run this grid");
@@ -1073,13 +1108,10 @@ int ww_sur_calibrate(int igrid, int npts, unsigned long long seed, float bimodal
     for (int p0 = 0; p0 < npts; p0 += kInferRows) {
       const int n = std::min(kInferRows, npts - p0);
       sur_scratch(*s, n);
-      prep(s->g, n, a.p + static_cast<size_t>(p0) * nspec, cg.p + static_cast<size_t>(p0) * nk,
-           kd.p + p0, s->net.ix0.p, s->net.din, s->ps.p, s->shift.p, st);
-      mlp_forward_infer(s->net, n, st);
-      WWB_CHECK(cudaMemsetAsync(s->nrej.p, 0, sizeof(int), st));
-      post(s->g, open, n, s->net.iout.p, s->net.dout, s->ps.p, s->shift.p,
-           so.p + static_cast<size_t>(p0) * nspec, dd.p + static_cast<size_t>(p0) * nspec,
-           nullptr, s->gv.p, s->rej.p, s->nrej.p, nullptr, st);
+      sur_chunk_out(*s, n, a.p + static_cast<size_t>(p0) * nspec,
+                    cg.p + static_cast<size_t>(p0) * nk, kd.p + p0,
+                    so.p + static_cast<size_t>(p0) * nspec, dd.p + static_cast<size_t>(p0) * nspec,
+                    nullptr, s->gv.p, open, nullptr, st);
       // The gate's two inputs per point: the head (column NSPEC) and the energy residual.
       std::vector<float> gv(static_cast<size_t>(n) * 2);
       WWB_CHECK(cudaMemcpyAsync(gv.data(), s->gv.p, gv.size() * 4, cudaMemcpyDeviceToHost, st));

@@ -35,6 +35,36 @@ enum Epilogue : int {
   kEpiF32 = 3,        ///< out_f32 = acc + bias
   kEpiDGelu = 4,      ///< g = acc * gelu'(aux): out = bf16(g), out_t = transpose
   kEpiAtomic = 5,     ///< out_f32 += acc (split reduction, red.global.add)
+  kEpiSurOut = 6,     ///< the surrogate's output side: S and D of every row, gate sums (below)
+};
+
+/// The original direction of canonical column j: the spectrum was rotated by the low 16 bits
+/// of `packed` and, when bit 16 is set, reflected (j -> -j), so column 0 is its dominant
+/// direction and columns 1..NTH/2-1 its heavier side. The DIA commutes with both (its index
+/// tables are circulant in direction and symmetric under reflection).
+__host__ __device__ inline int orig_col(int packed, int j, int nth) {
+  const int sh = packed & 0xFFFF;
+  int c = (packed >> 16) ? sh - j : sh + j;
+  if (c >= nth) c -= nth;
+  if (c < 0) c += nth;
+  return c;
+}
+
+/// What kEpiSurOut needs besides the accumulator: per row m (a sea point) its scales ps
+/// (2 NK floats: lambda, then the Hs-tendency weights) and packed direction shift; per
+/// frequency row the target scale. Column i < NSPEC of row m is the normalised S of canonical
+/// bin i: S(m, k NTH + orig_col(shift, j)) = (acc + bias) rowscale(k) e^lambda(k) (D, all
+/// zero, is the caller's memset), and the gate sums sum w v, sum w |v| (w = rowscale(k) times the weight) are added into
+/// gsum[2m], gsum[2m+1]; column NSPEC is the error head, stored in head[m].
+struct SurOut {
+  const float* ps;
+  const int* shift;
+  const float* rowscale;
+  float* s;
+  float* d;  ///< unused by the kernel (kept for the caller's bookkeeping)
+  float* head;
+  float* gsum;
+  int nspec, nth, nk;
 };
 
 /// One GEMM launch. Operands are described by TMA tensor maps built by make_operand().
@@ -49,6 +79,7 @@ struct GemmArgs {
   float* out_f32;       ///< M x N, row stride ldo (kEpiF32, kEpiAtomic)
   int ldo, ldt;
   int* err;             ///< device status word: set when a bounded wait gave up
+  SurOut sur;           ///< kEpiSurOut only
 };
 
 /// A K-major bf16 operand: `rows` rows of `k` elements, `ld` elements apart, read in boxes of
@@ -61,6 +92,12 @@ Operand make_operand(const __nv_bfloat16* base, int rows, int k, int ld, int box
 
 /// Whether the shapes suit the kernel (tile multiples, alignment); on false `why` says what.
 bool gemm_shape_ok(const GemmArgs& g, const Operand& a, const Operand& b, const char** why);
+
+/// Whether a launch of epilogue `mode` with tile width `bn` fits in shared memory.
+bool gemm_fits(int mode, int bn);
+
+/// Whether g.sur is complete for a kEpiSurOut launch; on false `why` says what is missing.
+bool sur_out_ok(const GemmArgs& g, const char** why);
 
 /// C = A . B^T with epilogue `mode` on `stream` (persistent grid of at most `max_ctas` CTAs,
 /// 0 = one per SM). Throws CudaError on a launch failure.

@@ -1,7 +1,7 @@
 // ww3-gpu_b200/csrc/mlp_gemm.cu
 // The surrogate MLP's GEMM on B200's fifth-generation tensor cores.
 //
-// One persistent CTA per SM (192 threads, about 194 KB of shared memory) walks the output tiles
+// One persistent CTA per SM (320 threads, up to 227 KB of shared memory) walks the output tiles
 // (128 x bn, bn <= 256) of C = A . B^T in a static round-robin:
 //   warp 0, one lane: TMA producer. Per stage it brings a 128 x 64 tile of A and a bn x 64 tile
 //     of B (bf16, 128-byte swizzle) into a 4-deep shared-memory ring, completing on the stage's
@@ -10,10 +10,12 @@
 //     lane issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulation, M=128, N=bn, K=16
 //     per instruction, four per stage) and commits each stage back to the producer's "empty"
 //     barrier and each finished tile to the epilogue's "tfull" barrier.
-//   warps 2-5: the epilogue. Thread r of the four warps owns TMEM lane r (tile row r); it reads
-//     its row 32 columns at a time (tcgen05.ld 32x32b.x32), applies the mode's bias, GELU,
-//     GELU' or split-reduction add, stores, and releases the accumulator, so tile i's epilogue
-//     overlaps tile i+1's MMAs in the other accumulator.
+//   warps 2-9: the epilogue, two warps per TMEM lane quarter taking alternate 32-column chunks
+//     (so one warp's loads hide behind the other's work). A thread owns TMEM lane r (tile row
+//     r); it reads its row 32 columns at a time (tcgen05.ld 32x32b.x32), applies the mode's
+//     bias, GELU, GELU' or split-reduction add, stores (the fp32 and surrogate-output modes
+//     through a shared-memory staging tile, so the stores go out row by row, coalesced), and
+//     releases the accumulator, so tile i's epilogue overlaps tile i+1's MMAs in the other one.
 // Every mbarrier wait is bounded: a wait that gives up sets the caller's status word, its role
 // leaves its loop, and the roles it feeds give up in turn; before TMEM is freed the MMA lane
 // waits for its own MMAs and the producer for its own copies, so the CTA never exits with
@@ -30,10 +32,9 @@ namespace wwb {
 namespace mlp {
 namespace {
 
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, taking alternate 32-column chunks
+constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kTileA = kBM * kBK * 2;
-constexpr uint32_t kTileB = kBNMax * kBK * 2;
-constexpr uint32_t kStageBytes = kTileA + kTileB;
 constexpr uint32_t kTmemCols = 2 * kBNMax;
 constexpr uint32_t kSpin = 1u << 24;  // polls before a wait gives up (seconds, never in a normal run)
 
@@ -45,7 +46,29 @@ struct Bars {
   uint64_t drain;
   uint32_t tmem_base;
 };
-constexpr size_t kSmemBytes = 1024 + kStages * kStageBytes + sizeof(Bars) + 64;
+static_assert(sizeof(Bars) <= 256, "barriers must fit their 256-byte slot");
+// kEpiF32 and kEpiSurOut stage each epilogue warp's 32 x 32 chunk through shared memory (padded
+// rows), so a thread-per-row tile is stored row by row, lane = column (coalesced); kEpiSurOut
+// also keeps each row's per-frequency scale and weight for the frequency rows the tile covers.
+constexpr int kStageLd = 33;
+constexpr int kRowsPerTile = 8;  // frequency rows a tile of <= 256 columns covers when NTH >= 36
+constexpr size_t kStageBytes32 = kEpiWarps * 32 * kStageLd * sizeof(float);
+constexpr size_t kRowConstBytes = kEpiWarps * 32 * kRowsPerTile * 2 * sizeof(float);
+constexpr size_t kSmemMax = 227 * 1024;
+
+/// Bytes of one pipeline stage: the A tile and a bn-row B tile (a multiple of 1024).
+__host__ __device__ constexpr uint32_t stage_bytes(int bn) {
+  return kTileA + static_cast<uint32_t>(bn) * kBK * 2;
+}
+
+/// Dynamic shared memory of a launch: alignment slack, the stages, the barriers' 256-byte slot
+/// and the epilogue's staging areas.
+__host__ __device__ constexpr size_t smem_bytes(int mode, int bn) {
+  return 1024 + kStages * static_cast<size_t>(stage_bytes(bn)) + 256 +
+         (mode == kEpiSurOut ? kStageBytes32 + kRowConstBytes
+          : mode == kEpiF32  ? kStageBytes32
+                             : 0);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -193,12 +216,20 @@ __device__ __forceinline__ void store_col32(__nv_bfloat16* dst_t, int ldt, int n
   for (int j = 0; j < 32; ++j) dst_t[static_cast<size_t>(n + j) * ldt + m] = __float2bfloat16_rn(v[j]);
 }
 
+/// One thread's 32 columns of the other epilogues. `bl` is bias[n + lane] (the warp's lanes
+/// hold the chunk's 32 bias values, read once with one coalesced load); every lane calls this,
+/// rows m >= M store nothing.
 template <int MODE>
 __device__ __forceinline__ void epilogue_chunk(const GemmArgs& g, int m, int n,
-                                               const uint32_t (&r)[32]) {
+                                               const uint32_t (&r)[32], float bl) {
   float v[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+  if constexpr (MODE == kEpiGeluTrain || MODE == kEpiGeluInfer) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] += __shfl_sync(0xffffffffu, bl, j);
+  }
+  if (m >= g.M) return;
   const size_t row = static_cast<size_t>(m) * g.ldo + n;
   if constexpr (MODE == kEpiAtomic) {
 #pragma unroll
@@ -213,30 +244,99 @@ __device__ __forceinline__ void epilogue_chunk(const GemmArgs& g, int m, int n,
     if (g.out_t) store_col32(g.out_t, g.ldt, n, m, v);
     return;
   } else {
-    const float4* b4 = reinterpret_cast<const float4*>(g.bias + n);
+    if constexpr (MODE == kEpiGeluTrain) store_row32(g.aux + row, v);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float4 b = __ldg(b4 + q);
-      v[4 * q + 0] += b.x;
-      v[4 * q + 1] += b.y;
-      v[4 * q + 2] += b.z;
-      v[4 * q + 3] += b.w;
-    }
-    if constexpr (MODE == kEpiF32) {
-      float4* o = reinterpret_cast<float4*>(g.out_f32 + row);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      return;
-    } else {
-      if constexpr (MODE == kEpiGeluTrain) store_row32(g.aux + row, v);
-#pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
-      store_row32(g.out + row, v);
-      if constexpr (MODE == kEpiGeluTrain) {
-        if (g.out_t) store_col32(g.out_t, g.ldt, n, m, v);
-      }
+    for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+    store_row32(g.out + row, v);
+    if constexpr (MODE == kEpiGeluTrain) {
+      if (g.out_t) store_col32(g.out_t, g.ldt, n, m, v);
     }
   }
+}
+
+/// kEpiF32 through the staging tile: each thread puts its row's 32 values (plus bias) in the
+/// warp's tile, then the warp stores the 32 rows one by one, 128 contiguous bytes each.
+__device__ __forceinline__ void f32_chunk(const GemmArgs& g, int m_base, int n,
+                                          const uint32_t (&r)[32], float bl, float* tile,
+                                          int lane) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j)
+    tile[lane * kStageLd + j] = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
+  __syncwarp();
+  for (int rr = 0; rr < 32; ++rr) {
+    const int mr = m_base + rr;
+    if (mr < g.M) g.out_f32[static_cast<size_t>(mr) * g.ldo + n + lane] = tile[rr * kStageLd + lane];
+  }
+  __syncwarp();
+}
+
+/// kEpiSurOut, once per tile and thread: the scale e^lambda rowscale and the Hs-tendency weight
+/// of the thread's row (sea point m) for the frequency rows k0 .. k0 + kRowsPerTile - 1, into
+/// the warp's row-constant area (all loads issued before any is used).
+__device__ __forceinline__ void sur_row_consts(const GemmArgs& g, int m, int k0, float* rc,
+                                               int lane) {
+  const SurOut& o = g.sur;
+  const float* pp = o.ps + static_cast<size_t>(m < g.M ? m : 0) * 2 * o.nk;
+  float lam[kRowsPerTile], wt[kRowsPerTile], rs[kRowsPerTile];
+#pragma unroll
+  for (int t = 0; t < kRowsPerTile; ++t) {
+    const int k = k0 + t;
+    const bool in = m < g.M && k < o.nk;
+    lam[t] = in ? pp[k] : 0.0f;
+    wt[t] = in ? pp[o.nk + k] : 0.0f;
+    rs[t] = in ? __ldg(o.rowscale + k) : 0.0f;
+  }
+#pragma unroll
+  for (int t = 0; t < kRowsPerTile; ++t) {
+    rc[(lane * kRowsPerTile + t) * 2] = rs[t] * __expf(lam[t]);
+    rc[(lane * kRowsPerTile + t) * 2 + 1] = rs[t] * wt[t];
+  }
+}
+
+/// kEpiSurOut for one 32-column chunk of the warp's 32 rows (see SurOut in mlp.cuh). NTH >= 32,
+/// so the chunk's columns lie in at most two frequency rows: columns j < jb in row k, the rest
+/// in row k + 1. Each thread scales its own row's values into the warp's staging tile and adds
+/// its gate sums; then the warp writes the tile out row by row, lane = column, so a sea point's
+/// S stores (permuted within its frequency rows) are contiguous. (D = 0 is set by the caller
+/// with a memset of the whole chunk before the launch.)
+__device__ __forceinline__ void sur_chunk(const GemmArgs& g, int m_base, int n, int k0,
+                                          const uint32_t (&r)[32], float bl, int my_shift,
+                                          float& racc, float& gacc, float* tile, const float* rc,
+                                          int lane) {
+  const SurOut& o = g.sur;
+  const int k = n / o.nth;
+  const int jb = (k + 1) * o.nth - n;  // first column of row k + 1 (>= 32: none)
+  const float* rc0 = rc + (lane * kRowsPerTile + (k - k0)) * 2;
+  const float s0 = rc0[0], w0 = rc0[1];
+  const float s1 = (k - k0 + 1 < kRowsPerTile) ? rc0[2] : 0.0f;
+  const float w1 = (k - k0 + 1 < kRowsPerTile) ? rc0[3] : 0.0f;
+  const int valid = o.nspec - n;  // columns below NSPEC in this chunk
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const float v = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
+    const bool second = j >= jb;
+    const float sk = second ? s1 : s0, wk = second ? w1 : w0;
+    const bool in = j < valid;
+    racc += in ? wk * v : 0.0f;
+    gacc += in ? wk * fabsf(v) : 0.0f;
+    tile[lane * kStageLd + j] = in ? v * sk : v;
+  }
+  __syncwarp();
+  const int i = n + lane;
+  const int kj = i / o.nth, jl = i - kj * o.nth;
+  const bool col_in = i < o.nspec;
+  for (int rr = 0; rr < 32; ++rr) {
+    const int mr = m_base + rr;
+    const int shr = __shfl_sync(0xffffffffu, my_shift, rr);
+    if (mr < g.M) {
+      const float v = tile[rr * kStageLd + lane];
+      if (col_in)
+        o.s[static_cast<size_t>(mr) * o.nspec + kj * o.nth + orig_col(shr, jl, o.nth)] = v;
+      else if (i == o.nspec && o.head)
+        o.head[mr] = v;
+    }
+  }
+  __syncwarp();
 }
 
 struct Unit {
@@ -259,7 +359,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* const smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-  Bars* const bars = reinterpret_cast<Bars*>(smem + kStages * kStageBytes);
+  const uint32_t stage_sz = stage_bytes(g.bn);
+  Bars* const bars = reinterpret_cast<Bars*>(smem + kStages * stage_sz);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   const int m_tiles = (g.M + kBM - 1) / kBM;
@@ -275,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&bars->tfull[b], 1);
-      mbar_init(&bars->tempty[b], 4);  // one arrival per epilogue warp
+      mbar_init(&bars->tempty[b], kEpiWarps);  // one arrival per epilogue warp
     }
     mbar_init(&bars->drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -307,7 +408,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = false;
             break;
           }
-          uint8_t* const sa = smem + s * kStageBytes;
+          uint8_t* const sa = smem + s * stage_sz;
           mbar_expect_tx(&bars->full[s], tx);
           const int kx = (w.ks * kb_per + kb) * kBK;
           tma_load_2d(sa, &ta, &bars->full[s], kx, w.mt * kBM);
@@ -348,7 +449,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t a_addr = smem_u32(smem + s * kStageBytes);
+          const uint32_t a_addr = smem_u32(smem + s * stage_sz);
           const uint32_t b_addr = a_addr + kTileA;
 #pragma unroll
           for (int j = 0; j < kBK / 16; ++j)
@@ -364,7 +465,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     const int q = warp & 3;  // the TMEM lane quarter this warp may read
+    const int ew = warp - 2, half = ew >> 2;  // epilogue warp; its chunks c = half, half + 2, ...
     const int row = q * 32 + lane;
+    float* const tile = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256) +
+                        static_cast<size_t>(ew) * 32 * kStageLd;
+    float* const rowc = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256 +
+                                                 kStageBytes32) +
+                        static_cast<size_t>(ew) * 32 * kRowsPerTile * 2;
     uint32_t local = 0;
     bool ok = true;
     for (int u = blockIdx.x; u < units; u += gridDim.x, ++local) {
@@ -378,10 +485,41 @@ __global__ void __launch_bounds__(kThreads, 1)
       tc_fence_after();
       const int m = w.mt * kBM + row;
       const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16) + b * kBNMax;
-      for (int c = 0; c < g.bn / 32; ++c) {
-        uint32_t r[32];
-        tmem_ld32(tbase + 32u * c, r);
-        if (m < g.M) epilogue_chunk<MODE>(g, m, w.nt * g.bn + 32 * c, r);
+      const int nchunks = g.bn / 32;
+      constexpr bool kBias = MODE == kEpiGeluTrain || MODE == kEpiGeluInfer ||
+                             MODE == kEpiF32 || MODE == kEpiSurOut;
+      if constexpr (MODE == kEpiSurOut) {
+        const int my_shift = m < g.M ? __ldg(g.sur.shift + m) : 0;
+        const int k0 = (w.nt * g.bn) / g.sur.nth;
+        sur_row_consts(g, m, k0, rowc, lane);
+        float racc = 0.0f, gacc = 0.0f;
+        for (int c = half; c < nchunks; c += 2) {
+          const int n = w.nt * g.bn + 32 * c;
+          const float bl = __ldg(g.bias + n + lane);
+          uint32_t r[32];
+          tmem_ld32(tbase + 32u * c, r);
+          sur_chunk(g, w.mt * kBM + q * 32, n, k0, r, bl, my_shift, racc, gacc, tile, rowc, lane);
+        }
+        if (m < g.M) {
+          atomicAdd(g.sur.gsum + 2 * m, racc);
+          atomicAdd(g.sur.gsum + 2 * m + 1, gacc);
+        }
+      } else if constexpr (MODE == kEpiF32) {
+        for (int c = half; c < nchunks; c += 2) {
+          const int n = w.nt * g.bn + 32 * c;
+          const float bl = __ldg(g.bias + n + lane);
+          uint32_t r[32];
+          tmem_ld32(tbase + 32u * c, r);
+          f32_chunk(g, w.mt * kBM + q * 32, n, r, bl, tile, lane);
+        }
+      } else {
+        for (int c = half; c < nchunks; c += 2) {
+          const int n = w.nt * g.bn + 32 * c;
+          const float bl = kBias ? __ldg(g.bias + n + lane) : 0.0f;
+          uint32_t r[32];
+          tmem_ld32(tbase + 32u * c, r);
+          epilogue_chunk<MODE>(g, m, n, r, bl);
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -420,10 +558,12 @@ EncodeTiled encode_tiled() {
 template <int MODE>
 void launch(const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t stream,
             int max_ctas) {
+  const size_t smem = smem_bytes(MODE, g.bn);
+  if (smem > kSmemMax) throw CudaError(cudaErrorInvalidValue, "GEMM tile needs too much shared memory");
   static std::once_flag once;
   std::call_once(once, [] {
     WWB_CHECK(cudaFuncSetAttribute(gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(kSmemBytes)));
+                                   static_cast<int>(kSmemMax)));
   });
   const int m_tiles = (g.M + kBM - 1) / kBM;
   const int units = m_tiles * (g.N / g.bn) * (MODE == kEpiAtomic ? g.splits : 1);
@@ -431,7 +571,7 @@ void launch(const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t 
   if (sms <= 0) WWB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
   int grid = max_ctas > 0 ? max_ctas : sms;
   if (grid > units) grid = units;
-  gemm_kernel<MODE><<<grid, kThreads, kSmemBytes, stream>>>(a.map, b.map, g);
+  gemm_kernel<MODE><<<grid, kThreads, smem, stream>>>(a.map, b.map, g);
   WWB_CHECK(cudaGetLastError());
 }
 
@@ -472,6 +612,23 @@ bool gemm_shape_ok(const GemmArgs& g, const Operand& a, const Operand& b, const 
   return true;
 }
 
+bool gemm_fits(int mode, int bn) { return smem_bytes(mode, bn) <= kSmemMax; }
+
+bool sur_out_ok(const GemmArgs& g, const char** why) {
+  auto no = [&](const char* w) {
+    if (why) *why = w;
+    return false;
+  };
+  const SurOut& o = g.sur;
+  if (!o.ps || !o.shift || !o.rowscale || !o.s || !o.gsum || !g.bias)
+    return no("surrogate output: missing array");
+  if (o.nth < 32 || o.nk < 1 || o.nspec != o.nk * o.nth || g.N <= o.nspec)
+    return no("surrogate output: shape (NTH >= 32, an error-head column after NSPEC)");
+  if ((g.bn + o.nth - 1) / o.nth + 1 > kRowsPerTile)
+    return no("surrogate output: a tile covers more frequency rows than the epilogue keeps");
+  return true;
+}
+
 void gemm(int mode, const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t stream,
           int max_ctas) {
   switch (mode) {
@@ -480,6 +637,7 @@ void gemm(int mode, const GemmArgs& g, const Operand& a, const Operand& b, cudaS
     case kEpiF32: launch<kEpiF32>(g, a, b, stream, max_ctas); break;
     case kEpiDGelu: launch<kEpiDGelu>(g, a, b, stream, max_ctas); break;
     case kEpiAtomic: launch<kEpiAtomic>(g, a, b, stream, max_ctas); break;
+    case kEpiSurOut: launch<kEpiSurOut>(g, a, b, stream, max_ctas); break;
     default: throw CudaError(cudaErrorInvalidValue, "unknown GEMM epilogue");
   }
 }

@@ -6,6 +6,7 @@
 
 #include <cmath>
 
+#include "mlp.cuh"
 #include "mlp_ops.cuh"
 #include "wwb_common.hpp"
 
@@ -153,17 +154,6 @@ __global__ void synth_kernel(SurGrid g, SynthDraw dr, long long p0, int npts, fl
 
 // ------------------------------------------------------------------------- input normalisation
 
-/// The original direction of canonical column j: the spectrum is rotated by `sh` and, when
-/// bit 16 of the packed shift is set, reflected (j -> -j), so column 0 is its dominant
-/// direction and columns 1..NTH/2-1 its heavier side. The DIA commutes with both (its index
-/// tables are circulant in direction and symmetric under reflection).
-__device__ __forceinline__ int orig_col(int packed, int j, int nth) {
-  const int sh = packed & 0xFFFF;
-  int c = (packed >> 16) ? sh - j : sh + j;
-  c %= nth;
-  return c < 0 ? c + nth : c;
-}
-
 /// ln of the quadrature weight DDEN(k) = DTH * DSII(k) * SIG(k), DSII = SIG (XFR - 1/XFR) / 2.
 __device__ __forceinline__ float ln_dden(const SurGrid& g, float sig) {
   return logf(g.dth * 0.5f * sig * (g.xfr - 1.0f / g.xfr) * sig);
@@ -210,10 +200,18 @@ __global__ void __launch_bounds__(32 * kPointsPerCta)
   if ((nth & 3) == 0 && (reinterpret_cast<uintptr_t>(ap) & 15) == 0) {
     const float4* a4 = reinterpret_cast<const float4*>(ap);
     float4* u4 = reinterpret_cast<float4*>(ue);
-    const int q4 = nth >> 2;
+    // Row of float4 q = lane + 32 t, tracked without a division per step.
+    const int q4 = nth >> 2, dk = 32 / q4, dr = 32 % q4;
+    int kq = lane / q4, rq = lane % q4;
     for (int q = lane; q < nspec / 4; q += 32) {
       float4 v = __ldg(a4 + q);
-      const float r = rcon[q / q4];
+      const float r = rcon[kq];
+      rq += dr;
+      kq += dk;
+      if (rq >= q4) {
+        rq -= q4;
+        ++kq;
+      }
       v.x *= r;
       v.y *= r;
       v.z *= r;
@@ -308,14 +306,20 @@ __global__ void __launch_bounds__(32 * kPointsPerCta)
     return c;
   };
   if ((nth & 1) == 0) {
-    const int half = nth >> 1;
-    for (int k = 0; k < nk; ++k) {
+    // Pairs of canonical bins (2p, 2p + 1), p = lane, lane + 32, ...: both in row k, column j.
+    int j = (2 * lane) % nth, k = (2 * lane) / nth;
+    const int dk = 64 / nth, dj = 64 % nth;
+    for (int i = 2 * lane; i < nspec; i += 64) {
       const float* row = ue + k * nth;
-      for (int l = lane; l < half; l += 32) {
-        const float u0 = row[col(2 * l)] * inv, u1 = row[col(2 * l + 1)] * inv;
-        const float x0 = __logf(u0 + kInputFloor) * kInputScale + 1.0f;
-        const float x1 = __logf(u1 + kInputFloor) * kInputScale + 1.0f;
-        *reinterpret_cast<__nv_bfloat162*>(xr + k * nth + 2 * l) = __floats2bfloat162_rn(x0, x1);
+      const float u0 = row[col(j)] * inv, u1 = row[col(j + 1)] * inv;
+      const float x0 = __logf(u0 + kInputFloor) * kInputScale + 1.0f;
+      const float x1 = __logf(u1 + kInputFloor) * kInputScale + 1.0f;
+      *reinterpret_cast<__nv_bfloat162*>(xr + i) = __floats2bfloat162_rn(x0, x1);
+      j += dj;
+      k += dk;
+      if (j >= nth) {
+        j -= nth;
+        ++k;
       }
     }
   } else {
@@ -373,63 +377,25 @@ __global__ void targets_kernel(SurGrid g, int npts, const float* __restrict__ s,
 
 // ------------------------------------------------------------------------ inference output side
 
-__global__ void __launch_bounds__(32 * kPointsPerCta)
-    post_kernel(SurGrid g, GateParams gate, int npts, const float* __restrict__ out, int ldo,
-                const float* __restrict__ ps, const int* __restrict__ shift,
-                float* __restrict__ s, float* __restrict__ d, int* __restrict__ accepted,
-                float* __restrict__ gv, int* __restrict__ rej_list, int* __restrict__ nrej,
-                int* __restrict__ nrej_total) {
-  __shared__ float rows[kPointsPerCta][2][64];  // per warp: scale and Hs-tendency weight per row
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ip = blockIdx.x * kPointsPerCta + warp;
-  if (ip >= npts) return;  // warp-uniform
-  const int nk = g.nk, nth = g.nth, nspec = g.nspec;
-  const float* op = out + static_cast<size_t>(ip) * ldo;
-  const float* pp = ps + static_cast<size_t>(ip) * 2 * nk;
-  float* const scl = rows[warp][0];
-  float* const wgt = rows[warp][1];
-  for (int k = lane; k < nk; k += 32) {
-    const float rsk = __ldg(g.rowscale + k);
-    scl[k] = rsk * expf(pp[k]);
-    wgt[k] = rsk * pp[nk + k];
-  }
-  __syncwarp();
-  float r = 0.0f, gs = 0.0f;
-  for (int i = lane; i < nspec; i += 32) {
-    const float w = wgt[i / nth], v = op[i];
-    r += w * v;
-    gs += w * fabsf(v);
-  }
-  r = warp_sum(r);
-  gs = warp_sum(gs);
-  const float head = g.dout > nspec ? op[nspec] : -INFINITY;
+__global__ void gate_kernel(GateParams gate, int npts, const float* __restrict__ gsum,
+                            const float* __restrict__ head, int* __restrict__ accepted,
+                            float* __restrict__ gv, int* __restrict__ rej_list,
+                            int* __restrict__ nrej, int* __restrict__ nrej_total) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= npts) return;
+  const float r = gsum[2 * ip], gs = gsum[2 * ip + 1];
+  const float h = head ? head[ip] : -INFINITY;
   const float resid = gs > 0.0f ? fabsf(r) / gs : 0.0f;
-  const bool ok = isfinite(r) && isfinite(gs) && isfinite(head) && resid <= gate.energy &&
-                  head <= gate.log_err;
-  if (lane == 0) {
-    if (accepted) accepted[ip] = ok ? 1 : 0;
-    if (gv) {
-      gv[2 * ip] = head;
-      gv[2 * ip + 1] = resid;
-    }
-    if (!ok) {
-      rej_list[atomicAdd(nrej, 1)] = ip;
-      if (nrej_total) atomicAdd(nrej_total, 1);
-    }
+  const bool ok = isfinite(r) && isfinite(gs) && isfinite(h) && resid <= gate.energy &&
+                  h <= gate.log_err;
+  if (accepted) accepted[ip] = ok ? 1 : 0;
+  if (gv) {
+    gv[2 * ip] = h;
+    gv[2 * ip + 1] = resid;
   }
-  if (!ok) return;  // the plain DIA writes this point's S and D
-  const int sh = shift[ip];
-  float* sp = s + static_cast<size_t>(ip) * nspec;
-  float* dp = d + static_cast<size_t>(ip) * nspec;
-  for (int i = lane; i < nspec; i += 32) {
-    const int k = i / nth, j = i - k * nth;
-    sp[k * nth + orig_col(sh, j, nth)] = op[i] * scl[k];
-  }
-  if ((nspec & 3) == 0 && (reinterpret_cast<uintptr_t>(dp) & 15) == 0) {
-    float4* d4 = reinterpret_cast<float4*>(dp);
-    for (int q = lane; q < nspec / 4; q += 32) d4[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  } else {
-    for (int i = lane; i < nspec; i += 32) dp[i] = 0.0f;
+  if (!ok) {
+    rej_list[atomicAdd(nrej, 1)] = ip;
+    if (nrej_total) atomicAdd(nrej_total, 1);
   }
 }
 
@@ -801,14 +767,12 @@ void targets(const SurGrid& g, int npts, const float* s, const float* ps, const 
   WWB_CHECK(cudaGetLastError());
 }
 
-void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, int ldo,
-          const float* ps, const int* shift, float* s, float* d, int* accepted, float* gv,
-          int* rej_list, int* nrej, int* nrej_total, cudaStream_t st) {
+void gate_points(const GateParams& gate, int npts, const float* gsum, const float* head,
+                 int* accepted, float* gv, int* rej_list, int* nrej, int* nrej_total,
+                 cudaStream_t st) {
   if (npts <= 0) return;
-  if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "post: NK above 64");
-  const unsigned blocks = static_cast<unsigned>((npts + kPointsPerCta - 1) / kPointsPerCta);
-  post_kernel<<<blocks, 32 * kPointsPerCta, 0, st>>>(g, gate, npts, out, ldo, ps, shift, s, d,
-                                                      accepted, gv, rej_list, nrej, nrej_total);
+  gate_kernel<<<(npts + 255) / 256, 256, 0, st>>>(gate, npts, gsum, head, accepted, gv, rej_list,
+                                                  nrej, nrej_total);
   WWB_CHECK(cudaGetLastError());
 }
 

@@ -74,13 +74,13 @@ void rowscale_acc(const SurGrid& g, int npts, const float* s, const float* ps, d
 void targets(const SurGrid& g, int npts, const float* s, const float* ps, const int* shift,
              float* t, int ldt, cudaStream_t st);
 
-/// Output side of inference: S (de-normalised, rotated back) and D = 0 for accepted points, the
-/// compacted list of rejected points (count at *nrej, zeroed by the caller; also added to
-/// *nrej_total when given), per-point flag, and (gv, may be null) each point's head output and
-/// energy residual.
-void post(const SurGrid& g, const GateParams& gate, int npts, const float* out, int ldo,
-          const float* ps, const int* shift, float* s, float* d, int* accepted, float* gv,
-          int* rej_list, int* nrej, int* nrej_total, cudaStream_t st);
+/// The gate of every point after the fused output epilogue (kEpiSurOut): from its gate sums
+/// (gsum, 2 per point) and head output, accept or add it to the compacted rejected list
+/// (count at *nrej, zeroed by the caller; also added to *nrej_total when given); per-point flag
+/// and (gv, may be null) head and energy residual.
+void gate_points(const GateParams& gate, int npts, const float* gsum, const float* head,
+                 int* accepted, float* gv, int* rej_list, int* nrej, int* nrej_total,
+                 cudaStream_t st);
 
 /// Training loss and the output gradient. out (m x ldo fp32), t (m x ldt): grad (m x dout bf16)
 /// = dL/dout; loss (3 floats: MSE, energy-budget, error-head terms) accumulated.
