@@ -17,7 +17,7 @@ Five workloads (--workload):
   e2e    -- the public host entry (ww_srce_batch / ww_snl1) on page-locked host buffers:
             host->device copies of the step's inputs and device->host copies of its results
             inside every step.
-  roofline -- the kernel's algorithmic HBM bytes per point (W3SRCE: 10,908 B = spectrum in and
+  roofline -- the kernel's algorithmic HBM bytes per point (W3SRCE: 10,928 B = spectrum in and
             out, WN1/CG1, the PIN/PSC packets, WHITECAP/TAUBBL/TAUICE, SHAVE; DIA: 15,700 B) per
             launch over its CUDA-event duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
   cpu_baseline -- the reference's own C++ (oracle/_ref, compiled from its sources) on this
@@ -66,7 +66,7 @@ UNIT = "sea-point*steps/s"
 WORKLOAD = ("W3SNL1 DIA 36x36 (config 0 spectra: deep-water JONSWAP, d=4000 m), "
             f"{NPTS_PER_GPU} sea points per GPU")
 SRCE_NPTS = 9520
-SRCE_BYTES_PER_POINT = 4 * (2 * NK * NTH + 2 * NK + 7 + 2 * 22 + 2 * 8 + 1)  # 10,908
+SRCE_BYTES_PER_POINT = 4 * (2 * NK * NTH + 2 * NK + 7 + 2 * 22 + 2 * 8 + 1)  # 10,928
 SRCE_WORKLOAD = ("W3SRCE + ST4 (W3SIN4, W3SDS4, W3SPR4) + DIA + W3SBT1 + W3SDB1, 36x36, "
                  f"{SRCE_NPTS} sea points per GPU, DTG 900 s with dynamic substeps")
 
@@ -402,9 +402,10 @@ def srce_inputs(synth, npts, seed):
     return st, t, sr, cfg, sig, pts
 
 
-def srce_config(args, world):
-    return {"workload": SRCE_WORKLOAD, "nk": NK, "nth": NTH, "npts_per_gpu": args.npts,
-            "global_points": args.npts * world, "dtg_s": 900.0,
+def srce_config(args, world, npts=None):
+    npts = npts or args.npts
+    return {"workload": SRCE_WORKLOAD, "nk": NK, "nth": NTH, "npts_per_gpu": npts,
+            "global_points": npts * world, "dtg_s": 900.0,
             "depth_m": "log-uniform 10-4000", "u10_ms": "U(3, 25)", "seed": 2026,
             "st4": "saturation breaking with the cumulative term, analytic high-frequency tail",
             "l2": ("every step restores its 55 MB of inputs and writes a 256 MB buffer (L2 flush) "
@@ -595,7 +596,7 @@ def run_b200_srce(args, quiet=False, npts=None, steps=None, warmup=None, igrid=1
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": srce_config(args, world),
+        "config": srce_config(args, world, npts),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * per_pt_in * npts,
                 "d2h_bytes_per_step": 4 * per_pt_out * npts, "steps": e2e_steps,
                 "host_entry": "ww_srce_batch", "matches_device_entry": same},
@@ -708,11 +709,23 @@ def run_b200_step(args):
         grid.batch_va(nsea, v, jsea, pk["wn1"], pk["cg1"], pk["pin"], pk["psc"], pk["whitecap"],
                       pk["taubbl"], pk["tauice"], shave)
 
-    one = step_calls((lambda c, it, v: pkg.ktp3_batch(c, it, 1, ig, v),
-                      lambda c, v: pkg.xyp3_batch(c, ig, v), srce), va, kc, xc, pts, nsea)
-    step = pkg.Step(ig)
-    with step:
-        one()
+    va0 = np.array(va, copy=True)
+    L = pkg.lib()
+    calls = (lambda c, it, v: pkg.ktp3_batch(c, it, 1, ig, v),
+             lambda c, v: pkg.xyp3_batch(c, ig, v), srce)
+
+    def fresh_step():
+        """The step recorded from the initial state: VA and per-point packets as generated, so
+        the device-timed run and the end-to-end run time the same steps."""
+        if L.ww_va_state(ig) >= 0:  # the host takes the VA back before it writes it
+            assert L.ww_va_host_write(ig, va.ctypes.data, va.shape[1], va.shape[0] - 1) == 0
+        va[...] = va0
+        st_ = pkg.Step(ig)
+        with st_:
+            step_calls(calls, va, kc, xc, pts, nsea)()
+        return st_
+
+    step = fresh_step()
     nodes = step.nodes()
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -746,9 +759,11 @@ def run_b200_step(args):
     per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     value = nsea * world * args.steps / (total_ms / 1e3)
 
-    # ---- end to end: the host VA uploaded, the step, the VA read back, every step
-    e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
-    L = pkg.lib()
+    # ---- end to end: the same steps from the same initial state (re-recorded), with the host
+    # VA uploaded before and read back after every step
+    e2e_steps = args.steps
+    step.free()
+    step = fresh_step()
     hva = va  # the Fortran array the resident VA mirrors
 
     def host_step():
@@ -756,7 +771,9 @@ def run_b200_step(args):
         step.run(1, None)
         assert L.ww_va_host_read(ig, hva.ctypes.data, hva.shape[1], hva.shape[0] - 1) == 0
 
-    host_step()
+    for _ in range(args.warmup):
+        step.run(1, None)
+    assert L.ww_va_host_read(ig, hva.ctypes.data, hva.shape[1], hva.shape[0] - 1) == 0
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):

@@ -284,7 +284,8 @@ int ww_utrn(int nx, int ny, int nsea, int trflag, float fice0, float ficen, floa
  * inputs copied to device buffers the step owns, but their kernels do not run: they are
  * recorded, in call order. ww_step_end captures them into one CUDA graph; ww_step_run replays
  * it nrep times on the resident VA (state DEVICE afterwards) on `stream` (NULL: the library's
- * stream, synchronised before returning), with no host work and no copies. Each replay repeats
+ * stream, synchronised before returning), with no host work and no copies besides one upload of
+ * the VA when the host holds the newer copy (after ww_va_host_write). Each replay repeats
  * the recorded calls with their recorded scalars (the time of day, the boundary times, DTG);
  * W3SRCE's per-point packets (PSC, WHITECAP, TAUBBL, TAUICE, SHAVE) and W3KTP3's CFL maxima stay
  * on the device, the packets carrying over from one replay to the next. ww_xyp3_batch_mpi is not

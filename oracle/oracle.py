@@ -45,12 +45,19 @@ class Snl1Config(ctypes.Structure):
         return cls(*[m[k] for k in cls.FIELDS])
 
 
+def reference_root():
+    """Where the reference checkout is: the WW_REFERENCE_ROOT environment variable, else a
+    checkout named `reference` beside this repository."""
+    env = os.environ.get("WW_REFERENCE_ROOT")
+    return pathlib.Path(env) if env else HERE.parent.parent / "reference"
+
+
 def build():
     """Compile liboracle.so (always) and the reference build (when the reference is present)."""
     import subprocess
 
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    ref = pathlib.Path(os.environ.get("WW_REFERENCE_ROOT", "/root/reference"))
+    ref = reference_root()
     if (ref / "kokkos/src/ww_kokkos/snl1_team.hpp").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
 

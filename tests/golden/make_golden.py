@@ -13,6 +13,7 @@ Run it where the reference is mounted:
 The .npz it writes is committed, so the tests never read the reference at run time.
 """
 
+import os
 import pathlib
 import sys
 
@@ -70,7 +71,12 @@ def read_bin(path):
 
 
 def main():
-    root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        root = pathlib.Path(sys.argv[1])
+    elif os.environ.get("WW_REFERENCE_ROOT"):
+        root = pathlib.Path(os.environ["WW_REFERENCE_ROOT"])
+    else:
+        root = pathlib.Path(__file__).resolve().parents[3] / "reference"
     src = root / "kokkos/tests/fixtures/snl1_nk25_nth24.bin"
     dst = pathlib.Path(__file__).with_name("snl1_nk25_nth24.npz")
     g = read_bin(src)

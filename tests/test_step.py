@@ -34,6 +34,8 @@ def _bind(L):
     L.ww_srce_last_error.restype = I
     L.ww_va_host_read.argtypes = [I, P, I, I]
     L.ww_va_host_read.restype = I
+    L.ww_va_host_write.argtypes = [I, P, I, I]
+    L.ww_va_host_write.restype = I
     return L
 
 
@@ -150,6 +152,15 @@ def test_step_graph_equals_calls_and_reference(pkg, oracle, synth, case):
     step.run(nsteps)
     va_rec = c_rec.read()
     assert_bitexact(va_rec, va_ref, "VA, replayed graph vs the reference")
+    # the host takes the VA back and rewrites it (ww_va_host_write): the next replay uploads it
+    va0 = np.array(xc["va"], np.float32)
+    for calls in (c_ref, c_rec):
+        assert calls.L.ww_va_host_write(calls.ig, calls.va.ctypes.data, calls.va.shape[1],
+                                        calls.va.shape[0] - 1) == 0
+        calls.va[...] = va0
+    c_ref.step()
+    step.run(1)
+    assert_bitexact(c_rec.read(), c_ref.read(), "VA, replay after a host write vs the reference")
     step.free()
 
 

@@ -179,6 +179,10 @@ int ww_step_run(int igrid, int nrep, void* stream) {
     if (!r || r->recording || !r->exec)
       return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_run: no recorded step for this grid");
     if (nrep < 0) return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_run: nrep < 0");
+    // The host may have written its VA since the last call (ww_va_host_write): upload first.
+    if (nrep > 0)
+      if (int rc = va_device_current(igrid); rc != WW_KOKKOS_OK)
+        return g_step.fail(rc, "ww_step_run: the grid's VA could not be made current on the device");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : runtime().stream;
     for (int i = 0; i < nrep; ++i) WWB_CHECK(cudaGraphLaunch(r->exec, s));
     if (nrep > 0) va_device_written(igrid);
@@ -205,6 +209,10 @@ int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream) {
     // The grids' graphs one after another on one stream: a graph of all the grids' steps, as
     // branches side by side or chained, measured slower (the grids' persistent W3SRCE launches
     // compete for the same SMs when side by side).
+    if (nrep > 0)
+      for (int k = 0; k < ngrids; ++k)
+        if (int rc = va_device_current(igrids[k]); rc != WW_KOKKOS_OK)
+          return g_step.fail(rc, "ww_steps_run: a grid's VA could not be made current on the device");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : runtime().stream;
     for (int i = 0; i < nrep; ++i)
       for (StepRecorder* r : rs) WWB_CHECK(cudaGraphLaunch(r->exec, s));

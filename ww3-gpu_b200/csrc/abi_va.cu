@@ -470,6 +470,14 @@ void va_device_written(int igrid) {
   if (it != registry().end()) it->second.kernel_wrote();
 }
 
+int va_device_current(int igrid) {
+  return as_status([&]() {
+    auto it = registry().find(igrid);
+    if (it == registry().end()) return static_cast<int>(WW_KOKKOS_OK);
+    return it->second.kernel_access(true);
+  });
+}
+
 void release_va_contexts() { registry().clear(); }
 
 }  // namespace wwb

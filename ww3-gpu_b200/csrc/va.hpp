@@ -24,6 +24,11 @@ int va_device(int igrid, float* va, int nspec, int nsealm, float** d_va);
 /// After a kernel wrote d_va of `igrid`: the device holds the newer bits.
 void va_device_written(int igrid);
 
+/// Before launches that read and write a bound grid's d_va without naming the host array (a
+/// recorded step): uploads the host copy when it is the newer one. An unbound grid is left
+/// alone. Returns a WwKokkosStatus.
+int va_device_current(int igrid);
+
 /// Frees every grid's device copy (ww_kokkos_finalize).
 void release_va_contexts();
 
