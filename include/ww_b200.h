@@ -104,12 +104,13 @@ int ww_snl1_enabled(void);
 /* Replaces ww_snl1_last_error (ww_kokkos_c.hpp:133). */
 int ww_snl1_last_error(void);
 
-/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the band kernel when
- * INSNL1's tables have the row-shift form and fit it, else the row-shift kernel, else the
- * gather kernel; measured fastest at 36x36 on B200), 1 the gather kernel over the
+/* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the pair kernel when
+ * INSNL1's tables have the row-shift form and fit it, else the band kernel, else the row-shift
+ * kernel, else the gather kernel; measured fastest in that order at 36x36 on B200), 1 the gather kernel over the
  * index tables, 2 the row-shift kernel (one CTA per point), 3 the band kernel (register
  * windows over frequency bands, TMA-staged input), 4 the tile kernel (the band kernel compiled
- * for 36 or 24 directions, zero-padded rows, no clamps).
+ * for 36 or 24 directions, zero-padded rows, no clamps), 5 the pair kernel (the band kernel over
+ * two points at once, the additions paired FADD2).
  * Returns the previous choice, or -1 for an unknown grid or a choice its tables cannot run. */
 int ww_snl1_select_kernel(int igrid, int which);
 

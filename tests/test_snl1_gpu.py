@@ -13,21 +13,22 @@ from conftest import assert_bitexact, cuda_available
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
 
-KERNELS = ["gather", "rowshift", "band", "tile"]
+KERNELS = ["gather", "rowshift", "band", "tile", "pair"]
 
 
 def kernel_id(pkg, name):
     return {"gather": pkg.KERNEL_GATHER, "rowshift": pkg.KERNEL_ROWSHIFT,
-            "band": pkg.KERNEL_BAND, "tile": pkg.KERNEL_TILE}[name]
+            "band": pkg.KERNEL_BAND, "tile": pkg.KERNEL_TILE, "pair": pkg.KERNEL_PAIR}[name]
 
 
 def try_select(pkg, grid, name):
     """Select kernel `name`; False when its instances do not fit the grid (only the tile
-    kernel, whose instances need 36 or 24 directions and NK a multiple of 4)."""
+    kernel, whose instances need 36 or 24 directions and NK a multiple of 4, and the pair
+    kernel, whose bulk copies need NSPEC and NK multiples of 4)."""
     try:
         grid.select_kernel(kernel_id(pkg, name))
     except ValueError:
-        assert name == "tile"
+        assert name in ("tile", "pair")
         return False
     return True
 
@@ -78,12 +79,15 @@ def test_36x36_bitexact(pkg, oracle, synth, cfg36, name, case):
     assert_bitexact(d, d_ref, "D")
 
 
-@pytest.mark.parametrize("npts", [1, 2, 287, 8191, 8192, 8193, 20000])
-def test_ragged_batch_sizes(pkg, oracle, synth, cfg36, npts):
-    """Sizes around the host pipeline's chunk (8192 points) and the CTA count."""
+@pytest.mark.parametrize("name", ["band", "pair"])
+@pytest.mark.parametrize("npts", [1, 2, 3, 287, 8191, 8192, 8193, 20000])
+def test_ragged_batch_sizes(pkg, oracle, synth, cfg36, npts, name):
+    """Sizes around the host pipeline's chunk (8192 points), the CTA count and, for the pair
+    kernel, odd counts (the last point paired with itself and stored once)."""
     cfg, sig = cfg36
     g = synth.sea_states(npts, seed=npts, depth_range=(5.0, 4000.0))
     grid = pkg.Snl1Grid(cfg, sig, igrid=2)
+    grid.select_kernel(kernel_id(pkg, name))
     s, d = grid(g["a"], g["cg"], g["kdmean"])
     s_ref, d_ref = oracle.w3snl1(cfg, sig, g["a"], g["cg"], g["kdmean"])
     assert_bitexact(s, s_ref, "S")
@@ -109,7 +113,7 @@ def test_other_spectral_grids(pkg, oracle, nk, nth):
         try:
             grid.select_kernel(kernel_id(pkg, name))
         except ValueError:
-            assert name in ("rowshift", "band", "tile")
+            assert name in ("rowshift", "band", "tile", "pair")
             continue
         s, d = grid(a, cg, kd)
         assert_bitexact(s, s_ref, f"S {nk}x{nth} {name}")
@@ -178,7 +182,7 @@ def test_two_grids_interleaved(pkg, oracle, golden, synth, cfg36):
 
 
 def test_full_size_properties(pkg, oracle, synth, cfg36):
-    """At the bench's size (262,144 points, 4 GB of traffic per pass): the two kernels agree on
+    """At the bench's size (262,144 points, 4 GB of traffic per pass): the kernels agree on
     every value, the run is deterministic, and a seeded sample of points equals the oracle."""
     import torch
 
@@ -192,7 +196,7 @@ def test_full_size_properties(pkg, oracle, synth, cfg36):
     kd = torch.from_numpy(g["kdmean"]).to(dev)
     outs = []
     stream = torch.cuda.current_stream().cuda_stream
-    for name in ("band", "band", "rowshift", "gather"):
+    for name in ("band", "band", "pair", "rowshift", "gather"):
         grid.select_kernel(kernel_id(pkg, name))
         s = torch.empty_like(a)
         d = torch.empty_like(a)

@@ -31,7 +31,7 @@ ERR_UNSUPPORTED = 5
 ERR_TABLE = 6
 
 # ww_snl1_select_kernel choices
-KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT, KERNEL_BAND, KERNEL_TILE = 0, 1, 2, 3, 4
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT, KERNEL_BAND, KERNEL_TILE, KERNEL_PAIR = 0, 1, 2, 3, 4, 5
 
 # Every symbol include/ww_b200.h declares.
 EXPORTS = (

@@ -134,14 +134,20 @@ void publish(Ctx& c) {
   p.ipim = c.ipim.ptr;
   p.ic = c.ic.ptr;
   p.af11 = c.af11.ptr;
-  c.kernel = !t.rowshift ? kSnl1Gather : snl1_band_ok(p) ? kSnl1Band : kSnl1RowShift;
+  c.kernel = !t.rowshift          ? kSnl1Gather
+             : snl1_pair_ok(p)    ? kSnl1Pair
+             : snl1_band_ok(p)    ? kSnl1Band
+                                  : kSnl1RowShift;
 }
 
 /// The kernel `which` asks for, or -1 when these tables cannot run it.
 int pick_kernel(const Ctx& c, int which) {
   switch (which) {
     case kSnl1Auto:
-      return !c.tab.rowshift ? kSnl1Gather : snl1_band_ok(c.dev) ? kSnl1Band : kSnl1RowShift;
+      return !c.tab.rowshift           ? kSnl1Gather
+             : snl1_pair_ok(c.dev)     ? kSnl1Pair
+             : snl1_band_ok(c.dev)     ? kSnl1Band
+                                       : kSnl1RowShift;
     case kSnl1Gather:
       return kSnl1Gather;
     case kSnl1RowShift:
@@ -150,6 +156,8 @@ int pick_kernel(const Ctx& c, int which) {
       return c.tab.rowshift && snl1_band_ok(c.dev) ? kSnl1Band : -1;
     case kSnl1Tile:
       return c.tab.rowshift && snl1_tile_ok(c.dev) ? kSnl1Tile : -1;
+    case kSnl1Pair:
+      return c.tab.rowshift && snl1_pair_ok(c.dev) ? kSnl1Pair : -1;
     default:
       return -1;
   }

@@ -470,7 +470,7 @@ void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* k
                   gate, s.nrej_total.p, st);
     if (fallback &&
         !launch_snl1_list(s.dia, n, s.rej.p, s.nrej.p, ap, cp, kd + p0, sp, dp, nullptr, st))
-      throw CudaError(cudaErrorInvalidValue, "gated DIA: the band kernel cannot run this grid");
+      throw CudaError(cudaErrorInvalidValue, "gated DIA: the pair and band kernels cannot run this grid");
   }
 }
 
@@ -782,7 +782,8 @@ int ww_sur_dataset(int igrid, long long npts, long long holdout, unsigned long l
     for (long long p0 = 0; p0 < npts; p0 += kChunk) {
       const int n = static_cast<int>(std::min<long long>(kChunk, npts - p0));
       synth(s->g, draw, p0, n, a.p, cg.p, kd.p, st);
-      launch_snl1(snl1_band_ok(s->dia) ? kSnl1Band : kSnl1Gather, s->dia, n, a.p, cg.p, kd.p,
+      launch_snl1(snl1_pair_ok(s->dia) ? kSnl1Pair : snl1_band_ok(s->dia) ? kSnl1Band : kSnl1Gather,
+                  s->dia, n, a.p, cg.p, kd.p,
                   so.p, dd.p, st);
       float* const psc = s->pss.p + static_cast<size_t>(p0) * 2 * nk;
       prep(s->g, n, a.p, cg.p, kd.p, s->xs.p + static_cast<size_t>(p0) * din, din, psc, sh.p, st);

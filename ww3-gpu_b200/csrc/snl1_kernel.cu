@@ -868,6 +868,358 @@ __global__ void __launch_bounds__(NTH * G, MINB) snl1_tile_kernel(
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Pair kernel: the band kernel over two sea points at once.
+//
+// The two points of a pair share every index: the same bins, rows, wrapped columns and table
+// entries. So each shared-memory slot holds both points' values side by side (a float2: .x the
+// first point, .y the second), each window load is one 64-bit load for both, and the additions
+// of the reference are paired FADD2 (__fadd2_rn: per component the IEEE addition of
+// __fadd_rn). Every component follows its own point's expression in the reference's order
+// (snl1_team.hpp:383-496), so the results are those of the band kernel bit for bit while the
+// instructions issued per point drop. A - B is A + (-B), the same IEEE result.
+//
+// One rule keeps the pairs exact: a product that feeds an addition is formed by two scalar
+// __fmul_rn (mulS), never by a paired multiply. Measured on B200 with this toolchain, a paired
+// multiply (__fmul2_rn, or mul.rn.f32x2 / fma.rn.f32x2 with a -0 addend in inline PTX) whose
+// result feeds a paired addition came out as a fused multiply-add in 21 % of 2^20 random cases
+// (and in 39 % of the S values of 1000 sea states), whatever -fmad says, while each paired
+// operation alone, and scalar products summed by paired additions, matched the scalar IEEE
+// operations on every case. Paired multiplies (mul2) are used only where the product feeds
+// another multiply or is stored.
+//
+// Shared memory (float2 unless noted): UE rows 0..NFRHGH; SA1, SA2, DA1P, DA1M, DA2P, DA2M (AS
+// float2 apart); DC over NSPEC bins; CON rows (2 x NK, double-buffered by pair parity); CONS of
+// the two points (2, by parity); AF11 rows (NFRCHG floats); the staging buffer (A of both points,
+// then CG of both, floats); the mbarrier. An odd last point is paired with itself and stored once.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+/// A product that feeds an addition: two scalar IEEE multiplies (see above).
+__device__ __forceinline__ float2 mulS(float2 a, float2 b) {
+  return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
+
+/// One elected thread: expect the bytes of two points and start the four bulk copies.
+__device__ __forceinline__ void tma_fetch_pair(uint64_t* bar, float* stage, const float* a,
+                                               const float* cg, int i0, int i1, int nspec,
+                                               int nk) {
+  const unsigned bytes_a = static_cast<unsigned>(nspec) * 4u;
+  const unsigned bytes_c = static_cast<unsigned>(nk) * 4u;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(2u * (bytes_a + bytes_c))
+               : "memory");
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int ip = j == 0 ? i0 : i1;
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(stage + j * nspec)),
+        "l"(a + static_cast<size_t>(ip) * nspec), "r"(bytes_a), "r"(smem_u32(bar))
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(stage + 2 * nspec + j * nk)),
+        "l"(cg + static_cast<size_t>(ip) * nk), "r"(bytes_c), "r"(smem_u32(bar))
+        : "memory");
+  }
+}
+
+template <int BLOCK, int MINB, int AS, bool LIST>
+__global__ void __launch_bounds__(BLOCK, MINB) snl1_pair_kernel(
+    const Snl1Dev p, int npts, const float* __restrict__ a, const float* __restrict__ cg,
+    const float* __restrict__ kdmean, float* __restrict__ s, float* __restrict__ d,
+    int* __restrict__ err, const int* __restrict__ pidx, const int* __restrict__ pcount) {
+  extern __shared__ __align__(16) float smem[];
+  if (LIST) npts = min(npts, __ldg(pcount));
+  auto pt = [&](int i) { return LIST ? __ldg(pidx + i) : i; };
+  const int npairs = (npts + 1) >> 1;
+  const int nth = p.nth, nfr = p.nfr, nfrhgh = p.nfrhgh, nfrchg = p.nfrchg;
+  const int nspec = p.nspec, nk = p.nk;
+  float2* const ue = reinterpret_cast<float2*>(smem);
+  float2* const arrs = ue + (nfrhgh + 1) * nth;
+  float2* const sa1 = arrs;
+  float2* const sa2 = arrs + AS;
+  float2* const da1p = arrs + 2 * AS;
+  float2* const da1m = arrs + 3 * AS;
+  float2* const da2p = arrs + 4 * AS;
+  float2* const da2m = arrs + 5 * AS;
+  float2* const dcs = arrs + 6 * AS;
+  float2* const conx2 = dcs + nspec;
+  float2* const cons2 = conx2 + 2 * nk;
+  float* const afr = reinterpret_cast<float*>(cons2 + 2);
+  const size_t stage_off =
+      (static_cast<size_t>(afr + nfrchg - smem) + 3) & ~static_cast<size_t>(3);
+  float* const stage = smem + stage_off;
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(stage + ((2 * (nspec + nk) + 3) & ~3));
+  const int tid = threadIdx.x;
+
+  // The points of pair pp: 2 pp and 2 pp + 1 of the batch (an odd last point twice).
+  auto first_of = [&](int pp) { return pt(2 * pp); };
+  auto second_of = [&](int pp) { return 2 * pp + 1 < npts ? pt(2 * pp + 1) : pt(2 * pp); };
+
+  for (int i = tid; i < nth; i += BLOCK) {
+    const float2 z = make_float2(0.0f, 0.0f);
+    ue[i] = z;
+    sa1[i] = sa2[i] = da1p[i] = da1m[i] = da2p[i] = da2m[i] = z;
+  }
+  for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
+  float kd0 = 0.0f, kd1 = 0.0f;  // thread 0: the KDMEAN of its CTA's next pair
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    if (blockIdx.x < npairs) {
+      const int i0 = first_of(blockIdx.x), i1 = second_of(blockIdx.x);
+      tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk);
+      kd0 = __ldg(kdmean + i0);
+      kd1 = __ldg(kdmean + i1);
+    }
+  }
+  __syncthreads();
+
+  const int G = BLOCK / nth;
+  const int ith = tid % nth, band = tid / nth;
+  const bool active = band < G;
+  const int br = (nfrchg + G - 1) / G;
+  const int f0 = 1 + band * br;
+  const int n3 = active ? max(0, min(br, nfrchg - f0 + 1)) : 0;
+  const int n4 = active ? max(0, min(br, nfr - f0 + 1)) : 0;
+  const int c0 = wrapc(ith + p.shift[0], nth), c1 = wrapc(ith + p.shift[1], nth);
+  const int c2 = wrapc(ith + p.shift[2], nth), c3 = wrapc(ith + p.shift[3], nth);
+  const int c4 = wrapc(ith + p.shift[4], nth), c5 = wrapc(ith + p.shift[5], nth);
+  const int c6 = wrapc(ith + p.shift[6], nth), c7 = wrapc(ith + p.shift[7], nth);
+  const int ifrp = p.ifrp, ifrm = p.ifrm;
+  const int dq = BLOCK / nth, dr = BLOCK % nth, q0 = tid / nth, r0 = tid % nth;
+
+  unsigned parity = 0;
+  int buf = 0;
+  for (int pp = blockIdx.x; pp < npairs; pp += gridDim.x, buf ^= 1) {
+    const int i0 = first_of(pp), i1 = second_of(pp);
+    const bool has1 = 2 * pp + 1 < npts;
+    float2* const conx = conx2 + buf * nk;
+    const bool lost = !mbar_wait(bar, parity, err);
+    parity ^= 1u;
+    // 1. CONS of both points (one thread); 2a. CON per frequency row.
+    if (tid == 0) cons2[buf] = make_float2(dia_cons(p, kd0), dia_cons(p, kd1));
+    for (int k = tid; k < nk; k += BLOCK) {
+      const float w = kTpiInv / __ldg(p.sig + k);
+      conx[k] = make_float2(w * stage[2 * nspec + k], w * stage[2 * nspec + nk + k]);
+    }
+    // A bulk copy whose wait gave up ends this CTA's work here, all its threads together.
+    if (__syncthreads_or(lost)) break;
+
+    // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
+    {
+      int ifr0 = q0, col = r0;
+      for (int isp = tid; isp < nspec; isp += BLOCK) {
+        const float2 cx = conx[ifr0];
+        const float2 v = make_float2(stage[isp] / cx.x, stage[nspec + isp] / cx.y);
+        ue[isp + nth] = v;
+        if (ifr0 == nfr - 1) {
+          float2 t = v;
+          const float2 fh = dup2(p.fachfe);
+          for (int r = nfr + 1; r <= nfrhgh; ++r) {
+            t = mul2(t, fh);
+            ue[r * nth + col] = t;
+          }
+        }
+        col += dr;
+        ifr0 += dq;
+        if (col >= nth) {
+          col -= nth;
+          ++ifr0;
+        }
+      }
+    }
+    __syncthreads();
+
+    // The next pair's A and CG stream into the staging buffer while this one is computed.
+    const int pnext = pp + gridDim.x;
+    if (tid == 0 && pnext < npairs) {
+      const int j0 = first_of(pnext), j1 = second_of(pnext);
+      tma_fetch_pair(bar, stage, a, cg, j0, j1, nspec, nk);
+      kd0 = __ldg(kdmean + j0);
+      kd1 = __ldg(kdmean + j1);
+    }
+    const float2 cons = cons2[buf];
+
+    // 3. Interactions over the extended spectrum, sliding up the band.
+    if (n3 > 0) {
+      const float2 w0 = dup2(p.awg[0]), w1 = dup2(p.awg[1]), w2 = dup2(p.awg[2]),
+                   w3 = dup2(p.awg[3]), w4 = dup2(p.awg[4]), w5 = dup2(p.awg[5]),
+                   w6 = dup2(p.awg[6]), w7 = dup2(p.awg[7]);
+      const float2 dl1 = dup2(p.dal1), dl2 = dup2(p.dal2), dl3 = dup2(p.dal3);
+      float2 pa[4], pb[4], ma[4], mb[4];  // plus rows: c1 c2 c5 c6; minus rows: c3 c4 c7 c8
+#define WWB_P2(ROW, W)                        \
+  {                                           \
+    const int b_ = (ROW) * nth;               \
+    W[0] = ue[b_ + c0];                       \
+    W[1] = ue[b_ + c1];                       \
+    W[2] = ue[b_ + c4];                       \
+    W[3] = ue[b_ + c5];                       \
+  }
+#define WWB_M2(ROW, W)                        \
+  {                                           \
+    const int r_ = (ROW);                     \
+    const int b_ = (r_ > 0 ? r_ : 0) * nth;   \
+    W[0] = ue[b_ + c2];                       \
+    W[1] = ue[b_ + c3];                       \
+    W[2] = ue[b_ + c6];                       \
+    W[3] = ue[b_ + c7];                       \
+  }
+      WWB_P2(f0 + ifrp, pa)
+      WWB_P2(f0 + ifrp + 1, pb)
+      WWB_M2(f0 + ifrm, ma)
+      WWB_M2(f0 + ifrm - 1, mb)
+#pragma unroll 1
+      for (int k = 0; k < n3; ++k) {
+        const int f = f0 + k;
+        const int o = f * nth + ith;
+        const float2 e00 = ue[o];
+        const float2 ep1 = add2(add2(add2(mulS(w0, pb[1]), mulS(w1, pb[0])), mulS(w2, pa[1])),
+                                mulS(w3, pa[0]));
+        const float2 em1 = add2(add2(add2(mulS(w4, mb[3]), mulS(w5, mb[2])), mulS(w6, ma[3])),
+                                mulS(w7, ma[2]));
+        const float2 ep2 = add2(add2(add2(mulS(w0, pb[3]), mulS(w1, pb[2])), mulS(w2, pa[3])),
+                                mulS(w3, pa[2]));
+        const float2 em2 = add2(add2(add2(mulS(w4, mb[1]), mulS(w5, mb[0])), mulS(w6, ma[1])),
+                                mulS(w7, ma[0]));
+        const float2 ca = mul2(cons, dup2(afr[f - 1]));
+        const float2 factor = mul2(ca, e00);
+        const float2 sa1a = mulS(e00, add2(mulS(ep1, dl1), mulS(em1, dl2)));
+        const float2 sa1b = sub2(sa1a, mulS(mul2(ep1, em1), dl3));
+        const float2 sa2a = mulS(e00, add2(mulS(ep2, dl1), mulS(em2, dl2)));
+        const float2 sa2b = sub2(sa2a, mulS(mul2(ep2, em2), dl3));
+        sa1[o] = mul2(factor, sa1b);
+        sa2[o] = mul2(factor, sa2b);
+        if (f <= nfr) dcs[o - nth] = add2(mulS(ca, add2(sa1a, sa1b)), mulS(ca, add2(sa2a, sa2b)));
+        da1p[o] = mul2(factor, sub2(mulS(dl1, e00), mulS(dl3, em1)));
+        da1m[o] = mul2(factor, sub2(mulS(dl2, e00), mulS(dl3, ep1)));
+        da2p[o] = mul2(factor, sub2(mulS(dl1, e00), mulS(dl3, em2)));
+        da2m[o] = mul2(factor, sub2(mulS(dl2, e00), mulS(dl3, ep2)));
+        if (k + 1 < n3) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            pa[j] = pb[j];
+            mb[j] = ma[j];
+          }
+          WWB_P2(f + 1 + ifrp + 1, pb)
+          WWB_M2(f + 1 + ifrm, ma)
+        }
+      }
+#undef WWB_P2
+#undef WWB_M2
+    }
+    __syncthreads();
+
+    // 4. Source and diagonal terms (as the band kernel: S in one pass, D in a second).
+    if (n4 > 0) {
+#define WWB_LO2(A1, A2, ROW, W)               \
+  {                                           \
+    const int r_ = (ROW);                     \
+    const int b_ = (r_ > 0 ? r_ : 0) * nth;   \
+    W[0] = A1[b_ + c4];                       \
+    W[1] = A1[b_ + c5];                       \
+    W[2] = A2[b_ + c0];                       \
+    W[3] = A2[b_ + c1];                       \
+  }
+#define WWB_HI2(A1, A2, ROW, W)               \
+  {                                           \
+    const int b_ = (ROW) * nth;               \
+    W[0] = A1[b_ + c2];                       \
+    W[1] = A1[b_ + c3];                       \
+    W[2] = A2[b_ + c6];                       \
+    W[3] = A2[b_ + c7];                       \
+  }
+      const float2 m2 = dup2(-2.0f);
+      float2 l5[4], l6[4], h7[4], h8[4];
+      {
+        const float2 w0 = dup2(p.awg[0]), w1 = dup2(p.awg[1]), w2 = dup2(p.awg[2]),
+                     w3 = dup2(p.awg[3]), w4 = dup2(p.awg[4]), w5 = dup2(p.awg[5]),
+                     w6 = dup2(p.awg[6]), w7 = dup2(p.awg[7]);
+        float* const sp0 = s + static_cast<size_t>(i0) * nspec;
+        float* const sp1 = s + static_cast<size_t>(i1) * nspec;
+        WWB_LO2(sa1, sa2, f0 - ifrp, l5)
+        WWB_LO2(sa1, sa2, f0 - ifrp - 1, l6)
+        WWB_HI2(sa1, sa2, f0 - ifrm, h7)
+        WWB_HI2(sa1, sa2, f0 - ifrm + 1, h8)
+#pragma unroll 1
+        for (int k = 0; k < n4; ++k) {
+          const int f = f0 + k;
+          const int isp = (f - 1) * nth + ith;
+          float2 t = mulS(m2, add2(sa1[isp + nth], sa2[isp + nth]));
+          t = add2(t, mulS(w0, add2(l6[1], l6[3])));
+          t = add2(t, mulS(w1, add2(l6[0], l6[2])));
+          t = add2(t, mulS(w2, add2(l5[1], l5[3])));
+          t = add2(t, mulS(w3, add2(l5[0], l5[2])));
+          t = add2(t, mulS(w4, add2(h8[1], h8[3])));
+          t = add2(t, mulS(w5, add2(h8[0], h8[2])));
+          t = add2(t, mulS(w6, add2(h7[1], h7[3])));
+          t = add2(t, mulS(w7, add2(h7[0], h7[2])));
+          const float2 sv = mul2(conx[f - 1], t);
+          __stcs(sp0 + isp, sv.x);
+          if (has1) __stcs(sp1 + isp, sv.y);
+          if (k + 1 < n4) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              l6[j] = l5[j];
+              h7[j] = h8[j];
+            }
+            WWB_LO2(sa1, sa2, f + 1 - ifrp, l5)
+            WWB_HI2(sa1, sa2, f + 1 - ifrm + 1, h8)
+          }
+        }
+      }
+      {
+        const float2 w0 = dup2(p.swg[0]), w1 = dup2(p.swg[1]), w2 = dup2(p.swg[2]),
+                     w3 = dup2(p.swg[3]), w4 = dup2(p.swg[4]), w5 = dup2(p.swg[5]),
+                     w6 = dup2(p.swg[6]), w7 = dup2(p.swg[7]);
+        float* const dp0 = d + static_cast<size_t>(i0) * nspec;
+        float* const dp1 = d + static_cast<size_t>(i1) * nspec;
+        WWB_LO2(da1p, da2p, f0 - ifrp, l5)
+        WWB_LO2(da1p, da2p, f0 - ifrp - 1, l6)
+        WWB_HI2(da1m, da2m, f0 - ifrm, h7)
+        WWB_HI2(da1m, da2m, f0 - ifrm + 1, h8)
+#pragma unroll 1
+        for (int k = 0; k < n4; ++k) {
+          const int f = f0 + k;
+          const int isp = (f - 1) * nth + ith;
+          float2 t = mulS(m2, dcs[isp]);
+          t = add2(t, mulS(w0, add2(l6[1], l6[3])));
+          t = add2(t, mulS(w1, add2(l6[0], l6[2])));
+          t = add2(t, mulS(w2, add2(l5[1], l5[3])));
+          t = add2(t, mulS(w3, add2(l5[0], l5[2])));
+          t = add2(t, mulS(w4, add2(h8[1], h8[3])));
+          t = add2(t, mulS(w5, add2(h8[0], h8[2])));
+          t = add2(t, mulS(w6, add2(h7[1], h7[3])));
+          t = add2(t, mulS(w7, add2(h7[0], h7[2])));
+          __stcs(dp0 + isp, t.x);
+          if (has1) __stcs(dp1 + isp, t.y);
+          if (k + 1 < n4) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              l6[j] = l5[j];
+              h7[j] = h8[j];
+            }
+            WWB_LO2(da1p, da2p, f + 1 - ifrp, l5)
+            WWB_HI2(da1m, da2m, f + 1 - ifrm + 1, h8)
+          }
+        }
+      }
+#undef WWB_LO2
+#undef WWB_HI2
+    }
+    // The next pair's barriers order its writes of UE and the arrays after this section 4.
+  }
+}
+
+constexpr int kPairBlock = 288;
+constexpr int kPairMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 113 registers
+constexpr int kPairStride = 1536;  // float2 slots per interaction array
+
 constexpr int kBandBlock = 288;
 constexpr int kTileMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 113 registers
 constexpr int kBandMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 96 registers
@@ -938,6 +1290,23 @@ bool snl1_band_ok(const Snl1Dev& p) {
   return snl1_band_smem(p) <= 227 * 1024;
 }
 
+size_t snl1_pair_smem(const Snl1Dev& p) {
+  size_t bytes = 8 * (static_cast<size_t>(p.nfrhgh + 1) * p.nth +
+                      6 * static_cast<size_t>(kPairStride) + p.nspec + 2 * p.nk + 2) +
+                 4 * static_cast<size_t>(p.nfrchg);
+  bytes = (bytes + 15) & ~static_cast<size_t>(15);
+  bytes += 4 * ((2 * static_cast<size_t>(p.nspec + p.nk) + 3) & ~static_cast<size_t>(3));
+  return bytes + 16;  // + the mbarrier
+}
+
+bool snl1_pair_ok(const Snl1Dev& p) {
+  if (p.ifrow == nullptr || p.af11_row == nullptr) return false;  // no row-shift form
+  if (p.nth > kPairBlock || p.ifrp < 0 || p.ifrm > 0) return false;
+  if ((p.nfrchg + 1) * p.nth > kPairStride) return false;
+  if (p.nspec % 4 != 0 || p.nk % 4 != 0) return false;  // the bulk copies
+  return snl1_pair_smem(p) <= 227 * 1024;
+}
+
 int snl1_take_error() {
   if (g_band_err == nullptr) return 0;
   int v = 0;
@@ -991,6 +1360,30 @@ void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, co
   WWB_CHECK(cudaGetLastError());
 }
 
+template <bool LIST>
+void launch_pair(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
+                 const float* a, const float* cg, const float* kd, float* s, float* d, int* err,
+                 cudaStream_t stream) {
+  static int per_sm = -1;
+  static size_t cached = 0;
+  const size_t smem = snl1_pair_smem(p);
+  auto k = snl1_pair_kernel<kPairBlock, kPairMinBlocks, kPairStride, LIST>;
+  if (per_sm < 0 || cached != smem) {
+    WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    int n = 0;
+    WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kPairBlock, smem));
+    if (n < 1) throw CudaError(cudaErrorInvalidConfiguration, "snl1 pair occupancy");
+    per_sm = n;
+    cached = smem;
+  }
+  const long long pairs = (static_cast<long long>(capacity) + 1) / 2;
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  const int grid = static_cast<int>(pairs < resident ? pairs : resident);
+  k<<<grid, kPairBlock, smem, stream>>>(p, capacity, a, cg, kd, s, d, err, pidx, pcount);
+  WWB_CHECK(cudaGetLastError());
+}
+
 /// The error flag of the band and tile kernels' bulk-copy waits (allocated on first use).
 int* band_err_flag() {
   if (g_band_err == nullptr) {
@@ -1015,11 +1408,16 @@ namespace {
 void launch_dispatch(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                      const float* kdmean, float* s, float* d, int* err, cudaStream_t stream) {
   if (npts <= 0) return;
-  if (kernel == kSnl1Tile || kernel == kSnl1Band) {
+  if (kernel == kSnl1Tile || kernel == kSnl1Band || kernel == kSnl1Pair) {
     if (err == nullptr) err = band_err_flag();
   }
   const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
                        (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
+  if (kernel == kSnl1Pair) {
+    if (aligned && snl1_pair_ok(p))
+      return launch_pair<false>(p, npts, nullptr, nullptr, a, cg, kdmean, s, d, err, stream);
+    kernel = kSnl1Band;  // caller arrays not 16-byte aligned: the band kernel reads them directly
+  }
   if (kernel == kSnl1Tile) {
     const int v = tile_variant(p);
     if (v == 36 && aligned) return launch_tile<36, 8, 5>(p, npts, a, cg, kdmean, s, d, err, stream);
@@ -1138,6 +1536,10 @@ bool launch_snl1_list(const Snl1Dev& p, int capacity, const int* pidx, const int
   if (err == nullptr) err = band_err_flag();
   const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
                        (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
+  if (aligned && snl1_pair_ok(p)) {
+    launch_pair<true>(p, capacity, pidx, pcount, a, cg, kdmean, s, d, err, stream);
+    return true;
+  }
   const bool tma = p.nspec % 4 == 0 && p.nk % 4 == 0 && aligned;
   if (band_stride(p) == 1536) {
     if (tma) launch_band_list<1536, true>(p, capacity, pidx, pcount, a, cg, kdmean, s, d, err, stream);

@@ -25,7 +25,14 @@ struct Snl1Dev {
   const float* sig;         ///< device, NK
 };
 
-enum Snl1Kernel { kSnl1Auto = 0, kSnl1Gather = 1, kSnl1RowShift = 2, kSnl1Band = 3, kSnl1Tile = 4 };
+enum Snl1Kernel {
+  kSnl1Auto = 0,
+  kSnl1Gather = 1,
+  kSnl1RowShift = 2,
+  kSnl1Band = 3,
+  kSnl1Tile = 4,
+  kSnl1Pair = 5,  ///< the band kernel over two points at once (paired FP32 additions)
+};
 
 /// Dynamic shared memory of each kernel, bytes.
 size_t snl1_gather_smem(const Snl1Dev& p);
@@ -35,6 +42,12 @@ size_t snl1_band_smem(const Snl1Dev& p);
 /// Whether the band kernel can run these tables (row-shift form, NTH within one CTA, the
 /// rows of a band within its register windows).
 bool snl1_band_ok(const Snl1Dev& p);
+
+size_t snl1_pair_smem(const Snl1Dev& p);
+
+/// Whether the pair kernel can run these tables (the band kernel's conditions, interaction
+/// arrays of at most 1536 bins, NSPEC and NK multiples of 4 for its bulk copies).
+bool snl1_pair_ok(const Snl1Dev& p);
 
 /// Whether a compile-time tile instance of the band kernel fits these tables (NTH 36 or 24,
 /// NSPEC and NK multiples of 4 for the bulk copies).
@@ -63,7 +76,8 @@ Snl1StaticScratch snl1_static_scratch();
 void launch_snl1_err(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                      const float* kdmean, float* s, float* d, int* err, cudaStream_t stream);
 
-/// The band kernel on the points pidx[0 .. min(capacity, *pcount)) of the arrays (pidx and
+/// The pair kernel (the band kernel where the pair kernel does not fit, or the arrays are not
+/// 16-byte aligned) on the points pidx[0 .. min(capacity, *pcount)) of the arrays (pidx and
 /// pcount device pointers; the count may be written by an earlier kernel on `stream`). Returns
 /// false, launching nothing, when the band kernel cannot run these tables.
 bool launch_snl1_list(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
