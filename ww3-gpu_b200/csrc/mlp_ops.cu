@@ -337,6 +337,179 @@ __global__ void __launch_bounds__(32 * kPointsPerCta)
   }
 }
 
+
+/// prep_kernel for one grid shape known at compile time (NK rows of NTH directions, 32 <= NK
+/// <= 64, NTH a multiple of 4), with the same outputs. One warp per sea point; lane k owns
+/// frequency row k (and row k + 32): it reads the row with 16-byte loads, scales it and keeps
+/// its maximum in registers, and later writes the row's network inputs. The spectrum is kept in
+/// shared memory with rows NTH + 1 floats apart, so lanes reading the same column of their rows
+/// hit different banks. Column sums run one lane per direction, in row order as in prep_kernel.
+template <int NK, int NTH>
+__global__ void __launch_bounds__(32 * kPointsPerCta)
+    prep_rows_kernel(SurGrid g, int npts, const float* __restrict__ a,
+                     const float* __restrict__ cg, const float* __restrict__ kdm,
+                     __nv_bfloat16* __restrict__ x, int ldx, float* __restrict__ ps,
+                     int* __restrict__ shift) {
+  static_assert(NK >= 32 && NK <= 64 && NTH % 4 == 0, "prep_rows_kernel shape");
+  constexpr int NSPEC = NK * NTH, LD = NTH + 1, Q = NTH / 4;
+  __shared__ float sm_ue[kPointsPerCta][NK * LD];
+  __shared__ float sm_lw[kPointsPerCta][NK];
+  __shared__ float sm_ds[kPointsPerCta][NTH];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ip = blockIdx.x * kPointsPerCta + warp;
+  if (ip >= npts) return;  // warp-uniform
+  float* const ue = sm_ue[warp];
+  float* const lw = sm_lw[warp];
+  float* const ds = sm_ds[warp];
+  const float* ap = a + static_cast<size_t>(ip) * NSPEC;
+  const float* cgp = cg + static_cast<size_t>(ip) * NK;
+  float* pp = ps + static_cast<size_t>(ip) * 2 * NK;
+
+  // UE = A / CONX row by row (lane k: rows k and k + 32), each row's largest value.
+  float rc[2] = {0.0f, 0.0f}, rmx[2] = {0.0f, 0.0f};
+  float mx = 0.0f;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int k = lane + 32 * r;
+    if (k < NK) {
+      const float rk = __ldg(g.sig + k) / (kTpiInvF * __ldg(cgp + k));
+      rc[r] = rk;
+      const float4* row = reinterpret_cast<const float4*>(ap + k * NTH);
+      float* const u = ue + k * LD;
+      float m = 0.0f;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        float4 v = __ldg(row + q);
+        v.x *= rk;
+        v.y *= rk;
+        v.z *= rk;
+        v.w *= rk;
+        u[4 * q] = v.x;
+        u[4 * q + 1] = v.y;
+        u[4 * q + 2] = v.z;
+        u[4 * q + 3] = v.w;
+        m = fmaxf(m, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+      }
+      rmx[r] = m;
+      mx = fmaxf(mx, m);
+    }
+  }
+  const float umax = warp_max(mx);
+  const float floor = fmaxf(umax * 1e-12f, 1e-30f);
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int k = lane + 32 * r;
+    if (k < NK)
+      lw[k] = 3.0f * __logf(fmaxf(rmx[r], floor)) + 11.0f * __logf(__ldg(g.sig + k) * kTpiInvF);
+  }
+  __syncwarp();
+  for (int t = lane; t < NTH; t += 32) {
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) s += ue[k * LD + t];
+    ds[t] = s;
+  }
+  __syncwarp();
+  // Dominant direction (lowest index on ties), then which side of it is heavier.
+  float bv = -1.0f;
+  int bi = 0;
+  for (int t = lane; t < NTH; t += 32)
+    if (ds[t] > bv) {
+      bv = ds[t];
+      bi = t;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  float up = 0.0f, lo = 0.0f;
+  for (int j = 1 + lane; j < (NTH + 1) / 2; j += 32) {
+    int cu = bi + j, cl = bi - j;
+    if (cu >= NTH) cu -= NTH;
+    if (cl < 0) cl += NTH;
+    up += ds[cu];
+    lo += ds[cl];
+  }
+  up = warp_sum(up);
+  lo = warp_sum(lo);
+  const int packed = bi | (lo > up ? 1 << 16 : 0);
+  const float kd = __ldg(kdm + ip);
+  const float cons = cons_of(g, kd);
+  const float lcons = __logf(cons);
+  // lambda(k) and the Hs-tendency weights, as prep_kernel.
+  constexpr int kReach = 5;
+  float lam[2] = {0.0f, 0.0f}, wl[2] = {-INFINITY, -INFINITY};
+  float wmax = -INFINITY;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int k = lane + 32 * r;
+    if (k < NK) {
+      float l = -INFINITY;
+      for (int q = max(0, k - kReach); q <= min(NK - 1, k + kReach); ++q) l = fmaxf(l, lw[q]);
+      lam[r] = umax > 0.0f ? lcons - __logf(rc[r]) + l : -1e30f;
+      wl[r] = lam[r] + ln_dden(g, __ldg(g.sig + k)) - __logf(__ldg(cgp + k));
+      wmax = fmaxf(wmax, wl[r]);
+    }
+  }
+  wmax = warp_max(wmax);
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int k = lane + 32 * r;
+    if (k < NK) {
+      pp[k] = lam[r];
+      pp[NK + k] = umax > 0.0f ? __expf(wl[r] - wmax) : 0.0f;
+    }
+  }
+  if (lane == 0) shift[ip] = packed;
+  // The network input in canonical order: lane k writes row k (four bins per 8-byte store),
+  // then the rows from 32 up are shared by all lanes.
+  const float inv = umax > 0.0f ? 1.0f / umax : 0.0f;
+  __nv_bfloat16* xr = x + static_cast<size_t>(ip) * ldx;
+  const int sh = packed & 0xFFFF;
+  const bool flip = (packed >> 16) != 0;
+  auto xval = [&](float u) { return __logf(u * inv + kInputFloor) * kInputScale + 1.0f; };
+  {
+    const float* row = ue + lane * LD;
+    const int step = flip ? -1 : 1;
+    int c = sh;
+#pragma unroll
+    for (int j = 0; j < NTH; j += 4) {
+      float v[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        v[e] = xval(row[c]);
+        c += step;
+        if (c >= NTH) c -= NTH;
+        if (c < 0) c += NTH;
+      }
+      const __nv_bfloat162 b0 = __floats2bfloat162_rn(v[0], v[1]);
+      const __nv_bfloat162 b1 = __floats2bfloat162_rn(v[2], v[3]);
+      uint2 pk;
+      pk.x = *reinterpret_cast<const unsigned*>(&b0);
+      pk.y = *reinterpret_cast<const unsigned*>(&b1);
+      *reinterpret_cast<uint2*>(xr + lane * NTH + j) = pk;
+    }
+  }
+  for (int i = lane; i < (NK - 32) * NTH; i += 32) {
+    const int k = 32 + i / NTH, j = i % NTH;
+    int c = flip ? sh - j : sh + j;
+    if (c >= NTH) c -= NTH;
+    if (c < 0) c += NTH;
+    xr[k * NTH + j] = __float2bfloat16_rn(xval(ue[k * LD + c]));
+  }
+  // Depth features: ln kdmean and the relative depth factor of CONS; zero padding.
+  for (int i = NSPEC + lane; i < g.din; i += 32) {
+    float v = 0.0f;
+    if (i == NSPEC) v = __logf(fmaxf(kd, 1e-2f)) * 0.2f;
+    if (i == NSPEC + 1) v = cons / g.snlc1 - 1.0f;
+    xr[i] = __float2bfloat16_rn(v);
+  }
+}
+
 // ------------------------------------------------------------------------------ target side
 
 __global__ void rowscale_kernel(SurGrid g, int npts, const float* __restrict__ s,
@@ -747,6 +920,16 @@ void prep(const SurGrid& g, int npts, const float* a, const float* cg, const flo
     set = smem;
   }
   const unsigned blocks = static_cast<unsigned>((npts + kPointsPerCta - 1) / kPointsPerCta);
+  // 36 x 36 with 16-byte aligned spectra and 8-byte aligned input rows: rows across lanes.
+  const bool rows36 = g.nk == 36 && g.nth == 36 && g.nspec == 1296 &&
+                      (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
+                      (reinterpret_cast<uintptr_t>(x) & 7u) == 0 && ldx % 4 == 0;
+  if (rows36) {
+    prep_rows_kernel<36, 36><<<blocks, 32 * kPointsPerCta, 0, st>>>(g, npts, a, cg, kdmean, x,
+                                                                     ldx, ps, shift);
+    WWB_CHECK(cudaGetLastError());
+    return;
+  }
   prep_kernel<<<blocks, 32 * kPointsPerCta, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, ps,
                                                          shift);
   WWB_CHECK(cudaGetLastError());
