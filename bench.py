@@ -102,7 +102,7 @@ def parse():
                         "with --train-steps 0 it times the kernels of the network path alone")
     p.add_argument("--no-srce-line", action="store_true",
                    help="surrogate workload: leave out the W3SRCE line it carries")
-    p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band", "tile", "pair"], default="auto",
+    p.add_argument("--kernel", choices=["auto", "gather", "rowshift", "band", "tile", "pair", "pair-general"], default="auto",
                    help="DIA kernel (ww_snl1_select_kernel); auto picks the pair kernel")
     a = p.parse_args()
     srce = a.workload == "srce"
@@ -296,11 +296,13 @@ def run_b200_dia(args):
     grid = pkg.Snl1Grid(cfg, sig, igrid=1)
     kernel_ids = {"auto": pkg.KERNEL_AUTO, "gather": pkg.KERNEL_GATHER,
                   "rowshift": pkg.KERNEL_ROWSHIFT, "band": pkg.KERNEL_BAND,
-                  "tile": pkg.KERNEL_TILE, "pair": pkg.KERNEL_PAIR}
+                  "tile": pkg.KERNEL_TILE, "pair": pkg.KERNEL_PAIR,
+                  "pair-general": pkg.KERNEL_PAIR_GENERAL}
     grid.select_kernel(kernel_ids[args.kernel])
     kernel_name = {pkg.KERNEL_GATHER: "snl1_gather_kernel", pkg.KERNEL_ROWSHIFT:
                    "snl1_rowshift_kernel", pkg.KERNEL_BAND: "snl1_band_kernel",
-                   pkg.KERNEL_TILE: "snl1_tile_kernel", pkg.KERNEL_PAIR: "snl1_pair_kernel"}[
+                   pkg.KERNEL_TILE: "snl1_tile_kernel", pkg.KERNEL_PAIR: "snl1_pairtile_kernel",
+                   pkg.KERNEL_PAIR_GENERAL: "snl1_pair_kernel"}[
                        grid.select_kernel(kernel_ids[args.kernel])]
     dev = torch.device("cuda", local)
     a = torch.from_numpy(g["a"]).to(dev)
@@ -1599,7 +1601,7 @@ def run_b200_surrogate(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network / f32 fallback",
         "data": "synthetic", "config": cfgd,
         "plain_dia": {"value": npts * world / (plain_ms / 1e3), "unit": UNIT,
-                      "ms_per_step": plain_ms, "kernel": "snl1_pair_kernel (the default DIA)",
+                      "ms_per_step": plain_ms, "kernel": "snl1_pairtile_kernel (the default DIA)",
                       "error_vs_fp64": err_plain},
         "speedup_vs_plain": plain_ms / gated_ms,
         "accepted_fraction": 1.0 - fallback / npts,

@@ -110,7 +110,9 @@ int ww_snl1_last_error(void);
  * index tables, 2 the row-shift kernel (one CTA per point), 3 the band kernel (register
  * windows over frequency bands, TMA-staged input), 4 the tile kernel (the band kernel compiled
  * for 36 or 24 directions, zero-padded rows, no clamps), 5 the pair kernel (the band kernel over
- * two points at once, the additions paired FADD2).
+ * two points at once, the additions paired FADD2; for 36 directions its form with the band
+ * shape fixed at compile time, unrolled rows and zero-padded matrices), 6 the pair kernel's
+ * general form for any grid it fits.
  * Returns the previous choice, or -1 for an unknown grid or a choice its tables cannot run. */
 int ww_snl1_select_kernel(int igrid, int which);
 

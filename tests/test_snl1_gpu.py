@@ -13,12 +13,13 @@ from conftest import assert_bitexact, cuda_available
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
 
-KERNELS = ["gather", "rowshift", "band", "tile", "pair"]
+KERNELS = ["gather", "rowshift", "band", "tile", "pair", "pair-general"]
 
 
 def kernel_id(pkg, name):
     return {"gather": pkg.KERNEL_GATHER, "rowshift": pkg.KERNEL_ROWSHIFT,
-            "band": pkg.KERNEL_BAND, "tile": pkg.KERNEL_TILE, "pair": pkg.KERNEL_PAIR}[name]
+            "band": pkg.KERNEL_BAND, "tile": pkg.KERNEL_TILE, "pair": pkg.KERNEL_PAIR,
+            "pair-general": pkg.KERNEL_PAIR_GENERAL}[name]
 
 
 def try_select(pkg, grid, name):
@@ -28,7 +29,7 @@ def try_select(pkg, grid, name):
     try:
         grid.select_kernel(kernel_id(pkg, name))
     except ValueError:
-        assert name in ("tile", "pair")
+        assert name in ("tile", "pair", "pair-general")
         return False
     return True
 
@@ -79,7 +80,7 @@ def test_36x36_bitexact(pkg, oracle, synth, cfg36, name, case):
     assert_bitexact(d, d_ref, "D")
 
 
-@pytest.mark.parametrize("name", ["band", "pair"])
+@pytest.mark.parametrize("name", ["band", "pair", "pair-general"])
 @pytest.mark.parametrize("npts", [1, 2, 3, 287, 8191, 8192, 8193, 20000])
 def test_ragged_batch_sizes(pkg, oracle, synth, cfg36, npts, name):
     """Sizes around the host pipeline's chunk (8192 points), the CTA count and, for the pair
@@ -113,7 +114,7 @@ def test_other_spectral_grids(pkg, oracle, nk, nth):
         try:
             grid.select_kernel(kernel_id(pkg, name))
         except ValueError:
-            assert name in ("rowshift", "band", "tile", "pair")
+            assert name in ("rowshift", "band", "tile", "pair", "pair-general")
             continue
         s, d = grid(a, cg, kd)
         assert_bitexact(s, s_ref, f"S {nk}x{nth} {name}")
@@ -196,7 +197,7 @@ def test_full_size_properties(pkg, oracle, synth, cfg36):
     kd = torch.from_numpy(g["kdmean"]).to(dev)
     outs = []
     stream = torch.cuda.current_stream().cuda_stream
-    for name in ("band", "band", "pair", "rowshift", "gather"):
+    for name in ("band", "band", "pair", "pair-general", "rowshift", "gather"):
         grid.select_kernel(kernel_id(pkg, name))
         s = torch.empty_like(a)
         d = torch.empty_like(a)

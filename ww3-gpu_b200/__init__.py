@@ -32,6 +32,7 @@ ERR_TABLE = 6
 
 # ww_snl1_select_kernel choices
 KERNEL_AUTO, KERNEL_GATHER, KERNEL_ROWSHIFT, KERNEL_BAND, KERNEL_TILE, KERNEL_PAIR = 0, 1, 2, 3, 4, 5
+KERNEL_PAIR_GENERAL = 6
 
 # Every symbol include/ww_b200.h declares.
 EXPORTS = (

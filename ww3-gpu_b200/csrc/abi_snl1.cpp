@@ -158,6 +158,8 @@ int pick_kernel(const Ctx& c, int which) {
       return c.tab.rowshift && snl1_tile_ok(c.dev) ? kSnl1Tile : -1;
     case kSnl1Pair:
       return c.tab.rowshift && snl1_pair_ok(c.dev) ? kSnl1Pair : -1;
+    case kSnl1PairGeneral:
+      return c.tab.rowshift && snl1_pair_ok(c.dev) ? kSnl1PairGeneral : -1;
     default:
       return -1;
   }

@@ -1216,6 +1216,279 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_pair_kernel(
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Pair-tile kernel: the pair kernel with the direction count NTH, the band count G and the band
+// height BR known at compile time (36 directions: 8 bands of 5 rows), every row loop unrolled.
+// Each matrix has zero rows below row 0 (PADU for UE, PADA for the interaction arrays), so the
+// clamped rows MAX(0, IFR + IFRM - 1) and MAX(0, IFR - IFRP - 1) of INSNL1 read zeros without a
+// clamp (row 0 is zero too). Every row a thread touches is then its band's first row plus a
+// compile-time offset: each window column keeps one shared-memory pointer, set once per thread,
+// and every load and store in the unrolled rows is that pointer plus an immediate. Every band
+// runs all BR rows in both sections with no branch (the tables fill G x BR rows of section 3
+// exactly); section 4's rows above NFR are computed and not stored, their reads landing in the
+// next matrix or in DC's slack rows. The arithmetic of each bin is the pair kernel's (and so the
+// reference's), with the same rule for paired operations.
+__device__ __forceinline__ float2 mulS1(float w, float2 x) {
+  return make_float2(__fmul_rn(w, x.x), __fmul_rn(w, x.y));
+}
+
+template <int NTH, int G, int BR, int PADU, int PADA>
+struct PairTileShape {
+  static constexpr int kBlock = NTH * G;
+  static constexpr int kRowsA = PADA + 1 + G * BR;  ///< interaction-array rows -PADA .. G BR
+  static constexpr int kAS = kRowsA * NTH;          ///< float2 slots per interaction array
+  static constexpr int kRowsU = PADU + 1 + G * BR + PADA + 1;  ///< UE rows -PADU .. G BR + PADA + 1
+  static constexpr int kDcs = G * BR * NTH;  ///< DC slots: NSPEC and the rows above NFR
+};
+
+template <int NTH, int G, int BR, int PADU, int PADA, bool LIST>
+__global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
+    const Snl1Dev p, int npts, const float* __restrict__ a, const float* __restrict__ cg,
+    const float* __restrict__ kdmean, float* __restrict__ s, float* __restrict__ d,
+    int* __restrict__ err, const int* __restrict__ pidx, const int* __restrict__ pcount) {
+  using S = PairTileShape<NTH, G, BR, PADU, PADA>;
+  constexpr int BLOCK = S::kBlock, AS = S::kAS;
+  extern __shared__ __align__(16) float smem[];
+  if (LIST) npts = min(npts, __ldg(pcount));
+  auto pt = [&](int i) { return LIST ? __ldg(pidx + i) : i; };
+  const int npairs = (npts + 1) >> 1;
+  const int nfr = p.nfr, nfrchg = p.nfrchg, nspec = p.nspec, nk = p.nk;
+  float2* const ue0 = reinterpret_cast<float2*>(smem);  // row -PADU
+  float2* const ue = ue0 + PADU * NTH;                  // row 0
+  float2* const arr0 = ue0 + S::kRowsU * NTH;           // SA1 row -PADA; the others AS apart
+  float2* const arr = arr0 + PADA * NTH;                // SA1 row 0
+  float2* const dcs = arr0 + 6 * AS;
+  float2* const conx2 = dcs + S::kDcs;
+  float2* const cons2 = conx2 + 2 * nk;
+  float* const afr = reinterpret_cast<float*>(cons2 + 2);
+  const size_t stage_off =
+      (static_cast<size_t>(afr + nfrchg - smem) + 3) & ~static_cast<size_t>(3);
+  float* const stage = smem + stage_off;
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(stage + ((2 * (nspec + nk) + 3) & ~3));
+  const int tid = threadIdx.x;
+
+  auto first_of = [&](int pp) { return pt(2 * pp); };
+  auto second_of = [&](int pp) { return 2 * pp + 1 < npts ? pt(2 * pp + 1) : pt(2 * pp); };
+
+  // Zero rows -PADU..0 of UE and -PADA..0 of the six arrays, once per CTA.
+  {
+    const float2 z = make_float2(0.0f, 0.0f);
+    for (int i = tid; i < (PADU + 1) * NTH; i += BLOCK) ue0[i] = z;
+    for (int i = tid; i < (PADA + 1) * NTH; i += BLOCK)
+#pragma unroll
+      for (int m = 0; m < 6; ++m) arr0[m * AS + i] = z;
+  }
+  for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
+  float kd0 = 0.0f, kd1 = 0.0f;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    if (blockIdx.x < npairs) {
+      const int i0 = first_of(blockIdx.x), i1 = second_of(blockIdx.x);
+      tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk);
+      kd0 = __ldg(kdmean + i0);
+      kd1 = __ldg(kdmean + i1);
+    }
+  }
+  __syncthreads();
+
+  const int ith = tid % NTH, band = tid / NTH;
+  const int f0 = 1 + band * BR;
+  const int ifrp = p.ifrp, ifrm = p.ifrm;
+  int c[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c[j] = wrapc(ith + p.shift[j], NTH);
+  // Section 3: the bin's own row, the plus rows (IF1 = f + IFRP, IF2 = IF1 + 1; columns c0 c1
+  // c4 c5) and the minus rows (IF4 = f + IFRM - 1, IF3 = IF4 + 1; columns c2 c3 c6 c7).
+  const float2* const pe = ue + f0 * NTH + ith;
+  const float2* const pp0 = ue + (f0 + ifrp) * NTH;
+  const float2* const pm0 = ue + (f0 + ifrm - 1) * NTH;
+  float2* const po = arr + f0 * NTH + ith;
+  float2* const pd = dcs + (f0 - 1) * NTH + ith;
+  // Section 4: the lo rows (IF6 = f - IFRP - 1, IF5 = IF6 + 1; columns c4 c5 of SA1/DA1P, c0 c1
+  // of SA2/DA2P) and the hi rows (IF7 = f - IFRM, IF8 = IF7 + 1; columns c2 c3 of SA1/DA1M, c6 c7
+  // of SA2/DA2M).
+  const float2* const pl0 = arr + (f0 - ifrp - 1) * NTH;
+  const float2* const ph0 = arr + (f0 - ifrm) * NTH;
+  const float w0 = p.awg[0], w1 = p.awg[1], w2 = p.awg[2], w3 = p.awg[3];
+  const float w4 = p.awg[4], w5 = p.awg[5], w6 = p.awg[6], w7 = p.awg[7];
+  const float dal1 = p.dal1, dal2 = p.dal2, dal3 = p.dal3;
+  constexpr int dq = BLOCK / NTH, dr = BLOCK % NTH;
+  const int q0 = tid / NTH, r0 = tid % NTH;
+
+  unsigned parity = 0;
+  int buf = 0;
+  for (int pp = blockIdx.x; pp < npairs; pp += gridDim.x, buf ^= 1) {
+    const int i0 = first_of(pp), i1 = second_of(pp);
+    const bool has1 = 2 * pp + 1 < npts;
+    float2* const conx = conx2 + buf * nk;
+    const bool lost = !mbar_wait(bar, parity, err);
+    parity ^= 1u;
+    if (tid == 0) cons2[buf] = make_float2(dia_cons(p, kd0), dia_cons(p, kd1));
+    for (int k = tid; k < nk; k += BLOCK) {
+      const float w = kTpiInv / __ldg(p.sig + k);
+      conx[k] = make_float2(w * stage[2 * nspec + k], w * stage[2 * nspec + nk + k]);
+    }
+    if (__syncthreads_or(lost)) break;
+
+    // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
+    {
+      int ifr0 = q0, col = r0;
+      for (int isp = tid; isp < nspec; isp += BLOCK) {
+        const float2 cx = conx[ifr0];
+        const float2 v = make_float2(stage[isp] / cx.x, stage[nspec + isp] / cx.y);
+        ue[isp + NTH] = v;
+        if (ifr0 == nfr - 1) {
+          float2 t = v;
+          const float2 fh = dup2(p.fachfe);
+          for (int r = nfr + 1; r <= p.nfrhgh; ++r) {
+            t = mul2(t, fh);
+            ue[r * NTH + col] = t;
+          }
+        }
+        col += dr;
+        ifr0 += dq;
+        if (col >= NTH) {
+          col -= NTH;
+          ++ifr0;
+        }
+      }
+    }
+    __syncthreads();
+
+    const int pnext = pp + gridDim.x;
+    if (tid == 0 && pnext < npairs) {
+      const int j0 = first_of(pnext), j1 = second_of(pnext);
+      tma_fetch_pair(bar, stage, a, cg, j0, j1, nspec, nk);
+      kd0 = __ldg(kdmean + j0);
+      kd1 = __ldg(kdmean + j1);
+    }
+    const float2 cons = cons2[buf];
+
+    // 3. Interactions, BR rows unrolled.
+    {
+      float2 pa[4], pb[4], ma[4], mb[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int cp = c[j < 2 ? j : j + 2];  // c0 c1 c4 c5
+        const int cm = c[j < 2 ? j + 2 : j + 4];  // c2 c3 c6 c7
+        pa[j] = pp0[cp];
+        pb[j] = pp0[NTH + cp];
+        mb[j] = pm0[cm];
+        ma[j] = pm0[NTH + cm];
+      }
+#pragma unroll
+      for (int k = 0; k < BR; ++k) {
+        {
+          const int f = f0 + k;
+          const float2 e00 = pe[k * NTH];
+          const float2 ep1 = add2(add2(add2(mulS1(w0, pb[1]), mulS1(w1, pb[0])), mulS1(w2, pa[1])),
+                                  mulS1(w3, pa[0]));
+          const float2 em1 = add2(add2(add2(mulS1(w4, mb[3]), mulS1(w5, mb[2])), mulS1(w6, ma[3])),
+                                  mulS1(w7, ma[2]));
+          const float2 ep2 = add2(add2(add2(mulS1(w0, pb[3]), mulS1(w1, pb[2])), mulS1(w2, pa[3])),
+                                  mulS1(w3, pa[2]));
+          const float2 em2 = add2(add2(add2(mulS1(w4, mb[1]), mulS1(w5, mb[0])), mulS1(w6, ma[1])),
+                                  mulS1(w7, ma[0]));
+          const float2 ca = mul2(cons, dup2(afr[f - 1]));
+          const float2 factor = mul2(ca, e00);
+          const float2 sa1a = mulS(e00, add2(mulS1(dal1, ep1), mulS1(dal2, em1)));
+          const float2 sa1b = sub2(sa1a, mulS1(dal3, mul2(ep1, em1)));
+          const float2 sa2a = mulS(e00, add2(mulS1(dal1, ep2), mulS1(dal2, em2)));
+          const float2 sa2b = sub2(sa2a, mulS1(dal3, mul2(ep2, em2)));
+          po[k * NTH] = mul2(factor, sa1b);
+          po[AS + k * NTH] = mul2(factor, sa2b);
+          if (f <= nfr)
+            pd[k * NTH] = add2(mulS(ca, add2(sa1a, sa1b)), mulS(ca, add2(sa2a, sa2b)));
+          po[2 * AS + k * NTH] = mul2(factor, sub2(mulS1(dal1, e00), mulS1(dal3, em1)));
+          po[3 * AS + k * NTH] = mul2(factor, sub2(mulS1(dal2, e00), mulS1(dal3, ep1)));
+          po[4 * AS + k * NTH] = mul2(factor, sub2(mulS1(dal1, e00), mulS1(dal3, em2)));
+          po[5 * AS + k * NTH] = mul2(factor, sub2(mulS1(dal2, e00), mulS1(dal3, ep2)));
+          if (k + 1 < BR) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int cp = c[j < 2 ? j : j + 2];
+              const int cm = c[j < 2 ? j + 2 : j + 4];
+              pa[j] = pb[j];
+              mb[j] = ma[j];
+              pb[j] = pp0[(k + 2) * NTH + cp];
+              ma[j] = pm0[(k + 2) * NTH + cm];
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // 4. Source and diagonal terms, S then D, BR rows unrolled.
+    {
+      float2 l5[4], l6[4], h7[4], h8[4];
+      float* const sp0 = s + static_cast<size_t>(i0) * nspec + (f0 - 1) * NTH + ith;
+      float* const sp1 = s + static_cast<size_t>(i1) * nspec + (f0 - 1) * NTH + ith;
+      float* const dp0 = d + static_cast<size_t>(i0) * nspec + (f0 - 1) * NTH + ith;
+      float* const dp1 = d + static_cast<size_t>(i1) * nspec + (f0 - 1) * NTH + ith;
+      const float2 m2 = dup2(-2.0f);
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        // pass 0: S from SA1 (lo c4 c5, hi c2 c3) and SA2 (lo c0 c1, hi c6 c7);
+        // pass 1: D from DA1P/DA2P (lo) and DA1M/DA2M (hi).
+        const int o1l = pass == 0 ? 0 : 2 * AS, o2l = pass == 0 ? AS : 4 * AS;
+        const int o1h = pass == 0 ? 0 : 3 * AS, o2h = pass == 0 ? AS : 5 * AS;
+        const float v0 = pass == 0 ? w0 : p.swg[0], v1 = pass == 0 ? w1 : p.swg[1];
+        const float v2 = pass == 0 ? w2 : p.swg[2], v3 = pass == 0 ? w3 : p.swg[3];
+        const float v4 = pass == 0 ? w4 : p.swg[4], v5 = pass == 0 ? w5 : p.swg[5];
+        const float v6 = pass == 0 ? w6 : p.swg[6], v7 = pass == 0 ? w7 : p.swg[7];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int cl = j < 2 ? c[j + 4] : c[j - 2];  // c4 c5 | c0 c1
+          const int ch = j < 2 ? c[j + 2] : c[j + 4];  // c2 c3 | c6 c7
+          const int ol = j < 2 ? o1l : o2l, oh = j < 2 ? o1h : o2h;
+          l6[j] = pl0[ol + cl];
+          l5[j] = pl0[ol + NTH + cl];
+          h7[j] = ph0[oh + ch];
+          h8[j] = ph0[oh + NTH + ch];
+        }
+#pragma unroll
+        for (int k = 0; k < BR; ++k) {
+          const bool store = f0 + k <= nfr;
+          {
+            float2 t = pass == 0 ? mulS(m2, add2(po[k * NTH], po[AS + k * NTH]))
+                                 : mulS(m2, pd[k * NTH]);
+            t = add2(t, mulS1(v0, add2(l6[1], l6[3])));
+            t = add2(t, mulS1(v1, add2(l6[0], l6[2])));
+            t = add2(t, mulS1(v2, add2(l5[1], l5[3])));
+            t = add2(t, mulS1(v3, add2(l5[0], l5[2])));
+            t = add2(t, mulS1(v4, add2(h8[1], h8[3])));
+            t = add2(t, mulS1(v5, add2(h8[0], h8[2])));
+            t = add2(t, mulS1(v6, add2(h7[1], h7[3])));
+            t = add2(t, mulS1(v7, add2(h7[0], h7[2])));
+            if (pass == 0) {
+              const float2 sv = mul2(conx[f0 + k - 1], t);
+              if (store) __stcs(sp0 + k * NTH, sv.x);
+              if (store && has1) __stcs(sp1 + k * NTH, sv.y);
+            } else {
+              if (store) __stcs(dp0 + k * NTH, t.x);
+              if (store && has1) __stcs(dp1 + k * NTH, t.y);
+            }
+            if (k + 1 < BR) {
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const int cl = j < 2 ? c[j + 4] : c[j - 2];
+                const int ch = j < 2 ? c[j + 2] : c[j + 4];
+                const int ol = j < 2 ? o1l : o2l, oh = j < 2 ? o1h : o2h;
+                l6[j] = l5[j];
+                h7[j] = h8[j];
+                l5[j] = pl0[ol + (k + 2) * NTH + cl];
+                h8[j] = ph0[oh + (k + 2) * NTH + ch];
+              }
+            }
+          }
+        }
+      }
+    }
+    // The next pair's barriers order its writes of UE and the arrays after this section 4.
+  }
+}
+
 constexpr int kPairBlock = 288;
 constexpr int kPairMinBlocks = 2;  // 2 CTAs of 288 threads per SM: at most 113 registers
 constexpr int kPairStride = 1536;  // float2 slots per interaction array
@@ -1360,10 +1633,65 @@ void launch_band(const Snl1Dev& p, int npts, const float* a, const float* cg, co
   WWB_CHECK(cudaGetLastError());
 }
 
+// The pair-tile instance: 36 directions, 8 bands of 5 rows, zero rows 3 below UE and 2 below the
+// interaction arrays.
+using PairTile36 = PairTileShape<36, 8, 5, 3, 2>;
+
+/// Whether the 36-direction pair-tile instance fits these tables (every row it reads within its
+/// padded matrices, the bulk copies 16-byte sized).
+bool pairtile36_ok(const Snl1Dev& p) {
+  if (p.ifrow == nullptr || p.af11_row == nullptr || p.nth != 36) return false;
+  if (p.nspec % 4 != 0 || p.nk % 4 != 0) return false;
+  if (p.ifrp < 0 || p.ifrm > 0 || p.ifrp > 2 || -p.ifrm > 3) return false;
+  // Section 3 fills the 8 x 5 rows exactly; section 4's NFR rows fit in them.
+  if (p.nfr > 40 || p.nfrchg != 40 || p.nfrchg + p.ifrp + 1 > p.nfrhgh) return false;
+  if (p.nspec > PairTile36::kDcs) return false;
+  if (p.nfrhgh > 40 + 2 + 1 || p.nfr - p.ifrm + 1 > p.nfrchg) return false;
+  return true;
+}
+
+size_t pairtile36_smem(const Snl1Dev& p) {
+  using S = PairTile36;
+  size_t bytes = 8 * (static_cast<size_t>(S::kRowsU) * 36 + 6 * static_cast<size_t>(S::kAS) +
+                      S::kDcs + 2 * p.nk + 2) +
+                 4 * static_cast<size_t>(p.nfrchg);
+  bytes = (bytes + 15) & ~static_cast<size_t>(15);
+  bytes += 4 * ((2 * static_cast<size_t>(p.nspec + p.nk) + 3) & ~static_cast<size_t>(3));
+  return bytes + 16;  // + the mbarrier
+}
+
+template <bool LIST>
+void launch_pairtile36(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
+                       const float* a, const float* cg, const float* kd, float* s, float* d,
+                       int* err, cudaStream_t stream) {
+  static int per_sm = -1;
+  static size_t cached = 0;
+  const size_t smem = pairtile36_smem(p);
+  auto k = snl1_pairtile_kernel<36, 8, 5, 3, 2, LIST>;
+  if (per_sm < 0 || cached != smem) {
+    WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    int n = 0;
+    WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, PairTile36::kBlock, smem));
+    if (n < 1) throw CudaError(cudaErrorInvalidConfiguration, "snl1 pair-tile occupancy");
+    per_sm = n;
+    cached = smem;
+  }
+  const long long pairs = (static_cast<long long>(capacity) + 1) / 2;
+  const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
+  const int grid = static_cast<int>(pairs < resident ? pairs : resident);
+  k<<<grid, PairTile36::kBlock, smem, stream>>>(p, capacity, a, cg, kd, s, d, err, pidx, pcount);
+  WWB_CHECK(cudaGetLastError());
+}
+
+/// The pair kernel: its 36-direction tile instance where that fits (unless `general`), else
+/// its general form.
 template <bool LIST>
 void launch_pair(const Snl1Dev& p, int capacity, const int* pidx, const int* pcount,
                  const float* a, const float* cg, const float* kd, float* s, float* d, int* err,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, bool general = false) {
+  if (pairtile36_ok(p) && !general)
+    return launch_pairtile36<LIST>(p, capacity, pidx, pcount, a, cg, kd, s, d, err, stream);
   static int per_sm = -1;
   static size_t cached = 0;
   const size_t smem = snl1_pair_smem(p);
@@ -1408,14 +1736,16 @@ namespace {
 void launch_dispatch(int kernel, const Snl1Dev& p, int npts, const float* a, const float* cg,
                      const float* kdmean, float* s, float* d, int* err, cudaStream_t stream) {
   if (npts <= 0) return;
-  if (kernel == kSnl1Tile || kernel == kSnl1Band || kernel == kSnl1Pair) {
+  if (kernel == kSnl1Tile || kernel == kSnl1Band || kernel == kSnl1Pair ||
+      kernel == kSnl1PairGeneral) {
     if (err == nullptr) err = band_err_flag();
   }
   const bool aligned = (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
                        (reinterpret_cast<uintptr_t>(cg) & 15u) == 0;
-  if (kernel == kSnl1Pair) {
+  if (kernel == kSnl1Pair || kernel == kSnl1PairGeneral) {
     if (aligned && snl1_pair_ok(p))
-      return launch_pair<false>(p, npts, nullptr, nullptr, a, cg, kdmean, s, d, err, stream);
+      return launch_pair<false>(p, npts, nullptr, nullptr, a, cg, kdmean, s, d, err, stream,
+                                kernel == kSnl1PairGeneral);
     kernel = kSnl1Band;  // caller arrays not 16-byte aligned: the band kernel reads them directly
   }
   if (kernel == kSnl1Tile) {

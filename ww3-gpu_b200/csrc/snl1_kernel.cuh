@@ -32,6 +32,7 @@ enum Snl1Kernel {
   kSnl1Band = 3,
   kSnl1Tile = 4,
   kSnl1Pair = 5,  ///< the band kernel over two points at once (paired FP32 additions)
+  kSnl1PairGeneral = 6,  ///< the pair kernel's general form even where its 36-direction tile fits
 };
 
 /// Dynamic shared memory of each kernel, bytes.
