@@ -263,6 +263,7 @@ __device__ __forceinline__ void f32_chunk(const GemmArgs& g, int m_base, int n,
   for (int j = 0; j < 32; ++j)
     tile[lane * kStageLd + j] = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
   __syncwarp();
+#pragma unroll 8
   for (int rr = 0; rr < 32; ++rr) {
     const int mr = m_base + rr;
     if (mr < g.M) g.out_f32[static_cast<size_t>(mr) * g.ldo + n + lane] = tile[rr * kStageLd + lane];
@@ -311,29 +312,57 @@ __device__ __forceinline__ void sur_chunk(const GemmArgs& g, int m_base, int n, 
   const float s1 = (k - k0 + 1 < kRowsPerTile) ? rc0[2] : 0.0f;
   const float w1 = (k - k0 + 1 < kRowsPerTile) ? rc0[3] : 0.0f;
   const int valid = o.nspec - n;  // columns below NSPEC in this chunk
+  if (valid >= 32) {  // the common case: every column a spectral bin
 #pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const float v = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
-    const bool second = j >= jb;
-    const float sk = second ? s1 : s0, wk = second ? w1 : w0;
-    const bool in = j < valid;
-    racc += in ? wk * v : 0.0f;
-    gacc += in ? wk * fabsf(v) : 0.0f;
-    tile[lane * kStageLd + j] = in ? v * sk : v;
+    for (int j = 0; j < 32; ++j) {
+      const float v = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
+      const bool second = j >= jb;
+      const float sk = second ? s1 : s0, wk = second ? w1 : w0;
+      racc += wk * v;
+      gacc += wk * fabsf(v);
+      tile[lane * kStageLd + j] = v * sk;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float v = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
+      const bool second = j >= jb;
+      const float sk = second ? s1 : s0, wk = second ? w1 : w0;
+      const bool in = j < valid;
+      racc += in ? wk * v : 0.0f;
+      gacc += in ? wk * fabsf(v) : 0.0f;
+      tile[lane * kStageLd + j] = in ? v * sk : v;
+    }
   }
   __syncwarp();
+  // Row rr goes to S(m_base + rr, kj NTH + its own rotation of jl): lane = canonical column.
   const int i = n + lane;
   const int kj = i / o.nth, jl = i - kj * o.nth;
-  const bool col_in = i < o.nspec;
-  for (int rr = 0; rr < 32; ++rr) {
-    const int mr = m_base + rr;
-    const int shr = __shfl_sync(0xffffffffu, my_shift, rr);
-    if (mr < g.M) {
-      const float v = tile[rr * kStageLd + lane];
-      if (col_in)
-        o.s[static_cast<size_t>(mr) * o.nspec + kj * o.nth + orig_col(shr, jl, o.nth)] = v;
-      else if (i == o.nspec && o.head)
-        o.head[mr] = v;
+  const int nth = o.nth;
+  float* const srow = o.s + kj * nth;
+  if (valid >= 32) {
+#pragma unroll 8
+    for (int rr = 0; rr < 32; ++rr) {
+      const int mr = m_base + rr;
+      const int shr = __shfl_sync(0xffffffffu, my_shift, rr);
+      const int sh = shr & 0xFFFF;
+      int c = (shr >> 16) ? sh - jl : sh + jl;
+      c += c < 0 ? nth : 0;
+      c -= c >= nth ? nth : 0;
+      if (mr < g.M) srow[static_cast<size_t>(mr) * o.nspec + c] = tile[rr * kStageLd + lane];
+    }
+  } else {
+    const bool col_in = i < o.nspec;
+    for (int rr = 0; rr < 32; ++rr) {
+      const int mr = m_base + rr;
+      const int shr = __shfl_sync(0xffffffffu, my_shift, rr);
+      if (mr < g.M) {
+        const float v = tile[rr * kStageLd + lane];
+        if (col_in)
+          o.s[static_cast<size_t>(mr) * o.nspec + kj * o.nth + orig_col(shr, jl, o.nth)] = v;
+        else if (i == o.nspec && o.head)
+          o.head[mr] = v;
+      }
     }
   }
   __syncwarp();
@@ -357,8 +386,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                 const GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t* const smem = reinterpret_cast<uint8_t*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  // The 1024-byte aligned base as an offset into the shared array (not through an integer
+  // cast), so the compiler keeps every derived pointer in the shared space (LDS/STS).
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const uint32_t stage_sz = stage_bytes(g.bn);
   Bars* const bars = reinterpret_cast<Bars*>(smem + kStages * stage_sz);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
