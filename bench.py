@@ -512,8 +512,8 @@ def run_b200_srce(args, quiet=False, npts=None, steps=None, warmup=None, igrid=1
     pkg = entry.load_package()
     synth = __import__("ww3_gpu_b200.synth", fromlist=["synth"])
     npts = npts or args.npts
-    steps = steps or steps
-    warmup = warmup or warmup
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     st, t, sr, cfg, sig, pts = srce_inputs(synth, npts, 2026 + rank)
     grid = pkg.SrceGrid(igrid, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig, sr)
     dev = torch.device("cuda", local)
@@ -938,8 +938,9 @@ MULTI_NGRIDS = 16
 MULTI_WORKLOAD = ("{ngrids} regional grids of uneven size (sea points log-uniform in {lo}-{hi}, "
                   "seeded; {total} in all), each with its own wind field and depth, 36x36: every "
                   "grid's resident whole step (W3KTP3, W3XYP3, W3KTP3, W3SRCE + ST4 + DIA) "
-                  "recorded once as a CUDA graph, all grids' graphs replayed one after another "
-                  "per step (ww_steps_run)")
+                  "recorded once, the grids' steps fused into one CUDA graph with ONE persistent "
+                  "W3SRCE launch over all grids' points (ww_steps_fuse, one work queue), replayed "
+                  "once per step (ww_steps_run)")
 
 
 def multi_shapes(scale, seed=2026):
@@ -991,15 +992,29 @@ def run_b200_multigrid(args):
             grid.batch_va(nsea, v, jsea, pk["wn1"], pk["cg1"], pk["pin"], pk["psc"],
                           pk["whitecap"], pk["taubbl"], pk["tauice"], shave)
 
-        one = step_calls((lambda c, it, v, ig=ig: pkg.ktp3_batch(c, it, 1, ig, v),
-                          lambda c, v, ig=ig: pkg.xyp3_batch(c, ig, v), srce), va, kc, xc, pts,
-                         nsea)
-        step = pkg.Step(ig)
-        with step:
-            one()
-        grids.append({"ig": ig, "nsea": nsea, "va": va, "step": step, "grid": grid,
+        calls = (lambda c, it, v, ig=ig: pkg.ktp3_batch(c, it, 1, ig, v),
+                 lambda c, v, ig=ig: pkg.xyp3_batch(c, ig, v), srce)
+        grids.append({"ig": ig, "nsea": nsea, "va": va, "va0": np.array(va, copy=True),
+                      "calls": calls, "inputs": (kc, xc, pts), "step": None, "grid": grid,
                       "nx": nx, "ny": ny})
     igs = [g["ig"] for g in grids]
+    L = pkg.lib()
+
+    def record_all():
+        """Every grid's step recorded from its initial VA and packets, so each variant times
+        the same steps."""
+        for g in grids:
+            if g["step"] is not None:
+                g["step"].free()
+            v = g["va"]
+            if L.ww_va_state(g["ig"]) >= 0:  # the host takes the VA back before it writes it
+                assert L.ww_va_host_write(g["ig"], v.ctypes.data, v.shape[1], v.shape[0] - 1) == 0
+            v[...] = g["va0"]
+            kc, xc, pts = g["inputs"]
+            step = pkg.Step(g["ig"])
+            with step:
+                step_calls(g["calls"], v, kc, xc, pts, g["nsea"])()
+            g["step"] = step
     total = sum(g["nsea"] for g in grids)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -1030,24 +1045,34 @@ def run_b200_multigrid(args):
 
     together = lambda: pkg.steps_run(igs, 1, handle)  # noqa: E731
 
-    def one_by_one():
-        for g in grids:
-            g["step"].run(1, handle)
-
+    # The grids' graphs one after another (the unfused form), from the initial state.
+    record_all()
+    pkg.steps_fuse([])
+    for _ in range(args.warmup):
+        together()
+    seq_ms, _ = timed(together, args.steps)
+    seq_value = total * world * args.steps / (seq_ms / 1e3)
+    # The fused graph: one W3SRCE launch over all grids' points, the same steps.
+    record_all()
+    pkg.steps_fuse(igs)
     for _ in range(args.warmup):
         together()
     barrier()
     with ClockSampler(local) as clk:
         time.sleep(0.3)
         total_ms, per = timed(together, args.steps)
-    seq_ms, _ = timed(one_by_one, max(1, min(args.steps, 3)))
-    seq_steps = max(1, min(args.steps, 3))
     value = total * world * args.steps / (total_ms / 1e3)
-    seq_value = total * world * seq_steps / (seq_ms / 1e3)
 
-    # ---- end to end: every grid's host VA uploaded, the combined step, every VA read back
-    L = pkg.lib()
-    e2e_steps = args.e2e_steps or max(2, min(args.steps, 3))
+    # ---- end to end: the same steps again from the initial state, every grid's host VA
+    # uploaded, the fused step, every VA read back
+    record_all()
+    pkg.steps_fuse(igs)
+    for _ in range(args.warmup):
+        together()
+    for g in grids:
+        v = g["va"]
+        assert L.ww_va_host_read(g["ig"], v.ctypes.data, v.shape[1], v.shape[0] - 1) == 0
+    e2e_steps = args.steps
 
     def host_step():
         for g in grids:
@@ -1058,7 +1083,6 @@ def run_b200_multigrid(args):
             v = g["va"]
             assert L.ww_va_host_read(g["ig"], v.ctypes.data, v.shape[1], v.shape[0] - 1) == 0
 
-    host_step()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -1079,12 +1103,14 @@ def run_b200_multigrid(args):
                    "nk": NK, "nth": NTH, "ngrids": len(grids), "scale": args.scale,
                    "grids": [[g["nx"], g["ny"], g["nsea"]] for g in grids],
                    "sea_points_per_gpu": total, "dtg_s": 900.0,
-                   "source_terms": "plain DIA (the learned surrogate is not built)",
+                   "source_terms": "plain DIA (the surrogate is not used inside W3SRCE)",
                    "l2": "the grids' resident VAs together are larger than L2",
                    "parallelism": f"all grids on each GPU ({world}), no collective"},
-        "sequential": {"value": seq_value, "unit": UNIT, "steps": seq_steps,
-                       "ms_per_step": seq_ms / seq_steps,
-                       "note": "the same recorded steps replayed grid after grid (ww_step_run)"},
+        "unfused": {"value": seq_value, "unit": UNIT, "steps": args.steps,
+                    "ms_per_step": seq_ms / args.steps,
+                    "note": ("the same steps from the same initial state, the grids' recorded "
+                             "graphs replayed one after another (one W3SRCE launch per grid)")},
+        "fused_speedup": seq_ms / total_ms,
         "e2e": {"value": total * world * e2e_steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": va_bytes, "d2h_bytes_per_step": va_bytes,
                 "steps": e2e_steps,
@@ -1092,9 +1118,9 @@ def run_b200_multigrid(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "traffic": None, "kernel": "the combined step graph (srce_kernel dominant)",
+                     "traffic": None, "kernel": "the fused step graph (srce_multi_kernel dominant)",
                      "launch_ms": step_ms, "algorithmic_bytes_per_point": STEP_BYTES_PER_POINT},
-        "gpu_launches": sum(g["step"].nodes() for g in grids) * args.steps,
+        "gpu_launches": (sum(g["step"].nodes() for g in grids) - 2 * len(grids) + 2) * args.steps,
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

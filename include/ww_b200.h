@@ -302,6 +302,13 @@ int ww_step_free(int igrid);
  * returning): several regional grids of uneven size on one GPU in one call, with no host work
  * besides the graph launches. Return WwKokkosStatus. */
 int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream);
+/* B200 extension: merges the recorded steps of ngrids distinct grids (each with exactly one
+ * ww_srce_batch_va call, all with the same spectral grid and ST4 tables) into one graph: every
+ * grid's calls before its W3SRCE batch, then ONE persistent W3SRCE launch over all the grids'
+ * points with a single work queue, then the calls after. ww_steps_run with the same list (same
+ * order) replays it instead of the grids' graphs one after another; recording or freeing a
+ * member grid's step drops it, as does ngrids == 0. Return WwKokkosStatus. */
+int ww_steps_fuse(const int* igrids, int ngrids);
 /* The number of calls the grid's step holds, or -1 for a grid without one. */
 int ww_step_ops(int igrid);
 /* The number of nodes (kernels, memsets) of the grid's captured step graph, or -1. */

@@ -220,5 +220,18 @@ def test_steps_run_grids_side_by_side(pkg, oracle, synth):
         assert not np.array_equal(va_com[k], cases[k][0]["va"])
     with pytest.raises(pkg.WwError):
         pkg.steps_run([730, 730], 1)  # a grid listed twice
-    for s in sep_steps + com_steps:
+    # The same steps fused: every grid's propagation, then one W3SRCE launch over all 3 grids'
+    # points with one work queue; bit-equal to the grids' own graphs.
+    fus_calls, fus_steps = record(740)
+    pkg.steps_fuse([740, 741, 742])
+    pkg.steps_run([740, 741, 742], 2)
+    va_fus = [np.array(c.read(), copy=True) for c in fus_calls]
+    for k in range(3):
+        assert_bitexact(va_fus[k], va_sep[k], f"grid {k}: fused W3SRCE launch vs ww_step_run")
+    with pytest.raises(pkg.WwError):
+        pkg.steps_fuse([740, 740])  # a grid listed twice
+    with pytest.raises(pkg.WwError):
+        pkg.steps_fuse([740, 799])  # a grid with no recorded step
+    pkg.steps_fuse([])
+    for s in sep_steps + com_steps + fus_steps:
         s.free()

@@ -41,7 +41,7 @@ EXPORTS = (
     "ww_kokkos_flag", "ww_kokkos_preset_status", "ww_kokkos_strict", "ww_kokkos_fallback_slot",
     "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
-    "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_ktp3_batch", "ww_ktp3_batch_va",
+    "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_steps_fuse", "ww_ktp3_batch", "ww_ktp3_batch_va",
     "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va", "ww_snl1_noalloc",
     "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_sds4", "ww_sin4",
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
@@ -541,8 +541,21 @@ class Step:
         self.L.ww_step_free(self.igrid)
 
 
+def steps_fuse(igrids):
+    """ww_steps_fuse: merge the recorded steps of these grids into one graph with a single W3SRCE
+    launch over all their points (an empty list drops it)."""
+    L = lib()
+    L.ww_steps_fuse.argtypes = [_P, _I]
+    L.ww_steps_fuse.restype = _I
+    ids = np.ascontiguousarray(igrids, np.int32)
+    rc = L.ww_steps_fuse(ids.ctypes.data if ids.size else None, ids.size)
+    if rc != OK:
+        raise WwError("ww_steps_fuse", rc)
+
+
 def steps_run(igrids, nrep=1, stream=None):
-    """ww_steps_run: the recorded steps of several grids replayed one grid after another."""
+    """ww_steps_run: the recorded steps of several grids replayed one grid after another (or as
+    their fused graph when ww_steps_fuse built one for this list)."""
     L = lib()
     L.ww_steps_run.argtypes = [_P, _I, _I, _P]
     L.ww_steps_run.restype = _I

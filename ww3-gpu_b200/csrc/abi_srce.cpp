@@ -138,10 +138,16 @@ void run_batch(int igrid, GridCtx& g, const SrceStep& step, int npts, float* spe
     step_keep(rec, dk);
     const pt::SrceLayout L = host.L;
     SrceWork* const w = work.get();
-    step_add(rec, [=](cudaStream_t ss) {
-      launch_srce(d, L, step, npts, va_dev, djsea, dwn, dcg, dpin, dpsc, dwc, dtb, dti, dsh, *w,
-                  ss);
-    });
+    auto job = std::make_shared<SrceRecorded>();
+    job->job = SrceJob{d, step, npts, 0, va_dev, djsea, dwn, dcg, dpin, dpsc, dwc, dtb, dti, dsh};
+    job->L = L;
+    step_add(
+        rec,
+        [=](cudaStream_t ss) {
+          launch_srce(d, L, step, npts, va_dev, djsea, dwn, dcg, dpin, dpsc, dwc, dtb, dti, dsh,
+                      *w, ss);
+        },
+        job);
     g_status.ok();
     return;
   }

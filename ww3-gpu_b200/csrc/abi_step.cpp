@@ -11,10 +11,12 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <vector>
 
+#include "st4_srce.cuh"
 #include "step.hpp"
 #include "va.hpp"
 #include "wwb_common.hpp"
@@ -24,6 +26,7 @@ namespace wwb {
 struct StepRecorder {
   bool recording = false;
   std::vector<std::function<void(cudaStream_t)>> ops;
+  std::vector<std::shared_ptr<void>> srce_jobs;  ///< per op: its W3SRCE job (SrceRecorded) or null
   std::vector<std::shared_ptr<void>> keep;
   cudaStream_t stage = nullptr;  ///< staging stream of the recorded calls
   cudaGraph_t graph = nullptr;
@@ -38,6 +41,7 @@ struct StepRecorder {
   void clear() {
     drop_graph();
     ops.clear();
+    srce_jobs.clear();
     keep.clear();
     recording = false;
     nops = 0;
@@ -68,6 +72,44 @@ StepRecorder* find(int igrid) {
   return it == recs().end() ? nullptr : it->second.get();
 }
 
+/// Several grids' recorded steps merged into one graph (ww_steps_fuse): every grid's calls
+/// before its W3SRCE batch, one W3SRCE launch over all the grids' points, then the calls after.
+struct FusedSteps {
+  std::vector<int> grids;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  SrceJob* jobs = nullptr;  ///< device copy of the jobs
+  SrceWork work;
+  int total = 0;
+  void clear() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (jobs) cudaFree(jobs);
+    work.release();
+    exec = nullptr;
+    graph = nullptr;
+    jobs = nullptr;
+    grids.clear();
+    total = 0;
+  }
+  ~FusedSteps() { clear(); }
+};
+
+FusedSteps& fused() {
+  static auto* f = new FusedSteps();
+  return *f;
+}
+
+/// A grid's recorded step changes or goes: a fused graph that holds it goes too.
+void drop_fused_with(int igrid) {
+  FusedSteps& f = fused();
+  for (int g : f.grids)
+    if (g == igrid) {
+      f.clear();
+      return;
+    }
+}
+
 template <class F>
 int guarded(F&& f) {
   try {
@@ -88,8 +130,10 @@ StepRecorder* step_recorder(int igrid) {
 
 void step_keep(StepRecorder* r, std::shared_ptr<void> obj) { r->keep.push_back(std::move(obj)); }
 
-void step_add(StepRecorder* r, std::function<void(cudaStream_t)> op) {
+void step_add(StepRecorder* r, std::function<void(cudaStream_t)> op,
+              std::shared_ptr<void> srce_job) {
   r->ops.push_back(std::move(op));
+  r->srce_jobs.push_back(std::move(srce_job));
 }
 
 cudaStream_t step_stream(StepRecorder* r) { return r->stage; }
@@ -116,6 +160,7 @@ void free_table(void* p) {
 }
 
 void release_steps() {
+  fused().clear();
   recs().clear();
   flush_retired();
 }
@@ -132,7 +177,8 @@ int ww_step_begin(int igrid) {
     auto& r = recs()[igrid];
     if (!r) r = std::make_unique<StepRecorder>();
     if (r->recording) return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_step_begin: already recording");
-    // Recording again replaces the grid's step.
+    // Recording again replaces the grid's step (and a fused graph that holds it).
+    drop_fused_with(igrid);
     r->clear();
     if (!r->stage) WWB_CHECK(cudaStreamCreateWithFlags(&r->stage, cudaStreamNonBlocking));
     r->recording = true;
@@ -214,8 +260,16 @@ int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream) {
         if (int rc = va_device_current(igrids[k]); rc != WW_KOKKOS_OK)
           return g_step.fail(rc, "ww_steps_run: a grid's VA could not be made current on the device");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : runtime().stream;
-    for (int i = 0; i < nrep; ++i)
-      for (StepRecorder* r : rs) WWB_CHECK(cudaGraphLaunch(r->exec, s));
+    const FusedSteps& f = fused();
+    const bool use_fused =
+        f.exec != nullptr && f.grids == std::vector<int>(igrids, igrids + ngrids);
+    for (int i = 0; i < nrep; ++i) {
+      if (use_fused) {
+        WWB_CHECK(cudaGraphLaunch(f.exec, s));
+      } else {
+        for (StepRecorder* r : rs) WWB_CHECK(cudaGraphLaunch(r->exec, s));
+      }
+    }
     if (nrep > 0)
       for (int k = 0; k < ngrids; ++k) va_device_written(igrids[k]);
     if (!stream) WWB_CHECK(cudaStreamSynchronize(s));
@@ -224,7 +278,86 @@ int ww_steps_run(const int* igrids, int ngrids, int nrep, void* stream) {
   });
 }
 
+int ww_steps_fuse(const int* igrids, int ngrids) {
+  return guarded([&] {
+    FusedSteps& f = fused();
+    f.clear();
+    if (ngrids == 0) {
+      g_step.ok();
+      return static_cast<int>(WW_KOKKOS_OK);
+    }
+    if (igrids == nullptr || ngrids < 1)
+      return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_fuse: bad grid list");
+    std::vector<StepRecorder*> rs;
+    std::vector<int> at;  // index of each grid's W3SRCE batch among its recorded calls
+    std::vector<SrceJob> jobs;
+    pt::SrceLayout L{};
+    int total = 0;
+    for (int k = 0; k < ngrids; ++k) {
+      for (int j = 0; j < k; ++j)
+        if (igrids[j] == igrids[k])
+          return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_fuse: a grid is listed twice");
+      StepRecorder* r = find(igrids[k]);
+      if (!r || r->recording || !r->exec)
+        return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_fuse: a grid has no recorded step");
+      int idx = -1, count = 0;
+      for (size_t i = 0; i < r->srce_jobs.size(); ++i)
+        if (r->srce_jobs[i]) {
+          idx = static_cast<int>(i);
+          ++count;
+        }
+      if (count != 1)
+        return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE,
+                           "ww_steps_fuse: every grid's step needs exactly one W3SRCE batch");
+      const auto* rec = static_cast<const SrceRecorded*>(r->srce_jobs[idx].get());
+      if (k == 0) L = rec->L;
+      if (std::memcmp(&L, &rec->L, sizeof L) != 0)
+        return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE,
+                           "ww_steps_fuse: the grids' W3SRCE working sets differ (spectral grid or ST4 tables)");
+      SrceJob j = rec->job;
+      j.first = total;
+      if (static_cast<long long>(total) + j.npts > (1LL << 30))
+        return g_step.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_steps_fuse: too many points");
+      total += j.npts;
+      jobs.push_back(j);
+      rs.push_back(r);
+      at.push_back(idx);
+    }
+    WWB_CHECK(cudaMalloc(&f.jobs, jobs.size() * sizeof(SrceJob)));
+    WWB_CHECK(cudaMemcpy(f.jobs, jobs.data(), jobs.size() * sizeof(SrceJob), cudaMemcpyHostToDevice));
+    srce_multi_reserve(L, total, f.work);
+    f.total = total;
+    cudaStream_t cap = nullptr;
+    WWB_CHECK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    WWB_CHECK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed));
+    bool failed = false;
+    try {
+      for (size_t k = 0; k < rs.size(); ++k)
+        for (int i = 0; i < at[k]; ++i) rs[k]->ops[i](cap);
+      launch_srce_multi(f.jobs, static_cast<int>(jobs.size()), total, L, f.work, cap);
+      for (size_t k = 0; k < rs.size(); ++k)
+        for (size_t i = at[k] + 1; i < rs[k]->ops.size(); ++i) rs[k]->ops[i](cap);
+    } catch (...) {
+      failed = true;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (failed || e != cudaSuccess || g == nullptr) {
+      if (g) cudaGraphDestroy(g);
+      f.clear();
+      return g_step.fail(WW_KOKKOS_ERR_KERNEL, "ww_steps_fuse: the launches could not be captured");
+    }
+    f.graph = g;
+    WWB_CHECK(cudaGraphInstantiate(&f.exec, f.graph, 0));
+    f.grids.assign(igrids, igrids + ngrids);
+    g_step.ok();
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
 int ww_step_free(int igrid) {
+  drop_fused_with(igrid);
   StepRecorder* r = find(igrid);
   if (r) r->clear();
   if (!any_step()) flush_retired();

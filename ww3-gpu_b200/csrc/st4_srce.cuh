@@ -85,6 +85,37 @@ void launch_spr4(const St4Dev* d, const st4::Params& hp, int npts, const float* 
 /// fit), so that a later launch allocates nothing.
 void srce_reserve(const pt::SrceLayout& L, int npts, SrceWork& work, cudaStream_t st);
 
+/// One grid's share of a W3SRCE launch over several grids: its tables (d), step flags, points
+/// [first, first + npts) of the launch's work queue and its arrays (as launch_srce takes them).
+struct SrceJob {
+  const SrceDev* d;
+  SrceStep step;
+  int npts, first;
+  float* spec;
+  const int* jsea;
+  const float *wn1, *cg1, *pin;
+  float *psc, *whitecap, *taubbl, *tauice;
+  int* shave;
+};
+
+/// A recorded W3SRCE batch: its job (first unset) and working-set layout.
+struct SrceRecorded {
+  SrceJob job;
+  pt::SrceLayout L;
+};
+
+/// CTAs of a W3SRCE launch on npts points of these tables (the resident grid, at most npts).
+int srce_resident_ctas(const pt::SrceLayout& L, int npts);
+
+/// Allocates launch_srce_multi's work buffers for `total` points of layout L (synchronous).
+void srce_multi_reserve(const pt::SrceLayout& L, int total, SrceWork& work);
+
+/// W3SRCE over several grids' points in one persistent launch with one work queue: jobs_dev
+/// (device, njobs entries in order of `first`, total points) all of layout L, work reserved for
+/// `total` points (srce_reserve). Launch work only, so it can be captured in a graph.
+void launch_srce_multi(const SrceJob* jobs_dev, int njobs, int total, const pt::SrceLayout& L,
+                       SrceWork& work, cudaStream_t st);
+
 /// W3SRCE for npts points on a persistent grid whose CTAs take points from a work queue
 /// (work.counter, zeroed here), so points with many substeps do not hold up the rest. Point n's
 /// spectrum is spec + n * nspec, or, with jsea non-null, the resident VA column

@@ -84,6 +84,41 @@ __global__ void __launch_bounds__(kSt4Block) spr4_kernel(
   }
 }
 
+/// One sea point of a W3SRCE batch by the whole CTA: its spectrum (VA column jsea[n], or row n)
+/// and packets into the working set, srce_point, and back. w is the CTA's dynamic shared
+/// memory, gw its slice of the global scratch.
+__device__ __forceinline__ void srce_one(const SrceDev* __restrict__ d, const SrceStep& step,
+                                         int n, float* spec, const int* jsea, const float* wn1,
+                                         const float* cg1, const float* pin, float* psc,
+                                         float* whitecap, float* taubbl, float* tauice,
+                                         int* shave, float* w, float* gw, pt::SrceSh& sh) {
+  const pt::SrceLayout& L = d->L;
+  const int ns = L.nspec, nk = L.nk;
+  const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  float* const sp = spec + (jsea ? static_cast<size_t>(jsea[n]) : static_cast<size_t>(n)) * ns;
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) w[L.spec + i] = sp[i];
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+    w[L.wn1 + i] = wn1[static_cast<size_t>(n) * nk + i];
+    w[L.cg1 + i] = cg1[static_cast<size_t>(n) * nk + i];
+  }
+  if (threadIdx.x == 0)
+    pt::srce_psc_in(sh, psc + static_cast<size_t>(n) * srce::NPSC,
+                    whitecap + 4 * static_cast<size_t>(n), taubbl + 2 * static_cast<size_t>(n),
+                    tauice + 2 * static_cast<size_t>(n));
+  __syncthreads();
+  const pt::SrceCtx x{&d->p, &d->g, &d->q, &d->f, &d->n,
+                      pt::srce_in(step.it, step.inflags24, step.flogrd57, step.flogrd58, step.dtg,
+                                  pin + static_cast<size_t>(n) * srce::NPIN),
+                      w, gw, &L, &sh};
+  pt::srce_point(cta, x);
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) sp[i] = w[L.spec + i];
+  if (threadIdx.x == 0)
+    pt::srce_psc_out(sh, psc + static_cast<size_t>(n) * srce::NPSC,
+                     whitecap + 4 * static_cast<size_t>(n), taubbl + 2 * static_cast<size_t>(n),
+                     tauice + 2 * static_cast<size_t>(n), shave + n);
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kSrceBlock, kSrceMinBlocks) srce_kernel(
     const SrceDev* __restrict__ d, SrceStep step, int npts, float* spec, const int* jsea,
     const float* wn1, const float* cg1, const float* pin, float* psc, float* whitecap,
@@ -91,38 +126,41 @@ __global__ void __launch_bounds__(kSrceBlock, kSrceMinBlocks) srce_kernel(
   extern __shared__ __align__(16) float w[];
   __shared__ pt::SrceSh sh;
   __shared__ int cur;
-  const pt::SrceLayout& L = d->L;
-  const int ns = L.nspec, nk = L.nk;
-  float* const gw = scratch + static_cast<size_t>(blockIdx.x) * static_cast<size_t>(L.total_g);
-  const pt::Cta cta{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  float* const gw = scratch + static_cast<size_t>(blockIdx.x) * static_cast<size_t>(d->L.total_g);
   for (;;) {
     if (threadIdx.x == 0) cur = atomicAdd(counter, 1);
     __syncthreads();
     const int n = cur;
     if (n >= npts) break;
-    float* const sp =
-        spec + (jsea ? static_cast<size_t>(jsea[n]) : static_cast<size_t>(n)) * ns;
-    for (int i = threadIdx.x; i < ns; i += blockDim.x) w[L.spec + i] = sp[i];
-    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
-      w[L.wn1 + i] = wn1[static_cast<size_t>(n) * nk + i];
-      w[L.cg1 + i] = cg1[static_cast<size_t>(n) * nk + i];
+    srce_one(d, step, n, spec, jsea, wn1, cg1, pin, psc, whitecap, taubbl, tauice, shave, w, gw,
+             sh);
+  }
+}
+
+/// W3SRCE over the points of several grids in one persistent launch: one work queue over
+/// (grid, point), the job of queue entry q the last one whose first entry is <= q. Every job has
+/// the same working-set layout (checked on the host), so one CTA takes any grid's points.
+__global__ void __launch_bounds__(kSrceBlock, kSrceMinBlocks) srce_multi_kernel(
+    const SrceJob* __restrict__ jobs, int njobs, int total, int* counter, float* scratch) {
+  extern __shared__ __align__(16) float w[];
+  __shared__ pt::SrceSh sh;
+  __shared__ int cur;
+  float* const gw =
+      scratch + static_cast<size_t>(blockIdx.x) * static_cast<size_t>(jobs[0].d->L.total_g);
+  for (;;) {
+    if (threadIdx.x == 0) cur = atomicAdd(counter, 1);
+    __syncthreads();
+    const int q = cur;
+    if (q >= total) break;
+    int lo = 0, hi = njobs - 1;  // the job holding q: first[lo] <= q < first[lo + 1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].first <= q) lo = mid;
+      else hi = mid - 1;
     }
-    if (threadIdx.x == 0)
-      pt::srce_psc_in(sh, psc + static_cast<size_t>(n) * srce::NPSC,
-                      whitecap + 4 * static_cast<size_t>(n), taubbl + 2 * static_cast<size_t>(n),
-                      tauice + 2 * static_cast<size_t>(n));
-    __syncthreads();
-    const pt::SrceCtx x{&d->p, &d->g, &d->q, &d->f, &d->n,
-                        pt::srce_in(step.it, step.inflags24, step.flogrd57, step.flogrd58,
-                                    step.dtg, pin + static_cast<size_t>(n) * srce::NPIN),
-                        w, gw, &L, &sh};
-    pt::srce_point(cta, x);
-    for (int i = threadIdx.x; i < ns; i += blockDim.x) sp[i] = w[L.spec + i];
-    if (threadIdx.x == 0)
-      pt::srce_psc_out(sh, psc + static_cast<size_t>(n) * srce::NPSC,
-                       whitecap + 4 * static_cast<size_t>(n), taubbl + 2 * static_cast<size_t>(n),
-                       tauice + 2 * static_cast<size_t>(n), shave + n);
-    __syncthreads();
+    const SrceJob& j = jobs[lo];
+    srce_one(j.d, j.step, q - j.first, j.spec, j.jsea, j.wn1, j.cg1, j.pin, j.psc, j.whitecap,
+             j.taubbl, j.tauice, j.shave, w, gw, sh);
   }
 }
 
@@ -200,6 +238,42 @@ void srce_reserve(const pt::SrceLayout& L, int npts, SrceWork& work, cudaStream_
     WWB_CHECK(cudaMalloc(&work.scratch, need * sizeof(float)));
     work.scratch_n = need;
   }
+}
+
+int srce_resident_ctas(const pt::SrceLayout& L, int npts) {
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  return resident_grid(srce_kernel, smem, npts, kSrceBlock);
+}
+
+void srce_multi_reserve(const pt::SrceLayout& L, int total, SrceWork& work) {
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  const int grid = resident_grid(srce_multi_kernel, smem, total > 0 ? total : 1, kSrceBlock);
+  const size_t need = static_cast<size_t>(grid) * static_cast<size_t>(L.total_g);
+  if (work.counter == nullptr) WWB_CHECK(cudaMalloc(&work.counter, sizeof(int)));
+  if (need > work.scratch_n) {
+    if (work.scratch) WWB_CHECK(cudaFree(work.scratch));
+    work.scratch = nullptr;
+    work.scratch_n = 0;
+    WWB_CHECK(cudaMalloc(&work.scratch, need * sizeof(float)));
+    work.scratch_n = need;
+  }
+}
+
+void launch_srce_multi(const SrceJob* jobs_dev, int njobs, int total, const pt::SrceLayout& L,
+                       SrceWork& work, cudaStream_t st) {
+  if (total <= 0) return;
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  const int grid = resident_grid(srce_multi_kernel, smem, total, kSrceBlock);
+  if (work.counter == nullptr ||
+      static_cast<size_t>(grid) * static_cast<size_t>(L.total_g) > work.scratch_n)
+    throw CudaError(cudaErrorInvalidValue, "launch_srce_multi: work buffers not reserved");
+  WWB_CHECK(cudaMemsetAsync(work.counter, 0, sizeof(int), st));
+  srce_multi_kernel<<<grid, kSrceBlock, smem, st>>>(jobs_dev, njobs, total, work.counter,
+                                                    work.scratch);
+  WWB_CHECK(cudaGetLastError());
 }
 
 void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int npts,

@@ -22,7 +22,10 @@ void step_keep(StepRecorder* r, std::shared_ptr<void> obj);
 
 /// Appends a recorded call's launches: kernels, memsets and device-to-device work only, no
 /// host synchronisation, allocation or host memory, so that a stream capture can record them.
-void step_add(StepRecorder* r, std::function<void(cudaStream_t)> op);
+/// A W3SRCE batch also passes its launch as a job (a SrceJob with its layout), so that the
+/// batches of several grids' steps can be merged into one launch (ww_steps_fuse).
+void step_add(StepRecorder* r, std::function<void(cudaStream_t)> op,
+              std::shared_ptr<void> srce_job = nullptr);
 
 /// The stream a recorded call stages its inputs on (synchronise it before returning).
 cudaStream_t step_stream(StepRecorder* r);
