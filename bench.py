@@ -86,6 +86,8 @@ def parse():
     p.add_argument("--npts", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="skip the autotuner (DIA kernel, W3SRCE CTAs per SM) before timing")
     p.add_argument("--train-steps", type=int, default=30000,
                    help="surrogate workload: AdamW steps of batch 8192 before the timing")
     p.add_argument("--sur-lr", type=float, default=1e-3)
@@ -299,11 +301,13 @@ def run_b200_dia(args):
                   "tile": pkg.KERNEL_TILE, "pair": pkg.KERNEL_PAIR,
                   "pair-general": pkg.KERNEL_PAIR_GENERAL}
     grid.select_kernel(kernel_ids[args.kernel])
+    cur = grid.select_kernel(kernel_ids[args.kernel])  # the kernel that choice resolves to
+    if args.kernel == "auto" and not args.no_autotune:
+        cur = pkg.snl1_autotune(1)
     kernel_name = {pkg.KERNEL_GATHER: "snl1_gather_kernel", pkg.KERNEL_ROWSHIFT:
                    "snl1_rowshift_kernel", pkg.KERNEL_BAND: "snl1_band_kernel",
                    pkg.KERNEL_TILE: "snl1_tile_kernel", pkg.KERNEL_PAIR: "snl1_pairtile_kernel",
-                   pkg.KERNEL_PAIR_GENERAL: "snl1_pair_kernel"}[
-                       grid.select_kernel(kernel_ids[args.kernel])]
+                   pkg.KERNEL_PAIR_GENERAL: "snl1_pair_kernel"}[cur]
     dev = torch.device("cuda", local)
     a = torch.from_numpy(g["a"]).to(dev)
     cg = torch.from_numpy(g["cg"]).to(dev)
@@ -378,6 +382,7 @@ def run_b200_dia(args):
                      "kernel": kernel_name, "launch_ms": launch_ms,
                      "algorithmic_bytes_per_point": BYTES_PER_POINT},
         "gpu_launches": args.steps,
+        "autotune": pkg.autotune_report(),
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -516,6 +521,8 @@ def run_b200_srce(args, quiet=False, npts=None, steps=None, warmup=None, igrid=1
     warmup = warmup or args.warmup
     st, t, sr, cfg, sig, pts = srce_inputs(synth, npts, 2026 + rank)
     grid = pkg.SrceGrid(igrid, t["rpar"], st["ipar"], synth.st4_registrations(st, t), cfg, sig, sr)
+    if not args.no_autotune:  # W3SRCE's CTAs per SM, timed on a sample of these points
+        pkg.srce_autotune(igrid, pts)
     dev = torch.device("cuda", local)
     d0 = {k: torch.from_numpy(pts[k]).to(dev) for k in SRCE_ARRAYS}
     d = {k: v.clone() for k, v in d0.items()}
@@ -611,6 +618,7 @@ def run_b200_srce(args, quiet=False, npts=None, steps=None, warmup=None, igrid=1
                      "note": ("W3SRCE is bound by FP32 issue and its serial ordered sums, not by "
                               "HBM; the fraction shows how far from the HBM ceiling it runs")},
         "gpu_launches": steps,
+        "autotune": pkg.autotune_report(),
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not quiet:
@@ -1045,6 +1053,8 @@ def run_b200_multigrid(args):
 
     together = lambda: pkg.steps_run(igs, 1, handle)  # noqa: E731
 
+    if not args.no_autotune:  # W3SRCE's CTAs per SM on the first grid's points (one layout)
+        pkg.srce_autotune(grids[0]["ig"], grids[0]["inputs"][2])
     # The grids' graphs one after another (the unfused form), from the initial state.
     record_all()
     pkg.steps_fuse([])
@@ -1121,6 +1131,7 @@ def run_b200_multigrid(args):
                      "traffic": None, "kernel": "the fused step graph (srce_multi_kernel dominant)",
                      "launch_ms": step_ms, "algorithmic_bytes_per_point": STEP_BYTES_PER_POINT},
         "gpu_launches": (sum(g["step"].nodes() for g in grids) - 2 * len(grids) + 2) * args.steps,
+        "autotune": pkg.autotune_report(),
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1500,6 +1511,8 @@ def run_b200_surrogate(args):
     sur = __import__("ww3_gpu_b200.surrogate", fromlist=["surrogate"])
     cfg, sig = synth.dia_config(NK, NTH)
     grid = pkg.Snl1Grid(cfg, sig, igrid=1)
+    if not args.no_autotune:  # the plain DIA kernel: every kernel that fits, timed
+        pkg.snl1_autotune(1)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     handle = stream.cuda_stream
@@ -1645,6 +1658,7 @@ def run_b200_surrogate(args):
                      "forward_ms_65536_rows": fwd_ms,
                      "algorithmic_flop_per_point": SUR_FLOP_PER_POINT},
         "gpu_launches": args.steps * chunks * 7,
+        "autotune": pkg.autotune_report(),
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -116,6 +116,28 @@ int ww_snl1_last_error(void);
  * Returns the previous choice, or -1 for an unknown grid or a choice its tables cannot run. */
 int ww_snl1_select_kernel(int igrid, int which);
 
+/* B200 extension (the autotuner; no counterpart in the reference). Times every DIA kernel that
+ * grid igrid's tables can run on 16,384 synthetic points of its spectral grid with CUDA events
+ * (median of three launches after a warm-up), selects the fastest for the grid and records the
+ * choice (ww_autotune_report). Synchronous; allocates its test arrays for the call. Returns the
+ * kernel chosen (as ww_snl1_select_kernel numbers them), or -1. */
+int ww_snl1_autotune(int igrid);
+
+/* B200 extension (the autotuner). The W3SRCE kernels' CTAs per SM, each count with the
+ * shared-memory carveout that fits it (the rest of the SM's memory is L1), timed on a sample
+ * of the caller's own points (arguments as ww_srce_batch takes them, host arrays, read only:
+ * the sample runs on device copies): the fastest is kept for every later W3SRCE launch in the
+ * process. Synchronous. Returns the CTAs per SM chosen, or -1. */
+int ww_srce_autotune(int igrid, int it, int inflags24, int flogrd57, int flogrd58, float dtg,
+                     int npts, const float* spec, const float* wn1, const float* cg1,
+                     const float* pin, const float* psc, const float* whitecap,
+                     const float* taubbl, const float* tauice);
+
+/* B200 extension: the autotuner's choices so far as a JSON object, {"<choice> <shape>
+ * <device>": {"choice": c, "ms": {"<candidate>": median ms, ...}}, ...}, written to buf (at
+ * most len - 1 characters and a NUL). Returns the full length, or -1. */
+int ww_autotune_report(char* buf, int len);
+
 /* ---------------------------------------------------------------- the resident spectrum VA */
 /* VA(NSPEC, 0:NSEALM) of grid igrid, kept in HBM beside the Fortran array (resident_c.hpp:1-42).
  * `va` is VA(1,0), nspec = SIZE(VA,1), nsealm = UBOUND(VA,2); the first call binds the grid to

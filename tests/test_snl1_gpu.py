@@ -210,3 +210,21 @@ def test_full_size_properties(pkg, oracle, synth, cfg36):
     s_ref, d_ref = oracle.w3snl1(cfg, sig, g["a"][idx], g["cg"][idx], g["kdmean"][idx])
     assert_bitexact(outs[0][0].view(torch.float32).cpu().numpy()[idx], s_ref, "S sample")
     assert_bitexact(outs[0][1].view(torch.float32).cpu().numpy()[idx], d_ref, "D sample")
+
+
+def test_autotune_picks_a_kernel_that_stays_bitexact(pkg, oracle, synth, cfg36):
+    """ww_snl1_autotune times every kernel the tables fit, selects one, records it in the
+    report; the grid then still gives the oracle's bits."""
+    cfg, sig = cfg36
+    grid = pkg.Snl1Grid(cfg, sig, igrid=7)
+    k = pkg.snl1_autotune(7)
+    assert k in (pkg.KERNEL_PAIR, pkg.KERNEL_PAIR_GENERAL, pkg.KERNEL_BAND, pkg.KERNEL_TILE,
+                 pkg.KERNEL_ROWSHIFT, pkg.KERNEL_GATHER)
+    rep = pkg.autotune_report()
+    key = next(x for x in rep if x.startswith("dia 36x36"))
+    assert rep[key]["choice"] == k and len(rep[key]["ms"]) >= 5
+    g = synth.sea_states(300, seed=77, depth_range=(5.0, 4000.0))
+    s, d = grid(g["a"], g["cg"], g["kdmean"])
+    s_ref, d_ref = oracle.w3snl1(cfg, sig, g["a"], g["cg"], g["kdmean"])
+    assert_bitexact(s, s_ref, "S after autotune")
+    assert_bitexact(d, d_ref, "D after autotune")

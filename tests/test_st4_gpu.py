@@ -121,6 +121,32 @@ def test_srce_bench_workload_bitexact(pkg, oracle, synth):
     assert np.array_equal(shave.cpu().numpy(), r["shave"])
 
 
+def test_srce_autotune_keeps_results_bitexact(pkg, oracle, synth, tables):
+    """ww_srce_autotune times the W3SRCE kernel at every CTA count per SM on device copies of
+    the caller's points (the host arrays stay as they were), keeps the fastest, and the
+    batches after it still give the reference's bits."""
+    st, t = tables["default"]
+    ig = 225
+    sr = synth.srce_setup(st)
+    ref = oracle.RefSt4(st, t, igrid=ig, srce=sr, dia=synth.dia_config(), scalar_mvec=True)
+    L, be = gpu_setup(pkg, oracle, synth, st, t, ig, srce=sr)
+    pts = synth.srce_points(700, seed=2027)
+    before = {k: np.array(v, copy=True) for k, v in pts.items()}
+    c = pkg.srce_autotune(ig, pts)
+    assert c >= 1
+    for k in before:
+        assert np.array_equal(pts[k], before[k]), k
+    rep = pkg.autotune_report()
+    key = next(x for x in rep if x.startswith("srce ctas/SM 36x36"))
+    assert rep[key]["choice"] == c
+    r = sc.ref_backend(ref.L, ig).srce_batch(pts, it=1)
+    g = be.srce_batch(pts, it=1)
+    assert L.ww_srce_last_error() == 0
+    for k in ("spec", "psc", "whitecap", "taubbl", "tauice"):
+        assert_bitexact(g[k], r[k], f"after autotune, {k}")
+    assert np.array_equal(g["shave"], r["shave"])
+
+
 def test_srce_batch_va_and_single_point(pkg, oracle, synth, tables):
     """The resident-VA batch writes the same spectra into the VA columns JSEA names, and the
     one-point entry ww_srce gives the batch's result for that point."""

@@ -41,7 +41,8 @@ EXPORTS = (
     "ww_kokkos_flag", "ww_kokkos_preset_status", "ww_kokkos_strict", "ww_kokkos_fallback_slot",
     "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
-    "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_steps_fuse", "ww_ktp3_batch", "ww_ktp3_batch_va",
+    "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_steps_fuse", "ww_snl1_autotune",
+    "ww_srce_autotune", "ww_autotune_report", "ww_ktp3_batch", "ww_ktp3_batch_va",
     "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va", "ww_snl1_noalloc",
     "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_sds4", "ww_sin4",
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
@@ -539,6 +540,47 @@ class Step:
 
     def free(self):
         self.L.ww_step_free(self.igrid)
+
+
+def autotune_report():
+    """The autotuner's choices so far (ww_autotune_report) as a dict."""
+    import json
+    L = lib()
+    L.ww_autotune_report.argtypes = [ctypes.c_char_p, _I]
+    L.ww_autotune_report.restype = _I
+    n = L.ww_autotune_report(None, 0)
+    if n < 0:
+        raise WwError("ww_autotune_report", n)
+    buf = ctypes.create_string_buffer(n + 1)
+    L.ww_autotune_report(buf, n + 1)
+    return json.loads(buf.value.decode())
+
+
+def snl1_autotune(igrid):
+    """ww_snl1_autotune: time the DIA kernels that fit grid igrid, select the fastest."""
+    L = lib()
+    L.ww_snl1_autotune.argtypes = [_I]
+    L.ww_snl1_autotune.restype = _I
+    k = L.ww_snl1_autotune(igrid)
+    if k < 0:
+        raise WwError("ww_snl1_autotune", last_error())
+    return k
+
+
+def srce_autotune(igrid, pts, it=1, dtg=900.0):
+    """ww_srce_autotune on the host packets of ``pts`` (as synth.srce_points makes them)."""
+    L = lib()
+    L.ww_srce_autotune.argtypes = [_I, _I, _I, _I, _I, ctypes.c_float, _I] + [_P] * 8
+    L.ww_srce_autotune.restype = _I
+    a = {k: np.ascontiguousarray(pts[k], np.float32)
+         for k in ("spec", "wn1", "cg1", "pin", "psc", "whitecap", "taubbl", "tauice")}
+    n = a["spec"].shape[0]
+    c = L.ww_srce_autotune(igrid, it, 0, 1, 1, dtg, n, *[a[k].ctypes.data for k in
+                                                          ("spec", "wn1", "cg1", "pin", "psc",
+                                                           "whitecap", "taubbl", "tauice")])
+    if c < 0:
+        raise WwError("ww_srce_autotune", lib().ww_srce_last_error())
+    return c
 
 
 def steps_fuse(igrids):

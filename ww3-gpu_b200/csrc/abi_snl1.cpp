@@ -15,6 +15,7 @@
 #include <new>
 #include <vector>
 
+#include "autotune.hpp"
 #include "snl1_kernel.cuh"
 #include "snl1_tables.hpp"
 #include "step.hpp"
@@ -451,6 +452,50 @@ void ww_snl1_noalloc(int igrid, int npts, const float* a, const float* cg, const
 int ww_snl1_enabled(void) { return ww_kokkos_flag("WW_KOKKOS_SNL1") != 0 ? 1 : 0; }
 
 int ww_snl1_last_error(void) { return g_status.get(); }
+
+int ww_snl1_autotune(int igrid) {
+  try {
+    auto it = contexts().find(igrid);
+    if (it == contexts().end() || !it->second->ready) return -1;
+    Ctx& c = *it->second;
+    std::vector<int> cands;
+    for (int k : {kSnl1Pair, kSnl1PairGeneral, kSnl1Band, kSnl1Tile, kSnl1RowShift, kSnl1Gather})
+      if (pick_kernel(c, k) == k) cands.push_back(k);
+    if (cands.empty()) return -1;
+    // 16,384 synthetic points (every point the same smooth spectrum): the DIA's work does not
+    // depend on the values, and the batch is large enough to fill every SM many times.
+    const int n = 16384;
+    const size_t nspec = c.cfg.nspec(), nk = c.cfg.nk;
+    std::vector<float> ha(nspec * n), hc(nk * n, 1.5f), hk(n, 3.0f);
+    for (size_t i = 0; i < nspec; ++i) ha[i] = 1e-4f * (1.0f + static_cast<float>(i % 37) / 37.0f);
+    for (int p = 1; p < n; ++p) std::copy(ha.begin(), ha.begin() + nspec, ha.begin() + p * nspec);
+    DevBuf<float> a, cg, kd, s, d;
+    a.alloc(ha.size());
+    cg.alloc(hc.size());
+    kd.alloc(hk.size());
+    s.alloc(ha.size());
+    d.alloc(ha.size());
+    WWB_CHECK(cudaMemcpy(a.ptr, ha.data(), ha.size() * 4, cudaMemcpyHostToDevice));
+    WWB_CHECK(cudaMemcpy(cg.ptr, hc.data(), hc.size() * 4, cudaMemcpyHostToDevice));
+    WWB_CHECK(cudaMemcpy(kd.ptr, hk.data(), hk.size() * 4, cudaMemcpyHostToDevice));
+    cudaStream_t st = runtime().stream;
+    const std::string key = "dia " + std::to_string(c.cfg.nk) + "x" + std::to_string(c.cfg.nth) +
+                            " " + tune::device_key();
+    const int k = tune::pick(
+        key, cands,
+        [&](int kern, cudaStream_t ss) {
+          launch_snl1(kern, c.dev, n, a.ptr, cg.ptr, kd.ptr, s.ptr, d.ptr, ss);
+        },
+        nullptr, st, 3);
+    WWB_CHECK(cudaStreamSynchronize(st));
+    c.kernel = k;
+    g_status.ok();
+    return k;
+  } catch (const std::exception& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+    return -1;
+  }
+}
 
 int ww_snl1_select_kernel(int igrid, int which) {
   auto it = contexts().find(igrid);

@@ -12,11 +12,14 @@
 // as UNSUPPORTED, as are DIA tables that are not in the row-shift form.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <map>
 #include <memory>
 #include <string>
 #include <vector>
 
+#include "autotune.hpp"
 #include "st4_srce.cuh"
 #include "staging.hpp"
 #include "step.hpp"
@@ -364,6 +367,82 @@ void ww_srce_batch_device(int igrid, int it, int inflags24, int flogrd57, int fl
     g_status.ok();
   } catch (const std::exception& e) {
     g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
+int ww_srce_autotune(int igrid, int it, int inflags24, int flogrd57, int flogrd58, float dtg,
+                     int npts, const float* spec, const float* wn1, const float* cg1,
+                     const float* pin, const float* psc, const float* whitecap,
+                     const float* taubbl, const float* tauice) {
+  try {
+    GridCtx* g = find(igrid, "ww_srce_autotune");
+    if (g == nullptr) return -1;
+    if (npts < 1 || !spec || !wn1 || !cg1 || !pin || !psc || !whitecap || !taubbl || !tauice) {
+      g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_srce_autotune: npts < 1 or a null array");
+      return -1;
+    }
+    SrceDev host{};
+    if (!prepare(igrid, *g, host, "ww_srce_autotune")) return -1;
+    const pt::SrceLayout& L = host.L;
+    const int maxc = srce_max_ctas_per_sm(L);
+    // A sample of the caller's points, four times the most CTAs that can be resident, so every
+    // candidate runs several points per CTA (the queue's tail is a small part of the time).
+    const int sms = runtime().sm_count;
+    const int n = std::min(npts, 4 * maxc * sms);
+    const size_t ns = static_cast<size_t>(n) * L.nspec, nk = static_cast<size_t>(n) * L.nk;
+    struct Buf {
+      float* p = nullptr;
+      ~Buf() { if (p) cudaFree(p); }
+      float* alloc(size_t k) { WWB_CHECK(cudaMalloc(&p, k * sizeof(float))); return p; }
+    };
+    Buf s0, s1, w, c, pn, q0, q1, wc0, wc1, tb0, tb1, ti0, ti1, sh;
+    s0.alloc(ns), s1.alloc(ns), w.alloc(nk), c.alloc(nk), pn.alloc(n * static_cast<size_t>(srce::NPIN));
+    q0.alloc(n * static_cast<size_t>(srce::NPSC)), q1.alloc(n * static_cast<size_t>(srce::NPSC));
+    wc0.alloc(4 * static_cast<size_t>(n)), wc1.alloc(4 * static_cast<size_t>(n));
+    tb0.alloc(2 * static_cast<size_t>(n)), tb1.alloc(2 * static_cast<size_t>(n));
+    ti0.alloc(2 * static_cast<size_t>(n)), ti1.alloc(2 * static_cast<size_t>(n));
+    sh.alloc(n);
+    auto up = [](float* d, const float* h, size_t k) {
+      WWB_CHECK(cudaMemcpy(d, h, k * sizeof(float), cudaMemcpyHostToDevice));
+    };
+    up(s0.p, spec, ns), up(w.p, wn1, nk), up(c.p, cg1, nk), up(pn.p, pin, n * static_cast<size_t>(srce::NPIN));
+    up(q0.p, psc, n * static_cast<size_t>(srce::NPSC)), up(wc0.p, whitecap, 4 * static_cast<size_t>(n));
+    up(tb0.p, taubbl, 2 * static_cast<size_t>(n)), up(ti0.p, tauice, 2 * static_cast<size_t>(n));
+    std::vector<int> cands;
+    for (int k = maxc; k >= 1; --k) cands.push_back(k);
+    cudaStream_t st = runtime().stream;
+    const SrceStep step{it, inflags24, flogrd57, flogrd58, dtg};
+    auto d2d = [&](float* d, const float* s_, size_t k, cudaStream_t ss) {
+      WWB_CHECK(cudaMemcpyAsync(d, s_, k * sizeof(float), cudaMemcpyDeviceToDevice, ss));
+    };
+    const std::string key = "srce ctas/SM " + std::to_string(L.nk) + "x" + std::to_string(L.nth) +
+                            " " + tune::device_key();
+    const int best = tune::pick(
+        key, cands,
+        [&](int ctas, cudaStream_t ss) {
+          launch_srce(g->dev, L, step, n, s1.p, nullptr, w.p, c.p, pn.p, q1.p, wc1.p, tb1.p, ti1.p,
+                      reinterpret_cast<int*>(sh.p), g->work, ss);
+          (void)ctas;
+        },
+        [&](int ctas, cudaStream_t ss) {
+          // the candidate's CTAs and carveout, and the sample's inputs restored (W3SRCE updates
+          // them in place)
+          WWB_CHECK(cudaStreamSynchronize(ss));
+          srce_set_ctas_per_sm(L, ctas);
+          srce_reserve(L, n, g->work, ss);
+          d2d(s1.p, s0.p, ns, ss), d2d(q1.p, q0.p, n * static_cast<size_t>(srce::NPSC), ss);
+          d2d(wc1.p, wc0.p, 4 * static_cast<size_t>(n), ss);
+          d2d(tb1.p, tb0.p, 2 * static_cast<size_t>(n), ss);
+          d2d(ti1.p, ti0.p, 2 * static_cast<size_t>(n), ss);
+        },
+        st, 2);
+    WWB_CHECK(cudaStreamSynchronize(st));
+    srce_set_ctas_per_sm(L, best == maxc ? 0 : best);
+    g_status.ok();
+    return best;
+  } catch (const std::exception& e) {
+    g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+    return -1;
   }
 }
 

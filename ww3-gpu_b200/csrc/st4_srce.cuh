@@ -104,6 +104,13 @@ struct SrceRecorded {
   pt::SrceLayout L;
 };
 
+/// CTAs per SM of the W3SRCE kernels when every one that fits is resident.
+int srce_max_ctas_per_sm(const pt::SrceLayout& L);
+
+/// Limits the W3SRCE kernels to `ctas` CTAs per SM (0: all that fit) with the shared-memory
+/// carveout they need, the rest of the SM's memory left to L1 (the autotuner's choice).
+void srce_set_ctas_per_sm(const pt::SrceLayout& L, int ctas);
+
 /// CTAs of a W3SRCE launch on npts points of these tables (the resident grid, at most npts).
 int srce_resident_ctas(const pt::SrceLayout& L, int npts);
 

@@ -164,19 +164,54 @@ __global__ void __launch_bounds__(kSrceBlock, kSrceMinBlocks) srce_multi_kernel(
   }
 }
 
-/// Resident CTAs per SM of a kernel at this shared memory, at least 1.
+/// CTAs per SM of the W3SRCE kernels (0: all that fit), set by the autotuner.
+int g_srce_ctas_per_sm = 0;
+
+/// Resident CTAs per SM of a kernel at this shared memory, at least 1 (for the W3SRCE kernels,
+/// at most the autotuner's choice).
 template <class K>
-int resident_grid(K k, size_t smem, int npts, int block = kSt4Block) {
+int resident_grid(K k, size_t smem, int npts, int block = kSt4Block, bool srce = false) {
   WWB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
   int per_sm = 0;
   WWB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem));
   if (per_sm < 1) throw CudaError(cudaErrorInvalidConfiguration, "st4/srce occupancy");
+  if (srce && g_srce_ctas_per_sm > 0 && g_srce_ctas_per_sm < per_sm)
+    per_sm = g_srce_ctas_per_sm;
   const long long resident = static_cast<long long>(per_sm) * runtime().sm_count;
   return static_cast<int>(npts < resident ? npts : resident);
 }
 
 }  // namespace
+
+int srce_max_ctas_per_sm(const pt::SrceLayout& L) {
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  const int keep = g_srce_ctas_per_sm;
+  g_srce_ctas_per_sm = 0;
+  WWB_CHECK(cudaFuncSetAttribute(srce_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutDefault));
+  const int all = resident_grid(srce_kernel, smem, 1 << 30, kSrceBlock, true) / runtime().sm_count;
+  srce_set_ctas_per_sm(L, keep);  // the carveout of the current choice again
+  return all;
+}
+
+void srce_set_ctas_per_sm(const pt::SrceLayout& L, int ctas) {
+  const size_t smem = srce_smem_bytes(L);
+  if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
+  g_srce_ctas_per_sm = ctas > 0 ? ctas : 0;
+  // The shared-memory carveout just large enough for that many CTAs (their dynamic and static
+  // shared memory and the 1 KiB the system keeps per CTA): the rest of the SM's 256 KiB is L1.
+  int pct = cudaSharedmemCarveoutDefault;
+  if (ctas > 0) {
+    const size_t per_cta = smem + sizeof(pt::SrceSh) + 16 + 1024;
+    pct = static_cast<int>((100 * ctas * per_cta + 228 * 1024 - 1) / (228 * 1024));
+    if (pct > 100) pct = 100;
+  }
+  WWB_CHECK(cudaFuncSetAttribute(srce_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+  WWB_CHECK(
+      cudaFuncSetAttribute(srce_multi_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+}
 
 size_t srce_smem_bytes(const pt::SrceLayout& L) {
   const size_t b = static_cast<size_t>(L.total_s) * sizeof(float) + 16;
@@ -227,7 +262,7 @@ void srce_reserve(const pt::SrceLayout& L, int npts, SrceWork& work, cudaStream_
   if (npts <= 0) return;
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
-  const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock);
+  const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock, true);
   const size_t need = static_cast<size_t>(grid) * static_cast<size_t>(L.total_g);
   if (work.counter == nullptr) WWB_CHECK(cudaMalloc(&work.counter, sizeof(int)));
   if (need > work.scratch_n) {
@@ -243,13 +278,13 @@ void srce_reserve(const pt::SrceLayout& L, int npts, SrceWork& work, cudaStream_
 int srce_resident_ctas(const pt::SrceLayout& L, int npts) {
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
-  return resident_grid(srce_kernel, smem, npts, kSrceBlock);
+  return resident_grid(srce_kernel, smem, npts, kSrceBlock, true);
 }
 
 void srce_multi_reserve(const pt::SrceLayout& L, int total, SrceWork& work) {
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
-  const int grid = resident_grid(srce_multi_kernel, smem, total > 0 ? total : 1, kSrceBlock);
+  const int grid = resident_grid(srce_multi_kernel, smem, total > 0 ? total : 1, kSrceBlock, true);
   const size_t need = static_cast<size_t>(grid) * static_cast<size_t>(L.total_g);
   if (work.counter == nullptr) WWB_CHECK(cudaMalloc(&work.counter, sizeof(int)));
   if (need > work.scratch_n) {
@@ -266,7 +301,7 @@ void launch_srce_multi(const SrceJob* jobs_dev, int njobs, int total, const pt::
   if (total <= 0) return;
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
-  const int grid = resident_grid(srce_multi_kernel, smem, total, kSrceBlock);
+  const int grid = resident_grid(srce_multi_kernel, smem, total, kSrceBlock, true);
   if (work.counter == nullptr ||
       static_cast<size_t>(grid) * static_cast<size_t>(L.total_g) > work.scratch_n)
     throw CudaError(cudaErrorInvalidValue, "launch_srce_multi: work buffers not reserved");
@@ -283,7 +318,7 @@ void launch_srce(const SrceDev* d, const pt::SrceLayout& L, SrceStep step, int n
   if (npts <= 0) return;
   const size_t smem = srce_smem_bytes(L);
   if (smem == 0) throw CudaError(cudaErrorInvalidConfiguration, "W3SRCE working set too large");
-  const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock);
+  const int grid = resident_grid(srce_kernel, smem, npts, kSrceBlock, true);
   // The work buffers fit after srce_reserve; otherwise (re)allocate them first, after the
   // previous launches on this stream that may still read the old ones.
   srce_reserve(L, npts, work, st);
