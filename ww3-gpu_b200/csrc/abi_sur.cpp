@@ -422,7 +422,9 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
                    float* dd, int* accepted, float* gv, const GateParams& gate, int* total,
                    cudaStream_t st) {
   Mlp& m = s.net;
-  prep(s.g, n, a, cg, kd, m.ix0.p, m.din, s.ps.p, s.shift.p, st);
+  // The inputs, and zeros for D (the surrogate does not model the diagonal term; the plain DIA
+  // overwrites the rejected points' D afterwards) and for the gate sums the epilogue adds to.
+  prep(s.g, n, a, cg, kd, m.ix0.p, m.din, s.ps.p, s.shift.p, st, dd, s.gsum.p);
   const bf16* in = m.ix0.p;
   int kin = m.din;
   for (int l = 0; l < 3; ++l) {
@@ -435,10 +437,6 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
     in = m.ih[l & 1].p;
     kin = m.dh;
   }
-  WWB_CHECK(cudaMemsetAsync(s.gsum.p, 0, static_cast<size_t>(n) * 2 * sizeof(float), st));
-  // D = 0 for every point (the surrogate does not model the diagonal term); the plain DIA
-  // overwrites the rejected points' D afterwards.
-  WWB_CHECK(cudaMemsetAsync(dd, 0, static_cast<size_t>(n) * s.g.nspec * sizeof(float), st));
   GemmArgs g = args(n, m.dout, m.dh, m);
   g.bias = m.L[3].b.p;
   g.ldo = m.dout;

@@ -54,7 +54,8 @@ __host__ __device__ inline int orig_col(int packed, int j, int nth) {
 /// (2 NK floats: lambda, then the Hs-tendency weights) and packed direction shift; per
 /// frequency row the target scale. Column i < NSPEC of row m is the normalised S of canonical
 /// bin i: S(m, k NTH + orig_col(shift, j)) = (acc + bias) rowscale(k) e^lambda(k) (D, all
-/// zero, is the caller's memset), and the gate sums sum w v, sum w |v| (w = rowscale(k) times the weight) are added into
+/// zero, is written by the caller), and the gate sums sum w v, sum w |v| (w = rowscale(k) times
+/// the weight; zeroed by the caller) are added into
 /// gsum[2m], gsum[2m+1]; column NSPEC is the error head, stored in head[m].
 struct SurOut {
   const float* ps;

@@ -298,8 +298,8 @@ __device__ __forceinline__ void sur_row_consts(const GemmArgs& g, int m, int k0,
 /// so the chunk's columns lie in at most two frequency rows: columns j < jb in row k, the rest
 /// in row k + 1. Each thread scales its own row's values into the warp's staging tile and adds
 /// its gate sums; then the warp writes the tile out row by row, lane = column, so a sea point's
-/// S stores (permuted within its frequency rows) are contiguous. (D = 0 is set by the caller
-/// with a memset of the whole chunk before the launch.)
+/// S stores (permuted within its frequency rows) are contiguous. (D = 0 is written by the
+/// caller before the launch.)
 __device__ __forceinline__ void sur_chunk(const GemmArgs& g, int m_base, int n, int k0,
                                           const uint32_t (&r)[32], float bl, int my_shift,
                                           float& racc, float& gacc, float* tile, const float* rc,

@@ -178,7 +178,8 @@ __host__ __device__ inline int prep_floats(int nspec, int nk, int nth) {
 __global__ void __launch_bounds__(32 * kPointsPerCta)
     prep_kernel(SurGrid g, int npts, const float* __restrict__ a, const float* __restrict__ cg,
                 const float* __restrict__ kdm, __nv_bfloat16* __restrict__ x, int ldx,
-                float* __restrict__ ps, int* __restrict__ shift) {
+                float* __restrict__ ps, int* __restrict__ shift, float* __restrict__ dzero,
+                float* __restrict__ gzero) {
   extern __shared__ float sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ip = blockIdx.x * kPointsPerCta + warp;
@@ -335,6 +336,13 @@ __global__ void __launch_bounds__(32 * kPointsPerCta)
     if (i == nspec + 1) v = cons / g.snlc1 - 1.0f;
     xr[i] = __float2bfloat16_rn(v);
   }
+  // The gated path's zeros: the point's D and its two gate sums.
+  if (dzero)
+    for (int i = lane; i < nspec; i += 32) dzero[static_cast<size_t>(ip) * nspec + i] = 0.0f;
+  if (gzero && lane == 0) {
+    gzero[2 * static_cast<size_t>(ip)] = 0.0f;
+    gzero[2 * static_cast<size_t>(ip) + 1] = 0.0f;
+  }
 }
 
 
@@ -349,7 +357,8 @@ __global__ void __launch_bounds__(32 * kPointsPerCta)
     prep_rows_kernel(SurGrid g, int npts, const float* __restrict__ a,
                      const float* __restrict__ cg, const float* __restrict__ kdm,
                      __nv_bfloat16* __restrict__ x, int ldx, float* __restrict__ ps,
-                     int* __restrict__ shift) {
+                     int* __restrict__ shift, float* __restrict__ dzero,
+                     float* __restrict__ gzero) {
   static_assert(NK >= 32 && NK <= 64 && NTH % 4 == 0, "prep_rows_kernel shape");
   constexpr int NSPEC = NK * NTH, LD = NTH + 1, Q = NTH / 4;
   __shared__ float sm_ue[kPointsPerCta][NK * LD];
@@ -507,6 +516,15 @@ __global__ void __launch_bounds__(32 * kPointsPerCta)
     if (i == NSPEC) v = __logf(fmaxf(kd, 1e-2f)) * 0.2f;
     if (i == NSPEC + 1) v = cons / g.snlc1 - 1.0f;
     xr[i] = __float2bfloat16_rn(v);
+  }
+  // The gated path's zeros: the point's D (16-byte stores) and its two gate sums.
+  if (dzero) {
+    float4* const d4 = reinterpret_cast<float4*>(dzero + static_cast<size_t>(ip) * NSPEC);
+    for (int i = lane; i < NSPEC / 4; i += 32) d4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+  if (gzero && lane == 0) {
+    gzero[2 * static_cast<size_t>(ip)] = 0.0f;
+    gzero[2 * static_cast<size_t>(ip) + 1] = 0.0f;
   }
 }
 
@@ -908,7 +926,8 @@ void synth(const SurGrid& g, const SynthDraw& d, long long p0, int npts, float* 
 }
 
 void prep(const SurGrid& g, int npts, const float* a, const float* cg, const float* kdmean,
-          __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st) {
+          __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st, float* dzero,
+          float* gzero) {
   if (npts <= 0) return;
   if (g.nk > 64) throw CudaError(cudaErrorInvalidValue, "prep: NK above 64");
   const size_t smem =
@@ -923,15 +942,16 @@ void prep(const SurGrid& g, int npts, const float* a, const float* cg, const flo
   // 36 x 36 with 16-byte aligned spectra and 8-byte aligned input rows: rows across lanes.
   const bool rows36 = g.nk == 36 && g.nth == 36 && g.nspec == 1296 &&
                       (reinterpret_cast<uintptr_t>(a) & 15u) == 0 &&
-                      (reinterpret_cast<uintptr_t>(x) & 7u) == 0 && ldx % 4 == 0;
+                      (reinterpret_cast<uintptr_t>(x) & 7u) == 0 && ldx % 4 == 0 &&
+                      (reinterpret_cast<uintptr_t>(dzero) & 15u) == 0;
   if (rows36) {
     prep_rows_kernel<36, 36><<<blocks, 32 * kPointsPerCta, 0, st>>>(g, npts, a, cg, kdmean, x,
-                                                                     ldx, ps, shift);
+                                                                     ldx, ps, shift, dzero, gzero);
     WWB_CHECK(cudaGetLastError());
     return;
   }
   prep_kernel<<<blocks, 32 * kPointsPerCta, smem, st>>>(g, npts, a, cg, kdmean, x, ldx, ps,
-                                                         shift);
+                                                         shift, dzero, gzero);
   WWB_CHECK(cudaGetLastError());
 }
 

@@ -61,9 +61,11 @@ void synth(const SurGrid& g, const SynthDraw& d, long long p0, int npts, float* 
            float* kdmean, cudaStream_t st);
 
 /// Network input rows x (npts x ldx bf16), the per-point scales ps (npts x 2 NK) and the
-/// direction shift.
+/// direction shift; with dzero (npts x NSPEC) and gzero (npts x 2) non-null, also zeros there
+/// (the gated path's D and gate sums).
 void prep(const SurGrid& g, int npts, const float* a, const float* cg, const float* kdmean,
-          __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st);
+          __nv_bfloat16* x, int ldx, float* ps, int* shift, cudaStream_t st,
+          float* dzero = nullptr, float* gzero = nullptr);
 
 /// Accumulate sum over points and directions of (S e^-lambda)^2 per row into acc (double, NK,
 /// zeroed by the caller), and count the points with a nonempty spectrum into cnt.

@@ -1261,8 +1261,9 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
   float2* const conx2 = dcs + S::kDcs;
   float2* const cons2 = conx2 + 2 * nk;
   float* const afr = reinterpret_cast<float*>(cons2 + 2);
+  float* const wrow = afr + nfrchg;  // TPIINV / SIG per frequency row
   const size_t stage_off =
-      (static_cast<size_t>(afr + nfrchg - smem) + 3) & ~static_cast<size_t>(3);
+      (static_cast<size_t>(wrow + nk - smem) + 3) & ~static_cast<size_t>(3);
   float* const stage = smem + stage_off;
   uint64_t* const bar = reinterpret_cast<uint64_t*>(stage + ((2 * (nspec + nk) + 3) & ~3));
   const int tid = threadIdx.x;
@@ -1279,6 +1280,7 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
       for (int m = 0; m < 6; ++m) arr0[m * AS + i] = z;
   }
   for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
+  for (int i = tid; i < nk; i += BLOCK) wrow[i] = kTpiInv / __ldg(p.sig + i);
   float kd0 = 0.0f, kd1 = 0.0f;
   if (tid == 0) {
     mbar_init(bar, 1);
@@ -1324,36 +1326,29 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
     const bool lost = !mbar_wait(bar, parity, err);
     parity ^= 1u;
     if (tid == 0) cons2[buf] = make_float2(dia_cons(p, kd0), dia_cons(p, kd1));
-    for (int k = tid; k < nk; k += BLOCK) {
-      const float w = kTpiInv / __ldg(p.sig + k);
-      conx[k] = make_float2(w * stage[2 * nspec + k], w * stage[2 * nspec + nk + k]);
-    }
-    if (__syncthreads_or(lost)) break;
-
-    // 2b. UE = A / CON, and the parametric tail up each column from row NFR.
-    {
-      int ifr0 = q0, col = r0;
-      for (int isp = tid; isp < nspec; isp += BLOCK) {
-        const float2 cx = conx[ifr0];
-        const float2 v = make_float2(stage[isp] / cx.x, stage[nspec + isp] / cx.y);
-        ue[isp + NTH] = v;
-        if (ifr0 == nfr - 1) {
-          float2 t = v;
-          const float2 fh = dup2(p.fachfe);
-          for (int r = nfr + 1; r <= p.nfrhgh; ++r) {
-            t = mul2(t, fh);
-            ue[r * NTH + col] = t;
-          }
-        }
-        col += dr;
-        ifr0 += dq;
-        if (col >= NTH) {
-          col -= NTH;
-          ++ifr0;
+    // 2a-2b. CON per frequency row and UE = A / CON, with the parametric tail up each column
+    // from row NFR. The CTA's width is a whole number of rows, so a thread's bins are column r0
+    // of rows q0, q0 + dq, ...: it forms each row's CON itself (the column-0 thread keeps it for
+    // section 4), and one barrier follows instead of two. A bulk copy whose wait gave up ends
+    // the CTA's work at that barrier, all its threads together.
+    static_assert(dr == 0, "a whole number of rows per CTA");
+    for (int row = q0; row < nk; row += dq) {
+      const float w = wrow[row];
+      const float2 cx = make_float2(w * stage[2 * nspec + row], w * stage[2 * nspec + nk + row]);
+      if (r0 == 0) conx[row] = cx;
+      const int isp = row * NTH + r0;
+      const float2 v = make_float2(stage[isp] / cx.x, stage[nspec + isp] / cx.y);
+      ue[isp + NTH] = v;
+      if (row == nfr - 1) {
+        float2 t = v;
+        const float2 fh = dup2(p.fachfe);
+        for (int r = nfr + 1; r <= p.nfrhgh; ++r) {
+          t = mul2(t, fh);
+          ue[r * NTH + r0] = t;
         }
       }
     }
-    __syncthreads();
+    if (__syncthreads_or(lost)) break;
 
     const int pnext = pp + gridDim.x;
     if (tid == 0 && pnext < npairs) {
@@ -1654,7 +1649,7 @@ size_t pairtile36_smem(const Snl1Dev& p) {
   using S = PairTile36;
   size_t bytes = 8 * (static_cast<size_t>(S::kRowsU) * 36 + 6 * static_cast<size_t>(S::kAS) +
                       S::kDcs + 2 * p.nk + 2) +
-                 4 * static_cast<size_t>(p.nfrchg);
+                 4 * static_cast<size_t>(p.nfrchg + p.nk);
   bytes = (bytes + 15) & ~static_cast<size_t>(15);
   bytes += 4 * ((2 * static_cast<size_t>(p.nspec + p.nk) + 3) & ~static_cast<size_t>(3));
   return bytes + 16;  // + the mbarrier
