@@ -577,7 +577,9 @@ int ww_mlp_forward(int handle, int rows, const void* x, float* out);
  * B bf16 (N x K, row stride ldb), tile width bn (64, 128, 192, 256; N a multiple), K a multiple
  * of 64, and epilogue `mode`: 1 z = C + bias -> aux = z, out = gelu(z), out_t = out^T; 2 out =
  * gelu(C + bias); 3 out_f32 = C + bias; 4 out = C * gelu'(aux), out_t = out^T; 5 out_f32 += C
- * with the reduction split in `splits` parts. Synchronous on `stream`. */
+ * with the reduction split in `splits` parts. Mode 2 or 3 plus 16: the same on paired tiles (two
+ * CTAs of a cluster per 256-row tile, tcgen05.mma.cta_group::2, each CTA holding half of B's
+ * tile), the form the surrogate's inference uses. Synchronous on `stream`. */
 int ww_mlp_gemm(int mode, int M, int N, int K, int bn, int splits, const void* a, int lda,
                 const void* b, int ldb, const float* bias, void* out, void* out_t, void* aux,
                 float* out_f32, int ldo, int ldt, void* stream);

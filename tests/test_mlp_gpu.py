@@ -74,6 +74,28 @@ def test_gemm_f32_epilogue_matches_torch(sur, M, N, K, bn):
     assert err < 1e-5, f"max relative error {err:.3e} (tile {bn})"
 
 
+@pytest.mark.parametrize("M,N,K,bn", [(256, 256, 64, 256), (1000, 1344, 1024, 192),
+                                      (4096, 1024, 1344, 256), (8320, 1024, 1024, 256),
+                                      (300, 512, 128, 128), (520, 192, 256, 64)])
+def test_gemm_paired_tiles_match_torch(sur, M, N, K, bn):
+    """Two CTAs of a cluster per 256-row tile (tcgen05.mma.cta_group::2, each CTA holding half
+    of B's tile): the f32 and GELU inference epilogues against FP32 torch; ragged M."""
+    import torch
+
+    a, b, bias = _operands(M, N, K, seed=M + 3 * N + K)
+    out = torch.full((M, N), float("nan"), device="cuda")
+    sur.gemm(sur.EPI_F32 | sur.PAIRED, a, b, bias=bias, out_f32=out, bn=bn)
+    torch.cuda.synchronize()
+    ref = _ref(a, b) + bias
+    scale = (a.float().abs() @ b.float().abs().T) + bias.abs()
+    err = ((out - ref).abs() / scale).max().item()
+    assert err < 1e-5, f"max relative error {err:.3e} (paired, tile {bn})"
+    g = torch.zeros(M, N, dtype=torch.bfloat16, device="cuda")
+    sur.gemm(sur.EPI_GELU_INFER | sur.PAIRED, a, b, bias=bias, out=g, bn=bn)
+    torch.cuda.synchronize()
+    assert torch.allclose(g.float(), _gelu(ref), rtol=2 ** -7, atol=2e-3)
+
+
 def test_gemm_gelu_train_epilogue(sur):
     import torch
 

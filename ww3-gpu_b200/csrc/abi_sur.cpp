@@ -170,6 +170,14 @@ void mlp_infer_alloc(Mlp& m, int rows) {
   m.icap = rows;
 }
 
+/// Inference GEMMs of at least this many rows would run with paired tiles (two CTAs of a
+/// cluster per 256-row tile, cta_group::2). At the surrogate's shapes (65,536 x 1024 x 1024 and
+/// x 1344) the paired kernel measured slower than one CTA per 128-row tile (the main loop is not
+/// short of shared-memory bandwidth; the epilogue is the limit), so the threshold keeps it off;
+/// ww_mlp_gemm's mode + 16 runs it.
+constexpr int kPairRows = 1 << 30;  // measured slower on B200 at these shapes: kept off
+int infer_pair(int rows) { return rows >= kPairRows ? 1 : 0; }
+
 GemmArgs args(int M, int N, int K, const Mlp& m) {
   GemmArgs g{};
   g.M = M;
@@ -195,20 +203,22 @@ void mlp_forward_infer(Mlp& m, int rows, cudaStream_t st, const bf16* x = nullpt
   int kin = m.din;
   for (int l = 0; l < 3; ++l) {
     GemmArgs g = args(rows, m.dh, kin, m);
+    g.pair = infer_pair(rows);
     g.bias = m.L[l].b.p;
     g.out = m.ih[l & 1].p;
     g.ldo = m.dh;
     run_gemm(kEpiGeluInfer, g, make_operand(in, rows, kin, kin, kBM),
-             make_operand(m.L[l].wb.p, m.dh, kin, kin, g.bn), st);
+             make_operand(m.L[l].wb.p, m.dh, kin, kin, gemm_b_box(g)), st);
     in = m.ih[l & 1].p;
     kin = m.dh;
   }
   GemmArgs g = args(rows, m.dout, m.dh, m);
+  g.pair = infer_pair(rows);
   g.bias = m.L[3].b.p;
   g.out_f32 = out ? out : m.iout.p;
   g.ldo = m.dout;
   run_gemm(kEpiF32, g, make_operand(in, rows, m.dh, m.dh, kBM),
-           make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, g.bn), st);
+           make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, gemm_b_box(g)), st);
 }
 
 /// One training step on rows [0, rows) of m.x0 (bf16) and targets t (rows x ldt fp32):
@@ -429,15 +439,17 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
   int kin = m.din;
   for (int l = 0; l < 3; ++l) {
     GemmArgs g = args(n, m.dh, kin, m);
+    g.pair = infer_pair(n);
     g.bias = m.L[l].b.p;
     g.out = m.ih[l & 1].p;
     g.ldo = m.dh;
     run_gemm(kEpiGeluInfer, g, make_operand(in, n, kin, kin, kBM),
-             make_operand(m.L[l].wb.p, m.dh, kin, kin, g.bn), st);
+             make_operand(m.L[l].wb.p, m.dh, kin, kin, gemm_b_box(g)), st);
     in = m.ih[l & 1].p;
     kin = m.dh;
   }
   GemmArgs g = args(n, m.dout, m.dh, m);
+  g.pair = infer_pair(n);
   g.bias = m.L[3].b.p;
   g.ldo = m.dout;
   g.sur = SurOut{s.ps.p, s.shift.p, s.rowscale.p, so, dd, s.head.p, s.gsum.p, s.g.nspec,
@@ -445,7 +457,7 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
   const char* why = nullptr;
   if (!sur_out_ok(g, &why)) throw CudaError(cudaErrorInvalidValue, why);
   run_gemm(kEpiSurOut, g, make_operand(in, n, m.dh, m.dh, kBM),
-           make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, g.bn), st);
+           make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, gemm_b_box(g)), st);
   WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
   gate_points(gate, n, s.gsum.p, s.head.p, accepted, gv, s.rej.p, s.nrej.p, total, st);
 }
@@ -649,7 +661,10 @@ int ww_mlp_gemm(int mode, int M, int N, int K, int bn, int splits, const void* a
       WWB_CHECK(cudaMalloc(&err, sizeof(int)));
       WWB_CHECK(cudaMemset(err, 0, sizeof(int)));
     }
+    const bool paired = (mode & 16) != 0;
+    mode &= ~16;
     GemmArgs g{};
+    g.pair = paired ? 1 : 0;
     g.M = M;
     g.N = N;
     g.K = K;
@@ -675,7 +690,10 @@ int ww_mlp_gemm(int mode, int M, int N, int K, int bn, int splits, const void* a
     if (mode != kEpiAtomic && splits != 1)
       return g_mlp_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_mlp_gemm: split reductions need the atomic epilogue");
     const Operand oa = make_operand(static_cast<const bf16*>(a), M, K, lda, kBM);
-    const Operand ob = make_operand(static_cast<const bf16*>(b), N, K, ldb, bn > 0 ? bn : 64);
+    if (paired && mode != kEpiGeluInfer && mode != kEpiF32)
+      return g_mlp_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_mlp_gemm: paired tiles for modes 2 and 3 only");
+    const Operand ob = make_operand(static_cast<const bf16*>(b), N, K, ldb,
+                                    bn > 0 ? gemm_b_box(g) : 64);
     const char* why = nullptr;
     if (!gemm_shape_ok(g, oa, ob, &why)) return g_mlp_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, why);
     cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -81,13 +81,18 @@ struct GemmArgs {
   int ldo, ldt;
   int* err;             ///< device status word: set when a bounded wait gave up
   SurOut sur;           ///< kEpiSurOut only
+  int pair;             ///< 1: two CTAs of a cluster share each 256-row tile (cta_group::2); B's
+                        ///< tensor map then has boxes of bn / 2 rows (gemm_b_box)
 };
+
+/// Rows of B's TMA box for this launch: bn, or bn / 2 when two CTAs share a tile.
+inline int gemm_b_box(const GemmArgs& g) { return g.pair ? g.bn / 2 : g.bn; }
 
 /// A K-major bf16 operand: `rows` rows of `k` elements, `ld` elements apart, read in boxes of
 /// `box_rows` x 64 with the 128-byte swizzle the MMA's shared-memory descriptors expect.
 struct Operand {
   CUtensorMap map;
-  int rows, k;
+  int rows, k, box;
 };
 Operand make_operand(const __nv_bfloat16* base, int rows, int k, int ld, int box_rows);
 

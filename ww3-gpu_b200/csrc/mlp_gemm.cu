@@ -38,9 +38,11 @@ constexpr uint32_t kTileA = kBM * kBK * 2;
 constexpr uint32_t kTmemCols = 2 * kBNMax;
 constexpr uint32_t kSpin = 1u << 24;  // polls before a wait gives up (seconds, never in a normal run)
 
+constexpr int kStagesMax = 8;  // the paired-tile kernel's ring (its stages are half as large)
+
 struct Bars {
-  uint64_t full[kStages];
-  uint64_t empty[kStages];
+  uint64_t full[kStagesMax];
+  uint64_t empty[kStagesMax];
   uint64_t tfull[2];
   uint64_t tempty[2];
   uint64_t drain;
@@ -53,7 +55,26 @@ static_assert(sizeof(Bars) <= 256, "barriers must fit their 256-byte slot");
 constexpr int kStageLd = 33;
 constexpr int kRowsPerTile = 8;  // frequency rows a tile of <= 256 columns covers when NTH >= 36
 constexpr size_t kStageBytes32 = kEpiWarps * 32 * kStageLd * sizeof(float);
+/// Epilogue warps of the single-CTA kernel per mode (a multiple of 4: one group per TMEM lane
+/// quarter, the groups' warps taking every (ew / 4)-th chunk): more where the registers allow,
+/// so the epilogue keeps up with the tensor cores.
+__host__ __device__ constexpr int epi_warps(int mode) {
+  return mode == 2 ? 12 : 8;
+}
+__host__ __device__ constexpr int epi_threads(int mode) { return 64 + 32 * epi_warps(mode); }
+// kEpiGeluInfer stages its bf16 chunk too: 32 rows of 16 words (+1 padding word), so the warp
+// stores rows of 64 contiguous bytes, eight lanes a row.
+constexpr int kStageLd16 = 17;
+constexpr size_t kStageBytes16 = kEpiWarps * 32 * kStageLd16 * sizeof(uint32_t);
 constexpr size_t kRowConstBytes = kEpiWarps * 32 * kRowsPerTile * 2 * sizeof(float);
+
+/// Staging bytes of `ew` epilogue warps for `mode`.
+__host__ __device__ constexpr size_t stage_bytes_w(int mode, int ew) {
+  return mode == 6   ? static_cast<size_t>(ew) * 32 * (kStageLd + kRowsPerTile * 2) * sizeof(float)
+         : mode == 3 ? static_cast<size_t>(ew) * 32 * kStageLd * sizeof(float)
+         : mode == 2 ? static_cast<size_t>(ew) * 32 * kStageLd16 * sizeof(uint32_t)
+                     : 0;
+}
 constexpr size_t kSmemMax = 227 * 1024;
 
 /// Bytes of one pipeline stage: the A tile and a bn-row B tile (a multiple of 1024).
@@ -65,9 +86,7 @@ __host__ __device__ constexpr uint32_t stage_bytes(int bn) {
 /// and the epilogue's staging areas.
 __host__ __device__ constexpr size_t smem_bytes(int mode, int bn) {
   return 1024 + kStages * static_cast<size_t>(stage_bytes(bn)) + 256 +
-         (mode == kEpiSurOut ? kStageBytes32 + kRowConstBytes
-          : mode == kEpiF32  ? kStageBytes32
-                             : 0);
+         stage_bytes_w(mode, epi_warps(mode));
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -142,7 +161,8 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+/// tcgen05.ld of 32 columns without waiting: the registers are valid after tmem_wait32 on them.
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
       "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
@@ -154,7 +174,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
         "=r"(r[31])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+/// Waits for this thread's tcgen05.ld; r (the last load's registers) is tied to the wait so no
+/// use of it moves above it.
+__device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
 }
 
 __device__ __forceinline__ float tanh_fast(float x) {
@@ -271,6 +304,31 @@ __device__ __forceinline__ void f32_chunk(const GemmArgs& g, int m_base, int n,
   __syncwarp();
 }
 
+/// kEpiGeluInfer through a bf16 staging tile: each thread packs its row's 32 GELU values into 16
+/// words of the warp's tile, then eight lanes store one row's 64 contiguous bytes (four rows
+/// per instruction), so every store fills whole 32-byte sectors.
+__device__ __forceinline__ void gelu_infer_chunk(const GemmArgs& g, int m_base, int n,
+                                                 const uint32_t (&r)[32], float bl,
+                                                 uint32_t* tile16, int lane) {
+#pragma unroll
+  for (int j = 0; j < 32; j += 2) {
+    const float v0 = gelu(__uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j));
+    const float v1 = gelu(__uint_as_float(r[j + 1]) + __shfl_sync(0xffffffffu, bl, j + 1));
+    tile16[lane * kStageLd16 + j / 2] = pack_bf16(v0, v1);
+  }
+  __syncwarp();
+  const int sub = lane >> 3, w = 2 * (lane & 7);
+#pragma unroll 4
+  for (int rr = 0; rr < 32; rr += 4) {
+    const int row = rr + sub;
+    const int mr = m_base + row;
+    const uint2 v = make_uint2(tile16[row * kStageLd16 + w], tile16[row * kStageLd16 + w + 1]);
+    if (mr < g.M)
+      *reinterpret_cast<uint2*>(g.out + static_cast<size_t>(mr) * g.ldo + n + 2 * w) = v;
+  }
+  __syncwarp();
+}
+
 /// kEpiSurOut, once per tile and thread: the scale e^lambda rowscale and the Hs-tendency weight
 /// of the thread's row (sea point m) for the frequency rows k0 .. k0 + kRowsPerTile - 1, into
 /// the warp's row-constant area (all loads issued before any is used).
@@ -368,6 +426,77 @@ __device__ __forceinline__ void sur_chunk(const GemmArgs& g, int m_base, int n, 
   __syncwarp();
 }
 
+/// The epilogue of one accumulator tile by one warp: TMEM lanes q*32.. (tile rows m_base +
+/// q*32 + lane), its chunks half, half + 2, ... of the tile's bn columns from n_base.
+/// Calls body(c, r) for chunks c = c0, c0 + 2, ... < nchunks with r the chunk's 32 TMEM
+/// columns, the next chunk's load in flight while body runs on the current one.
+template <class Body>
+__device__ __forceinline__ void for_chunks(uint32_t tbase, int c0, int nchunks, int step,
+                                           Body&& body) {
+  uint32_t ra[32], rb[32];
+  int c = c0;
+  if (c >= nchunks) return;
+  tmem_ld32_async(tbase + 32u * c, ra);
+  tmem_wait32(ra);
+  for (;;) {
+    if (c + step < nchunks) tmem_ld32_async(tbase + 32u * (c + step), rb);
+    body(c, ra);
+    c += step;
+    if (c >= nchunks) break;
+    tmem_wait32(rb);
+    if (c + step < nchunks) tmem_ld32_async(tbase + 32u * (c + step), ra);
+    body(c, rb);
+    c += step;
+    if (c >= nchunks) break;
+    tmem_wait32(ra);
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void epilogue_tile(const GemmArgs& g, int m_base, int n_base,
+                                              uint32_t tbase, int q, int half, int step, int lane,
+                                              float* tile, float* rowc) {
+  const int row = q * 32 + lane;
+  const int m = m_base + row;
+  const int nchunks = g.bn / 32;
+  constexpr bool kBias = MODE == kEpiGeluTrain || MODE == kEpiGeluInfer ||
+                         MODE == kEpiF32 || MODE == kEpiSurOut;
+  if constexpr (MODE == kEpiSurOut) {
+    const int my_shift = m < g.M ? __ldg(g.sur.shift + m) : 0;
+    const int k0 = n_base / g.sur.nth;
+    sur_row_consts(g, m, k0, rowc, lane);
+    float racc = 0.0f, gacc = 0.0f;
+    for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
+      const int n = n_base + 32 * c;
+      const float bl = __ldg(g.bias + n + lane);
+      sur_chunk(g, m_base + q * 32, n, k0, r, bl, my_shift, racc, gacc, tile, rowc, lane);
+    });
+    if (m < g.M) {
+      atomicAdd(g.sur.gsum + 2 * m, racc);
+      atomicAdd(g.sur.gsum + 2 * m + 1, gacc);
+    }
+  } else if constexpr (MODE == kEpiF32) {
+    for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
+      const int n = n_base + 32 * c;
+      const float bl = __ldg(g.bias + n + lane);
+      f32_chunk(g, m_base + q * 32, n, r, bl, tile, lane);
+    });
+  } else if constexpr (MODE == kEpiGeluInfer) {
+    uint32_t* const tile16 = reinterpret_cast<uint32_t*>(tile);
+    for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
+      const int n = n_base + 32 * c;
+      const float bl = __ldg(g.bias + n + lane);
+      gelu_infer_chunk(g, m_base + q * 32, n, r, bl, tile16, lane);
+    });
+  } else {
+    for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
+      const int n = n_base + 32 * c;
+      const float bl = kBias ? __ldg(g.bias + n + lane) : 0.0f;
+      epilogue_chunk<MODE>(g, m, n, r, bl);
+    });
+  }
+}
+
 struct Unit {
   int mt, nt, ks;
 };
@@ -382,7 +511,7 @@ __device__ __forceinline__ Unit decode(int u, int m_tiles, int n_tiles) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(epi_threads(MODE), 1)
     gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                 const GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
@@ -406,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&bars->tfull[b], 1);
-      mbar_init(&bars->tempty[b], kEpiWarps);  // one arrival per epilogue warp
+      mbar_init(&bars->tempty[b], epi_warps(MODE));  // one arrival per epilogue warp
     }
     mbar_init(&bars->drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -495,12 +624,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     const int q = warp & 3;  // the TMEM lane quarter this warp may read
-    const int ew = warp - 2, half = ew >> 2;  // epilogue warp; its chunks c = half, half + 2, ...
-    const int row = q * 32 + lane;
+    constexpr int EW = epi_warps(MODE);
+    // Epilogue warp ew; its chunks c = ew / 4, ew / 4 + EW / 4, ...
+    const int ew = warp - 2, half = ew >> 2;
     float* const tile = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256) +
-                        static_cast<size_t>(ew) * 32 * kStageLd;
-    float* const rowc = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256 +
-                                                 kStageBytes32) +
+                        static_cast<size_t>(ew) * 32 *
+                            (MODE == kEpiGeluInfer ? kStageLd16 : kStageLd);
+    float* const rowc = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256) +
+                        static_cast<size_t>(EW) * 32 * kStageLd +
                         static_cast<size_t>(ew) * 32 * kRowsPerTile * 2;
     uint32_t local = 0;
     bool ok = true;
@@ -513,44 +644,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         break;
       }
       tc_fence_after();
-      const int m = w.mt * kBM + row;
       const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16) + b * kBNMax;
-      const int nchunks = g.bn / 32;
-      constexpr bool kBias = MODE == kEpiGeluTrain || MODE == kEpiGeluInfer ||
-                             MODE == kEpiF32 || MODE == kEpiSurOut;
-      if constexpr (MODE == kEpiSurOut) {
-        const int my_shift = m < g.M ? __ldg(g.sur.shift + m) : 0;
-        const int k0 = (w.nt * g.bn) / g.sur.nth;
-        sur_row_consts(g, m, k0, rowc, lane);
-        float racc = 0.0f, gacc = 0.0f;
-        for (int c = half; c < nchunks; c += 2) {
-          const int n = w.nt * g.bn + 32 * c;
-          const float bl = __ldg(g.bias + n + lane);
-          uint32_t r[32];
-          tmem_ld32(tbase + 32u * c, r);
-          sur_chunk(g, w.mt * kBM + q * 32, n, k0, r, bl, my_shift, racc, gacc, tile, rowc, lane);
-        }
-        if (m < g.M) {
-          atomicAdd(g.sur.gsum + 2 * m, racc);
-          atomicAdd(g.sur.gsum + 2 * m + 1, gacc);
-        }
-      } else if constexpr (MODE == kEpiF32) {
-        for (int c = half; c < nchunks; c += 2) {
-          const int n = w.nt * g.bn + 32 * c;
-          const float bl = __ldg(g.bias + n + lane);
-          uint32_t r[32];
-          tmem_ld32(tbase + 32u * c, r);
-          f32_chunk(g, w.mt * kBM + q * 32, n, r, bl, tile, lane);
-        }
-      } else {
-        for (int c = half; c < nchunks; c += 2) {
-          const int n = w.nt * g.bn + 32 * c;
-          const float bl = kBias ? __ldg(g.bias + n + lane) : 0.0f;
-          uint32_t r[32];
-          tmem_ld32(tbase + 32u * c, r);
-          epilogue_chunk<MODE>(g, m, n, r, bl);
-        }
-      }
+      epilogue_tile<MODE>(g, w.mt * kBM, w.nt * g.bn, tbase, q, half, EW / 4, lane, tile, rowc);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bars->tempty[b]);
@@ -563,6 +658,251 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols));
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Paired tiles: two CTAs of a cluster share one 256-row output tile (cta_group::2). Each CTA
+// brings its own 128 rows of A and half of the tile's bn rows of B into its shared memory, at
+// the same offsets in both CTAs; the first CTA of the pair (the leader) issues one
+// tcgen05.mma.cta_group::2 per K step of 16, which reads A and B from both CTAs and writes rows
+// 0-127 of the accumulator into the leader's TMEM and rows 128-255 into the peer's. So each CTA
+// loads 128 x 64 + bn/2 x 64 elements per stage for the same tensor-core work as a 128 x bn x 64
+// stage of the single-CTA kernel: a third less shared-memory fill per flop, and stages half as
+// large, so the ring is deeper. Protocol (no TMA multicast anywhere):
+//   - both producers wait on their own "empty" barrier of a stage; the leader's producer posts
+//     the stage's whole byte count (both CTAs' copies) on its own "full" barrier; both issue
+//     their copies with .cta_group::2 so the bytes complete on the leader's "full" barrier;
+//   - the leader's MMA lane waits on "full", issues, and commits with .multicast::cluster to
+//     the "empty" barriers of both CTAs, and each finished tile to both CTAs' "tfull";
+//   - every epilogue warp of both CTAs reads its own TMEM and arrives on the leader's "tempty"
+//     (2 x 8 arrivals) through its cluster address (mapa);
+//   - a cluster barrier after set-up (barriers initialised, TMEM allocated in both CTAs) and
+//     before TMEM is freed, so no CTA touches a peer that has not started or has left.
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+/// The shared::cluster address of the same variable in the cluster's CTA 0.
+__device__ __forceinline__ uint32_t leader_addr(const void* p) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(0));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map,
+                                                 uint32_t bar_leader, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_leader), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16_pair(uint32_t d_tmem, uint64_t a, uint64_t b,
+                                               uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+/// Arrive on `bar` in both CTAs of the pair once every MMA this thread issued has completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+  const uint16_t mask = 0x3;
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(smem_u32(bar)),
+      "h"(mask)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+/// Bytes of one stage of the paired kernel in each CTA: 128 rows of A and bn / 2 of B.
+__host__ __device__ constexpr uint32_t pair_stage_bytes(int bn) {
+  return kTileA + static_cast<uint32_t>(bn / 2) * kBK * 2;
+}
+
+__host__ __device__ constexpr size_t epi_bytes(int mode) {
+  return mode == kEpiSurOut      ? kStageBytes32 + kRowConstBytes
+         : mode == kEpiF32       ? kStageBytes32
+         : mode == kEpiGeluInfer ? kStageBytes16
+                                 : 0;
+}
+
+/// Stages of the paired kernel's ring: as many as fit beside the epilogue's staging.
+__host__ __device__ constexpr int pair_stages(int mode, int bn) {
+  const size_t room = kSmemMax - 1024 - 256 - epi_bytes(mode);
+  const int n = static_cast<int>(room / pair_stage_bytes(bn));
+  return n > kStagesMax ? kStagesMax : n;
+}
+
+template <int MODE>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    gemm_pair_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+                     const GemmArgs g) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const uint32_t stage_sz = pair_stage_bytes(g.bn);
+  const int stages = pair_stages(MODE, g.bn);
+  Bars* const bars = reinterpret_cast<Bars*>(smem + stages * stage_sz);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+
+  const int m_tiles = (g.M + 2 * kBM - 1) / (2 * kBM);
+  const int n_tiles = g.N / g.bn;
+  const int kb_per = g.K / kBK;
+  const int units = m_tiles * n_tiles;
+  const int cid = static_cast<int>(blockIdx.x >> 1), ncl = static_cast<int>(gridDim.x >> 1);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(&bars->full[s], 1);
+      mbar_init(&bars->empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&bars->tfull[b], 1);
+      mbar_init(&bars->tempty[b], 2 * kEpiWarps);  // every epilogue warp of both CTAs
+    }
+    mbar_init(&bars->drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&bars->tmem_base)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem = bars->tmem_base;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+      const uint32_t tx = 2 * stage_sz;  // both CTAs' copies complete on the leader's barrier
+      uint32_t it = 0;
+      bool ok = true;
+      for (int u = cid; u < units && ok; u += ncl) {
+        const Unit w = decode(u, m_tiles, n_tiles);
+        for (int kb = 0; kb < kb_per; ++kb, ++it) {
+          const int s = static_cast<int>(it % stages);
+          const uint32_t ph = (it / stages) & 1u;
+          if (!mbar_wait(&bars->empty[s], ph ^ 1u)) {
+            ok = false;
+            break;
+          }
+          uint8_t* const sa = smem + s * stage_sz;
+          if (leader) mbar_expect_tx(&bars->full[s], tx);
+          const uint32_t full_l = leader_addr(&bars->full[s]);
+          const int kx = kb * kBK;
+          tma_load_2d_pair(sa, &ta, full_l, kx, w.mt * 2 * kBM + static_cast<int>(rank) * kBM);
+          tma_load_2d_pair(sa + kTileA, &tb, full_l, kx,
+                           w.nt * g.bn + static_cast<int>(rank) * (g.bn / 2));
+        }
+      }
+      if (!ok) atomicExch(g.err, 1);
+      if (leader) {
+        // The last stages' copies (both CTAs') have landed before the leader goes on.
+        const uint32_t issued = it;
+        for (uint32_t k = 0; k < static_cast<uint32_t>(stages) && k < issued; ++k) {
+          const uint32_t last = issued - 1 - k;
+          if (!mbar_wait(&bars->full[last % stages], (last / stages) & 1u)) atomicExch(g.err, 1);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      if (leader) {
+        // kind::f16 instruction descriptor as the single-CTA kernel's, M = 256.
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                               (static_cast<uint32_t>(g.bn >> 3) << 17) |
+                               (static_cast<uint32_t>((2 * kBM) >> 4) << 24);
+        uint32_t it = 0, local = 0;
+        bool ok = true;
+        for (int u = cid; u < units && ok; u += ncl, ++local) {
+          const uint32_t b = local & 1u, tph = (local >> 1) & 1u;
+          if (!mbar_wait(&bars->tempty[b], tph ^ 1u)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + b * kBNMax;
+          for (int kb = 0; kb < kb_per; ++kb, ++it) {
+            const int s = static_cast<int>(it % stages);
+            const uint32_t ph = (it / stages) & 1u;
+            if (!mbar_wait(&bars->full[s], ph)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a_addr = smem_u32(smem + s * stage_sz);
+            const uint32_t b_addr = a_addr + kTileA;
+#pragma unroll
+            for (int j = 0; j < kBK / 16; ++j)
+              umma_bf16_pair(d, sdesc(a_addr + 32u * j), sdesc(b_addr + 32u * j), idesc,
+                             (kb | j) != 0 ? 1u : 0u);
+            umma_commit_pair(&bars->empty[s]);
+          }
+          if (ok) umma_commit_pair(&bars->tfull[b]);
+        }
+        if (!ok) atomicExch(g.err, 1);
+        umma_commit_pair(&bars->drain);
+      }
+      // Both CTAs: every MMA (which reads this CTA's stages and writes its TMEM) has completed.
+      if (!mbar_wait(&bars->drain, 0)) atomicExch(g.err, 1);
+    }
+  } else {
+    const int q = warp & 3;
+    const int ew = warp - 2, half = ew >> 2;
+    float* const tile = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256) +
+                        static_cast<size_t>(ew) * 32 *
+                            (MODE == kEpiGeluInfer ? kStageLd16 : kStageLd);
+    float* const rowc = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256 +
+                                                 kStageBytes32) +
+                        static_cast<size_t>(ew) * 32 * kRowsPerTile * 2;
+    uint32_t local = 0;
+    bool ok = true;
+    for (int u = cid; u < units; u += ncl, ++local) {
+      const Unit w = decode(u, m_tiles, n_tiles);
+      const uint32_t b = local & 1u, tph = (local >> 1) & 1u;
+      if (!__all_sync(0xffffffffu, mbar_wait(&bars->tfull[b], tph))) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16) + b * kBNMax;
+      epilogue_tile<MODE>(g, w.mt * 2 * kBM + static_cast<int>(rank) * kBM, w.nt * g.bn, tbase,
+                          q, half, 2, lane, tile, rowc);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(leader_addr(&bars->tempty[b]));
+    }
+    if (!ok && lane == 0) atomicExch(g.err, 1);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTmemCols));
   }
 }
@@ -601,7 +941,31 @@ void launch(const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t 
   if (sms <= 0) WWB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
   int grid = max_ctas > 0 ? max_ctas : sms;
   if (grid > units) grid = units;
-  gemm_kernel<MODE><<<grid, kThreads, smem, stream>>>(a.map, b.map, g);
+  gemm_kernel<MODE><<<grid, epi_threads(MODE), smem, stream>>>(a.map, b.map, g);
+  WWB_CHECK(cudaGetLastError());
+}
+
+template <int MODE>
+void launch_pair(const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t stream) {
+  const int stages = pair_stages(MODE, g.bn);
+  const size_t smem = 1024 + static_cast<size_t>(stages) * pair_stage_bytes(g.bn) + 256 +
+                      epi_bytes(MODE);
+  if (stages < 2 || smem > kSmemMax)
+    throw CudaError(cudaErrorInvalidValue, "paired GEMM tile needs too much shared memory");
+  static std::once_flag once;
+  std::call_once(once, [] {
+    WWB_CHECK(cudaFuncSetAttribute(gemm_pair_kernel<MODE>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kSmemMax)));
+  });
+  const int m_tiles = (g.M + 2 * kBM - 1) / (2 * kBM);
+  const int units = m_tiles * (g.N / g.bn);
+  int sms = runtime().sm_count;
+  if (sms <= 0) WWB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+  int clusters = sms / 2;
+  if (clusters > units) clusters = units;
+  if (clusters < 1) clusters = 1;
+  gemm_pair_kernel<MODE><<<2 * clusters, kThreads, smem, stream>>>(a.map, b.map, g);
   WWB_CHECK(cudaGetLastError());
 }
 
@@ -611,6 +975,7 @@ Operand make_operand(const __nv_bfloat16* base, int rows, int k, int ld, int box
   Operand op{};
   op.rows = rows;
   op.k = k;
+  op.box = box_rows;
   const cuuint64_t dims[2] = {static_cast<cuuint64_t>(k), static_cast<cuuint64_t>(rows)};
   const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
   const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(box_rows)};
@@ -639,6 +1004,9 @@ bool gemm_shape_ok(const GemmArgs& g, const Operand& a, const Operand& b, const 
   if (g.ldo % 8 || g.ldo < g.N) return no("output row stride not a multiple of 8 or below N");
   if (g.out_t && g.ldt < g.M) return no("transposed row stride below M");
   if (g.err == nullptr) return no("no status word");
+  if (a.box != kBM || b.box != gemm_b_box(g)) return no("operand box rows do not match the tiles");
+  if (g.pair && (g.splits != 1 || g.out_t != nullptr))
+    return no("paired tiles only for the inference epilogues");
   return true;
 }
 
@@ -661,6 +1029,14 @@ bool sur_out_ok(const GemmArgs& g, const char** why) {
 
 void gemm(int mode, const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t stream,
           int max_ctas) {
+  if (g.pair) {
+    switch (mode) {
+      case kEpiGeluInfer: return launch_pair<kEpiGeluInfer>(g, a, b, stream);
+      case kEpiF32: return launch_pair<kEpiF32>(g, a, b, stream);
+      case kEpiSurOut: return launch_pair<kEpiSurOut>(g, a, b, stream);
+      default: throw CudaError(cudaErrorInvalidValue, "paired tiles: inference epilogues only");
+    }
+  }
   switch (mode) {
     case kEpiGeluTrain: launch<kEpiGeluTrain>(g, a, b, stream, max_ctas); break;
     case kEpiGeluInfer: launch<kEpiGeluInfer>(g, a, b, stream, max_ctas); break;

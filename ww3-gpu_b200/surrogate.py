@@ -14,6 +14,7 @@ import numpy as np
 from . import OK, WwError, init, lib
 
 EPI_GELU_TRAIN, EPI_GELU_INFER, EPI_F32, EPI_DGELU, EPI_ATOMIC = 1, 2, 3, 4, 5
+PAIRED = 16  # with EPI_GELU_INFER or EPI_F32: two CTAs of a cluster per 256-row tile
 
 # Per-point columns of ww_sur_judge's statistics.
 J_HS, J_TAU_REF, J_TAU_CAND, J_TAU_GROSS, J_BAND_ERR, J_BAND_REF, J_S_ERR2, J_S_REF2, \
