@@ -59,8 +59,11 @@ constexpr size_t kStageBytes32 = kEpiWarps * 32 * kStageLd * sizeof(float);
 /// quarter, the groups' warps taking every (ew / 4)-th chunk): more where the registers allow,
 /// so the epilogue keeps up with the tensor cores.
 __host__ __device__ constexpr int epi_warps(int mode) {
-  return mode == 2 ? 12 : 8;
+  return mode == 2 || mode == 6 ? 12 : 8;
 }
+/// Pipeline stages of the single-CTA kernel per mode: the surrogate-output mode trades one for
+/// its larger epilogue staging.
+__host__ __device__ constexpr int stages_of(int mode) { return mode == 6 ? 3 : kStages; }
 __host__ __device__ constexpr int epi_threads(int mode) { return 64 + 32 * epi_warps(mode); }
 // kEpiGeluInfer stages its bf16 chunk too: 32 rows of 16 words (+1 padding word), so the warp
 // stores rows of 64 contiguous bytes, eight lanes a row.
@@ -85,7 +88,7 @@ __host__ __device__ constexpr uint32_t stage_bytes(int bn) {
 /// Dynamic shared memory of a launch: alignment slack, the stages, the barriers' 256-byte slot
 /// and the epilogue's staging areas.
 __host__ __device__ constexpr size_t smem_bytes(int mode, int bn) {
-  return 1024 + kStages * static_cast<size_t>(stage_bytes(bn)) + 256 +
+  return 1024 + stages_of(mode) * static_cast<size_t>(stage_bytes(bn)) + 256 +
          stage_bytes_w(mode, epi_warps(mode));
 }
 
@@ -430,9 +433,18 @@ __device__ __forceinline__ void sur_chunk(const GemmArgs& g, int m_base, int n, 
 /// q*32 + lane), its chunks half, half + 2, ... of the tile's bn columns from n_base.
 /// Calls body(c, r) for chunks c = c0, c0 + 2, ... < nchunks with r the chunk's 32 TMEM
 /// columns, the next chunk's load in flight while body runs on the current one.
-template <class Body>
+template <bool DB = true, class Body>
 __device__ __forceinline__ void for_chunks(uint32_t tbase, int c0, int nchunks, int step,
                                            Body&& body) {
+  if constexpr (!DB) {  // one buffer: fewer registers, no load in flight during body
+    for (int c = c0; c < nchunks; c += step) {
+      uint32_t r[32];
+      tmem_ld32_async(tbase + 32u * c, r);
+      tmem_wait32(r);
+      body(c, r);
+    }
+    return;
+  }
   uint32_t ra[32], rb[32];
   int c = c0;
   if (c >= nchunks) return;
@@ -466,7 +478,7 @@ __device__ __forceinline__ void epilogue_tile(const GemmArgs& g, int m_base, int
     const int k0 = n_base / g.sur.nth;
     sur_row_consts(g, m, k0, rowc, lane);
     float racc = 0.0f, gacc = 0.0f;
-    for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
+    for_chunks<false>(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
       const int n = n_base + 32 * c;
       const float bl = __ldg(g.bias + n + lane);
       sur_chunk(g, m_base + q * 32, n, k0, r, bl, my_shift, racc, gacc, tile, rowc, lane);
@@ -519,7 +531,8 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
   // cast), so the compiler keeps every derived pointer in the shared space (LDS/STS).
   uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const uint32_t stage_sz = stage_bytes(g.bn);
-  Bars* const bars = reinterpret_cast<Bars*>(smem + kStages * stage_sz);
+  constexpr int ST = stages_of(MODE);
+  Bars* const bars = reinterpret_cast<Bars*>(smem + ST * stage_sz);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   const int m_tiles = (g.M + kBM - 1) / kBM;
@@ -529,7 +542,7 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
   const int units = m_tiles * n_tiles * splits;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < ST; ++s) {
       mbar_init(&bars->full[s], 1);
       mbar_init(&bars->empty[s], 1);
     }
@@ -561,8 +574,8 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
       for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
         const Unit w = decode(u, m_tiles, n_tiles);
         for (int kb = 0; kb < kb_per; ++kb, ++it) {
-          const int s = static_cast<int>(it % kStages);
-          const uint32_t ph = (it / kStages) & 1u;
+          const int s = static_cast<int>(it % ST);
+          const uint32_t ph = (it / ST) & 1u;
           if (!mbar_wait(&bars->empty[s], ph ^ 1u)) {
             ok = false;
             break;
@@ -578,9 +591,9 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
       // Every copy this lane started has landed before the CTA can exit (in a normal run the
       // MMA lane has already consumed them all and these waits return at once).
       const uint32_t issued = it;
-      for (uint32_t k = 0; k < kStages && k < issued; ++k) {
+      for (uint32_t k = 0; k < ST && k < issued; ++k) {
         const uint32_t last = issued - 1 - k;
-        if (!mbar_wait(&bars->full[last % kStages], (last / kStages) & 1u)) atomicExch(g.err, 1);
+        if (!mbar_wait(&bars->full[last % ST], (last / ST) & 1u)) atomicExch(g.err, 1);
       }
     }
   } else if (warp == 1) {
@@ -601,8 +614,8 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
         tc_fence_after();
         const uint32_t d = tmem + b * kBNMax;
         for (int kb = 0; kb < kb_per; ++kb, ++it) {
-          const int s = static_cast<int>(it % kStages);
-          const uint32_t ph = (it / kStages) & 1u;
+          const int s = static_cast<int>(it % ST);
+          const uint32_t ph = (it / ST) & 1u;
           if (!mbar_wait(&bars->full[s], ph)) {
             ok = false;
             break;
