@@ -123,6 +123,13 @@ int ww_snl1_select_kernel(int igrid, int which);
  * kernel chosen (as ww_snl1_select_kernel numbers them), or -1. */
 int ww_snl1_autotune(int igrid);
 
+/* B200 extension, a test of the failure path (no counterpart in the reference). With bytes > 0
+ * (at most 1024), every CTA of grid igrid's pair kernels expects that many bytes more than its
+ * first bulk copy brings, so its bounded wait (about a second) runs out: the CTA stops, the
+ * launch completes with the DIA's status word set, and ww_snl1 returns ERR_KERNEL; nothing
+ * faults, hangs or stays in flight, and the next call with bytes = 0 runs normally. */
+int ww_snl1_test_stall(int igrid, int bytes);
+
 /* B200 extension (the autotuner). The W3SRCE kernels' CTAs per SM, each count with the
  * shared-memory carveout that fits it (the rest of the SM's memory is L1), timed on a sample
  * of the caller's own points (arguments as ww_srce_batch takes them, host arrays, read only:

@@ -228,3 +228,33 @@ def test_autotune_picks_a_kernel_that_stays_bitexact(pkg, oracle, synth, cfg36):
     s_ref, d_ref = oracle.w3snl1(cfg, sig, g["a"], g["cg"], g["kdmean"])
     assert_bitexact(s, s_ref, "S after autotune")
     assert_bitexact(d, d_ref, "D after autotune")
+
+
+def test_bounded_wait_reports_instead_of_hanging(pkg, oracle, synth, cfg36):
+    """The failure path of the DIA's bulk-copy waits, made to run out on purpose: with the test
+    hook every CTA expects bytes its first copy never brings; its bounded wait gives up (about a
+    second), the launch ends, ww_snl1 reports ERR_KERNEL, and the next call is exact again."""
+    import ctypes
+    import time
+
+    cfg, sig = cfg36
+    grid = pkg.Snl1Grid(cfg, sig, igrid=8)
+    grid.select_kernel(pkg.KERNEL_PAIR)
+    L = pkg.lib()
+    L.ww_snl1_test_stall.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.ww_snl1_test_stall.restype = ctypes.c_int
+    g = synth.sea_states(600, seed=88, depth_range=(5.0, 4000.0))
+    assert L.ww_snl1_test_stall(8, 16) == pkg.OK
+    t0 = time.time()
+    try:
+        grid(g["a"], g["cg"], g["kdmean"])
+    except pkg.WwError:
+        pass
+    assert pkg.last_error() == pkg.ERR_KERNEL
+    assert time.time() - t0 < 120
+    assert L.ww_snl1_test_stall(8, 0) == pkg.OK
+    s, d = grid(g["a"], g["cg"], g["kdmean"])
+    assert pkg.last_error() == pkg.OK
+    s_ref, d_ref = oracle.w3snl1(cfg, sig, g["a"], g["cg"], g["kdmean"])
+    assert_bitexact(s, s_ref, "S after the stalled call")
+    assert_bitexact(d, d_ref, "D after the stalled call")

@@ -42,7 +42,7 @@ EXPORTS = (
     "ww_kokkos_fallback_add", "ww_va_host_read", "ww_va_host_write", "ww_va_host_read_cols",
     "ww_va_host_wrote_cols", "ww_va_host_update", "ww_va_device_zero_cols", "ww_va_device",
     "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_steps_fuse", "ww_snl1_autotune",
-    "ww_srce_autotune", "ww_autotune_report", "ww_ktp3_batch", "ww_ktp3_batch_va",
+    "ww_srce_autotune", "ww_autotune_report", "ww_snl1_test_stall", "ww_ktp3_batch", "ww_ktp3_batch_va",
     "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va", "ww_snl1_noalloc",
     "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_sds4", "ww_sin4",
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",

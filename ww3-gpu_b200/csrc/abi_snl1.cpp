@@ -453,6 +453,14 @@ int ww_snl1_enabled(void) { return ww_kokkos_flag("WW_KOKKOS_SNL1") != 0 ? 1 : 0
 
 int ww_snl1_last_error(void) { return g_status.get(); }
 
+int ww_snl1_test_stall(int igrid, int bytes) {
+  auto it = contexts().find(igrid);
+  if (it == contexts().end() || !it->second->ready) return WW_KOKKOS_ERR_NOT_INITIALISED;
+  if (bytes < 0 || bytes > 1024) return WW_KOKKOS_ERR_BAD_SHAPE;
+  it->second->dev.stall_tx = bytes;
+  return WW_KOKKOS_OK;
+}
+
 int ww_snl1_autotune(int igrid) {
   try {
     auto it = contexts().find(igrid);

@@ -371,6 +371,7 @@ struct Sur {
   // inference scratch (per chunk)
   DBuf<float> ps, gv, gsum, head;
   DBuf<int> shift, rej, nrej, nrej_total;
+  DBuf<int> rej_all;  ///< the rejected points of one gated call (all its chunks)
   GateParams gate{0.05f, 1e30f};
   LossWeights lw{0.0f, 0.0f, 1};
   // FP64 judge
@@ -420,6 +421,7 @@ void sur_scratch(Sur& s, int rows) {
     s.shift.alloc(rows);
     s.rej.alloc(rows);
   }
+  if (s.rej_all.n < static_cast<size_t>(rows)) s.rej_all.alloc(rows);
   if (!s.nrej.p) {
     s.nrej.alloc(1);
     s.nrej_total.alloc(1);
@@ -427,10 +429,11 @@ void sur_scratch(Sur& s, int rows) {
 }
 
 /// One chunk (n <= kInferRows points) through the network with the fused output epilogue:
-/// S and D of every point, then the gate (rejected points listed in s.rej, counted in s.nrej).
+/// S and D of every point, then the gate: rejected points listed in s.rej and counted in s.nrej
+/// (zeroed here), or, with `rej` given, appended as base + index to rej at the count *rej_n.
 void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* kd, float* so,
                    float* dd, int* accepted, float* gv, const GateParams& gate, int* total,
-                   cudaStream_t st) {
+                   cudaStream_t st, int* rej = nullptr, int* rej_n = nullptr, int base = 0) {
   Mlp& m = s.net;
   // The inputs, and zeros for D (the surrogate does not model the diagonal term; the plain DIA
   // overwrites the rejected points' D afterwards) and for the gate sums the epilogue adds to.
@@ -458,8 +461,12 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
   if (!sur_out_ok(g, &why)) throw CudaError(cudaErrorInvalidValue, why);
   run_gemm(kEpiSurOut, g, make_operand(in, n, m.dh, m.dh, kBM),
            make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, gemm_b_box(g)), st);
-  WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
-  gate_points(gate, n, s.gsum.p, s.head.p, accepted, gv, s.rej.p, s.nrej.p, total, st);
+  if (rej == nullptr) {
+    WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
+    rej = s.rej.p;
+    rej_n = s.nrej.p;
+  }
+  gate_points(gate, n, s.gsum.p, s.head.p, accepted, gv, rej, rej_n, total, st, base);
 }
 
 /// The surrogate's S for npts points (device arrays) into s/d, gated, with the plain DIA on the
@@ -469,19 +476,21 @@ void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* k
                bool reset_count = true) {
   const int nspec = s.g.nspec, nk = s.g.nk;
   sur_scratch(s, std::min(npts, kInferRows));
+  if (s.rej_all.n < static_cast<size_t>(npts)) s.rej_all.alloc(npts);
   if (reset_count) WWB_CHECK(cudaMemsetAsync(s.nrej_total.p, 0, sizeof(int), st));
+  // Every chunk's rejected points go into one list of the call's points, so the plain DIA runs
+  // once on all of them (one launch that fills the GPU) instead of once per chunk.
+  WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
   for (int p0 = 0; p0 < npts; p0 += kInferRows) {
     const int n = std::min(kInferRows, npts - p0);
-    const float* ap = a + static_cast<size_t>(p0) * nspec;
-    const float* cp = cg + static_cast<size_t>(p0) * nk;
-    float* sp = so + static_cast<size_t>(p0) * nspec;
-    float* dp = dd + static_cast<size_t>(p0) * nspec;
-    sur_chunk_out(s, n, ap, cp, kd + p0, sp, dp, accepted ? accepted + p0 : nullptr, nullptr,
-                  gate, s.nrej_total.p, st);
-    if (fallback &&
-        !launch_snl1_list(s.dia, n, s.rej.p, s.nrej.p, ap, cp, kd + p0, sp, dp, nullptr, st))
-      throw CudaError(cudaErrorInvalidValue, "gated DIA: the pair and band kernels cannot run this grid");
+    sur_chunk_out(s, n, a + static_cast<size_t>(p0) * nspec, cg + static_cast<size_t>(p0) * nk,
+                  kd + p0, so + static_cast<size_t>(p0) * nspec,
+                  dd + static_cast<size_t>(p0) * nspec, accepted ? accepted + p0 : nullptr,
+                  nullptr, gate, s.nrej_total.p, st, s.rej_all.p, s.nrej.p, p0);
   }
+  if (fallback && !launch_snl1_list(s.dia, npts, s.rej_all.p, s.nrej.p, a, cg, kd, so, dd,
+                                    nullptr, st))
+    throw CudaError(cudaErrorInvalidValue, "gated DIA: the pair and band kernels cannot run this grid");
 }
 
 void build_f64(Sur& s) {

@@ -571,7 +571,7 @@ __global__ void targets_kernel(SurGrid g, int npts, const float* __restrict__ s,
 __global__ void gate_kernel(GateParams gate, int npts, const float* __restrict__ gsum,
                             const float* __restrict__ head, int* __restrict__ accepted,
                             float* __restrict__ gv, int* __restrict__ rej_list,
-                            int* __restrict__ nrej, int* __restrict__ nrej_total) {
+                            int* __restrict__ nrej, int* __restrict__ nrej_total, int base) {
   const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= npts) return;
   const float r = gsum[2 * ip], gs = gsum[2 * ip + 1];
@@ -585,7 +585,7 @@ __global__ void gate_kernel(GateParams gate, int npts, const float* __restrict__
     gv[2 * ip + 1] = resid;
   }
   if (!ok) {
-    rej_list[atomicAdd(nrej, 1)] = ip;
+    rej_list[atomicAdd(nrej, 1)] = base + ip;
     if (nrej_total) atomicAdd(nrej_total, 1);
   }
 }
@@ -972,10 +972,10 @@ void targets(const SurGrid& g, int npts, const float* s, const float* ps, const 
 
 void gate_points(const GateParams& gate, int npts, const float* gsum, const float* head,
                  int* accepted, float* gv, int* rej_list, int* nrej, int* nrej_total,
-                 cudaStream_t st) {
+                 cudaStream_t st, int base) {
   if (npts <= 0) return;
   gate_kernel<<<(npts + 255) / 256, 256, 0, st>>>(gate, npts, gsum, head, accepted, gv, rej_list,
-                                                  nrej, nrej_total);
+                                                  nrej, nrej_total, base);
   WWB_CHECK(cudaGetLastError());
 }
 

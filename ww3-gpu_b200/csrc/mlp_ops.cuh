@@ -78,11 +78,12 @@ void targets(const SurGrid& g, int npts, const float* s, const float* ps, const 
 
 /// The gate of every point after the fused output epilogue (kEpiSurOut): from its gate sums
 /// (gsum, 2 per point) and head output, accept or add it to the compacted rejected list
-/// (count at *nrej, zeroed by the caller; also added to *nrej_total when given); per-point flag
-/// and (gv, may be null) head and energy residual.
+/// (count at *nrej, zeroed by the caller; also added to *nrej_total when given; a point's entry
+/// is base + its index, so several chunks can fill one list); per-point flag and (gv, may be
+/// null) head and energy residual.
 void gate_points(const GateParams& gate, int npts, const float* gsum, const float* head,
                  int* accepted, float* gv, int* rej_list, int* nrej, int* nrej_total,
-                 cudaStream_t st);
+                 cudaStream_t st, int base = 0);
 
 /// Training loss and the output gradient. out (m x ldo fp32), t (m x ldt): grad (m x dout bf16)
 /// = dL/dout; loss (3 floats: MSE, energy-budget, error-head terms) accumulated.

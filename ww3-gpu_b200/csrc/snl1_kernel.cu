@@ -906,12 +906,12 @@ __device__ __forceinline__ float2 mulS(float2 a, float2 b) {
 /// One elected thread: expect the bytes of two points and start the four bulk copies.
 __device__ __forceinline__ void tma_fetch_pair(uint64_t* bar, float* stage, const float* a,
                                                const float* cg, int i0, int i1, int nspec,
-                                               int nk) {
+                                               int nk, unsigned extra = 0) {
   const unsigned bytes_a = static_cast<unsigned>(nspec) * 4u;
   const unsigned bytes_c = static_cast<unsigned>(nk) * 4u;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(2u * (bytes_a + bytes_c))
+               "r"(2u * (bytes_a + bytes_c) + extra)
                : "memory");
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -973,7 +973,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) snl1_pair_kernel(
     mbar_init(bar, 1);
     if (blockIdx.x < npairs) {
       const int i0 = first_of(blockIdx.x), i1 = second_of(blockIdx.x);
-      tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk);
+      tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk, static_cast<unsigned>(p.stall_tx));
       kd0 = __ldg(kdmean + i0);
       kd1 = __ldg(kdmean + i1);
     }
@@ -1286,7 +1286,7 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
     mbar_init(bar, 1);
     if (blockIdx.x < npairs) {
       const int i0 = first_of(blockIdx.x), i1 = second_of(blockIdx.x);
-      tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk);
+      tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk, static_cast<unsigned>(p.stall_tx));
       kd0 = __ldg(kdmean + i0);
       kd1 = __ldg(kdmean + i1);
     }

@@ -23,6 +23,10 @@ struct Snl1Dev {
   const int* ic;            ///< device, 16 x NSPEC (gather form)
   const float* af11;        ///< device, NSPECX (gather form)
   const float* sig;         ///< device, NK
+  /// Test of the failure path (0 in every normal run): bytes added to the bytes each CTA of the
+  /// pair kernels expects for its first bulk copy, which therefore never completes, so its
+  /// bounded wait runs out and the launch reports it (ww_snl1_test_stall).
+  int stall_tx;
 };
 
 enum Snl1Kernel {
