@@ -1281,14 +1281,11 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
   }
   for (int i = tid; i < nfrchg; i += BLOCK) afr[i] = p.af11_row[i];
   for (int i = tid; i < nk; i += BLOCK) wrow[i] = kTpiInv / __ldg(p.sig + i);
-  float kd0 = 0.0f, kd1 = 0.0f;
   if (tid == 0) {
     mbar_init(bar, 1);
     if (blockIdx.x < npairs) {
       const int i0 = first_of(blockIdx.x), i1 = second_of(blockIdx.x);
       tma_fetch_pair(bar, stage, a, cg, i0, i1, nspec, nk, static_cast<unsigned>(p.stall_tx));
-      kd0 = __ldg(kdmean + i0);
-      kd1 = __ldg(kdmean + i1);
     }
   }
   __syncthreads();
@@ -1323,9 +1320,11 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
     const int i0 = first_of(pp), i1 = second_of(pp);
     const bool has1 = 2 * pp + 1 < npts;
     float2* const conx = conx2 + buf * nk;
+    // CONS of the two points by two threads of different warps, before the copy is awaited.
+    if (tid == 0) cons2[buf].x = dia_cons(p, __ldg(kdmean + i0));
+    if (tid == 32) cons2[buf].y = dia_cons(p, __ldg(kdmean + i1));
     const bool lost = !mbar_wait(bar, parity, err);
     parity ^= 1u;
-    if (tid == 0) cons2[buf] = make_float2(dia_cons(p, kd0), dia_cons(p, kd1));
     // 2a-2b. CON per frequency row and UE = A / CON, with the parametric tail up each column
     // from row NFR. The CTA's width is a whole number of rows, so a thread's bins are column r0
     // of rows q0, q0 + dq, ...: it forms each row's CON itself (the column-0 thread keeps it for
@@ -1354,8 +1353,6 @@ __global__ void __launch_bounds__(NTH * G, 2) snl1_pairtile_kernel(
     if (tid == 0 && pnext < npairs) {
       const int j0 = first_of(pnext), j1 = second_of(pnext);
       tma_fetch_pair(bar, stage, a, cg, j0, j1, nspec, nk);
-      kd0 = __ldg(kdmean + j0);
-      kd1 = __ldg(kdmean + j1);
     }
     const float2 cons = cons2[buf];
 
