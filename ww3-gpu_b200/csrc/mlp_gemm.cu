@@ -36,6 +36,12 @@ constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, taking alternate 32-
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kTileA = kBM * kBK * 2;
 constexpr uint32_t kTmemCols = 2 * kBNMax;
+// The GELU-inference mode keeps the whole bias vector in shared memory, so each chunk reads its
+// 32 values as 8 broadcast 16-byte loads instead of 32 shuffles (the surrogate-output mode,
+// whose epilogue is shared-memory heavy already, measured slower that way and keeps shuffles).
+constexpr int kBiasMax = 1536;
+constexpr size_t kBiasBytes = kBiasMax * sizeof(float);
+__host__ __device__ constexpr bool bias_in_smem(int mode) { return mode == 2; }
 constexpr uint32_t kSpin = 1u << 24;  // polls before a wait gives up (seconds, never in a normal run)
 
 constexpr int kStagesMax = 8;  // the paired-tile kernel's ring (its stages are half as large)
@@ -89,7 +95,7 @@ __host__ __device__ constexpr uint32_t stage_bytes(int bn) {
 /// and the epilogue's staging areas.
 __host__ __device__ constexpr size_t smem_bytes(int mode, int bn) {
   return 1024 + stages_of(mode) * static_cast<size_t>(stage_bytes(bn)) + 256 +
-         stage_bytes_w(mode, epi_warps(mode));
+         stage_bytes_w(mode, epi_warps(mode)) + (bias_in_smem(mode) ? kBiasBytes : 0);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -204,8 +210,10 @@ constexpr float kGeluC = 0.7978845608028654f;
 constexpr float kGeluA = 0.044715f;
 
 __device__ __forceinline__ float gelu(float z) {
-  const float t = tanh_fast(kGeluC * (z + kGeluA * z * z * z));
-  return 0.5f * z * (1.0f + t);
+  // c (z + a z^3) = z (c + c a z^2); 0.5 z (1 + t) = h + h t with h = z / 2.
+  const float t = tanh_fast(z * fmaf(kGeluC * kGeluA, z * z, kGeluC));
+  const float h = 0.5f * z;
+  return fmaf(h, t, h);
 }
 
 __device__ __forceinline__ float dgelu(float z) {
@@ -311,13 +319,17 @@ __device__ __forceinline__ void f32_chunk(const GemmArgs& g, int m_base, int n,
 /// words of the warp's tile, then eight lanes store one row's 64 contiguous bytes (four rows
 /// per instruction), so every store fills whole 32-byte sectors.
 __device__ __forceinline__ void gelu_infer_chunk(const GemmArgs& g, int m_base, int n,
-                                                 const uint32_t (&r)[32], float bl,
+                                                 const uint32_t (&r)[32], const float* bs,
                                                  uint32_t* tile16, int lane) {
 #pragma unroll
-  for (int j = 0; j < 32; j += 2) {
-    const float v0 = gelu(__uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j));
-    const float v1 = gelu(__uint_as_float(r[j + 1]) + __shfl_sync(0xffffffffu, bl, j + 1));
+  for (int j = 0; j < 32; j += 4) {
+    const float4 b = *reinterpret_cast<const float4*>(bs + j);
+    const float v0 = gelu(__uint_as_float(r[j]) + b.x);
+    const float v1 = gelu(__uint_as_float(r[j + 1]) + b.y);
+    const float v2 = gelu(__uint_as_float(r[j + 2]) + b.z);
+    const float v3 = gelu(__uint_as_float(r[j + 3]) + b.w);
     tile16[lane * kStageLd16 + j / 2] = pack_bf16(v0, v1);
+    tile16[lane * kStageLd16 + j / 2 + 1] = pack_bf16(v2, v3);
   }
   __syncwarp();
   const int sub = lane >> 3, w = 2 * (lane & 7);
@@ -467,7 +479,7 @@ __device__ __forceinline__ void for_chunks(uint32_t tbase, int c0, int nchunks, 
 template <int MODE>
 __device__ __forceinline__ void epilogue_tile(const GemmArgs& g, int m_base, int n_base,
                                               uint32_t tbase, int q, int half, int step, int lane,
-                                              float* tile, float* rowc) {
+                                              float* tile, float* rowc, const float* bias_s) {
   const int row = q * 32 + lane;
   const int m = m_base + row;
   const int nchunks = g.bn / 32;
@@ -497,8 +509,7 @@ __device__ __forceinline__ void epilogue_tile(const GemmArgs& g, int m_base, int
     uint32_t* const tile16 = reinterpret_cast<uint32_t*>(tile);
     for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
       const int n = n_base + 32 * c;
-      const float bl = __ldg(g.bias + n + lane);
-      gelu_infer_chunk(g, m_base + q * 32, n, r, bl, tile16, lane);
+      gelu_infer_chunk(g, m_base + q * 32, n, r, bias_s + n, tile16, lane);
     });
   } else {
     for_chunks(tbase, half, nchunks, step, [&](int c, const uint32_t(&r)[32]) {
@@ -559,6 +570,11 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  // The bias vector after the epilogue staging (the modes that read it from shared memory).
+  float* const bias_s = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256 +
+                                                 stage_bytes_w(MODE, epi_warps(MODE)));
+  if constexpr (bias_in_smem(MODE))
+    for (int i = threadIdx.x; i < g.N; i += blockDim.x) bias_s[i] = __ldg(g.bias + i);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -658,7 +674,8 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
       }
       tc_fence_after();
       const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16) + b * kBNMax;
-      epilogue_tile<MODE>(g, w.mt * kBM, w.nt * g.bn, tbase, q, half, EW / 4, lane, tile, rowc);
+      epilogue_tile<MODE>(g, w.mt * kBM, w.nt * g.bn, tbase, q, half, EW / 4, lane, tile, rowc,
+                          bias_s);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bars->tempty[b]);
@@ -749,10 +766,11 @@ __host__ __device__ constexpr uint32_t pair_stage_bytes(int bn) {
 }
 
 __host__ __device__ constexpr size_t epi_bytes(int mode) {
-  return mode == kEpiSurOut      ? kStageBytes32 + kRowConstBytes
-         : mode == kEpiF32       ? kStageBytes32
-         : mode == kEpiGeluInfer ? kStageBytes16
-                                 : 0;
+  return (mode == kEpiSurOut      ? kStageBytes32 + kRowConstBytes
+          : mode == kEpiF32       ? kStageBytes32
+          : mode == kEpiGeluInfer ? kStageBytes16
+                                  : 0) +
+         (bias_in_smem(mode) ? kBiasBytes : 0);
 }
 
 /// Stages of the paired kernel's ring: as many as fit beside the epilogue's staging.
@@ -799,6 +817,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
   }
+  float* const bias_s = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256 +
+                                                 (epi_bytes(MODE) - (bias_in_smem(MODE) ? kBiasBytes : 0)));
+  if constexpr (bias_in_smem(MODE))
+    for (int i = threadIdx.x; i < g.N; i += blockDim.x) bias_s[i] = __ldg(g.bias + i);
   tc_fence_before();
   __syncthreads();
   cluster_sync();
@@ -902,7 +924,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       tc_fence_after();
       const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16) + b * kBNMax;
       epilogue_tile<MODE>(g, w.mt * 2 * kBM + static_cast<int>(rank) * kBM, w.nt * g.bn, tbase,
-                          q, half, 2, lane, tile, rowc);
+                          q, half, 2, lane, tile, rowc, bias_s);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(leader_addr(&bars->tempty[b]));
@@ -1042,6 +1064,8 @@ bool sur_out_ok(const GemmArgs& g, const char** why) {
 
 void gemm(int mode, const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t stream,
           int max_ctas) {
+  if (bias_in_smem(mode) && g.N > kBiasMax)
+    throw CudaError(cudaErrorInvalidValue, "GEMM: more output columns than the bias buffer holds");
   if (g.pair) {
     switch (mode) {
       case kEpiGeluInfer: return launch_pair<kEpiGeluInfer>(g, a, b, stream);
