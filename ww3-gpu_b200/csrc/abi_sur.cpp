@@ -395,6 +395,23 @@ struct Sur {
         if (x) cudaStreamDestroy(x);
     }
   } pipe;
+  /// A side stream for the D zeros of a gated call, so they overlap the network's GEMMs (which
+  /// leave most of the HBM bandwidth unused) instead of adding a pass of their own.
+  struct Side {
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    void make() {
+      if (st) return;
+      WWB_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      WWB_CHECK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+      WWB_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    }
+    ~Side() {
+      if (fork) cudaEventDestroy(fork);
+      if (join) cudaEventDestroy(join);
+      if (st) cudaStreamDestroy(st);
+    }
+  } side;
 };
 
 std::map<int, std::unique_ptr<Sur>>& surs() {
@@ -435,9 +452,9 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
                    float* dd, int* accepted, float* gv, const GateParams& gate, int* total,
                    cudaStream_t st, int* rej = nullptr, int* rej_n = nullptr, int base = 0) {
   Mlp& m = s.net;
-  // The inputs, and zeros for D (the surrogate does not model the diagonal term; the plain DIA
-  // overwrites the rejected points' D afterwards) and for the gate sums the epilogue adds to.
-  prep(s.g, n, a, cg, kd, m.ix0.p, m.din, s.ps.p, s.shift.p, st, dd, s.gsum.p);
+  // The inputs, and zeros for the gate sums the output epilogue adds to (D is zeroed by the
+  // caller).
+  prep(s.g, n, a, cg, kd, m.ix0.p, m.din, s.ps.p, s.shift.p, st, nullptr, s.gsum.p);
   const bf16* in = m.ix0.p;
   int kin = m.din;
   for (int l = 0; l < 3; ++l) {
@@ -481,6 +498,13 @@ void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* k
   // Every chunk's rejected points go into one list of the call's points, so the plain DIA runs
   // once on all of them (one launch that fills the GPU) instead of once per chunk.
   WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
+  // D = 0 for every point (the surrogate does not model the diagonal term), on the side stream
+  // while the network runs; the plain DIA overwrites the rejected points' D after it.
+  s.side.make();
+  WWB_CHECK(cudaEventRecord(s.side.fork, st));
+  WWB_CHECK(cudaStreamWaitEvent(s.side.st, s.side.fork, 0));
+  WWB_CHECK(cudaMemsetAsync(dd, 0, static_cast<size_t>(npts) * nspec * sizeof(float), s.side.st));
+  WWB_CHECK(cudaEventRecord(s.side.join, s.side.st));
   for (int p0 = 0; p0 < npts; p0 += kInferRows) {
     const int n = std::min(kInferRows, npts - p0);
     sur_chunk_out(s, n, a + static_cast<size_t>(p0) * nspec, cg + static_cast<size_t>(p0) * nk,
@@ -488,6 +512,7 @@ void sur_apply(Sur& s, int npts, const float* a, const float* cg, const float* k
                   dd + static_cast<size_t>(p0) * nspec, accepted ? accepted + p0 : nullptr,
                   nullptr, gate, s.nrej_total.p, st, s.rej_all.p, s.nrej.p, p0);
   }
+  WWB_CHECK(cudaStreamWaitEvent(st, s.side.join, 0));
   if (fallback && !launch_snl1_list(s.dia, npts, s.rej_all.p, s.nrej.p, a, cg, kd, so, dd,
                                     nullptr, st))
     throw CudaError(cudaErrorInvalidValue, "gated DIA: the pair and band kernels cannot run this grid");
