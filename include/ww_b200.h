@@ -384,6 +384,20 @@ int ww_wave_mapt(int nsea, int msea, int ncell, const int* mapsf, const float* a
 /* NAR1D must be 121; ewn1, ecg1 (0:NAR1D) in: the Fortran's tables (the differing values are
  * counted on stderr), out: the device's; n1max, dsie likewise. */
 int ww_wave_distab(int nar1d, float* ewn1, float* ecg1, int* n1max, float* dsie);
+/* W3CFLXY (w3pro3md.F90:1980-2136; the reference's device form prop_cflxy.hpp:61-135, which its
+ * W3WAVE driver calls for JSEA = 1..NSEAL when FLOGRD(9,3), wave_w3wave.hpp:548-574; the
+ * reference exports no C entry for it). cflxymax[ISEA-1] = CFLXYMAX(ISEA), ISEA = 1..NSEA: the
+ * largest spatial CFL number over every (IK, ITH), with the compiled loop's MAX operand order.
+ * mapsf (MSEA,3), columns 1-2 read; clats (0:NSEA); ecos, esin (NTH); dpdx..dqdy (NY,NX); cg
+ * (0:NK+1, 0:NSEA); cx, cy (0:NSEA), read when flcur (may be NULL otherwise); mgp 0/1: the W3_MGP
+ * form (VGX, VGY subtracted; the reference's driver uses 0). While grid igrid (> 0) records a step
+ * (ww_step_begin) the call is recorded and CFLXYMAX of the replays stays on the device, as
+ * ww_ktp3_batch_va's CFLTHMAX does; igrid 0 runs at once. */
+int ww_wave_cflxy(int igrid, int nsea, int msea, int nx, int ny, int nk, int nth, int flcur,
+                  int mgp, float dtg, float vgx, float vgy, const int* mapsf, const float* clats,
+                  const float* ecos, const float* esin, const float* dpdx, const float* dpdy,
+                  const float* dqdx, const float* dqdy, const float* cg, const float* cx,
+                  const float* cy, float* cflxymax);
 
 /* ---------------------------------------------------------------- gridded output (W3OUTG) */
 /* Replaces ww_outg_va (outg_c.hpp:97-120): W3OUTG (VA, .FALSE., FLOUTG, FLOUTG2) of
@@ -444,7 +458,9 @@ int ww_outg_last_error(void);
  * copies them to the device. TAUT, TAUHFT, TAUHFT2, FWTABLE and the DEL* scalars are one copy per
  * process, the last registration wins. Point entries take npts points, every per-point scalar an
  * array of npts; OUT arguments are copied in as well as out; status in ww_st4_last_error().
- * WW_KOKKOS_ST4_TABLES=1 is accepted and the registered tables are used. */
+ * WW_KOKKOS_ST4_TABLES=1: ww_st4_commit rebuilds the grid's and the module's tables with INSIN4 on
+ * the device (the reference does it with its host C++, st4_shim.cpp:301-345), prints how many
+ * values differ from the registered ones and uses the rebuilt ones. */
 
 /* Replaces ww_st4_init (ww_kokkos_c.hpp:158). OK, NOT_INITIALISED, BAD_SHAPE, UNSUPPORTED (W3_FLX5,
  * or NTH > 128). */
@@ -458,6 +474,20 @@ int ww_st4_set_int(int igrid, int id, const int* data, int rank, const int* lbou
 
 /* Replaces ww_st4_commit (ww_kokkos_c.hpp:172). OK, NOT_INITIALISED, TABLE, RUNTIME. */
 int ww_st4_commit(int igrid);
+
+/* INSIN4(FLTABS) (w3src4md.F90:1014-1288 with TABU_STRESS, TABU_TAUHF, TABU_TAUHF2; the
+ * reference's host C++ st4_insin4.cpp:96-264, st4_tabu_*.cpp, which it runs under
+ * WW_KOKKOS_ST4_TABLES) on the device, bit for bit, for the packet rpar/ipar (ww_st4_init's) and
+ * SIG, DSIP (0:MK+1), TH (MTH), ECOS (MSPEC+MTH). Outputs, column-major, each may be NULL:
+ * satweights, satindices (2*(MTH/2-1)+1, MTH); iktab (MK, 2000); dcki, qbi (2000, 1300); cumulw
+ * (MSPEC, MSPEC); taut (201, 201), tauhft (101, 201) when SINTAILPAR(1) > 0.5 and fltabs;
+ * tauhft2 (101, 201, 51) when also TTAUWSHELTER > 0; del[5] = DELUST, DELALP, DELTAUW, DELU,
+ * DELTAIL (the packet's values where INSIN4 sets none). OK, NOT_INITIALISED, BAD_SHAPE, KERNEL,
+ * RUNTIME. */
+int ww_st4_tables(const float* rpar, int nrpar, const int* ipar, int nipar, const float* sig,
+                  const float* dsip, const float* th, const float* ecos, int fltabs,
+                  float* satweights, int* satindices, int* iktab, float* dcki, float* qbi,
+                  float* cumulw, float* taut, float* tauhft, float* tauhft2, float* del);
 
 /* Replaces ww_sds4 (ww_kokkos_c.hpp:177): W3SDS4. a, srhs, ddiag, brlambda (nspec, npts);
  * k, cg (nk, npts); whitecap (4, npts); the scalars (npts). */

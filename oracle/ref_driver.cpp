@@ -188,3 +188,45 @@ extern "C" int ref_st4_tables(const float* rpar, const int* ipar, const float* s
   del[4] = p.deltail;
   return 0;
 }
+
+// W3CFLXY of the reference (kokkos/src/ww_kokkos/prop_cflxy.hpp:61-135) for ISEA = 1..NSEA, as
+// its W3WAVE driver calls it (wave_w3wave.hpp:563-572; mgp selects the W3_MGP form): mapsf
+// (NSEA,3) column-major, clats (0:NSEA), ecos/esin (NTH), dpdx..dqdy (NY,NX), cg (0:NK+1,0:NSEA),
+// cx/cy (0:NSEA) in; cflxymax (NSEA) out.
+#include "ww_kokkos/prop_cflxy.hpp"
+
+extern "C" int ref_w3cflxy(int nsea, int nx, int ny, int nk, int nth, int flcur, int mgp,
+                           float dtg, float vgx, float vgy, const int* mapsf, const float* clats,
+                           const float* ecos, const float* esin, const float* dpdx,
+                           const float* dpdy, const float* dqdx, const float* dqdy,
+                           const float* cg, const float* cx, const float* cy, float* cflxymax) {
+  using namespace ww::prop;
+  Params p{};
+  p.nx = nx;
+  p.ny = ny;
+  p.nsea = nsea;
+  p.nk = nk;
+  p.nth = nth;
+  p.nspec = nk * nth;
+  p.flcur = flcur;
+  Grid g{};
+  g.mapsf = mapsf;
+  g.clats = clats;
+  g.ecos = ecos;
+  g.esin = esin;
+  g.dpdx = dpdx;
+  g.dpdy = dpdy;
+  g.dqdx = dqdx;
+  g.dqdy = dqdy;
+  Step s{};
+  s.cg = cg;
+  s.cx = cx;
+  s.cy = cy;
+  for (int isea = 1; isea <= nsea; ++isea) {
+    if (mgp)
+      w3cflxy<true>(isea, dtg, nullptr, nullptr, cflxymax[isea - 1], vgx, vgy, p, g, s);
+    else
+      w3cflxy<false>(isea, dtg, nullptr, nullptr, cflxymax[isea - 1], vgx, vgy, p, g, s);
+  }
+  return 0;
+}

@@ -36,6 +36,9 @@ def _bind(L):
     L.ww_va_host_read.restype = I
     L.ww_va_host_write.argtypes = [I, P, I, I]
     L.ww_va_host_write.restype = I
+    if hasattr(L, "ww_wave_cflxy"):
+        L.ww_wave_cflxy.argtypes = [I] * 9 + [F, F, F] + [P] * 12
+        L.ww_wave_cflxy.restype = I
     return L
 
 
@@ -85,7 +88,23 @@ class Calls:
                            sc.p(p["taubbl"]), sc.p(p["tauice"]), self.shave.ctypes.data)
         assert L.ww_srce_last_error() == 0
 
-    def step(self):
+    def cflxy(self):
+        """W3CFLXY, W3WAVE's CFL diagnostic before the propagation (wave_w3wave.hpp:548-574)."""
+        x, xs = self.xc, self.xcs
+        ip = x["ipar"]  # NX, NY, NSEA, NK, NTH, NSPEC, ICLOSE, FLCX, FLCY, FLAGLL, FLCUR
+        nsea = int(ip[2])
+        self.cfl = np.zeros(nsea, np.float32)
+        rc = self.L.ww_wave_cflxy(self.ig, nsea, nsea, int(ip[0]), int(ip[1]), int(ip[3]),
+                                  int(ip[4]), int(ip[10]), 0, xs["dtg"], 0.0, 0.0,
+                                  *[x[a].ctypes.data for a in ("mapsf", "clats", "ecos", "esin",
+                                                               "dpdx", "dpdy", "dqdx", "dqdy",
+                                                               "cg", "cx", "cy")],
+                                  self.cfl.ctypes.data)
+        assert rc == 0, rc
+
+    def step(self, cflxy=False):
+        if cflxy:
+            self.cflxy()
         self.ktp3(1)
         self.xyp3()
         self.ktp3(2)
@@ -147,8 +166,8 @@ def test_step_graph_equals_calls_and_reference(pkg, oracle, synth, case):
     _gpu_grid(pkg, oracle, synth, st, t, sr, 703)
     c_rec = Calls(L, 703, np.array(xc["va"], np.float32, copy=True), kc, xc, pts)
     with pkg.Step(703) as step:
-        c_rec.step()
-    assert step.ops() == 4
+        c_rec.step(cflxy=True)
+    assert step.ops() == 5
     step.run(nsteps)
     va_rec = c_rec.read()
     assert_bitexact(va_rec, va_ref, "VA, replayed graph vs the reference")

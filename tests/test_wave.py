@@ -1,6 +1,8 @@
 """W3WAVE's per-step support routines through the reference's C ABI names (ww_wave_gath,
 ww_wave_scat, ww_wave_uwnd, ww_wave_utrn, ww_wave_dzxy, ww_wave_map3, ww_wave_mapt,
-ww_wave_distab) against the reference's own shim (kokkos/src/fortran_iface/wave_support_shim.cpp
+ww_wave_distab, and ww_wave_cflxy for W3CFLXY, which the reference calls from its W3WAVE driver
+only and is reached here through oracle/ref_driver.cpp's ref_w3cflxy) against the reference's
+own shim (kokkos/src/fortran_iface/wave_support_shim.cpp
 with its headers wave_gath_scat.hpp, updt_uwnd.hpp, updt_utrn.hpp, updt_dzxy.hpp, prop_map3.hpp,
 prop_mapt.hpp, disp_distab.hpp, compiled into oracle/_ref/libref_ww3.so): every output element,
 bit for bit, on seeded grids with MAPSF carrying more rows than sea points (MSEA > NSEA)."""
@@ -248,3 +250,137 @@ def test_wave_statuses_match_reference(pkg, synth):
     bad = sf.copy()
     bad[2 * msea] = 20 * 12 + 1  # the library refuses a cell outside the grid
     assert L.ww_wave_gath(1, 4, nsea, nsea + 1, msea, 20, 12, p(va), p(bad), p(f)) == BAD_SHAPE
+
+
+def _cflxy_case(synth, nx, ny, nk, nth, seed, ties):
+    """A seeded W3CFLXY case on a synthetic grid; ties=True plants zero group velocities and
+    signed-zero metric terms so that the MAX operand order decides the sign of zero results."""
+    sta, sf, nsea, msea = grid(synth, nx, ny, seed)
+    rng = np.random.default_rng(seed + 40)
+    th = (np.arange(nth) + 0.5) * (2 * np.pi / nth)
+    ecos = np.cos(th).astype(np.float32)
+    esin = np.sin(th).astype(np.float32)
+    clats = rng.uniform(0.2, 1.0, nsea + 1).astype(np.float32)
+    met = [rng.uniform(-4e-4, 4e-4, nx * ny).astype(np.float32) for _ in range(4)]
+    cg = rng.uniform(0.5, 25.0, (nsea + 1, nk + 2)).astype(np.float32)
+    cx = rng.uniform(-1.5, 1.5, nsea + 1).astype(np.float32)
+    cy = rng.uniform(-1.5, 1.5, nsea + 1).astype(np.float32)
+    if ties:
+        cg[1::5, :] = 0.0  # every fifth point: no advection, all CFL numbers are +-0
+        for m in met:
+            m[::7] = -0.0
+        cx[::3] = 0.0
+        cy[::3] = -0.0
+    return sf, nsea, msea, clats, ecos, esin, met, np.ascontiguousarray(cg.reshape(-1)), cx, cy
+
+
+@needs_ref
+@pytest.mark.gpu
+@pytest.mark.parametrize("nk,nth,flcur,mgp,ties", [
+    (36, 36, 0, 0, False), (36, 36, 1, 0, False), (36, 36, 0, 0, True), (36, 36, 1, 0, True),
+    (5, 7, 0, 0, True), (5, 7, 1, 0, True), (5, 7, 1, 1, True), (4, 1, 0, 0, True),
+    (4, 1, 0, 1, True), (4, 1, 1, 0, True), (3, 2, 0, 1, True)])
+def test_cflxy(pkg, synth, nk, nth, flcur, mgp, ties):
+    nx, ny = 41, 29
+    sf, nsea, msea, clats, ecos, esin, met, cg, cx, cy = _cflxy_case(synth, nx, ny, nk, nth,
+                                                                      nk * 10 + nth, ties)
+    dtg, vgx, vgy = 900.0, 0.75, -0.5
+    L = _gpu(pkg)
+    L.ww_wave_cflxy.argtypes = [I] * 9 + [F, F, F] + [P] * 12
+    L.ww_wave_cflxy.restype = I
+    R = _oracle.ref_lib()
+    R.ref_w3cflxy.argtypes = [I] * 7 + [F, F, F] + [P] * 12
+    R.ref_w3cflxy.restype = I
+    sf_n = np.ascontiguousarray(sf.reshape(3, msea)[:, :nsea].reshape(-1))
+    ref = np.full(nsea, 7.0, np.float32)
+    assert R.ref_w3cflxy(nsea, nx, ny, nk, nth, flcur, mgp, dtg, vgx, vgy, p(sf_n), p(clats),
+                         p(ecos), p(esin), *[p(m) for m in met], p(cg), p(cx), p(cy),
+                         p(ref)) == 0
+    dev = np.full(nsea, 7.0, np.float32)
+    rc = L.ww_wave_cflxy(0, nsea, msea, nx, ny, nk, nth, flcur, mgp, dtg, vgx, vgy, p(sf),
+                         p(clats), p(ecos), p(esin), *[p(m) for m in met], p(cg), p(cx), p(cy),
+                         p(dev))
+    assert rc == OK
+    assert_bitexact(dev, ref, f"CFLXYMAX nk {nk} nth {nth} flcur {flcur} mgp {mgp}")
+    assert np.all(ref >= 0)  # CFLXYMAX starts at 0
+    if ties and not mgp:
+        assert np.any(ref == 0)
+
+
+def test_cflxy_refuses_bad_maps(pkg, synth):
+    """A MAPSF entry off the grid is BAD_SHAPE before any device work (no GPU needed)."""
+    L = pkg.lib()
+    L.ww_wave_cflxy.argtypes = [I] * 9 + [F, F, F] + [P] * 12
+    L.ww_wave_cflxy.restype = I
+    nx, ny, nk, nth = 12, 9, 3, 4
+    sf, nsea, msea, clats, ecos, esin, met, cg, cx, cy = _cflxy_case(synth, nx, ny, nk, nth, 5,
+                                                                      False)
+    sf = sf.copy()
+    sf[msea + 1] = ny + 1
+    out = np.zeros(nsea, np.float32)
+    rc = L.ww_wave_cflxy(0, nsea, msea, nx, ny, nk, nth, 0, 0, 900.0, 0.0, 0.0, p(sf), p(clats),
+                         p(ecos), p(esin), *[p(m) for m in met], p(cg), None, None, p(out))
+    assert rc == BAD_SHAPE
+
+
+@needs_ref
+@pytest.mark.gpu
+def test_cflxy_on_a_propagation_case(pkg, synth):
+    """W3CFLXY on the arrays of a W3XYP3 case (regular 0.25-degree grid, currents on, NK = NTH =
+    36): the module arrays exactly as the propagation reads them."""
+    xc = synth.xyp3_case(48, 32, seed=7, ref=_oracle.ref_w3map3)
+    ip = xc["ipar"]
+    nx, ny, nsea, nk, nth, flcur = (int(ip[i]) for i in (0, 1, 2, 3, 4, 10))
+    arrs = [np.ascontiguousarray(xc[a]) for a in ("mapsf", "clats", "ecos", "esin", "dpdx",
+                                                  "dpdy", "dqdx", "dqdy", "cg", "cx", "cy")]
+    L = _gpu(pkg)
+    L.ww_wave_cflxy.argtypes = [I] * 9 + [F, F, F] + [P] * 12
+    L.ww_wave_cflxy.restype = I
+    R = _oracle.ref_lib()
+    R.ref_w3cflxy.argtypes = [I] * 7 + [F, F, F] + [P] * 12
+    R.ref_w3cflxy.restype = I
+    ref = np.zeros(nsea, np.float32)
+    assert R.ref_w3cflxy(nsea, nx, ny, nk, nth, flcur, 0, xc["dtg"], 0.0, 0.0,
+                         *[p(a) for a in arrs], p(ref)) == 0
+    dev = np.zeros(nsea, np.float32)
+    assert L.ww_wave_cflxy(0, nsea, nsea, nx, ny, nk, nth, flcur, 0, xc["dtg"], 0.0, 0.0,
+                           *[p(a) for a in arrs], p(dev)) == OK
+    assert_bitexact(dev, ref, "CFLXYMAX, propagation case")
+    assert ref.max() > 0
+
+
+@needs_ref
+@pytest.mark.parametrize("flcur,mgp", [(0, 0), (1, 0), (1, 1)])
+def test_ref_cflxy_is_the_formula(synth, flcur, mgp):
+    """The reference's W3CFLXY as oracle/ref_driver.cpp binds it equals the routine's formula
+    (w3pro3md.F90:2105-2128) restated in float32 numpy, up to the sign of zero: pins the driver's
+    array layouts (MAPSF, CG, the metric fields) before the device is compared with it."""
+    nx, ny, nk, nth = 23, 17, 6, 9
+    sf, nsea, msea, clats, ecos, esin, met, cg, cx, cy = _cflxy_case(synth, nx, ny, nk, nth, 3,
+                                                                      False)
+    dtg, vgx, vgy = np.float32(600.0), np.float32(0.3), np.float32(-0.2)
+    R = _oracle.ref_lib()
+    R.ref_w3cflxy.argtypes = [I] * 7 + [F, F, F] + [P] * 12
+    R.ref_w3cflxy.restype = I
+    sf_n = np.ascontiguousarray(sf.reshape(3, msea)[:, :nsea].reshape(-1))
+    ref = np.zeros(nsea, np.float32)
+    assert R.ref_w3cflxy(nsea, nx, ny, nk, nth, flcur, mgp, float(dtg), float(vgx), float(vgy),
+                         p(sf_n), p(clats), p(ecos), p(esin), *[p(m) for m in met], p(cg), p(cx),
+                         p(cy), p(ref)) == 0
+    isea = np.arange(1, nsea + 1)
+    ixy = (sf_n[:nsea] - 1) * ny + (sf_n[nsea:2 * nsea] - 1)
+    dpdx, dpdy, dqdx, dqdy = (m[ixy][:, None, None] for m in met)
+    cl = clats[isea][:, None, None]
+    cgk = cg.reshape(nsea + 1, nk + 2)[isea, 1:nk + 1][:, :, None]
+    cxt = (ecos[None, None, :] * cgk) / cl
+    cyt = esin[None, None, :] * cgk
+    if mgp:
+        cxt, cyt = cxt - vgx / cl, cyt - vgy
+    if flcur:
+        cxt = cxt + cx[isea][:, None, None] / cl
+        cyt = cyt + cy[isea][:, None, None]
+    vx = (cxt * dpdx + cyt * dpdy) * dtg
+    vy = (cxt * dqdx + cyt * dqdy) * dtg
+    want = np.maximum(np.maximum(vx, vy).max(axis=(1, 2)), np.float32(0))
+    assert want.dtype == np.float32
+    np.testing.assert_array_equal(ref, want)

@@ -44,7 +44,7 @@ EXPORTS = (
     "ww_va_report", "ww_va_device_ptr", "ww_va_state", "ww_steps_fuse", "ww_snl1_autotune",
     "ww_srce_autotune", "ww_autotune_report", "ww_snl1_test_stall", "ww_ktp3_batch", "ww_ktp3_batch_va",
     "ww_prop3_last_error", "ww_xyp3_batch", "ww_xyp3_batch_va", "ww_snl1_noalloc",
-    "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_sds4", "ww_sin4",
+    "ww_st4_init", "ww_st4_set_real", "ww_st4_set_int", "ww_st4_commit", "ww_st4_tables", "ww_sds4", "ww_sin4",
     "ww_spr4", "ww_st4_enabled", "ww_st4_last_error", "ww_srce_init", "ww_srce",
     "ww_srce_batch", "ww_srce_batch_va", "ww_srce_enabled", "ww_srce_last_error",
     "ww_srce_batch_device", "ww_xyp3_batch_mpi", "ww_xyp3_mpi_pack", "ww_xyp3_mpi_unpack",
@@ -52,6 +52,7 @@ EXPORTS = (
     "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes", "ww_steps_run", "ww_outg_va", "ww_outg_part",
     "ww_outg_last_error", "ww_outg_device", "ww_wave_gath", "ww_wave_scat", "ww_wave_uwnd",
     "ww_wave_utrn", "ww_wave_dzxy", "ww_wave_map3", "ww_wave_mapt", "ww_wave_distab",
+    "ww_wave_cflxy",
     "ww_mlp_create", "ww_mlp_destroy", "ww_mlp_param_count", "ww_mlp_set_params",
     "ww_mlp_get_params", "ww_mlp_get_grads", "ww_mlp_train_step", "ww_mlp_forward",
     "ww_mlp_gemm", "ww_mlp_last_error", "ww_sur_init", "ww_sur_synth", "ww_sur_dataset",

@@ -7,12 +7,14 @@
 // status codes (NOT_INITIALISED before init, BAD_SHAPE for packet lengths, UNSUPPORTED for
 // W3_FLX5, TABLE for a bad registration or a missing / short array at commit), module arrays one
 // per process with the last registration winning, OUT arguments copied in as well as out,
-// npts == 0 a no-op. WW_KOKKOS_ST4_TABLES=1 asks the reference to rebuild the tables with its C++
-// INSIN4; this library takes the registered tables, which the Fortran's INSIN4 built (the
-// reference's rebuild has the same bits by construction).
+// npts == 0 a no-op. WW_KOKKOS_ST4_TABLES=1 makes ww_st4_commit rebuild the tables with INSIN4
+// (the reference: its C++ on the host, st4_shim.cpp:301-345; here: st4_tables_kernel.cu on the
+// device), print how many values differ from the registered ones and use the rebuilt ones.
+// ww_st4_tables runs the same device INSIN4 on a packet and host arrays and returns its tables.
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <string>
@@ -20,6 +22,7 @@
 
 #include "st4_registry.hpp"
 #include "st4_srce.cuh"
+#include "st4_tables_kernel.cuh"
 #include "staging.hpp"
 #include "step.hpp"
 #include "wwb_common.hpp"
@@ -142,6 +145,134 @@ void out(T* h, const T* d, size_t n, cudaStream_t s) {
   if (n) WWB_CHECK(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
 }
 
+
+/// INSIN4's tables on the host, as the device builds them (shapes of st4_tables_kernel.cuh).
+struct HostTables {
+  std::vector<float> satweights, dcki, qbi, cumulw, taut, tauhft, tauhft2;
+  std::vector<int> satindices, iktab;
+};
+
+/// A device buffer of n elements, freed on scope exit.
+template <class T>
+struct Scratch {
+  T* ptr = nullptr;
+  explicit Scratch(size_t n) {
+    if (n) WWB_CHECK(cudaMalloc(&ptr, n * sizeof(T)));
+  }
+  ~Scratch() {
+    if (ptr) cudaFree(ptr);
+  }
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+};
+
+/// Runs INSIN4(FLTABS) on the device for packet p with SIG, DSIP (0:MK+1), TH (MTH), ECOS
+/// (MSPEC+MTH) from the host and brings every table back; the TABU_* tables only where INSIN4
+/// builds them. Returns INSIN4's branches and DEL* values.
+St4TablesPlan build_tables(const st4::Params& p, bool fltabs, const float* sig, const float* dsip,
+                           const float* th, const float* ecos, HostTables& t) {
+  const St4TablesPlan q = st4_tables_plan(p, fltabs);
+  cudaStream_t s = runtime().stream;
+  cudaStream_t s2 = nullptr;
+  WWB_CHECK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t st;
+    ~StreamGuard() { cudaStreamDestroy(st); }
+  } guard{s2};
+  const size_t nsig = static_cast<size_t>(p.mk) + 2;
+  Scratch<float> d_sig(nsig), d_dsip(nsig), d_th(p.mth), d_ecos(p.mspec + p.mth);
+  WWB_CHECK(cudaMemcpyAsync(d_sig.ptr, sig, nsig * 4, cudaMemcpyHostToDevice, s));
+  WWB_CHECK(cudaMemcpyAsync(d_dsip.ptr, dsip, nsig * 4, cudaMemcpyHostToDevice, s));
+  WWB_CHECK(cudaMemcpyAsync(d_th.ptr, th, sizeof(float) * p.mth, cudaMemcpyHostToDevice, s));
+  WWB_CHECK(cudaMemcpyAsync(d_ecos.ptr, ecos, sizeof(float) * (p.mspec + p.mth),
+                            cudaMemcpyHostToDevice, s));
+  const size_t nsat = static_cast<size_t>(q.nsat) * p.mth, nik = static_cast<size_t>(p.mk) * st4::kNdtab;
+  const size_t ntab = static_cast<size_t>(st4::kNkhs) * st4::kNkd;
+  const size_t ncum = static_cast<size_t>(p.mspec) * p.mspec;
+  const size_t ntaut = (q.taut ? static_cast<size_t>(st4::kItauMax + 1) * (st4::kJuMax + 1) : 0);
+  const size_t nhf = (q.tauhf || q.tauhf2)
+                         ? static_cast<size_t>(st4::kIustar + 1) * (st4::kIalpha + 1) : 0;
+  const size_t nhf2 = q.tauhf2 ? nhf * (st4::kIlevTail + 1) : 0;
+  Scratch<float> satw(nsat), dcki(ntab), qbi(ntab), cumulw(ncum), taut(ntaut), tauhft(nhf),
+      tauhft2(nhf2);
+  Scratch<int> sati(nsat), iktab(nik);
+  St4TablesOut o{satw.ptr, sati.ptr, iktab.ptr, dcki.ptr, qbi.ptr, cumulw.ptr,
+                 taut.ptr, tauhft.ptr, tauhft2.ptr};
+  launch_st4_tables(p, q, St4TablesIn{d_sig.ptr, d_dsip.ptr, d_th.ptr, d_ecos.ptr}, o, s, s2);
+  auto back = [&](auto& v, const auto* d, size_t n) {
+    v.resize(n);
+    if (n) WWB_CHECK(cudaMemcpyAsync(v.data(), d, n * sizeof(v[0]), cudaMemcpyDeviceToHost, s));
+  };
+  back(t.satweights, satw.ptr, nsat);
+  back(t.satindices, sati.ptr, nsat);
+  back(t.iktab, iktab.ptr, nik);
+  back(t.dcki, dcki.ptr, ntab);
+  back(t.qbi, qbi.ptr, ntab);
+  back(t.cumulw, cumulw.ptr, ncum);
+  back(t.taut, taut.ptr, ntaut);
+  back(t.tauhft, tauhft.ptr, nhf);
+  back(t.tauhft2, tauhft2.ptr, nhf2);
+  WWB_CHECK(cudaStreamSynchronize(s));
+  return q;
+}
+
+/// Values of b that are not bitwise equal to a's (a missing array counts all of b).
+template <class T>
+long long count_diff(const std::vector<T>& a, const std::vector<T>& b) {
+  if (a.size() != b.size()) return static_cast<long long>(b.size());
+  long long n = 0;
+  for (size_t k = 0; k < a.size(); ++k)
+    if (std::memcmp(&a[k], &b[k], sizeof(T)) != 0) ++n;
+  return n;
+}
+
+/// WW_KOKKOS_ST4_TABLES=1 at commit: grid g's and the module's tables rebuilt by the device
+/// INSIN4(FLTABS=.TRUE.) from g's registered SIG, DSIP, TH and ECOS; the count of values that
+/// differ from the registered ones is printed, and the rebuilt ones replace them. TAUT/TAUHFT
+/// (SINTAILPAR(1) > 0.5) and TAUHFT2 (also TTAUWSHELTER > 0) and their DEL* change only where
+/// INSIN4 builds them, as the Fortran's module state does.
+void rebuild_tables(GridCtx& g, ModuleCtx& m) {
+  const st4::Params& p = g.reg.p;
+  HostTables t;
+  const St4TablesPlan q = build_tables(p, true, g.reg.a[st4::A_SIG].f.data(),
+                                       g.reg.a[st4::A_DSIP].f.data(),
+                                       g.reg.a[st4::A_TH].f.data(),
+                                       g.reg.a[st4::A_ECOS].f.data(), t);
+  auto& ga = g.reg.a;
+  auto& ma = m.reg.a;
+  long long diff = count_diff(ga[st4::A_SATWEIGHTS].f, t.satweights) +
+                   count_diff(ga[st4::A_SATINDICES].i, t.satindices) +
+                   count_diff(ga[st4::A_IKTAB].i, t.iktab) + count_diff(ga[st4::A_DCKI].f, t.dcki) +
+                   count_diff(ga[st4::A_QBI].f, t.qbi) + count_diff(ga[st4::A_CUMULW].f, t.cumulw);
+  if (q.taut) diff += count_diff(ma[st4::A_TAUT].f, t.taut);
+  if (q.tauhf || q.tauhf2) diff += count_diff(ma[st4::A_TAUHFT].f, t.tauhft);
+  if (q.tauhf2) diff += count_diff(ma[st4::A_TAUHFT2].f, t.tauhft2);
+  std::fprintf(stderr,
+               "ww_b200: ST4 tables rebuilt on the device: %lld values differ from the "
+               "registered ones\n",
+               diff);
+  ga[st4::A_SATWEIGHTS].f = std::move(t.satweights);
+  ga[st4::A_SATINDICES].i = std::move(t.satindices);
+  ga[st4::A_IKTAB].i = std::move(t.iktab);
+  ga[st4::A_DCKI].f = std::move(t.dcki);
+  ga[st4::A_QBI].f = std::move(t.qbi);
+  ga[st4::A_CUMULW].f = std::move(t.cumulw);
+  if (q.taut) {
+    ma[st4::A_TAUT].f = std::move(t.taut);
+    m.reg.delu = q.delu;
+    m.reg.deltauw = q.deltauw;
+  }
+  if (q.tauhf || q.tauhf2) {
+    ma[st4::A_TAUHFT].f = std::move(t.tauhft);
+    m.reg.delust = q.delust;
+    m.reg.delalp = q.delalp;
+  }
+  if (q.tauhf2) {
+    ma[st4::A_TAUHFT2].f = std::move(t.tauhft2);
+    m.reg.deltail = q.deltail;
+  }
+}
+
 }  // namespace
 
 /// The committed ST4 state of grid igrid for W3SRCE: scalars, fields (device pointers).
@@ -235,6 +366,49 @@ int ww_st4_set_int(int igrid, int id, const int* data, int rank, const int* lbou
   }
 }
 
+int ww_st4_tables(const float* rpar, int nrpar, const int* ipar, int nipar, const float* sig,
+                  const float* dsip, const float* th, const float* ecos, int fltabs,
+                  float* satweights, int* satindices, int* iktab, float* dcki, float* qbi,
+                  float* cumulw, float* taut, float* tauhft, float* tauhft2, float* del) {
+  try {
+    if (!runtime().ready)
+      return g_status.fail(WW_KOKKOS_ERR_NOT_INITIALISED, "ww_st4_tables before ww_kokkos_init");
+    if (rpar == nullptr || ipar == nullptr || nrpar != st4::NRPAR || nipar != st4::NIPAR ||
+        !sig || !dsip || !th || !ecos || !del)
+      return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_st4_tables: bad packet or null array");
+    const st4::Params p = st4::unpack(rpar, ipar);
+    if (p.nk <= 0 || p.nth <= 1 || p.nspec != p.nk * p.nth || p.mk < p.nk || p.mth < p.nth ||
+        p.mspec < p.nspec)
+      return g_status.fail(WW_KOKKOS_ERR_BAD_SHAPE,
+                           "ww_st4_tables: NK, NTH, NSPEC, MK, MTH, MSPEC inconsistent");
+    HostTables t;
+    const St4TablesPlan q = build_tables(p, fltabs != 0, sig, dsip, th, ecos, t);
+    auto put = [](auto* dst, const auto& v) {
+      if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    put(satweights, t.satweights);
+    put(satindices, t.satindices);
+    put(iktab, t.iktab);
+    put(dcki, t.dcki);
+    put(qbi, t.qbi);
+    put(cumulw, t.cumulw);
+    put(taut, t.taut);
+    put(tauhft, t.tauhft);
+    put(tauhft2, t.tauhft2);
+    del[0] = q.delust;
+    del[1] = q.delalp;
+    del[2] = q.deltauw;
+    del[3] = q.delu;
+    del[4] = q.deltail;
+    g_status.ok();
+    return WW_KOKKOS_OK;
+  } catch (const std::bad_alloc& e) {
+    return g_status.fail(WW_KOKKOS_ERR_RUNTIME, e.what());
+  } catch (const std::exception& e) {
+    return g_status.fail(WW_KOKKOS_ERR_KERNEL, e.what());
+  }
+}
+
 int ww_st4_commit(int igrid) {
   try {
     auto it = grids().find(igrid);
@@ -246,6 +420,7 @@ int ww_st4_commit(int igrid) {
     std::string why;
     if (!st4::reg_check(g.reg, m.reg, why))
       return g_status.fail(WW_KOKKOS_ERR_TABLE, ("ww_st4_commit: " + why).c_str());
+    if (ww_kokkos_flag("WW_KOKKOS_ST4_TABLES") != 0) rebuild_tables(g, m);
     for (int id = 0; id < st4::NARRAYS; ++id) {
       if (st4::kArraySpecs[id].module) {
         m.f[id].upload(m.reg.a[id].f);

@@ -8,6 +8,11 @@
 // run the kernels of ww_utrn, ww_map3 and ww_mapt (MAPSF(MSEA,3) compacted to its first NSEA
 // rows); the others run wave_kernel.cu. WW_KOKKOS_WAVE_COUNT=1 prints "ww_kokkos: W3<R> calls: N"
 // per routine at exit.
+//
+// ww_wave_cflxy (W3CFLXY) has no entry in the reference's C ABI: there the device W3WAVE driver
+// calls it (wave_w3wave.hpp:548-574). Its argument list follows the other routines' (sizes, then
+// the module arrays), and like the _va propagation calls it is recorded into grid igrid's step
+// while that grid records one.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -19,15 +24,16 @@
 #include <vector>
 
 #include "staging.hpp"
+#include "step.hpp"
 #include "wave_kernel.cuh"
 #include "wwb_common.hpp"
 
 namespace wwb {
 namespace {
 
-enum Routine { GATH, SCAT, UWND, UTRN, DZXY, MAP3, MAPT, DISTAB, NROUTINES };
-const char* const kName[NROUTINES] = {"W3GATH", "W3SCAT", "W3UWND", "W3UTRN",
-                                      "W3DZXY", "W3MAP3", "W3MAPT", "DISTAB"};
+enum Routine { GATH, SCAT, UWND, UTRN, DZXY, MAP3, MAPT, DISTAB, CFLXY, NROUTINES };
+const char* const kName[NROUTINES] = {"W3GATH", "W3SCAT", "W3UWND", "W3UTRN", "W3DZXY",
+                                      "W3MAP3", "W3MAPT", "DISTAB", "W3CFLXY"};
 std::atomic<long long> g_calls[NROUTINES];
 
 void print_counts() {
@@ -272,6 +278,65 @@ int ww_wave_dzxy(int nsea, int nx, int ny, const float* zz, const int* mapsta, c
     launch_wave_dzxy(a, s);
     d2h(dzzdx, a.dzzdx, nc, s);
     d2h(dzzdy, a.dzzdy, nc, s);
+    WWB_CHECK(cudaStreamSynchronize(s));
+    return static_cast<int>(WW_KOKKOS_OK);
+  });
+}
+
+int ww_wave_cflxy(int igrid, int nsea, int msea, int nx, int ny, int nk, int nth, int flcur,
+                  int mgp, float dtg, float vgx, float vgy, const int* mapsf, const float* clats,
+                  const float* ecos, const float* esin, const float* dpdx, const float* dpdy,
+                  const float* dqdx, const float* dqdy, const float* cg, const float* cx,
+                  const float* cy, float* cflxymax) {
+  if (nsea < 1 || msea < nsea || nx < 1 || ny < 1 || nk < 1 || nth < 1 || nth > 4096 ||
+      !mapsf || !clats || !ecos || !esin || !dpdx || !dpdy || !dqdx || !dqdy || !cg ||
+      (flcur && (!cx || !cy)) || !cflxymax)
+    return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_wave_cflxy: bad sizes or null pointer");
+  for (int i = 0; i < nsea; ++i) {  // the kernel reads DPDX..DQDY at (MAPSF(ISEA,1:2))
+    const int ix = mapsf[i], iy = mapsf[static_cast<size_t>(msea) + i];
+    if (ix < 1 || ix > nx || iy < 1 || iy > ny)
+      return fail(WW_KOKKOS_ERR_BAD_SHAPE, "ww_wave_cflxy: MAPSF of a sea point off the grid");
+  }
+  return run(CFLXY, [&] {
+    // While grid igrid records a step, the inputs go to buffers the step owns (see step.hpp).
+    StepRecorder* const rec = igrid > 0 ? step_recorder(igrid) : nullptr;
+    std::shared_ptr<Staging> own = rec ? std::make_shared<Staging>() : nullptr;
+    Staging& st = rec ? *own : staging();
+    cudaStream_t s = rec ? step_stream(rec) : runtime().stream;
+    const size_t nc = static_cast<size_t>(nx) * ny, n1 = static_cast<size_t>(nsea) + 1;
+    CflxyArgs a{};
+    a.nsea = nsea;
+    a.msea = msea;
+    a.ny = ny;
+    a.nk = nk;
+    a.nth = nth;
+    a.flcur = flcur != 0;
+    a.mgp = mgp != 0;
+    a.dtg = dtg;
+    a.vgx = vgx;
+    a.vgy = vgy;
+    int k = 60;
+    a.mapsf = st.in(k++, mapsf, 2 * static_cast<size_t>(msea), s);
+    a.clats = st.in(k++, clats, n1, s);
+    a.ecos = st.in(k++, ecos, static_cast<size_t>(nth), s);
+    a.esin = st.in(k++, esin, static_cast<size_t>(nth), s);
+    a.dpdx = st.in(k++, dpdx, nc, s);
+    a.dpdy = st.in(k++, dpdy, nc, s);
+    a.dqdx = st.in(k++, dqdx, nc, s);
+    a.dqdy = st.in(k++, dqdy, nc, s);
+    a.cg = st.in(k++, cg, static_cast<size_t>(nk + 2) * n1, s);
+    a.cx = a.flcur ? st.in(k++, cx, n1, s) : nullptr;
+    a.cy = a.flcur ? st.in(k++, cy, n1, s) : nullptr;
+    a.cflxymax = static_cast<float*>(st.get(72, static_cast<size_t>(nsea) * sizeof(float)));
+    if (rec) {
+      // CFLXYMAX of the replays stays on the device, as W3KTP3's CFLTHMAX does.
+      WWB_CHECK(cudaStreamSynchronize(s));
+      step_keep(rec, own);
+      step_add(rec, [a](cudaStream_t ss) { launch_wave_cflxy(a, ss); });
+      return static_cast<int>(WW_KOKKOS_OK);
+    }
+    launch_wave_cflxy(a, s);
+    d2h(cflxymax, a.cflxymax, static_cast<size_t>(nsea), s);
     WWB_CHECK(cudaStreamSynchronize(s));
     return static_cast<int>(WW_KOKKOS_OK);
   });

@@ -8,19 +8,19 @@
 //
 // Reference: ww3-gpu kokkos/src/ww_kokkos/wave_gath_scat.hpp:48-93 (W3GATH, W3SCAT),
 // updt_uwnd.hpp:70-217 (W3UWND under WNT1 and RWND), updt_dzxy.hpp:60-224 (W3DZXY),
-// disp_distab.hpp:77-185 (WAVNU2 and DISTAB).
+// disp_distab.hpp:77-185 (WAVNU2 and DISTAB), prop_cflxy.hpp:25-135 (W3CFLXY).
 #include "wave_kernel.cuh"
 
 #include "libm_dev.cuh"
+#include "wavnu2_dev.cuh"
 #include "wwb_common.hpp"
 
 namespace wwb {
 namespace {
 
-// constants.F90's PI as REAL and TPI = 2*PI (an exact doubling); GRAV.
+// constants.F90's PI as REAL and TPI = 2*PI (an exact doubling). GRAV is disp::kGravD.
 constexpr float kPi = static_cast<float>(3.141592653589793);
 constexpr float kTpi = 2.0f * kPi;
-constexpr float kGrav = 9.806f;
 
 /// Fortran MAX of two REALs as the build's maxss: a NaN or a tie gives the first operand.
 __device__ __forceinline__ float fmax2(float a, float b) { return (b > a) ? b : a; }
@@ -190,45 +190,7 @@ __global__ void dzxy_trpl_kernel(DzxyArgs a) {
   }
 }
 
-// ---------------------------------------------------------------------------- WAVNU2, DISTAB
-/// WAVNU2(W, H, K, CG, EPS, NMAX, ICON) (w3dispmd.F90:204-346): Newton iteration on
-/// w**2 = g k tanh(k h); the statements' operand order as the reference's object.
-__device__ void wavnu2(float w, float h, float& k, float& cg, float eps, int nmax) {
-  const float zero = 0.0f;
-  float kold = zero;
-  const float w0 = fabsf(w);
-  if (sqrtf(kGrav / h) > w0) {
-    k = w0 / sqrtf(h * kGrav);
-  } else {
-    k = w * w / kGrav;
-  }
-  for (int i = 1; i <= nmax; ++i) {
-    const float dif = fabsf(k - kold);
-    const float rdif = (k != zero) ? dif / k : zero;
-    if (dif < eps && rdif < eps) break;  // ICON = 1; DISTAB discards ICON
-    kold = k;
-    const float gk = kold * kGrav;
-    const float kh = h * kold;
-    const float th = dm::tanhf(kh);
-    const float f = gk * th - w * w;
-    float fd;
-    if (kh > 25.0f) {
-      fd = th * kGrav;
-    } else {
-      const float c = dm::coshf(kh);
-      fd = th * kGrav + (h * gk) / (c * c);
-    }
-    k = kold - f / fd;
-  }
-  const float kh2 = h * (k + k);
-  const float cgd = w0 / k * 0.5f;
-  cg = (kh2 > 25.0f) ? cgd : cgd * (1.0f + kh2 / dm::sinhf(kh2));
-  if (w < zero) {
-    k = -k;
-    cg = -cg;
-  }
-}
-
+// ---------------------------------------------------------------------------- DISTAB
 __global__ void distab_kernel(int nar1d, float dsie, float ecg0, float* ewn1, float* ecg1) {
   WWB_GRID_LOOP(t, nar1d + 1) {
     const int i = static_cast<int>(t);
@@ -239,10 +201,101 @@ __global__ void distab_kernel(int nar1d, float dsie, float ecg0, float* ewn1, fl
     }
     const float si = static_cast<float>(i) * dsie;
     float k = 0.0f, cg = 0.0f;
-    wavnu2(si, 1.0f, k, cg, 1e-7f, 15);
+    disp::wavnu2(si, 1.0f, k, cg, 1e-7f, 15);
     ewn1[i] = k;
     ecg1[i] = cg;
   }
+}
+
+/// max_r of the reference's W3CFLXY: a > b ? a : b (x86 MAXSS/MAXPS with a as destination), so a
+/// NaN or a tie of zeros of opposite sign yields b, as the CPU code's operand order decides.
+__device__ __forceinline__ float maxr(float a, float b) { return a > b ? a : b; }
+
+/// The operands of one sea point's CFL numbers (prop_cflxy.hpp:28-48, w3pro3md.F90:2111-2127):
+/// for a direction (ECOS, ESIN) and a group velocity CG(IK), the advection velocity
+/// CXTOT = ECOS*CG/CLATS (- VGX/CLATS under W3_MGP, + CX/CLATS with currents), CYTOT likewise
+/// without the latitude factor, and the two CFL numbers (CXTOT*DPDX + CYTOT*DPDY)*DTG and
+/// (CXTOT*DQDX + CYTOT*DQDY)*DTG, every operation rounded on its own.
+struct CflPoint {
+  float clat, dpdx, dpdy, dqdx, dqdy, dtg, vgx, vgy, cxs, cys;
+  bool flcur, mgp;
+  __device__ __forceinline__ void at(float ec, float es, float cgk, float& vx, float& vy) const {
+    float cxt = __fdiv_rn(__fmul_rn(ec, cgk), clat);
+    float cyt = __fmul_rn(es, cgk);
+    if (mgp) {
+      cxt = __fsub_rn(cxt, __fdiv_rn(vgx, clat));
+      cyt = __fsub_rn(cyt, vgy);
+    }
+    if (flcur) {
+      cxt = __fadd_rn(cxt, __fdiv_rn(cxs, clat));
+      cyt = __fadd_rn(cyt, cys);
+    }
+    vx = __fmul_rn(__fadd_rn(__fmul_rn(cxt, dpdx), __fmul_rn(cyt, dpdy)), dtg);
+    vy = __fmul_rn(__fadd_rn(__fmul_rn(cxt, dqdx), __fmul_rn(cyt, dqdy)), dtg);
+  }
+};
+
+/// W3CFLXY, one thread per sea point (ISEA = JSEA under W3_SHRD). CFLXYMAX starts at 0 and is
+/// raised frequency by frequency in the order the reference's compiled loop takes
+/// (prop_cflxy.hpp:61-135): for NTH >= 2 four running maxima per IK over the direction pairs
+/// (lanes VLCFLX(ITH), VLCFLY(ITH), VLCFLX(ITH+1), VLCFLY(ITH+1)), each started from the value
+/// after the previous IK and reduced as max(max(l3,l1), max(l2,l0)), then an odd last direction;
+/// for NTH = 1 one scalar step. The order only shows for NaNs and signed zeros; it is kept so
+/// that every output bit matches. ECOS/ESIN sit in shared memory (2*NTH floats).
+__global__ void cflxy_kernel(CflxyArgs a) {
+  extern __shared__ float trig[];
+  const int nth = a.nth;
+  for (int i = threadIdx.x; i < nth; i += blockDim.x) {
+    trig[i] = a.ecos[i];
+    trig[nth + i] = a.esin[i];
+  }
+  __syncthreads();
+  const int isea = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (isea > a.nsea) return;
+  const int ix = a.mapsf[isea - 1];
+  const int iy = a.mapsf[static_cast<size_t>(a.msea) + isea - 1];
+  const size_t ixy = static_cast<size_t>(ix - 1) * a.ny + (iy - 1);
+  CflPoint q;
+  q.clat = a.clats[isea];
+  q.dpdx = a.dpdx[ixy];
+  q.dpdy = a.dpdy[ixy];
+  q.dqdx = a.dqdx[ixy];
+  q.dqdy = a.dqdy[ixy];
+  q.dtg = a.dtg;
+  q.vgx = a.vgx;
+  q.vgy = a.vgy;
+  q.flcur = a.flcur;
+  q.mgp = a.mgp;
+  q.cxs = a.flcur ? a.cx[isea] : 0.0f;
+  q.cys = a.flcur ? a.cy[isea] : 0.0f;
+  const float* cg = a.cg + static_cast<size_t>(isea) * (a.nk + 2);
+  const int npair = nth / 2;
+  float c = 0.0f;
+  for (int ik = 1; ik <= a.nk; ++ik) {
+    const float cgk = cg[ik];
+    float vx, vy;
+    if (nth >= 2) {
+      float m0 = c, m1 = c, m2 = c, m3 = c;
+      for (int j = 0; j < npair; ++j) {
+        float vx1, vy1;
+        q.at(trig[2 * j], trig[nth + 2 * j], cgk, vx, vy);
+        q.at(trig[2 * j + 1], trig[nth + 2 * j + 1], cgk, vx1, vy1);
+        m0 = maxr(m0, vx);
+        m1 = maxr(m1, vy);
+        m2 = maxr(m2, vx1);
+        m3 = maxr(m3, vy1);
+      }
+      c = maxr(maxr(m3, m1), maxr(m2, m0));
+      if (nth & 1) {
+        q.at(trig[nth - 1], trig[2 * nth - 1], cgk, vx, vy);
+        c = maxr(c, a.flcur ? maxr(vx, vy) : maxr(vy, vx));
+      }
+    } else {
+      q.at(trig[0], trig[1], cgk, vx, vy);
+      c = maxr(c, (a.flcur || a.mgp) ? maxr(vx, vy) : maxr(vy, vx));
+    }
+  }
+  a.cflxymax[isea - 1] = c;
 }
 
 }  // namespace
@@ -283,6 +336,12 @@ void launch_wave_dzxy(const DzxyArgs& a, cudaStream_t s) {
 void launch_wave_distab(int nar1d, float dsie, float ecg0, float* ewn1, float* ecg1,
                         cudaStream_t s) {
   distab_kernel<<<1, 128, 0, s>>>(nar1d, dsie, ecg0, ewn1, ecg1);
+  WWB_CHECK(cudaGetLastError());
+}
+
+void launch_wave_cflxy(const CflxyArgs& a, cudaStream_t s) {
+  if (a.nsea > 0)
+    cflxy_kernel<<<blocks(a.nsea, 256), 256, 2 * a.nth * sizeof(float), s>>>(a);
   WWB_CHECK(cudaGetLastError());
 }
 
