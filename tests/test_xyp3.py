@@ -43,6 +43,7 @@ def test_reference_xyp3_runs(oracle, synth, maps):
 
 CASES = [
     dict(nx=48, ny=32, seed=1, iclose=2, flcur=True, flbpi=True),
+    dict(nx=203, ny=77, seed=5, iclose=2, flcur=True, flbpi=False, on_fraction=0.1),
     dict(nx=48, ny=32, seed=2, iclose=-1, flcur=False, flbpi=False),
     dict(nx=37, ny=29, seed=3, iclose=2, flcur=True, flbpi=True, on_fraction=0.5),
     dict(nx=60, ny=20, seed=4, iclose=-1, flcur=True, flbpi=True, dtg=3600.0),
@@ -96,3 +97,22 @@ def test_xyp3_validation(pkg, synth, maps):
     bad = dict(c)
     bad["rpar"] = c["rpar"][:4]
     assert pkg.xyp3_batch(bad)[0] == pkg.ERR_BAD_SHAPE
+
+
+@needs_ref
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [CASES[0], CASES[2], CASES[4]])
+def test_xyp3_list_sweeps_bitexact(pkg, oracle, synth, maps, case, monkeypatch):
+    """The sweeps as list kernels (WW_B200_XYP3_LISTS=1, one thread per MAPX2/MAPY2/MAPAXY
+    entry) and tiled in shared memory (the default) both give the reference's bits."""
+    if not cuda_available():
+        pytest.skip("needs a CUDA device")
+    c = synth.xyp3_case(ref=maps, **case)
+    rc_r, va_r = oracle.xyp3_call(oracle.ref_lib(), c)
+    monkeypatch.setenv("WW_B200_XYP3_LISTS", "1")
+    rc, va_l = pkg.xyp3_batch(c)
+    monkeypatch.delenv("WW_B200_XYP3_LISTS")
+    rc2, va_t = pkg.xyp3_batch(c)
+    assert rc_r == 0 and rc == 0 and rc2 == 0
+    assert_bitexact(va_l, va_r, "VA after W3XYP3, list sweeps")
+    assert_bitexact(va_t, va_r, "VA after W3XYP3, tiled sweeps")

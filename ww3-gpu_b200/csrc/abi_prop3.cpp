@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 #include <new>
 #include <vector>
@@ -256,6 +257,23 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
       mapstx[(1 - 2 * ny + j) + 2 * ny - 1] = a.mapsta[(nx - 2) * ny + j];
       mapstx[(nxy + 1 + j) + 2 * ny - 1] = a.mapsta[j];
     }
+  // The dense cell map of the tiled W3QCK3 sweeps (Xyp3Grid::cell_kind).
+  std::vector<unsigned char> kind(static_cast<size_t>(nxy), 0);
+  bool unique = true;
+  auto mark = [&](const int* m, int n0, int n1, int n2, int shift) {
+    for (int ip = 1; ip <= n2; ++ip) {
+      unsigned char& k = kind[m[ip - 1] - 1];
+      if ((k >> shift) & 3) unique = false;
+      k = static_cast<unsigned char>(k | ((ip <= n0 ? 1 : ip <= n1 ? 2 : 3) << shift));
+    }
+  };
+  mark(a.mapx2, g.nmx0, g.nmx1, g.nmx2, 0);
+  mark(a.mapy2, g.nmy0, g.nmy1, g.nmy2, 2);
+  for (int ip = 1; ip <= g.nact; ++ip) {
+    unsigned char& k = kind[a.mapaxy[ip - 1] - 1];
+    if (k & 16) unique = false;
+    k = static_cast<unsigned char>(k | 16);
+  }
   std::vector<int> list;
   for (int isp = 1; isp <= g.nspec; ++isp)
     if (a.on[isp - 1] != 0) list.push_back(isp);
@@ -290,6 +308,10 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
   g.cell_sea = st.in(slot++, cell_sea.data(), cell_sea.size(), s);
   g.sea_pos = st.in(slot++, sea_pos.data(), sea_pos.size(), s);
   g.bnd_last = st.in(slot++, bnd_last.data(), bnd_last.size(), s);
+  // WW_B200_XYP3_LISTS=1 runs the sweeps as list kernels (the same bits; for comparisons).
+  const char* lists = std::getenv("WW_B200_XYP3_LISTS");
+  const bool tiled = unique && !(lists != nullptr && std::strcmp(lists, "1") == 0);
+  g.cell_kind = tiled ? st.in(slot++, kind.data(), kind.size(), s) : nullptr;
   g.cg = st.in(slot++, a.cg, nk2 * (static_cast<size_t>(nsea) + 1), s);
   g.cx = st.in(slot++, a.cx, static_cast<size_t>(nsea) + 1, s);
   g.cy = st.in(slot++, a.cy, static_cast<size_t>(nsea) + 1, s);

@@ -18,8 +18,18 @@
 //  * The boundary restore, the global closure of the averaging and the x GSQRT that follow
 //    it are applied by the same thread to its own cell (the closure needs the ghost cell's
 //    gathered value, which the thread gathers as well).
-//  * W3QCK3's flux and propagation loops write one element per iteration; its closures copy
-//    whole rows; each is a kernel over (component, element).
+//  * W3QCK3's sweep is tiled in shared memory over the lon/lat grid: a CTA takes a tile of
+//    32 rows x 8 columns of one component, stages Q and the CFL numbers of the tile and of its
+//    halo (two cells up- and downstream along the sweep), computes the fluxes of the tile's
+//    faces and of the one upstream halo face, and writes the propagated Q of its active cells
+//    (and the unchanged Q of the others) into the component's second buffer; the buffers swap
+//    after the sweep. The reference's flux loop reads only the Q from before the sweep and its
+//    propagation loop writes each cell once, so reading one buffer and writing the other gives
+//    its bits; the one face a tile cannot see (the closed grid's face west of column 1, which
+//    is the face east of column NX) is computed from global memory. The faces and active cells
+//    come from a dense map of MAPX2/MAPY2/MAPAXY (Xyp3Grid::cell_kind); the list kernels
+//    (one thread per MAPX2/MAPY2/MAPAXY entry) remain for maps that name a cell twice.
+//    The closure copies whole rows (a kernel over rows).
 //  * The boundary update takes, for each boundary point, the value of the last IBI naming it
 //    (the serial loop's last write), found on the host once per call.
 // Arithmetic: the reference's per-element expressions and operand order (-fmad=false).
@@ -478,6 +488,147 @@ __global__ void qck3_prop_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int i
   }
 }
 
+// ---- W3QCK3 tiled in shared memory (the sweep's flux and propagation in one kernel) -------
+constexpr int kTileY = 32, kTileX = 8;  // core tile: 32 rows (IY, the fast index) x 8 columns
+
+/// The flux of one face of kind `kind` (Xyp3Grid::cell_kind) from the CFL numbers at the face's
+/// cell and the next one along the sweep (cf0, cf1) and Q at offsets -1, 0, 1, 2 along it (q4):
+/// prop_qck3.hpp:103-157 for interior faces (the UQ scheme), :162-186 for the boundary ones.
+/// Every expression as in qck3_flux_kernel, with IXYC, IXYU, IXYD as offsets from the face.
+__device__ __forceinline__ float qck3_face_flux(int kind, float cf0, float cf1, const float* q4) {
+  if (kind == 0) return 0.0f;
+  if (kind == 1) {
+    const float cfl = (cf1 + cf0) * 0.5f;
+    const float s = copysignf(1.1f, cfl);
+    const int oc = -fint(min_r(s, 0.0f));  // IXYC = IXY + OC*INC
+    const float c2 = cfl * cfl;
+    const float t1 = (1.0f - cfl) * q4[2];
+    const float t2 = (cfl + 1.0f) * q4[1];
+    const float h1 = (t1 + t2) * 0.5f;
+    const float h2 = (1.0f - c2) / 6.0f;
+    const float qixyc = q4[oc + 1];
+    const float d2 = (q4[oc] - qixyc * 2.0f) + q4[oc + 2];
+    const float qb = h1 - h2 * d2;
+    const int ou = oc - fint(s);
+    const int od = 2 * oc - ou;
+    const float qixyu = q4[ou + 1];
+    const float dq = q4[od + 1] - qixyu;
+    const float dqnz = copysignf(max_r(fabsf(dq), 1.E-15f), dq);
+    const float qcn = min_r(max_r((qixyc - qixyu) / dqnz, -0.1f), 1.1f);
+    const float qbn0 = max_r((qb - qixyu) / dqnz, qcn);
+    const float u = min_r(qcn / max_r(fabsf(cfl), 1.E-10f), 1.0f);
+    const float qbn = min_r(qbn0, u);
+    const float qbr = qixyu + qbn * dq;
+    const float cfac = static_cast<float>(fint(fabsf(qcn - 0.5f) * 2.0f));
+    const float qb2 = qixyc * cfac + (1.0f - cfac) * qbr;
+    return cfl * qb2;
+  }
+  const float cfl = kind == 2 ? cf0 : cf1;
+  const float s = copysignf(1.1f, cfl);
+  const int oc = -fint(min_r(s, 0.0f));
+  return q4[oc + 1] * cfl;
+}
+
+/// The flux of face IXY (1..NX*NY) read from global memory: the closed grid's face east of
+/// column NX, which the tile of column 1 needs as its face west of column 1.
+__device__ __forceinline__ float qck3_face_global(const Xyp3Grid& g, const float* q,
+                                                  const float* cfll, int ixy, int inc, int sh) {
+  const int kind = (g.cell_kind[ixy - 1] >> sh) & 3;
+  if (kind == 0) return 0.0f;
+  const int qoff = g.ny - 1;
+  const float q4[4] = {q[ixy - inc + qoff], q[ixy + qoff], q[ixy + inc + qoff],
+                       q[ixy + 2 * inc + qoff]};
+  return qck3_face_flux(kind, cfll[ixy - 1], cfll[ixy + inc - 1], q4);
+}
+
+/// One W3QCK3 sweep (X: along IX, INC = NY; else along IY, INC = 1) for one tile of one
+/// component: blockIdx.y the component, blockIdx.x the tile (row blocks fastest). The tiles
+/// cover Q's columns 0..NX+2 (the ghost columns are copied); k.q is read, k.a written.
+template <bool X>
+__global__ void __launch_bounds__(kTileY * kTileX)
+    qck3_tile_kernel(Xyp3Grid g, const Comp* comps, int itloc, Sweep w, int nty) {
+  constexpr int RY = kTileY + (X ? 0 : 4), RX = kTileX + (X ? 4 : 0);  // staged rows, columns
+  constexpr int OY = X ? 0 : 2, OX = X ? 2 : 0;  // local position of the first core cell
+  constexpr int SH = X ? 0 : 2;                  // the sweep's bits in cell_kind
+  __shared__ float qs[RX][RY];
+  __shared__ float cs[RX][RY];
+  __shared__ float fs[RX][RY];  // the flux of the face at each local cell
+  const Comp& k = comps[blockIdx.y];
+  if (itloc > k.ntloc) return;
+  const int ny = g.ny, nx = g.nx, nxy = nx * ny, qoff = ny - 1, inc = X ? ny : 1;
+  const long long nq = static_cast<long long>(ny) * (nx + 3), n1 = static_cast<long long>(ny) * (nx + 1);
+  const int iy0 = 1 + (blockIdx.x % nty) * kTileY;
+  const int ix0 = (blockIdx.x / nty) * kTileX;
+  const float* __restrict__ q = k.q;
+  const float* __restrict__ cfll = X ? k.vlcflx : k.vlcfly;
+  // Cell (r, c) of the staged block is IXY = (IX-1)*NY + IY with IY = IY0-OY+r, IX = IX0-OX+c,
+  // the reference's linear index (a row outside 1..NY is a cell of the next or previous column,
+  // as the linear offsets of the y sweep make it).
+  for (int i = threadIdx.x; i < RX * RY; i += blockDim.x) {
+    const int c = i / RY, r = i % RY;
+    const long long ixy = static_cast<long long>(ix0 - OX + c - 1) * ny + (iy0 - OY + r);
+    const long long qi = ixy + qoff;
+    qs[c][r] = (qi >= 0 && qi < nq) ? q[qi] : 0.0f;
+    cs[c][r] = (ixy >= 1 && ixy <= n1) ? cfll[ixy - 1] : 0.0f;
+  }
+  __syncthreads();
+  // The faces at the core cells and at the one upstream halo cell along the sweep.
+  constexpr int FR = X ? kTileY : kTileY + 1, FC = X ? kTileX + 1 : kTileX;
+  for (int i = threadIdx.x; i < FR * FC; i += blockDim.x) {
+    const int c = OX - (X ? 1 : 0) + i / FR, r = OY - (X ? 0 : 1) + i % FR;
+    const long long f = static_cast<long long>(ix0 - OX + c - 1) * ny + (iy0 - OY + r);
+    const int kind = (f >= 1 && f <= nxy) ? (g.cell_kind[f - 1] >> SH) & 3 : 0;
+    float flux = 0.0f;
+    if (kind != 0) {
+      float q4[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) q4[j] = X ? qs[c - 1 + j][r] : qs[c][r - 1 + j];
+      flux = qck3_face_flux(kind, cs[c][r], X ? cs[c + 1][r] : cs[c][r + 1], q4);
+    }
+    fs[c][r] = flux;
+  }
+  __syncthreads();
+  // The core cells: W3QCK3's propagation loop (prop_qck3.hpp:190-214) at the active ones.
+  const int r = threadIdx.x % kTileY, cc = threadIdx.x / kTileY;
+  const int iy = iy0 + r, ix = ix0 + cc;
+  if (iy > ny || ix > nx + 2) return;
+  const int lr = OY + r, lc = OX + cc;
+  const int ixy = (ix - 1) * ny + iy;
+  float v = qs[lc][lr];
+  if (ixy >= 1 && ixy <= nxy && (g.cell_kind[ixy - 1] & 16)) {
+    const int jm = ixy - inc;
+    const float fm = (w.close && jm <= 0) ? qck3_face_global(g, q, cfll, jm + nxy, inc, SH)
+                                          : fs[lc - (X ? 1 : 0)][lr - (X ? 0 : 1)];
+    const float fp = fs[lc][lr];
+    const int jn = (fm > 0.0f) ? -1 : 0;
+    const int jp = (fp < 0.0f) ? 1 : 0;
+    const float tt = v + fm * w.trans[static_cast<long>(jn + 1) * nxy + ixy - 1];
+    const float u = tt - fp * w.trans[static_cast<long>(jp + 1) * nxy + ixy - 1];
+    v = max_r(u, 0.0f);
+  }
+  k.a[ixy + qoff] = v;
+}
+
+/// The x sweep's closure part 1 (prop_qck3.hpp:87-112) alone, a row per thread: the tiled
+/// sweep needs no zeroed FLA.
+__global__ void qck3_closure_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc) {
+  const int ny = g.ny, nx = g.nx, my = ny, qoff = my - 1;
+  const long long n = static_cast<long long>(ncomp) * ny;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const Comp& k = comps[static_cast<int>(t / ny)];
+    if (itloc > k.ntloc) continue;
+    const int iy = static_cast<int>(t % ny) + 1;
+    float* q = k.q;
+    const int iad00 = -my, iad02 = my, iadn0 = iad00 + my * nx, iadn1 = my * nx,
+              iadn2 = iad02 + my * nx;
+    q[iy + iad00 + qoff] = q[iy + iadn0 + qoff];
+    q[iy + iadn1 + qoff] = q[iy + qoff];
+    q[iy + iadn2 + qoff] = q[iy + iad02 + qoff];
+    k.vlcflx[iy + iadn1 - 1] = k.vlcflx[iy - 1];
+  }
+}
+
 // ---- x 1/GSQRT (:1368-1373) and the boundary update (:1395-1415), per sea point -----------
 __global__ void finish_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc) {
   const long long n = static_cast<long long>(ncomp) * g.nsea;
@@ -683,6 +834,19 @@ void launch_xyp3_chunk(const Xyp3Grid& g, const Xyp3Chunk& ch, float* va, int nt
     const Sweep order[2] = {yfirst ? sy : sx, yfirst ? sx : sy};
     for (const Sweep& w : order) {
       if ((w.x && g.flcx == 0) || (!w.x && g.flcy == 0)) continue;
+      if (g.cell_kind != nullptr) {
+        if (w.close)
+          qck3_closure_kernel<<<blocks_for(static_cast<long long>(nc) * g.ny), kBlock, 0, s>>>(
+              g, nc, ch.comp, itloc);
+        const int nty = (g.ny + kTileY - 1) / kTileY, ntx = (g.nx + 3 + kTileX - 1) / kTileX;
+        const dim3 grid(static_cast<unsigned>(nty * ntx), static_cast<unsigned>(nc));
+        if (w.x)
+          qck3_tile_kernel<true><<<grid, kTileY * kTileX, 0, s>>>(g, ch.comp, itloc, w, nty);
+        else
+          qck3_tile_kernel<false><<<grid, kTileY * kTileX, 0, s>>>(g, ch.comp, itloc, w, nty);
+        swap_kernel<<<(nc + 127) / 128, 128, 0, s>>>(nc, ch.comp, itloc);
+        continue;
+      }
       qck3_zero_closure_kernel<<<blocks_for(nfla), kBlock, 0, s>>>(g, nc, ch.comp, itloc, w);
       if (w.nb2 > 0)
         qck3_flux_kernel<<<blocks_for(static_cast<long long>(nc) * w.nb2), kBlock, 0, s>>>(

@@ -34,6 +34,11 @@ struct Xyp3Grid {
   const int* cell_sea;              ///< ISEA of cell IXY (0 for land), NY*NX
   const int* sea_pos;               ///< position (1-based) of ISEA in MAPCXY, NSEA
   const int* bnd_last;              ///< IBI of the last ISBPI entry naming ISEA, or 0; NSEA
+  /// Per cell IXY (NY*NX), or null: bits 0-1 the kind of the x face at IXY in MAPX2 (0 none,
+  /// 1 interior, 2 boundary with the CFL at IXY, 3 boundary with the CFL at IXY+INC), bits 2-3
+  /// the same for MAPY2, bit 4 set when IXY is in MAPAXY. Null when a list names a cell twice:
+  /// the sweeps then run as list kernels.
+  const unsigned char* cell_kind;
   const float* cg;                  ///< (0:NK+1, 0:NSEA)
   const float* cx;                  ///< (0:NSEA)
   const float* cy;
