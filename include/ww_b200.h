@@ -104,6 +104,25 @@ int ww_snl1_enabled(void);
 /* Replaces ww_snl1_last_error (ww_kokkos_c.hpp:133). */
 int ww_snl1_last_error(void);
 
+/* B200 extension: the table builders of the GQM form of NL1 (INSNLGQM's helpers, w3snl1md.F90
+ * :1185-1500; the reference's host C++ snl1_couple.hpp, snl1_gauleg.hpp, snl1_f1f1f1.hpp, which
+ * it exports through no C entry), bit for bit as the reference computes them.
+ * ww_snl1_gqm_couple: COUPLE, the Webb four-wave coupling coefficient, in FP64 on the device for
+ * n quadruplets; k is (8, n) column-major (XK1, YK1, XK2, YK2, XK3, YK3, XK4, YK4 per column),
+ * coef (n) out, diag (n) out or NULL: bits 1/2 (term 1-3 is 0/0 / infinite) and 4/8 (term
+ * 1-4), the Fortran's warnings, the term left out. OK, NOT_INITIALISED, BAD_SHAPE, KERNEL.
+ * ww_snl1_gqm_gauleg: GAULEG on the host (the host's double cos), NPOIN-point Gauss-Legendre
+ * weights and abscissas on [-1, 1]; nothing written for npoin < 1. OK, BAD_SHAPE, KERNEL (a
+ * root whose Newton iteration does not converge in 1000 steps; the Fortran's has no limit).
+ * ww_snl1_gqm_f1f1f1: F1F1F1 on the host, the f1/f ratios of layout iq_om1 (1..7) into f1sf
+ * (NF1+1 entries; layout 4 sets *nf1 = 40); returns the Fortran's message bits (0 when NF1 fits
+ * the layout; 1, 2, 4, 8, 16 for layouts 1, 2, 3, 4, 7), or -BAD_SHAPE for a null pointer.
+ * Status of all three in ww_snl1_gqm_last_error(). */
+int ww_snl1_gqm_couple(int n, const double* k, double* coef, int* diag);
+int ww_snl1_gqm_gauleg(int npoin, double* w_leg, double* x_leg);
+int ww_snl1_gqm_f1f1f1(int* nf1, int iq_om1, double* f1sf);
+int ww_snl1_gqm_last_error(void);
+
 /* B200 extension. Selects the DIA kernel of grid `igrid`: 0 automatic (the pair kernel when
  * INSNL1's tables have the row-shift form and fit it, else the band kernel, else the row-shift
  * kernel, else the gather kernel; measured fastest in that order at 36x36 on B200), 1 the gather kernel over the

@@ -230,3 +230,29 @@ extern "C" int ref_w3cflxy(int nsea, int nx, int ny, int nk, int nth, int flcur,
   }
   return 0;
 }
+
+// The GQM table builders of the reference (kokkos/src/ww_kokkos/snl1_couple.hpp:37-88,
+// snl1_gauleg.hpp:28-61, snl1_f1f1f1.hpp:37-145), header-only, for the tests: COUPLE over n
+// quadruplets k (8, n) column-major; GAULEG; F1F1F1 (returns its diagnostic bits).
+#include "ww_kokkos/snl1_couple.hpp"
+#include "ww_kokkos/snl1_f1f1f1.hpp"
+#include "ww_kokkos/snl1_gauleg.hpp"
+
+extern "C" int ref_gqm_couple(int n, const double* k, double* coef, int* diag) {
+  for (int i = 0; i < n; ++i) {
+    const double* c = k + 8 * static_cast<size_t>(i);
+    int d = 0;
+    coef[i] = ww::snl1::couple(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], d);
+    diag[i] = d;
+  }
+  return 0;
+}
+
+extern "C" int ref_gqm_gauleg(int npoin, double* w_leg, double* x_leg) {
+  ww::snl1::gauleg(w_leg, x_leg, npoin);
+  return 0;
+}
+
+extern "C" int ref_gqm_f1f1f1(int* nf1, int iq_om1, double* f1sf) {
+  return ww::snl1::f1f1f1(f1sf, *nf1, iq_om1);
+}

@@ -52,7 +52,8 @@ EXPORTS = (
     "ww_step_run", "ww_step_free", "ww_step_ops", "ww_step_nodes", "ww_steps_run", "ww_outg_va", "ww_outg_part",
     "ww_outg_last_error", "ww_outg_device", "ww_wave_gath", "ww_wave_scat", "ww_wave_uwnd",
     "ww_wave_utrn", "ww_wave_dzxy", "ww_wave_map3", "ww_wave_mapt", "ww_wave_distab",
-    "ww_wave_cflxy",
+    "ww_wave_cflxy", "ww_snl1_gqm_couple", "ww_snl1_gqm_gauleg", "ww_snl1_gqm_f1f1f1",
+    "ww_snl1_gqm_last_error",
     "ww_mlp_create", "ww_mlp_destroy", "ww_mlp_param_count", "ww_mlp_set_params",
     "ww_mlp_get_params", "ww_mlp_get_grads", "ww_mlp_train_step", "ww_mlp_forward",
     "ww_mlp_gemm", "ww_mlp_last_error", "ww_sur_init", "ww_sur_synth", "ww_sur_dataset",
