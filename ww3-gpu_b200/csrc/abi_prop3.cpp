@@ -326,6 +326,11 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
   g.dsec_bpin = a.flbpi != 0 ? a.tscal[2] : 0.0f;
   g.dtg = a.dtg;
   if (g.flcur != 0) xyp3_current_range(g, s);
+  if (g.cell_kind != nullptr && ny >= 3) {  // the tiled averaging's source lists (grid only)
+    g.gather_order = static_cast<unsigned long long*>(
+        st.get(slot++, sizeof(unsigned long long) * static_cast<size_t>(ny) * (nx + 3)));
+    launch_xyp3_gather_order(g, s);
+  }
   float* d_va = nullptr;
   if (resident) {
     const int rc = va_device(igrid, a.va, nspec_va, nsealm, &d_va);
@@ -364,8 +369,9 @@ int xyp3_entry(int igrid, bool resident, const Xyp3Args& a, int nspec_va, int ns
     ch.fla = ch.vlcfly + n1 * chunk;
     ch.rdi = ch.fla + n1 * chunk;
     ch.iixy = reinterpret_cast<int*>(ch.rdi + 4 * static_cast<size_t>(nsea) * chunk);
+    ch.tcode = reinterpret_cast<unsigned*>(ch.iixy + 4 * static_cast<size_t>(nsea) * chunk);
     ch.comp = reinterpret_cast<Comp*>(
-        (reinterpret_cast<uintptr_t>(ch.iixy + 4 * static_cast<size_t>(nsea) * chunk) + 63) &
+        (reinterpret_cast<uintptr_t>(ch.tcode + static_cast<size_t>(nsea) * chunk) + 63) &
         ~static_cast<uintptr_t>(63));
     if (rec) {
       // The chunks share the work arrays (they run one after another); each keeps its own

@@ -55,6 +55,7 @@ struct Comp {
   float* fla;
   float* rdi;  ///< 4 x NSEA
   int* iixy;   ///< 4 x NSEA
+  unsigned* tcode;  ///< NSEA: 8 x 4 bits, the neighbour index j of each averaging statement
 };
 
 namespace {
@@ -156,6 +157,57 @@ __device__ __forceinline__ void corner(float dxcgc, float dycgc, int ny, int& ii
   }
 }
 
+// ---- the averaging's neighbourhood: T - D(j), j = 0..8 --------------------------------------
+/// D(j) of the nine cells an averaging statement of a sea point can reach (the order in which
+/// gather_cell lists candidate sources), as (DX, DY) with D = DX*NY + DY.
+__device__ __constant__ const signed char kNbDx[9] = {0, 0, 0, 1, -1, 1, 1, -1, -1};
+__device__ __constant__ const signed char kNbDy[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+
+/// j with D(j) = off, for off one of the nine (NY >= 3 keeps them distinct).
+__device__ __forceinline__ unsigned nb_index(int off, int ny) {
+  if (off == 0) return 0;
+  if (off == 1) return 1;
+  if (off == -1) return 2;
+  if (off == ny) return 3;
+  if (off == -ny) return 4;
+  if (off == ny + 1) return 5;
+  if (off == ny - 1) return 6;
+  if (off == -ny + 1) return 7;
+  return 8;
+}
+
+/// MAPSTX(j), j in 1-2NY .. NY*(NX+2).
+__device__ __forceinline__ int stx(const Xyp3Grid& g, int j) { return g.mapstx[j + 2 * g.ny - 1]; }
+
+/// The cells the eight averaging statements of sea point S (cell IXY = S) send their shares to,
+/// as nb_index codes in statement order (bits 4m..4m+3 for statement m): a central point
+/// +I1 +I2 +I3 +I4 -I1 -I2 -I3 -I4 (:1166-1180), a near-coast one +I1 -I1 +I2 -I2 +I3 -I3 +I4
+/// -I4 with a land target sent back to the centre (:1195-1270), as gather_cell replays them.
+__device__ __forceinline__ unsigned statement_codes(const Xyp3Grid& g, int S, bool central, int i1,
+                                                    int i2, int i3, int i4) {
+  const int ny = g.ny;
+  int t[8];
+  if (central) {
+    t[0] = i1; t[1] = i2; t[2] = i3; t[3] = i4;
+    t[4] = -i1; t[5] = -i2; t[6] = -i3; t[7] = -i4;
+  } else {
+    auto diag = [&](int i, int sgn) {
+      const int ixc = (ny ^ i) < 0 ? -ny : ny, iyc = i - ixc;
+      return (stx(g, S + sgn * i) >= 1 &&
+              !(stx(g, S + sgn * ixc) <= 0 && stx(g, S + sgn * iyc) <= 0))
+                 ? sgn * i
+                 : 0;
+    };
+    auto side = [&](int i, int sgn) { return stx(g, S + sgn * i) >= 1 ? sgn * i : 0; };
+    t[0] = diag(i1, 1); t[1] = diag(i1, -1); t[2] = side(i2, 1); t[3] = side(i2, -1);
+    t[4] = diag(i3, 1); t[5] = diag(i3, -1); t[6] = side(i4, 1); t[7] = side(i4, -1);
+  }
+  unsigned code = 0;
+#pragma unroll
+  for (int m = 0; m < 8; ++m) code |= nb_index(t[m], ny) << (4 * m);
+  return code;
+}
+
 /// W3GATH's value of component isp (the l-th listed) at sea point isea: VA under W3_SHRD, this
 /// rank's VA column or the received block of its owner under W3_MPI (prop3_shim.cpp:111-141).
 __device__ __forceinline__ float va_get(const Xyp3Grid& g, const float* __restrict__ va, int isea,
@@ -218,6 +270,9 @@ __global__ void sea_setup_kernel(Xyp3Grid g, int ncomp, int l0, Comp* comps,
     ii[g.nsea] = i2;
     ii[2 * g.nsea] = i3;
     ii[3 * g.nsea] = i4;
+    if (g.gather_order != nullptr)
+      k.tcode[isea - 1] =
+          statement_codes(g, ixy, g.sea_pos[isea - 1] <= g.ncent, i1, i2, i3, i4);
     // W3GATH then section 2.a (:1080-1137): this sea point's cell only.
     const float cgi = g.cg[isea * (g.nk + 2) + k.ik];
     const float v = va_get(g, va, isea, l0 + c, k.isp);
@@ -236,9 +291,6 @@ __global__ void sea_setup_kernel(Xyp3Grid g, int ncomp, int l0, Comp* comps,
 }
 
 // ---- section 3.a: the averaging as an ordered gather ---------------------------------------
-/// MAPSTX(j), j in 1-2NY .. NY*(NX+2).
-__device__ __forceinline__ int stx(const Xyp3Grid& g, int j) { return g.mapstx[j + 2 * g.ny - 1]; }
-
 /// VQ(T) after the averaging loops of one component, from AQ = a (section 3.a.1, 3.a.2).
 __device__ float gather_cell(const Xyp3Grid& g, const Comp& k, const float* __restrict__ a,
                              int T) {
@@ -367,6 +419,127 @@ __global__ void average_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itl
     }
     k.a[T + qoff] = v;
   }
+}
+
+/// The sources of every cell T in the averaging loop's order (Xyp3Grid::gather_order): the
+/// candidates of gather_cell, sorted by MAPCXY position. Depends on the grid only.
+__global__ void gather_order_kernel(Xyp3Grid g) {
+  const int ny = g.ny, nxy = g.nx * g.ny;
+  const long long nq = static_cast<long long>(ny) * (g.nx + 3);
+  const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (t >= nq) return;
+  const int T = static_cast<int>(t) + 1 - ny;
+  int pos[9], idx[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    const int S = T - (kNbDx[j] * ny + kNbDy[j]);
+    int p = INT_MAX;
+    if (S >= 1 && S <= nxy) {
+      const int isea = g.cell_sea[S - 1];
+      if (isea > 0) {
+        p = g.sea_pos[isea - 1];
+        if (p > g.ncent && g.mapsta[S - 1] <= 0) p = INT_MAX;  // skipped by the loop (:1191)
+      }
+    }
+    pos[j] = p;
+    idx[j] = j;
+  }
+  // Insertion sort by position (distinct for real sources).
+  for (int a = 1; a < 9; ++a)
+    for (int b = a; b > 0 && pos[b] < pos[b - 1]; --b) {
+      const int tp = pos[b]; pos[b] = pos[b - 1]; pos[b - 1] = tp;
+      const int ti = idx[b]; idx[b] = idx[b - 1]; idx[b - 1] = ti;
+    }
+  unsigned long long w = 0;
+  for (int m = 0; m < 9; ++m)
+    w |= static_cast<unsigned long long>(pos[m] == INT_MAX ? 0xFu : static_cast<unsigned>(idx[m]))
+         << (4 * m);
+  g.gather_order[t] = w;
+}
+
+/// Sections 3.a-3.b up to the sweeps as average_kernel, tiled in shared memory: a CTA takes
+/// 32 rows x 8 columns of one component's FIELD (columns 0..NX+2); each sea point of the tile
+/// and its one-cell halo computes its averaging shares once (the centre's and C1..C4, or its
+/// MAPTRN value), then each cell of the tile adds the shares that reach it, source by source in
+/// the loop's order (gather_order) and statement by statement (Comp::tcode), as gather_cell
+/// does. The global closure's far-column terms go through gather_cell.
+constexpr int kAvgY = 32, kAvgX = 8;
+__global__ void __launch_bounds__(kAvgY * kAvgX)
+    average_tile_kernel(Xyp3Grid g, const Comp* comps, int itloc, int nty) {
+  constexpr int RY = kAvgY + 2, RX = kAvgX + 2;
+  __shared__ float sh_c[5][RX][RY];  // the centre's share, C1..C4 (or AQ under MAPTRN)
+  __shared__ unsigned sh_code[RX][RY];
+  __shared__ unsigned char sh_flag[RX][RY];  // 1 MAPTRN, 2 central point
+  const Comp& k = comps[blockIdx.y];
+  if (itloc > k.ntloc) return;
+  const int ny = g.ny, nx = g.nx, nxy = nx * ny, nsea = g.nsea, qoff = ny - 1;
+  const int iy0 = 1 + (blockIdx.x % nty) * kAvgY, ix0 = (blockIdx.x / nty) * kAvgX;
+  const float* __restrict__ a = k.q;
+  for (int i = threadIdx.x; i < RX * RY; i += blockDim.x) {
+    const int c = i / RY, r = i % RY;
+    const long long S = static_cast<long long>(ix0 - 1 + c - 1) * ny + (iy0 - 1 + r);
+    if (S < 1 || S > nxy) continue;  // never a source (gather_order lists real cells only)
+    const int isea = g.cell_sea[S - 1];
+    if (isea <= 0) continue;
+    const float av = a[S + qoff];
+    if (g.maptrn[S - 1] != 0) {
+      sh_flag[c][r] = 1;
+      sh_c[0][c][r] = av;
+      continue;
+    }
+    const float cgi = g.cg[isea * (g.nk + 2) + k.ik];
+    const float* rd = k.rdi + (isea - 1);
+    const float rd1 = rd[0];
+    const float rd2 = min_r(rd[nsea] * cgi, 1.0f);
+    const float rd3 = rd[2 * nsea];
+    const float rd4 = min_r(cgi * rd[3 * nsea], 1.0f);
+    sh_c[0][c][r] = (((3.0f - rd2) - rd4) * av) / 3.0f;
+    sh_c[1][c][r] = ((rd2 * av) * rd1) / 6.0f;
+    sh_c[2][c][r] = (((1.0f - rd1) * av) * rd2) / 6.0f;
+    sh_c[3][c][r] = ((rd4 * av) * rd3) / 6.0f;
+    sh_c[4][c][r] = (((1.0f - rd3) * av) * rd4) / 6.0f;
+    sh_code[c][r] = k.tcode[isea - 1];
+    sh_flag[c][r] = g.sea_pos[isea - 1] <= g.ncent ? 2 : 0;
+  }
+  __syncthreads();
+  const int r = threadIdx.x % kAvgY, cc = threadIdx.x / kAvgY;
+  const int iy = iy0 + r, ix = ix0 + cc;
+  if (iy > ny || ix > nx + 2) return;
+  const int T = (ix - 1) * ny + iy;
+  const unsigned long long word = g.gather_order[T + qoff];
+  float acc = 0.0f;
+#pragma unroll 1
+  for (int m = 0; m < 9; ++m) {
+    const unsigned j = static_cast<unsigned>(word >> (4 * m)) & 0xFu;
+    if (j == 0xFu) break;
+    const int sc = cc + 1 - kNbDx[j], sr = r + 1 - kNbDy[j];
+    const unsigned f = sh_flag[sc][sr];
+    if (f & 1u) {  // MAPTRN: the centre is assigned (:1157-1158, :1192-1193)
+      if (j == 0) acc = sh_c[0][sc][sr];
+      continue;
+    }
+    if (j == 0) acc = acc + sh_c[0][sc][sr];
+    const unsigned code = sh_code[sc][sr];
+#pragma unroll
+    for (int st = 0; st < 8; ++st)
+      if (((code >> (4 * st)) & 0xFu) == j)
+        acc = acc + sh_c[1 + ((f & 2u) ? (st & 3) : (st >> 1))][sc][sr];
+  }
+  float v = acc;
+  if (T >= 1 && T <= nxy) {
+    if (g.mapsta[T - 1] == 2) v = a[T + qoff];
+    if (g.global) {
+      const int col = (T - 1) / ny + 1;
+      if (col == 1) v = v + gather_cell(g, k, a, T + nxy);
+      if (col == nx) v = v + gather_cell(g, k, a, T - nxy);
+    }
+    const int isea = g.cell_sea[T - 1];
+    if (isea > 0) {
+      const int sx = g.mapsf[isea - 1], sy = g.mapsf[g.nsea + isea - 1];
+      v = v * grid2(g.gsqrt, ny, sy, sx);
+    }
+  }
+  k.a[T + qoff] = v;
 }
 
 __global__ void comp_reset_kernel(int ncomp, Comp* comps, float* vq, float* aq, size_t nq) {
@@ -729,7 +902,12 @@ size_t xyp3_bytes_per_component(const Xyp3Grid& g) {
   const size_t nq = static_cast<size_t>(g.ny) * (g.nx + 3);
   const size_t n1 = static_cast<size_t>(g.ny) * (g.nx + 1);
   return sizeof(float) * (2 * nq + 3 * n1 + 4 * static_cast<size_t>(g.nsea)) +
-         sizeof(int) * 4 * static_cast<size_t>(g.nsea) + sizeof(Comp);
+         sizeof(int) * 5 * static_cast<size_t>(g.nsea) + sizeof(Comp);
+}
+
+void launch_xyp3_gather_order(const Xyp3Grid& g, cudaStream_t s) {
+  gather_order_kernel<<<blocks_for(static_cast<long long>(g.ny) * (g.nx + 3)), kBlock, 0, s>>>(g);
+  WWB_CHECK(cudaGetLastError());
 }
 
 void xyp3_current_range(Xyp3Grid& g, cudaStream_t s) {
@@ -794,6 +972,7 @@ int setup_xyp3_chunk(const Xyp3Grid& g, Xyp3Chunk& ch, cudaStream_t s) {
     hc[c].fla = ch.fla + c * n1;
     hc[c].rdi = ch.rdi + static_cast<size_t>(c) * 4 * g.nsea;
     hc[c].iixy = ch.iixy + static_cast<size_t>(c) * 4 * g.nsea;
+    hc[c].tcode = ch.tcode + static_cast<size_t>(c) * g.nsea;
   }
   WWB_CHECK(cudaMemcpyAsync(ch.comp, hc.data(), sizeof(Comp) * nc, cudaMemcpyHostToDevice, s));
   comp_setup_kernel<<<(nc + 127) / 128, 128, 0, s>>>(g, nc, ch.isp, ch.comp);
@@ -828,8 +1007,14 @@ void launch_xyp3_chunk(const Xyp3Grid& g, const Xyp3Chunk& ch, float* va, int nt
   const Sweep sy{1, 0, g.mapy2, g.nmy0, g.nmy1, g.nmy2, g.atrny, false};
   const long long nfla = static_cast<long long>(nc) * n1;
   for (int itloc = 1; itloc <= ntmax; ++itloc) {
-    average_kernel<<<blocks_for(static_cast<long long>(nc) * nq), kBlock, 0, s>>>(g, nc, ch.comp,
-                                                                                 itloc);
+    if (g.gather_order != nullptr) {
+      const int nty = (g.ny + kAvgY - 1) / kAvgY, ntx = (g.nx + 3 + kAvgX - 1) / kAvgX;
+      average_tile_kernel<<<dim3(static_cast<unsigned>(nty * ntx), static_cast<unsigned>(nc)),
+                            kAvgY * kAvgX, 0, s>>>(g, ch.comp, itloc, nty);
+    } else {
+      average_kernel<<<blocks_for(static_cast<long long>(nc) * nq), kBlock, 0, s>>>(
+          g, nc, ch.comp, itloc);
+    }
     swap_kernel<<<(nc + 127) / 128, 128, 0, s>>>(nc, ch.comp, itloc);
     const Sweep order[2] = {yfirst ? sy : sx, yfirst ? sx : sy};
     for (const Sweep& w : order) {

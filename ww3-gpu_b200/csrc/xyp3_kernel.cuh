@@ -39,6 +39,12 @@ struct Xyp3Grid {
   /// the same for MAPY2, bit 4 set when IXY is in MAPAXY. Null when a list names a cell twice:
   /// the sweeps then run as list kernels.
   const unsigned char* cell_kind;
+  /// Per cell T of FIELD (NY*(NX+3), T = 1-NY .. NY*(NX+2) at T+NY-1), or null: the sea points
+  /// whose averaging statements can reach T (T - D(j), D = 0, 1, -1, NY, -NY, NY+1, NY-1,
+  /// -NY+1, -NY-1), as 4-bit j in the averaging loop's order (their MAPCXY positions), 0xF
+  /// after the last; built once per call (launch_xyp3_gather_order). With it the averaging
+  /// runs tiled (average_tile_kernel); it needs cell_kind and NY >= 3.
+  unsigned long long* gather_order;
   const float* cg;                  ///< (0:NK+1, 0:NSEA)
   const float* cx;                  ///< (0:NSEA)
   const float* cy;
@@ -69,6 +75,7 @@ struct Xyp3Chunk {
   float* fla;         ///< ncomp x NY*(NX+1): FLA(1-NY : NY*NX)
   float* rdi;         ///< ncomp x 4 x NSEA
   int* iixy;          ///< ncomp x 4 x NSEA
+  unsigned* tcode;    ///< ncomp x NSEA: the cells of each point's 8 averaging statements
   struct Comp* comp;  ///< ncomp per-component constants (device)
 };
 
@@ -99,5 +106,8 @@ void launch_va_components(bool unpack, float* va, int nspec, int nsealm, const i
 /// MINVAL/MAXVAL of CX(1:NSEA), CY(1:NSEA) as gfortran evaluates them (NaN entries skipped,
 /// NaN when all are NaN, +-HUGE when empty), into g.cxmin .. g.cymax.
 void xyp3_current_range(Xyp3Grid& g, cudaStream_t s);
+
+/// Fills g.gather_order (allocated, NY*(NX+3) words) on stream s.
+void launch_xyp3_gather_order(const Xyp3Grid& g, cudaStream_t s);
 
 }  // namespace wwb
