@@ -278,3 +278,31 @@ def test_gated_host_entry_equals_device_entry(model, dia):
     assert model.fallback_count() == nrej
     assert_bitexact(hs.numpy(), s.cpu().numpy(), "host entry S")
     assert_bitexact(hd.numpy(), d.cpu().numpy(), "host entry D")
+
+
+def test_tma_output_epilogue_equals_row_epilogue(model, dia, monkeypatch):
+    """The output layer's two fused epilogues give the same S: tiles of four frequency rows
+    rotated in shared memory and stored by TMA (the default) and 256-column tiles stored row by
+    row (WW_B200_SUR_EPILOGUE=6). Two inference chunks, the last M tile partial."""
+    import torch
+
+    n = 70000
+    a, cg, kd = _inputs(model, n, seed=34)
+    model.gate(1e30, 1e30)
+    out = {}
+    for mode in ("6", None):
+        if mode:
+            monkeypatch.setenv("WW_B200_SUR_EPILOGUE", mode)
+        else:
+            monkeypatch.delenv("WW_B200_SUR_EPILOGUE", raising=False)
+        s = torch.full((n, 1296), float("nan"), device="cuda")
+        d = torch.full_like(s, float("nan"))
+        acc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        model.gated(n, a, cg, kd, s, d, acc)
+        torch.cuda.synchronize()
+        out[mode] = (s.cpu().numpy(), d.cpu().numpy(), acc.cpu().numpy())
+    s6, d6, acc6 = out["6"]
+    s7, d7, acc7 = out[None]
+    assert np.isfinite(s7).all()
+    assert_bitexact(s7, s6, "S, TMA-store epilogue vs row epilogue")
+    assert (d7 == 0).all() and (acc7 == acc6).all()

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -445,6 +446,15 @@ void sur_scratch(Sur& s, int rows) {
   }
 }
 
+/// Whether the output layer runs the TMA-store epilogue (kEpiSurOutTma): when the spectral grid
+/// suits it, unless WW_B200_SUR_EPILOGUE=6 asks for the row-by-row one (kEpiSurOut; the same
+/// S bits, for comparisons).
+bool sur_tma_epilogue(const Sur& s) {
+  const char* e = std::getenv("WW_B200_SUR_EPILOGUE");
+  if (e != nullptr && std::strcmp(e, "6") == 0) return false;
+  return sur_tma_ok(s.g.nk, s.g.nth);
+}
+
 /// One chunk (n <= kInferRows points) through the network with the fused output epilogue:
 /// S and D of every point, then the gate: rejected points listed in s.rej and counted in s.nrej
 /// (zeroed here), or, with `rej` given, appended as base + index to rej at the count *rej_n.
@@ -475,9 +485,23 @@ void sur_chunk_out(Sur& s, int n, const float* a, const float* cg, const float* 
   g.sur = SurOut{s.ps.p, s.shift.p, s.rowscale.p, so, dd, s.head.p, s.gsum.p, s.g.nspec,
                  s.g.nth, s.g.nk};
   const char* why = nullptr;
-  if (!sur_out_ok(g, &why)) throw CudaError(cudaErrorInvalidValue, why);
-  run_gemm(kEpiSurOut, g, make_operand(in, n, m.dh, m.dh, kBM),
-           make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, gemm_b_box(g)), st);
+  if (sur_tma_epilogue(s) && !g.pair) {
+    // Tiles of four frequency rows, each quarter rotated in shared memory and stored by TMA;
+    // N padded to whole tiles (B's rows past DOUT read as zeros).
+    g.bn = 4 * s.g.nth;
+    g.N = (m.dout + g.bn - 1) / g.bn * g.bn;
+    g.ldo = g.N;  // S goes through the store map; the row stride check is moot
+    g.b_rows = m.dout;
+    const CUtensorMap smap = make_store_map(so, n, s.g.nspec, g.bn);
+    g.store = &smap;
+    if (!sur_out_ok(g, &why)) throw CudaError(cudaErrorInvalidValue, why);
+    run_gemm(kEpiSurOutTma, g, make_operand(in, n, m.dh, m.dh, kBM),
+             make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, g.bn), st);
+  } else {
+    if (!sur_out_ok(g, &why)) throw CudaError(cudaErrorInvalidValue, why);
+    run_gemm(kEpiSurOut, g, make_operand(in, n, m.dh, m.dh, kBM),
+             make_operand(m.L[3].wb.p, m.dout, m.dh, m.dh, gemm_b_box(g)), st);
+  }
   if (rej == nullptr) {
     WWB_CHECK(cudaMemsetAsync(s.nrej.p, 0, sizeof(int), st));
     rej = s.rej.p;

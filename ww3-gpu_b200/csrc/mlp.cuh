@@ -36,6 +36,8 @@ enum Epilogue : int {
   kEpiDGelu = 4,      ///< g = acc * gelu'(aux): out = bf16(g), out_t = transpose
   kEpiAtomic = 5,     ///< out_f32 += acc (split reduction, red.global.add)
   kEpiSurOut = 6,     ///< the surrogate's output side: S and D of every row, gate sums (below)
+  kEpiSurOutTma = 7,  ///< kEpiSurOut with tiles of 4 frequency rows (bn = 4 NTH): each 32-row
+                      ///< quarter of a tile is rotated back in shared memory and stored by TMA
 };
 
 /// The original direction of canonical column j: the spectrum was rotated by the low 16 bits
@@ -83,6 +85,9 @@ struct GemmArgs {
   SurOut sur;           ///< kEpiSurOut only
   int pair;             ///< 1: two CTAs of a cluster share each 256-row tile (cta_group::2); B's
                         ///< tensor map then has boxes of bn / 2 rows (gemm_b_box)
+  int b_rows;           ///< kEpiSurOutTma: rows of B and entries of bias (N is padded past them;
+                        ///< the padding rows of B read as zeros)
+  const CUtensorMap* store;  ///< kEpiSurOutTma: host pointer to S's store map (make_store_map)
 };
 
 /// Rows of B's TMA box for this launch: bn, or bn / 2 when two CTAs share a tile.
@@ -98,6 +103,14 @@ Operand make_operand(const __nv_bfloat16* base, int rows, int k, int ld, int box
 
 /// Whether the shapes suit the kernel (tile multiples, alignment); on false `why` says what.
 bool gemm_shape_ok(const GemmArgs& g, const Operand& a, const Operand& b, const char** why);
+
+/// The TMA store map of kEpiSurOutTma: S as `rows` rows of `cols` f32 (row stride `cols`),
+/// written in boxes of 32 rows x `box_cols` columns.
+CUtensorMap make_store_map(float* s, int rows, int cols, int box_cols);
+
+/// Whether kEpiSurOutTma suits the surrogate's shape: bn = 4 NTH a multiple of 16 and at most
+/// 256, NSPEC a multiple of bn (the error head alone in the last tile).
+bool sur_tma_ok(int nk, int nth);
 
 /// Whether a launch of epilogue `mode` with tile width `bn` fits in shared memory.
 bool gemm_fits(int mode, int bn);

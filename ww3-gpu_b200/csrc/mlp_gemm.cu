@@ -65,11 +65,13 @@ constexpr size_t kStageBytes32 = kEpiWarps * 32 * kStageLd * sizeof(float);
 /// quarter, the groups' warps taking every (ew / 4)-th chunk): more where the registers allow,
 /// so the epilogue keeps up with the tensor cores.
 __host__ __device__ constexpr int epi_warps(int mode) {
-  return mode == 2 || mode == 6 ? 12 : 8;
+  return mode == 2 || mode == 6 || mode == 7 ? 12 : 8;
 }
 /// Pipeline stages of the single-CTA kernel per mode: the surrogate-output mode trades one for
 /// its larger epilogue staging.
-__host__ __device__ constexpr int stages_of(int mode) { return mode == 6 ? 3 : kStages; }
+__host__ __device__ constexpr int stages_of(int mode) {
+  return mode == 6 || mode == 7 ? 3 : kStages;
+}
 __host__ __device__ constexpr int epi_threads(int mode) { return 64 + 32 * epi_warps(mode); }
 // kEpiGeluInfer stages its bf16 chunk too: 32 rows of 16 words (+1 padding word), so the warp
 // stores rows of 64 contiguous bytes, eight lanes a row.
@@ -93,9 +95,16 @@ __host__ __device__ constexpr uint32_t stage_bytes(int bn) {
 
 /// Dynamic shared memory of a launch: alignment slack, the stages, the barriers' 256-byte slot
 /// and the epilogue's staging areas.
+/// kEpiSurOutTma's staging: the whole 128 x bn output tile (four 32-row quarters, each the
+/// dense box of one TMA store).
+__host__ __device__ constexpr size_t sur_tma_stage_bytes(int bn) {
+  return static_cast<size_t>(kBM) * bn * sizeof(float);
+}
+
 __host__ __device__ constexpr size_t smem_bytes(int mode, int bn) {
   return 1024 + stages_of(mode) * static_cast<size_t>(stage_bytes(bn)) + 256 +
-         stage_bytes_w(mode, epi_warps(mode)) + (bias_in_smem(mode) ? kBiasBytes : 0);
+         (mode == 7 ? sur_tma_stage_bytes(bn) : stage_bytes_w(mode, epi_warps(mode))) +
+         (bias_in_smem(mode) ? kBiasBytes : 0);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -168,6 +177,87 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
           smem_u32(bar))
       : "memory");
+}
+
+// ---- kEpiSurOutTma: named barriers per TMEM lane quarter, 16-column TMEM loads, TMA stores ----
+/// bar.sync on barrier `id` for `n` threads (the three epilogue warps of one lane quarter).
+__device__ __forceinline__ void named_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+/// bar.red.and over barrier `id` for `n` threads: true when v is true in every one of them.
+__device__ __forceinline__ bool named_and(int id, int n, bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, %2, %3, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(out)
+      : "r"(v ? 1u : 0u), "r"(id), "r"(n)
+      : "memory");
+  return out != 0;
+}
+/// tcgen05.ld of 16 columns and its wait.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+}
+/// tcgen05.ld of 16 columns without waiting (tmem_wait48 before use).
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+/// Waits for this thread's tcgen05.ld of three 16-column chunks, tied to their registers.
+__device__ __forceinline__ void tmem_wait48(uint32_t (&a)[16], uint32_t (&b)[16],
+                                            uint32_t (&c)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]),
+                 "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]),
+                 "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15]), "+r"(b[0]), "+r"(b[1]),
+                 "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7]),
+                 "+r"(b[8]), "+r"(b[9]), "+r"(b[10]), "+r"(b[11]), "+r"(b[12]), "+r"(b[13]),
+                 "+r"(b[14]), "+r"(b[15]), "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3]),
+                 "+r"(c[4]), "+r"(c[5]), "+r"(c[6]), "+r"(c[7]), "+r"(c[8]), "+r"(c[9]),
+                 "+r"(c[10]), "+r"(c[11]), "+r"(c[12]), "+r"(c[13]), "+r"(c[14]), "+r"(c[15])
+               :
+               : "memory");
+}
+/// Generic-proxy writes to shared memory made visible to the TMA engine.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+/// TMA store of a box from shared memory to (x, y) of `map`; completion tracked per bulk group.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x,
+                                             int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+/// Until this thread's stores have read their shared memory (the staging is free again).
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+/// Until this thread's stores are complete.
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 /// tcgen05.ld of 32 columns without waiting: the registers are valid after tmem_wait32 on them.
@@ -441,6 +531,120 @@ __device__ __forceinline__ void sur_chunk(const GemmArgs& g, int m_base, int n, 
   __syncwarp();
 }
 
+/// kEpiSurOutTma's per-row inputs of one tile, loaded before the tile's accumulator is ready.
+struct SurTmaRow {
+  float lam[4], wt[4], rs[4], bias[3];
+  int shift;
+};
+__device__ __forceinline__ SurTmaRow sur_tma_row(const GemmArgs& g, int m_base, int n_base, int q,
+                                                 int hf, int lane) {
+  const SurOut& o = g.sur;
+  SurTmaRow x;
+  const int m = m_base + q * 32 + lane;
+  const bool in = m < g.M && n_base < o.nspec;
+  const int k0 = n_base / o.nth;
+  const float* pp = o.ps + static_cast<size_t>(m < g.M ? m : 0) * 2 * o.nk;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    x.lam[t] = in ? pp[k0 + t] : 0.0f;
+    x.wt[t] = in ? pp[o.nk + k0 + t] : 0.0f;
+    x.rs[t] = in ? __ldg(o.rowscale + k0 + t) : 0.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int c0 = 16 * (hf + 3 * i);
+    x.bias[i] = (lane < 16 && n_base < o.nspec && c0 < g.bn) ? __ldg(g.bias + n_base + c0 + lane)
+                                                             : 0.0f;
+  }
+  x.shift = m < g.M ? __ldg(o.shift + m) : 0;
+  return x;
+}
+
+/// One 16-column chunk of kEpiSurOutTma (tile columns c0..c0+15): bias, scale, gate sums, and
+/// the rotated write into the thread's row of the staging box.
+__device__ __forceinline__ void sur_tma_chunk(const uint32_t (&r)[16], int c0, int nth, float bl,
+                                              const float (&sk)[4], const float (&wk)[4],
+                                              int shift, float* srow, float& racc, float& gacc) {
+  const int kk0 = c0 / nth;             // the chunk's first frequency row in the tile (0..3)
+  const int jb = (kk0 + 1) * nth - c0;  // first column of the next frequency row
+  const int jl0 = c0 - kk0 * nth;
+  const float sa = kk0 == 0 ? sk[0] : kk0 == 1 ? sk[1] : kk0 == 2 ? sk[2] : sk[3];
+  const float wa = kk0 == 0 ? wk[0] : kk0 == 1 ? wk[1] : kk0 == 2 ? wk[2] : wk[3];
+  const float sb = kk0 == 0 ? sk[1] : kk0 == 1 ? sk[2] : kk0 == 2 ? sk[3] : 0.0f;
+  const float wb = kk0 == 0 ? wk[1] : kk0 == 1 ? wk[2] : kk0 == 2 ? wk[3] : 0.0f;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const float v = __uint_as_float(r[j]) + __shfl_sync(0xffffffffu, bl, j);
+    const bool second = j >= jb;
+    const float s = second ? sb : sa, w = second ? wb : wa;
+    racc += w * v;
+    gacc += w * fabsf(v);
+    const int kk = second ? kk0 + 1 : kk0;
+    const int jl = second ? jl0 + j - nth : jl0 + j;
+    srow[kk * nth + orig_col(shift, jl, nth)] = v * s;
+  }
+}
+
+/// kEpiSurOutTma for one tile (128 rows x bn = 4 NTH columns, frequency rows k0..k0+3) by the
+/// three warps of TMEM lane quarter q (warp hf of them takes the 16-column chunks hf, hf+3 and
+/// hf+6, loaded together): each thread (row m) adds the bias, scales its values into S's units
+/// and writes them, rotated back to their directions (a permutation within each frequency row),
+/// into the quarter's staging box; then one thread stores the 32 x bn box with TMA. The values
+/// and the gate sums are those of kEpiSurOut (sur_chunk): the same expressions on the same
+/// accumulator. The tile past NSPEC holds the error head in its first column, stored to head[m].
+__device__ __forceinline__ void sur_tma_tile(const GemmArgs& g, const CUtensorMap* tc, int m_base,
+                                             int n_base, uint32_t tbase, int q, int hf, int lane,
+                                             float* stq, const SurTmaRow& x) {
+  const SurOut& o = g.sur;
+  const int nth = o.nth, bn = g.bn;
+  const int m = m_base + q * 32 + lane;
+  if (n_base >= o.nspec) {
+    if (hf == 0) {
+      uint32_t r[16];
+      tmem_ld16(tbase, r);
+      const float v = __uint_as_float(r[0]) + __ldg(g.bias + o.nspec);
+      if (m < g.M && o.head) o.head[m] = v;
+    }
+    return;
+  }
+  float sk[4], wk[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    sk[t] = x.rs[t] * __expf(x.lam[t]);
+    wk[t] = x.rs[t] * x.wt[t];
+  }
+  float racc = 0.0f, gacc = 0.0f;
+  float* const srow = stq + lane * bn;
+  const int nch = bn / 16;
+  if (hf + 6 < nch) {  // three chunks (bn = 144: every warp)
+    uint32_t r0[16], r1[16], r2[16];
+    tmem_ld16_async(tbase + 16u * hf, r0);
+    tmem_ld16_async(tbase + 16u * (hf + 3), r1);
+    tmem_ld16_async(tbase + 16u * (hf + 6), r2);
+    tmem_wait48(r0, r1, r2);
+    sur_tma_chunk(r0, 16 * hf, nth, x.bias[0], sk, wk, x.shift, srow, racc, gacc);
+    sur_tma_chunk(r1, 16 * (hf + 3), nth, x.bias[1], sk, wk, x.shift, srow, racc, gacc);
+    sur_tma_chunk(r2, 16 * (hf + 6), nth, x.bias[2], sk, wk, x.shift, srow, racc, gacc);
+  } else {
+    for (int i = 0, c = hf; c < nch; ++i, c += 3) {
+      uint32_t r[16];
+      tmem_ld16(tbase + 16u * c, r);
+      const float bl = i == 0 ? x.bias[0] : i == 1 ? x.bias[1] : x.bias[2];
+      sur_tma_chunk(r, 16 * c, nth, bl, sk, wk, x.shift, srow, racc, gacc);
+    }
+  }
+  fence_proxy_async_smem();
+  named_sync(1 + q, 96);
+  if (hf == 0 && lane == 0 && m_base + q * 32 < g.M) {
+    tma_store_2d(tc, stq, n_base, m_base + q * 32);
+    bulk_commit();
+  }
+  if (m < g.M) {
+    atomicAdd(o.gsum + 2 * m, racc);
+    atomicAdd(o.gsum + 2 * m + 1, gacc);
+  }
+}
+
 /// The epilogue of one accumulator tile by one warp: TMEM lanes q*32.. (tile rows m_base +
 /// q*32 + lane), its chunks half, half + 2, ... of the tile's bn columns from n_base.
 /// Calls body(c, r) for chunks c = c0, c0 + 2, ... < nchunks with r the chunk's 32 TMEM
@@ -536,7 +740,7 @@ __device__ __forceinline__ Unit decode(int u, int m_tiles, int n_tiles) {
 template <int MODE>
 __global__ void __launch_bounds__(epi_threads(MODE), 1)
     gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
-                const GemmArgs g) {
+                const __grid_constant__ CUtensorMap tc, const GemmArgs g) {
   extern __shared__ uint8_t smem_raw[];
   // The 1024-byte aligned base as an offset into the shared array (not through an integer
   // cast), so the compiler keeps every derived pointer in the shared space (LDS/STS).
@@ -571,8 +775,9 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   // The bias vector after the epilogue staging (the modes that read it from shared memory).
-  float* const bias_s = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256 +
-                                                 stage_bytes_w(MODE, epi_warps(MODE)));
+  float* const bias_s = reinterpret_cast<float*>(
+      reinterpret_cast<uint8_t*>(bars) + 256 +
+      (MODE == kEpiSurOutTma ? sur_tma_stage_bytes(g.bn) : stage_bytes_w(MODE, epi_warps(MODE))));
   if constexpr (bias_in_smem(MODE))
     for (int i = threadIdx.x; i < g.N; i += blockDim.x) bias_s[i] = __ldg(g.bias + i);
   tc_fence_before();
@@ -664,23 +869,41 @@ __global__ void __launch_bounds__(epi_threads(MODE), 1)
                         static_cast<size_t>(ew) * 32 * kRowsPerTile * 2;
     uint32_t local = 0;
     bool ok = true;
+    // kEpiSurOutTma: the quarter's staging box, and its store issuer (first warp, lane 0).
+    float* const stq = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(bars) + 256) +
+                       static_cast<size_t>(q) * 32 * g.bn;
+    const bool issuer = MODE == kEpiSurOutTma && half == 0 && lane == 0;
     for (int u = blockIdx.x; u < units; u += gridDim.x, ++local) {
       const Unit w = decode(u, m_tiles, n_tiles);
       const uint32_t b = local & 1u, tph = (local >> 1) & 1u;
+      // kEpiSurOutTma: the tile's row inputs are loaded while its accumulator is computed.
+      SurTmaRow xr;
+      if constexpr (MODE == kEpiSurOutTma) xr = sur_tma_row(g, w.mt * kBM, w.nt * g.bn, q, half, lane);
       // Warp-uniform decision: tcgen05.ld below is a warp-wide (.sync.aligned) instruction.
-      if (!__all_sync(0xffffffffu, mbar_wait(&bars->tfull[b], tph))) {
+      bool okw = __all_sync(0xffffffffu, mbar_wait(&bars->tfull[b], tph));
+      if constexpr (MODE == kEpiSurOutTma) {
+        // The quarter's three warps decide together (they share named barriers), and the
+        // staging box is free once the previous tile's store has read it.
+        if (issuer) bulk_wait_read();
+        okw = named_and(1 + q, 96, okw);
+      }
+      if (!okw) {
         ok = false;
         break;
       }
       tc_fence_after();
       const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16) + b * kBNMax;
-      epilogue_tile<MODE>(g, w.mt * kBM, w.nt * g.bn, tbase, q, half, EW / 4, lane, tile, rowc,
-                          bias_s);
+      if constexpr (MODE == kEpiSurOutTma)
+        sur_tma_tile(g, &tc, w.mt * kBM, w.nt * g.bn, tbase, q, half, lane, stq, xr);
+      else
+        epilogue_tile<MODE>(g, w.mt * kBM, w.nt * g.bn, tbase, q, half, EW / 4, lane, tile,
+                            rowc, bias_s);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bars->tempty[b]);
     }
     if (!ok && lane == 0) atomicExch(g.err, 1);
+    if (issuer) bulk_wait_all();  // the tiles' stores are complete before the CTA exits
   }
 
   tc_fence_before();
@@ -976,7 +1199,8 @@ void launch(const GemmArgs& g, const Operand& a, const Operand& b, cudaStream_t 
   if (sms <= 0) WWB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
   int grid = max_ctas > 0 ? max_ctas : sms;
   if (grid > units) grid = units;
-  gemm_kernel<MODE><<<grid, epi_threads(MODE), smem, stream>>>(a.map, b.map, g);
+  const CUtensorMap& tc = (MODE == kEpiSurOutTma && g.store) ? *g.store : a.map;
+  gemm_kernel<MODE><<<grid, epi_threads(MODE), smem, stream>>>(a.map, b.map, tc, g);
   WWB_CHECK(cudaGetLastError());
 }
 
@@ -1030,11 +1254,18 @@ bool gemm_shape_ok(const GemmArgs& g, const Operand& a, const Operand& b, const 
     return false;
   };
   if (g.M <= 0 || g.N <= 0 || g.K <= 0) return no("empty GEMM");
-  if (g.bn != 64 && g.bn != 128 && g.bn != 192 && g.bn != 256) return no("tile width not 64/128/192/256");
+  if (g.b_rows > 0) {  // kEpiSurOutTma: tiles of 4 NTH columns, B padded by the TMA unit
+    if (g.bn % 16 || g.bn < 16 || g.bn > 256) return no("tile width not a multiple of 16 to 256");
+    if (b.rows != g.b_rows || g.b_rows > g.N) return no("B rows differ from the declared count");
+  } else {
+    if (g.bn != 64 && g.bn != 128 && g.bn != 192 && g.bn != 256)
+      return no("tile width not 64/128/192/256");
+    if (b.rows < g.N) return no("operand has fewer rows than the output");
+  }
   if (g.N % g.bn) return no("N not a multiple of the tile width");
   if (g.K % kBK) return no("K not a multiple of 64");
   if (a.k != g.K || b.k != g.K) return no("operand reduction length differs from K");
-  if (a.rows < g.M || b.rows < g.N) return no("operand has fewer rows than the output");
+  if (a.rows < g.M) return no("operand has fewer rows than the output");
   if (g.splits < 1 || (g.K / kBK) % g.splits) return no("split does not divide the K blocks");
   if (g.ldo % 8 || g.ldo < g.N) return no("output row stride not a multiple of 8 or below N");
   if (g.out_t && g.ldt < g.M) return no("transposed row stride below M");
@@ -1043,6 +1274,26 @@ bool gemm_shape_ok(const GemmArgs& g, const Operand& a, const Operand& b, const 
   if (g.pair && (g.splits != 1 || g.out_t != nullptr))
     return no("paired tiles only for the inference epilogues");
   return true;
+}
+
+CUtensorMap make_store_map(float* base, int rows, int cols, int box_cols) {
+  CUtensorMap map{};
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 4};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(box_cols), 32u};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_tiled()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims,
+                                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError(cudaErrorInvalidValue, "cuTensorMapEncodeTiled (S)");
+  return map;
+}
+
+bool sur_tma_ok(int nk, int nth) {
+  const int bn = 4 * nth;
+  return nth >= 4 && bn % 16 == 0 && bn <= 256 && (nk * nth) % bn == 0 &&
+         smem_bytes(kEpiSurOutTma, bn) <= kSmemMax;
 }
 
 bool gemm_fits(int mode, int bn) { return smem_bytes(mode, bn) <= kSmemMax; }
@@ -1081,6 +1332,11 @@ void gemm(int mode, const GemmArgs& g, const Operand& a, const Operand& b, cudaS
     case kEpiDGelu: launch<kEpiDGelu>(g, a, b, stream, max_ctas); break;
     case kEpiAtomic: launch<kEpiAtomic>(g, a, b, stream, max_ctas); break;
     case kEpiSurOut: launch<kEpiSurOut>(g, a, b, stream, max_ctas); break;
+    case kEpiSurOutTma:
+      if (g.store == nullptr || g.pair)
+        throw CudaError(cudaErrorInvalidValue, "GEMM: the TMA output epilogue needs S's store map");
+      launch<kEpiSurOutTma>(g, a, b, stream, max_ctas);
+      break;
     default: throw CudaError(cudaErrorInvalidValue, "unknown GEMM epilogue");
   }
 }
