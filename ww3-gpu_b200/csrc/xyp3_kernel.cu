@@ -661,6 +661,30 @@ __global__ void qck3_prop_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int i
   }
 }
 
+// ---- x 1/GSQRT (:1368-1373) and the boundary update (:1395-1415), per sea point -----------
+/// The value of sea point isea (cell ixy) after the sub-step's sweeps: the boundary input
+/// interpolated in time where the point takes one (the last IBI naming it), else v / GSQRT.
+__device__ __forceinline__ float finish_value(const Xyp3Grid& g, const Comp& k, int itloc,
+                                              int isea, int ixy, float v) {
+  const int ibi = g.flbpi ? g.bnd_last[isea - 1] : 0;
+  if (ibi > 0) {
+    float rd1 = g.dsec_bpi0 - ((g.dtg * static_cast<float>(k.ntloc - itloc)) / k.rntloc);
+    float rd2 = g.dsec_bpin;
+    if (rd2 > 0.001f) {
+      const float qq = rd1 / rd2;
+      rd2 = min_r(max_r(qq, 0.0f), 1.0f);
+      rd1 = 1.0f - rd2;
+    } else {
+      rd1 = 0.0f;
+      rd2 = 1.0f;
+    }
+    const float b0 = g.bbpi0[static_cast<size_t>(ibi) * g.nspec + k.isp - 1];
+    const float bn = g.bbpin[static_cast<size_t>(ibi) * g.nspec + k.isp - 1];
+    return (((b0 * rd1) + (bn * rd2)) / g.cg[isea * (g.nk + 2) + k.ik]) * g.clats[isea];
+  }
+  return v / g.gsqrt[ixy - 1];
+}
+
 // ---- W3QCK3 tiled in shared memory (the sweep's flux and propagation in one kernel) -------
 constexpr int kTileY = 32, kTileX = 8;  // core tile: 32 rows (IY, the fast index) x 8 columns
 
@@ -719,7 +743,7 @@ __device__ __forceinline__ float qck3_face_global(const Xyp3Grid& g, const float
 /// cover Q's columns 0..NX+2 (the ghost columns are copied); k.q is read, k.a written.
 template <bool X>
 __global__ void __launch_bounds__(kTileY * kTileX)
-    qck3_tile_kernel(Xyp3Grid g, const Comp* comps, int itloc, Sweep w, int nty) {
+    qck3_tile_kernel(Xyp3Grid g, const Comp* comps, int itloc, Sweep w, int nty, int fin) {
   constexpr int RY = kTileY + (X ? 0 : 4), RX = kTileX + (X ? 4 : 0);  // staged rows, columns
   constexpr int OY = X ? 0 : 2, OX = X ? 2 : 0;  // local position of the first core cell
   constexpr int SH = X ? 0 : 2;                  // the sweep's bits in cell_kind
@@ -779,6 +803,10 @@ __global__ void __launch_bounds__(kTileY * kTileX)
     const float u = tt - fp * w.trans[static_cast<long>(jp + 1) * nxy + ixy - 1];
     v = max_r(u, 0.0f);
   }
+  if (fin && ixy >= 1 && ixy <= nxy) {  // the sub-step's last sweep: finish_kernel's step here
+    const int isea = g.cell_sea[ixy - 1];
+    if (isea > 0) v = finish_value(g, k, itloc, isea, ixy, v);
+  }
   k.a[ixy + qoff] = v;
 }
 
@@ -802,7 +830,7 @@ __global__ void qck3_closure_kernel(Xyp3Grid g, int ncomp, const Comp* comps, in
   }
 }
 
-// ---- x 1/GSQRT (:1368-1373) and the boundary update (:1395-1415), per sea point -----------
+// ---- finish_value per sea point, when no tiled sweep took it -------------------------------
 __global__ void finish_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itloc) {
   const long long n = static_cast<long long>(ncomp) * g.nsea;
   const int qoff = g.ny - 1;
@@ -812,27 +840,8 @@ __global__ void finish_kernel(Xyp3Grid g, int ncomp, const Comp* comps, int itlo
     const Comp& k = comps[c];
     if (itloc > k.ntloc) continue;
     const int isea = 1 + static_cast<int>(t % g.nsea);
-    const int ix = g.mapsf[isea - 1], iy = g.mapsf[g.nsea + isea - 1];
     const int ixy = g.mapsf[2 * g.nsea + isea - 1];
-    const int ibi = g.flbpi ? g.bnd_last[isea - 1] : 0;
-    if (ibi > 0) {
-      float rd1 = g.dsec_bpi0 - ((g.dtg * static_cast<float>(k.ntloc - itloc)) / k.rntloc);
-      float rd2 = g.dsec_bpin;
-      if (rd2 > 0.001f) {
-        const float qq = rd1 / rd2;
-        rd2 = min_r(max_r(qq, 0.0f), 1.0f);
-        rd1 = 1.0f - rd2;
-      } else {
-        rd1 = 0.0f;
-        rd2 = 1.0f;
-      }
-      const float b0 = g.bbpi0[static_cast<size_t>(ibi) * g.nspec + k.isp - 1];
-      const float bn = g.bbpin[static_cast<size_t>(ibi) * g.nspec + k.isp - 1];
-      k.q[ixy + qoff] = (((b0 * rd1) + (bn * rd2)) / g.cg[isea * (g.nk + 2) + k.ik]) *
-                        g.clats[isea];
-    } else {
-      k.q[ixy + qoff] = k.q[ixy + qoff] / grid2(g.gsqrt, g.ny, iy, ix);
-    }
+    k.q[ixy + qoff] = finish_value(g, k, itloc, isea, ixy, k.q[ixy + qoff]);
   }
 }
 
@@ -1017,18 +1026,24 @@ void launch_xyp3_chunk(const Xyp3Grid& g, const Xyp3Chunk& ch, float* va, int nt
     }
     swap_kernel<<<(nc + 127) / 128, 128, 0, s>>>(nc, ch.comp, itloc);
     const Sweep order[2] = {yfirst ? sy : sx, yfirst ? sx : sy};
-    for (const Sweep& w : order) {
-      if ((w.x && g.flcx == 0) || (!w.x && g.flcy == 0)) continue;
+    auto runs = [&](const Sweep& w) { return w.x ? g.flcx != 0 : g.flcy != 0; };
+    // The tiled path applies finish_value in the sub-step's last sweep.
+    const int last = runs(order[1]) ? 1 : runs(order[0]) ? 0 : -1;
+    const bool fused_finish = g.cell_kind != nullptr && last >= 0;
+    for (int o = 0; o < 2; ++o) {
+      const Sweep& w = order[o];
+      if (!runs(w)) continue;
       if (g.cell_kind != nullptr) {
         if (w.close)
           qck3_closure_kernel<<<blocks_for(static_cast<long long>(nc) * g.ny), kBlock, 0, s>>>(
               g, nc, ch.comp, itloc);
         const int nty = (g.ny + kTileY - 1) / kTileY, ntx = (g.nx + 3 + kTileX - 1) / kTileX;
         const dim3 grid(static_cast<unsigned>(nty * ntx), static_cast<unsigned>(nc));
+        const int fin = o == last ? 1 : 0;
         if (w.x)
-          qck3_tile_kernel<true><<<grid, kTileY * kTileX, 0, s>>>(g, ch.comp, itloc, w, nty);
+          qck3_tile_kernel<true><<<grid, kTileY * kTileX, 0, s>>>(g, ch.comp, itloc, w, nty, fin);
         else
-          qck3_tile_kernel<false><<<grid, kTileY * kTileX, 0, s>>>(g, ch.comp, itloc, w, nty);
+          qck3_tile_kernel<false><<<grid, kTileY * kTileX, 0, s>>>(g, ch.comp, itloc, w, nty, fin);
         swap_kernel<<<(nc + 127) / 128, 128, 0, s>>>(nc, ch.comp, itloc);
         continue;
       }
@@ -1040,7 +1055,8 @@ void launch_xyp3_chunk(const Xyp3Grid& g, const Xyp3Chunk& ch, float* va, int nt
         qck3_prop_kernel<<<blocks_for(static_cast<long long>(nc) * g.nact), kBlock, 0, s>>>(
             g, nc, ch.comp, itloc, w);
     }
-    finish_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, itloc);
+    if (!fused_finish)
+      finish_kernel<<<blocks_for(nsea_c), kBlock, 0, s>>>(g, nc, ch.comp, itloc);
     WWB_CHECK(cudaGetLastError());
     yfirst = !yfirst;
   }
