@@ -1647,9 +1647,15 @@ def run_b200_surrogate(args):
         "error_vs_fp64": err_gated,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": int((h_a.numel() + h_cg.numel() + h_kd.numel()) * 4),
-                "d2h_bytes_per_step": int((h_s.numel() + h_d.numel()) * 4),
+                # S whole; of D only each chunk's packed rejected rows (8,192-row slot, its
+                # index list and count): the accepted points' D is zero and the entry clears it
+                # on the host while the device works (a chunk rejecting more than 8,192 points
+                # would bring its whole D; none did when this line was measured)
+                "d2h_bytes_per_step": int(h_s.numel() * 4 + chunks * (4 + 8192 * 4 +
+                                                                      8192 * 1296 * 4)),
                 "steps": e2e_steps, "host_entry": "ww_snl1_gated_host (page-locked host buffers; copies "
-                                                  "pipelined with the compute in 65,536-point chunks)",
+                                                  "pipelined with the compute in 65,536-point chunks; "
+                                                  "D cleared on the host, rejected rows copied back)",
                 "matches_device_entry": same},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,

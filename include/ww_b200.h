@@ -679,8 +679,10 @@ void ww_snl1_gated(int igrid, int npts, const float* a, const float* cg, const f
                    float* s, float* d, int* accepted, void* stream);
 /* The gated W3SNL1 on host arrays, as ww_snl1 (ww_kokkos_c.hpp:115-116) takes them: the
  * copies in and out are pipelined with the compute in chunks of 65,536 points on three slots
- * (page-locked caller memory copies fastest); D is 0 where the surrogate was kept. Synchronous.
- * Status in ww_sur_last_error(). */
+ * (page-locked caller memory copies fastest); D is 0 where the surrogate was kept. Only S and
+ * the rejected points' D rows cross the bus: host threads clear D while the device works (a
+ * chunk rejecting more than 8,192 points brings its whole D). Synchronous. Status in
+ * ww_sur_last_error(). */
 void ww_snl1_gated_host(int igrid, int npts, const float* a, const float* cg,
                         const float* kdmean, float* s, float* d);
 /* The network alone: out fp32 (rows x the padded output width, NSPEC + 1 rounded up to 64)

@@ -259,18 +259,52 @@ def test_training_gains_over_the_untrained_network(model, sur):
     assert cal1["mean_err_gated"] <= 0.02 + 1e-6
 
 
-def test_gated_host_entry_equals_device_entry(model, dia):
-    """ww_snl1_gated_host (host arrays, copies pipelined over three chunk slots) gives the
-    device entry's bits, on a batch of three chunks with a partial gate."""
+def _gated_device(model, n, a, cg, kd):
+    import torch
+
+    s = torch.zeros(n, 1296, device="cuda")
+    d = torch.zeros_like(s)
+    acc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    model.gated(n, a, cg, kd, s, d, acc)
+    torch.cuda.synchronize()
+    return s, d, acc
+
+
+@pytest.mark.parametrize("gate", ["open", "few", "many"])
+def test_gated_host_entry_equals_device_entry(model, dia, gate):
+    """ww_snl1_gated_host (host arrays, copies pipelined over three chunk slots, D cleared on
+    the host and only the rejected points' rows copied back) gives the device entry's bits, on a
+    batch of three chunks: with no point rejected, with a few (the packed rows), and with more
+    than a chunk's packed rows hold (the whole D of such chunks)."""
     import torch
 
     n = 150_000
     a, cg, kd = _inputs(model, n, seed=34)
-    model.gate(0.05, 1e30)
-    s = torch.zeros(n, 1296, device="cuda")
-    d = torch.zeros_like(s)
-    model.gated(n, a, cg, kd, s, d)
+    if gate == "open":
+        model.gate(1e30, 1e30)
+    elif gate == "many":
+        model.gate(0.05, 1e30)
+    else:
+        # a log-error threshold that rejects a few percent of the points (bisection on the
+        # device entry's count)
+        lo, hi = -50.0, 50.0
+        for _ in range(30):
+            mid = 0.5 * (lo + hi)
+            model.gate(1e30, mid)
+            _, _, acc = _gated_device(model, n, a, cg, kd)
+            frac = 1.0 - float(acc.float().mean())
+            if frac > 0.06:
+                lo = mid
+            elif frac < 0.01:
+                hi = mid
+            else:
+                break
+    s, d, acc = _gated_device(model, n, a, cg, kd)
     nrej = model.fallback_count()
+    if gate == "open":
+        assert nrej == 0
+    elif gate == "few":
+        assert 0 < nrej <= n // 8
     h = [t.cpu().pin_memory() for t in (a, cg, kd)]
     hs = torch.full((n, 1296), float("nan")).pin_memory()
     hd = torch.full((n, 1296), float("nan")).pin_memory()

@@ -24,6 +24,7 @@
 #include <map>
 #include <memory>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "mlp.cuh"
@@ -382,15 +383,25 @@ struct Sur {
   // host-pointer entry: three chunk slots, copies in and out overlapping the compute
   struct Pipe {
     static constexpr int kSlots = 3;
+    /// Rows of D per chunk that come back packed (the rejected points'); a chunk with more
+    /// rejected points brings its whole D back.
+    static constexpr int kDRows = kInferRows / 8;
     cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
     cudaEvent_t copied[kSlots] = {}, computed[kSlots] = {}, drained[kSlots] = {};
-    DBuf<float> a[kSlots], cg[kSlots], kd[kSlots], s[kSlots], d[kSlots];
+    DBuf<float> a[kSlots], cg[kSlots], kd[kSlots], s[kSlots], d[kSlots], dc[kSlots];
+    DBuf<int> dl[kSlots], dn[kSlots];
+    float* h_dc[kSlots] = {};  ///< page-locked: the packed D rows of the slot's chunk
+    int* h_dl[kSlots] = {};    ///< their point indices in the chunk
+    int* h_dn[kSlots] = {};    ///< the chunk's count of rejected points
     bool ready = false;
     ~Pipe() {
       for (int k = 0; k < kSlots; ++k) {
         if (copied[k]) cudaEventDestroy(copied[k]);
         if (computed[k]) cudaEventDestroy(computed[k]);
         if (drained[k]) cudaEventDestroy(drained[k]);
+        if (h_dc[k]) cudaFreeHost(h_dc[k]);
+        if (h_dl[k]) cudaFreeHost(h_dl[k]);
+        if (h_dn[k]) cudaFreeHost(h_dn[k]);
       }
       for (cudaStream_t x : {in, comp, out})
         if (x) cudaStreamDestroy(x);
@@ -1059,29 +1070,85 @@ void ww_snl1_gated_host(int igrid, int npts, const float* a, const float* cg,
         P.kd[k].alloc(kInferRows);
         P.s[k].alloc(kInferRows * nspec);
         P.d[k].alloc(kInferRows * nspec);
+        P.dc[k].alloc(static_cast<size_t>(Sur::Pipe::kDRows) * nspec);
+        P.dl[k].alloc(Sur::Pipe::kDRows);
+        P.dn[k].alloc(1);
+        WWB_CHECK(cudaHostAlloc(&P.h_dc[k], sizeof(float) * Sur::Pipe::kDRows * nspec,
+                                cudaHostAllocDefault));
+        WWB_CHECK(cudaHostAlloc(&P.h_dl[k], sizeof(int) * Sur::Pipe::kDRows, cudaHostAllocDefault));
+        WWB_CHECK(cudaHostAlloc(&P.h_dn[k], sizeof(int), cudaHostAllocDefault));
       }
       P.ready = true;
     }
     timers::Region t_call("snl1.gated.call");
+    // D is zero for the accepted points (the surrogate does not model the diagonal term): host
+    // threads clear the caller's D while the device works, and only the rejected points' rows
+    // cross the bus, packed on the device (at most kDRows a chunk; a chunk with more brings its
+    // whole D). S crosses whole.
+    const size_t dbytes = static_cast<size_t>(npts) * nspec * sizeof(float);
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthr = static_cast<int>(std::max(1u, std::min(16u, hw == 0 ? 4u : hw)));
+    std::vector<std::thread> zeroers;
+    for (int t = 0; t < nthr; ++t) {
+      const size_t b0 = dbytes * t / nthr, b1 = dbytes * (t + 1) / nthr;
+      zeroers.emplace_back([=] { std::memset(reinterpret_cast<char*>(d) + b0, 0, b1 - b0); });
+    }
+    bool zeroed = false;
+    auto join_zeroers = [&] {
+      if (zeroed) return;
+      for (auto& th : zeroers) th.join();
+      zeroed = true;
+    };
+    // The rejected rows of chunk cc (slot k) into the caller's D, once its copies are done.
+    auto place_d = [&](int cc, int k) {
+      WWB_CHECK(cudaEventSynchronize(P.drained[k]));
+      join_zeroers();
+      const size_t p0 = static_cast<size_t>(cc) * kInferRows;
+      const size_t n = std::min(static_cast<size_t>(kInferRows), static_cast<size_t>(npts) - p0);
+      const int cnt = *P.h_dn[k];
+      if (cnt <= Sur::Pipe::kDRows) {
+        for (int i = 0; i < cnt; ++i)
+          std::memcpy(d + (p0 + static_cast<size_t>(P.h_dl[k][i])) * nspec,
+                      P.h_dc[k] + static_cast<size_t>(i) * nspec, nspec * sizeof(float));
+      } else {
+        WWB_CHECK(cudaMemcpy(d + p0 * nspec, P.d[k].p, n * nspec * sizeof(float),
+                             cudaMemcpyDeviceToHost));
+      }
+    };
     // Chunk c: copy in on `in`, compute on `comp`, copy out on `out`, slot c % 3; a slot is
-    // refilled only after its previous chunk's results left (the event of its copy out).
+    // refilled only after its previous chunk's results left and its D rows were placed.
     int c = 0;
-    for (int p0 = 0; p0 < npts; p0 += kInferRows, ++c) {
-      const int k = c % Sur::Pipe::kSlots;
-      const size_t n = static_cast<size_t>(std::min(kInferRows, npts - p0));
-      WWB_CHECK(cudaStreamWaitEvent(P.in, P.drained[k], 0));
-      WWB_CHECK(cudaMemcpyAsync(P.a[k].p, a + p0 * nspec, n * nspec * 4, cudaMemcpyHostToDevice, P.in));
-      WWB_CHECK(cudaMemcpyAsync(P.cg[k].p, cg + p0 * nk, n * nk * 4, cudaMemcpyHostToDevice, P.in));
-      WWB_CHECK(cudaMemcpyAsync(P.kd[k].p, kdmean + p0, n * 4, cudaMemcpyHostToDevice, P.in));
-      WWB_CHECK(cudaEventRecord(P.copied[k], P.in));
-      WWB_CHECK(cudaStreamWaitEvent(P.comp, P.copied[k], 0));
-      sur_apply(S, static_cast<int>(n), P.a[k].p, P.cg[k].p, P.kd[k].p, P.s[k].p, P.d[k].p,
-                nullptr, S.gate, P.comp, true, c == 0);
-      WWB_CHECK(cudaEventRecord(P.computed[k], P.comp));
-      WWB_CHECK(cudaStreamWaitEvent(P.out, P.computed[k], 0));
-      WWB_CHECK(cudaMemcpyAsync(s + p0 * nspec, P.s[k].p, n * nspec * 4, cudaMemcpyDeviceToHost, P.out));
-      WWB_CHECK(cudaMemcpyAsync(d + p0 * nspec, P.d[k].p, n * nspec * 4, cudaMemcpyDeviceToHost, P.out));
-      WWB_CHECK(cudaEventRecord(P.drained[k], P.out));
+    int placed = 0;  // chunks whose D rows are in the caller's D
+    try {
+      for (int p0 = 0; p0 < npts; p0 += kInferRows, ++c) {
+        const int k = c % Sur::Pipe::kSlots;
+        if (c >= Sur::Pipe::kSlots) place_d(placed++, k);
+        const size_t n = static_cast<size_t>(std::min(kInferRows, npts - p0));
+        WWB_CHECK(cudaStreamWaitEvent(P.in, P.drained[k], 0));
+        WWB_CHECK(cudaMemcpyAsync(P.a[k].p, a + p0 * nspec, n * nspec * 4, cudaMemcpyHostToDevice, P.in));
+        WWB_CHECK(cudaMemcpyAsync(P.cg[k].p, cg + p0 * nk, n * nk * 4, cudaMemcpyHostToDevice, P.in));
+        WWB_CHECK(cudaMemcpyAsync(P.kd[k].p, kdmean + p0, n * 4, cudaMemcpyHostToDevice, P.in));
+        WWB_CHECK(cudaEventRecord(P.copied[k], P.in));
+        WWB_CHECK(cudaStreamWaitEvent(P.comp, P.copied[k], 0));
+        sur_apply(S, static_cast<int>(n), P.a[k].p, P.cg[k].p, P.kd[k].p, P.s[k].p, P.d[k].p,
+                  nullptr, S.gate, P.comp, true, c == 0);
+        gather_listed_rows(S.nrej.p, S.rej_all.p, Sur::Pipe::kDRows, static_cast<int>(nspec),
+                           P.d[k].p, P.dc[k].p, P.dl[k].p, P.dn[k].p, P.comp);
+        WWB_CHECK(cudaEventRecord(P.computed[k], P.comp));
+        WWB_CHECK(cudaStreamWaitEvent(P.out, P.computed[k], 0));
+        WWB_CHECK(cudaMemcpyAsync(s + p0 * nspec, P.s[k].p, n * nspec * 4, cudaMemcpyDeviceToHost, P.out));
+        WWB_CHECK(cudaMemcpyAsync(P.h_dn[k], P.dn[k].p, sizeof(int), cudaMemcpyDeviceToHost, P.out));
+        WWB_CHECK(cudaMemcpyAsync(P.h_dl[k], P.dl[k].p, sizeof(int) * Sur::Pipe::kDRows,
+                                  cudaMemcpyDeviceToHost, P.out));
+        WWB_CHECK(cudaMemcpyAsync(P.h_dc[k], P.dc[k].p,
+                                  sizeof(float) * Sur::Pipe::kDRows * nspec,
+                                  cudaMemcpyDeviceToHost, P.out));
+        WWB_CHECK(cudaEventRecord(P.drained[k], P.out));
+      }
+      for (; placed < c; ++placed) place_d(placed, placed % Sur::Pipe::kSlots);
+    } catch (...) {
+      join_zeroers();
+      throw;
     }
     WWB_CHECK(cudaStreamSynchronize(P.out));
     WWB_CHECK(cudaStreamSynchronize(P.comp));

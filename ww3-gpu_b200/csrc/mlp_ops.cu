@@ -970,6 +970,25 @@ void targets(const SurGrid& g, int npts, const float* s, const float* ps, const 
   WWB_CHECK(cudaGetLastError());
 }
 
+namespace {
+
+__global__ void gather_rows_kernel(const int* __restrict__ count, const int* __restrict__ rows,
+                                   int cap, int width, const float* __restrict__ src,
+                                   float* __restrict__ dst, int* __restrict__ list_dst,
+                                   int* __restrict__ count_dst) {
+  const int n = *count;
+  const int m = n < cap ? n : cap;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *count_dst = n;
+  for (int i = blockIdx.x; i < m; i += gridDim.x) {
+    const int r = rows[i];
+    if (threadIdx.x == 0) list_dst[i] = r;
+    const float4* s4 = reinterpret_cast<const float4*>(src + static_cast<size_t>(r) * width);
+    float4* d4 = reinterpret_cast<float4*>(dst + static_cast<size_t>(i) * width);
+    for (int j = threadIdx.x; j < width / 4; j += blockDim.x) d4[j] = s4[j];
+  }
+}
+}  // namespace
+
 void gate_points(const GateParams& gate, int npts, const float* gsum, const float* head,
                  int* accepted, float* gv, int* rej_list, int* nrej, int* nrej_total,
                  cudaStream_t st, int base) {
@@ -1066,5 +1085,17 @@ void dia_f64_judge(const DiaF64& t, int npts, const float* a, const float* cg,
   WWB_CHECK(cudaGetLastError());
 }
 
+}  // namespace mlp
+}  // namespace wwb
+
+namespace wwb {
+namespace mlp {
+void gather_listed_rows(const int* count, const int* rows, int cap, int width, const float* src,
+                        float* dst, int* list_dst, int* count_dst, cudaStream_t st) {
+  if (width % 4 != 0)
+    throw CudaError(cudaErrorInvalidValue, "gather_listed_rows: row width not a multiple of 4");
+  gather_rows_kernel<<<512, 256, 0, st>>>(count, rows, cap, width, src, dst, list_dst, count_dst);
+  WWB_CHECK(cudaGetLastError());
+}
 }  // namespace mlp
 }  // namespace wwb

@@ -85,6 +85,12 @@ void gate_points(const GateParams& gate, int npts, const float* gsum, const floa
                  int* accepted, float* gv, int* rej_list, int* nrej, int* nrej_total,
                  cudaStream_t st, int base = 0);
 
+/// The rows of `rows` (a list of *count entries) of src (rows of `width` floats) packed into
+/// dst, at most `cap` of them, with the list's entries into list_dst and *count into count_dst:
+/// the rejected points' D of one chunk, for a copy to the host of those rows alone.
+void gather_listed_rows(const int* count, const int* rows, int cap, int width, const float* src,
+                        float* dst, int* list_dst, int* count_dst, cudaStream_t st);
+
 /// Training loss and the output gradient. out (m x ldo fp32), t (m x ldt): grad (m x dout bf16)
 /// = dL/dout; loss (3 floats: MSE, energy-budget, error-head terms) accumulated.
 struct LossWeights {
