@@ -1089,9 +1089,14 @@ void ww_snl1_gated_host(int igrid, int npts, const float* a, const float* cg,
     const unsigned hw = std::thread::hardware_concurrency();
     const int nthr = static_cast<int>(std::max(1u, std::min(16u, hw == 0 ? 4u : hw)));
     std::vector<std::thread> zeroers;
-    for (int t = 0; t < nthr; ++t) {
-      const size_t b0 = dbytes * t / nthr, b1 = dbytes * (t + 1) / nthr;
-      zeroers.emplace_back([=] { std::memset(reinterpret_cast<char*>(d) + b0, 0, b1 - b0); });
+    try {
+      for (int t = 0; t < nthr; ++t) {
+        const size_t b0 = dbytes * t / nthr, b1 = dbytes * (t + 1) / nthr;
+        zeroers.emplace_back([=] { std::memset(reinterpret_cast<char*>(d) + b0, 0, b1 - b0); });
+      }
+    } catch (...) {  // a thread that could not start: the started ones finish first
+      for (auto& th : zeroers) th.join();
+      throw;
     }
     bool zeroed = false;
     auto join_zeroers = [&] {
